@@ -1,0 +1,263 @@
+"""ctypes wrapper around the CPU oracle (``oracle/_build/libtcloth_oracle.so``).
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py``.  The product never imports it.
+
+``OracleSim`` mirrors the constructor and setters of the reference's
+``taremin_cloth_core.ClothSimulator`` (crates/cloth_py/src/lib.rs:1556-1767)
+so parity tests read like the reference's own tests.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libtcloth_oracle.so")
+_lib = None
+
+_f = np.float32
+_u = np.uint32
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        P = C.c_void_p
+        fp = np.ctypeslib.ndpointer(dtype=_f, flags="C_CONTIGUOUS")
+        up = np.ctypeslib.ndpointer(dtype=_u, flags="C_CONTIGUOUS")
+        L.ocl_create.restype = P
+        L.ocl_create.argtypes = [P, C.c_int, P, C.c_int, P, C.c_int, P, P, P, C.c_uint32,
+                                 C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]
+        L.ocl_destroy.argtypes = [P]
+        for name, n in [("ocl_set_gravity", 3), ("ocl_set_damping_all", 4), ("ocl_set_compliance_all", 4)]:
+            getattr(L, name).argtypes = [P] + [C.c_float] * n
+        L.ocl_set_damping.argtypes = [P, C.c_float]
+        L.ocl_set_solver_iterations.argtypes = [P, C.c_int]
+        L.ocl_set_enable_self_collision.argtypes = [P, C.c_int]
+        L.ocl_set_coupled_collider.argtypes = [P, C.c_int]
+        L.ocl_set_self_collision_options.argtypes = [P, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int]
+        L.ocl_add_sphere.argtypes = [P, fp, C.c_float, C.c_float, C.c_float]
+        L.ocl_add_capsule.argtypes = [P, fp, fp, C.c_float, C.c_float, C.c_float]
+        L.ocl_add_plane.argtypes = [P, fp, fp, C.c_float, C.c_float]
+        L.ocl_set_mesh_triangles.argtypes = [P, fp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_int, P]
+        L.ocl_clear_colliders.argtypes = [P]
+        L.ocl_set_pin.argtypes = [P, C.c_uint32, fp, C.c_float]
+        L.ocl_clear_pins.argtypes = [P]
+        L.ocl_step.argtypes = [P, C.c_float, C.c_int]
+        L.ocl_num_vertices.argtypes = [P]
+        L.ocl_num_vertices.restype = C.c_int
+        L.ocl_get_positions.argtypes = [P, fp]
+        L.ocl_get_state.argtypes = [P, P, P, P]
+        L.ocl_set_state.argtypes = [P, fp, P]
+        L.ocl_counts.argtypes = [P, np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")]
+        L.ocl_get_distance.argtypes = [P, up, fp, fp, fp, up]
+        L.ocl_get_bending.argtypes = [P, up, fp, fp, fp]
+        L.ocl_get_dist_colors.argtypes = [P, up, up]
+        L.ocl_get_bend_colors.argtypes = [P, up, up]
+        L.ocl_get_edges.argtypes = [P, up, up]
+        L.ocl_topology_sizes.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.ocl_topology_sizes.restype = C.c_int
+        L.ocl_get_topology.argtypes = [P, up, up, up, up, fp, fp, up, up, up, up]
+        L.ocl_cell_size.argtypes = [P]
+        L.ocl_cell_size.restype = C.c_float
+        L.ocl_build_hash.argtypes = [P, C.c_int, up, up]
+        L.ocl_get_mesh_triangles.argtypes = [P, fp]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class OracleSim:
+    """Sequential CPU restatement of GpuClothSimulator (test oracle)."""
+
+    def __init__(self, positions, edges, faces=None, inv_masses=None, layer_ids=None,
+                 thicknesses=None, layer_id=0, thickness=0.005, stiffness=1000.0,
+                 bending_stiffness=10.0, compression_stiffness=None, shear_stiffness=None):
+        L = lib()
+        self._keep = []
+        pos = np.ascontiguousarray(positions, dtype=_f).reshape(-1, 3)
+        e = np.ascontiguousarray(edges, dtype=_u).reshape(-1, 2)
+        f = None if faces is None else np.ascontiguousarray(faces, dtype=_u).reshape(-1, 3)
+        im = None if inv_masses is None else np.ascontiguousarray(inv_masses, dtype=_f)
+        li = None if layer_ids is None else np.ascontiguousarray(layer_ids, dtype=_u)
+        th = None if thicknesses is None else np.ascontiguousarray(thicknesses, dtype=_f)
+        comp = stiffness if compression_stiffness is None else compression_stiffness
+        shear = stiffness * 0.5 if shear_stiffness is None else shear_stiffness
+        self.n = pos.shape[0]
+        self._h = L.ocl_create(_ptr(pos), pos.shape[0], _ptr(e), e.shape[0], _ptr(f),
+                               0 if f is None else f.shape[0], _ptr(im), _ptr(li), _ptr(th),
+                               layer_id, thickness, stiffness, comp, shear, bending_stiffness)
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().ocl_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    # --- setters -----------------------------------------------------
+    def set_gravity(self, gx, gy, gz):
+        lib().ocl_set_gravity(self._h, gx, gy, gz)
+
+    def set_damping(self, d):
+        lib().ocl_set_damping(self._h, d)
+
+    def set_damping_all(self, t, c, s, b):
+        lib().ocl_set_damping_all(self._h, t, c, s, b)
+
+    def set_solver_iterations(self, n):
+        lib().ocl_set_solver_iterations(self._h, int(n))
+
+    def set_enable_self_collision(self, on):
+        lib().ocl_set_enable_self_collision(self._h, int(bool(on)))
+
+    def set_coupled_collider(self, on):
+        lib().ocl_set_coupled_collider(self._h, int(bool(on)))
+
+    def set_self_collision_options(self, relief_factor=0.2, max_displacement_ratio=0.2,
+                                   exclude_neighbors=True, enable_normal_untangling=True,
+                                   max_iterations=128):
+        lib().ocl_set_self_collision_options(self._h, relief_factor, max_displacement_ratio,
+                                             int(exclude_neighbors), int(enable_normal_untangling),
+                                             int(max_iterations))
+
+    def set_compliance_all(self, tension, compression, shear, bending):
+        lib().ocl_set_compliance_all(self._h, tension, compression, shear, bending)
+
+    def add_sphere_collider(self, center, radius, friction=0.0, restitution=0.0):
+        lib().ocl_add_sphere(self._h, np.asarray(center, _f), radius, friction, restitution)
+
+    def add_capsule_collider(self, point_a, point_b, radius, friction=0.0, restitution=0.0):
+        lib().ocl_add_capsule(self._h, np.asarray(point_a, _f), np.asarray(point_b, _f), radius,
+                              friction, restitution)
+
+    def add_plane_collider(self, point, normal, friction=0.0, restitution=0.0):
+        lib().ocl_add_plane(self._h, np.asarray(point, _f), np.asarray(normal, _f), friction,
+                            restitution)
+
+    def set_mesh_collider_triangles(self, triangles, friction=0.3, thickness=0.01, restitution=0.0,
+                                    single_sided=True, attributes=None):
+        t = np.ascontiguousarray(triangles, dtype=_f).reshape(-1, 9)
+        a = None if attributes is None else np.ascontiguousarray(attributes, dtype=_f)
+        self._keep = [t, a]
+        lib().ocl_set_mesh_triangles(self._h, t, t.shape[0], friction, thickness, restitution,
+                                     int(single_sided), _ptr(a))
+
+    def clear_colliders(self):
+        lib().ocl_clear_colliders(self._h)
+
+    def set_pin(self, vertex_idx, target_pos, weight=1.0):
+        lib().ocl_set_pin(self._h, int(vertex_idx), np.asarray(target_pos, _f), weight)
+
+    def clear_pins(self):
+        lib().ocl_clear_pins(self._h)
+
+    # --- stepping / state -----------------------------------------------
+    def step(self, dt=1.0 / 60.0, substeps=None, solver_iterations=None):
+        if solver_iterations is not None:
+            self.set_solver_iterations(solver_iterations)
+        lib().ocl_step(self._h, dt, 0 if substeps is None else int(substeps))
+        return 20 if substeps is None else int(substeps)
+
+    def get_positions(self, out=None):
+        o = np.empty(self.n * 3, _f) if out is None else out
+        lib().ocl_get_positions(self._h, o)
+        return o
+
+    def get_state(self):
+        x = np.empty((self.n, 3), _f)
+        p = np.empty((self.n, 3), _f)
+        v = np.empty((self.n, 3), _f)
+        lib().ocl_get_state(self._h, _ptr(x), _ptr(p), _ptr(v))
+        return x, p, v
+
+    def set_state(self, x, v=None):
+        x = np.ascontiguousarray(x, _f).reshape(-1)
+        vv = None if v is None else np.ascontiguousarray(v, _f).reshape(-1)
+        lib().ocl_set_state(self._h, x, _ptr(vv))
+
+    # --- introspection --------------------------------------------------
+    def counts(self):
+        o = np.zeros(8, np.int32)
+        lib().ocl_counts(self._h, o)
+        keys = ["nd", "nb", "n_dist_colors", "n_bend_colors", "n_edges", "table_size",
+                "num_virtual", "multi_layer"]
+        return dict(zip(keys, (int(v) for v in o)))
+
+    def distance_constraints(self):
+        c = self.counts()
+        nd = c["nd"]
+        v = np.zeros(2 * max(nd, 1), _u)
+        r, tc, cc = (np.zeros(max(nd, 1), _f) for _ in range(3))
+        ty = np.zeros(max(nd, 1), _u)
+        lib().ocl_get_distance(self._h, v, r, tc, cc, ty)
+        return dict(v=v[:2 * nd].reshape(-1, 2), rest=r[:nd], tc=tc[:nd], cc=cc[:nd], type=ty[:nd])
+
+    def bending_constraints(self):
+        nb = self.counts()["nb"]
+        v = np.zeros(4 * max(nb, 1), _u)
+        r, cp, p0 = (np.zeros(max(nb, 1), _f) for _ in range(3))
+        lib().ocl_get_bending(self._h, v, r, cp, p0)
+        return dict(v=v[:4 * nb].reshape(-1, 4), rest=r[:nb], comp=cp[:nb], pad0=p0[:nb])
+
+    def colors(self):
+        c = self.counts()
+        do, dc = np.zeros(max(c["n_dist_colors"], 1), _u), np.zeros(max(c["n_dist_colors"], 1), _u)
+        bo, bc = np.zeros(max(c["n_bend_colors"], 1), _u), np.zeros(max(c["n_bend_colors"], 1), _u)
+        lib().ocl_get_dist_colors(self._h, do, dc)
+        lib().ocl_get_bend_colors(self._h, bo, bc)
+        k, m = c["n_dist_colors"], c["n_bend_colors"]
+        return dict(dist_off=do[:k], dist_cnt=dc[:k], bend_off=bo[:m], bend_cnt=bc[:m])
+
+    def edges(self):
+        ne = self.counts()["n_edges"]
+        e = np.zeros(2 * max(ne, 1), _u)
+        b = np.zeros(max((ne + 31) // 32, 1), _u)
+        lib().ocl_get_edges(self._h, e, b)
+        return e[:2 * ne].reshape(-1, 2), b[:(ne + 31) // 32]
+
+    def topology(self):
+        a, t, s = C.c_int(), C.c_int(), C.c_int()
+        n = lib().ocl_topology_sizes(self._h, C.byref(a), C.byref(t), C.byref(s))
+        out = dict(adj_off=np.zeros(n + 1, _u), adj_idx=np.zeros(max(a.value, 1), _u),
+                   th_off=np.zeros(n + 1, _u), th_idx=np.zeros(max(t.value, 1), _u),
+                   th_rest=np.zeros(max(t.value, 1), _f), local_len=np.zeros(max(n, 1), _f),
+                   star_off=np.zeros(n + 1, _u), star_idx=np.zeros(2 * max(s.value, 1), _u),
+                   island=np.zeros(max(n, 1), _u), layer=np.zeros(max(n, 1), _u))
+        lib().ocl_get_topology(self._h, out["adj_off"], out["adj_idx"], out["th_off"], out["th_idx"],
+                               out["th_rest"], out["local_len"], out["star_off"], out["star_idx"],
+                               out["island"], out["layer"])
+        out["adj_idx"] = out["adj_idx"][:a.value]
+        out["th_idx"] = out["th_idx"][:t.value]
+        out["th_rest"] = out["th_rest"][:t.value]
+        out["star_idx"] = out["star_idx"][:2 * s.value].reshape(-1, 2)
+        return out
+
+    def cell_size(self):
+        return float(lib().ocl_cell_size(self._h))
+
+    def build_hash(self, which=0):
+        c = self.counts()
+        T = c["table_size"]
+        cnt = self.n if which == 0 else c["n_edges"]
+        cs = np.zeros(T + 1, _u)
+        srt = np.zeros(max(cnt, 1), _u)
+        lib().ocl_build_hash(self._h, which, cs, srt)
+        return cs, srt[:cnt]

@@ -1,0 +1,92 @@
+/*
+ * tcloth_oracle.h -- CPU oracle for the XPBD cloth substep.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library restates, as plain sequential C,
+ * the algorithm of Taremin/TareminCloth's cloth_core substep so that the
+ * CUDA product can be checked against it.  Nothing in the product links,
+ * loads or calls it; only tests/, __graft_entry__.smoke() and bench.py's
+ * CPU-baseline leg do.
+ *
+ * Parity pin: the reference's golden vectors
+ * tests/fixtures/golden_master/step_case{1,2,3}_f1.npz (< 10 um after one
+ * 20x2 frame) and case{1..4}.npz (per-frame tolerances), copied under
+ * tests/golden/ by tests/golden/make_fixtures.py.
+ *
+ * Every function cites the reference file:line it follows (paths relative
+ * to the reference project root).
+ */
+#ifndef TCLOTH_ORACLE_H
+#define TCLOTH_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OSim OSim;
+
+/* Mesh + simulator construction.  Mirrors ClothMesh::from_raw_with_opts
+ * (crates/cloth_core/src/mesh.rs:407-1377) without sewing / coarse
+ * constraints, followed by GpuClothSimulator::with_options
+ * (crates/cloth_core/src/simulation/mod.rs:363-697) and
+ * build_simulation_resources (simulation/pipelines.rs:114-912). */
+OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne,
+                 const uint32_t *faces, int nf, const float *inv_masses,
+                 const uint32_t *layer_ids, const float *thicknesses,
+                 uint32_t layer_id, float thickness, float tension_k,
+                 float compression_k, float shear_k, float bending_k);
+void ocl_destroy(OSim *s);
+
+/* setters (simulation/mod.rs, cloth_py/src/lib.rs) */
+void ocl_set_gravity(OSim *s, float gx, float gy, float gz);
+void ocl_set_damping(OSim *s, float d);
+void ocl_set_damping_all(OSim *s, float t, float c, float sh, float b);
+void ocl_set_solver_iterations(OSim *s, int it);
+void ocl_set_enable_self_collision(OSim *s, int on);
+void ocl_set_self_collision_options(OSim *s, float relief, float max_disp_ratio,
+                                    int exclude_neighbors, int untangle, int max_iter);
+void ocl_set_compliance_all(OSim *s, float tension, float compression, float shear,
+                            float bending);
+void ocl_add_sphere(OSim *s, const float *c, float r, float fric, float rest);
+void ocl_add_capsule(OSim *s, const float *a, const float *b, float r, float fric, float rest);
+void ocl_add_plane(OSim *s, const float *pt, const float *nrm, float fric, float rest);
+/* tris: T x 9 floats; attrs (nullable): T x 4 (friction, thickness, restitution, flags) */
+void ocl_set_mesh_triangles(OSim *s, const float *tris, int T, float fric, float thick,
+                            float rest, int single_sided, const float *attrs);
+void ocl_clear_colliders(OSim *s);
+void ocl_set_pin(OSim *s, uint32_t v, const float *target, float w);
+void ocl_clear_pins(OSim *s);
+void ocl_set_coupled_collider(OSim *s, int on);
+
+/* time stepping: GpuClothSimulator::step (simulation/dispatch.rs:610-671) */
+void ocl_step(OSim *s, float dt, int substeps);
+
+/* state access */
+int ocl_num_vertices(const OSim *s);
+void ocl_get_positions(const OSim *s, float *out);            /* N*3 */
+void ocl_get_state(const OSim *s, float *x, float *p, float *v); /* N*3 each */
+void ocl_set_state(OSim *s, const float *x, const float *v);
+
+/* introspection for parity tests */
+void ocl_counts(const OSim *s, int *out8);
+/* out8: [nd, nb, n_dist_colors, n_bend_colors, n_edges, table_size, num_virtual, multi_layer] */
+void ocl_get_distance(const OSim *s, uint32_t *v01, float *rest, float *tc, float *cc,
+                      uint32_t *type);
+void ocl_get_bending(const OSim *s, uint32_t *v0123, float *rest, float *comp, float *pad0);
+void ocl_get_dist_colors(const OSim *s, uint32_t *off, uint32_t *cnt);
+void ocl_get_bend_colors(const OSim *s, uint32_t *off, uint32_t *cnt);
+void ocl_get_edges(const OSim *s, uint32_t *e2, uint32_t *bits);
+int ocl_topology_sizes(const OSim *s, int *adj_n, int *twohop_n, int *star_n);
+void ocl_get_topology(const OSim *s, uint32_t *adj_off, uint32_t *adj_idx, uint32_t *th_off,
+                      uint32_t *th_idx, float *th_rest, float *local_len, uint32_t *star_off,
+                      uint32_t *star_idx, uint32_t *island, uint32_t *layer);
+float ocl_cell_size(const OSim *s);
+/* Builds the vertex (which=0) or edge (which=1) hash from the current
+ * predicted positions; outputs cell_starts (table+1) and sorted (n). */
+void ocl_build_hash(OSim *s, int which, uint32_t *cell_starts, uint32_t *sorted);
+void ocl_get_mesh_triangles(const OSim *s, float *tris16);  /* T x 16 floats (sorted) */
+
+#ifdef __cplusplus
+}
+#endif
+#endif
