@@ -1,0 +1,299 @@
+#!/usr/bin/env python
+"""Benchmark of the XPBD cloth substep on B200.
+
+Workload (one "step" = one frame): two stacked 256 x 256 sheets (131,072
+vertices, 521,220 distance + 259,080 bending constraints) dropped onto a
+20,480-triangle icosphere mesh collider with spatial-hash self-collision on,
+20 substeps x 4 iterations per frame.  Seeded synthetic inputs.
+
+Metric: vertex-substeps/s (N x substeps / device time), whole job over all
+ranks.  Multi-GPU runs are independent replicas (one cloth per GPU, no
+collective on the data path); the barrier and max-over-ranks timing use
+torch.distributed over NCCL.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "vertex-substeps/s at equal constraint residual: learned+batched vs plain XPBD"
+UNIT = "vertex-substeps/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(pass_name, sim_counts, n_tris):
+    """Compulsory DRAM/L2 bytes of one launch group of a pass (each array read
+    and written once).  Layout: x4/p4/v4 float4 records (16 B), distance
+    constraint = uint2 ids + float4 params (24 B), bending = uint4 + float4
+    (32 B), lambda 4 B, self-collision accumulator 64 B per vertex."""
+    n, nd, nb, ne = sim_counts["n"], sim_counts["nd"], sim_counts["nb"], sim_counts["n_edges"]
+    if pass_name == "distance":       # all colours of one iteration
+        return nd * (24 + 4 + 4) + 2 * nd * (16 + 16 + 16)  # constraint+lambda r/w, 2x (p read, x.w read, p write)
+    if pass_name == "bending":
+        return nb * (32 + 4 + 4) + 2 * nb * (16 + 16 + 16)
+    if pass_name == "predict":
+        return n * (16 + 16 + 16 + 16)      # x, v read; p, v write
+    if pass_name == "update_vel":
+        return n * (16 + 16 + 16 + 16 + 16)  # x, p, v read; x, v write
+    if pass_name == "collision":
+        return n * (16 + 16 + 16 + 16) + n_tris * (64 + 16)  # x, p r/w + triangles + bounds once
+    if pass_name == "sc_solve":
+        return n * (16 + 16 + 16 + 4 + 64) + 8 * 65537  # x, p, v, local len, accum + cell starts
+    if pass_name == "sc_solve_ee":
+        return ne * 8 + n * (16 + 16 + 16 + 64) + 4 * 65537
+    if pass_name == "sc_apply":
+        return n * (16 + 16 + 16 + 4 + 64 + 64)
+    if pass_name.startswith("hash"):
+        cnt = n if pass_name == "hash_vertices" else ne
+        return cnt * (16 + 4 + 4 + 4) + 65537 * 4 * 4
+    return 0
+
+
+def run_reference(args, rank):
+    """CPU implementation of the reference algorithm (the oracle, OpenMP over
+    the host's cores) on the same workload; each step is a bounded sample of
+    one substep."""
+    if rank != 0:
+        return
+    from oracle import oracle
+    from taremincloth_b200 import scenes
+    oracle.build()
+    sc = scenes.config2()
+    s = scenes.build(oracle.OracleSim, sc)
+    n = len(sc["positions"])
+    dts = sc["dt"] / sc["substeps"]
+    for _ in range(args.warmup):
+        s.step(dts, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.step(dts, 1)
+    t = time.perf_counter() - t0
+    value = n * args.steps / t
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": sc["name"] + " (one substep per step)", "vertices": n, "substeps_per_step": 1,
+                   "iterations": sc["iterations"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} substeps of the full workload, OpenMP over {cores} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample():
+    from oracle import oracle
+    from taremincloth_b200 import scenes
+    oracle.build()
+    sc = scenes.config2()
+    s = scenes.build(oracle.OracleSim, sc)
+    dts = sc["dt"] / sc["substeps"]
+    s.step(dts, 1)
+    t0 = time.perf_counter()
+    s.step(dts, 1)
+    t = time.perf_counter() - t0
+    cores = os.cpu_count()
+    return {"value": len(sc["positions"]) / t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"1 timed substep of the full workload after 1 warm-up substep, OpenMP over {cores} threads"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from taremincloth_b200 import ClothSimulator, scenes
+
+    sc = scenes.config2()
+    n = len(sc["positions"])
+    sim = scenes.build(ClothSimulator, sc, device=local)
+    dt, sub = sc["dt"], sc["substeps"]
+    counts = sim.get_counts()
+    for _ in range(max(args.warmup, 3)):
+        sim.step(dt, sub)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed region: K frames, L2 flushed before each
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        sim.step(dt, sub)
+        total_ms += sim.last_frame_ms()
+    barrier()
+    clk = clocks.stop()
+    t_max = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    total_ms = float(t_max.item())
+    value = world * n * sub * args.steps / (total_ms / 1e3)
+    kernels = sim.frame_kernel_count()
+
+    # ---- end to end through the public API: per frame upload the collider
+    # triangles from host memory, step, read positions back to host memory
+    tris = np.ascontiguousarray(sc["mesh"]["triangles"], np.float32)
+    out = np.empty(n * 3, np.float32)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.set_mesh_collider_triangles(tris, friction=0.3, thickness=0.01, single_sided=True)
+        sim.step(dt, sub)
+        sim.get_positions(out)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    t_e2e = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * sub * args.steps / float(t_e2e.item())
+
+    # ---- per-pass CUDA-event profile of two frames for the roofline
+    sim.set_residual_tracking(True)
+    sim.step(dt, sub)
+    res = sim.get_residuals()
+    sim.set_residual_tracking(False)
+    sim.set_profiling_enabled(True)
+    for _ in range(2):
+        sim.step(dt, sub)
+    prof = sim.take_profile()
+    sim.set_profiling_enabled(False)
+    prof.sort(key=lambda r: -r[1])
+    top_name, top_ms, top_launches = prof[0]
+    avg_ms = top_ms / max(top_launches, 1)
+    alg = algorithmic_bytes(top_name, counts, len(tris))
+    peak, peak_kind = peaks()
+    achieved = alg / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    traffic = None
+    tj = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tj):
+        traffic = json.load(open(tj)).get(top_name)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "two 256x256 sheets (131072 vertices) on a 20480-triangle icosphere mesh collider, "
+                               "self-collision on, 20 substeps x 4 iterations per step",
+                   "vertices": n, "substeps": sub, "iterations": sc["iterations"],
+                   "distance_constraints": counts["nd"], "bending_constraints": counts["nb"],
+                   "l2": "256 MB buffer written before every timed step", "parallelism": f"replicas x{world}",
+                   "path": "plain XPBD, CUDA graph per frame"},
+        "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs", "traffic": traffic,
+                     "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms},
+        "profile_ms_per_frame": {k: round(v / 2, 4) for k, v, _ in prof},
+        "residual": {"dist_rms": res["dist_rms_total"], "dist_max": res["dist_max_total"],
+                     "bend_rms": res["bend_rms_total"], "bend_max": res["bend_max_total"]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(tris.nbytes),
+                "d2h_bytes_per_step": int(out.nbytes)},
+        "gpu_launches": kernels * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,164 @@
+/*
+ * tcloth.h -- C ABI of the B200 XPBD cloth substep (libtcloth.so).
+ *
+ * Drop-in replacement for the device half of Taremin/TareminCloth's
+ * cloth_core: the entry points are what the crate's FFI (cloth_py's
+ * ClothSimulator, crates/cloth_py/src/lib.rs:1549-3100, over
+ * GpuClothSimulator, crates/cloth_core/src/simulation/mod.rs:57-355) binds.
+ * Plain pointers and sizes only.  Every function returns a tc_status; on a
+ * non-zero status tc_last_error() returns a thread-local message.
+ * Input arrays are copied during the call; output arrays are caller-owned.
+ * A tc_sim is used from one host thread at a time.
+ */
+#ifndef TCLOTH_H
+#define TCLOTH_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TC_OK = 0,
+  TC_ERR_INVALID = 1, /* bad shape / index / argument (PyO3 ValueError)  */
+  TC_ERR_CUDA = 2,    /* device unavailable or CUDA failure (RuntimeError) */
+  TC_ERR_NOMEM = 3,   /* device or host allocation failed                 */
+  TC_ERR_TIMEOUT = 4  /* a bounded device-side wait gave up               */
+} tc_status;
+
+typedef struct tc_sim tc_sim;
+
+/* Last error message of this thread ("" when none). */
+const char *tc_last_error(void);
+/* 1 when a CUDA device of compute capability 10.x is visible. */
+int tc_gpu_available(void);
+/* Device name of `device` into buf (nul-terminated). */
+tc_status tc_device_name(int device, char *buf, size_t len);
+
+/* ClothSimulator::new (crates/cloth_py/src/lib.rs:1556-1767) with
+ * ClothMesh::from_raw_with_opts (crates/cloth_core/src/mesh.rs:407-1377).
+ * faces, inv_masses, layer_ids, thicknesses may be NULL.  Stiffness in N/m
+ * maps to compliance 1/k (k >= 5000 -> 0, k <= 0 -> 1e10).  Indices out of
+ * range return TC_ERR_INVALID, like the reference's ValueError. */
+tc_status tc_create(tc_sim **out, const float *positions, uint32_t n, const uint32_t *edges, uint32_t ne,
+                    const uint32_t *faces, uint32_t nf, const float *inv_masses, const uint32_t *layer_ids,
+                    const float *thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
+                    float compression_stiffness, float shear_stiffness, float bending_stiffness, int device);
+tc_status tc_destroy(tc_sim *s);
+
+/* GpuClothSimulator::step (crates/cloth_core/src/simulation/dispatch.rs:610-671):
+ * one frame of `substeps` substeps (0 -> 20), synchronous.  The frame is
+ * recorded once into a CUDA graph and replayed while parameters are unchanged. */
+tc_status tc_step(tc_sim *s, float dt, uint32_t substeps, uint32_t *effective_substeps);
+/* step_async (dispatch.rs:740-806): enqueue a frame on the simulator's stream
+ * and return; fetch_positions (lib.rs:1834-1846) waits and copies. */
+tc_status tc_step_async(tc_sim *s, float dt, uint32_t substeps);
+tc_status tc_fetch_positions(tc_sim *s, float *out, size_t out_len, int *ok);
+/* get_positions (lib.rs:2110-2120): out holds n*3 floats. */
+tc_status tc_get_positions(tc_sim *s, float *out, size_t out_len);
+/* set_positions_and_velocities (dispatch.rs:953-988); vel may be NULL. */
+tc_status tc_set_positions_and_velocities(tc_sim *s, const float *pos, const float *vel, uint32_t n);
+/* reset (dispatch.rs:1411-1427) */
+tc_status tc_reset(tc_sim *s);
+
+/* parameters (simulation/mod.rs:1091-1106, :1429-1449, lib.rs:2751-2800) */
+tc_status tc_set_gravity(tc_sim *s, float gx, float gy, float gz);
+tc_status tc_set_damping(tc_sim *s, float damping);
+tc_status tc_set_damping_all(tc_sim *s, float tension, float compression, float shear, float bending);
+tc_status tc_set_solver_iterations(tc_sim *s, uint32_t iterations);
+tc_status tc_set_stiffness_all(tc_sim *s, float tension, float compression, float shear, float bending);
+/* Sets compliances directly (m/N); no stiffness mapping.  New entry point:
+ * the reference reaches compliance only through stiffness. */
+tc_status tc_set_compliance_all(tc_sim *s, float tension, float compression, float shear, float bending);
+tc_status tc_set_edge_stiffness_multipliers(tc_sim *s, const uint32_t *edge_idx, const float *mult, uint32_t count);
+tc_status tc_set_enable_self_collision(tc_sim *s, int enable);
+/* set_self_collision_options (simulation/mod.rs:920-950) */
+tc_status tc_set_self_collision_options(tc_sim *s, float relief_factor, float max_displacement_ratio,
+                                        int exclude_neighbors, int enable_normal_untangling, uint32_t max_iterations);
+tc_status tc_set_coupled_collider(tc_sim *s, int enable);
+tc_status tc_set_auto_coupled_on_low_substeps(tc_sim *s, int enable);
+tc_status tc_set_collider_options(tc_sim *s, int enable_cluster_culling, int enable_single_sided_recovery,
+                                  float sweep_margin);
+
+/* colliders (simulation/mod.rs:1571-1628, lib.rs:2157-2240) */
+tc_status tc_add_sphere_collider(tc_sim *s, const float center[3], float radius, float friction, float restitution);
+tc_status tc_add_capsule_collider(tc_sim *s, const float a[3], const float b[3], float radius, float friction,
+                                  float restitution);
+tc_status tc_add_plane_collider(tc_sim *s, const float point[3], const float normal[3], float friction,
+                                float restitution);
+/* triangles: T x 3 x 3 floats; attributes (nullable): T x 4 (friction,
+ * thickness, restitution, flags) */
+tc_status tc_set_mesh_collider_triangles(tc_sim *s, const float *triangles, uint32_t T, float friction,
+                                         float thickness, float restitution, int single_sided, const float *attributes);
+tc_status tc_clear_colliders(tc_sim *s);
+
+/* pins (simulation/mod.rs:2768-2860) */
+tc_status tc_set_pin(tc_sim *s, uint32_t vertex, const float target[3], float weight);
+tc_status tc_set_pins_batch(tc_sim *s, const uint32_t *idx, const float *targets, const float *weights, uint32_t count);
+tc_status tc_release_pin(tc_sim *s, uint32_t vertex);
+tc_status tc_clear_pins(tc_sim *s);
+tc_status tc_set_vertex_inv_masses(tc_sim *s, const uint32_t *idx, const float *inv_masses, uint32_t count);
+tc_status tc_get_vertex_inv_masses(tc_sim *s, float *out, uint32_t n);
+
+/* counts (lib.rs:2928-2950): out[8] = n, distance, bending, edges,
+ * distance colours, bending colours, hash table size, multi-layer flag */
+tc_status tc_get_counts(tc_sim *s, uint32_t out[8]);
+tc_status tc_get_cell_size(tc_sim *s, float *cell);
+
+/* ---- parity introspection (new; no reference counterpart) ---- */
+/* x, p, v: n*3 each (any may be NULL) */
+tc_status tc_get_state(tc_sim *s, float *x, float *p, float *v);
+/* colour-sorted constraints: v01 (nd*2), par (nd*4: rest, tc, cc, type),
+ * off/cnt per colour */
+tc_status tc_get_distance_constraints(tc_sim *s, uint32_t *v01, float *par, uint32_t *off, uint32_t *cnt);
+tc_status tc_get_bending_constraints(tc_sim *s, uint32_t *v0123, float *par, uint32_t *off, uint32_t *cnt);
+/* Build the spatial hash from the current predicted positions on the device
+ * (which = 0 vertices, 1 edges) and copy cell_starts (table+1) and sorted. */
+tc_status tc_get_hash_state(tc_sim *s, int which, uint32_t *cell_starts, uint32_t *sorted);
+/* Sorted unique edges (ne*2) and open-boundary bits ((ne+31)/32). */
+tc_status tc_get_edges(tc_sim *s, uint32_t *edges, uint32_t *bits);
+/* Per-colour residual |C(x) + alpha~ lambda| after the last iteration of the
+ * last substep of the latest frame, when tracking is on.  rms/max arrays are
+ * sized by the colour counts; totals[4] = dist rms, dist max, bend rms, bend max. */
+tc_status tc_set_residual_tracking(tc_sim *s, int enable);
+tc_status tc_get_residuals(tc_sim *s, float *dist_rms, float *dist_max, float *bend_rms, float *bend_max,
+                           float totals[4]);
+/* ---- host-only topology build (no device needed) ----
+ * Runs the same constraint / colouring / topology builder that tc_create
+ * uses, so the host half of the path can be checked without a GPU. */
+typedef struct tc_mesh tc_mesh;
+tc_status tc_mesh_build(tc_mesh **out, const float *positions, uint32_t n, const uint32_t *edges, uint32_t ne,
+                        const uint32_t *faces, uint32_t nf, const float *inv_masses, const uint32_t *layer_ids,
+                        const float *thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
+                        float compression_stiffness, float shear_stiffness, float bending_stiffness);
+tc_status tc_mesh_destroy(tc_mesh *m);
+/* out[10] = n, distance, bending, edges, distance colours, bending colours,
+ * table size, multi-layer flag, virtual-particle count, adjacency length;
+ * cell[1] = hash cell size */
+tc_status tc_mesh_counts(tc_mesh *m, uint32_t out[10], float *cell);
+tc_status tc_mesh_constraints(tc_mesh *m, uint32_t *dist_v01, float *dist_par, uint32_t *dist_off, uint32_t *dist_cnt,
+                              uint32_t *bend_v0123, float *bend_par, uint32_t *bend_off, uint32_t *bend_cnt);
+/* th_n = length of the two-hop CSR, star_n = number of star pairs */
+tc_status tc_mesh_topology_sizes(tc_mesh *m, uint32_t *adj_n, uint32_t *th_n, uint32_t *star_n);
+tc_status tc_mesh_topology(tc_mesh *m, uint32_t *adj_off, uint32_t *adj_idx, uint32_t *th_off, uint32_t *th_idx,
+                           float *th_rest, float *local_len, uint32_t *star_off, uint32_t *star_idx, uint32_t *island,
+                           uint32_t *layer, uint32_t *edges, uint32_t *edge_bits);
+
+/* set_profiling_enabled / take_profile (simulation/mod.rs:1038-1053): while
+ * enabled, frames run without the CUDA graph and every pass is bracketed by
+ * CUDA events.  take_profile returns, per pass, its name (names joined by
+ * newlines), total milliseconds and number of timed launch groups, then
+ * clears the record. */
+tc_status tc_set_profiling_enabled(tc_sim *s, int enable);
+tc_status tc_take_profile(tc_sim *s, char *names, size_t names_len, float *ms, uint32_t *launches,
+                          uint32_t max_entries, uint32_t *n_entries);
+/* Kernel launches in the recorded frame (kernel nodes of its CUDA graph). */
+tc_status tc_frame_kernel_count(tc_sim *s, uint32_t *count);
+/* Device time of the latest frame in milliseconds (CUDA events). */
+tc_status tc_last_frame_ms(tc_sim *s, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -909,6 +909,7 @@ void ocl_clear_pins(OSim *s) {
 /* shaders/predict.wgsl:33-55 */
 static void k_predict(OSim *s, float dt_sub) {
     float dt = fmaxf(dt_sub, 1e-8f);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < s->n; i++) {
         if (s->w[i] <= 0.0f) { s->v[i] = V3(0, 0, 0); s->p[i] = s->x[i]; }
         else {
@@ -942,6 +943,7 @@ static void k_pin(OSim *s, float dt_sub) {
 /* shaders/distance.wgsl:60-124 */
 static void k_distance(OSim *s, int cidx, float dt_sub) {
     uint32_t off = s->dc_off[cidx], cnt = s->dc_cnt[cidx];
+#pragma omp parallel for schedule(static) if (cnt > 4096)
     for (uint32_t q = 0; q < cnt; q++) {
         uint32_t ci = off + q;
         ODist *c = &s->dist[ci];
@@ -974,6 +976,7 @@ static void k_distance(OSim *s, int cidx, float dt_sub) {
 /* shaders/bending.wgsl:59-126 */
 static void k_bending(OSim *s, int cidx, float dt_sub) {
     uint32_t off = s->bc_off[cidx], cnt = s->bc_cnt[cidx];
+#pragma omp parallel for schedule(static) if (cnt > 4096)
     for (uint32_t q = 0; q < cnt; q++) {
         uint32_t ci = off + q;
         OBend *c = &s->bend[ci];
@@ -1145,6 +1148,7 @@ static void mesh_tri(const OTri *tri, float thickness, v3 xpos, v3 *p, v3 *xn, f
 }
 /* shaders/collision.wgsl:378-652 (cluster culling OFF, the default) */
 static void k_collision(OSim *s, float dt) {
+#pragma omp parallel for schedule(dynamic, 64)
     for (int i = 0; i < s->n; i++) {
         if (s->w[i] <= 0.0f) continue;
         v3 p = s->p[i];
@@ -1206,6 +1210,7 @@ static void k_collision(OSim *s, float dt) {
 /* shaders/update_vel.wgsl:33-53 */
 static void k_update_vel(OSim *s, float dt_sub) {
     float dt = fmaxf(dt_sub, 1e-8f);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < s->n; i++) {
         if (s->w[i] > 0.0f) s->v[i] = vdiv(vsub(s->p[i], s->x[i]), dt);
         else s->v[i] = V3(0, 0, 0);
@@ -1214,6 +1219,7 @@ static void k_update_vel(OSim *s, float dt_sub) {
 }
 /* shaders/compute_normals.wgsl:25-58 */
 static void k_normals(OSim *s) {
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < s->n; i++) {
         v3 pi = s->x[i];
         v3 sum = V3(0, 0, 0);
@@ -1263,31 +1269,42 @@ static void build_hash(OSim *s, int which) {
     free(key); free(count);
 }
 static inline int32_t to_fixed(float x) { return f2i(clampf(x * 1000000.0f, -50000000.0f, 50000000.0f)); }
-static inline void acc_add(int32_t *a, int32_t v) { *a = (int32_t)((uint32_t)*a + (uint32_t)v); }
+/* Integer accumulation is order-free; with OpenMP threads the updates are
+ * atomic, so threaded and serial runs give identical bits. */
+static inline void acc_add(int32_t *a, int32_t v) { __atomic_fetch_add((uint32_t *)a, (uint32_t)v, __ATOMIC_RELAXED); }
+static inline void acc_inc(int32_t *a) { __atomic_fetch_add((uint32_t *)a, 1u, __ATOMIC_RELAXED); }
+static inline void acc_max(int32_t *a, int32_t v) {
+    int32_t cur = __atomic_load_n(a, __ATOMIC_RELAXED);
+    while (v > cur && !__atomic_compare_exchange_n(a, &cur, v, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {}
+}
+static inline void acc_min(int32_t *a, int32_t v) {
+    int32_t cur = __atomic_load_n(a, __ATOMIC_RELAXED);
+    while (v < cur && !__atomic_compare_exchange_n(a, &cur, v, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {}
+}
 /* add_disp_atomic, shaders/self_collision.wgsl:77-85 */
 static void add_disp(OSim *s, uint32_t v, v3 d) {
     int32_t *a = s->acc + (size_t)v * A_N;
     acc_add(&a[A_DX], to_fixed(d.x)); acc_add(&a[A_DY], to_fixed(d.y)); acc_add(&a[A_DZ], to_fixed(d.z));
-    a[A_CNT] = (int32_t)((uint32_t)a[A_CNT] + 1u);
+    acc_inc(&a[A_CNT]);
 }
 /* add_pin_disp_atomic, shaders/self_collision.wgsl:87-95 */
 static void add_pin(OSim *s, uint32_t v, v3 d) {
     int32_t *a = s->acc + (size_t)v * A_N;
     acc_add(&a[A_PDX], to_fixed(d.x)); acc_add(&a[A_PDY], to_fixed(d.y)); acc_add(&a[A_PDZ], to_fixed(d.z));
-    a[A_PCNT] = (int32_t)((uint32_t)a[A_PCNT] + 1u);
+    acc_inc(&a[A_PCNT]);
 }
 /* add_ccd_atomic, shaders/self_collision.wgsl:97-118 and
  * shaders/self_collision_ee_direct.wgsl:97-125 (count_ee variant) */
 static void add_ccd(OSim *s, uint32_t v, v3 d, int count_ee) {
     int32_t *a = s->acc + (size_t)v * A_N;
     int32_t ix = to_fixed(d.x), iy = to_fixed(d.y), iz = to_fixed(d.z);
-    if (ix > 0) { if (ix > a[A_CPX]) a[A_CPX] = ix; } else if (ix < 0) { if (ix < a[A_CNX]) a[A_CNX] = ix; }
-    if (iy > 0) { if (iy > a[A_CPY]) a[A_CPY] = iy; } else if (iy < 0) { if (iy < a[A_CNY]) a[A_CNY] = iy; }
-    if (iz > 0) { if (iz > a[A_CPZ]) a[A_CPZ] = iz; } else if (iz < 0) { if (iz < a[A_CNZ]) a[A_CNZ] = iz; }
+    if (ix > 0) acc_max(&a[A_CPX], ix); else if (ix < 0) acc_min(&a[A_CNX], ix);
+    if (iy > 0) acc_max(&a[A_CPY], iy); else if (iy < 0) acc_min(&a[A_CNY], iy);
+    if (iz > 0) acc_max(&a[A_CPZ], iz); else if (iz < 0) acc_min(&a[A_CNZ], iz);
     if (count_ee) {
         float lf = clampf(vlen(d) * 1000000.0f, 0.0f, 2000000000.0f);
         uint32_t u = lf != lf ? 0u : (uint32_t)lf;
-        if (u > 0u) a[A_EEC] = (int32_t)((uint32_t)a[A_EEC] + 1u);
+        if (u > 0u) acc_inc(&a[A_EEC]);
     }
 }
 static int th_search(const OSim *s, uint32_t a, uint32_t b, uint32_t *pos) {
@@ -1326,6 +1343,7 @@ static inline int cell_eq(const int32_t *a, int32_t x, int32_t y, int32_t z) { r
 /* sc_solve, shaders/self_collision.wgsl:317-681 */
 static void k_sc_solve(OSim *s, int untangle) {
     const float cs = s->cell;
+#pragma omp parallel for schedule(dynamic, 64)
     for (uint32_t index = 0; index < (uint32_t)s->n; index++) {
         float wi = s->w[index];
         int pin_i = wi <= 0.0f;
@@ -1554,6 +1572,7 @@ static int th_range_has(const OSim *s, uint32_t start, uint32_t end, uint32_t b)
     return 0;
 }
 static void k_untangle(OSim *s) {
+#pragma omp parallel for schedule(dynamic, 64)
     for (uint32_t index = 0; index < (uint32_t)s->n; index++) {
         int32_t *ai = s->acc + (size_t)index * A_N;
         uint32_t cand = (uint32_t)ai[A_UT];
@@ -1717,6 +1736,7 @@ static inline int ebit(const OSim *s, uint32_t e) { return (s->ebits[e >> 5] >> 
 /* sc_solve_ee, shaders/self_collision_ee_direct.wgsl:266-776 */
 static void k_ee(OSim *s, int untangle) {
     const float cs = s->cell;
+#pragma omp parallel for schedule(dynamic, 64)
     for (uint32_t ei = 0; ei < (uint32_t)s->ne; ei++) {
         uint32_t u0 = s->edges[2 * ei], u1 = s->edges[2 * ei + 1];
         float w_u0 = s->w[u0], w_u1 = s->w[u1];
@@ -1732,10 +1752,11 @@ static void k_ee(OSim *s, int untangle) {
         v3 pmid = vmul(vadd(p_u0, p_u1), 0.5f);
         int32_t base[3]; cell_of(pmid, cs, base);
         uint32_t search = 0;
+        int stop = 0;
         uint32_t la = s->layer[u0];
-        for (int dz = -1; dz <= 1; dz++)
-        for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++) {
+        for (int dz = -1; dz <= 1 && !stop; dz++)
+        for (int dy = -1; dy <= 1 && !stop; dy++)
+        for (int dx = -1; dx <= 1 && !stop; dx++) {
             int32_t nx = base[0] + dx, ny = base[1] + dy, nz = base[2] + dz;
             uint32_t h = hash3(nx, ny, nz, s->table);
             uint32_t st = s->ecs[h], en = s->ecs[h + 1];
@@ -1755,7 +1776,7 @@ static void k_ee(OSim *s, int untangle) {
                 if (amin.x > bmax.x || amin.y > bmax.y || amin.z > bmax.z ||
                     amax.x < bmin.x || amax.y < bmin.y || amax.z < bmin.z) continue;
                 search++;
-                if (search > (uint32_t)s->max_search) goto next_edge;
+                if (search > (uint32_t)s->max_search) { stop = 1; break; }
                 float w_j = s->w[j], w_vj = s->w[vj];
                 float thj = s->thick[j], thvj = s->thick[vj];
                 uint32_t lb = s->layer[j];
@@ -1960,12 +1981,12 @@ static void k_ee(OSim *s, int untangle) {
                 }
             }
         }
-    next_edge:;
     }
 }
 
 /* sc_apply, shaders/self_collision_apply.wgsl:57-177 */
 static void k_apply(OSim *s) {
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < s->n; i++) {
         int32_t *a = s->acc + (size_t)i * A_N;
         int pinned = s->w[i] <= 0.0f;

@@ -1,0 +1,110 @@
+"""Loader for the in-tree CUDA library ``libtcloth.so`` (C ABI in include/tcloth.h).
+
+There is no CPU fallback: importing works without a GPU (so the C ABI can be
+inspected), but creating a simulator fails with ``RuntimeError`` when the
+library is missing or no CUDA device is visible.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtcloth.so")
+
+TC_OK, TC_ERR_INVALID, TC_ERR_CUDA, TC_ERR_NOMEM, TC_ERR_TIMEOUT = range(5)
+
+_P = C.c_void_p
+_U = C.c_uint32
+_F = C.c_float
+_I = C.c_int
+
+# name -> argtypes (all return tc_status unless listed in _RESTYPES)
+SIGNATURES = {
+    "tc_last_error": [],
+    "tc_gpu_available": [],
+    "tc_device_name": [_I, C.c_char_p, C.c_size_t],
+    "tc_create": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F, _I],
+    "tc_destroy": [_P],
+    "tc_step": [_P, _F, _U, C.POINTER(_U)],
+    "tc_step_async": [_P, _F, _U],
+    "tc_fetch_positions": [_P, _P, C.c_size_t, C.POINTER(_I)],
+    "tc_get_positions": [_P, _P, C.c_size_t],
+    "tc_set_positions_and_velocities": [_P, _P, _P, _U],
+    "tc_reset": [_P],
+    "tc_set_gravity": [_P, _F, _F, _F],
+    "tc_set_damping": [_P, _F],
+    "tc_set_damping_all": [_P, _F, _F, _F, _F],
+    "tc_set_solver_iterations": [_P, _U],
+    "tc_set_stiffness_all": [_P, _F, _F, _F, _F],
+    "tc_set_compliance_all": [_P, _F, _F, _F, _F],
+    "tc_set_edge_stiffness_multipliers": [_P, _P, _P, _U],
+    "tc_set_enable_self_collision": [_P, _I],
+    "tc_set_self_collision_options": [_P, _F, _F, _I, _I, _U],
+    "tc_set_coupled_collider": [_P, _I],
+    "tc_set_auto_coupled_on_low_substeps": [_P, _I],
+    "tc_set_collider_options": [_P, _I, _I, _F],
+    "tc_add_sphere_collider": [_P, _P, _F, _F, _F],
+    "tc_add_capsule_collider": [_P, _P, _P, _F, _F, _F],
+    "tc_add_plane_collider": [_P, _P, _P, _F, _F],
+    "tc_set_mesh_collider_triangles": [_P, _P, _U, _F, _F, _F, _I, _P],
+    "tc_clear_colliders": [_P],
+    "tc_set_pin": [_P, _U, _P, _F],
+    "tc_set_pins_batch": [_P, _P, _P, _P, _U],
+    "tc_release_pin": [_P, _U],
+    "tc_clear_pins": [_P],
+    "tc_set_vertex_inv_masses": [_P, _P, _P, _U],
+    "tc_get_vertex_inv_masses": [_P, _P, _U],
+    "tc_get_counts": [_P, _P],
+    "tc_get_cell_size": [_P, C.POINTER(_F)],
+    "tc_get_state": [_P, _P, _P, _P],
+    "tc_get_distance_constraints": [_P, _P, _P, _P, _P],
+    "tc_get_bending_constraints": [_P, _P, _P, _P, _P],
+    "tc_get_hash_state": [_P, _I, _P, _P],
+    "tc_get_edges": [_P, _P, _P],
+    "tc_set_residual_tracking": [_P, _I],
+    "tc_get_residuals": [_P, _P, _P, _P, _P, _P],
+    "tc_last_frame_ms": [_P, C.POINTER(_F)],
+    "tc_set_profiling_enabled": [_P, _I],
+    "tc_frame_kernel_count": [_P, C.POINTER(_U)],
+    "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],
+    "tc_mesh_build": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F],
+    "tc_mesh_destroy": [_P],
+    "tc_mesh_counts": [_P, _P, C.POINTER(_F)],
+    "tc_mesh_constraints": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "tc_mesh_topology_sizes": [_P, C.POINTER(_U), C.POINTER(_U), C.POINTER(_U)],
+    "tc_mesh_topology": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+}
+_RESTYPES = {"tc_last_error": C.c_char_p, "tc_gpu_available": _I}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libtcloth.so and bind every declared symbol (raises if absent)."""
+    global _lib
+    if _lib is not None and path == LIB_PATH:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"libtcloth.so not found at {path}; build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+    L = C.CDLL(path)
+    for name, args in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPES.get(name, _I)
+    if path == LIB_PATH:
+        _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    """Map a tc_status to the reference's Python exceptions."""
+    if status == TC_OK:
+        return
+    msg = load().tc_last_error().decode("utf-8", "replace")
+    if status == TC_ERR_INVALID:
+        raise ValueError(msg)
+    if status == TC_ERR_NOMEM:
+        raise MemoryError(msg)
+    raise RuntimeError(msg)

@@ -1,0 +1,892 @@
+// Self-collision kernels: area-weighted normals, the spatial-hash counting
+// sort (vertex and edge-midpoint keys), vertex-vertex / vertex-triangle
+// contacts, multi-layer untangling, edge-edge contacts and the apply pass.
+//
+// Contacts accumulate into a per-vertex 16 x int32 record with integer
+// atomics (fixed point x1e6), so results do not depend on thread order.
+// The one order-dependent piece of the reference, the in-bucket order of the
+// counting sort (atomic scatter, shaders/spatial_grid_sort.wgsl:182-194), is
+// made canonical here: each bucket is sorted by ascending element index.
+#pragma once
+#include "vmath.cuh"
+
+namespace tcloth {
+
+enum : int {
+  A_DX, A_DY, A_DZ, A_CNT, A_PDX, A_PDY, A_PDZ, A_PCNT,
+  A_CPX, A_CPY, A_CPZ, A_CNX, A_CNY, A_CNZ, A_UT, A_EEC, A_N
+};
+
+struct SCArgs {
+  uint32_t n, ne, table;
+  float cell;
+  float relief;
+  int enable_relief;
+  float max_disp_ratio;
+  int exclude_neighbors;
+  int untangle;  // effective: option && multiple layers
+  uint32_t max_search;
+  const float4* x4;
+  const float4* p4;
+  const float4* v4;  // layer bits in .w
+  const float* local_len;
+  const uint32_t* adj_off;
+  const uint32_t* adj_idx;
+  const uint32_t* th_off;
+  const uint32_t* th_idx;
+  const float* th_rest;
+  const uint32_t* star_off;
+  const uint2* star_idx;
+  const uint2* edges;
+  const uint32_t* edge_bits;
+  const uint32_t* cs;    // vertex cell starts (table + 1)
+  const uint32_t* srt;   // vertex sorted indices
+  const uint32_t* ecs;   // edge cell starts
+  const uint32_t* esrt;  // edge sorted indices
+  const float4* nrm;
+  int32_t* acc;
+};
+
+__device__ __forceinline__ uint32_t layer_of(const float4* v4, uint32_t i) { return __float_as_uint(v4[i].w); }
+
+// ---------------- normals: shaders/compute_normals.wgsl:25-58
+__global__ void k_normals(uint32_t n, const float4* __restrict__ x4, const uint32_t* __restrict__ star_off,
+                          const uint2* __restrict__ star_idx, float4* __restrict__ nrm) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V3 pi = mk(x4[i]);
+  V3 s = mk(0.f, 0.f, 0.f);
+  for (uint32_t k = star_off[i]; k < star_off[i + 1]; ++k) {
+    const uint2 pr = star_idx[k];
+    s = s + cross(mk(x4[pr.x]) - pi, mk(x4[pr.y]) - pi);
+  }
+  const float l = length(s);
+  V3 r = l > kEps ? s / l : mk(0.f, 0.f, 0.f);
+  nrm[i] = make_float4(r.x, r.y, r.z, 0.f);
+}
+
+// ---------------- spatial hash (spatial_hash.rs:158-247, spatial_grid_sort*.wgsl)
+// which == 0: key of vertex i is its predicted position; which == 1: key of
+// edge i is the midpoint of its two predicted endpoints.
+__global__ void k_hash_count(uint32_t cnt, int which, const float4* __restrict__ p4, const uint2* __restrict__ edges,
+                             float cell, uint32_t table, uint32_t* __restrict__ keys, uint32_t* __restrict__ counts) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  V3 q;
+  if (which == 0) {
+    q = mk(p4[i]);
+  } else {
+    const uint2 e = edges[i];
+    q = (mk(p4[e.x]) + mk(p4[e.y])) * 0.5f;
+  }
+  const I3 c = cell_of(q, cell);
+  const uint32_t h = hash3(c.x, c.y, c.z, table);
+  keys[i] = h;
+  // warp-aggregated increment: lanes with the same bucket share one atomic
+  const uint32_t active = __activemask();
+  const uint32_t peers = __match_any_sync(active, h);
+  const int leader = __ffs(peers) - 1;
+  const int lane = threadIdx.x & 31;
+  if (lane == leader) atomicAdd(&counts[h], __popc(peers));
+}
+
+// exclusive scan of counts[table] into starts[table + 1]; one block of 1024
+// threads, each owning a contiguous chunk, warp-shuffle scans of chunk sums.
+__global__ void k_hash_scan(uint32_t table, const uint32_t* __restrict__ counts, uint32_t* __restrict__ starts) {
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t tid = threadIdx.x;
+  const uint32_t per = (table + blockDim.x - 1) / blockDim.x;
+  const uint32_t b = tid * per, e = min(b + per, table);
+  uint32_t local = 0;
+  for (uint32_t k = b; k < e; ++k) local += counts[k];
+  // inclusive warp scan
+  uint32_t v = local;
+  const int lane = tid & 31, wid = tid >> 5;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) warp_tot[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    warp_tot[lane] = w;
+  }
+  __syncthreads();
+  uint32_t base = (wid > 0 ? warp_tot[wid - 1] : 0u) + v - local;
+  for (uint32_t k = b; k < e; ++k) {
+    starts[k] = base;
+    base += counts[k];
+  }
+  if (tid == blockDim.x - 1) starts[table] = warp_tot[(blockDim.x >> 5) - 1];
+}
+
+__global__ void k_hash_scatter(uint32_t cnt, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ starts,
+                               uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  const uint32_t h = keys[i];
+  sorted[starts[h] + atomicAdd(&cursor[h], 1u)] = i;
+}
+
+// canonical in-bucket order: ascending index (insertion sort; buckets are small)
+__global__ void k_hash_sort_buckets(uint32_t table, const uint32_t* __restrict__ starts, uint32_t* __restrict__ sorted) {
+  uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= table) return;
+  const uint32_t b = starts[h], e = starts[h + 1];
+  for (uint32_t k = b + 1; k < e; ++k) {
+    uint32_t v = sorted[k];
+    uint32_t j = k;
+    while (j > b && sorted[j - 1] > v) {
+      sorted[j] = sorted[j - 1];
+      --j;
+    }
+    sorted[j] = v;
+  }
+}
+
+// ---------------- accumulation helpers (shaders/self_collision.wgsl:77-118)
+__device__ __forceinline__ int32_t to_fixed(float x) { return f2i(clampf(x * 1000000.0f, -50000000.0f, 50000000.0f)); }
+__device__ __forceinline__ void add_disp(int32_t* acc, uint32_t v, V3 d) {
+  int32_t* a = acc + (size_t)v * A_N;
+  atomicAdd(&a[A_DX], to_fixed(d.x));
+  atomicAdd(&a[A_DY], to_fixed(d.y));
+  atomicAdd(&a[A_DZ], to_fixed(d.z));
+  atomicAdd((uint32_t*)&a[A_CNT], 1u);
+}
+__device__ __forceinline__ void add_pin(int32_t* acc, uint32_t v, V3 d) {
+  int32_t* a = acc + (size_t)v * A_N;
+  atomicAdd(&a[A_PDX], to_fixed(d.x));
+  atomicAdd(&a[A_PDY], to_fixed(d.y));
+  atomicAdd(&a[A_PDZ], to_fixed(d.z));
+  atomicAdd((uint32_t*)&a[A_PCNT], 1u);
+}
+__device__ __forceinline__ void add_ccd(int32_t* acc, uint32_t v, V3 d, bool count_ee) {
+  int32_t* a = acc + (size_t)v * A_N;
+  const int32_t ix = to_fixed(d.x), iy = to_fixed(d.y), iz = to_fixed(d.z);
+  if (ix > 0) atomicMax(&a[A_CPX], ix); else if (ix < 0) atomicMin(&a[A_CNX], ix);
+  if (iy > 0) atomicMax(&a[A_CPY], iy); else if (iy < 0) atomicMin(&a[A_CNY], iy);
+  if (iz > 0) atomicMax(&a[A_CPZ], iz); else if (iz < 0) atomicMin(&a[A_CNZ], iz);
+  if (count_ee) {
+    const float lf = clampf(length(d) * 1000000.0f, 0.0f, 2000000000.0f);
+    const uint32_t u = lf != lf ? 0u : (uint32_t)lf;
+    if (u > 0u) atomicAdd((uint32_t*)&a[A_EEC], 1u);
+  }
+}
+
+__device__ __forceinline__ bool th_search(const SCArgs& s, uint32_t a, uint32_t b, uint32_t& pos) {
+  uint32_t lo = s.th_off[a], hi = s.th_off[a + 1];
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2u;
+    const uint32_t v = s.th_idx[mid];
+    if (v == b) { pos = mid; return true; }
+    if (v < b) lo = mid + 1u; else hi = mid;
+  }
+  return false;
+}
+// is_within_two_hops (shaders/self_collision.wgsl:243-264)
+__device__ __forceinline__ bool within2(const SCArgs& s, uint32_t a, uint32_t b) {
+  uint32_t q;
+  if (a == b) return true;
+  return th_search(s, a, b, q);
+}
+// is_topologically_near_folded (:268-293)
+__device__ __forceinline__ bool near_folded(const SCArgs& s, uint32_t a, uint32_t b, float d) {
+  uint32_t q;
+  if (a == b) return true;
+  if (!th_search(s, a, b, q)) return false;
+  return !(d < s.th_rest[q] * 0.5f);
+}
+// is_topologically_near_folded_sq (shaders/self_collision_ee_direct.wgsl:237-262)
+__device__ __forceinline__ bool near_folded_sq(const SCArgs& s, uint32_t a, uint32_t b, float d2) {
+  uint32_t q;
+  if (a == b) return true;
+  if (!th_search(s, a, b, q)) return false;
+  const float l0 = s.th_rest[q];
+  return !(d2 < (l0 * l0) * 0.25f);
+}
+
+// ---------------- sc_solve: shaders/self_collision.wgsl:317-681
+__global__ void __launch_bounds__(128) k_sc_solve(SCArgs s) {
+  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= s.n) return;
+  const float4 xi4 = s.x4[index], pi4 = s.p4[index];
+  const float wi = xi4.w;
+  const bool pin_i = wi <= 0.0f;
+  const V3 xi = mk(xi4), pi = mk(pi4);
+  const float mli = length(pi - xi);
+  if (pin_i && mli < kEps) return;
+  const float thi = pi4.w;
+  const float lli = s.local_len[index];
+  const float cs = s.cell;
+  const I3 cell = cell_of(pi, cs);
+  const uint32_t li = layer_of(s.v4, index);
+  const bool untangle = s.untangle != 0;
+  const bool track = untangle && !pin_i && li > 0u;
+  float best_in = 1e20f;
+  uint32_t best_j = 0xFFFFFFFFu;
+  int32_t* acc = s.acc;
+  for (int32_t cx = cell.x - 1; cx <= cell.x + 1; ++cx)
+    for (int32_t cy = cell.y - 1; cy <= cell.y + 1; ++cy)
+      for (int32_t cz = cell.z - 1; cz <= cell.z + 1; ++cz) {
+        const uint32_t h = hash3(cx, cy, cz, s.table);
+        const uint32_t kb = s.cs[h], ke = s.cs[h + 1];
+        for (uint32_t k = kb; k < ke; ++k) {
+          const uint32_t j = s.srt[k];
+          if (j >= s.n || j == index) continue;
+          const float4 pj4 = s.p4[j];
+          const V3 pj = mk(pj4);
+          const I3 jc = cell_of(pj, cs);
+          if (!(jc.x == cx && jc.y == cy && jc.z == cz)) continue;
+          const V3 dvv = pi - pj;
+          const float d2 = dot(dvv, dvv);
+          const float thj = pj4.w, llj = s.local_len[j];
+          const float eth = fmaxf(thi + thj, fminf(lli, llj) * 0.06f);
+          const float mgd = eth + (lli + llj) * 1.3f;
+          const uint32_t lj = layer_of(s.v4, j);
+          if (track && lj < li && d2 < best_in) {
+            const float ur = eth * 2.5f + llj * 1.3f;
+            if (d2 <= ur * ur && !within2(s, index, j)) { best_in = d2; best_j = j; }
+          }
+          if (!(d2 <= mgd * mgd)) continue;
+          const float dvl = sqrtf(fmaxf(d2, 0.0f));
+          if (near_folded(s, index, j, dvl)) continue;
+          const float4 xj4 = s.x4[j];
+          const V3 pjo = mk(xj4);
+          const float wj = xj4.w;
+          const bool both = wj > 0.0f;
+          const float eth2 = eth * eth;
+          // 1. vertex-vertex
+          if (!pin_i && (!both || index < j)) {
+            if (d2 < eth2 && d2 > kEps * kEps) {
+              bool utv = false;
+              if (untangle && li != lj) {
+                const V3 ni = mk(s.nrm[index]), nj = mk(s.nrm[j]);
+                const float nil = length(ni), njl = length(nj);
+                if (li > lj) {
+                  if (njl > 0.5f) {
+                    const V3 nju = nj / njl;
+                    const bool allow = (wj <= 0.0f) || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), nju) > 0.0f);
+                    utv = allow && (dot(dvv, nju) < 0.0f);
+                  }
+                } else if (both && nil > 0.5f) {
+                  const V3 niu = ni / nil;
+                  const bool allow = (njl <= 0.5f) || (dot(nj / fmaxf(njl, kEps), niu) > 0.0f);
+                  utv = allow && (dot(-dvv, niu) < 0.0f);
+                }
+              }
+              if (!utv) {
+                const V3 nn = dvv / dvl;
+                const float pen = eth - dvl;
+                const float ws = wi + wj;
+                if (ws > kEps) {
+                  if (wj <= 0.0f) {
+                    add_pin(acc, index, nn * pen + (pj - pjo) * 0.5f);
+                  } else {
+                    const V3 disp = nn * (pen * 0.5f);
+                    add_disp(acc, index, disp * (wi / ws));
+                    add_disp(acc, j, (-disp) * (wj / ws));
+                  }
+                }
+              }
+            }
+          }
+          // 2. vertex-triangle
+          const float mlj = length(pj - pjo);
+          const float vtb = eth + llj * 1.3f + mli + mlj;
+          if (!(d2 <= vtb * vtb) || within2(s, index, j)) continue;
+          for (uint32_t st = s.star_off[j]; st < s.star_off[j + 1]; ++st) {
+            const uint2 pr = s.star_idx[st];
+            const uint32_t v0 = pr.x, v1 = pr.y;
+            if (v0 == index || v1 == index) continue;
+            const float4 q0 = s.p4[v0], q1 = s.p4[v1];
+            const float4 o0 = s.x4[v0], o1 = s.x4[v1];
+            const V3 pv0 = mk(q0), pv1 = mk(q1), pv0o = mk(o0), pv1o = mk(o1);
+            const float wv0 = o0.w, wv1 = o1.w;
+            const V3 d0 = pi - pv0;
+            const float ll0 = s.local_len[v0];
+            const float et0 = fmaxf(thi + q0.w, fminf(lli, ll0) * 0.06f);
+            const float b0 = et0 + ll0 * 1.3f + mli + length(pv0 - pv0o);
+            const I3 c0 = cell_of(pv0, cs);
+            const bool in0 = abs(c0.x - cell.x) <= 1 && abs(c0.y - cell.y) <= 1 && abs(c0.z - cell.z) <= 1 &&
+                             (dot(d0, d0) <= b0 * b0);
+            const V3 d1 = pi - pv1;
+            const float ll1 = s.local_len[v1];
+            const float et1 = fmaxf(thi + q1.w, fminf(lli, ll1) * 0.06f);
+            const float b1 = et1 + ll1 * 1.3f + mli + length(pv1 - pv1o);
+            const I3 c1 = cell_of(pv1, cs);
+            const bool in1 = abs(c1.x - cell.x) <= 1 && abs(c1.y - cell.y) <= 1 && abs(c1.z - cell.z) <= 1 &&
+                             (dot(d1, d1) <= b1 * b1);
+            if ((in0 && j > v0) || (in1 && j > v1)) continue;
+            const V3 tmove = (((pj - pjo) + (pv0 - pv0o)) + (pv1 - pv1o)) / 3.0f;
+            const bool tpin = (wj <= 0.0f) || (wv0 <= 0.0f) || (wv1 <= 0.0f);
+            const V3 rel = xi + tmove;
+            const V3 E = mk(eth, eth, eth);
+            const V3 smin = vmin(rel, pi) - E, smax = vmax(rel, pi) + E;
+            const V3 tmin = vmin(vmin(pj, pv0), pv1), tmax = vmax(vmax(pj, pv0), pv1);
+            if (smin.x > tmax.x || smin.y > tmax.y || smin.z > tmax.z || smax.x < tmin.x || smax.y < tmin.y ||
+                smax.z < tmin.z)
+              continue;
+            if (within2(s, index, v0) || within2(s, index, v1)) continue;
+            const V3 mv = pi - rel;
+            const float msq = dot(mv, mv);
+            float ht = 1.0f, hu = 0.0f, hv = 0.0f;
+            bool hit = false;
+            if (msq > 1e-12f) hit = seg_tri(rel, pi, pj, pv0, pv1, ht, hu, hv);
+            if (hit) {
+              const V3 hp = rel + mv * ht;
+              const V3 tc = cross(pv0 - pj, pv1 - pj);
+              const float tl = length(tc);
+              const V3 tn = tl > 1e-12f ? tc / tl : mk(0.0f, 1.0f, 0.0f);
+              const float hor = dot(rel - pj, tn);
+              bool utc = false;
+              if (untangle && !pin_i && (li > lj) && tl > 1e-12f) {
+                const V3 ni = mk(s.nrm[index]);
+                const float nil = length(ni);
+                const bool allow = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
+                const bool ret = (hor < 0.0f) && (dot(mv, tn) > 0.0f);
+                utc = allow && ret;
+              }
+              if (!utc) {
+                const float ss = fabsf(hor) > 1e-6f ? hor : dot(-mv, tn);
+                const V3 ns = ss >= 0.0f ? tn : -tn;
+                const float ho = fmaxf(dot(rel - hp, ns), 0.0f);
+                const float hs = fmaxf(ho, eth * 0.25f);
+                const V3 psafe = hp + ns * hs;
+                const V3 tccd = psafe - pi;
+                const float pcs = fmaxf(0.0f, eth - hs);
+                if (tpin) {
+                  if (!pin_i) add_ccd(acc, index, tccd + ns * pcs, false);
+                } else if (pin_i) {
+                  const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
+                  const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
+                  if (wt > kEps) {
+                    const V3 full = tccd + ns * pcs;
+                    if (wj > 0.0f) add_ccd(acc, j, (-full) * (bc.x * wj / wt), false);
+                    if (wv0 > 0.0f) add_ccd(acc, v0, (-full) * (bc.y * wv0 / wt), false);
+                    if (wv1 > 0.0f) add_ccd(acc, v1, (-full) * (bc.z * wv1 / wt), false);
+                  }
+                } else {
+                  const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
+                  const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
+                  const float wtot = wi + wt;
+                  if (wtot > kEps) {
+                    add_ccd(acc, index, tccd * (wi / wtot), false);
+                    if (wj > 0.0f) add_ccd(acc, j, (-tccd) * (bc.x * wj / wtot), false);
+                    if (wv0 > 0.0f) add_ccd(acc, v0, (-tccd) * (bc.y * wv0 / wtot), false);
+                    if (wv1 > 0.0f) add_ccd(acc, v1, (-tccd) * (bc.z * wv1 / wtot), false);
+                    if (pcs > kEps) {
+                      const V3 tp = ns * (pcs * 0.6f);
+                      add_disp(acc, index, tp * (wi / wtot));
+                      if (wj > 0.0f) add_disp(acc, j, (-tp) * (bc.x * wj / wtot));
+                      if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bc.y * wv0 / wtot));
+                      if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bc.z * wv1 / wtot));
+                    }
+                  }
+                }
+              }
+            } else {
+              bool isf;
+              V3 bary;
+              const V3 cp = closest_tri(pi, pj, pv0, pv1, isf, bary);
+              const V3 dvt = pi - cp;
+              const float d2vt = dot(dvt, dvt);
+              if (!pin_i && d2vt < eth2 && d2vt > kEps * kEps) {
+                const float dvtl = sqrtf(d2vt);
+                bool utv = false;
+                if (untangle && li > lj) {
+                  const V3 tc = cross(pv0 - pj, pv1 - pj);
+                  const float tl = length(tc);
+                  if (tl > kEps) {
+                    const V3 tn = tc / tl;
+                    if (dot(dvt, tn) < 0.0f) {
+                      const V3 ni = mk(s.nrm[index]);
+                      const float nil = length(ni);
+                      utv = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
+                    }
+                  }
+                }
+                if (!utv) {
+                  const V3 nvt = dvt / dvtl;
+                  const float pvt = eth - dvtl;
+                  if (tpin) {
+                    add_pin(acc, index, nvt * pvt + tmove * 0.5f);
+                  } else {
+                    const float wt = bary.x * bary.x * wj + bary.y * bary.y * wv0 + bary.z * bary.z * wv1;
+                    const float wtot = wi + wt;
+                    if (wtot > kEps) {
+                      const V3 tp = nvt * (pvt * 0.6f);
+                      add_disp(acc, index, tp * (wi / wtot));
+                      if (wj > 0.0f) add_disp(acc, j, (-tp) * (bary.x * wj / wtot));
+                      if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bary.y * wv0 / wtot));
+                      if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bary.z * wv1 / wtot));
+                    }
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+  if (track && best_j < 0x3FFFFEu) acc[(size_t)index * A_N + A_UT] = (int32_t)(best_j + 1u);
+}
+
+// ---------------- sc_untangle: shaders/self_collision_untangle.wgsl:199-394
+__device__ __forceinline__ bool th_range_has(const SCArgs& s, uint32_t b0, uint32_t e0, uint32_t v) {
+  if (b0 >= e0) return false;
+  uint32_t lo = b0, hi = e0;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2u;
+    const uint32_t x = s.th_idx[mid];
+    if (x == v) return true;
+    if (x < v) lo = mid + 1u; else hi = mid;
+  }
+  return false;
+}
+
+__global__ void k_untangle(SCArgs s) {
+  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= s.n || !s.untangle) return;
+  int32_t* ai = s.acc + (size_t)index * A_N;
+  const uint32_t cand = (uint32_t)ai[A_UT];
+  if (cand == 0u) return;
+  ai[A_UT] = 0;
+  const float wi = s.x4[index].w;
+  const uint32_t li = layer_of(s.v4, index);
+  if (wi <= 0.0f || li == 0u) return;
+  const uint32_t j1e = cand & 0x3FFFFFu;
+  if (j1e == 0u) return;
+  const uint32_t j1 = j1e - 1u;
+  if (j1 >= s.n || j1 == index) return;
+  const float4 pi4 = s.p4[index];
+  const V3 pi = mk(pi4);
+  const float thi = pi4.w, lli = s.local_len[index];
+  const uint32_t ts = s.th_off[index], te = s.th_off[index + 1];
+  uint32_t j2 = 0xFFFFFFFFu;
+  float bnd = 1e20f;
+  for (uint32_t a = s.adj_off[j1]; a < s.adj_off[j1 + 1]; ++a) {
+    const uint32_t nb = s.adj_idx[a];
+    if (nb < s.n && nb != index && layer_of(s.v4, nb) < li) {
+      const V3 dn = pi - mk(s.p4[nb]);
+      const float dns = dot(dn, dn);
+      if (dns < bnd && !th_range_has(s, ts, te, nb)) { bnd = dns; j2 = nb; }
+    }
+  }
+  float bd2 = 1e20f, bh = 0.0f;
+  uint32_t bj = 0xFFFFFFFFu, bv0 = 0, bv1 = 0;
+  for (int ci = 0; ci < 2; ++ci) {
+    const uint32_t j = ci == 0 ? j1 : j2;
+    if (j == 0xFFFFFFFFu) continue;
+    const float4 pj4 = s.p4[j];
+    const V3 pj = mk(pj4);
+    const float eth = fmaxf(thi + pj4.w, fminf(lli, s.local_len[j]) * 0.06f);
+    const float capt = eth * 2.5f;
+    const float capsq = capt * capt;
+    for (uint32_t st = s.star_off[j]; st < s.star_off[j + 1]; ++st) {
+      const uint2 pr = s.star_idx[st];
+      const uint32_t v0 = pr.x, v1 = pr.y;
+      if (v0 == index || v1 == index) continue;
+      if (ci == 1 && (v0 == j1 || v1 == j1)) continue;
+      const V3 pv0 = mk(s.p4[v0]), pv1 = mk(s.p4[v1]);
+      const V3 tmin = vmin(vmin(pj, pv0), pv1), tmax = vmax(vmax(pj, pv0), pv1);
+      const V3 z = mk(0.f, 0.f, 0.f);
+      const V3 ad = vmax(tmin - pi, z) + vmax(pi - tmax, z);
+      const float lim = fminf(capsq, bd2 + 1e-10f);
+      if (dot(ad, ad) >= lim) continue;
+      bool isf;
+      V3 bary;
+      const V3 pt = closest_tri(pi, pj, pv0, pv1, isf, bary);
+      const V3 du = pi - pt;
+      const float dsu = dot(du, du);
+      if (dsu >= capsq) continue;
+      if (bj != 0xFFFFFFFFu && dsu > bd2 + 1e-10f) continue;
+      const V3 tc = cross(pv0 - pj, pv1 - pj);
+      const float tl = length(tc);
+      if (tl <= kEps) continue;
+      const float hu = dot(du, tc / tl);
+      const bool same = fabsf(dsu - bd2) <= 1e-10f;
+      const bool better = (hu >= 0.0f && bh < 0.0f) || (((hu >= 0.0f) == (bh >= 0.0f)) && fabsf(hu) > fabsf(bh));
+      if (bj == 0xFFFFFFFFu || dsu < bd2 - 1e-10f || (same && better)) {
+        if (th_range_has(s, ts, te, j) || th_range_has(s, ts, te, v0) || th_range_has(s, ts, te, v1)) continue;
+        bd2 = dsu; bh = hu; bj = j; bv0 = v0; bv1 = v1;
+      }
+    }
+  }
+  if (bj != 0xFFFFFFFFu && bh < 0.0f) {
+    const float4 qj = s.p4[bj], q0 = s.p4[bv0], q1 = s.p4[bv1];
+    const V3 upj = mk(qj), up0 = mk(q0), up1 = mk(q1);
+    const float wj = s.x4[bj].w, w0 = s.x4[bv0].w, w1 = s.x4[bv1].w;
+    bool isf;
+    V3 bary;
+    const V3 pt = closest_tri(pi, upj, up0, up1, isf, bary);
+    const V3 du = pi - pt;
+    const float dl = length(du);
+    const V3 tc = cross(up0 - upj, up1 - upj);
+    const float tl = length(tc);
+    if (tl > kEps && dl > kEps) {
+      const V3 tn = tc / tl;
+      const float hu = dot(du, tn);
+      if (hu < 0.0f) {
+        const V3 ni = mk(s.nrm[index]);
+        const float nil = length(ni);
+        const bool tpin = (wj <= 0.0f) || (w0 <= 0.0f) || (w1 <= 0.0f);
+        const bool allow = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
+        const float etu = fmaxf(thi + qj.w, fminf(lli, s.local_len[bj]) * 0.06f);
+        const float cb = -hu / dl;
+        const float rt = sqrtf(fmaxf(dl * dl - hu * hu, 0.0f));
+        const float rl = fmaxf(etu * 0.5f, kEps);
+        if (allow && cb > 0.707f && rt < rl) {
+          const V3 ni2 = (mk(s.nrm[bj]) * bary.x + mk(s.nrm[bv0]) * bary.y) + mk(s.nrm[bv1]) * bary.z;
+          const float nl = length(ni2);
+          const bool behind = (nl <= 0.5f) || (dot(du, ni2) < 0.0f);
+          if (behind) {
+            const float cw = clampf((cb - 0.707f) / 0.2f, 0.0f, 1.0f);
+            const float rw = clampf(1.0f - rt / rl, 0.0f, 1.0f);
+            const float pen = fminf(etu - hu, etu * 2.0f) * cw * rw;
+            if (pen > kEps) {
+              if (tpin) {
+                add_disp(s.acc, index, tn * pen);
+              } else {
+                const float wt = bary.x * bary.x * wj + bary.y * bary.y * w0 + bary.z * bary.z * w1;
+                const float wtot = wi + wt;
+                if (wtot > kEps) {
+                  const V3 disp = tn * (pen * 0.5f);
+                  add_disp(s.acc, index, disp * (wi / wtot));
+                  if (wj > 0.0f) add_disp(s.acc, bj, (-disp) * (bary.x * wj / wtot));
+                  if (w0 > 0.0f) add_disp(s.acc, bv0, (-disp) * (bary.y * w0 / wtot));
+                  if (w1 > 0.0f) add_disp(s.acc, bv1, (-disp) * (bary.z * w1 / wtot));
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---------------- sc_solve_ee: shaders/self_collision_ee_direct.wgsl:266-776
+__device__ __forceinline__ float seg_eval(V3 a0o, V3 a0, V3 a1o, V3 a1, V3 b0o, V3 b0, V3 b1o, V3 b1, float tau,
+                                          float& so, float& to) {
+  const V3 A0 = vmix(a0o, a0, tau), A1 = vmix(a1o, a1, tau), B0 = vmix(b0o, b0, tau), B1 = vmix(b1o, b1, tau);
+  seg_seg(A0, A1, B0, B1, so, to);
+  const V3 d = vmix(A0, A1, so) - vmix(B0, B1, to);
+  return dot(d, d);
+}
+__device__ __forceinline__ float seg_vol(V3 a0o, V3 a0, V3 a1o, V3 a1, V3 b0o, V3 b0, V3 b1o, V3 b1, float tau) {
+  const V3 A0 = vmix(a0o, a0, tau), A1 = vmix(a1o, a1, tau), B0 = vmix(b0o, b0, tau), B1 = vmix(b1o, b1, tau);
+  return dot(cross(A1 - A0, B1 - B0), B0 - A0);
+}
+__device__ __forceinline__ bool outer_behind(const SCArgs& s, uint32_t la, uint32_t lb, uint32_t a0, uint32_t a1,
+                                             uint32_t b0, uint32_t b1, bool afix, bool bfix, V3 dab) {
+  if (la == lb) return false;
+  const V3 na = mk(s.nrm[a0]) + mk(s.nrm[a1]), nb = mk(s.nrm[b0]) + mk(s.nrm[b1]);
+  const float nal = length(na), nbl = length(nb);
+  if (la > lb) {
+    if (nbl <= 0.5f) return false;
+    const V3 ni = nb / nbl;
+    const bool allow = bfix || (nal <= 0.5f) || (dot(na / fmaxf(nal, kEps), ni) > 0.0f);
+    return allow && (dot(dab, ni) < 0.0f);
+  }
+  if (nal <= 0.5f) return false;
+  const V3 ni = na / nal;
+  const bool allow = afix || (nbl <= 0.5f) || (dot(nb / fmaxf(nbl, kEps), ni) > 0.0f);
+  return allow && (dot(-dab, ni) < 0.0f);
+}
+
+__global__ void __launch_bounds__(128) k_ee(SCArgs s) {
+  const uint32_t ei = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ei >= s.ne) return;
+  const uint2 ea = s.edges[ei];
+  const uint32_t u0 = ea.x, u1 = ea.y;
+  const float4 xu0 = s.x4[u0], xu1 = s.x4[u1], qu0 = s.p4[u0], qu1 = s.p4[u1];
+  const float w_u0 = xu0.w, w_u1 = xu1.w;
+  const bool apin = (w_u0 <= 0.0f) || (w_u1 <= 0.0f);
+  const V3 p_u0 = mk(qu0), p_u1 = mk(qu1), p_u0o = mk(xu0), p_u1o = mk(xu1);
+  const float thu0 = qu0.w, thu1 = qu1.w;
+  const float mta = fmaxf(thu0, thu1);
+  const bool bnda = ((s.edge_bits[ei >> 5] >> (ei & 31u)) & 1u) != 0u;
+  const V3 m2 = mk(mta * 2.0f, mta * 2.0f, mta * 2.0f);
+  const V3 amin = vmin(vmin(p_u0, p_u1), vmin(p_u0o, p_u1o)) - m2;
+  const V3 amax = vmax(vmax(p_u0, p_u1), vmax(p_u0o, p_u1o)) + m2;
+  const I3 base = cell_of((p_u0 + p_u1) * 0.5f, s.cell);
+  const uint32_t la = layer_of(s.v4, u0);
+  const bool untangle = s.untangle != 0;
+  int32_t* acc = s.acc;
+  uint32_t search = 0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int32_t nx = base.x + dx, ny = base.y + dy, nz = base.z + dz;
+        const uint32_t h = hash3(nx, ny, nz, s.table);
+        const uint32_t st = s.ecs[h], en = s.ecs[h + 1];
+        if (st >= en) continue;
+        for (uint32_t q = 0; q < en - st; ++q) {
+          const uint32_t eb = s.esrt[st + q];
+          if (ei >= eb) continue;
+          const uint2 ebv = s.edges[eb];
+          const uint32_t j = ebv.x, vj = ebv.y;
+          if (j == u0 || j == u1 || vj == u0 || vj == u1) continue;
+          const float4 qj = s.p4[j], qvj = s.p4[vj];
+          const V3 p_j = mk(qj), p_vj = mk(qvj);
+          const I3 bc = cell_of((p_j + p_vj) * 0.5f, s.cell);
+          if (!(bc.x == nx && bc.y == ny && bc.z == nz)) continue;
+          const float4 xj = s.x4[j], xvj = s.x4[vj];
+          const V3 p_jo = mk(xj), p_vjo = mk(xvj);
+          const V3 bmin = vmin(vmin(p_j, p_vj), vmin(p_jo, p_vjo));
+          const V3 bmax = vmax(vmax(p_j, p_vj), vmax(p_jo, p_vjo));
+          if (amin.x > bmax.x || amin.y > bmax.y || amin.z > bmax.z || amax.x < bmin.x || amax.y < bmin.y ||
+              amax.z < bmin.z)
+            continue;
+          ++search;
+          if (search > s.max_search) return;
+          const float w_j = xj.w, w_vj = xvj.w;
+          const float thj = qj.w, thvj = qvj.w;
+          const uint32_t lb = layer_of(s.v4, j);
+          const bool bndb = ((s.edge_bits[eb >> 5] >> (eb & 31u)) & 1u) != 0u;
+          const bool bpair = bnda || bndb;
+          bool run_ccd = bpair, has1 = false;
+          float s1 = 0.f, t1 = 0.f, d2c = 0.f, ethc = 0.f;
+          V3 dl1 = mk(0.f, 0.f, 0.f);
+          if (!run_ccd) {
+            seg_seg(p_u0, p_u1, p_j, p_vj, s1, t1);
+            dl1 = vmix(p_u0, p_u1, s1) - vmix(p_j, p_vj, t1);
+            d2c = dot(dl1, dl1);
+            ethc = mixf(thu0, thu1, s1) + mixf(thj, thvj, t1);
+            const float meg = mta + fmaxf(thj, thvj);
+            const V3 dv0 = p_u0 - p_u0o, dv1 = p_u1 - p_u1o, dvj = p_j - p_jo, dvvj = p_vj - p_vjo;
+            const V3 va = (dv0 + dv1) * 0.5f, vb = (dvj + dvvj) * 0.5f;
+            const float rdg = length(va - vb) + 0.5f * (length(dv1 - dv0) + length(dvvj - dvj));
+            const float reach = meg + rdg;
+            if (d2c > reach * reach) continue;
+            has1 = true;
+            const V3 d0g = vmix(p_u0o, p_u1o, s1) - vmix(p_jo, p_vjo, t1);
+            run_ccd = (rdg > ethc * 0.5f) || (dot(d0g, dl1) <= 0.0f);
+          }
+          if (run_ccd) {
+            float msd = 1e20f, btau = 0.0f, hs = 0.125f, ms = 0.f, mt = 0.f;
+            float pv = seg_vol(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, 0.0f);
+            float zc = -1.0f;
+            for (uint32_t k = 0; k <= 8u; ++k) {
+              const float tk = (float)k * 0.125f;
+              float es, et;
+              const float ed = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, tk, es, et);
+              if (ed < msd) { msd = ed; btau = tk; ms = es; mt = et; }
+              if (k > 0u) {
+                const float vol = seg_vol(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, tk);
+                if (pv * vol <= 0.0f && zc < 0.0f) zc = tk - 0.0625f;
+                pv = vol;
+              }
+            }
+            if (zc >= 0.0f) {
+              float es, et;
+              const float ed = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, zc, es, et);
+              if (ed < msd) { msd = ed; btau = zc; hs = 0.0625f; ms = es; mt = et; }
+            }
+            float tlo = fmaxf(0.0f, btau - hs), thi = fminf(1.0f, btau + hs);
+            float tstar = btau, dstar = msd, ss = ms, ts = mt;
+            for (int it = 0; it < 6; ++it) {
+              const float m1 = tlo + (thi - tlo) * (1.0f / 3.0f);
+              const float mm2 = thi - (thi - tlo) * (1.0f / 3.0f);
+              float e1s, e1t, e2s, e2t;
+              const float e1 = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, m1, e1s, e1t);
+              const float e2 = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, mm2, e2s, e2t);
+              if (e1 < dstar) { dstar = e1; tstar = m1; ss = e1s; ts = e1t; }
+              if (e2 < dstar) { dstar = e2; tstar = mm2; ss = e2s; ts = e2t; }
+              if (e1 < e2) thi = mm2; else tlo = m1;
+            }
+            const float ets = mixf(thu0, thu1, ss) + mixf(thj, thvj, ts);
+            if (dstar >= ets * ets) continue;
+            if (s.exclude_neighbors) {
+              const V3 a0s = vmix(p_u0o, p_u0, tstar), a1s = vmix(p_u1o, p_u1, tstar);
+              const V3 b0s = vmix(p_jo, p_j, tstar), b1s = vmix(p_vjo, p_vj, tstar);
+              const V3 t0 = a0s - b0s, t1v = a0s - b1s, t2 = a1s - b0s, t3 = a1s - b1s;
+              if (near_folded_sq(s, u0, j, dot(t0, t0)) || near_folded_sq(s, u0, vj, dot(t1v, t1v)) ||
+                  near_folded_sq(s, u1, j, dot(t2, t2)) || near_folded_sq(s, u1, vj, dot(t3, t3)))
+                continue;
+            }
+            bool utc = false;
+            if (untangle && la != lb) {
+              const bool afx = (w_u0 == 0.0f) && (w_u1 == 0.0f);
+              const bool bfx = (w_j == 0.0f) && (w_vj == 0.0f);
+              const V3 d0u = ((p_u0o + p_u1o) - (p_jo + p_vjo)) * 0.5f;
+              const V3 d1u = ((p_u0 + p_u1) - (p_j + p_vj)) * 0.5f;
+              const V3 mu = d1u - d0u;
+              if (la > lb && !afx) {
+                const V3 ni = mk(s.nrm[j]), no = mk(s.nrm[u0]);
+                const bool allow = bfx || (dot(no, no) <= 0.25f);
+                utc = allow && (dot(ni, ni) > 0.25f) && (dot(d0u, ni) < 0.0f) && (dot(mu, ni) > 0.0f);
+              } else if (lb > la && !bfx) {
+                const V3 ni = mk(s.nrm[u0]), no = mk(s.nrm[j]);
+                const bool allow = afx || (dot(no, no) <= 0.25f);
+                utc = allow && (dot(ni, ni) > 0.25f) && (dot(-d0u, ni) < 0.0f) && (dot(-mu, ni) > 0.0f);
+              }
+            }
+            if (utc) continue;
+            float s0, t0p;
+            seg_seg(p_u0o, p_u1o, p_jo, p_vjo, s0, t0p);
+            const V3 d0 = vmix(p_u0o, p_u1o, s0) - vmix(p_jo, p_vjo, t0p);
+            const float dist0 = length(d0);
+            if (dist0 > kEps) {
+              const V3 n0 = d0 / dist0;
+              float s1b, t1b;
+              seg_seg(p_u0, p_u1, p_j, p_vj, s1b, t1b);
+              const V3 d1 = vmix(p_u0, p_u1, s1b) - vmix(p_j, p_vj, t1b);
+              const float dist1 = length(d1);
+              const V3 de = vmix(p_u0, p_u1, ss) - vmix(p_j, p_vj, ts);
+              const float he = dot(de, n0);
+              const bool crossed = (he <= 0.0f) || (dot(d1, n0) <= 0.0f) || (bpair && dist1 >= ets && tstar < 1.0f);
+              if (he < ets && crossed) {
+                const float pc = ets - he;
+                const bool bpin = (w_j <= 0.0f) || (w_vj <= 0.0f);
+                if (apin && bpin) continue;
+                const bool aall = (w_u0 == 0.0f) && (w_u1 == 0.0f);
+                const bool ball = (w_j == 0.0f) && (w_vj == 0.0f);
+                const bool cpe = !(aall || ball);
+                if (bpin) {
+                  const V3 em = ((p_j - p_jo) + (p_vj - p_vjo)) * 0.5f;
+                  const float a = 1.0f - ss, b = ss;
+                  const float den = a * a * w_u0 + b * b * w_u1;
+                  if (den > kEps) {
+                    const V3 pb = n0 * pc + em * 0.5f;
+                    if (w_u0 > 0.0f) add_ccd(acc, u0, pb * fminf((a * w_u0) / den, 2.0f), cpe);
+                    if (w_u1 > 0.0f) add_ccd(acc, u1, pb * fminf((b * w_u1) / den, 2.0f), cpe);
+                  }
+                } else if (apin) {
+                  const V3 em = ((p_u0 - p_u0o) + (p_u1 - p_u1o)) * 0.5f;
+                  const float a = 1.0f - ts, b = ts;
+                  const float den = a * a * w_j + b * b * w_vj;
+                  if (den > kEps) {
+                    const V3 pb = (-n0) * pc + em * 0.5f;
+                    if (w_j > 0.0f) add_ccd(acc, j, pb * fminf((a * w_j) / den, 2.0f), cpe);
+                    if (w_vj > 0.0f) add_ccd(acc, vj, pb * fminf((b * w_vj) / den, 2.0f), cpe);
+                  }
+                } else {
+                  const float we1 = (1.0f - ss) * (1.0f - ss) * w_u0 + ss * ss * w_u1;
+                  const float we2 = (1.0f - ts) * (1.0f - ts) * w_j + ts * ts * w_vj;
+                  const float wtot = we1 + we2;
+                  if (wtot > kEps) {
+                    const V3 tcc = n0 * pc;
+                    if (w_u0 > 0.0f) add_ccd(acc, u0, tcc * ((1.0f - ss) * w_u0 / wtot), true);
+                    if (w_u1 > 0.0f) add_ccd(acc, u1, tcc * (ss * w_u1 / wtot), true);
+                    if (w_j > 0.0f) add_ccd(acc, j, (-tcc) * ((1.0f - ts) * w_j / wtot), true);
+                    if (w_vj > 0.0f) add_ccd(acc, vj, (-tcc) * (ts * w_vj / wtot), true);
+                  }
+                }
+                continue;
+              }
+            }
+          }
+          {
+            float sst, tst, d2e, eth;
+            V3 de;
+            if (has1) {
+              sst = s1; tst = t1; de = dl1; d2e = d2c; eth = ethc;
+            } else {
+              seg_seg(p_u0, p_u1, p_j, p_vj, sst, tst);
+              de = (p_u0 + (p_u1 - p_u0) * sst) - (p_j + (p_vj - p_j) * tst);
+              d2e = dot(de, de);
+              eth = mixf(thu0, thu1, sst) + mixf(thj, thvj, tst);
+            }
+            if (d2e >= eth * eth || d2e <= kEps * kEps) continue;
+            if (s.exclude_neighbors) {
+              const V3 e0 = p_u0 - p_j, e1 = p_u0 - p_vj, e2 = p_u1 - p_j, e3 = p_u1 - p_vj;
+              if (near_folded_sq(s, u0, j, dot(e0, e0)) || near_folded_sq(s, u0, vj, dot(e1, e1)) ||
+                  near_folded_sq(s, u1, j, dot(e2, e2)) || near_folded_sq(s, u1, vj, dot(e3, e3)))
+                continue;
+            }
+            const float del = sqrtf(d2e);
+            bool ute = false;
+            if (untangle) {
+              const bool afx = (w_u0 <= 0.0f) && (w_u1 <= 0.0f);
+              const bool bfx = (w_j <= 0.0f) && (w_vj <= 0.0f);
+              ute = outer_behind(s, la, lb, u0, u1, j, vj, afx, bfx, de);
+            }
+            if (!ute) {
+              const V3 ne = de / del;
+              const float pe = eth - del;
+              const bool bpin = (w_j <= 0.0f) || (w_vj <= 0.0f);
+              if (apin && bpin) continue;
+              if (bpin) {
+                const V3 em = ((p_j - p_jo) + (p_vj - p_vjo)) * 0.5f;
+                const float a = 1.0f - sst, b = sst;
+                const float den = a * a * w_u0 + b * b * w_u1;
+                if (den > kEps) {
+                  const V3 pb = ne * pe + em * 0.5f;
+                  if (w_u0 > 0.0f) add_pin(acc, u0, pb * fminf((a * w_u0) / den, 2.0f));
+                  if (w_u1 > 0.0f) add_pin(acc, u1, pb * fminf((b * w_u1) / den, 2.0f));
+                }
+              } else if (apin) {
+                const V3 em = ((p_u0 - p_u0o) + (p_u1 - p_u1o)) * 0.5f;
+                const float a = 1.0f - tst, b = tst;
+                const float den = a * a * w_j + b * b * w_vj;
+                if (den > kEps) {
+                  const V3 pb = (-ne) * pe + em * 0.5f;
+                  if (w_j > 0.0f) add_pin(acc, j, pb * fminf((a * w_j) / den, 2.0f));
+                  if (w_vj > 0.0f) add_pin(acc, vj, pb * fminf((b * w_vj) / den, 2.0f));
+                }
+              } else {
+                const float we1 = (1.0f - sst) * (1.0f - sst) * w_u0 + sst * sst * w_u1;
+                const float we2 = (1.0f - tst) * (1.0f - tst) * w_j + tst * tst * w_vj;
+                const float wtot = we1 + we2;
+                if (wtot > kEps) {
+                  const V3 td = ne * (pe * 0.6f);
+                  if (w_u0 > 0.0f) add_disp(acc, u0, td * ((1.0f - sst) * w_u0 / wtot));
+                  if (w_u1 > 0.0f) add_disp(acc, u1, td * (sst * w_u1 / wtot));
+                  if (w_j > 0.0f) add_disp(acc, j, (-td) * ((1.0f - tst) * w_j / wtot));
+                  if (w_vj > 0.0f) add_disp(acc, vj, (-td) * (tst * w_vj / wtot));
+                }
+              }
+            }
+          }
+        }
+      }
+}
+
+// ---------------- sc_apply: shaders/self_collision_apply.wgsl:57-177
+__global__ void k_apply(uint32_t n, const float4* __restrict__ x4, float4* __restrict__ p4,
+                        const float* __restrict__ local_len, int32_t* __restrict__ acc, float relief, int enable_relief,
+                        float max_disp_ratio) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int4* a4 = reinterpret_cast<int4*>(acc + (size_t)i * A_N);
+  const int4 r0 = a4[0], r1 = a4[1], r2 = a4[2], r3 = a4[3];
+  const bool pinned = x4[i].w <= 0.0f;
+  V3 fd = mk(0.f, 0.f, 0.f);
+  const uint32_t cnt = (uint32_t)r0.w;
+  if (cnt > 0u && !pinned) {
+    const V3 tdp = mk((float)r0.x, (float)r0.y, (float)r0.z) * (1.0f / 1000000.0f);
+    V3 ed = tdp / fmaxf(1.0f, sqrtf((float)cnt));
+    if (enable_relief) ed = ed * relief;
+    const float pl = length(ed);
+    const float ratio = max_disp_ratio > 0.0f ? max_disp_ratio : 0.50f;
+    const float ms = fminf(local_len[i] * ratio, 0.10f);
+    if (pl > ms && pl > kEps) ed = (ed / pl) * ms;
+    fd = fd + ed;
+  }
+  const uint32_t pc = (uint32_t)r1.w;
+  V3 avg = mk(0.f, 0.f, 0.f);
+  if (pc > 0u && !pinned) avg = (mk((float)r1.x, (float)r1.y, (float)r1.z) * (1.0f / 1000000.0f)) / (float)pc;
+  const uint32_t eec = (uint32_t)r3.w;
+  if (!pinned) {
+    const V3 cp = mk((float)r2.x, (float)r2.y, (float)r2.z) * (1.0f / 1000000.0f);
+    const V3 cn = mk((float)r2.w, (float)r3.x, (float)r3.y) * (1.0f / 1000000.0f);
+    V3 env = cp + cn;
+    if (eec >= 4u) env = env * fmaxf(0.5f, sqrtf(3.0f / (float)eec));
+    const V3 z = mk(0.f, 0.f, 0.f);
+    fd = fd + (vmax(vmax(env, z), vmax(avg, z)) + vmin(vmin(env, z), vmin(avg, z)));
+  }
+  const int4 zero = make_int4(0, 0, 0, 0);
+  a4[0] = zero; a4[1] = zero; a4[2] = zero; a4[3] = zero;
+  if (length(fd) > kEps) {
+    float4 p = p4[i];
+    p.x += fd.x; p.y += fd.y; p.z += fd.z;
+    p4[i] = p;
+  }
+}
+
+}  // namespace tcloth

@@ -1,0 +1,1208 @@
+// Simulator state, frame encoding and the C ABI (include/tcloth.h).
+//
+// One tc_sim owns all device buffers of one cloth.  A frame (substeps x
+// iterations x colours of launches) is recorded once into a CUDA graph on the
+// simulator's own stream and replayed while no parameter changes; any setter
+// marks the graph stale.  Pass order follows encode_simulation_steps
+// (crates/cloth_core/src/simulation/dispatch.rs:7-354) with the reference
+// defaults: decoupled colliders (coupled when the auto-coupling test fires),
+// self-collision once per substep after the final pin pass.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tcloth.h"
+#include "mesh.hpp"
+#include "selfcol_kernels.cuh"
+#include "solver_kernels.cuh"
+
+namespace tcloth {
+
+struct TcError : std::runtime_error {
+  tc_status code;
+  TcError(tc_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define TC_CK(expr)                                                                              \
+  do {                                                                                           \
+    cudaError_t e__ = (expr);                                                                    \
+    if (e__ != cudaSuccess)                                                                      \
+      throw TcError(e__ == cudaErrorMemoryAllocation ? TC_ERR_NOMEM : TC_ERR_CUDA,               \
+                    std::string(#expr) + ": " + cudaGetErrorString(e__));                        \
+  } while (0)
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { if (p) cudaFree(p); }
+  void alloc(size_t cnt) {
+    if (cnt <= n && p) return;
+    if (p) { cudaFree(p); p = nullptr; }
+    n = std::max<size_t>(cnt, 1);
+    TC_CK(cudaMalloc(&p, n * sizeof(T)));
+  }
+  void upload(const T* h, size_t cnt, cudaStream_t st) {
+    alloc(cnt);
+    if (cnt) TC_CK(cudaMemcpyAsync(p, h, cnt * sizeof(T), cudaMemcpyHostToDevice, st));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t st) { upload(v.data(), v.size(), st); }
+};
+
+struct PinH {
+  float target[3];
+  float weight;
+};
+
+struct Sim {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  MeshData m;
+  uint32_t n = 0, nd = 0, nb = 0, ne = 0;
+  // host mirrors
+  std::vector<float> orig_w, init_w, init_pos;
+  std::vector<int64_t> orig_edge_to_dist;
+  std::vector<float> mult;  // per sorted distance constraint
+  std::vector<DistC> dist_h;
+  std::vector<BendC> bend_h;
+  std::vector<float> base_rest;
+  float base_tc = 0, base_cc = 0, base_shc = 0, base_bk = 0;
+  // device state
+  DBuf<float4> x4, p4, v4;
+  DBuf<float> local_len, dlam, blam, th_rest;
+  DBuf<uint2> dist_ids, star_idx, edges;
+  DBuf<float4> dist_par, bend_par;
+  DBuf<uint4> bend_ids;
+  DBuf<uint32_t> adj_off, adj_idx, th_off, th_idx, star_off, edge_bits;
+  DBuf<uint32_t> keys, counts, cursor, cs, srt, ekeys, ecs, esrt;
+  DBuf<float4> nrm;
+  DBuf<int32_t> acc;
+  // colliders
+  std::vector<Prim> prims_h;
+  std::vector<MeshTri> tris_h;
+  DBuf<Prim> prims;
+  DBuf<MeshTri> tris;
+  DBuf<float4> bounds, cl16, cl256;
+  // pins
+  std::map<uint32_t, PinH> pins;
+  DBuf<uint32_t> pin_v;
+  DBuf<float4> pin_t;
+  // residual instrumentation
+  bool track_residual = false;
+  DBuf<float> res_sum, res_max;  // [ndc + nbc] each
+  // parameters (simulation/mod.rs:607-690 defaults)
+  float g[3] = {0.f, 0.f, -9.81f};
+  float damping = 1.0f, td = 0.f, cd = 0.f, sd = 0.f, bd = 0.f;
+  uint32_t iters = 2;
+  bool self_collision = true;
+  float relief = 0.2f, max_disp_ratio = 0.2f;
+  bool enable_relief = true, exclude_neighbors = true, untangle_opt = true;
+  uint32_t max_search = 256;
+  bool coupled = false, auto_coupled = true, recovery = true;
+  float cloth_thickness = 0.005f;
+  float last_max_disp = 0.f, last_eff_disp = 0.f;
+  std::vector<float> prev_frame_pos;
+  // graph cache
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_dirty = true;
+  float g_dt = -1.f;
+  uint32_t g_sub = 0;
+  bool g_coupled = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool async_pending = false;
+  // per-pass profiling (GpuProfiler / take_profile, simulation/profile.rs:38-252):
+  // when on, frames run eagerly with an event pair around every launch group
+  bool profiling = false;
+  struct Mark { const char* name; cudaEvent_t a, b; };
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<std::string> prof_names;
+  std::vector<double> prof_ms;
+  std::vector<uint32_t> prof_cnt;
+
+  cudaEvent_t ev_get() {
+    if (ev_used == ev_pool.size()) {
+      cudaEvent_t e;
+      TC_CK(cudaEventCreate(&e));
+      ev_pool.push_back(e);
+    }
+    return ev_pool[ev_used++];
+  }
+  template <class F>
+  void timed(const char* name, F&& f) {
+    if (!profiling) { f(); return; }
+    cudaEvent_t a = ev_get(), b = ev_get();
+    TC_CK(cudaEventRecord(a, st));
+    f();
+    TC_CK(cudaEventRecord(b, st));
+    marks.push_back({name, a, b});
+  }
+  void collect_marks() {
+    for (const auto& mk : marks) {
+      float ms = 0.f;
+      TC_CK(cudaEventElapsedTime(&ms, mk.a, mk.b));
+      size_t k = 0;
+      while (k < prof_names.size() && prof_names[k] != mk.name) ++k;
+      if (k == prof_names.size()) { prof_names.push_back(mk.name); prof_ms.push_back(0.0); prof_cnt.push_back(0); }
+      prof_ms[k] += ms;
+      prof_cnt[k] += 1;
+    }
+    marks.clear();
+    ev_used = 0;
+  }
+
+  ~Sim() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  void mark() { graph_dirty = true; }
+
+  // ---- upload of the vertex state from host arrays
+  void upload_vertices(const float* pos, const float* vel, const float* w) {
+    std::vector<float4> hx(n), hp(n), hv(n);
+    for (uint32_t i = 0; i < n; ++i) {
+      hx[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], w[i]);
+      hp[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], m.thickness[i]);
+      float vx = vel ? vel[3 * i] : 0.f, vy = vel ? vel[3 * i + 1] : 0.f, vz = vel ? vel[3 * i + 2] : 0.f;
+      uint32_t layer = m.layer[i];
+      float lf;
+      std::memcpy(&lf, &layer, 4);
+      hv[i] = make_float4(vx, vy, vz, lf);
+    }
+    x4.upload(hx, st);
+    p4.upload(hp, st);
+    v4.upload(hv, st);
+    TC_CK(cudaStreamSynchronize(st));
+  }
+
+  void upload_dist() {
+    std::vector<uint2> ids(nd);
+    std::vector<float4> par(nd);
+    for (uint32_t i = 0; i < nd; ++i) {
+      ids[i] = make_uint2(dist_h[i].v0, dist_h[i].v1);
+      par[i] = make_float4(dist_h[i].rest, dist_h[i].tc, dist_h[i].cc, dist_h[i].type == 1 ? 1.f : 0.f);
+    }
+    dist_ids.upload(ids, st);
+    dist_par.upload(par, st);
+    TC_CK(cudaStreamSynchronize(st));
+  }
+  void upload_bend() {
+    std::vector<uint4> ids(nb);
+    std::vector<float4> par(nb);
+    for (uint32_t i = 0; i < nb; ++i) {
+      const BendC& c = bend_h[i];
+      ids[i] = make_uint4(c.v0, c.v1, c.v2, c.v3);
+      par[i] = make_float4(c.rest, c.comp, c.pad0, c.pad1);
+    }
+    bend_ids.upload(ids, st);
+    bend_par.upload(par, st);
+    TC_CK(cudaStreamSynchronize(st));
+  }
+
+  void init(const MeshInput& in, int dev) {
+    device = dev;
+    TC_CK(cudaSetDevice(device));
+    TC_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    TC_CK(cudaEventCreate(&ev0));
+    TC_CK(cudaEventCreate(&ev1));
+    m = build_mesh(in);
+    n = m.n;
+    nd = uint32_t(m.dist.size());
+    nb = uint32_t(m.bend.size());
+    ne = uint32_t(m.edges.size() / 2);
+    dist_h = m.dist;
+    bend_h = m.bend;
+    orig_edge_to_dist = m.orig_edge_to_dist;
+    mult.assign(nd, 1.f);
+    base_rest.resize(nd);
+    for (uint32_t i = 0; i < nd; ++i) base_rest[i] = dist_h[i].rest;
+    // base compliances (simulation/mod.rs:419-434)
+    base_tc = base_cc = 1.f / 500.f;
+    base_shc = 1.f / 250.f;
+    bool got_t = false, got_s = false;
+    for (const auto& c : dist_h) {
+      if (c.type == 1) { if (!got_s) { base_shc = c.tc; got_s = true; } }
+      else if (!got_t) { base_tc = c.tc; base_cc = c.cc; got_t = true; }
+    }
+    base_bk = in.bending_k > 0.f ? in.bending_k : 0.f;
+    orig_w = m.inv_mass;
+    init_w = m.inv_mass;
+    init_pos = m.pos;
+    prev_frame_pos = m.pos;
+    upload_vertices(m.pos.data(), nullptr, m.inv_mass.data());
+    local_len.upload(m.local_len, st);
+    upload_dist();
+    upload_bend();
+    dlam.alloc(nd);
+    blam.alloc(nb);
+    adj_off.upload(m.adj_off, st);
+    adj_idx.upload(m.adj_idx, st);
+    th_off.upload(m.th_off, st);
+    th_idx.upload(m.th_idx, st);
+    th_rest.upload(m.th_rest, st);
+    star_off.upload(m.star_off, st);
+    star_idx.upload(reinterpret_cast<const uint2*>(m.star_idx.data()), m.star_idx.size() / 2, st);
+    edges.upload(reinterpret_cast<const uint2*>(m.edges.data()), ne, st);
+    edge_bits.upload(m.edge_bits, st);
+    const size_t T = m.table;
+    keys.alloc(n); counts.alloc(T + 1); cursor.alloc(T + 1); cs.alloc(T + 1); srt.alloc(n);
+    ekeys.alloc(ne); ecs.alloc(T + 1); esrt.alloc(ne);
+    nrm.alloc(n);
+    acc.alloc(size_t(n) * A_N);
+    TC_CK(cudaMemsetAsync(acc.p, 0, size_t(n) * A_N * sizeof(int32_t), st));
+    TC_CK(cudaMemsetAsync(nrm.p, 0, size_t(n) * sizeof(float4), st));
+    res_sum.alloc(m.dist_cnt.size() + m.bend_cnt.size() + 1);
+    res_max.alloc(m.dist_cnt.size() + m.bend_cnt.size() + 1);
+    prims.alloc(1); tris.alloc(1); bounds.alloc(1); cl16.alloc(1); cl256.alloc(1);
+    pin_v.alloc(1); pin_t.alloc(1);
+    TC_CK(cudaStreamSynchronize(st));
+  }
+
+  // ---- colliders
+  void upload_prims() {
+    prims.upload(prims_h, st);
+    TC_CK(cudaStreamSynchronize(st));
+    mark();
+  }
+  uint32_t graph_ntris = UINT32_MAX;
+  void set_mesh(const float* t9, uint32_t T, float fric, float thick, float rest, bool single, const float* attr) {
+    std::vector<MeshTri> v(T);
+    for (uint32_t t = 0; t < T; ++t) {
+      const float* q = t9 + 9 * size_t(t);
+      float f = fric, th = thick, r = rest;
+      uint32_t flags = single ? 1u : 0u;
+      if (attr) {
+        f = attr[4 * t]; th = attr[4 * t + 1]; r = attr[4 * t + 2];
+        float fl = std::round(attr[4 * t + 3]);
+        flags = fl > 0.f ? (fl >= 4294967295.f ? UINT32_MAX : uint32_t(fl)) : 0u;
+      }
+      float fb;
+      std::memcpy(&fb, &flags, 4);
+      v[t] = MeshTri{make_float4(q[0], q[1], q[2], f), make_float4(q[3], q[4], q[5], th),
+                     make_float4(q[6], q[7], q[8], r), make_float4(fb, 0.f, 0.f, 0.f)};
+    }
+    tris_h.swap(v);
+    upload_tris();
+  }
+  // Morton sort of centroids (stable), bounding spheres
+  // (simulation/mod.rs:2613-2670) and the two conservative culling levels.
+  void upload_tris() {
+    const uint32_t T = uint32_t(tris_h.size());
+    if (T == 0) { mark(); graph_ntris = 0; return; }
+    auto cen = [](const MeshTri& t, int a) {
+      const float* p0 = &t.p0f.x; const float* p1 = &t.p1t.x; const float* p2 = &t.p2r.x;
+      return (p0[a] + p1[a] + p2[a]) / 3.0f;
+    };
+    float bmin[3] = {3.4028235e38f, 3.4028235e38f, 3.4028235e38f}, bmax[3] = {-3.4028235e38f, -3.4028235e38f, -3.4028235e38f};
+    for (const auto& t : tris_h)
+      for (int a = 0; a < 3; ++a) { bmin[a] = std::fmin(bmin[a], cen(t, a)); bmax[a] = std::fmax(bmax[a], cen(t, a)); }
+    float inv[3];
+    for (int a = 0; a < 3; ++a) inv[a] = 1.f / std::fmax(bmax[a] - bmin[a], 1e-5f);
+    std::vector<std::pair<uint32_t, uint32_t>> ki(T);
+    for (uint32_t t = 0; t < T; ++t) ki[t] = {morton3(cen(tris_h[t], 0), cen(tris_h[t], 1), cen(tris_h[t], 2), bmin, inv), t};
+    std::sort(ki.begin(), ki.end());
+    std::vector<MeshTri> sorted(T);
+    for (uint32_t t = 0; t < T; ++t) sorted[t] = tris_h[ki[t].second];
+    tris_h.swap(sorted);
+    std::vector<float4> bd(T);
+    for (uint32_t t = 0; t < T; ++t) {
+      const MeshTri& q = tris_h[t];
+      float cx = cen(q, 0), cy = cen(q, 1), cz = cen(q, 2);
+      auto d2 = [&](const float4& p) {
+        float ax = p.x - cx, ay = p.y - cy, az = p.z - cz;
+        return ax * ax + ay * ay + az * az;
+      };
+      float r = std::sqrt(std::fmax(std::fmax(d2(q.p0f), d2(q.p1t)), d2(q.p2r))) + q.p1t.w;
+      bd[t] = make_float4(cx, cy, cz, r);
+    }
+    auto group = [&](uint32_t b, uint32_t e) {
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (uint32_t t = b; t < e; ++t) {
+        double R = 1.5 * double(bd[t].w);
+        const double c[3] = {bd[t].x, bd[t].y, bd[t].z};
+        for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], c[a] - R); hi[a] = std::max(hi[a], c[a] + R); }
+      }
+      double C[3] = {(lo[0] + hi[0]) * 0.5, (lo[1] + hi[1]) * 0.5, (lo[2] + hi[2]) * 0.5};
+      double Rg = 0.0;
+      for (uint32_t t = b; t < e; ++t) {
+        double dx = bd[t].x - C[0], dy = bd[t].y - C[1], dz = bd[t].z - C[2];
+        Rg = std::max(Rg, std::sqrt(dx * dx + dy * dy + dz * dz) + 1.5 * double(bd[t].w));
+      }
+      Rg = Rg * (1.0 + 1e-5) + 1e-7;
+      return make_float4(float(C[0]), float(C[1]), float(C[2]), float(Rg));
+    };
+    const uint32_t n16 = (T + 15) / 16, n256 = (T + 255) / 256;
+    std::vector<float4> g16(n16), g256(n256);
+    for (uint32_t g = 0; g < n16; ++g) g16[g] = group(g * 16, std::min(T, g * 16 + 16));
+    for (uint32_t g = 0; g < n256; ++g) g256[g] = group(g * 256, std::min(T, g * 256 + 256));
+    const void* before[4] = {tris.p, bounds.p, cl16.p, cl256.p};
+    tris.upload(tris_h, st);
+    bounds.upload(bd, st);
+    cl16.upload(g16, st);
+    cl256.upload(g256, st);
+    TC_CK(cudaStreamSynchronize(st));
+    // the recorded frame only holds pointers and the triangle count: new
+    // contents of the same size replay without re-recording
+    const void* after[4] = {tris.p, bounds.p, cl16.p, cl256.p};
+    if (T != graph_ntris || std::memcmp(before, after, sizeof before) != 0) mark();
+    graph_ntris = T;
+  }
+
+  // ---- pins
+  void upload_pins() {
+    std::vector<uint32_t> v;
+    std::vector<float4> t;
+    for (const auto& kv : pins) {
+      v.push_back(kv.first);
+      t.push_back(make_float4(kv.second.target[0], kv.second.target[1], kv.second.target[2], kv.second.weight));
+    }
+    pin_v.upload(v, st);
+    pin_t.upload(t, st);
+    TC_CK(cudaStreamSynchronize(st));
+    mark();
+  }
+  void write_inv_mass(uint32_t v, float w) {
+    TC_CK(cudaMemcpyAsync(reinterpret_cast<char*>(x4.p) + size_t(v) * sizeof(float4) + 12, &w, 4,
+                          cudaMemcpyHostToDevice, st));
+    TC_CK(cudaStreamSynchronize(st));
+  }
+  static float clamp_w(float w) { return std::isfinite(w) ? std::fmin(std::fmax(w, 0.f), 1.f) : 0.f; }
+
+  // ---- compliance
+  static float scale_compliance(float base, float mlt) {
+    if (base >= 1e9f) return base;
+    if (base <= 0.f) return 0.f;
+    return base / mlt;
+  }
+  void apply_distance_compliances() {
+    for (uint32_t i = 0; i < nd; ++i) {
+      float ml = std::fmax(mult[i], 1e-3f);
+      if (dist_h[i].type == 1) dist_h[i].tc = dist_h[i].cc = scale_compliance(base_shc, ml);
+      else { dist_h[i].tc = scale_compliance(base_tc, ml); dist_h[i].cc = scale_compliance(base_cc, ml); }
+    }
+    upload_dist();
+    mark();
+  }
+
+  SCArgs sc_args() {
+    SCArgs a;
+    a.n = n; a.ne = ne; a.table = m.table; a.cell = m.cell;
+    a.relief = relief; a.enable_relief = enable_relief; a.max_disp_ratio = max_disp_ratio;
+    a.exclude_neighbors = exclude_neighbors; a.untangle = (untangle_opt && m.multi_layer) ? 1 : 0;
+    a.max_search = max_search;
+    a.x4 = x4.p; a.p4 = p4.p; a.v4 = v4.p; a.local_len = local_len.p;
+    a.adj_off = adj_off.p; a.adj_idx = adj_idx.p; a.th_off = th_off.p; a.th_idx = th_idx.p; a.th_rest = th_rest.p;
+    a.star_off = star_off.p; a.star_idx = star_idx.p; a.edges = edges.p; a.edge_bits = edge_bits.p;
+    a.cs = cs.p; a.srt = srt.p; a.ecs = ecs.p; a.esrt = esrt.p; a.nrm = nrm.p; a.acc = acc.p;
+    return a;
+  }
+
+  static unsigned grid(uint32_t cnt, unsigned b) { return (cnt + b - 1) / b; }
+
+  void encode_hash(int which) {
+    const uint32_t cnt = which == 0 ? n : ne;
+    const uint32_t T = m.table;
+    uint32_t* k = which == 0 ? keys.p : ekeys.p;
+    uint32_t* start = which == 0 ? cs.p : ecs.p;
+    uint32_t* sorted = which == 0 ? srt.p : esrt.p;
+    TC_CK(cudaMemsetAsync(counts.p, 0, (T + 1) * sizeof(uint32_t), st));
+    TC_CK(cudaMemsetAsync(cursor.p, 0, (T + 1) * sizeof(uint32_t), st));
+    timed(which == 0 ? "hash_vertices" : "hash_edges", [&] {
+      if (cnt) k_hash_count<<<grid(cnt, 256), 256, 0, st>>>(cnt, which, p4.p, edges.p, m.cell, T, k, counts.p);
+      k_hash_scan<<<1, 1024, 0, st>>>(T, counts.p, start);
+      if (cnt) k_hash_scatter<<<grid(cnt, 256), 256, 0, st>>>(cnt, k, start, cursor.p, sorted);
+      k_hash_sort_buckets<<<grid(T, 256), 256, 0, st>>>(T, start, sorted);
+    });
+  }
+
+  void encode_self_collision() {
+    SCArgs a = sc_args();
+    if (a.untangle) timed("sc_normals", [&] { k_normals<<<grid(n, 256), 256, 0, st>>>(n, x4.p, star_off.p, star_idx.p, nrm.p); });
+    encode_hash(0);
+    if (ne > 0) encode_hash(1);
+    timed("sc_solve", [&] { k_sc_solve<<<grid(n, 128), 128, 0, st>>>(a); });
+    if (a.untangle) timed("sc_untangle", [&] { k_untangle<<<grid(n, 128), 128, 0, st>>>(a); });
+    if (ne > 0) timed("sc_solve_ee", [&] { k_ee<<<grid(ne, 128), 128, 0, st>>>(a); });
+    timed("sc_apply", [&] {
+      k_apply<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, local_len.p, acc.p, relief, enable_relief ? 1 : 0,
+                                             max_disp_ratio);
+    });
+  }
+
+  ColliderArgs collider_args() {
+    ColliderArgs c;
+    c.prims = prims.p; c.nprims = uint32_t(prims_h.size());
+    c.tris = tris.p; c.bounds = bounds.p; c.cl16 = cl16.p; c.cl256 = cl256.p; c.ntris = uint32_t(tris_h.size());
+    c.recovery = recovery;
+    return c;
+  }
+
+  void encode_residual(const SubstepParams& sp);
+
+  // encode_simulation_steps (dispatch.rs:7-354) for one frame
+  void encode_frame(float dt, uint32_t substeps, bool use_coupled) {
+    const float dts = dt / float(substeps);
+    SubstepParams sp{dts, g[0], g[1], g[2], damping, td, cd, sd, bd};
+    const bool ddamp = td != 0.f || cd != 0.f || sd != 0.f;
+    const bool bdamp = bd != 0.f;
+    const bool hascol = !prims_h.empty() || !tris_h.empty();
+    const uint32_t npins = uint32_t(pins.size());
+    ColliderArgs ca = collider_args();
+    for (uint32_t s = 0; s < substeps; ++s) {
+      if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
+      if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
+      timed("predict", [&] { k_predict<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp); });
+      for (uint32_t it = 0; it < iters; ++it) {
+        if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
+        timed("distance", [&] {
+          for (size_t c = 0; c < m.dist_cnt.size(); ++c)
+            if (m.dist_cnt[c])
+              k_distance<<<grid(m.dist_cnt[c], 256), 256, 0, st>>>(m.dist_off[c], m.dist_cnt[c], dist_ids.p,
+                                                                    dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
+        });
+        timed("bending", [&] {
+          for (size_t c = 0; c < m.bend_cnt.size(); ++c)
+            if (m.bend_cnt[c])
+              k_bending<<<grid(m.bend_cnt[c], 256), 256, 0, st>>>(m.bend_off[c], m.bend_cnt[c], bend_ids.p,
+                                                                   bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
+        });
+        if (hascol && use_coupled) timed("collision", [&] { k_collision<<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts); });
+      }
+      if (track_residual && s + 1 == substeps) encode_residual(sp);
+      if (hascol && !use_coupled) timed("collision", [&] { k_collision<<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts); });
+      if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
+      if (self_collision) encode_self_collision();
+      timed("update_vel", [&] { k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, dts); });
+    }
+    TC_CK(cudaGetLastError());
+  }
+
+  // auto-coupled decision (dispatch.rs:93-102)
+  bool coupled_for(float dt, uint32_t substeps) const {
+    const float dts = dt / float(substeps);
+    const float ga = std::sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+    const float ff = 0.5f * ga * dts * dts;
+    const float emd = std::fmax(last_eff_disp, last_max_disp);
+    const float sdp = std::fmax(ff, emd / std::fmax(float(substeps), 1.f));
+    const float sm = std::fmax(cloth_thickness * 0.8f, 0.002f);
+    return coupled || (auto_coupled && sdp > sm * 0.25f);
+  }
+
+  void launch_frame(float dt, uint32_t substeps) {
+    if (n == 0) return;
+    const bool use_coupled = coupled_for(dt, substeps);
+    if (profiling) {
+      TC_CK(cudaEventRecord(ev0, st));
+      encode_frame(dt, substeps, use_coupled);
+      TC_CK(cudaEventRecord(ev1, st));
+      TC_CK(cudaStreamSynchronize(st));
+      collect_marks();
+      return;
+    }
+    if (graph_dirty || !gexec || g_dt != dt || g_sub != substeps || g_coupled != use_coupled) {
+      if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+      cudaGraph_t graph = nullptr;
+      TC_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        encode_frame(dt, substeps, use_coupled);
+      } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      TC_CK(cudaStreamEndCapture(st, &graph));
+      size_t nn = 0;
+      TC_CK(cudaGraphGetNodes(graph, nullptr, &nn));
+      std::vector<cudaGraphNode_t> nodes(nn);
+      if (nn) TC_CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+      graph_kernels = 0;
+      for (auto nd_ : nodes) {
+        cudaGraphNodeType t;
+        TC_CK(cudaGraphNodeGetType(nd_, &t));
+        if (t == cudaGraphNodeTypeKernel) ++graph_kernels;
+      }
+      cudaError_t e = cudaGraphInstantiate(&gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      TC_CK(e);
+      graph_dirty = false;
+      g_dt = dt;
+      g_sub = substeps;
+      g_coupled = use_coupled;
+    }
+    if (track_residual) {
+      const size_t k = m.dist_cnt.size() + m.bend_cnt.size();
+      TC_CK(cudaMemsetAsync(res_sum.p, 0, (k + 1) * sizeof(float), st));
+      TC_CK(cudaMemsetAsync(res_max.p, 0, (k + 1) * sizeof(float), st));
+    }
+    TC_CK(cudaEventRecord(ev0, st));
+    TC_CK(cudaGraphLaunch(gexec, st));
+    TC_CK(cudaEventRecord(ev1, st));
+  }
+
+  uint32_t graph_kernels = 0;
+  void step(float dt, uint32_t substeps) {
+    launch_frame(dt, substeps);
+    TC_CK(cudaStreamSynchronize(st));
+    TC_CK(cudaGetLastError());
+  }
+
+  void get_positions(float* out) {
+    std::vector<float4> h(n);
+    TC_CK(cudaMemcpyAsync(h.data(), x4.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < n; ++i) { out[3 * i] = h[i].x; out[3 * i + 1] = h[i].y; out[3 * i + 2] = h[i].z; }
+  }
+};
+
+// Residual |C(x) + alpha~ lambda| per constraint after the last iteration,
+// reduced per colour into (sum of squares, max).
+__global__ void k_residual_dist(uint32_t off, uint32_t cnt, const uint2* ids, const float4* par, const float4* p4,
+                                const float* lam, float dt, float* sum, float* mx) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  float r = 0.f;
+  if (k < cnt) {
+    const uint32_t ci = off + k;
+    const uint2 e = ids[ci];
+    const float4 c = par[ci];
+    const float dist = length(mk(p4[e.x]) - mk(p4[e.y]));
+    const float cv = dist - c.x;
+    const float comp = cv >= 0.f ? c.y : c.z;
+    if (comp < 1e9f) r = fabsf(cv + comp / (dt * dt) * lam[ci]);
+  }
+  float s = r * r, m2 = r;
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    m2 = fmaxf(m2, __shfl_down_sync(0xffffffffu, m2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(sum, s);
+    atomicMax(reinterpret_cast<int*>(mx), __float_as_int(m2));
+  }
+}
+__global__ void k_residual_bend(uint32_t off, uint32_t cnt, const uint4* ids, const float4* par, const float4* p4,
+                                const float* lam, float dt, float* sum, float* mx) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  float r = 0.f;
+  if (k < cnt) {
+    const uint32_t ci = off + k;
+    const uint4 e = ids[ci];
+    const float4 c = par[ci];
+    if (c.y < 1e9f) {
+      const float cv = length(mk(p4[e.z]) - mk(p4[e.w])) - c.x;
+      r = fabsf(cv + c.y / (dt * dt) * lam[ci]);
+    }
+  }
+  float s = r * r, m2 = r;
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    m2 = fmaxf(m2, __shfl_down_sync(0xffffffffu, m2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(sum, s);
+    atomicMax(reinterpret_cast<int*>(mx), __float_as_int(m2));
+  }
+}
+
+void Sim::encode_residual(const SubstepParams& sp) {
+  const float dt = fmaxf(sp.dt, 1e-8f);
+  const size_t kd = m.dist_cnt.size();
+  for (size_t c = 0; c < kd; ++c)
+    if (m.dist_cnt[c])
+      k_residual_dist<<<grid(m.dist_cnt[c], 256), 256, 0, st>>>(m.dist_off[c], m.dist_cnt[c], dist_ids.p, dist_par.p,
+                                                                 p4.p, dlam.p, dt, res_sum.p + c, res_max.p + c);
+  for (size_t c = 0; c < m.bend_cnt.size(); ++c)
+    if (m.bend_cnt[c])
+      k_residual_bend<<<grid(m.bend_cnt[c], 256), 256, 0, st>>>(m.bend_off[c], m.bend_cnt[c], bend_ids.p, bend_par.p,
+                                                                 p4.p, blam.p, dt, res_sum.p + kd + c,
+                                                                 res_max.p + kd + c);
+}
+
+}  // namespace tcloth
+
+// ===================================================================
+// C ABI
+// ===================================================================
+using tcloth::Sim;
+using tcloth::TcError;
+
+struct tc_sim {
+  Sim s;
+};
+
+static thread_local std::string g_err;
+
+template <class F>
+static tc_status guard(F&& f) {
+  try {
+    f();
+    g_err.clear();
+    return TC_OK;
+  } catch (const TcError& e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return TC_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return TC_ERR_CUDA;
+  }
+}
+static void need(bool ok, const char* msg) {
+  if (!ok) throw TcError(TC_ERR_INVALID, msg);
+}
+static Sim& S(tc_sim* s) {
+  need(s != nullptr, "null simulator handle");
+  TC_CK(cudaSetDevice(s->s.device));
+  return s->s;
+}
+
+extern "C" {
+
+const char* tc_last_error(void) { return g_err.c_str(); }
+
+int tc_gpu_available(void) {
+  int cnt = 0;
+  if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+    cudaGetLastError();
+    return 0;
+  }
+  for (int d = 0; d < cnt; ++d) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10) return 1;
+  }
+  return 0;
+}
+
+tc_status tc_device_name(int device, char* buf, size_t len) {
+  return guard([&] {
+    need(buf && len > 0, "buffer required");
+    cudaDeviceProp p;
+    TC_CK(cudaGetDeviceProperties(&p, device));
+    std::snprintf(buf, len, "%s", p.name);
+  });
+}
+
+tc_status tc_create(tc_sim** out, const float* positions, uint32_t n, const uint32_t* edges, uint32_t ne,
+                    const uint32_t* faces, uint32_t nf, const float* inv_masses, const uint32_t* layer_ids,
+                    const float* thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
+                    float compression_stiffness, float shear_stiffness, float bending_stiffness, int device) {
+  return guard([&] {
+    need(out != nullptr, "out handle required");
+    *out = nullptr;
+    need(positions != nullptr || n == 0, "positions required");
+    need(edges != nullptr || ne == 0, "edges required");
+    for (uint32_t e = 0; e < ne; ++e)
+      need(edges[2 * size_t(e)] < n && edges[2 * size_t(e) + 1] < n, "edges contain an index >= number of vertices");
+    for (uint32_t f = 0; f < nf; ++f)
+      for (int k = 0; k < 3; ++k) need(faces[3 * size_t(f) + k] < n, "faces contain an index >= number of vertices");
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || device < 0 || device >= cnt) {
+      cudaGetLastError();
+      throw TcError(TC_ERR_CUDA, "GPU initialisation failed: no CUDA device " + std::to_string(device));
+    }
+    tcloth::MeshInput in;
+    in.pos = positions; in.n = n; in.edges = edges; in.ne = ne;
+    in.faces = nf ? faces : nullptr; in.nf = nf;
+    in.inv_masses = inv_masses; in.layer_ids = layer_ids; in.thicknesses = thicknesses;
+    in.layer_id = layer_id; in.thickness = thickness;
+    in.tension_k = tension_stiffness; in.compression_k = compression_stiffness;
+    in.shear_k = shear_stiffness; in.bending_k = bending_stiffness;
+    std::unique_ptr<tc_sim> h(new tc_sim);
+    h->s.init(in, device);
+    *out = h.release();
+  });
+}
+
+tc_status tc_destroy(tc_sim* s) {
+  return guard([&] {
+    if (!s) return;
+    cudaSetDevice(s->s.device);
+    cudaStreamSynchronize(s->s.st);
+    delete s;
+  });
+}
+
+tc_status tc_step(tc_sim* s, float dt, uint32_t substeps, uint32_t* eff) {
+  return guard([&] {
+    Sim& m = S(s);
+    const uint32_t sub = substeps ? substeps : 20u;
+    m.step(dt, sub);
+    if (eff) *eff = sub;
+  });
+}
+
+tc_status tc_step_async(tc_sim* s, float dt, uint32_t substeps) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.launch_frame(dt, substeps ? substeps : 20u);
+    m.async_pending = true;
+  });
+}
+
+// fetch_positions (dispatch.rs:808-863): waits for the pending frame, copies
+// positions and updates the displacement feedback used by auto-coupling.
+tc_status tc_fetch_positions(tc_sim* s, float* out, size_t out_len, int* ok) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (ok) *ok = 0;
+    if (!m.async_pending) return;
+    need(out != nullptr && out_len >= size_t(m.n) * 3, "out_array too small");
+    m.get_positions(out);
+    m.async_pending = false;
+    float md = 0.f;
+    for (size_t i = 0; i < size_t(m.n) * 3; ++i) md = std::fmax(md, std::fabs(out[i] - m.prev_frame_pos[i]));
+    std::memcpy(m.prev_frame_pos.data(), out, size_t(m.n) * 3 * sizeof(float));
+    m.last_max_disp = md;
+    if (ok) *ok = 1;
+  });
+}
+
+tc_status tc_get_positions(tc_sim* s, float* out, size_t out_len) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr && out_len >= size_t(m.n) * 3, "output array too small");
+    m.get_positions(out);
+  });
+}
+
+tc_status tc_set_positions_and_velocities(tc_sim* s, const float* pos, const float* vel, uint32_t n) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (m.n == 0 || n != m.n || !pos) return;  // the reference ignores a length mismatch
+    std::vector<float> w(m.n);
+    for (uint32_t i = 0; i < m.n; ++i) {
+      auto it = m.pins.find(i);
+      w[i] = it != m.pins.end() ? m.orig_w[i] * (1.f - Sim::clamp_w(it->second.weight)) : m.orig_w[i];
+    }
+    m.upload_vertices(pos, vel, w.data());
+  });
+}
+
+tc_status tc_reset(tc_sim* s) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.pins.clear();
+    m.upload_pins();
+    m.upload_vertices(m.init_pos.data(), nullptr, m.init_w.data());
+    for (uint32_t i = 0; i < m.nd; ++i) m.dist_h[i].rest = m.base_rest[i];
+    std::fill(m.mult.begin(), m.mult.end(), 1.f);
+    m.apply_distance_compliances();
+    TC_CK(cudaMemsetAsync(m.acc.p, 0, size_t(m.n) * tcloth::A_N * sizeof(int32_t), m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+  });
+}
+
+tc_status tc_set_gravity(tc_sim* s, float gx, float gy, float gz) {
+  return guard([&] { Sim& m = S(s); m.g[0] = gx; m.g[1] = gy; m.g[2] = gz; m.mark(); });
+}
+tc_status tc_set_damping(tc_sim* s, float d) {
+  return guard([&] { Sim& m = S(s); m.damping = std::fmax(d, 0.f); m.mark(); });
+}
+tc_status tc_set_damping_all(tc_sim* s, float t, float c, float sh, float b) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.td = std::fmax(t, 0.f); m.cd = std::fmax(c, 0.f); m.sd = std::fmax(sh, 0.f); m.bd = std::fmax(b, 0.f);
+    m.mark();
+  });
+}
+tc_status tc_set_solver_iterations(tc_sim* s, uint32_t it) {
+  return guard([&] { Sim& m = S(s); m.iters = std::max(it, 1u); m.mark(); });
+}
+// set_stiffness_all (simulation/mod.rs:1106-1170)
+tc_status tc_set_stiffness_all(tc_sim* s, float t, float c, float sh, float b) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.base_tc = tcloth::stiffness_to_compliance(t);
+    m.base_cc = tcloth::stiffness_to_compliance(c);
+    m.base_shc = tcloth::stiffness_to_compliance(sh);
+    m.base_bk = b > 0.f ? b : 0.f;
+    m.apply_distance_compliances();
+    const float bc = b > 0.f ? 1.f / b : 1e10f;
+    for (auto& q : m.bend_h) q.comp = q.pad0 > 1.5f ? std::fmax(bc * 10.f, 0.5f) : bc;
+    m.upload_bend();
+    m.mark();
+  });
+}
+tc_status tc_set_compliance_all(tc_sim* s, float t, float c, float sh, float b) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.base_tc = t; m.base_cc = c; m.base_shc = sh;
+    for (auto& q : m.dist_h) {
+      if (q.type == 1) q.tc = q.cc = sh;
+      else { q.tc = t; q.cc = c; }
+    }
+    m.upload_dist();
+    for (auto& q : m.bend_h) q.comp = q.pad0 > 1.5f ? std::fmax(b * 10.f, 0.5f) : b;
+    m.upload_bend();
+    m.mark();
+  });
+}
+// set_edge_stiffness_multipliers (simulation/mod.rs:1494-1525)
+tc_status tc_set_edge_stiffness_multipliers(tc_sim* s, const uint32_t* idx, const float* ml, uint32_t count) {
+  return guard([&] {
+    Sim& m = S(s);
+    bool changed = false;
+    for (uint32_t i = 0; i < count; ++i) {
+      const uint32_t e = idx[i];
+      if (e >= m.orig_edge_to_dist.size()) continue;
+      const int64_t ci = m.orig_edge_to_dist[e];
+      if (ci < 0) continue;
+      const float v = std::isfinite(ml[i]) ? std::fmax(ml[i], 1e-3f) : 1.f;
+      if (std::fabs(m.mult[size_t(ci)] - v) > 1e-6f) { m.mult[size_t(ci)] = v; changed = true; }
+    }
+    if (changed) m.apply_distance_compliances();
+  });
+}
+tc_status tc_set_enable_self_collision(tc_sim* s, int on) {
+  return guard([&] { Sim& m = S(s); m.self_collision = on != 0; m.mark(); });
+}
+tc_status tc_set_self_collision_options(tc_sim* s, float relief, float ratio, int excl, int untangle, uint32_t maxit) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.relief = relief; m.max_disp_ratio = ratio; m.enable_relief = relief < 0.999f;
+    m.exclude_neighbors = excl != 0; m.untangle_opt = untangle != 0; m.max_search = maxit;
+    m.mark();
+  });
+}
+tc_status tc_set_coupled_collider(tc_sim* s, int on) {
+  return guard([&] { Sim& m = S(s); m.coupled = on != 0; m.mark(); });
+}
+tc_status tc_set_auto_coupled_on_low_substeps(tc_sim* s, int on) {
+  return guard([&] { Sim& m = S(s); m.auto_coupled = on != 0; m.mark(); });
+}
+tc_status tc_set_collider_options(tc_sim* s, int cluster, int recovery, float sweep) {
+  return guard([&] {
+    Sim& m = S(s);
+    (void)cluster;  // the exact broadphase makes cluster culling unnecessary
+    (void)sweep;
+    m.recovery = recovery != 0;
+    m.mark();
+  });
+}
+
+static tcloth::Prim make_prim(uint32_t type, const float* a, const float* b, float r, float f, float rest) {
+  float tf;
+  std::memcpy(&tf, &type, 4);
+  return tcloth::Prim{make_float4(f, rest, r, tf), make_float4(a[0], a[1], a[2], 0.f),
+                      make_float4(b ? b[0] : 0.f, b ? b[1] : 0.f, b ? b[2] : 0.f, 0.f)};
+}
+tc_status tc_add_sphere_collider(tc_sim* s, const float c[3], float r, float f, float rest) {
+  return guard([&] { Sim& m = S(s); need(c, "center required"); m.prims_h.push_back(make_prim(0, c, nullptr, r, f, rest)); m.upload_prims(); });
+}
+tc_status tc_add_capsule_collider(tc_sim* s, const float a[3], const float b[3], float r, float f, float rest) {
+  return guard([&] { Sim& m = S(s); need(a && b, "points required"); m.prims_h.push_back(make_prim(1, a, b, r, f, rest)); m.upload_prims(); });
+}
+tc_status tc_add_plane_collider(tc_sim* s, const float p[3], const float nrm[3], float f, float rest) {
+  return guard([&] { Sim& m = S(s); need(p && nrm, "point and normal required"); m.prims_h.push_back(make_prim(2, p, nrm, 0.f, f, rest)); m.upload_prims(); });
+}
+tc_status tc_set_mesh_collider_triangles(tc_sim* s, const float* t, uint32_t T, float f, float th, float r, int single,
+                                         const float* attr) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(t != nullptr || T == 0, "triangles required");
+    m.set_mesh(t, T, f, th, r, single != 0, attr);
+  });
+}
+tc_status tc_clear_colliders(tc_sim* s) {
+  return guard([&] { Sim& m = S(s); m.prims_h.clear(); m.tris_h.clear(); m.graph_ntris = 0; m.mark(); });
+}
+
+tc_status tc_set_pin(tc_sim* s, uint32_t v, const float target[3], float w) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (v >= m.n) return;  // the reference ignores out-of-range pins
+    need(target != nullptr, "target required");
+    m.pins[v] = tcloth::PinH{{target[0], target[1], target[2]}, w};
+    m.upload_pins();
+    m.write_inv_mass(v, m.orig_w[v] * (1.f - Sim::clamp_w(w)));
+  });
+}
+tc_status tc_set_pins_batch(tc_sim* s, const uint32_t* idx, const float* targets, const float* weights, uint32_t count) {
+  return guard([&] {
+    Sim& m = S(s);
+    for (uint32_t i = 0; i < count; ++i) {
+      const uint32_t v = idx[i];
+      if (v >= m.n) continue;
+      m.pins[v] = tcloth::PinH{{targets[3 * i], targets[3 * i + 1], targets[3 * i + 2]}, weights[i]};
+      m.write_inv_mass(v, m.orig_w[v] * (1.f - Sim::clamp_w(weights[i])));
+    }
+    m.upload_pins();
+  });
+}
+tc_status tc_release_pin(tc_sim* s, uint32_t v) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (m.pins.erase(v)) {
+      m.upload_pins();
+      m.write_inv_mass(v, m.orig_w[v]);
+    }
+  });
+}
+tc_status tc_clear_pins(tc_sim* s) {
+  return guard([&] {
+    Sim& m = S(s);
+    for (const auto& kv : m.pins) m.write_inv_mass(kv.first, m.orig_w[kv.first]);
+    m.pins.clear();
+    m.upload_pins();
+  });
+}
+tc_status tc_set_vertex_inv_masses(tc_sim* s, const uint32_t* idx, const float* w, uint32_t count) {
+  return guard([&] {
+    Sim& m = S(s);
+    for (uint32_t i = 0; i < count; ++i) {
+      const uint32_t v = idx[i];
+      if (v >= m.n) continue;
+      m.orig_w[v] = w[i];
+      auto it = m.pins.find(v);
+      m.write_inv_mass(v, it != m.pins.end() ? w[i] * (1.f - Sim::clamp_w(it->second.weight)) : w[i]);
+    }
+    m.mark();
+  });
+}
+tc_status tc_get_vertex_inv_masses(tc_sim* s, float* out, uint32_t n) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out && n >= m.n, "output too small");
+    std::copy(m.orig_w.begin(), m.orig_w.end(), out);
+  });
+}
+
+tc_status tc_get_counts(tc_sim* s, uint32_t out[8]) {
+  return guard([&] {
+    Sim& m = S(s);
+    out[0] = m.n; out[1] = m.nd; out[2] = m.nb; out[3] = m.ne;
+    out[4] = uint32_t(m.m.dist_cnt.size()); out[5] = uint32_t(m.m.bend_cnt.size());
+    out[6] = m.m.table; out[7] = m.m.multi_layer ? 1u : 0u;
+  });
+}
+tc_status tc_get_cell_size(tc_sim* s, float* cell) {
+  return guard([&] { Sim& m = S(s); *cell = m.m.cell; });
+}
+
+tc_status tc_get_state(tc_sim* s, float* x, float* p, float* v) {
+  return guard([&] {
+    Sim& m = S(s);
+    std::vector<float4> hx(m.n), hp(m.n), hv(m.n);
+    TC_CK(cudaMemcpyAsync(hx.data(), m.x4.p, m.n * sizeof(float4), cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaMemcpyAsync(hp.data(), m.p4.p, m.n * sizeof(float4), cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaMemcpyAsync(hv.data(), m.v4.p, m.n * sizeof(float4), cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    for (uint32_t i = 0; i < m.n; ++i) {
+      if (x) { x[3 * i] = hx[i].x; x[3 * i + 1] = hx[i].y; x[3 * i + 2] = hx[i].z; }
+      if (p) { p[3 * i] = hp[i].x; p[3 * i + 1] = hp[i].y; p[3 * i + 2] = hp[i].z; }
+      if (v) { v[3 * i] = hv[i].x; v[3 * i + 1] = hv[i].y; v[3 * i + 2] = hv[i].z; }
+    }
+  });
+}
+tc_status tc_get_distance_constraints(tc_sim* s, uint32_t* v01, float* par, uint32_t* off, uint32_t* cnt) {
+  return guard([&] {
+    Sim& m = S(s);
+    for (uint32_t i = 0; i < m.nd; ++i) {
+      const auto& c = m.dist_h[i];
+      if (v01) { v01[2 * i] = c.v0; v01[2 * i + 1] = c.v1; }
+      if (par) { par[4 * i] = c.rest; par[4 * i + 1] = c.tc; par[4 * i + 2] = c.cc; par[4 * i + 3] = float(c.type); }
+    }
+    if (off) std::copy(m.m.dist_off.begin(), m.m.dist_off.end(), off);
+    if (cnt) std::copy(m.m.dist_cnt.begin(), m.m.dist_cnt.end(), cnt);
+  });
+}
+tc_status tc_get_bending_constraints(tc_sim* s, uint32_t* v, float* par, uint32_t* off, uint32_t* cnt) {
+  return guard([&] {
+    Sim& m = S(s);
+    for (uint32_t i = 0; i < m.nb; ++i) {
+      const auto& c = m.bend_h[i];
+      if (v) { v[4 * i] = c.v0; v[4 * i + 1] = c.v1; v[4 * i + 2] = c.v2; v[4 * i + 3] = c.v3; }
+      if (par) { par[4 * i] = c.rest; par[4 * i + 1] = c.comp; par[4 * i + 2] = c.pad0; par[4 * i + 3] = c.pad1; }
+    }
+    if (off) std::copy(m.m.bend_off.begin(), m.m.bend_off.end(), off);
+    if (cnt) std::copy(m.m.bend_cnt.begin(), m.m.bend_cnt.end(), cnt);
+  });
+}
+tc_status tc_get_hash_state(tc_sim* s, int which, uint32_t* cell_starts, uint32_t* sorted) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(which == 0 || which == 1, "which must be 0 (vertices) or 1 (edges)");
+    m.encode_hash(which);
+    const uint32_t cnt = which == 0 ? m.n : m.ne;
+    TC_CK(cudaMemcpyAsync(cell_starts, which == 0 ? m.cs.p : m.ecs.p, (m.m.table + 1) * sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost, m.st));
+    if (cnt)
+      TC_CK(cudaMemcpyAsync(sorted, which == 0 ? m.srt.p : m.esrt.p, cnt * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    TC_CK(cudaGetLastError());
+  });
+}
+tc_status tc_get_edges(tc_sim* s, uint32_t* e, uint32_t* bits) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (e) std::copy(m.m.edges.begin(), m.m.edges.end(), e);
+    if (bits) std::copy(m.m.edge_bits.begin(), m.m.edge_bits.end(), bits);
+  });
+}
+tc_status tc_set_residual_tracking(tc_sim* s, int on) {
+  return guard([&] { Sim& m = S(s); m.track_residual = on != 0; m.mark(); });
+}
+tc_status tc_get_residuals(tc_sim* s, float* drms, float* dmax, float* brms, float* bmax, float totals[4]) {
+  return guard([&] {
+    Sim& m = S(s);
+    const size_t kd = m.m.dist_cnt.size(), kb = m.m.bend_cnt.size();
+    std::vector<float> sum(kd + kb + 1), mx(kd + kb + 1);
+    TC_CK(cudaMemcpyAsync(sum.data(), m.res_sum.p, sum.size() * 4, cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaMemcpyAsync(mx.data(), m.res_max.p, mx.size() * 4, cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    double ds = 0, bs = 0;
+    float dm = 0, bm = 0;
+    for (size_t c = 0; c < kd; ++c) {
+      if (drms) drms[c] = m.m.dist_cnt[c] ? std::sqrt(sum[c] / float(m.m.dist_cnt[c])) : 0.f;
+      if (dmax) dmax[c] = mx[c];
+      ds += sum[c]; dm = std::fmax(dm, mx[c]);
+    }
+    for (size_t c = 0; c < kb; ++c) {
+      if (brms) brms[c] = m.m.bend_cnt[c] ? std::sqrt(sum[kd + c] / float(m.m.bend_cnt[c])) : 0.f;
+      if (bmax) bmax[c] = mx[kd + c];
+      bs += sum[kd + c]; bm = std::fmax(bm, mx[kd + c]);
+    }
+    if (totals) {
+      totals[0] = m.nd ? float(std::sqrt(ds / m.nd)) : 0.f;
+      totals[1] = dm;
+      totals[2] = m.nb ? float(std::sqrt(bs / m.nb)) : 0.f;
+      totals[3] = bm;
+    }
+  });
+}
+struct tc_mesh {
+  tcloth::MeshData m;
+};
+
+tc_status tc_mesh_build(tc_mesh** out, const float* positions, uint32_t n, const uint32_t* edges, uint32_t ne,
+                        const uint32_t* faces, uint32_t nf, const float* inv_masses, const uint32_t* layer_ids,
+                        const float* thicknesses, uint32_t layer_id, float thickness, float tk, float ck, float sk,
+                        float bk) {
+  return guard([&] {
+    need(out != nullptr, "out handle required");
+    *out = nullptr;
+    for (uint32_t e = 0; e < ne; ++e)
+      need(edges[2 * size_t(e)] < n && edges[2 * size_t(e) + 1] < n, "edges contain an index >= number of vertices");
+    for (uint32_t f = 0; f < nf; ++f)
+      for (int k = 0; k < 3; ++k) need(faces[3 * size_t(f) + k] < n, "faces contain an index >= number of vertices");
+    tcloth::MeshInput in;
+    in.pos = positions; in.n = n; in.edges = edges; in.ne = ne; in.faces = nf ? faces : nullptr; in.nf = nf;
+    in.inv_masses = inv_masses; in.layer_ids = layer_ids; in.thicknesses = thicknesses;
+    in.layer_id = layer_id; in.thickness = thickness;
+    in.tension_k = tk; in.compression_k = ck; in.shear_k = sk; in.bending_k = bk;
+    std::unique_ptr<tc_mesh> h(new tc_mesh);
+    h->m = tcloth::build_mesh(in);
+    *out = h.release();
+  });
+}
+tc_status tc_mesh_destroy(tc_mesh* m) {
+  return guard([&] { delete m; });
+}
+tc_status tc_mesh_counts(tc_mesh* h, uint32_t out[10], float* cell) {
+  return guard([&] {
+    need(h && out, "handle and output required");
+    const auto& m = h->m;
+    out[0] = m.n; out[1] = uint32_t(m.dist.size()); out[2] = uint32_t(m.bend.size()); out[3] = uint32_t(m.edges.size() / 2);
+    out[4] = uint32_t(m.dist_cnt.size()); out[5] = uint32_t(m.bend_cnt.size()); out[6] = m.table;
+    out[7] = m.multi_layer ? 1u : 0u; out[8] = m.num_virtual; out[9] = uint32_t(m.adj_idx.size());
+    if (cell) *cell = m.cell;
+  });
+}
+tc_status tc_mesh_constraints(tc_mesh* h, uint32_t* dv, float* dp, uint32_t* doff, uint32_t* dcnt, uint32_t* bv,
+                              float* bp, uint32_t* boff, uint32_t* bcnt) {
+  return guard([&] {
+    need(h != nullptr, "handle required");
+    const auto& m = h->m;
+    for (size_t i = 0; i < m.dist.size(); ++i) {
+      const auto& c = m.dist[i];
+      if (dv) { dv[2 * i] = c.v0; dv[2 * i + 1] = c.v1; }
+      if (dp) { dp[4 * i] = c.rest; dp[4 * i + 1] = c.tc; dp[4 * i + 2] = c.cc; dp[4 * i + 3] = float(c.type); }
+    }
+    for (size_t i = 0; i < m.bend.size(); ++i) {
+      const auto& c = m.bend[i];
+      if (bv) { bv[4 * i] = c.v0; bv[4 * i + 1] = c.v1; bv[4 * i + 2] = c.v2; bv[4 * i + 3] = c.v3; }
+      if (bp) { bp[4 * i] = c.rest; bp[4 * i + 1] = c.comp; bp[4 * i + 2] = c.pad0; bp[4 * i + 3] = c.pad1; }
+    }
+    if (doff) std::copy(m.dist_off.begin(), m.dist_off.end(), doff);
+    if (dcnt) std::copy(m.dist_cnt.begin(), m.dist_cnt.end(), dcnt);
+    if (boff) std::copy(m.bend_off.begin(), m.bend_off.end(), boff);
+    if (bcnt) std::copy(m.bend_cnt.begin(), m.bend_cnt.end(), bcnt);
+  });
+}
+tc_status tc_mesh_topology_sizes(tc_mesh* h, uint32_t* a, uint32_t* t, uint32_t* s) {
+  return guard([&] {
+    need(h != nullptr, "handle required");
+    *a = uint32_t(h->m.adj_idx.size()); *t = uint32_t(h->m.th_idx.size()); *s = uint32_t(h->m.star_idx.size() / 2);
+  });
+}
+tc_status tc_mesh_topology(tc_mesh* h, uint32_t* adj_off, uint32_t* adj_idx, uint32_t* th_off, uint32_t* th_idx,
+                           float* th_rest, float* local_len, uint32_t* star_off, uint32_t* star_idx, uint32_t* island,
+                           uint32_t* layer, uint32_t* edges, uint32_t* edge_bits) {
+  return guard([&] {
+    need(h != nullptr, "handle required");
+    const auto& m = h->m;
+    auto cp = [](const auto& v, auto* dst) { if (dst) std::copy(v.begin(), v.end(), dst); };
+    cp(m.adj_off, adj_off); cp(m.adj_idx, adj_idx); cp(m.th_off, th_off); cp(m.th_idx, th_idx);
+    cp(m.th_rest, th_rest); cp(m.local_len, local_len); cp(m.star_off, star_off); cp(m.star_idx, star_idx);
+    cp(m.island, island); cp(m.layer, layer); cp(m.edges, edges); cp(m.edge_bits, edge_bits);
+  });
+}
+
+tc_status tc_set_profiling_enabled(tc_sim* s, int on) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.profiling = on != 0;
+    m.prof_names.clear(); m.prof_ms.clear(); m.prof_cnt.clear();
+  });
+}
+tc_status tc_take_profile(tc_sim* s, char* names, size_t names_len, float* ms, uint32_t* launches, uint32_t max_entries,
+                          uint32_t* n_entries) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(n_entries != nullptr, "n_entries required");
+    std::string joined;
+    const uint32_t k = uint32_t(std::min<size_t>(m.prof_names.size(), max_entries));
+    for (uint32_t i = 0; i < k; ++i) {
+      joined += m.prof_names[i];
+      joined += '\n';
+      if (ms) ms[i] = float(m.prof_ms[i]);
+      if (launches) launches[i] = m.prof_cnt[i];
+    }
+    if (names && names_len) std::snprintf(names, names_len, "%s", joined.c_str());
+    *n_entries = k;
+    m.prof_names.clear(); m.prof_ms.clear(); m.prof_cnt.clear();
+  });
+}
+
+tc_status tc_frame_kernel_count(tc_sim* s, uint32_t* count) {
+  return guard([&] { Sim& m = S(s); need(count != nullptr, "count required"); *count = m.graph_kernels; });
+}
+
+tc_status tc_last_frame_ms(tc_sim* s, float* ms) {
+  return guard([&] {
+    Sim& m = S(s);
+    TC_CK(cudaEventSynchronize(m.ev1));
+    TC_CK(cudaEventElapsedTime(ms, m.ev0, m.ev1));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,383 @@
+// XPBD solver kernels: predict, pins, graph-coloured distance / bending
+// projection, primitive + triangle-mesh collider response, velocity update.
+//
+// Device layout (structure of arrays, 16-byte records):
+//   x4[i] = (x, inv_mass)        committed position ("position" in the reference)
+//   p4[i] = (p, thickness)       predicted / corrected position ("prev_pos")
+//   v4[i] = (v, layer bits)
+// One thread per vertex / constraint; each kernel restates one WGSL entry
+// point of crates/cloth_core/src/shaders/.
+#pragma once
+#include "vmath.cuh"
+
+namespace tcloth {
+
+struct SubstepParams {
+  float dt;       // substep dt (already max(dt, 1e-8) where the shaders do so)
+  float gx, gy, gz;
+  float damping;  // air damping
+  float td, cd, sd, bd;  // Rayleigh damping: tension, compression, shear, bending
+};
+
+// shaders/predict.wgsl:33-55
+__global__ void k_predict(uint32_t n, const float4* __restrict__ x4, float4* __restrict__ p4,
+                          float4* __restrict__ v4, SubstepParams sp) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 x = x4[i], p = p4[i], v = v4[i];
+  const float dt = fmaxf(sp.dt, 1e-8f);
+  if (x.w <= 0.0f) {
+    v.x = 0.f; v.y = 0.f; v.z = 0.f;
+    p.x = x.x; p.y = x.y; p.z = x.z;
+  } else {
+    const float s = fmaxf(0.0f, 1.0f - sp.damping * dt);
+    V3 vv = mk(v) * s + mk(sp.gx, sp.gy, sp.gz) * dt;
+    V3 pp = mk(x) + vv * dt;
+    v.x = vv.x; v.y = vv.y; v.z = vv.z;
+    p.x = pp.x; p.y = pp.y; p.z = pp.z;
+  }
+  p4[i] = p;
+  v4[i] = v;
+}
+
+// shaders/pin.wgsl:56-92; pins are on distinct vertices, so order is free
+__global__ void k_pin(uint32_t npins, const uint32_t* __restrict__ pin_v, const float4* __restrict__ pin_t,
+                      const float4* __restrict__ x4, float4* __restrict__ p4, float dt_sub) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npins) return;
+  const uint32_t vi = pin_v[k];
+  const float4 t = pin_t[k];  // target xyz, weight
+  const float w = clampf(t.w, 0.0f, 1.0f);
+  if (w <= 0.0f) return;
+  const float im = x4[vi].w;
+  float4 p = p4[vi];
+  if (im <= 0.0f) {
+    p.x = t.x; p.y = t.y; p.z = t.z;
+    p4[vi] = p;
+    return;
+  }
+  V3 d = mk(p) - mk(t);
+  float dist = length(d);
+  if (!(dist > kEps)) return;
+  V3 nn = d / dist;
+  float dt = fmaxf(dt_sub, 1e-8f);
+  float comp = 1e-3f * (1.0f - w) / fmaxf(w, 1e-6f);
+  float alpha = comp / (dt * dt);
+  float corr = -dist / (im + alpha);
+  V3 np = mk(p) + nn * (im * corr);
+  p.x = np.x; p.y = np.y; p.z = np.z;
+  p4[vi] = p;
+}
+
+// One distance constraint (shaders/distance.wgsl:60-124).  dist_par =
+// (rest, tension compliance, compression compliance, shear flag).
+__device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __restrict__ ids,
+                                                 const float4* __restrict__ par, float4* __restrict__ x4,
+                                                 float4* __restrict__ p4, float* __restrict__ lam,
+                                                 const SubstepParams& sp, bool damped) {
+  const uint2 e = ids[ci];
+  const float4 c = par[ci];
+  const float w0 = x4[e.x].w, w1 = x4[e.y].w;
+  const float ws = w0 + w1;
+  if (ws <= kEps) return;
+  const float4 q0 = p4[e.x], q1 = p4[e.y];
+  const V3 p0 = mk(q0), p1 = mk(q1);
+  const V3 delta = p0 - p1;
+  const float dist = length(delta);
+  if (dist <= kEps) return;
+  const float cv = dist - c.x;
+  const float comp = cv >= 0.0f ? c.y : c.z;
+  if (comp >= 1e9f) return;
+  const V3 dir = delta / dist;
+  const float dt = fmaxf(sp.dt, 1e-8f);
+  const float alpha = comp / (dt * dt);
+  if (damped) {
+    const float damp = c.w != 0.0f ? sp.sd : (cv >= 0.0f ? sp.td : sp.cd);
+    const float tau = damp * 1e-5f;
+    const float gamma = fminf(tau / dt, 1e4f);
+    const V3 rel = (p0 - mk(x4[e.x])) - (p1 - mk(x4[e.y]));
+    const float vp = dot(dir, rel);
+    const float l = lam[ci];
+    const float dl = (-cv - alpha * l - gamma * vp) / ((1.0f + gamma) * ws + alpha);
+    lam[ci] = l + dl;
+    const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
+    p4[e.x] = make_float4(n0.x, n0.y, n0.z, q0.w);
+    p4[e.y] = make_float4(n1.x, n1.y, n1.z, q1.w);
+    return;
+  }
+  const float l = lam[ci];
+  // gamma == 0: (-cv - alpha*l - 0*vp) / (1*ws + alpha)
+  const float dl = (-cv - alpha * l) / (1.0f * ws + alpha);
+  lam[ci] = l + dl;
+  const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
+  p4[e.x] = make_float4(n0.x, n0.y, n0.z, q0.w);
+  p4[e.y] = make_float4(n1.x, n1.y, n1.z, q1.w);
+}
+
+__global__ void k_distance(uint32_t off, uint32_t cnt, const uint2* __restrict__ ids, const float4* __restrict__ par,
+                           float4* __restrict__ x4, float4* __restrict__ p4, float* __restrict__ lam,
+                           SubstepParams sp, bool damped) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cnt) return;
+  project_distance(off + k, ids, par, x4, p4, lam, sp, damped);
+}
+
+// One bending constraint (shaders/bending.wgsl:59-126).  bend_par =
+// (rest, compliance, kind, seam gap).
+__device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __restrict__ ids,
+                                                const float4* __restrict__ par, float4* __restrict__ x4,
+                                                float4* __restrict__ p4, float* __restrict__ lam,
+                                                const SubstepParams& sp, bool damped) {
+  const float4 c = par[ci];
+  if (c.y >= 1e9f) return;
+  const uint4 e = ids[ci];
+  const float w2 = x4[e.z].w, w3 = x4[e.w].w;
+  const float ws = w2 + w3;
+  if (ws <= kEps) return;
+  const float4 q2 = p4[e.z], q3 = p4[e.w];
+  const V3 p2 = mk(q2), p3 = mk(q3);
+  const V3 delta = p2 - p3;
+  const float dist = length(delta);
+  if (dist <= kEps) return;
+  if (c.z > 0.5f && c.z < 1.5f) {
+    if (dist >= c.x) return;
+    float gap = length(mk(p4[e.x]) - mk(p4[e.y]));
+    if (gap > c.w) return;
+  }
+  const V3 dir = delta / dist;
+  const float dt = fmaxf(sp.dt, 1e-8f);
+  const float alpha = c.y / (dt * dt);
+  const float cv = dist - c.x;
+  const float l = lam[ci];
+  float dl;
+  if (damped) {
+    const float tau = sp.bd * 1e-5f;
+    const float gamma = fminf(tau / dt, 1e4f);
+    const V3 rel = (p2 - mk(x4[e.z])) - (p3 - mk(x4[e.w]));
+    const float vp = dot(dir, rel);
+    dl = (-cv - alpha * l - gamma * vp) / ((1.0f + gamma) * ws + alpha);
+  } else {
+    dl = (-cv - alpha * l) / (1.0f * ws + alpha);
+  }
+  lam[ci] = l + dl;
+  const V3 n2 = p2 + dir * (w2 * dl), n3 = p3 + dir * (-w3 * dl);
+  p4[e.z] = make_float4(n2.x, n2.y, n2.z, q2.w);
+  p4[e.w] = make_float4(n3.x, n3.y, n3.z, q3.w);
+}
+
+__global__ void k_bending(uint32_t off, uint32_t cnt, const uint4* __restrict__ ids, const float4* __restrict__ par,
+                          float4* __restrict__ x4, float4* __restrict__ p4, float* __restrict__ lam,
+                          SubstepParams sp, bool damped) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cnt) return;
+  project_bending(off + k, ids, par, x4, p4, lam, sp, damped);
+}
+
+// shaders/update_vel.wgsl:33-53
+__global__ void k_update_vel(uint32_t n, float4* __restrict__ x4, const float4* __restrict__ p4,
+                             float4* __restrict__ v4, float dt_sub) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 x = x4[i];
+  const float4 p = p4[i];
+  float4 v = v4[i];
+  const float dt = fmaxf(dt_sub, 1e-8f);
+  if (x.w > 0.0f) {
+    V3 vv = (mk(p) - mk(x)) / dt;
+    v.x = vv.x; v.y = vv.y; v.z = vv.z;
+  } else {
+    v.x = 0.f; v.y = 0.f; v.z = 0.f;
+  }
+  x.x = p.x; x.y = p.y; x.z = p.z;
+  x4[i] = x;
+  v4[i] = v;
+}
+
+// ---------------------------------------------------------------------
+// colliders
+// ---------------------------------------------------------------------
+struct Prim {      // sphere (0), capsule (1), plane (2)
+  float4 h;        // friction, restitution, radius, type
+  float4 a, b;     // point a / b (plane: point, normal)
+};
+struct MeshTri {   // 64 B, Morton-sorted (simulation/mod.rs:2613-2641)
+  float4 p0f;      // p0, friction
+  float4 p1t;      // p1, thickness
+  float4 p2r;      // p2, restitution
+  float4 fl;       // flags bits, 0, 0, 0
+};
+
+// apply_contact_response (shaders/collision.wgsl:83-108)
+__device__ __forceinline__ void contact(V3 target, V3 n, float fric, float rest, float dt, V3 p_init, V3& xn,
+                                        V3& p) {
+  V3 total = target - xn;
+  V3 tang = total - n * dot(total, n);
+  p = target - tang * clampf(fric, 0.0f, 1.0f);
+  float edt = fmaxf(dt, 1e-6f);
+  float vin = dot((p_init - xn) / edt, n);
+  float des = 0.0f;
+  if (vin < 0.0f) des = -clampf(rest, 0.0f, 1.0f) * vin;
+  float dxn = dot(target - xn, n) - des * edt;
+  xn = xn + n * dxn;
+}
+
+struct MeshState {
+  bool front = false, has_rec = false;
+  float best_depth = 999999.0f, bf = 0.f, br = 0.f;
+  V3 bpos, bn;
+};
+
+// one triangle of the mesh collider loop (shaders/collision.wgsl:461-541)
+__device__ __forceinline__ void mesh_triangle(const MeshTri& tri, float thickness, V3 xpos, V3& p, V3& xn, float dt,
+                                              V3 pinit, bool recovery_on, MeshState& st) {
+  const V3 t0 = mk(tri.p0f), t1 = mk(tri.p1t), t2 = mk(tri.p2r);
+  const float fric = tri.p0f.w, tthick = tri.p1t.w, rest = tri.p2r.w;
+  const uint32_t flags = __float_as_uint(tri.fl.x);
+  const float td = thickness + tthick;
+  const V3 cr = cross(t1 - t0, t2 - t0);
+  const float cl = length(cr);
+  if (cl < kEps) return;
+  const V3 fn = cr / cl;
+  const bool single = (flags & 1u) != 0u;
+  float th, tu, tv;
+  if (seg_tri(xpos, p, t0, t1, t2, th, tu, tv)) {
+    V3 hit = xpos + (p - xpos) * th;
+    V3 nn = fn;
+    if (dot(p - xpos, fn) > 0.0f && !single) nn = -fn;
+    contact(hit + nn * td, nn, fric, rest, dt, pinit, xn, p);
+    st.front = true;
+  }
+  bool isf;
+  V3 bary;
+  const V3 q = closest_tri(p, t0, t1, t2, isf, bary);
+  const V3 delta = p - q;
+  const float dist = length(delta);
+  const float sd = dot(delta, fn);
+  if (single) {
+    if (sd >= 0.0f) {
+      if (dist < td) {
+        V3 nn = fn;
+        if (dist > kEps) nn = delta / dist;
+        contact(p + nn * (td - dist), nn, fric, rest, dt, pinit, xn, p);
+        st.front = true;
+      }
+    } else {
+      const bool rdis = (flags & 2u) != 0u;
+      if (recovery_on && !rdis) {
+        const float maxd = td * 3.0f;
+        if (isf && dist < maxd && dist <= fabsf(sd) * 1.1f + kEps) {
+          if (dist < st.best_depth) {
+            st.best_depth = dist;
+            st.bn = fn;
+            st.bpos = p + fn * (td - sd);
+            st.bf = fric;
+            st.br = rest;
+            st.has_rec = true;
+          }
+        }
+      }
+    }
+  } else {
+    if (dist < td && sd >= -td) {
+      V3 nn = fn;
+      if (dist > kEps) nn = delta / dist;
+      contact(p + nn * (td - dist), nn, fric, rest, dt, pinit, xn, p);
+      st.front = true;
+    }
+  }
+}
+
+struct ColliderArgs {
+  const Prim* prims;
+  uint32_t nprims;
+  const MeshTri* tris;
+  const float4* bounds;   // per triangle: centroid, r
+  const float4* cl16;     // per 16 triangles: conservative sphere for 1.5 r
+  const float4* cl256;    // per 256 triangles
+  uint32_t ntris;
+  bool recovery;
+};
+
+// Conservative skip test for a group of triangles: true only when every
+// member triangle would fail its own test seg_point_d2 > (1.5 r + th)^2.
+__device__ __forceinline__ bool group_far(V3 a, V3 b, float4 g, float th) {
+  float R = g.w + th;
+  float d2 = seg_point_d2(a, b, mk(g));
+  return d2 > R * R * 1.0004f + 1e-12f;
+}
+
+// shaders/collision.wgsl:378-652 (cluster culling off, the reference
+// default).  The triangle loop visits triangles in ascending (Morton) order
+// exactly like the reference; two levels of conservative bounding spheres
+// skip runs of triangles none of which could pass the per-triangle test, so
+// the sequence of applied contacts is unchanged.
+__global__ void k_collision(uint32_t n, float4* __restrict__ x4, float4* __restrict__ p4, ColliderArgs ca,
+                            float dt) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 x = x4[i];
+  if (x.w <= 0.0f) return;
+  float4 pr = p4[i];
+  V3 p = mk(pr), pinit = p, xn = mk(x);
+  const V3 xpos = mk(x);
+  const float th = pr.w;
+  for (uint32_t k = 0; k < ca.nprims; ++k) {
+    const Prim c = ca.prims[k];
+    const uint32_t type = __float_as_uint(c.h.w);
+    const float fric = c.h.x, rest = c.h.y, r = c.h.z;
+    if (type == 0u) {
+      float tr = r + th;
+      V3 d = p - mk(c.a);
+      float dist = length(d);
+      if (dist < tr) {
+        V3 nn = mk(0.f, 0.f, 1.f);
+        if (dist > kEps) nn = d / dist;
+        contact(mk(c.a) + nn * tr, nn, fric, rest, dt, pinit, xn, p);
+      }
+    } else if (type == 1u) {
+      float tr = r + th;
+      V3 A = mk(c.a), ab = mk(c.b) - A;
+      float l2 = dot(ab, ab);
+      float t = 0.0f;
+      if (l2 > kEps) t = clampf(dot(p - A, ab) / l2, 0.0f, 1.0f);
+      V3 cl = A + ab * t;
+      V3 d = p - cl;
+      float dist = length(d);
+      if (dist < tr) {
+        V3 nn = mk(0.f, 0.f, 1.f);
+        if (dist > kEps) nn = d / dist;
+        contact(cl + nn * tr, nn, fric, rest, dt, pinit, xn, p);
+      }
+    } else if (type == 2u) {
+      V3 B = mk(c.b);
+      V3 pn = B / length(B);
+      float dist = dot(p - mk(c.a), pn);
+      if (dist < th) contact(p + pn * (th - dist), pn, fric, rest, dt, pinit, xn, p);
+    }
+  }
+  if (ca.ntris > 0) {
+    MeshState st;
+    st.bpos = p;
+    st.bn = mk(0.f, 0.f, 0.f);
+    const uint32_t ng256 = (ca.ntris + 255u) / 256u;
+    for (uint32_t g = 0; g < ng256; ++g) {
+      if (group_far(xpos, p, ca.cl256[g], th)) continue;
+      const uint32_t c_end = min((g + 1u) * 16u, (ca.ntris + 15u) / 16u);
+      for (uint32_t cgi = g * 16u; cgi < c_end; ++cgi) {
+        if (group_far(xpos, p, ca.cl16[cgi], th)) continue;
+        const uint32_t t_end = min((cgi + 1u) * 16u, ca.ntris);
+        for (uint32_t t = cgi * 16u; t < t_end; ++t) {
+          const float4 b = ca.bounds[t];
+          const float r = b.w * 1.5f + th;
+          if (seg_point_d2(xpos, p, mk(b)) > r * r) continue;
+          mesh_triangle(ca.tris[t], th, xpos, p, xn, dt, pinit, ca.recovery, st);
+        }
+      }
+    }
+    if (!st.front && st.has_rec) contact(st.bpos, st.bn, st.bf, st.br, dt, pinit, xn, p);
+  }
+  p4[i] = make_float4(p.x, p.y, p.z, pr.w);
+  x4[i] = make_float4(xn.x, xn.y, xn.z, x.w);
+}
+
+}  // namespace tcloth

@@ -1,0 +1,358 @@
+"""``ClothSimulator``: the reference's PyO3 class, re-homed on the C ABI.
+
+Mirrors ``taremin_cloth_core.ClothSimulator`` (crates/cloth_py/src/lib.rs:1549-3100)
+for the XPBD substep: same constructor arguments and defaults, same setter
+names, same exceptions (``ValueError`` for bad shapes or indices,
+``RuntimeError`` when the GPU cannot be initialised).  All work runs in
+``libtcloth.so`` on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+_f32 = np.float32
+_u32 = np.uint32
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _arr(a, dtype, cols=None, name="array"):
+    if a is None:
+        return None
+    x = np.ascontiguousarray(np.asarray(a), dtype=dtype)
+    if cols is not None:
+        if x.ndim != 2 or x.shape[1] != cols:
+            raise ValueError(f"{name} must have shape (N, {cols}), got {tuple(x.shape)}")
+    return x
+
+
+def is_gpu_available() -> bool:
+    try:
+        return bool(_lib.load().tc_gpu_available())
+    except RuntimeError:
+        return False
+
+
+def get_gpu_device_name(device: int = 0) -> str:
+    buf = C.create_string_buffer(256)
+    _lib.check(_lib.load().tc_device_name(device, buf, 256))
+    return buf.value.decode()
+
+
+class ClothSimulator:
+    """GPU XPBD cloth simulator (drop-in for the reference's ClothSimulator)."""
+
+    def __init__(self, positions, edges, faces=None, inv_masses=None, sewing_springs=None, layer_ids=None,
+                 thicknesses=None, layer_id=0, thickness=0.005, stiffness=1000.0, bending_stiffness=10.0,
+                 sewing_shrink_speed=1.0, sewing_stiffness=None, enable_sewing_lock=None,
+                 sewing_lock_distance=None, compression_stiffness=None, shear_stiffness=None, workgroup_size=32,
+                 solver_mode=0, enable_compact_readback=None, enable_pair_cache=None, areal_density=None,
+                 enable_coarse_constraints=None, self_collision_algorithm=None, device=0):
+        L = _lib.load()
+        self._h = None
+        pos = _arr(positions, _f32, 3, "positions")
+        e = _arr(edges, _u32, 2, "edges")
+        if sewing_springs is not None and len(np.asarray(sewing_springs)) > 0:
+            raise NotImplementedError("sewing springs are not part of this substep build")
+        if solver_mode not in (0,):
+            raise NotImplementedError("only the graph-coloured solver (solver_mode=0) is built")
+        f = _arr(faces, _u32, 3, "faces") if faces is not None else None
+        n = pos.shape[0]
+
+        def per_vertex(a, dtype, name):
+            if a is None:
+                return None
+            x = np.ascontiguousarray(np.asarray(a).reshape(-1), dtype=dtype)
+            if x.shape[0] != n:
+                raise ValueError(f"{name} length ({x.shape[0]}) does not match the vertex count ({n})")
+            return x
+
+        im = per_vertex(inv_masses, _f32, "inv_masses")
+        li = per_vertex(layer_ids, _u32, "layer_ids")
+        th = per_vertex(thicknesses, _f32, "thicknesses")
+        comp = stiffness if compression_stiffness is None else compression_stiffness
+        shear = stiffness * 0.5 if shear_stiffness is None else shear_stiffness
+        h = C.c_void_p()
+        nf = 0 if f is None else f.shape[0]
+        _lib.check(L.tc_create(C.byref(h), _ptr(pos), n, _ptr(e), e.shape[0], _ptr(f), nf, _ptr(im), _ptr(li),
+                               _ptr(th), int(layer_id), float(thickness), float(stiffness), float(comp),
+                               float(shear), float(bending_stiffness), int(device)))
+        self._h = h
+        self._L = L
+        self._n = n
+        self._solver_iterations = 2
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                self._L.tc_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+    def _c(self, status):
+        _lib.check(status)
+
+    # ---------------- stepping
+    def step(self, dt=0.016666667, substeps=None, solver_iterations=None):
+        if solver_iterations is not None:
+            self.set_solver_iterations(solver_iterations)
+        eff = C.c_uint32()
+        self._c(self._L.tc_step(self._h, float(dt), 0 if substeps is None else int(substeps), C.byref(eff)))
+        return eff.value
+
+    def step_async(self, dt=0.016666667, substeps=None, solver_iterations=None):
+        if solver_iterations is not None:
+            self.set_solver_iterations(solver_iterations)
+        self._c(self._L.tc_step_async(self._h, float(dt), 0 if substeps is None else int(substeps)))
+
+    def fetch_positions(self, out_array):
+        out = self._out(out_array)
+        ok = C.c_int()
+        self._c(self._L.tc_fetch_positions(self._h, _ptr(out), out.size, C.byref(ok)))
+        return bool(ok.value)
+
+    def _out(self, out_array):
+        if not isinstance(out_array, np.ndarray) or out_array.dtype != _f32 or not out_array.flags.c_contiguous \
+                or not out_array.flags.writeable:
+            raise ValueError("out_array must be a writable, contiguous float32 NumPy array")
+        if out_array.size < self._n * 3:
+            raise ValueError(f"out_array needs at least {self._n * 3} elements")
+        return out_array
+
+    def get_positions(self, out_array):
+        out = self._out(out_array)
+        self._c(self._L.tc_get_positions(self._h, _ptr(out), out.size))
+
+    def set_positions_and_velocities(self, positions, velocities=None):
+        p = _arr(positions, _f32, 3, "positions")
+        v = None if velocities is None else _arr(velocities, _f32, 3, "velocities")
+        self._c(self._L.tc_set_positions_and_velocities(self._h, _ptr(p), _ptr(v), p.shape[0]))
+
+    def reset(self):
+        self._c(self._L.tc_reset(self._h))
+
+    # ---------------- parameters
+    def set_gravity(self, gx, gy, gz):
+        self._c(self._L.tc_set_gravity(self._h, gx, gy, gz))
+
+    def set_damping(self, damping):
+        self._c(self._L.tc_set_damping(self._h, damping))
+
+    def set_damping_all(self, tension_damp, compression_damp, shear_damp, bending_damp):
+        self._c(self._L.tc_set_damping_all(self._h, tension_damp, compression_damp, shear_damp, bending_damp))
+
+    def set_solver_iterations(self, iterations):
+        self._solver_iterations = max(int(iterations), 1)
+        self._c(self._L.tc_set_solver_iterations(self._h, int(iterations)))
+
+    def get_effective_solver_iterations(self):
+        return self._solver_iterations
+
+    def set_stiffness(self, stretch_stiffness, bending_stiffness):
+        self.set_stiffness_all(stretch_stiffness, stretch_stiffness, stretch_stiffness * 0.5, bending_stiffness)
+
+    def set_stiffness_all(self, tension_stiffness, compression_stiffness, shear_stiffness, bending_stiffness):
+        self._c(self._L.tc_set_stiffness_all(self._h, tension_stiffness, compression_stiffness, shear_stiffness,
+                                             bending_stiffness))
+
+    def set_compliance_all(self, tension, compression, shear, bending):
+        """Set XPBD compliances (m/N) directly (no stiffness mapping)."""
+        self._c(self._L.tc_set_compliance_all(self._h, tension, compression, shear, bending))
+
+    def set_edge_stiffness_multipliers(self, edge_indices, multipliers):
+        i = np.ascontiguousarray(edge_indices, _u32)
+        m = np.ascontiguousarray(multipliers, _f32)
+        k = min(i.size, m.size)
+        self._c(self._L.tc_set_edge_stiffness_multipliers(self._h, _ptr(i), _ptr(m), k))
+
+    def set_enable_self_collision(self, enable):
+        self._c(self._L.tc_set_enable_self_collision(self._h, int(bool(enable))))
+
+    def set_self_collision_options(self, relief_factor=0.2, max_displacement_ratio=0.2, exclude_neighbors=True,
+                                   enable_normal_untangling=True, max_iterations=128):
+        self._c(self._L.tc_set_self_collision_options(self._h, relief_factor, max_displacement_ratio,
+                                                      int(exclude_neighbors), int(enable_normal_untangling),
+                                                      int(max_iterations)))
+
+    def set_coupled_collider(self, enabled):
+        self._c(self._L.tc_set_coupled_collider(self._h, int(bool(enabled))))
+
+    def set_auto_coupled_on_low_substeps(self, enabled):
+        self._c(self._L.tc_set_auto_coupled_on_low_substeps(self._h, int(bool(enabled))))
+
+    def set_collider_options(self, enable_cluster_culling=False, enable_single_sided_recovery=True,
+                             sweep_margin=0.05):
+        self._c(self._L.tc_set_collider_options(self._h, int(enable_cluster_culling),
+                                                int(enable_single_sided_recovery), sweep_margin))
+
+    # ---------------- colliders
+    def add_sphere_collider(self, center, radius, friction=0.0, restitution=0.0):
+        self._c(self._L.tc_add_sphere_collider(self._h, _ptr(np.asarray(center, _f32)), radius, friction,
+                                               restitution))
+
+    def add_capsule_collider(self, point_a, point_b, radius, friction=0.0, restitution=0.0):
+        self._c(self._L.tc_add_capsule_collider(self._h, _ptr(np.asarray(point_a, _f32)),
+                                                _ptr(np.asarray(point_b, _f32)), radius, friction, restitution))
+
+    def add_plane_collider(self, point, normal, friction=0.0, restitution=0.0):
+        self._c(self._L.tc_add_plane_collider(self._h, _ptr(np.asarray(point, _f32)), _ptr(np.asarray(normal, _f32)),
+                                              friction, restitution))
+
+    def set_mesh_collider_triangles(self, triangles, friction=0.3, thickness=0.01, restitution=0.0,
+                                    single_sided=True, attributes=None):
+        t = np.ascontiguousarray(triangles, _f32)
+        if t.ndim != 3 or t.shape[1:] != (3, 3):
+            raise ValueError("each triangle must have shape [3, 3]")
+        a = None
+        if attributes is not None:
+            a = np.ascontiguousarray(attributes, _f32)
+            if a.ndim != 2 or a.shape[0] < t.shape[0] or a.shape[1] < 4:
+                raise ValueError("attributes must have shape (N_triangles, >=4)")
+            a = np.ascontiguousarray(a[:, :4])
+        self._c(self._L.tc_set_mesh_collider_triangles(self._h, _ptr(t), t.shape[0], friction, thickness,
+                                                       restitution, int(bool(single_sided)), _ptr(a)))
+
+    def clear_colliders(self):
+        self._c(self._L.tc_clear_colliders(self._h))
+
+    # ---------------- pins
+    def set_pin(self, vertex_idx, target_pos, weight=1.0):
+        self._c(self._L.tc_set_pin(self._h, int(vertex_idx), _ptr(np.asarray(target_pos, _f32)), weight))
+
+    def set_pins_batch(self, indices, targets, weights):
+        i = np.ascontiguousarray(indices, _u32)
+        t = _arr(targets, _f32, 3, "targets")
+        w = np.ascontiguousarray(weights, _f32)
+        k = min(i.size, t.shape[0], w.size)
+        self._c(self._L.tc_set_pins_batch(self._h, _ptr(i), _ptr(t), _ptr(w), k))
+
+    def release_pin(self, vertex_idx):
+        self._c(self._L.tc_release_pin(self._h, int(vertex_idx)))
+
+    def release_pins_batch(self, indices):
+        for v in indices:
+            self.release_pin(v)
+
+    def clear_pins(self):
+        self._c(self._L.tc_clear_pins(self._h))
+
+    def set_vertex_inv_masses(self, indices, inv_masses):
+        i = np.ascontiguousarray(indices, _u32)
+        w = np.ascontiguousarray(inv_masses, _f32)
+        self._c(self._L.tc_set_vertex_inv_masses(self._h, _ptr(i), _ptr(w), min(i.size, w.size)))
+
+    def get_vertex_inv_masses(self):
+        o = np.empty(self._n, _f32)
+        self._c(self._L.tc_get_vertex_inv_masses(self._h, _ptr(o), self._n))
+        return o
+
+    # ---------------- counts / introspection
+    def _counts(self):
+        o = np.zeros(8, _u32)
+        self._c(self._L.tc_get_counts(self._h, _ptr(o)))
+        return o
+
+    def get_num_vertices(self):
+        return int(self._counts()[0])
+
+    def get_num_distance_constraints(self):
+        return int(self._counts()[1])
+
+    def get_num_bending_constraints(self):
+        return int(self._counts()[2])
+
+    def get_num_sewing_constraints(self):
+        return 0
+
+    def get_has_multiple_layers(self):
+        return bool(self._counts()[7])
+
+    def get_counts(self):
+        c = self._counts()
+        keys = ["n", "nd", "nb", "n_edges", "n_dist_colors", "n_bend_colors", "table_size", "multi_layer"]
+        return dict(zip(keys, (int(v) for v in c)))
+
+    def get_cell_size(self):
+        v = C.c_float()
+        self._c(self._L.tc_get_cell_size(self._h, C.byref(v)))
+        return v.value
+
+    def get_state(self):
+        x, p, v = (np.empty((self._n, 3), _f32) for _ in range(3))
+        self._c(self._L.tc_get_state(self._h, _ptr(x), _ptr(p), _ptr(v)))
+        return x, p, v
+
+    def get_coloring(self):
+        c = self.get_counts()
+        dv = np.zeros((max(c["nd"], 1), 2), _u32)
+        dp = np.zeros((max(c["nd"], 1), 4), _f32)
+        do, dc = np.zeros(max(c["n_dist_colors"], 1), _u32), np.zeros(max(c["n_dist_colors"], 1), _u32)
+        self._c(self._L.tc_get_distance_constraints(self._h, _ptr(dv), _ptr(dp), _ptr(do), _ptr(dc)))
+        bv = np.zeros((max(c["nb"], 1), 4), _u32)
+        bp = np.zeros((max(c["nb"], 1), 4), _f32)
+        bo, bc = np.zeros(max(c["n_bend_colors"], 1), _u32), np.zeros(max(c["n_bend_colors"], 1), _u32)
+        self._c(self._L.tc_get_bending_constraints(self._h, _ptr(bv), _ptr(bp), _ptr(bo), _ptr(bc)))
+        k, m = c["n_dist_colors"], c["n_bend_colors"]
+        return dict(dist_v=dv[:c["nd"]], dist_par=dp[:c["nd"]], dist_off=do[:k], dist_cnt=dc[:k],
+                    bend_v=bv[:c["nb"]], bend_par=bp[:c["nb"]], bend_off=bo[:m], bend_cnt=bc[:m])
+
+    def get_hash_state(self, which=0):
+        c = self.get_counts()
+        cs = np.zeros(c["table_size"] + 1, _u32)
+        cnt = self._n if which == 0 else c["n_edges"]
+        srt = np.zeros(max(cnt, 1), _u32)
+        self._c(self._L.tc_get_hash_state(self._h, int(which), _ptr(cs), _ptr(srt)))
+        return cs, srt[:cnt]
+
+    def get_edges(self):
+        ne = self.get_counts()["n_edges"]
+        e = np.zeros((max(ne, 1), 2), _u32)
+        b = np.zeros(max((ne + 31) // 32, 1), _u32)
+        self._c(self._L.tc_get_edges(self._h, _ptr(e), _ptr(b)))
+        return e[:ne], b[:(ne + 31) // 32]
+
+    def set_residual_tracking(self, enable=True):
+        self._c(self._L.tc_set_residual_tracking(self._h, int(bool(enable))))
+
+    def get_residuals(self):
+        c = self.get_counts()
+        k, m = max(c["n_dist_colors"], 1), max(c["n_bend_colors"], 1)
+        dr, dm, br, bm = np.zeros(k, _f32), np.zeros(k, _f32), np.zeros(m, _f32), np.zeros(m, _f32)
+        tot = np.zeros(4, _f32)
+        self._c(self._L.tc_get_residuals(self._h, _ptr(dr), _ptr(dm), _ptr(br), _ptr(bm), _ptr(tot)))
+        return dict(dist_rms=dr[:c["n_dist_colors"]], dist_max=dm[:c["n_dist_colors"]],
+                    bend_rms=br[:c["n_bend_colors"]], bend_max=bm[:c["n_bend_colors"]],
+                    dist_rms_total=float(tot[0]), dist_max_total=float(tot[1]),
+                    bend_rms_total=float(tot[2]), bend_max_total=float(tot[3]))
+
+    def set_profiling_enabled(self, enable):
+        self._c(self._L.tc_set_profiling_enabled(self._h, int(bool(enable))))
+        return bool(enable)
+
+    def take_profile(self):
+        """[(pass name, total ms, launch groups)] since the last call."""
+        buf = C.create_string_buffer(4096)
+        ms = np.zeros(64, _f32)
+        cnt = np.zeros(64, _u32)
+        k = C.c_uint32()
+        self._c(self._L.tc_take_profile(self._h, buf, 4096, _ptr(ms), _ptr(cnt), 64, C.byref(k)))
+        names = buf.value.decode().split("\n")[:k.value]
+        return [(nm, float(ms[i]), int(cnt[i])) for i, nm in enumerate(names)]
+
+    def frame_kernel_count(self):
+        """Kernel launches in the recorded frame graph."""
+        v = C.c_uint32()
+        self._c(self._L.tc_frame_kernel_count(self._h, C.byref(v)))
+        return v.value
+
+    def last_frame_ms(self):
+        v = C.c_float()
+        self._c(self._L.tc_last_frame_ms(self._h, C.byref(v)))
+        return v.value

@@ -1,0 +1,142 @@
+"""CUDA path (through the C ABI) against the oracle and the reference goldens.
+
+Tolerances (floating point, stated by the build's target): positions within
+1e-5 of the cloth extent per frame and 1e-4 of the extent after 600 substeps.
+The kernels are built with --fmad=false and IEEE div/sqrt and follow the
+oracle's operation order, so in practice the match is bit-exact; the tests
+also report the fraction of bit-identical coordinates.  Integer outputs (hash
+cell starts, sorted indices) must be bit-exact.
+"""
+import numpy as np
+import pytest
+
+import golden_cases as gc
+from gpu_common import compare_frames, extent
+from taremincloth_b200 import ClothSimulator, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", ["case1", "case2", "case3"])
+def test_golden_single_step_exact(oracle_lib, case):
+    pin, pout = gc.step_input(case)
+    s = gc.make(ClothSimulator, case, positions=pin)
+    s.step(1.0 / 60.0, 20, 2)
+    out = np.empty(len(pin) * 3, np.float32)
+    s.get_positions(out)
+    out = out.reshape(-1, 3)
+    assert float(np.linalg.norm(out - pout, axis=1).max()) < 1e-5
+    o = gc.make(oracle_lib.OracleSim, case, positions=pin)
+    o.step(1.0 / 60.0, 20, 2)
+    assert float(np.abs(out - o.get_positions().reshape(-1, 3)).max()) <= 1e-6
+
+
+@pytest.mark.parametrize("case", ["case1", "case2", "case3", "case4"])
+def test_golden_trajectories_match_oracle(oracle_lib, case):
+    c, d, pos, inv = gc.load(case)
+    g = gc.make(ClothSimulator, case)
+    o = gc.make(oracle_lib.OracleSim, case)
+    worst, same = compare_frames(g, o, 25, 1.0 / 60.0, 20, extent(pos))
+    assert worst.max() <= 1e-4, worst
+    assert worst[:5].max() <= 1e-5, worst
+
+
+def test_config1_600_substeps(oracle_lib):
+    sc = scenes.config1()
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    worst, same = compare_frames(g, o, sc["frames"], sc["dt"], sc["substeps"], extent(sc["positions"]))
+    assert worst[0] <= 1e-5 and worst.max() <= 1e-4, (worst.max(), same.min())
+
+
+def test_config2_small_with_mesh_and_self_collision(oracle_lib):
+    sc = scenes.config2(n=40, subdiv=3)
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    worst, same = compare_frames(g, o, 12, sc["dt"], sc["substeps"], extent(sc["positions"]))
+    assert worst[0] <= 1e-5 and worst.max() <= 1e-4, (worst, same)
+
+
+def test_config2_full_one_substep(oracle_lib):
+    """Full-size configuration, one substep (the oracle takes ~30 s)."""
+    sc = scenes.config2()
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    dts = sc["dt"] / sc["substeps"]
+    g.step(dts, 1)
+    o.step(dts, 1)
+    xg, _, _ = g.get_state()
+    xo, _, _ = o.get_state()
+    assert float(np.abs(xg - xo).max()) / extent(sc["positions"]) <= 1e-5
+
+
+def test_hash_state_bit_exact(oracle_lib):
+    """Cell starts and sorted indices of the vertex and edge grids."""
+    sc = scenes.config2(n=64, subdiv=3)
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    for _ in range(3):
+        o.step(sc["dt"], sc["substeps"])
+    x, _, v = o.get_state()
+    g.set_positions_and_velocities(x, v)
+    o.set_state(x, v)
+    for which in (0, 1):
+        cs_g, s_g = g.get_hash_state(which)
+        cs_o, s_o = o.build_hash(which)
+        np.testing.assert_array_equal(cs_g, cs_o)
+        np.testing.assert_array_equal(s_g, s_o)
+
+
+def test_colouring_on_device_matches_oracle(oracle_lib):
+    sc = scenes.config1()
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    col = g.get_coloring()
+    oc = o.colors()
+    np.testing.assert_array_equal(col["dist_cnt"], oc["dist_cnt"])
+    np.testing.assert_array_equal(col["dist_v"], o.distance_constraints()["v"])
+
+
+def test_config2_full_frame_properties():
+    """Size-independent properties at full size: finite, no deep penetration of
+    the sphere, pinned-free cloth falls, residual reported."""
+    sc = scenes.config2()
+    g = scenes.build(ClothSimulator, sc)
+    g.set_residual_tracking(True)
+    y0 = float(sc["positions"][:, 1].mean())
+    for _ in range(3):
+        g.step(sc["dt"], sc["substeps"])
+    x, _, v = g.get_state()
+    assert np.isfinite(x).all() and np.isfinite(v).all()
+    assert float(x[:, 1].mean()) < y0
+    r = np.linalg.norm(x - np.array([0.5, 0.0, 0.5], np.float32), axis=1)
+    assert float(r.min()) > 0.4 - 0.01
+    res = g.get_residuals()
+    assert np.isfinite(res["dist_rms_total"]) and res["dist_rms_total"] >= 0.0
+
+
+def test_reset_and_state_roundtrip():
+    sc = scenes.config1()
+    g = scenes.build(ClothSimulator, sc)
+    x0, _, _ = g.get_state()
+    g.step(sc["dt"], sc["substeps"])
+    x1, _, v1 = g.get_state()
+    assert not np.array_equal(x0, x1)
+    g.reset()
+    xr, _, vr = g.get_state()
+    np.testing.assert_array_equal(xr, x0)
+    assert not vr.any()
+    g.set_positions_and_velocities(x1, v1)
+    x2, _, v2 = g.get_state()
+    np.testing.assert_array_equal(x2, x1)
+    np.testing.assert_array_equal(v2, v1)
+
+
+def test_invalid_inputs_raise():
+    with pytest.raises(ValueError):
+        ClothSimulator(np.zeros((3, 3), np.float32), np.array([[0, 9]], np.uint32))
+    with pytest.raises(ValueError):
+        ClothSimulator(np.zeros((3, 2), np.float32), np.array([[0, 1]], np.uint32))
+    s = ClothSimulator(np.zeros((3, 3), np.float32), np.array([[0, 1]], np.uint32))
+    with pytest.raises(ValueError):
+        s.get_positions(np.empty(2, np.float32))
