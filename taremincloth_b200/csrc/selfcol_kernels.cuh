@@ -211,228 +211,288 @@ __device__ __forceinline__ bool near_folded_sq(const SCArgs& s, uint32_t a, uint
 }
 
 // ---------------- sc_solve: shaders/self_collision.wgsl:317-681
-__global__ void __launch_bounds__(128) k_sc_solve(SCArgs s) {
-  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  if (index >= s.n) return;
-  const float4 xi4 = s.x4[index], pi4 = s.p4[index];
-  const float wi = xi4.w;
-  const bool pin_i = wi <= 0.0f;
-  const V3 xi = mk(xi4), pi = mk(pi4);
-  const float mli = length(pi - xi);
-  if (pin_i && mli < kEps) return;
-  const float thi = pi4.w;
-  const float lli = s.local_len[index];
+// One warp per vertex i.  The 27 neighbour buckets are flattened in the
+// reference's visiting order (cx outer, cz inner, bucket order inside a cell)
+// and lane L takes flattened candidates L, L+32, ...  Contacts accumulate with
+// integer atomics (order-free); the multi-layer untangle candidate, which the
+// reference picks with a first-strict-minimum scan, is the warp argmin of
+// (distance^2, flattened position).
+struct VertCtx {
+  uint32_t index;
+  float wi;
+  bool pin_i;
+  V3 xi, pi;
+  float mli, thi, lli;
+  I3 cell;
+  uint32_t li;
+  bool untangle, track;
+};
+
+__device__ __forceinline__ void sc_candidate(const SCArgs& s, const VertCtx& c, uint32_t j, int32_t cx, int32_t cy,
+                                             int32_t cz, uint32_t t, float& best_in, uint32_t& best_j,
+                                             uint32_t& best_t) {
+  const uint32_t index = c.index;
+  if (j >= s.n || j == index) return;
+  const float wi = c.wi;
+  const bool pin_i = c.pin_i;
+  const V3 xi = c.xi, pi = c.pi;
+  const float mli = c.mli, thi = c.thi, lli = c.lli;
+  const I3 cell = c.cell;
+  const uint32_t li = c.li;
+  const bool untangle = c.untangle, track = c.track;
   const float cs = s.cell;
-  const I3 cell = cell_of(pi, cs);
-  const uint32_t li = layer_of(s.v4, index);
-  const bool untangle = s.untangle != 0;
-  const bool track = untangle && !pin_i && li > 0u;
-  float best_in = 1e20f;
-  uint32_t best_j = 0xFFFFFFFFu;
   int32_t* acc = s.acc;
-  for (int32_t cx = cell.x - 1; cx <= cell.x + 1; ++cx)
-    for (int32_t cy = cell.y - 1; cy <= cell.y + 1; ++cy)
-      for (int32_t cz = cell.z - 1; cz <= cell.z + 1; ++cz) {
-        const uint32_t h = hash3(cx, cy, cz, s.table);
-        const uint32_t kb = s.cs[h], ke = s.cs[h + 1];
-        for (uint32_t k = kb; k < ke; ++k) {
-          const uint32_t j = s.srt[k];
-          if (j >= s.n || j == index) continue;
-          const float4 pj4 = s.p4[j];
-          const V3 pj = mk(pj4);
-          const I3 jc = cell_of(pj, cs);
-          if (!(jc.x == cx && jc.y == cy && jc.z == cz)) continue;
-          const V3 dvv = pi - pj;
-          const float d2 = dot(dvv, dvv);
-          const float thj = pj4.w, llj = s.local_len[j];
-          const float eth = fmaxf(thi + thj, fminf(lli, llj) * 0.06f);
-          const float mgd = eth + (lli + llj) * 1.3f;
-          const uint32_t lj = layer_of(s.v4, j);
-          if (track && lj < li && d2 < best_in) {
-            const float ur = eth * 2.5f + llj * 1.3f;
-            if (d2 <= ur * ur && !within2(s, index, j)) { best_in = d2; best_j = j; }
+  const float4 pj4 = s.p4[j];
+  const V3 pj = mk(pj4);
+  const I3 jc = cell_of(pj, cs);
+  if (!(jc.x == cx && jc.y == cy && jc.z == cz)) return;
+  const V3 dvv = pi - pj;
+  const float d2 = dot(dvv, dvv);
+  const float thj = pj4.w, llj = s.local_len[j];
+  const float eth = fmaxf(thi + thj, fminf(lli, llj) * 0.06f);
+  const float mgd = eth + (lli + llj) * 1.3f;
+  const uint32_t lj = layer_of(s.v4, j);
+  if (track && lj < li && d2 < best_in) {
+    const float ur = eth * 2.5f + llj * 1.3f;
+    if (d2 <= ur * ur && !within2(s, index, j)) { best_in = d2; best_j = j; best_t = t; }
+  }
+  if (!(d2 <= mgd * mgd)) return;
+  const float dvl = sqrtf(fmaxf(d2, 0.0f));
+  if (near_folded(s, index, j, dvl)) return;
+  const float4 xj4 = s.x4[j];
+  const V3 pjo = mk(xj4);
+  const float wj = xj4.w;
+  const bool both = wj > 0.0f;
+  const float eth2 = eth * eth;
+  // 1. vertex-vertex
+  if (!pin_i && (!both || index < j)) {
+    if (d2 < eth2 && d2 > kEps * kEps) {
+      bool utv = false;
+      if (untangle && li != lj) {
+        const V3 ni = mk(s.nrm[index]), nj = mk(s.nrm[j]);
+        const float nil = length(ni), njl = length(nj);
+        if (li > lj) {
+          if (njl > 0.5f) {
+            const V3 nju = nj / njl;
+            const bool allow = (wj <= 0.0f) || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), nju) > 0.0f);
+            utv = allow && (dot(dvv, nju) < 0.0f);
           }
-          if (!(d2 <= mgd * mgd)) continue;
-          const float dvl = sqrtf(fmaxf(d2, 0.0f));
-          if (near_folded(s, index, j, dvl)) continue;
-          const float4 xj4 = s.x4[j];
-          const V3 pjo = mk(xj4);
-          const float wj = xj4.w;
-          const bool both = wj > 0.0f;
-          const float eth2 = eth * eth;
-          // 1. vertex-vertex
-          if (!pin_i && (!both || index < j)) {
-            if (d2 < eth2 && d2 > kEps * kEps) {
-              bool utv = false;
-              if (untangle && li != lj) {
-                const V3 ni = mk(s.nrm[index]), nj = mk(s.nrm[j]);
-                const float nil = length(ni), njl = length(nj);
-                if (li > lj) {
-                  if (njl > 0.5f) {
-                    const V3 nju = nj / njl;
-                    const bool allow = (wj <= 0.0f) || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), nju) > 0.0f);
-                    utv = allow && (dot(dvv, nju) < 0.0f);
-                  }
-                } else if (both && nil > 0.5f) {
-                  const V3 niu = ni / nil;
-                  const bool allow = (njl <= 0.5f) || (dot(nj / fmaxf(njl, kEps), niu) > 0.0f);
-                  utv = allow && (dot(-dvv, niu) < 0.0f);
-                }
-              }
-              if (!utv) {
-                const V3 nn = dvv / dvl;
-                const float pen = eth - dvl;
-                const float ws = wi + wj;
-                if (ws > kEps) {
-                  if (wj <= 0.0f) {
-                    add_pin(acc, index, nn * pen + (pj - pjo) * 0.5f);
-                  } else {
-                    const V3 disp = nn * (pen * 0.5f);
-                    add_disp(acc, index, disp * (wi / ws));
-                    add_disp(acc, j, (-disp) * (wj / ws));
-                  }
-                }
-              }
-            }
+        } else if (both && nil > 0.5f) {
+          const V3 niu = ni / nil;
+          const bool allow = (njl <= 0.5f) || (dot(nj / fmaxf(njl, kEps), niu) > 0.0f);
+          utv = allow && (dot(-dvv, niu) < 0.0f);
+        }
+      }
+      if (!utv) {
+        const V3 nn = dvv / dvl;
+        const float pen = eth - dvl;
+        const float ws = wi + wj;
+        if (ws > kEps) {
+          if (wj <= 0.0f) {
+            add_pin(acc, index, nn * pen + (pj - pjo) * 0.5f);
+          } else {
+            const V3 disp = nn * (pen * 0.5f);
+            add_disp(acc, index, disp * (wi / ws));
+            add_disp(acc, j, (-disp) * (wj / ws));
           }
-          // 2. vertex-triangle
-          const float mlj = length(pj - pjo);
-          const float vtb = eth + llj * 1.3f + mli + mlj;
-          if (!(d2 <= vtb * vtb) || within2(s, index, j)) continue;
-          for (uint32_t st = s.star_off[j]; st < s.star_off[j + 1]; ++st) {
-            const uint2 pr = s.star_idx[st];
-            const uint32_t v0 = pr.x, v1 = pr.y;
-            if (v0 == index || v1 == index) continue;
-            const float4 q0 = s.p4[v0], q1 = s.p4[v1];
-            const float4 o0 = s.x4[v0], o1 = s.x4[v1];
-            const V3 pv0 = mk(q0), pv1 = mk(q1), pv0o = mk(o0), pv1o = mk(o1);
-            const float wv0 = o0.w, wv1 = o1.w;
-            const V3 d0 = pi - pv0;
-            const float ll0 = s.local_len[v0];
-            const float et0 = fmaxf(thi + q0.w, fminf(lli, ll0) * 0.06f);
-            const float b0 = et0 + ll0 * 1.3f + mli + length(pv0 - pv0o);
-            const I3 c0 = cell_of(pv0, cs);
-            const bool in0 = abs(c0.x - cell.x) <= 1 && abs(c0.y - cell.y) <= 1 && abs(c0.z - cell.z) <= 1 &&
-                             (dot(d0, d0) <= b0 * b0);
-            const V3 d1 = pi - pv1;
-            const float ll1 = s.local_len[v1];
-            const float et1 = fmaxf(thi + q1.w, fminf(lli, ll1) * 0.06f);
-            const float b1 = et1 + ll1 * 1.3f + mli + length(pv1 - pv1o);
-            const I3 c1 = cell_of(pv1, cs);
-            const bool in1 = abs(c1.x - cell.x) <= 1 && abs(c1.y - cell.y) <= 1 && abs(c1.z - cell.z) <= 1 &&
-                             (dot(d1, d1) <= b1 * b1);
-            if ((in0 && j > v0) || (in1 && j > v1)) continue;
-            const V3 tmove = (((pj - pjo) + (pv0 - pv0o)) + (pv1 - pv1o)) / 3.0f;
-            const bool tpin = (wj <= 0.0f) || (wv0 <= 0.0f) || (wv1 <= 0.0f);
-            const V3 rel = xi + tmove;
-            const V3 E = mk(eth, eth, eth);
-            const V3 smin = vmin(rel, pi) - E, smax = vmax(rel, pi) + E;
-            const V3 tmin = vmin(vmin(pj, pv0), pv1), tmax = vmax(vmax(pj, pv0), pv1);
-            if (smin.x > tmax.x || smin.y > tmax.y || smin.z > tmax.z || smax.x < tmin.x || smax.y < tmin.y ||
-                smax.z < tmin.z)
-              continue;
-            if (within2(s, index, v0) || within2(s, index, v1)) continue;
-            const V3 mv = pi - rel;
-            const float msq = dot(mv, mv);
-            float ht = 1.0f, hu = 0.0f, hv = 0.0f;
-            bool hit = false;
-            if (msq > 1e-12f) hit = seg_tri(rel, pi, pj, pv0, pv1, ht, hu, hv);
-            if (hit) {
-              const V3 hp = rel + mv * ht;
-              const V3 tc = cross(pv0 - pj, pv1 - pj);
-              const float tl = length(tc);
-              const V3 tn = tl > 1e-12f ? tc / tl : mk(0.0f, 1.0f, 0.0f);
-              const float hor = dot(rel - pj, tn);
-              bool utc = false;
-              if (untangle && !pin_i && (li > lj) && tl > 1e-12f) {
-                const V3 ni = mk(s.nrm[index]);
-                const float nil = length(ni);
-                const bool allow = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
-                const bool ret = (hor < 0.0f) && (dot(mv, tn) > 0.0f);
-                utc = allow && ret;
-              }
-              if (!utc) {
-                const float ss = fabsf(hor) > 1e-6f ? hor : dot(-mv, tn);
-                const V3 ns = ss >= 0.0f ? tn : -tn;
-                const float ho = fmaxf(dot(rel - hp, ns), 0.0f);
-                const float hs = fmaxf(ho, eth * 0.25f);
-                const V3 psafe = hp + ns * hs;
-                const V3 tccd = psafe - pi;
-                const float pcs = fmaxf(0.0f, eth - hs);
-                if (tpin) {
-                  if (!pin_i) add_ccd(acc, index, tccd + ns * pcs, false);
-                } else if (pin_i) {
-                  const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
-                  const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
-                  if (wt > kEps) {
-                    const V3 full = tccd + ns * pcs;
-                    if (wj > 0.0f) add_ccd(acc, j, (-full) * (bc.x * wj / wt), false);
-                    if (wv0 > 0.0f) add_ccd(acc, v0, (-full) * (bc.y * wv0 / wt), false);
-                    if (wv1 > 0.0f) add_ccd(acc, v1, (-full) * (bc.z * wv1 / wt), false);
-                  }
-                } else {
-                  const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
-                  const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
-                  const float wtot = wi + wt;
-                  if (wtot > kEps) {
-                    add_ccd(acc, index, tccd * (wi / wtot), false);
-                    if (wj > 0.0f) add_ccd(acc, j, (-tccd) * (bc.x * wj / wtot), false);
-                    if (wv0 > 0.0f) add_ccd(acc, v0, (-tccd) * (bc.y * wv0 / wtot), false);
-                    if (wv1 > 0.0f) add_ccd(acc, v1, (-tccd) * (bc.z * wv1 / wtot), false);
-                    if (pcs > kEps) {
-                      const V3 tp = ns * (pcs * 0.6f);
-                      add_disp(acc, index, tp * (wi / wtot));
-                      if (wj > 0.0f) add_disp(acc, j, (-tp) * (bc.x * wj / wtot));
-                      if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bc.y * wv0 / wtot));
-                      if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bc.z * wv1 / wtot));
-                    }
-                  }
-                }
-              }
-            } else {
-              bool isf;
-              V3 bary;
-              const V3 cp = closest_tri(pi, pj, pv0, pv1, isf, bary);
-              const V3 dvt = pi - cp;
-              const float d2vt = dot(dvt, dvt);
-              if (!pin_i && d2vt < eth2 && d2vt > kEps * kEps) {
-                const float dvtl = sqrtf(d2vt);
-                bool utv = false;
-                if (untangle && li > lj) {
-                  const V3 tc = cross(pv0 - pj, pv1 - pj);
-                  const float tl = length(tc);
-                  if (tl > kEps) {
-                    const V3 tn = tc / tl;
-                    if (dot(dvt, tn) < 0.0f) {
-                      const V3 ni = mk(s.nrm[index]);
-                      const float nil = length(ni);
-                      utv = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
-                    }
-                  }
-                }
-                if (!utv) {
-                  const V3 nvt = dvt / dvtl;
-                  const float pvt = eth - dvtl;
-                  if (tpin) {
-                    add_pin(acc, index, nvt * pvt + tmove * 0.5f);
-                  } else {
-                    const float wt = bary.x * bary.x * wj + bary.y * bary.y * wv0 + bary.z * bary.z * wv1;
-                    const float wtot = wi + wt;
-                    if (wtot > kEps) {
-                      const V3 tp = nvt * (pvt * 0.6f);
-                      add_disp(acc, index, tp * (wi / wtot));
-                      if (wj > 0.0f) add_disp(acc, j, (-tp) * (bary.x * wj / wtot));
-                      if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bary.y * wv0 / wtot));
-                      if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bary.z * wv1 / wtot));
-                    }
-                  }
-                }
-              }
+        }
+      }
+    }
+  }
+  // 2. vertex-triangle
+  const float mlj = length(pj - pjo);
+  const float vtb = eth + llj * 1.3f + mli + mlj;
+  if (!(d2 <= vtb * vtb) || within2(s, index, j)) return;
+  for (uint32_t st = s.star_off[j]; st < s.star_off[j + 1]; ++st) {
+    const uint2 pr = s.star_idx[st];
+    const uint32_t v0 = pr.x, v1 = pr.y;
+    if (v0 == index || v1 == index) continue;
+    const float4 q0 = s.p4[v0], q1 = s.p4[v1];
+    const float4 o0 = s.x4[v0], o1 = s.x4[v1];
+    const V3 pv0 = mk(q0), pv1 = mk(q1), pv0o = mk(o0), pv1o = mk(o1);
+    const float wv0 = o0.w, wv1 = o1.w;
+    const V3 d0 = pi - pv0;
+    const float ll0 = s.local_len[v0];
+    const float et0 = fmaxf(thi + q0.w, fminf(lli, ll0) * 0.06f);
+    const float b0 = et0 + ll0 * 1.3f + mli + length(pv0 - pv0o);
+    const I3 c0 = cell_of(pv0, cs);
+    const bool in0 = abs(c0.x - cell.x) <= 1 && abs(c0.y - cell.y) <= 1 && abs(c0.z - cell.z) <= 1 &&
+                     (dot(d0, d0) <= b0 * b0);
+    const V3 d1 = pi - pv1;
+    const float ll1 = s.local_len[v1];
+    const float et1 = fmaxf(thi + q1.w, fminf(lli, ll1) * 0.06f);
+    const float b1 = et1 + ll1 * 1.3f + mli + length(pv1 - pv1o);
+    const I3 c1 = cell_of(pv1, cs);
+    const bool in1 = abs(c1.x - cell.x) <= 1 && abs(c1.y - cell.y) <= 1 && abs(c1.z - cell.z) <= 1 &&
+                     (dot(d1, d1) <= b1 * b1);
+    if ((in0 && j > v0) || (in1 && j > v1)) continue;
+    const V3 tmove = (((pj - pjo) + (pv0 - pv0o)) + (pv1 - pv1o)) / 3.0f;
+    const bool tpin = (wj <= 0.0f) || (wv0 <= 0.0f) || (wv1 <= 0.0f);
+    const V3 rel = xi + tmove;
+    const V3 E = mk(eth, eth, eth);
+    const V3 smin = vmin(rel, pi) - E, smax = vmax(rel, pi) + E;
+    const V3 tmin = vmin(vmin(pj, pv0), pv1), tmax = vmax(vmax(pj, pv0), pv1);
+    if (smin.x > tmax.x || smin.y > tmax.y || smin.z > tmax.z || smax.x < tmin.x || smax.y < tmin.y ||
+        smax.z < tmin.z)
+      continue;
+    if (within2(s, index, v0) || within2(s, index, v1)) continue;
+    const V3 mv = pi - rel;
+    const float msq = dot(mv, mv);
+    float ht = 1.0f, hu = 0.0f, hv = 0.0f;
+    bool hit = false;
+    if (msq > 1e-12f) hit = seg_tri(rel, pi, pj, pv0, pv1, ht, hu, hv);
+    if (hit) {
+      const V3 hp = rel + mv * ht;
+      const V3 tc = cross(pv0 - pj, pv1 - pj);
+      const float tl = length(tc);
+      const V3 tn = tl > 1e-12f ? tc / tl : mk(0.0f, 1.0f, 0.0f);
+      const float hor = dot(rel - pj, tn);
+      bool utc = false;
+      if (untangle && !pin_i && (li > lj) && tl > 1e-12f) {
+        const V3 ni = mk(s.nrm[index]);
+        const float nil = length(ni);
+        const bool allow = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
+        const bool ret = (hor < 0.0f) && (dot(mv, tn) > 0.0f);
+        utc = allow && ret;
+      }
+      if (!utc) {
+        const float ss = fabsf(hor) > 1e-6f ? hor : dot(-mv, tn);
+        const V3 ns = ss >= 0.0f ? tn : -tn;
+        const float ho = fmaxf(dot(rel - hp, ns), 0.0f);
+        const float hs = fmaxf(ho, eth * 0.25f);
+        const V3 psafe = hp + ns * hs;
+        const V3 tccd = psafe - pi;
+        const float pcs = fmaxf(0.0f, eth - hs);
+        if (tpin) {
+          if (!pin_i) add_ccd(acc, index, tccd + ns * pcs, false);
+        } else if (pin_i) {
+          const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
+          const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
+          if (wt > kEps) {
+            const V3 full = tccd + ns * pcs;
+            if (wj > 0.0f) add_ccd(acc, j, (-full) * (bc.x * wj / wt), false);
+            if (wv0 > 0.0f) add_ccd(acc, v0, (-full) * (bc.y * wv0 / wt), false);
+            if (wv1 > 0.0f) add_ccd(acc, v1, (-full) * (bc.z * wv1 / wt), false);
+          }
+        } else {
+          const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
+          const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
+          const float wtot = wi + wt;
+          if (wtot > kEps) {
+            add_ccd(acc, index, tccd * (wi / wtot), false);
+            if (wj > 0.0f) add_ccd(acc, j, (-tccd) * (bc.x * wj / wtot), false);
+            if (wv0 > 0.0f) add_ccd(acc, v0, (-tccd) * (bc.y * wv0 / wtot), false);
+            if (wv1 > 0.0f) add_ccd(acc, v1, (-tccd) * (bc.z * wv1 / wtot), false);
+            if (pcs > kEps) {
+              const V3 tp = ns * (pcs * 0.6f);
+              add_disp(acc, index, tp * (wi / wtot));
+              if (wj > 0.0f) add_disp(acc, j, (-tp) * (bc.x * wj / wtot));
+              if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bc.y * wv0 / wtot));
+              if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bc.z * wv1 / wtot));
             }
           }
         }
       }
-  if (track && best_j < 0x3FFFFEu) acc[(size_t)index * A_N + A_UT] = (int32_t)(best_j + 1u);
+    } else {
+      bool isf;
+      V3 bary;
+      const V3 cp = closest_tri(pi, pj, pv0, pv1, isf, bary);
+      const V3 dvt = pi - cp;
+      const float d2vt = dot(dvt, dvt);
+      if (!pin_i && d2vt < eth2 && d2vt > kEps * kEps) {
+        const float dvtl = sqrtf(d2vt);
+        bool utv = false;
+        if (untangle && li > lj) {
+          const V3 tc = cross(pv0 - pj, pv1 - pj);
+          const float tl = length(tc);
+          if (tl > kEps) {
+            const V3 tn = tc / tl;
+            if (dot(dvt, tn) < 0.0f) {
+              const V3 ni = mk(s.nrm[index]);
+              const float nil = length(ni);
+              utv = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
+            }
+          }
+        }
+        if (!utv) {
+          const V3 nvt = dvt / dvtl;
+          const float pvt = eth - dvtl;
+          if (tpin) {
+            add_pin(acc, index, nvt * pvt + tmove * 0.5f);
+          } else {
+            const float wt = bary.x * bary.x * wj + bary.y * bary.y * wv0 + bary.z * bary.z * wv1;
+            const float wtot = wi + wt;
+            if (wtot > kEps) {
+              const V3 tp = nvt * (pvt * 0.6f);
+              add_disp(acc, index, tp * (wi / wtot));
+              if (wj > 0.0f) add_disp(acc, j, (-tp) * (bary.x * wj / wtot));
+              if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bary.y * wv0 / wtot));
+              if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bary.z * wv1 / wtot));
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_sc_solve(SCArgs s) {
+  __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t index = blockIdx.x * 8u + warp;
+  if (index >= s.n) return;  // whole warp
+  VertCtx c;
+  c.index = index;
+  const float4 xi4 = s.x4[index], pi4 = s.p4[index];
+  c.wi = xi4.w;
+  c.pin_i = c.wi <= 0.0f;
+  c.xi = mk(xi4);
+  c.pi = mk(pi4);
+  c.mli = length(c.pi - c.xi);
+  if (c.pin_i && c.mli < kEps) return;  // whole warp
+  c.thi = pi4.w;
+  c.lli = s.local_len[index];
+  c.cell = cell_of(c.pi, s.cell);
+  c.li = layer_of(s.v4, index);
+  c.untangle = s.untangle != 0;
+  c.track = c.untangle && !c.pin_i && c.li > 0u;
+  // bucket ranges of the 27 neighbour cells, lane k = (dx+1)*9 + (dy+1)*3 + (dz+1)
+  uint32_t cnt = 0, beg = 0;
+  if (lane < 27) {
+    const uint32_t h = hash3(c.cell.x - 1 + lane / 9, c.cell.y - 1 + (lane / 3) % 3, c.cell.z - 1 + lane % 3, s.table);
+    beg = s.cs[h];
+    cnt = s.cs[h + 1] - beg;
+  }
+  uint32_t incl = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane < 27) {
+    sh_start[warp][lane] = incl - cnt;
+    sh_end[warp][lane] = incl;
+    sh_beg[warp][lane] = beg;
+  }
+  __syncwarp();
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 26);
+  float best_in = 1e20f;
+  uint32_t best_j = 0xFFFFFFFFu, best_t = 0xFFFFFFFFu;
+  int k = 0;
+  for (uint32_t t = lane; t < total; t += 32u) {
+    while (t >= sh_end[warp][k]) ++k;
+    const uint32_t j = s.srt[sh_beg[warp][k] + (t - sh_start[warp][k])];
+    sc_candidate(s, c, j, c.cell.x - 1 + k / 9, c.cell.y - 1 + (k / 3) % 3, c.cell.z - 1 + k % 3, t, best_in, best_j,
+                 best_t);
+  }
+  if (c.track) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ob = __shfl_xor_sync(0xffffffffu, best_in, o);
+      const uint32_t ot = __shfl_xor_sync(0xffffffffu, best_t, o);
+      const uint32_t oj = __shfl_xor_sync(0xffffffffu, best_j, o);
+      if (ob < best_in || (ob == best_in && ot < best_t)) { best_in = ob; best_t = ot; best_j = oj; }
+    }
+    if (lane == 0 && best_j < 0x3FFFFEu) s.acc[(size_t)index * A_N + A_UT] = (int32_t)(best_j + 1u);
+  }
 }
 
 // ---------------- sc_untangle: shaders/self_collision_untangle.wgsl:199-394
@@ -598,253 +658,315 @@ __device__ __forceinline__ bool outer_behind(const SCArgs& s, uint32_t la, uint3
   return allow && (dot(-dab, ni) < 0.0f);
 }
 
-__global__ void __launch_bounds__(128) k_ee(SCArgs s) {
-  const uint32_t ei = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ei >= s.ne) return;
-  const uint2 ea = s.edges[ei];
-  const uint32_t u0 = ea.x, u1 = ea.y;
-  const float4 xu0 = s.x4[u0], xu1 = s.x4[u1], qu0 = s.p4[u0], qu1 = s.p4[u1];
-  const float w_u0 = xu0.w, w_u1 = xu1.w;
-  const bool apin = (w_u0 <= 0.0f) || (w_u1 <= 0.0f);
-  const V3 p_u0 = mk(qu0), p_u1 = mk(qu1), p_u0o = mk(xu0), p_u1o = mk(xu1);
-  const float thu0 = qu0.w, thu1 = qu1.w;
-  const float mta = fmaxf(thu0, thu1);
-  const bool bnda = ((s.edge_bits[ei >> 5] >> (ei & 31u)) & 1u) != 0u;
-  const V3 m2 = mk(mta * 2.0f, mta * 2.0f, mta * 2.0f);
-  const V3 amin = vmin(vmin(p_u0, p_u1), vmin(p_u0o, p_u1o)) - m2;
-  const V3 amax = vmax(vmax(p_u0, p_u1), vmax(p_u0o, p_u1o)) + m2;
-  const I3 base = cell_of((p_u0 + p_u1) * 0.5f, s.cell);
-  const uint32_t la = layer_of(s.v4, u0);
-  const bool untangle = s.untangle != 0;
+struct EdgeCtx {
+  uint32_t ei, u0, u1;
+  float w_u0, w_u1;
+  bool apin, bnda;
+  V3 p_u0, p_u1, p_u0o, p_u1o;
+  float thu0, thu1, mta;
+  V3 amin, amax;
+  uint32_t la;
+  bool untangle;
+};
+
+// Contact work for one counted edge pair (shaders/self_collision_ee_direct.wgsl:356-774).
+__device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, uint32_t eb, uint32_t j, uint32_t vj,
+                                        const float4& qj, const float4& qvj, const float4& xj, const float4& xvj) {
+  const uint32_t u0 = c.u0, u1 = c.u1;
+  const float w_u0 = c.w_u0, w_u1 = c.w_u1;
+  const bool apin = c.apin, bnda = c.bnda;
+  const V3 p_u0 = c.p_u0, p_u1 = c.p_u1, p_u0o = c.p_u0o, p_u1o = c.p_u1o;
+  const float thu0 = c.thu0, thu1 = c.thu1, mta = c.mta;
+  const uint32_t la = c.la;
+  const bool untangle = c.untangle;
   int32_t* acc = s.acc;
-  uint32_t search = 0;
-  for (int dz = -1; dz <= 1; ++dz)
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int32_t nx = base.x + dx, ny = base.y + dy, nz = base.z + dz;
-        const uint32_t h = hash3(nx, ny, nz, s.table);
-        const uint32_t st = s.ecs[h], en = s.ecs[h + 1];
-        if (st >= en) continue;
-        for (uint32_t q = 0; q < en - st; ++q) {
-          const uint32_t eb = s.esrt[st + q];
-          if (ei >= eb) continue;
-          const uint2 ebv = s.edges[eb];
-          const uint32_t j = ebv.x, vj = ebv.y;
-          if (j == u0 || j == u1 || vj == u0 || vj == u1) continue;
-          const float4 qj = s.p4[j], qvj = s.p4[vj];
-          const V3 p_j = mk(qj), p_vj = mk(qvj);
-          const I3 bc = cell_of((p_j + p_vj) * 0.5f, s.cell);
-          if (!(bc.x == nx && bc.y == ny && bc.z == nz)) continue;
-          const float4 xj = s.x4[j], xvj = s.x4[vj];
-          const V3 p_jo = mk(xj), p_vjo = mk(xvj);
-          const V3 bmin = vmin(vmin(p_j, p_vj), vmin(p_jo, p_vjo));
-          const V3 bmax = vmax(vmax(p_j, p_vj), vmax(p_jo, p_vjo));
-          if (amin.x > bmax.x || amin.y > bmax.y || amin.z > bmax.z || amax.x < bmin.x || amax.y < bmin.y ||
-              amax.z < bmin.z)
-            continue;
-          ++search;
-          if (search > s.max_search) return;
-          const float w_j = xj.w, w_vj = xvj.w;
-          const float thj = qj.w, thvj = qvj.w;
-          const uint32_t lb = layer_of(s.v4, j);
-          const bool bndb = ((s.edge_bits[eb >> 5] >> (eb & 31u)) & 1u) != 0u;
-          const bool bpair = bnda || bndb;
-          bool run_ccd = bpair, has1 = false;
-          float s1 = 0.f, t1 = 0.f, d2c = 0.f, ethc = 0.f;
-          V3 dl1 = mk(0.f, 0.f, 0.f);
-          if (!run_ccd) {
-            seg_seg(p_u0, p_u1, p_j, p_vj, s1, t1);
-            dl1 = vmix(p_u0, p_u1, s1) - vmix(p_j, p_vj, t1);
-            d2c = dot(dl1, dl1);
-            ethc = mixf(thu0, thu1, s1) + mixf(thj, thvj, t1);
-            const float meg = mta + fmaxf(thj, thvj);
-            const V3 dv0 = p_u0 - p_u0o, dv1 = p_u1 - p_u1o, dvj = p_j - p_jo, dvvj = p_vj - p_vjo;
-            const V3 va = (dv0 + dv1) * 0.5f, vb = (dvj + dvvj) * 0.5f;
-            const float rdg = length(va - vb) + 0.5f * (length(dv1 - dv0) + length(dvvj - dvj));
-            const float reach = meg + rdg;
-            if (d2c > reach * reach) continue;
-            has1 = true;
-            const V3 d0g = vmix(p_u0o, p_u1o, s1) - vmix(p_jo, p_vjo, t1);
-            run_ccd = (rdg > ethc * 0.5f) || (dot(d0g, dl1) <= 0.0f);
+  const V3 p_j = mk(qj), p_vj = mk(qvj), p_jo = mk(xj), p_vjo = mk(xvj);
+  const float w_j = xj.w, w_vj = xvj.w;
+  const float thj = qj.w, thvj = qvj.w;
+  const uint32_t lb = layer_of(s.v4, j);
+  const bool bndb = ((s.edge_bits[eb >> 5] >> (eb & 31u)) & 1u) != 0u;
+  const bool bpair = bnda || bndb;
+  bool run_ccd = bpair, has1 = false;
+  float s1 = 0.f, t1 = 0.f, d2c = 0.f, ethc = 0.f;
+  V3 dl1 = mk(0.f, 0.f, 0.f);
+  if (!run_ccd) {
+    seg_seg(p_u0, p_u1, p_j, p_vj, s1, t1);
+    dl1 = vmix(p_u0, p_u1, s1) - vmix(p_j, p_vj, t1);
+    d2c = dot(dl1, dl1);
+    ethc = mixf(thu0, thu1, s1) + mixf(thj, thvj, t1);
+    const float meg = mta + fmaxf(thj, thvj);
+    const V3 dv0 = p_u0 - p_u0o, dv1 = p_u1 - p_u1o, dvj = p_j - p_jo, dvvj = p_vj - p_vjo;
+    const V3 va = (dv0 + dv1) * 0.5f, vb = (dvj + dvvj) * 0.5f;
+    const float rdg = length(va - vb) + 0.5f * (length(dv1 - dv0) + length(dvvj - dvj));
+    const float reach = meg + rdg;
+    if (d2c > reach * reach) return;
+    has1 = true;
+    const V3 d0g = vmix(p_u0o, p_u1o, s1) - vmix(p_jo, p_vjo, t1);
+    run_ccd = (rdg > ethc * 0.5f) || (dot(d0g, dl1) <= 0.0f);
+  }
+  if (run_ccd) {
+    float msd = 1e20f, btau = 0.0f, hs = 0.125f, ms = 0.f, mt = 0.f;
+    float pv = seg_vol(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, 0.0f);
+    float zc = -1.0f;
+    for (uint32_t k = 0; k <= 8u; ++k) {
+      const float tk = (float)k * 0.125f;
+      float es, et;
+      const float ed = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, tk, es, et);
+      if (ed < msd) { msd = ed; btau = tk; ms = es; mt = et; }
+      if (k > 0u) {
+        const float vol = seg_vol(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, tk);
+        if (pv * vol <= 0.0f && zc < 0.0f) zc = tk - 0.0625f;
+        pv = vol;
+      }
+    }
+    if (zc >= 0.0f) {
+      float es, et;
+      const float ed = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, zc, es, et);
+      if (ed < msd) { msd = ed; btau = zc; hs = 0.0625f; ms = es; mt = et; }
+    }
+    float tlo = fmaxf(0.0f, btau - hs), thi = fminf(1.0f, btau + hs);
+    float tstar = btau, dstar = msd, ss = ms, ts = mt;
+    for (int it = 0; it < 6; ++it) {
+      const float m1 = tlo + (thi - tlo) * (1.0f / 3.0f);
+      const float mm2 = thi - (thi - tlo) * (1.0f / 3.0f);
+      float e1s, e1t, e2s, e2t;
+      const float e1 = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, m1, e1s, e1t);
+      const float e2 = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, mm2, e2s, e2t);
+      if (e1 < dstar) { dstar = e1; tstar = m1; ss = e1s; ts = e1t; }
+      if (e2 < dstar) { dstar = e2; tstar = mm2; ss = e2s; ts = e2t; }
+      if (e1 < e2) thi = mm2; else tlo = m1;
+    }
+    const float ets = mixf(thu0, thu1, ss) + mixf(thj, thvj, ts);
+    if (dstar >= ets * ets) return;
+    if (s.exclude_neighbors) {
+      const V3 a0s = vmix(p_u0o, p_u0, tstar), a1s = vmix(p_u1o, p_u1, tstar);
+      const V3 b0s = vmix(p_jo, p_j, tstar), b1s = vmix(p_vjo, p_vj, tstar);
+      const V3 t0 = a0s - b0s, t1v = a0s - b1s, t2 = a1s - b0s, t3 = a1s - b1s;
+      if (near_folded_sq(s, u0, j, dot(t0, t0)) || near_folded_sq(s, u0, vj, dot(t1v, t1v)) ||
+          near_folded_sq(s, u1, j, dot(t2, t2)) || near_folded_sq(s, u1, vj, dot(t3, t3)))
+        return;
+    }
+    bool utc = false;
+    if (untangle && la != lb) {
+      const bool afx = (w_u0 == 0.0f) && (w_u1 == 0.0f);
+      const bool bfx = (w_j == 0.0f) && (w_vj == 0.0f);
+      const V3 d0u = ((p_u0o + p_u1o) - (p_jo + p_vjo)) * 0.5f;
+      const V3 d1u = ((p_u0 + p_u1) - (p_j + p_vj)) * 0.5f;
+      const V3 mu = d1u - d0u;
+      if (la > lb && !afx) {
+        const V3 ni = mk(s.nrm[j]), no = mk(s.nrm[u0]);
+        const bool allow = bfx || (dot(no, no) <= 0.25f);
+        utc = allow && (dot(ni, ni) > 0.25f) && (dot(d0u, ni) < 0.0f) && (dot(mu, ni) > 0.0f);
+      } else if (lb > la && !bfx) {
+        const V3 ni = mk(s.nrm[u0]), no = mk(s.nrm[j]);
+        const bool allow = afx || (dot(no, no) <= 0.25f);
+        utc = allow && (dot(ni, ni) > 0.25f) && (dot(-d0u, ni) < 0.0f) && (dot(-mu, ni) > 0.0f);
+      }
+    }
+    if (utc) return;
+    float s0, t0p;
+    seg_seg(p_u0o, p_u1o, p_jo, p_vjo, s0, t0p);
+    const V3 d0 = vmix(p_u0o, p_u1o, s0) - vmix(p_jo, p_vjo, t0p);
+    const float dist0 = length(d0);
+    if (dist0 > kEps) {
+      const V3 n0 = d0 / dist0;
+      float s1b, t1b;
+      seg_seg(p_u0, p_u1, p_j, p_vj, s1b, t1b);
+      const V3 d1 = vmix(p_u0, p_u1, s1b) - vmix(p_j, p_vj, t1b);
+      const float dist1 = length(d1);
+      const V3 de = vmix(p_u0, p_u1, ss) - vmix(p_j, p_vj, ts);
+      const float he = dot(de, n0);
+      const bool crossed = (he <= 0.0f) || (dot(d1, n0) <= 0.0f) || (bpair && dist1 >= ets && tstar < 1.0f);
+      if (he < ets && crossed) {
+        const float pc = ets - he;
+        const bool bpin = (w_j <= 0.0f) || (w_vj <= 0.0f);
+        if (apin && bpin) return;
+        const bool aall = (w_u0 == 0.0f) && (w_u1 == 0.0f);
+        const bool ball = (w_j == 0.0f) && (w_vj == 0.0f);
+        const bool cpe = !(aall || ball);
+        if (bpin) {
+          const V3 em = ((p_j - p_jo) + (p_vj - p_vjo)) * 0.5f;
+          const float a = 1.0f - ss, b = ss;
+          const float den = a * a * w_u0 + b * b * w_u1;
+          if (den > kEps) {
+            const V3 pb = n0 * pc + em * 0.5f;
+            if (w_u0 > 0.0f) add_ccd(acc, u0, pb * fminf((a * w_u0) / den, 2.0f), cpe);
+            if (w_u1 > 0.0f) add_ccd(acc, u1, pb * fminf((b * w_u1) / den, 2.0f), cpe);
           }
-          if (run_ccd) {
-            float msd = 1e20f, btau = 0.0f, hs = 0.125f, ms = 0.f, mt = 0.f;
-            float pv = seg_vol(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, 0.0f);
-            float zc = -1.0f;
-            for (uint32_t k = 0; k <= 8u; ++k) {
-              const float tk = (float)k * 0.125f;
-              float es, et;
-              const float ed = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, tk, es, et);
-              if (ed < msd) { msd = ed; btau = tk; ms = es; mt = et; }
-              if (k > 0u) {
-                const float vol = seg_vol(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, tk);
-                if (pv * vol <= 0.0f && zc < 0.0f) zc = tk - 0.0625f;
-                pv = vol;
-              }
-            }
-            if (zc >= 0.0f) {
-              float es, et;
-              const float ed = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, zc, es, et);
-              if (ed < msd) { msd = ed; btau = zc; hs = 0.0625f; ms = es; mt = et; }
-            }
-            float tlo = fmaxf(0.0f, btau - hs), thi = fminf(1.0f, btau + hs);
-            float tstar = btau, dstar = msd, ss = ms, ts = mt;
-            for (int it = 0; it < 6; ++it) {
-              const float m1 = tlo + (thi - tlo) * (1.0f / 3.0f);
-              const float mm2 = thi - (thi - tlo) * (1.0f / 3.0f);
-              float e1s, e1t, e2s, e2t;
-              const float e1 = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, m1, e1s, e1t);
-              const float e2 = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, mm2, e2s, e2t);
-              if (e1 < dstar) { dstar = e1; tstar = m1; ss = e1s; ts = e1t; }
-              if (e2 < dstar) { dstar = e2; tstar = mm2; ss = e2s; ts = e2t; }
-              if (e1 < e2) thi = mm2; else tlo = m1;
-            }
-            const float ets = mixf(thu0, thu1, ss) + mixf(thj, thvj, ts);
-            if (dstar >= ets * ets) continue;
-            if (s.exclude_neighbors) {
-              const V3 a0s = vmix(p_u0o, p_u0, tstar), a1s = vmix(p_u1o, p_u1, tstar);
-              const V3 b0s = vmix(p_jo, p_j, tstar), b1s = vmix(p_vjo, p_vj, tstar);
-              const V3 t0 = a0s - b0s, t1v = a0s - b1s, t2 = a1s - b0s, t3 = a1s - b1s;
-              if (near_folded_sq(s, u0, j, dot(t0, t0)) || near_folded_sq(s, u0, vj, dot(t1v, t1v)) ||
-                  near_folded_sq(s, u1, j, dot(t2, t2)) || near_folded_sq(s, u1, vj, dot(t3, t3)))
-                continue;
-            }
-            bool utc = false;
-            if (untangle && la != lb) {
-              const bool afx = (w_u0 == 0.0f) && (w_u1 == 0.0f);
-              const bool bfx = (w_j == 0.0f) && (w_vj == 0.0f);
-              const V3 d0u = ((p_u0o + p_u1o) - (p_jo + p_vjo)) * 0.5f;
-              const V3 d1u = ((p_u0 + p_u1) - (p_j + p_vj)) * 0.5f;
-              const V3 mu = d1u - d0u;
-              if (la > lb && !afx) {
-                const V3 ni = mk(s.nrm[j]), no = mk(s.nrm[u0]);
-                const bool allow = bfx || (dot(no, no) <= 0.25f);
-                utc = allow && (dot(ni, ni) > 0.25f) && (dot(d0u, ni) < 0.0f) && (dot(mu, ni) > 0.0f);
-              } else if (lb > la && !bfx) {
-                const V3 ni = mk(s.nrm[u0]), no = mk(s.nrm[j]);
-                const bool allow = afx || (dot(no, no) <= 0.25f);
-                utc = allow && (dot(ni, ni) > 0.25f) && (dot(-d0u, ni) < 0.0f) && (dot(-mu, ni) > 0.0f);
-              }
-            }
-            if (utc) continue;
-            float s0, t0p;
-            seg_seg(p_u0o, p_u1o, p_jo, p_vjo, s0, t0p);
-            const V3 d0 = vmix(p_u0o, p_u1o, s0) - vmix(p_jo, p_vjo, t0p);
-            const float dist0 = length(d0);
-            if (dist0 > kEps) {
-              const V3 n0 = d0 / dist0;
-              float s1b, t1b;
-              seg_seg(p_u0, p_u1, p_j, p_vj, s1b, t1b);
-              const V3 d1 = vmix(p_u0, p_u1, s1b) - vmix(p_j, p_vj, t1b);
-              const float dist1 = length(d1);
-              const V3 de = vmix(p_u0, p_u1, ss) - vmix(p_j, p_vj, ts);
-              const float he = dot(de, n0);
-              const bool crossed = (he <= 0.0f) || (dot(d1, n0) <= 0.0f) || (bpair && dist1 >= ets && tstar < 1.0f);
-              if (he < ets && crossed) {
-                const float pc = ets - he;
-                const bool bpin = (w_j <= 0.0f) || (w_vj <= 0.0f);
-                if (apin && bpin) continue;
-                const bool aall = (w_u0 == 0.0f) && (w_u1 == 0.0f);
-                const bool ball = (w_j == 0.0f) && (w_vj == 0.0f);
-                const bool cpe = !(aall || ball);
-                if (bpin) {
-                  const V3 em = ((p_j - p_jo) + (p_vj - p_vjo)) * 0.5f;
-                  const float a = 1.0f - ss, b = ss;
-                  const float den = a * a * w_u0 + b * b * w_u1;
-                  if (den > kEps) {
-                    const V3 pb = n0 * pc + em * 0.5f;
-                    if (w_u0 > 0.0f) add_ccd(acc, u0, pb * fminf((a * w_u0) / den, 2.0f), cpe);
-                    if (w_u1 > 0.0f) add_ccd(acc, u1, pb * fminf((b * w_u1) / den, 2.0f), cpe);
-                  }
-                } else if (apin) {
-                  const V3 em = ((p_u0 - p_u0o) + (p_u1 - p_u1o)) * 0.5f;
-                  const float a = 1.0f - ts, b = ts;
-                  const float den = a * a * w_j + b * b * w_vj;
-                  if (den > kEps) {
-                    const V3 pb = (-n0) * pc + em * 0.5f;
-                    if (w_j > 0.0f) add_ccd(acc, j, pb * fminf((a * w_j) / den, 2.0f), cpe);
-                    if (w_vj > 0.0f) add_ccd(acc, vj, pb * fminf((b * w_vj) / den, 2.0f), cpe);
-                  }
-                } else {
-                  const float we1 = (1.0f - ss) * (1.0f - ss) * w_u0 + ss * ss * w_u1;
-                  const float we2 = (1.0f - ts) * (1.0f - ts) * w_j + ts * ts * w_vj;
-                  const float wtot = we1 + we2;
-                  if (wtot > kEps) {
-                    const V3 tcc = n0 * pc;
-                    if (w_u0 > 0.0f) add_ccd(acc, u0, tcc * ((1.0f - ss) * w_u0 / wtot), true);
-                    if (w_u1 > 0.0f) add_ccd(acc, u1, tcc * (ss * w_u1 / wtot), true);
-                    if (w_j > 0.0f) add_ccd(acc, j, (-tcc) * ((1.0f - ts) * w_j / wtot), true);
-                    if (w_vj > 0.0f) add_ccd(acc, vj, (-tcc) * (ts * w_vj / wtot), true);
-                  }
-                }
-                continue;
-              }
-            }
+        } else if (apin) {
+          const V3 em = ((p_u0 - p_u0o) + (p_u1 - p_u1o)) * 0.5f;
+          const float a = 1.0f - ts, b = ts;
+          const float den = a * a * w_j + b * b * w_vj;
+          if (den > kEps) {
+            const V3 pb = (-n0) * pc + em * 0.5f;
+            if (w_j > 0.0f) add_ccd(acc, j, pb * fminf((a * w_j) / den, 2.0f), cpe);
+            if (w_vj > 0.0f) add_ccd(acc, vj, pb * fminf((b * w_vj) / den, 2.0f), cpe);
           }
-          {
-            float sst, tst, d2e, eth;
-            V3 de;
-            if (has1) {
-              sst = s1; tst = t1; de = dl1; d2e = d2c; eth = ethc;
-            } else {
-              seg_seg(p_u0, p_u1, p_j, p_vj, sst, tst);
-              de = (p_u0 + (p_u1 - p_u0) * sst) - (p_j + (p_vj - p_j) * tst);
-              d2e = dot(de, de);
-              eth = mixf(thu0, thu1, sst) + mixf(thj, thvj, tst);
-            }
-            if (d2e >= eth * eth || d2e <= kEps * kEps) continue;
-            if (s.exclude_neighbors) {
-              const V3 e0 = p_u0 - p_j, e1 = p_u0 - p_vj, e2 = p_u1 - p_j, e3 = p_u1 - p_vj;
-              if (near_folded_sq(s, u0, j, dot(e0, e0)) || near_folded_sq(s, u0, vj, dot(e1, e1)) ||
-                  near_folded_sq(s, u1, j, dot(e2, e2)) || near_folded_sq(s, u1, vj, dot(e3, e3)))
-                continue;
-            }
-            const float del = sqrtf(d2e);
-            bool ute = false;
-            if (untangle) {
-              const bool afx = (w_u0 <= 0.0f) && (w_u1 <= 0.0f);
-              const bool bfx = (w_j <= 0.0f) && (w_vj <= 0.0f);
-              ute = outer_behind(s, la, lb, u0, u1, j, vj, afx, bfx, de);
-            }
-            if (!ute) {
-              const V3 ne = de / del;
-              const float pe = eth - del;
-              const bool bpin = (w_j <= 0.0f) || (w_vj <= 0.0f);
-              if (apin && bpin) continue;
-              if (bpin) {
-                const V3 em = ((p_j - p_jo) + (p_vj - p_vjo)) * 0.5f;
-                const float a = 1.0f - sst, b = sst;
-                const float den = a * a * w_u0 + b * b * w_u1;
-                if (den > kEps) {
-                  const V3 pb = ne * pe + em * 0.5f;
-                  if (w_u0 > 0.0f) add_pin(acc, u0, pb * fminf((a * w_u0) / den, 2.0f));
-                  if (w_u1 > 0.0f) add_pin(acc, u1, pb * fminf((b * w_u1) / den, 2.0f));
-                }
-              } else if (apin) {
-                const V3 em = ((p_u0 - p_u0o) + (p_u1 - p_u1o)) * 0.5f;
-                const float a = 1.0f - tst, b = tst;
-                const float den = a * a * w_j + b * b * w_vj;
-                if (den > kEps) {
-                  const V3 pb = (-ne) * pe + em * 0.5f;
-                  if (w_j > 0.0f) add_pin(acc, j, pb * fminf((a * w_j) / den, 2.0f));
-                  if (w_vj > 0.0f) add_pin(acc, vj, pb * fminf((b * w_vj) / den, 2.0f));
-                }
-              } else {
-                const float we1 = (1.0f - sst) * (1.0f - sst) * w_u0 + sst * sst * w_u1;
-                const float we2 = (1.0f - tst) * (1.0f - tst) * w_j + tst * tst * w_vj;
-                const float wtot = we1 + we2;
-                if (wtot > kEps) {
-                  const V3 td = ne * (pe * 0.6f);
-                  if (w_u0 > 0.0f) add_disp(acc, u0, td * ((1.0f - sst) * w_u0 / wtot));
-                  if (w_u1 > 0.0f) add_disp(acc, u1, td * (sst * w_u1 / wtot));
-                  if (w_j > 0.0f) add_disp(acc, j, (-td) * ((1.0f - tst) * w_j / wtot));
-                  if (w_vj > 0.0f) add_disp(acc, vj, (-td) * (tst * w_vj / wtot));
-                }
-              }
-            }
+        } else {
+          const float we1 = (1.0f - ss) * (1.0f - ss) * w_u0 + ss * ss * w_u1;
+          const float we2 = (1.0f - ts) * (1.0f - ts) * w_j + ts * ts * w_vj;
+          const float wtot = we1 + we2;
+          if (wtot > kEps) {
+            const V3 tcc = n0 * pc;
+            if (w_u0 > 0.0f) add_ccd(acc, u0, tcc * ((1.0f - ss) * w_u0 / wtot), true);
+            if (w_u1 > 0.0f) add_ccd(acc, u1, tcc * (ss * w_u1 / wtot), true);
+            if (w_j > 0.0f) add_ccd(acc, j, (-tcc) * ((1.0f - ts) * w_j / wtot), true);
+            if (w_vj > 0.0f) add_ccd(acc, vj, (-tcc) * (ts * w_vj / wtot), true);
+          }
+        }
+        return;
+      }
+    }
+  }
+  {
+    float sst, tst, d2e, eth;
+    V3 de;
+    if (has1) {
+      sst = s1; tst = t1; de = dl1; d2e = d2c; eth = ethc;
+    } else {
+      seg_seg(p_u0, p_u1, p_j, p_vj, sst, tst);
+      de = (p_u0 + (p_u1 - p_u0) * sst) - (p_j + (p_vj - p_j) * tst);
+      d2e = dot(de, de);
+      eth = mixf(thu0, thu1, sst) + mixf(thj, thvj, tst);
+    }
+    if (d2e >= eth * eth || d2e <= kEps * kEps) return;
+    if (s.exclude_neighbors) {
+      const V3 e0 = p_u0 - p_j, e1 = p_u0 - p_vj, e2 = p_u1 - p_j, e3 = p_u1 - p_vj;
+      if (near_folded_sq(s, u0, j, dot(e0, e0)) || near_folded_sq(s, u0, vj, dot(e1, e1)) ||
+          near_folded_sq(s, u1, j, dot(e2, e2)) || near_folded_sq(s, u1, vj, dot(e3, e3)))
+        return;
+    }
+    const float del = sqrtf(d2e);
+    bool ute = false;
+    if (untangle) {
+      const bool afx = (w_u0 <= 0.0f) && (w_u1 <= 0.0f);
+      const bool bfx = (w_j <= 0.0f) && (w_vj <= 0.0f);
+      ute = outer_behind(s, la, lb, u0, u1, j, vj, afx, bfx, de);
+    }
+    if (!ute) {
+      const V3 ne = de / del;
+      const float pe = eth - del;
+      const bool bpin = (w_j <= 0.0f) || (w_vj <= 0.0f);
+      if (apin && bpin) return;
+      if (bpin) {
+        const V3 em = ((p_j - p_jo) + (p_vj - p_vjo)) * 0.5f;
+        const float a = 1.0f - sst, b = sst;
+        const float den = a * a * w_u0 + b * b * w_u1;
+        if (den > kEps) {
+          const V3 pb = ne * pe + em * 0.5f;
+          if (w_u0 > 0.0f) add_pin(acc, u0, pb * fminf((a * w_u0) / den, 2.0f));
+          if (w_u1 > 0.0f) add_pin(acc, u1, pb * fminf((b * w_u1) / den, 2.0f));
+        }
+      } else if (apin) {
+        const V3 em = ((p_u0 - p_u0o) + (p_u1 - p_u1o)) * 0.5f;
+        const float a = 1.0f - tst, b = tst;
+        const float den = a * a * w_j + b * b * w_vj;
+        if (den > kEps) {
+          const V3 pb = (-ne) * pe + em * 0.5f;
+          if (w_j > 0.0f) add_pin(acc, j, pb * fminf((a * w_j) / den, 2.0f));
+          if (w_vj > 0.0f) add_pin(acc, vj, pb * fminf((b * w_vj) / den, 2.0f));
+        }
+      } else {
+        const float we1 = (1.0f - sst) * (1.0f - sst) * w_u0 + sst * sst * w_u1;
+        const float we2 = (1.0f - tst) * (1.0f - tst) * w_j + tst * tst * w_vj;
+        const float wtot = we1 + we2;
+        if (wtot > kEps) {
+          const V3 td = ne * (pe * 0.6f);
+          if (w_u0 > 0.0f) add_disp(acc, u0, td * ((1.0f - sst) * w_u0 / wtot));
+          if (w_u1 > 0.0f) add_disp(acc, u1, td * (sst * w_u1 / wtot));
+          if (w_j > 0.0f) add_disp(acc, j, (-td) * ((1.0f - tst) * w_j / wtot));
+          if (w_vj > 0.0f) add_disp(acc, vj, (-td) * (tst * w_vj / wtot));
+        }
+      }
+    }
+  }
+}
+
+// One warp per edge; candidates of the 27 cells around the edge midpoint are
+// flattened in the reference's order (dz outer, dx inner) and visited 32 per
+// round.  The per-edge cap on counted candidates (search_count >
+// max_search_iterations, :356-359) is applied with a ballot prefix count, so
+// exactly the reference's first max_search counted pairs are processed.
+__global__ void __launch_bounds__(256) k_ee(SCArgs s) {
+  __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ei = blockIdx.x * 8u + warp;
+  if (ei >= s.ne) return;  // whole warp
+  EdgeCtx c;
+  c.ei = ei;
+  const uint2 ea = s.edges[ei];
+  c.u0 = ea.x;
+  c.u1 = ea.y;
+  const float4 xu0 = s.x4[c.u0], xu1 = s.x4[c.u1], qu0 = s.p4[c.u0], qu1 = s.p4[c.u1];
+  c.w_u0 = xu0.w;
+  c.w_u1 = xu1.w;
+  c.apin = (c.w_u0 <= 0.0f) || (c.w_u1 <= 0.0f);
+  c.p_u0 = mk(qu0); c.p_u1 = mk(qu1); c.p_u0o = mk(xu0); c.p_u1o = mk(xu1);
+  c.thu0 = qu0.w;
+  c.thu1 = qu1.w;
+  c.mta = fmaxf(c.thu0, c.thu1);
+  c.bnda = ((s.edge_bits[ei >> 5] >> (ei & 31u)) & 1u) != 0u;
+  const V3 m2 = mk(c.mta * 2.0f, c.mta * 2.0f, c.mta * 2.0f);
+  c.amin = vmin(vmin(c.p_u0, c.p_u1), vmin(c.p_u0o, c.p_u1o)) - m2;
+  c.amax = vmax(vmax(c.p_u0, c.p_u1), vmax(c.p_u0o, c.p_u1o)) + m2;
+  const I3 base = cell_of((c.p_u0 + c.p_u1) * 0.5f, s.cell);
+  c.la = layer_of(s.v4, c.u0);
+  c.untangle = s.untangle != 0;
+  // lane k = (dz+1)*9 + (dy+1)*3 + (dx+1)
+  uint32_t cnt = 0, beg = 0;
+  if (lane < 27) {
+    const uint32_t h = hash3(base.x - 1 + lane % 3, base.y - 1 + (lane / 3) % 3, base.z - 1 + lane / 9, s.table);
+    beg = s.ecs[h];
+    const uint32_t en = s.ecs[h + 1];
+    cnt = en > beg ? en - beg : 0u;
+  }
+  uint32_t incl = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane < 27) {
+    sh_start[warp][lane] = incl - cnt;
+    sh_end[warp][lane] = incl;
+    sh_beg[warp][lane] = beg;
+  }
+  __syncwarp();
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 26);
+  uint32_t counted = 0;
+  int k = 0;
+  for (uint32_t base_t = 0; base_t < total && counted < s.max_search; base_t += 32u) {
+    const uint32_t t = base_t + lane;
+    bool pass = false;
+    uint32_t eb = 0, j = 0, vj = 0;
+    float4 qj, qvj, xj, xvj;
+    if (t < total) {
+      while (t >= sh_end[warp][k]) ++k;
+      eb = s.esrt[sh_beg[warp][k] + (t - sh_start[warp][k])];
+      if (ei < eb) {
+        const uint2 ebv = s.edges[eb];
+        j = ebv.x;
+        vj = ebv.y;
+        if (!(j == c.u0 || j == c.u1 || vj == c.u0 || vj == c.u1)) {
+          qj = s.p4[j];
+          qvj = s.p4[vj];
+          const I3 bc = cell_of((mk(qj) + mk(qvj)) * 0.5f, s.cell);
+          if (bc.x == base.x - 1 + k % 3 && bc.y == base.y - 1 + (k / 3) % 3 && bc.z == base.z - 1 + k / 9) {
+            xj = s.x4[j];
+            xvj = s.x4[vj];
+            const V3 p_j = mk(qj), p_vj = mk(qvj), p_jo = mk(xj), p_vjo = mk(xvj);
+            const V3 bmin = vmin(vmin(p_j, p_vj), vmin(p_jo, p_vjo));
+            const V3 bmax = vmax(vmax(p_j, p_vj), vmax(p_jo, p_vjo));
+            pass = !(c.amin.x > bmax.x || c.amin.y > bmax.y || c.amin.z > bmax.z || c.amax.x < bmin.x ||
+                     c.amax.y < bmin.y || c.amax.z < bmin.z);
           }
         }
       }
+    }
+    const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
+    const uint32_t rank = counted + __popc(ballot & ((1u << lane) - 1u));
+    counted += __popc(ballot);
+    if (pass && rank < s.max_search) ee_pair(s, c, eb, j, vj, qj, qvj, xj, xvj);
+  }
 }
 
 // ---------------- sc_apply: shaders/self_collision_apply.wgsl:57-177

@@ -437,9 +437,9 @@ struct Sim {
     if (a.untangle) timed("sc_normals", [&] { k_normals<<<grid(n, 256), 256, 0, st>>>(n, x4.p, star_off.p, star_idx.p, nrm.p); });
     encode_hash(0);
     if (ne > 0) encode_hash(1);
-    timed("sc_solve", [&] { k_sc_solve<<<grid(n, 128), 128, 0, st>>>(a); });
+    timed("sc_solve", [&] { k_sc_solve<<<grid(n, 8), 256, 0, st>>>(a); });
     if (a.untangle) timed("sc_untangle", [&] { k_untangle<<<grid(n, 128), 128, 0, st>>>(a); });
-    if (ne > 0) timed("sc_solve_ee", [&] { k_ee<<<grid(ne, 128), 128, 0, st>>>(a); });
+    if (ne > 0) timed("sc_solve_ee", [&] { k_ee<<<grid(ne, 8), 256, 0, st>>>(a); });
     timed("sc_apply", [&] {
       k_apply<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, local_len.p, acc.p, relief, enable_relief ? 1 : 0,
                                              max_disp_ratio);
