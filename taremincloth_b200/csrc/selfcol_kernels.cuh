@@ -45,7 +45,80 @@ struct SCArgs {
   const uint32_t* esrt;  // edge sorted indices
   const float4* nrm;
   int32_t* acc;
+  // per-substep caches written by the hash pass (same float operations as
+  // the reference performs per candidate, done once per element)
+  const int4* vcell;    // floor(p / cell) per vertex
+  const float* mlen;    // |p - x| per vertex
+  const int4* ecell;    // floor(midpoint / cell) per edge
+  const float4* eamin;  // min of both endpoints' p and x per edge
+  const float4* eamax;
+  // candidate records in hash-sorted order (slot k of the sorted arrays)
+  const float4* vs_p;   // p, thickness of vertex srt[k]
+  const int4* vs_c;     // cell, index of vertex srt[k]
+  const int4* es_c;     // cell, index of edge esrt[k]
+  const uint2* es_v;    // endpoints of edge esrt[k]
+  const float4* es_lo;  // swept AABB of edge esrt[k]
+  const float4* es_hi;
 };
+
+// A vertex's sorted two-hop list (and rest lengths), in shared memory when it
+// fits, else in global memory; binary search as in
+// shaders/self_collision.wgsl:243-293.
+struct TwoHop {
+  const uint32_t* idx;
+  const float* rest;
+  uint32_t n;
+};
+__device__ __forceinline__ bool th_find(const TwoHop& t, uint32_t b, uint32_t& pos) {
+  uint32_t lo = 0, hi = t.n;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2u;
+    const uint32_t v = t.idx[mid];
+    if (v == b) { pos = mid; return true; }
+    if (v < b) lo = mid + 1u; else hi = mid;
+  }
+  return false;
+}
+__device__ __forceinline__ bool within2_t(const TwoHop& t, uint32_t a, uint32_t b) {
+  uint32_t q;
+  if (a == b) return true;
+  return th_find(t, b, q);
+}
+__device__ __forceinline__ bool near_folded_t(const TwoHop& t, uint32_t a, uint32_t b, float d) {
+  uint32_t q;
+  if (a == b) return true;
+  if (!th_find(t, b, q)) return false;
+  return !(d < t.rest[q] * 0.5f);
+}
+__device__ __forceinline__ bool near_folded_sq_t(const TwoHop& t, uint32_t a, uint32_t b, float d2) {
+  uint32_t q;
+  if (a == b) return true;
+  if (!th_find(t, b, q)) return false;
+  const float l0 = t.rest[q];
+  return !(d2 < (l0 * l0) * 0.25f);
+}
+constexpr uint32_t kTwoHopCache = 64;
+constexpr uint32_t kRounds = 4;  // candidates per warp chunk = 32 * kRounds
+// Stage vertex v's two-hop list in shared memory (whole warp participates).
+__device__ __forceinline__ TwoHop stage_two_hop(const uint32_t* th_off, const uint32_t* th_idx, const float* th_rest,
+                                               uint32_t v, uint32_t* sh_idx, float* sh_rest, int lane) {
+  const uint32_t b = th_off[v], e = th_off[v + 1];
+  TwoHop t;
+  t.n = e - b;
+  if (t.n <= kTwoHopCache) {
+    for (uint32_t k = lane; k < t.n; k += 32u) {
+      sh_idx[k] = th_idx[b + k];
+      sh_rest[k] = th_rest[b + k];
+    }
+    __syncwarp();
+    t.idx = sh_idx;
+    t.rest = sh_rest;
+  } else {
+    t.idx = th_idx + b;
+    t.rest = th_rest + b;
+  }
+  return t;
+}
 
 __device__ __forceinline__ uint32_t layer_of(const float4* v4, uint32_t i) { return __float_as_uint(v4[i].w); }
 
@@ -68,18 +141,27 @@ __global__ void k_normals(uint32_t n, const float4* __restrict__ x4, const uint3
 // ---------------- spatial hash (spatial_hash.rs:158-247, spatial_grid_sort*.wgsl)
 // which == 0: key of vertex i is its predicted position; which == 1: key of
 // edge i is the midpoint of its two predicted endpoints.
-__global__ void k_hash_count(uint32_t cnt, int which, const float4* __restrict__ p4, const uint2* __restrict__ edges,
-                             float cell, uint32_t table, uint32_t* __restrict__ keys, uint32_t* __restrict__ counts) {
+__global__ void k_hash_count(uint32_t cnt, int which, const float4* __restrict__ x4, const float4* __restrict__ p4,
+                             const uint2* __restrict__ edges, float cell, uint32_t table, uint32_t* __restrict__ keys,
+                             uint32_t* __restrict__ counts, int4* __restrict__ cells, float* __restrict__ mlen,
+                             float4* __restrict__ amin, float4* __restrict__ amax) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= cnt) return;
   V3 q;
   if (which == 0) {
     q = mk(p4[i]);
+    mlen[i] = length(q - mk(x4[i]));
   } else {
     const uint2 e = edges[i];
-    q = (mk(p4[e.x]) + mk(p4[e.y])) * 0.5f;
+    const V3 p0 = mk(p4[e.x]), p1 = mk(p4[e.y]);
+    q = (p0 + p1) * 0.5f;
+    const V3 lo = vmin(vmin(p0, p1), vmin(mk(x4[e.x]), mk(x4[e.y])));
+    const V3 hi = vmax(vmax(p0, p1), vmax(mk(x4[e.x]), mk(x4[e.y])));
+    amin[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    amax[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
   }
   const I3 c = cell_of(q, cell);
+  cells[i] = make_int4(c.x, c.y, c.z, 0);
   const uint32_t h = hash3(c.x, c.y, c.z, table);
   keys[i] = h;
   // warp-aggregated increment: lanes with the same bucket share one atomic
@@ -131,6 +213,31 @@ __global__ void k_hash_scatter(uint32_t cnt, const uint32_t* __restrict__ keys, 
   if (i >= cnt) return;
   const uint32_t h = keys[i];
   sorted[starts[h] + atomicAdd(&cursor[h], 1u)] = i;
+}
+
+// Candidate records in sorted order, so a warp scanning one bucket reads
+// consecutive slots instead of chasing sorted index -> element -> data.
+__global__ void k_gather_vertices(uint32_t n, const uint32_t* __restrict__ srt, const float4* __restrict__ p4,
+                                  const int4* __restrict__ vcell, float4* __restrict__ vs_p, int4* __restrict__ vs_c) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t j = srt[k];
+  vs_p[k] = p4[j];
+  const int4 c = vcell[j];
+  vs_c[k] = make_int4(c.x, c.y, c.z, (int)j);
+}
+__global__ void k_gather_edges(uint32_t ne, const uint32_t* __restrict__ esrt, const uint2* __restrict__ edges,
+                               const int4* __restrict__ ecell, const float4* __restrict__ amin,
+                               const float4* __restrict__ amax, int4* __restrict__ es_c, uint2* __restrict__ es_v,
+                               float4* __restrict__ es_lo, float4* __restrict__ es_hi) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ne) return;
+  const uint32_t e = esrt[k];
+  const int4 c = ecell[e];
+  es_c[k] = make_int4(c.x, c.y, c.z, (int)e);
+  es_v[k] = edges[e];
+  es_lo[k] = amin[e];
+  es_hi[k] = amax[e];
 }
 
 // canonical in-bucket order: ascending index (insertion sort; buckets are small)
@@ -228,24 +335,23 @@ struct VertCtx {
   bool untangle, track;
 };
 
-__device__ __forceinline__ void sc_candidate(const SCArgs& s, const VertCtx& c, uint32_t j, int32_t cx, int32_t cy,
-                                             int32_t cz, uint32_t t, float& best_in, uint32_t& best_j,
-                                             uint32_t& best_t) {
+// Cheap tests of one candidate (shaders/self_collision.wgsl:356-391): bucket
+// cell match, untangle-candidate tracking, and the geometric bound; true when
+// the contact work must run.
+__device__ __forceinline__ bool sc_filter(const SCArgs& s, const VertCtx& c, const TwoHop& th, uint32_t slot,
+                                          int32_t cx, int32_t cy, int32_t cz, uint32_t t, float& best_in,
+                                          uint32_t& best_j, uint32_t& best_t) {
   const uint32_t index = c.index;
-  if (j >= s.n || j == index) return;
-  const float wi = c.wi;
-  const bool pin_i = c.pin_i;
-  const V3 xi = c.xi, pi = c.pi;
-  const float mli = c.mli, thi = c.thi, lli = c.lli;
-  const I3 cell = c.cell;
+  const int4 jc = s.vs_c[slot];
+  const uint32_t j = (uint32_t)jc.w;
+  if (j >= s.n || j == index) return false;
+  const V3 pi = c.pi;
+  const float thi = c.thi, lli = c.lli;
   const uint32_t li = c.li;
-  const bool untangle = c.untangle, track = c.track;
-  const float cs = s.cell;
-  int32_t* acc = s.acc;
-  const float4 pj4 = s.p4[j];
+  const bool track = c.track;
+  const float4 pj4 = s.vs_p[slot];
   const V3 pj = mk(pj4);
-  const I3 jc = cell_of(pj, cs);
-  if (!(jc.x == cx && jc.y == cy && jc.z == cz)) return;
+  if (!(jc.x == cx && jc.y == cy && jc.z == cz)) return false;
   const V3 dvv = pi - pj;
   const float d2 = dot(dvv, dvv);
   const float thj = pj4.w, llj = s.local_len[j];
@@ -254,11 +360,34 @@ __device__ __forceinline__ void sc_candidate(const SCArgs& s, const VertCtx& c, 
   const uint32_t lj = layer_of(s.v4, j);
   if (track && lj < li && d2 < best_in) {
     const float ur = eth * 2.5f + llj * 1.3f;
-    if (d2 <= ur * ur && !within2(s, index, j)) { best_in = d2; best_j = j; best_t = t; }
+    if (d2 <= ur * ur && !within2_t(th, index, j)) { best_in = d2; best_j = j; best_t = t; }
   }
-  if (!(d2 <= mgd * mgd)) return;
+  return d2 <= mgd * mgd;
+}
+
+// Contact work for one candidate that passed sc_filter
+// (shaders/self_collision.wgsl:392-670).
+__device__ __forceinline__ void sc_work(const SCArgs& s, const VertCtx& c, const TwoHop& th, uint32_t slot) {
+  const uint32_t index = c.index;
+  const int4 jc = s.vs_c[slot];
+  const uint32_t j = (uint32_t)jc.w;
+  const float wi = c.wi;
+  const bool pin_i = c.pin_i;
+  const V3 xi = c.xi, pi = c.pi;
+  const float mli = c.mli, thi = c.thi, lli = c.lli;
+  const I3 cell = c.cell;
+  const uint32_t li = c.li;
+  const bool untangle = c.untangle;
+  int32_t* acc = s.acc;
+  const float4 pj4 = s.vs_p[slot];
+  const V3 pj = mk(pj4);
+  const V3 dvv = pi - pj;
+  const float d2 = dot(dvv, dvv);
+  const float thj = pj4.w, llj = s.local_len[j];
+  const float eth = fmaxf(thi + thj, fminf(lli, llj) * 0.06f);
+  const uint32_t lj = layer_of(s.v4, j);
   const float dvl = sqrtf(fmaxf(d2, 0.0f));
-  if (near_folded(s, index, j, dvl)) return;
+  if (near_folded_t(th, index, j, dvl)) return;
   const float4 xj4 = s.x4[j];
   const V3 pjo = mk(xj4);
   const float wj = xj4.w;
@@ -300,9 +429,9 @@ __device__ __forceinline__ void sc_candidate(const SCArgs& s, const VertCtx& c, 
     }
   }
   // 2. vertex-triangle
-  const float mlj = length(pj - pjo);
+  const float mlj = s.mlen[j];
   const float vtb = eth + llj * 1.3f + mli + mlj;
-  if (!(d2 <= vtb * vtb) || within2(s, index, j)) return;
+  if (!(d2 <= vtb * vtb) || within2_t(th, index, j)) return;
   for (uint32_t st = s.star_off[j]; st < s.star_off[j + 1]; ++st) {
     const uint2 pr = s.star_idx[st];
     const uint32_t v0 = pr.x, v1 = pr.y;
@@ -314,15 +443,15 @@ __device__ __forceinline__ void sc_candidate(const SCArgs& s, const VertCtx& c, 
     const V3 d0 = pi - pv0;
     const float ll0 = s.local_len[v0];
     const float et0 = fmaxf(thi + q0.w, fminf(lli, ll0) * 0.06f);
-    const float b0 = et0 + ll0 * 1.3f + mli + length(pv0 - pv0o);
-    const I3 c0 = cell_of(pv0, cs);
+    const float b0 = et0 + ll0 * 1.3f + mli + s.mlen[v0];
+    const int4 c0 = s.vcell[v0];
     const bool in0 = abs(c0.x - cell.x) <= 1 && abs(c0.y - cell.y) <= 1 && abs(c0.z - cell.z) <= 1 &&
                      (dot(d0, d0) <= b0 * b0);
     const V3 d1 = pi - pv1;
     const float ll1 = s.local_len[v1];
     const float et1 = fmaxf(thi + q1.w, fminf(lli, ll1) * 0.06f);
-    const float b1 = et1 + ll1 * 1.3f + mli + length(pv1 - pv1o);
-    const I3 c1 = cell_of(pv1, cs);
+    const float b1 = et1 + ll1 * 1.3f + mli + s.mlen[v1];
+    const int4 c1 = s.vcell[v1];
     const bool in1 = abs(c1.x - cell.x) <= 1 && abs(c1.y - cell.y) <= 1 && abs(c1.z - cell.z) <= 1 &&
                      (dot(d1, d1) <= b1 * b1);
     if ((in0 && j > v0) || (in1 && j > v1)) continue;
@@ -335,7 +464,7 @@ __device__ __forceinline__ void sc_candidate(const SCArgs& s, const VertCtx& c, 
     if (smin.x > tmax.x || smin.y > tmax.y || smin.z > tmax.z || smax.x < tmin.x || smax.y < tmin.y ||
         smax.z < tmin.z)
       continue;
-    if (within2(s, index, v0) || within2(s, index, v1)) continue;
+    if (within2_t(th, index, v0) || within2_t(th, index, v1)) continue;
     const V3 mv = pi - rel;
     const float msq = dot(mv, mv);
     float ht = 1.0f, hu = 0.0f, hv = 0.0f;
@@ -438,6 +567,9 @@ __device__ __forceinline__ void sc_candidate(const SCArgs& s, const VertCtx& c, 
 
 __global__ void __launch_bounds__(256) k_sc_solve(SCArgs s) {
   __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
+  __shared__ uint32_t sh_th[8][kTwoHopCache];
+  __shared__ float sh_thr[8][kTwoHopCache];
+  __shared__ uint32_t sh_q[8][32 * kRounds];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t index = blockIdx.x * 8u + warp;
   if (index >= s.n) return;  // whole warp
@@ -448,11 +580,15 @@ __global__ void __launch_bounds__(256) k_sc_solve(SCArgs s) {
   c.pin_i = c.wi <= 0.0f;
   c.xi = mk(xi4);
   c.pi = mk(pi4);
-  c.mli = length(c.pi - c.xi);
+  c.mli = s.mlen[index];
   if (c.pin_i && c.mli < kEps) return;  // whole warp
+  const TwoHop th = stage_two_hop(s.th_off, s.th_idx, s.th_rest, index, sh_th[warp], sh_thr[warp], lane);
   c.thi = pi4.w;
   c.lli = s.local_len[index];
-  c.cell = cell_of(c.pi, s.cell);
+  {
+    const int4 vc = s.vcell[index];
+    c.cell = I3{vc.x, vc.y, vc.z};
+  }
   c.li = layer_of(s.v4, index);
   c.untangle = s.untangle != 0;
   c.track = c.untangle && !c.pin_i && c.li > 0u;
@@ -478,11 +614,29 @@ __global__ void __launch_bounds__(256) k_sc_solve(SCArgs s) {
   float best_in = 1e20f;
   uint32_t best_j = 0xFFFFFFFFu, best_t = 0xFFFFFFFFu;
   int k = 0;
-  for (uint32_t t = lane; t < total; t += 32u) {
-    while (t >= sh_end[warp][k]) ++k;
-    const uint32_t j = s.srt[sh_beg[warp][k] + (t - sh_start[warp][k])];
-    sc_candidate(s, c, j, c.cell.x - 1 + k / 9, c.cell.y - 1 + (k / 3) % 3, c.cell.z - 1 + k % 3, t, best_in, best_j,
-                 best_t);
+  uint32_t* queue = sh_q[warp];
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  for (uint32_t chunk = 0; chunk < total; chunk += 32u * kRounds) {
+    // phase 1: cheap filters on 32 x kRounds candidates, survivors compacted
+    uint32_t qn = 0;
+    for (uint32_t r = 0; r < kRounds; ++r) {
+      const uint32_t t = chunk + r * 32u + lane;
+      bool pass = false;
+      uint32_t slot = 0;
+      if (t < total) {
+        while (t >= sh_end[warp][k]) ++k;
+        slot = sh_beg[warp][k] + (t - sh_start[warp][k]);
+        pass = sc_filter(s, c, th, slot, c.cell.x - 1 + k / 9, c.cell.y - 1 + (k / 3) % 3, c.cell.z - 1 + k % 3, t,
+                         best_in, best_j, best_t);
+      }
+      const uint32_t b = __ballot_sync(0xffffffffu, pass);
+      if (pass) queue[qn + __popc(b & lt_mask)] = slot;
+      qn += __popc(b);
+    }
+    __syncwarp();
+    // phase 2: contact work on the survivors, all lanes busy
+    for (uint32_t q = lane; q < qn; q += 32u) sc_work(s, c, th, queue[q]);
+    __syncwarp();
   }
   if (c.track) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -670,8 +824,9 @@ struct EdgeCtx {
 };
 
 // Contact work for one counted edge pair (shaders/self_collision_ee_direct.wgsl:356-774).
-__device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, uint32_t eb, uint32_t j, uint32_t vj,
-                                        const float4& qj, const float4& qvj, const float4& xj, const float4& xvj) {
+__device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, const TwoHop& th0, const TwoHop& th1,
+                                        uint32_t eb, uint32_t j, uint32_t vj, const float4& qj, const float4& qvj,
+                                        const float4& xj, const float4& xvj) {
   const uint32_t u0 = c.u0, u1 = c.u1;
   const float w_u0 = c.w_u0, w_u1 = c.w_u1;
   const bool apin = c.apin, bnda = c.bnda;
@@ -742,8 +897,8 @@ __device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, uint3
       const V3 a0s = vmix(p_u0o, p_u0, tstar), a1s = vmix(p_u1o, p_u1, tstar);
       const V3 b0s = vmix(p_jo, p_j, tstar), b1s = vmix(p_vjo, p_vj, tstar);
       const V3 t0 = a0s - b0s, t1v = a0s - b1s, t2 = a1s - b0s, t3 = a1s - b1s;
-      if (near_folded_sq(s, u0, j, dot(t0, t0)) || near_folded_sq(s, u0, vj, dot(t1v, t1v)) ||
-          near_folded_sq(s, u1, j, dot(t2, t2)) || near_folded_sq(s, u1, vj, dot(t3, t3)))
+      if (near_folded_sq_t(th0, u0, j, dot(t0, t0)) || near_folded_sq_t(th0, u0, vj, dot(t1v, t1v)) ||
+          near_folded_sq_t(th1, u1, j, dot(t2, t2)) || near_folded_sq_t(th1, u1, vj, dot(t3, t3)))
         return;
     }
     bool utc = false;
@@ -832,8 +987,8 @@ __device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, uint3
     if (d2e >= eth * eth || d2e <= kEps * kEps) return;
     if (s.exclude_neighbors) {
       const V3 e0 = p_u0 - p_j, e1 = p_u0 - p_vj, e2 = p_u1 - p_j, e3 = p_u1 - p_vj;
-      if (near_folded_sq(s, u0, j, dot(e0, e0)) || near_folded_sq(s, u0, vj, dot(e1, e1)) ||
-          near_folded_sq(s, u1, j, dot(e2, e2)) || near_folded_sq(s, u1, vj, dot(e3, e3)))
+      if (near_folded_sq_t(th0, u0, j, dot(e0, e0)) || near_folded_sq_t(th0, u0, vj, dot(e1, e1)) ||
+          near_folded_sq_t(th1, u1, j, dot(e2, e2)) || near_folded_sq_t(th1, u1, vj, dot(e3, e3)))
         return;
     }
     const float del = sqrtf(d2e);
@@ -889,6 +1044,9 @@ __device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, uint3
 // exactly the reference's first max_search counted pairs are processed.
 __global__ void __launch_bounds__(256) k_ee(SCArgs s) {
   __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
+  __shared__ uint32_t sh_th[8][2][kTwoHopCache];
+  __shared__ float sh_thr[8][2][kTwoHopCache];
+  __shared__ uint32_t sh_q[8][32 * kRounds];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t ei = blockIdx.x * 8u + warp;
   if (ei >= s.ne) return;  // whole warp
@@ -909,8 +1067,11 @@ __global__ void __launch_bounds__(256) k_ee(SCArgs s) {
   const V3 m2 = mk(c.mta * 2.0f, c.mta * 2.0f, c.mta * 2.0f);
   c.amin = vmin(vmin(c.p_u0, c.p_u1), vmin(c.p_u0o, c.p_u1o)) - m2;
   c.amax = vmax(vmax(c.p_u0, c.p_u1), vmax(c.p_u0o, c.p_u1o)) + m2;
-  const I3 base = cell_of((c.p_u0 + c.p_u1) * 0.5f, s.cell);
+  const int4 bc4 = s.ecell[ei];
+  const I3 base = I3{bc4.x, bc4.y, bc4.z};
   c.la = layer_of(s.v4, c.u0);
+  const TwoHop th0 = stage_two_hop(s.th_off, s.th_idx, s.th_rest, c.u0, sh_th[warp][0], sh_thr[warp][0], lane);
+  const TwoHop th1 = stage_two_hop(s.th_off, s.th_idx, s.th_rest, c.u1, sh_th[warp][1], sh_thr[warp][1], lane);
   c.untangle = s.untangle != 0;
   // lane k = (dz+1)*9 + (dy+1)*3 + (dx+1)
   uint32_t cnt = 0, beg = 0;
@@ -934,38 +1095,47 @@ __global__ void __launch_bounds__(256) k_ee(SCArgs s) {
   const uint32_t total = __shfl_sync(0xffffffffu, incl, 26);
   uint32_t counted = 0;
   int k = 0;
-  for (uint32_t base_t = 0; base_t < total && counted < s.max_search; base_t += 32u) {
-    const uint32_t t = base_t + lane;
-    bool pass = false;
-    uint32_t eb = 0, j = 0, vj = 0;
-    float4 qj, qvj, xj, xvj;
-    if (t < total) {
-      while (t >= sh_end[warp][k]) ++k;
-      eb = s.esrt[sh_beg[warp][k] + (t - sh_start[warp][k])];
-      if (ei < eb) {
-        const uint2 ebv = s.edges[eb];
-        j = ebv.x;
-        vj = ebv.y;
-        if (!(j == c.u0 || j == c.u1 || vj == c.u0 || vj == c.u1)) {
-          qj = s.p4[j];
-          qvj = s.p4[vj];
-          const I3 bc = cell_of((mk(qj) + mk(qvj)) * 0.5f, s.cell);
-          if (bc.x == base.x - 1 + k % 3 && bc.y == base.y - 1 + (k / 3) % 3 && bc.z == base.z - 1 + k / 9) {
-            xj = s.x4[j];
-            xvj = s.x4[vj];
-            const V3 p_j = mk(qj), p_vj = mk(qvj), p_jo = mk(xj), p_vjo = mk(xvj);
-            const V3 bmin = vmin(vmin(p_j, p_vj), vmin(p_jo, p_vjo));
-            const V3 bmax = vmax(vmax(p_j, p_vj), vmax(p_jo, p_vjo));
+  uint32_t* queue = sh_q[warp];
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  for (uint32_t chunk = 0; chunk < total && counted < s.max_search; chunk += 32u * kRounds) {
+    // phase 1: counting filter; the first max_search counted pairs are queued
+    uint32_t qn = 0;
+    for (uint32_t r = 0; r < kRounds; ++r) {
+      const uint32_t t = chunk + r * 32u + lane;
+      bool pass = false;
+      uint32_t slot = 0;
+      if (t < total) {
+        while (t >= sh_end[warp][k]) ++k;
+        slot = sh_beg[warp][k] + (t - sh_start[warp][k]);
+        const int4 bc = s.es_c[slot];
+        const uint32_t eb = (uint32_t)bc.w;
+        if (ei < eb) {
+          const uint2 ebv = s.es_v[slot];
+          if (!(ebv.x == c.u0 || ebv.x == c.u1 || ebv.y == c.u0 || ebv.y == c.u1) &&
+              bc.x == base.x - 1 + k % 3 && bc.y == base.y - 1 + (k / 3) % 3 && bc.z == base.z - 1 + k / 9) {
+            const float4 bmin = s.es_lo[slot], bmax = s.es_hi[slot];
             pass = !(c.amin.x > bmax.x || c.amin.y > bmax.y || c.amin.z > bmax.z || c.amax.x < bmin.x ||
                      c.amax.y < bmin.y || c.amax.z < bmin.z);
           }
         }
       }
+      const uint32_t b = __ballot_sync(0xffffffffu, pass);
+      const uint32_t rank = counted + __popc(b & lt_mask);
+      if (pass && rank < s.max_search) queue[qn + __popc(b & lt_mask)] = slot;
+      const uint32_t nb = __popc(b);
+      qn += counted + nb <= s.max_search ? nb : (counted < s.max_search ? s.max_search - counted : 0u);
+      counted += nb;
     }
-    const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
-    const uint32_t rank = counted + __popc(ballot & ((1u << lane) - 1u));
-    counted += __popc(ballot);
-    if (pass && rank < s.max_search) ee_pair(s, c, eb, j, vj, qj, qvj, xj, xvj);
+    __syncwarp();
+    // phase 2: contact work on the queued pairs
+    for (uint32_t q = lane; q < qn; q += 32u) {
+      const uint32_t slot = queue[q];
+      const uint32_t eb = (uint32_t)s.es_c[slot].w;
+      const uint2 ebv = s.es_v[slot];
+      const float4 qj = s.p4[ebv.x], qvj = s.p4[ebv.y], xj = s.x4[ebv.x], xvj = s.x4[ebv.y];
+      ee_pair(s, c, th0, th1, eb, ebv.x, ebv.y, qj, qvj, xj, xvj);
+    }
+    __syncwarp();
   }
 }
 
