@@ -55,6 +55,7 @@ struct SCArgs {
   // candidate records in hash-sorted order (slot k of the sorted arrays)
   const float4* vs_p;   // p, thickness of vertex srt[k]
   const int4* vs_c;     // cell, index of vertex srt[k]
+  const float4* vs_q;   // local edge length, layer bits, inverse mass, |p - x| of vertex srt[k]
   const int4* es_c;     // cell, index of edge esrt[k]
   const uint2* es_v;    // endpoints of edge esrt[k]
   const float4* es_lo;  // swept AABB of edge esrt[k]
@@ -172,39 +173,56 @@ __global__ void k_hash_count(uint32_t cnt, int which, const float4* __restrict__
   if (lane == leader) atomicAdd(&counts[h], __popc(peers));
 }
 
-// exclusive scan of counts[table] into starts[table + 1]; one block of 1024
-// threads, each owning a contiguous chunk, warp-shuffle scans of chunk sums.
-__global__ void k_hash_scan(uint32_t table, const uint32_t* __restrict__ counts, uint32_t* __restrict__ starts) {
-  __shared__ uint32_t warp_tot[32];
-  const uint32_t tid = threadIdx.x;
-  const uint32_t per = (table + blockDim.x - 1) / blockDim.x;
-  const uint32_t b = tid * per, e = min(b + per, table);
-  uint32_t local = 0;
-  for (uint32_t k = b; k < e; ++k) local += counts[k];
-  // inclusive warp scan
-  uint32_t v = local;
-  const int lane = tid & 31, wid = tid >> 5;
+// Exclusive scan of counts[table] into starts[table + 1] in two launches:
+// k_scan_blocks scans 1024-entry tiles (coalesced loads, warp-shuffle scans)
+// and writes tile totals; k_scan_finish adds the scanned tile totals.
+__device__ __forceinline__ uint32_t block_incl_scan_1024(uint32_t v, uint32_t* warp_tot, uint32_t& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+    const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
     if (lane >= o) v += t;
   }
   if (lane == 31) warp_tot[wid] = v;
   __syncthreads();
   if (wid == 0) {
-    uint32_t w = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0u;
+    uint32_t w = warp_tot[lane];
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+      const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
       if (lane >= o) w += t;
     }
     warp_tot[lane] = w;
   }
   __syncthreads();
-  uint32_t base = (wid > 0 ? warp_tot[wid - 1] : 0u) + v - local;
-  for (uint32_t k = b; k < e; ++k) {
-    starts[k] = base;
-    base += counts[k];
+  total = warp_tot[31];
+  return v + (wid > 0 ? warp_tot[wid - 1] : 0u);
+}
+__global__ void __launch_bounds__(1024) k_scan_blocks(uint32_t table, const uint32_t* __restrict__ counts,
+                                                      uint32_t* __restrict__ starts, uint32_t* __restrict__ tile_sum) {
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t i = blockIdx.x * 1024u + threadIdx.x;
+  const uint32_t c = i < table ? counts[i] : 0u;
+  uint32_t total;
+  const uint32_t incl = block_incl_scan_1024(c, warp_tot, total);
+  if (i < table) starts[i] = incl - c;
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+__global__ void __launch_bounds__(1024) k_scan_finish(uint32_t table, uint32_t ntiles, const uint32_t* __restrict__ tile_sum,
+                                                      uint32_t* __restrict__ starts) {
+  __shared__ uint32_t tile_off[64];
+  if (threadIdx.x < 64) {
+    // ntiles <= 64 (table <= 65536): scan of tile sums by the first warp pair
+    uint32_t v = threadIdx.x < ntiles ? tile_sum[threadIdx.x] : 0u;
+    tile_off[threadIdx.x] = v;
   }
-  if (tid == blockDim.x - 1) starts[table] = warp_tot[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t t = 0; t < ntiles; ++t) { const uint32_t v = tile_off[t]; tile_off[t] = acc; acc += v; }
+    starts[table] = acc;
+  }
+  __syncthreads();
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < table; i += gridDim.x * blockDim.x)
+    starts[i] += tile_off[i >> 10];
 }
 
 __global__ void k_hash_scatter(uint32_t cnt, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ starts,
@@ -217,14 +235,18 @@ __global__ void k_hash_scatter(uint32_t cnt, const uint32_t* __restrict__ keys, 
 
 // Candidate records in sorted order, so a warp scanning one bucket reads
 // consecutive slots instead of chasing sorted index -> element -> data.
-__global__ void k_gather_vertices(uint32_t n, const uint32_t* __restrict__ srt, const float4* __restrict__ p4,
-                                  const int4* __restrict__ vcell, float4* __restrict__ vs_p, int4* __restrict__ vs_c) {
+__global__ void k_gather_vertices(uint32_t n, const uint32_t* __restrict__ srt, const float4* __restrict__ x4,
+                                  const float4* __restrict__ p4, const float4* __restrict__ v4,
+                                  const float* __restrict__ local_len, const float* __restrict__ mlen,
+                                  const int4* __restrict__ vcell, float4* __restrict__ vs_p, int4* __restrict__ vs_c,
+                                  float4* __restrict__ vs_q) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const uint32_t j = srt[k];
   vs_p[k] = p4[j];
   const int4 c = vcell[j];
   vs_c[k] = make_int4(c.x, c.y, c.z, (int)j);
+  vs_q[k] = make_float4(local_len[j], v4[j].w, x4[j].w, mlen[j]);
 }
 __global__ void k_gather_edges(uint32_t ne, const uint32_t* __restrict__ esrt, const uint2* __restrict__ edges,
                                const int4* __restrict__ ecell, const float4* __restrict__ amin,
@@ -240,18 +262,32 @@ __global__ void k_gather_edges(uint32_t ne, const uint32_t* __restrict__ esrt, c
   es_hi[k] = amax[e];
 }
 
-// canonical in-bucket order: ascending index (insertion sort; buckets are small)
+// Canonical in-bucket order: ascending index.  Buckets hold a few to a few
+// dozen entries; each thread sorts one bucket in a local array (registers /
+// L1) and writes it back; larger buckets fall back to in-place insertion.
 __global__ void k_hash_sort_buckets(uint32_t table, const uint32_t* __restrict__ starts, uint32_t* __restrict__ sorted) {
-  uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= table) return;
   const uint32_t b = starts[h], e = starts[h + 1];
-  for (uint32_t k = b + 1; k < e; ++k) {
-    uint32_t v = sorted[k];
-    uint32_t j = k;
-    while (j > b && sorted[j - 1] > v) {
-      sorted[j] = sorted[j - 1];
-      --j;
+  const uint32_t n = e - b;
+  if (n < 2) return;
+  constexpr uint32_t kLocal = 64;
+  if (n <= kLocal) {
+    uint32_t a[kLocal];
+    for (uint32_t k = 0; k < n; ++k) a[k] = sorted[b + k];
+    for (uint32_t k = 1; k < n; ++k) {
+      const uint32_t v = a[k];
+      uint32_t j = k;
+      while (j > 0 && a[j - 1] > v) { a[j] = a[j - 1]; --j; }
+      a[j] = v;
     }
+    for (uint32_t k = 0; k < n; ++k) sorted[b + k] = a[k];
+    return;
+  }
+  for (uint32_t k = b + 1; k < e; ++k) {
+    const uint32_t v = sorted[k];
+    uint32_t j = k;
+    while (j > b && sorted[j - 1] > v) { sorted[j] = sorted[j - 1]; --j; }
     sorted[j] = v;
   }
 }
@@ -342,22 +378,24 @@ __device__ __forceinline__ bool sc_filter(const SCArgs& s, const VertCtx& c, con
                                           int32_t cx, int32_t cy, int32_t cz, uint32_t t, float& best_in,
                                           uint32_t& best_j, uint32_t& best_t) {
   const uint32_t index = c.index;
+  // one level of loads: the three hash-ordered records of this slot
   const int4 jc = s.vs_c[slot];
+  const float4 pj4 = s.vs_p[slot];
+  const float4 q = s.vs_q[slot];
   const uint32_t j = (uint32_t)jc.w;
   if (j >= s.n || j == index) return false;
   const V3 pi = c.pi;
   const float thi = c.thi, lli = c.lli;
   const uint32_t li = c.li;
   const bool track = c.track;
-  const float4 pj4 = s.vs_p[slot];
   const V3 pj = mk(pj4);
   if (!(jc.x == cx && jc.y == cy && jc.z == cz)) return false;
   const V3 dvv = pi - pj;
   const float d2 = dot(dvv, dvv);
-  const float thj = pj4.w, llj = s.local_len[j];
+  const float thj = pj4.w, llj = q.x;
   const float eth = fmaxf(thi + thj, fminf(lli, llj) * 0.06f);
   const float mgd = eth + (lli + llj) * 1.3f;
-  const uint32_t lj = layer_of(s.v4, j);
+  const uint32_t lj = __float_as_uint(q.y);
   if (track && lj < li && d2 < best_in) {
     const float ur = eth * 2.5f + llj * 1.3f;
     if (d2 <= ur * ur && !within2_t(th, index, j)) { best_in = d2; best_j = j; best_t = t; }
@@ -380,17 +418,17 @@ __device__ __forceinline__ void sc_work(const SCArgs& s, const VertCtx& c, const
   const bool untangle = c.untangle;
   int32_t* acc = s.acc;
   const float4 pj4 = s.vs_p[slot];
+  const float4 q = s.vs_q[slot];
   const V3 pj = mk(pj4);
   const V3 dvv = pi - pj;
   const float d2 = dot(dvv, dvv);
-  const float thj = pj4.w, llj = s.local_len[j];
+  const float thj = pj4.w, llj = q.x;
   const float eth = fmaxf(thi + thj, fminf(lli, llj) * 0.06f);
-  const uint32_t lj = layer_of(s.v4, j);
+  const uint32_t lj = __float_as_uint(q.y);
   const float dvl = sqrtf(fmaxf(d2, 0.0f));
   if (near_folded_t(th, index, j, dvl)) return;
-  const float4 xj4 = s.x4[j];
-  const V3 pjo = mk(xj4);
-  const float wj = xj4.w;
+  const V3 pjo = mk(s.x4[j]);
+  const float wj = q.z;
   const bool both = wj > 0.0f;
   const float eth2 = eth * eth;
   // 1. vertex-vertex
@@ -429,7 +467,7 @@ __device__ __forceinline__ void sc_work(const SCArgs& s, const VertCtx& c, const
     }
   }
   // 2. vertex-triangle
-  const float mlj = s.mlen[j];
+  const float mlj = q.w;
   const float vtb = eth + llj * 1.3f + mli + mlj;
   if (!(d2 <= vtb * vtb) || within2_t(th, index, j)) return;
   for (uint32_t st = s.star_off[j]; st < s.star_off[j + 1]; ++st) {
@@ -565,7 +603,7 @@ __device__ __forceinline__ void sc_work(const SCArgs& s, const VertCtx& c, const
   }
 }
 
-__global__ void __launch_bounds__(256) k_sc_solve(SCArgs s) {
+__global__ void __launch_bounds__(256, 4) k_sc_solve(SCArgs s) {
   __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
   __shared__ uint32_t sh_th[8][kTwoHopCache];
   __shared__ float sh_thr[8][kTwoHopCache];
@@ -1042,7 +1080,7 @@ __device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, const
 // round.  The per-edge cap on counted candidates (search_count >
 // max_search_iterations, :356-359) is applied with a ballot prefix count, so
 // exactly the reference's first max_search counted pairs are processed.
-__global__ void __launch_bounds__(256) k_ee(SCArgs s) {
+__global__ void __launch_bounds__(256, 3) k_ee(SCArgs s) {
   __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
   __shared__ uint32_t sh_th[8][2][kTwoHopCache];
   __shared__ float sh_thr[8][2][kTwoHopCache];
@@ -1107,17 +1145,15 @@ __global__ void __launch_bounds__(256) k_ee(SCArgs s) {
       if (t < total) {
         while (t >= sh_end[warp][k]) ++k;
         slot = sh_beg[warp][k] + (t - sh_start[warp][k]);
+        // one level of loads for the whole filter
         const int4 bc = s.es_c[slot];
+        const uint2 ebv = s.es_v[slot];
+        const float4 bmin = s.es_lo[slot], bmax = s.es_hi[slot];
         const uint32_t eb = (uint32_t)bc.w;
-        if (ei < eb) {
-          const uint2 ebv = s.es_v[slot];
-          if (!(ebv.x == c.u0 || ebv.x == c.u1 || ebv.y == c.u0 || ebv.y == c.u1) &&
-              bc.x == base.x - 1 + k % 3 && bc.y == base.y - 1 + (k / 3) % 3 && bc.z == base.z - 1 + k / 9) {
-            const float4 bmin = s.es_lo[slot], bmax = s.es_hi[slot];
-            pass = !(c.amin.x > bmax.x || c.amin.y > bmax.y || c.amin.z > bmax.z || c.amax.x < bmin.x ||
-                     c.amax.y < bmin.y || c.amax.z < bmin.z);
-          }
-        }
+        pass = ei < eb && !(ebv.x == c.u0 || ebv.x == c.u1 || ebv.y == c.u0 || ebv.y == c.u1) &&
+               bc.x == base.x - 1 + k % 3 && bc.y == base.y - 1 + (k / 3) % 3 && bc.z == base.z - 1 + k / 9 &&
+               !(c.amin.x > bmax.x || c.amin.y > bmax.y || c.amin.z > bmax.z || c.amax.x < bmin.x ||
+                 c.amax.y < bmin.y || c.amax.z < bmin.z);
       }
       const uint32_t b = __ballot_sync(0xffffffffu, pass);
       const uint32_t rank = counted + __popc(b & lt_mask);

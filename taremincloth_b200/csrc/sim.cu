@@ -92,7 +92,8 @@ struct Sim {
   DBuf<int4> vcell, ecell;
   DBuf<float> mlen;
   DBuf<float4> eamin, eamax;
-  DBuf<float4> vs_p, es_lo, es_hi;
+  DBuf<float4> vs_p, vs_q, es_lo, es_hi;
+  DBuf<uint32_t> tile_sum;
   DBuf<int4> vs_c, es_c;
   DBuf<uint2> es_v;
   // colliders
@@ -273,7 +274,7 @@ struct Sim {
     nrm.alloc(n);
     acc.alloc(size_t(n) * A_N);
     vcell.alloc(n); mlen.alloc(n); ecell.alloc(ne); eamin.alloc(ne); eamax.alloc(ne);
-    vs_p.alloc(n); vs_c.alloc(n); es_c.alloc(ne); es_v.alloc(ne); es_lo.alloc(ne); es_hi.alloc(ne);
+    vs_p.alloc(n); vs_q.alloc(n); vs_c.alloc(n); tile_sum.alloc(64); es_c.alloc(ne); es_v.alloc(ne); es_lo.alloc(ne); es_hi.alloc(ne);
     TC_CK(cudaMemsetAsync(acc.p, 0, size_t(n) * A_N * sizeof(int32_t), st));
     TC_CK(cudaMemsetAsync(nrm.p, 0, size_t(n) * sizeof(float4), st));
     res_sum.alloc(m.dist_cnt.size() + m.bend_cnt.size() + 1);
@@ -420,7 +421,7 @@ struct Sim {
     a.star_off = star_off.p; a.star_idx = star_idx.p; a.edges = edges.p; a.edge_bits = edge_bits.p;
     a.cs = cs.p; a.srt = srt.p; a.ecs = ecs.p; a.esrt = esrt.p; a.nrm = nrm.p; a.acc = acc.p;
     a.vcell = vcell.p; a.mlen = mlen.p; a.ecell = ecell.p; a.eamin = eamin.p; a.eamax = eamax.p;
-    a.vs_p = vs_p.p; a.vs_c = vs_c.p; a.es_c = es_c.p; a.es_v = es_v.p; a.es_lo = es_lo.p; a.es_hi = es_hi.p;
+    a.vs_p = vs_p.p; a.vs_q = vs_q.p; a.vs_c = vs_c.p; a.es_c = es_c.p; a.es_v = es_v.p; a.es_lo = es_lo.p; a.es_hi = es_hi.p;
     return a;
   }
 
@@ -438,10 +439,14 @@ struct Sim {
       if (cnt)
         k_hash_count<<<grid(cnt, 256), 256, 0, st>>>(cnt, which, x4.p, p4.p, edges.p, m.cell, T, k, counts.p,
                                                       which == 0 ? vcell.p : ecell.p, mlen.p, eamin.p, eamax.p);
-      k_hash_scan<<<1, 1024, 0, st>>>(T, counts.p, start);
+      const uint32_t ntiles = (T + 1023) / 1024;
+      k_scan_blocks<<<ntiles, 1024, 0, st>>>(T, counts.p, start, tile_sum.p);
+      k_scan_finish<<<ntiles, 1024, 0, st>>>(T, ntiles, tile_sum.p, start);
       if (cnt) k_hash_scatter<<<grid(cnt, 256), 256, 0, st>>>(cnt, k, start, cursor.p, sorted);
       k_hash_sort_buckets<<<grid(T, 256), 256, 0, st>>>(T, start, sorted);
-      if (cnt && which == 0) k_gather_vertices<<<grid(cnt, 256), 256, 0, st>>>(cnt, sorted, p4.p, vcell.p, vs_p.p, vs_c.p);
+      if (cnt && which == 0)
+        k_gather_vertices<<<grid(cnt, 256), 256, 0, st>>>(cnt, sorted, x4.p, p4.p, v4.p, local_len.p, mlen.p, vcell.p,
+                                                           vs_p.p, vs_c.p, vs_q.p);
       if (cnt && which == 1)
         k_gather_edges<<<grid(cnt, 256), 256, 0, st>>>(cnt, sorted, edges.p, ecell.p, eamin.p, eamax.p, es_c.p, es_v.p,
                                                         es_lo.p, es_hi.p);
