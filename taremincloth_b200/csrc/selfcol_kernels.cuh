@@ -60,6 +60,10 @@ struct SCArgs {
   const uint2* es_v;    // endpoints of edge esrt[k]
   const float4* es_lo;  // swept AABB of edge esrt[k]
   const float4* es_hi;
+  // pairs that need the continuous (CCD) search are deferred to k_ee_ccd
+  uint2* ccd_q;
+  uint32_t* ccd_n;
+  uint32_t ccd_cap;
 };
 
 // A vertex's sorted two-hop list (and rest lengths), in shared memory when it
@@ -862,9 +866,11 @@ struct EdgeCtx {
 };
 
 // Contact work for one counted edge pair (shaders/self_collision_ee_direct.wgsl:356-774).
+// defer_ccd: the warp pass hands pairs that need the CCD search to the
+// one-thread-per-pair k_ee_ccd (inline when the queue is full).
 __device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, const TwoHop& th0, const TwoHop& th1,
                                         uint32_t eb, uint32_t j, uint32_t vj, const float4& qj, const float4& qvj,
-                                        const float4& xj, const float4& xvj) {
+                                        const float4& xj, const float4& xvj, bool defer_ccd) {
   const uint32_t u0 = c.u0, u1 = c.u1;
   const float w_u0 = c.w_u0, w_u1 = c.w_u1;
   const bool apin = c.apin, bnda = c.bnda;
@@ -896,6 +902,13 @@ __device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, const
     has1 = true;
     const V3 d0g = vmix(p_u0o, p_u1o, s1) - vmix(p_jo, p_vjo, t1);
     run_ccd = (rdg > ethc * 0.5f) || (dot(d0g, dl1) <= 0.0f);
+  }
+  if (run_ccd && defer_ccd) {
+    const uint32_t q = atomicAdd(s.ccd_n, 1u);
+    if (q < s.ccd_cap) {
+      s.ccd_q[q] = make_uint2(c.ei, eb);
+      return;
+    }
   }
   if (run_ccd) {
     float msd = 1e20f, btau = 0.0f, hs = 0.125f, ms = 0.f, mt = 0.f;
@@ -1075,19 +1088,7 @@ __device__ __forceinline__ void ee_pair(const SCArgs& s, const EdgeCtx& c, const
   }
 }
 
-// One warp per edge; candidates of the 27 cells around the edge midpoint are
-// flattened in the reference's order (dz outer, dx inner) and visited 32 per
-// round.  The per-edge cap on counted candidates (search_count >
-// max_search_iterations, :356-359) is applied with a ballot prefix count, so
-// exactly the reference's first max_search counted pairs are processed.
-__global__ void __launch_bounds__(256, 3) k_ee(SCArgs s) {
-  __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
-  __shared__ uint32_t sh_th[8][2][kTwoHopCache];
-  __shared__ float sh_thr[8][2][kTwoHopCache];
-  __shared__ uint32_t sh_q[8][32 * kRounds];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t ei = blockIdx.x * 8u + warp;
-  if (ei >= s.ne) return;  // whole warp
+__device__ __forceinline__ EdgeCtx edge_ctx(const SCArgs& s, uint32_t ei) {
   EdgeCtx c;
   c.ei = ei;
   const uint2 ea = s.edges[ei];
@@ -1105,18 +1106,62 @@ __global__ void __launch_bounds__(256, 3) k_ee(SCArgs s) {
   const V3 m2 = mk(c.mta * 2.0f, c.mta * 2.0f, c.mta * 2.0f);
   c.amin = vmin(vmin(c.p_u0, c.p_u1), vmin(c.p_u0o, c.p_u1o)) - m2;
   c.amax = vmax(vmax(c.p_u0, c.p_u1), vmax(c.p_u0o, c.p_u1o)) + m2;
+  c.la = layer_of(s.v4, c.u0);
+  c.untangle = s.untangle != 0;
+  return c;
+}
+
+// Deferred CCD pairs, one thread each (the CCD search plus the discrete
+// fall-through of shaders/self_collision_ee_direct.wgsl:404-774).
+__global__ void __launch_bounds__(256) k_ee_ccd(SCArgs s) {
+  const uint32_t total = min(*s.ccd_n, s.ccd_cap);
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+    const uint2 pr = s.ccd_q[q];
+    const EdgeCtx c = edge_ctx(s, pr.x);
+    TwoHop th0, th1;
+    th0.idx = s.th_idx + s.th_off[c.u0];
+    th0.rest = s.th_rest + s.th_off[c.u0];
+    th0.n = s.th_off[c.u0 + 1] - s.th_off[c.u0];
+    th1.idx = s.th_idx + s.th_off[c.u1];
+    th1.rest = s.th_rest + s.th_off[c.u1];
+    th1.n = s.th_off[c.u1 + 1] - s.th_off[c.u1];
+    const uint2 ebv = s.edges[pr.y];
+    ee_pair(s, c, th0, th1, pr.y, ebv.x, ebv.y, s.p4[ebv.x], s.p4[ebv.y], s.x4[ebv.x], s.x4[ebv.y], false);
+  }
+}
+
+// One warp per edge; candidates of the 27 cells around the edge midpoint are
+// flattened in the reference's order (dz outer, dx inner) and visited 32 per
+// round.  The per-edge cap on counted candidates (search_count >
+// max_search_iterations, :356-359) is applied with a ballot prefix count, so
+// exactly the reference's first max_search counted pairs are processed.
+__global__ void __launch_bounds__(256, 3) k_ee(SCArgs s) {
+  __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
+  __shared__ uint32_t sh_th[8][2][kTwoHopCache];
+  __shared__ float sh_thr[8][2][kTwoHopCache];
+  __shared__ uint32_t sh_q[8][32 * kRounds];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ei = blockIdx.x * 8u + warp;
+  if (ei >= s.ne) return;  // whole warp
+  const EdgeCtx c = edge_ctx(s, ei);
   const int4 bc4 = s.ecell[ei];
   const I3 base = I3{bc4.x, bc4.y, bc4.z};
-  c.la = layer_of(s.v4, c.u0);
   const TwoHop th0 = stage_two_hop(s.th_off, s.th_idx, s.th_rest, c.u0, sh_th[warp][0], sh_thr[warp][0], lane);
   const TwoHop th1 = stage_two_hop(s.th_off, s.th_idx, s.th_rest, c.u1, sh_th[warp][1], sh_thr[warp][1], lane);
-  c.untangle = s.untangle != 0;
   // lane k = (dz+1)*9 + (dy+1)*3 + (dx+1)
   uint32_t cnt = 0, beg = 0;
   if (lane < 27) {
     const uint32_t h = hash3(base.x - 1 + lane % 3, base.y - 1 + (lane / 3) % 3, base.z - 1 + lane / 9, s.table);
     beg = s.ecs[h];
     const uint32_t en = s.ecs[h + 1];
+    // buckets are in ascending edge order and a pair belongs to its smaller
+    // edge index: skip straight to the first edge > ei (never counted before)
+    uint32_t lo = beg, hi = en > beg ? en : beg;
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo) / 2u;
+      if ((uint32_t)s.es_c[mid].w <= ei) lo = mid + 1u; else hi = mid;
+    }
+    beg = lo;
     cnt = en > beg ? en - beg : 0u;
   }
   uint32_t incl = cnt;
@@ -1169,7 +1214,7 @@ __global__ void __launch_bounds__(256, 3) k_ee(SCArgs s) {
       const uint32_t eb = (uint32_t)s.es_c[slot].w;
       const uint2 ebv = s.es_v[slot];
       const float4 qj = s.p4[ebv.x], qvj = s.p4[ebv.y], xj = s.x4[ebv.x], xvj = s.x4[ebv.y];
-      ee_pair(s, c, th0, th1, eb, ebv.x, ebv.y, qj, qvj, xj, xvj);
+      ee_pair(s, c, th0, th1, eb, ebv.x, ebv.y, qj, qvj, xj, xvj, true);
     }
     __syncwarp();
   }

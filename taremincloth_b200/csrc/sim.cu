@@ -95,7 +95,8 @@ struct Sim {
   DBuf<float4> vs_p, vs_q, es_lo, es_hi;
   DBuf<uint32_t> tile_sum;
   DBuf<int4> vs_c, es_c;
-  DBuf<uint2> es_v;
+  DBuf<uint2> es_v, ccd_q;
+  DBuf<uint32_t> ccd_n;
   // colliders
   std::vector<Prim> prims_h;
   std::vector<MeshTri> tris_h;
@@ -274,6 +275,7 @@ struct Sim {
     nrm.alloc(n);
     acc.alloc(size_t(n) * A_N);
     vcell.alloc(n); mlen.alloc(n); ecell.alloc(ne); eamin.alloc(ne); eamax.alloc(ne);
+    ccd_q.alloc(size_t(ne) * 4 + 1024); ccd_n.alloc(1);
     vs_p.alloc(n); vs_q.alloc(n); vs_c.alloc(n); tile_sum.alloc(64); es_c.alloc(ne); es_v.alloc(ne); es_lo.alloc(ne); es_hi.alloc(ne);
     TC_CK(cudaMemsetAsync(acc.p, 0, size_t(n) * A_N * sizeof(int32_t), st));
     TC_CK(cudaMemsetAsync(nrm.p, 0, size_t(n) * sizeof(float4), st));
@@ -421,6 +423,7 @@ struct Sim {
     a.star_off = star_off.p; a.star_idx = star_idx.p; a.edges = edges.p; a.edge_bits = edge_bits.p;
     a.cs = cs.p; a.srt = srt.p; a.ecs = ecs.p; a.esrt = esrt.p; a.nrm = nrm.p; a.acc = acc.p;
     a.vcell = vcell.p; a.mlen = mlen.p; a.ecell = ecell.p; a.eamin = eamin.p; a.eamax = eamax.p;
+    a.ccd_q = ccd_q.p; a.ccd_n = ccd_n.p; a.ccd_cap = uint32_t(ccd_q.n);
     a.vs_p = vs_p.p; a.vs_q = vs_q.p; a.vs_c = vs_c.p; a.es_c = es_c.p; a.es_v = es_v.p; a.es_lo = es_lo.p; a.es_hi = es_hi.p;
     return a;
   }
@@ -460,7 +463,13 @@ struct Sim {
     if (ne > 0) encode_hash(1);
     timed("sc_solve", [&] { k_sc_solve<<<grid(n, 8), 256, 0, st>>>(a); });
     if (a.untangle) timed("sc_untangle", [&] { k_untangle<<<grid(n, 128), 128, 0, st>>>(a); });
-    if (ne > 0) timed("sc_solve_ee", [&] { k_ee<<<grid(ne, 8), 256, 0, st>>>(a); });
+    if (ne > 0) {
+      timed("sc_solve_ee", [&] {
+        TC_CK(cudaMemsetAsync(ccd_n.p, 0, sizeof(uint32_t), st));
+        k_ee<<<grid(ne, 8), 256, 0, st>>>(a);
+      });
+      timed("sc_solve_ee_ccd", [&] { k_ee_ccd<<<148 * 8, 256, 0, st>>>(a); });
+    }
     timed("sc_apply", [&] {
       k_apply<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, local_len.p, acc.p, relief, enable_relief ? 1 : 0,
                                              max_disp_ratio);
