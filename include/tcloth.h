@@ -158,6 +158,21 @@ tc_status tc_frame_kernel_count(tc_sim *s, uint32_t *count);
 /* Device time of the latest frame in milliseconds (CUDA events). */
 tc_status tc_last_frame_ms(tc_sim *s, float *ms);
 
+/* Spatial-hash build that allocates nothing; no counterpart in the reference.
+ * For callers that cannot allocate device memory: applications whose device
+ * buffers all come from their own allocator, threads that must not call
+ * cudaMalloc / cudaFree (they synchronise the device), memory-capped hosts.
+ * Builds the same cell_starts / sorted arrays as tc_get_hash_state from
+ * `positions` (device, n x 4 floats: x, y, z, unused), on `stream`
+ * (cudaStream_t, NULL = legacy default stream).  All buffers are the
+ * caller's device memory; scratch is a static array in the library of fixed
+ * size, so n <= 262144 and 1024 <= table_size <= 65536, else TC_ERR_INVALID.
+ * The first call on a device looks up that array's device address, so make
+ * it before any stream capture.  All calls on a device share the array:
+ * calls that overlap on the GPU (different streams, or threads) race. */
+tc_status tc_hash_build_static(const float *positions, uint32_t n, float cell_size, uint32_t table_size,
+                               uint32_t *cell_starts, uint32_t *sorted, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

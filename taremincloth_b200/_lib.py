@@ -67,6 +67,7 @@ SIGNATURES = {
     "tc_last_frame_ms": [_P, C.POINTER(_F)],
     "tc_set_profiling_enabled": [_P, _I],
     "tc_frame_kernel_count": [_P, C.POINTER(_U)],
+    "tc_hash_build_static": [_P, _U, _F, _U, _P, _P, _P],
     "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],
     "tc_mesh_build": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F],
     "tc_mesh_destroy": [_P],

@@ -1236,3 +1236,79 @@ tc_status tc_last_frame_ms(tc_sim* s, float* ms) {
 }
 
 }  // extern "C"
+
+// ===================================================================
+// Spatial-hash build without any allocation
+// ===================================================================
+// For callers that cannot allocate device memory themselves: a host
+// application that owns every device buffer through its own allocator (for
+// example a DCC tool or game-engine plugin), a thread that must not call
+// cudaMalloc / cudaFree because they synchronise the device, or a
+// memory-capped service.  Their scratch space is this file-scope array,
+// sized for the largest cloth the reference's hash supports (its table is
+// capped at 65,536 buckets); every GPU that loads the library holds it
+// (about 1.6 MB) until the process exits.
+namespace {
+constexpr uint32_t kStaticMaxElems = 262144;  // vertices (or edges) per call
+constexpr uint32_t kStaticMaxTable = 65536;   // hash buckets per call
+constexpr uint32_t kStaticTiles = kStaticMaxTable / 1024;
+struct StaticHashScratch {
+  uint32_t keys[kStaticMaxElems];
+  uint32_t counts[kStaticMaxTable + 1];
+  uint32_t cursor[kStaticMaxTable + 1];
+  uint32_t tile_sum[kStaticTiles];
+};
+}  // namespace
+static __device__ __align__(256) StaticHashScratch g_static_hash_scratch;
+
+// bucket key of each position (the count pass of spatial_grid_sort.wgsl:44-52)
+__global__ void k_static_hash_count(uint32_t n, const float4* __restrict__ pos, float cell, uint32_t table,
+                                    uint32_t* __restrict__ keys, uint32_t* __restrict__ counts) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const tcloth::I3 c = tcloth::cell_of(tcloth::mk(pos[i]), cell);
+  const uint32_t h = tcloth::hash3(c.x, c.y, c.z, table);
+  keys[i] = h;
+  atomicAdd(&counts[h], 1u);
+}
+
+static StaticHashScratch* static_scratch_for_current_device() {
+  // One device address per device, looked up on the first call with that
+  // device current (the host-side name of the array is not a device address).
+  static StaticHashScratch* ptrs[64] = {};
+  int dev = 0;
+  TC_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw TcError(TC_ERR_CUDA, "device index out of range for the static scratch table");
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    TC_CK(cudaGetSymbolAddress(&p, g_static_hash_scratch));
+    ptrs[dev] = static_cast<StaticHashScratch*>(p);
+  }
+  return ptrs[dev];
+}
+
+extern "C" tc_status tc_hash_build_static(const float* positions, uint32_t n, float cell_size, uint32_t table_size,
+                                          uint32_t* cell_starts, uint32_t* sorted, void* stream) {
+  return guard([&] {
+    need(n <= kStaticMaxElems, "tc_hash_build_static: n exceeds the static scratch limit of 262144 elements");
+    need(table_size >= 1024 && table_size <= kStaticMaxTable,
+         "tc_hash_build_static: table_size must be in [1024, 65536]");
+    need(cell_size > 0.f, "tc_hash_build_static: cell_size must be positive");
+    need(cell_starts != nullptr && (sorted != nullptr || n == 0) && (positions != nullptr || n == 0),
+         "tc_hash_build_static: positions, cell_starts and sorted are required");
+    StaticHashScratch* sc = static_scratch_for_current_device();
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float4* pos = reinterpret_cast<const float4*>(positions);
+    const uint32_t T = table_size;
+    // the array keeps the previous call's contents: zero what must start at zero
+    TC_CK(cudaMemsetAsync(sc->counts, 0, (T + 1) * sizeof(uint32_t), st));
+    TC_CK(cudaMemsetAsync(sc->cursor, 0, (T + 1) * sizeof(uint32_t), st));
+    if (n) k_static_hash_count<<<(n + 255) / 256, 256, 0, st>>>(n, pos, cell_size, T, sc->keys, sc->counts);
+    const uint32_t ntiles = (T + 1023) / 1024;
+    tcloth::k_scan_blocks<<<ntiles, 1024, 0, st>>>(T, sc->counts, cell_starts, sc->tile_sum);
+    tcloth::k_scan_finish<<<ntiles, 1024, 0, st>>>(T, ntiles, sc->tile_sum, cell_starts);
+    if (n) tcloth::k_hash_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, sc->keys, cell_starts, sc->cursor, sorted);
+    tcloth::k_hash_sort_buckets<<<(T + 255) / 256, 256, 0, st>>>(T, cell_starts, sorted);
+    TC_CK(cudaGetLastError());
+  });
+}
