@@ -153,6 +153,18 @@ tc_status tc_mesh_topology(tc_mesh *m, uint32_t *adj_off, uint32_t *adj_idx, uin
 tc_status tc_set_profiling_enabled(tc_sim *s, int enable);
 tc_status tc_take_profile(tc_sim *s, char *names, size_t names_len, float *ms, uint32_t *launches,
                           uint32_t max_entries, uint32_t *n_entries);
+/* Persistent solver (default on when the device supports cooperative
+ * launch): the constraint phase of a substep (of a whole frame when
+ * self-collision is off) is one cooperative launch whose colours are
+ * separated by bounded grid barriers; off = one launch per colour.  Both give
+ * the same bits.  A barrier that waits past its poll limit makes tc_step
+ * return TC_ERR_TIMEOUT.  New; the reference dispatches one pass per colour
+ * (dispatch.rs:1449-1455). */
+tc_status tc_set_persistent_solver(tc_sim *s, int enable);
+/* Diagnostics for the failure path: runs one barrier that can never be
+ * released, with the given poll limit (1..4194304), and returns
+ * TC_ERR_TIMEOUT when every wait ended by the limit.  Touches no state. */
+tc_status tc_check_barrier_timeout(tc_sim *s, uint32_t spin_limit);
 /* Kernel launches in the recorded frame (kernel nodes of its CUDA graph). */
 tc_status tc_frame_kernel_count(tc_sim *s, uint32_t *count);
 /* Device time of the latest frame in milliseconds (CUDA events). */

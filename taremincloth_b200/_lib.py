@@ -67,6 +67,8 @@ SIGNATURES = {
     "tc_last_frame_ms": [_P, C.POINTER(_F)],
     "tc_set_profiling_enabled": [_P, _I],
     "tc_frame_kernel_count": [_P, C.POINTER(_U)],
+    "tc_set_persistent_solver": [_P, _I],
+    "tc_check_barrier_timeout": [_P, _U],
     "tc_hash_build_static": [_P, _U, _F, _U, _P, _P, _P],
     "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],
     "tc_mesh_build": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F],
@@ -99,6 +101,10 @@ def load(path: str = LIB_PATH):
     return L
 
 
+class BarrierTimeout(RuntimeError):
+    """A bounded grid-barrier wait of the persistent solver gave up."""
+
+
 def check(status: int) -> None:
     """Map a tc_status to the reference's Python exceptions."""
     if status == TC_OK:
@@ -106,6 +112,8 @@ def check(status: int) -> None:
     msg = load().tc_last_error().decode("utf-8", "replace")
     if status == TC_ERR_INVALID:
         raise ValueError(msg)
+    if status == TC_ERR_TIMEOUT:
+        raise BarrierTimeout(msg)
     if status == TC_ERR_NOMEM:
         raise MemoryError(msg)
     raise RuntimeError(msg)

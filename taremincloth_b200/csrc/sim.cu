@@ -107,6 +107,13 @@ struct Sim {
   std::map<uint32_t, PinH> pins;
   DBuf<uint32_t> pin_v;
   DBuf<float4> pin_t;
+  // persistent solver (one cooperative launch per substep / frame)
+  bool persistent = true;
+  unsigned int persist_blocks = 0;
+  unsigned int spin_limit = 1u << 22;  // ~0.5 s of polling per barrier
+  DBuf<GridBar> bar;
+  DBuf<uint32_t> dist_offc, dist_cntc, bend_offc, bend_cntc;
+  int* h_err = nullptr;  // pinned
   // residual instrumentation
   bool track_residual = false;
   DBuf<float> res_sum, res_max;  // [ndc + nbc] each
@@ -178,6 +185,7 @@ struct Sim {
     if (ev1) cudaEventDestroy(ev1);
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
+    if (h_err) cudaFreeHost(h_err);
   }
 
   void mark() { graph_dirty = true; }
@@ -282,6 +290,20 @@ struct Sim {
     res_sum.alloc(m.dist_cnt.size() + m.bend_cnt.size() + 1);
     res_max.alloc(m.dist_cnt.size() + m.bend_cnt.size() + 1);
     prims.alloc(1); tris.alloc(1); bounds.alloc(1); cl16.alloc(1); cl256.alloc(1);
+    dist_offc.upload(m.dist_off, st); dist_cntc.upload(m.dist_cnt, st);
+    bend_offc.upload(m.bend_off, st); bend_cntc.upload(m.bend_cnt, st);
+    bar.alloc(2);
+    TC_CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(GridBar), st));
+    TC_CK(cudaHostAlloc(&h_err, sizeof(int), cudaHostAllocDefault));
+    *h_err = 0;
+    {
+      int coop = 0, nsm = 0, per_sm = 0;
+      TC_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+      TC_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+      TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solver_persistent, 256, 0));
+      persist_blocks = coop && per_sm > 0 ? unsigned(nsm * std::min(per_sm, 4)) : 0u;
+      if (!persist_blocks) persistent = false;
+    }
     pin_v.alloc(1); pin_t.alloc(1);
     TC_CK(cudaStreamSynchronize(st));
   }
@@ -486,8 +508,58 @@ struct Sim {
 
   void encode_residual(const SubstepParams& sp);
 
+  SolverArgs solver_args(const SubstepParams& sp, uint32_t nsub, bool use_coupled, bool with_update) {
+    SolverArgs a;
+    a.n = n; a.nsub = nsub; a.iters = iters; a.npins = uint32_t(pins.size());
+    a.ndc = uint32_t(m.dist_cnt.size()); a.nbc = uint32_t(m.bend_cnt.size());
+    a.hascol = !prims_h.empty() || !tris_h.empty();
+    a.coupled = use_coupled;
+    a.ddamp = td != 0.f || cd != 0.f || sd != 0.f;
+    a.bdamp = bd != 0.f;
+    a.with_update = with_update;
+    a.sp = sp;
+    a.x4 = x4.p; a.p4 = p4.p; a.v4 = v4.p;
+    a.dist_ids = dist_ids.p; a.dist_par = dist_par.p; a.dlam = dlam.p; a.nd = nd;
+    a.bend_ids = bend_ids.p; a.bend_par = bend_par.p; a.blam = blam.p; a.nb = nb;
+    a.dist_off = dist_offc.p; a.dist_cnt = dist_cntc.p; a.bend_off = bend_offc.p; a.bend_cnt = bend_cntc.p;
+    a.pin_v = pin_v.p; a.pin_t = pin_t.p;
+    a.ca = collider_args();
+    a.bar = bar.p;
+    a.expected = persist_blocks;
+    a.spin_limit = spin_limit;
+    return a;
+  }
+  void launch_persistent(const SolverArgs& a) {
+    TC_CK(cudaMemsetAsync(a.bar, 0, sizeof(GridBar), st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(persist_blocks);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TC_CK(cudaLaunchKernelEx(&cfg, k_solver_persistent, a));
+  }
+
   // encode_simulation_steps (dispatch.rs:7-354) for one frame
   void encode_frame(float dt, uint32_t substeps, bool use_coupled) {
+    if (persistent && !profiling && !track_residual) {
+      const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
+      if (!self_collision) {
+        launch_persistent(solver_args(sp, substeps, use_coupled, true));
+      } else {
+        for (uint32_t s = 0; s < substeps; ++s) {
+          launch_persistent(solver_args(sp, 1, use_coupled, false));
+          encode_self_collision();
+          k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp.dt);
+        }
+      }
+      TC_CK(cudaMemcpyAsync(h_err, &bar.p->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      TC_CK(cudaGetLastError());
+      return;
+    }
     const float dts = dt / float(substeps);
     SubstepParams sp{dts, g[0], g[1], g[2], damping, td, cd, sd, bd};
     const bool ddamp = td != 0.f || cd != 0.f || sd != 0.f;
@@ -587,10 +659,19 @@ struct Sim {
   }
 
   uint32_t graph_kernels = 0;
+  void check_barrier_status() {
+    if (*h_err != 0) {
+      *h_err = 0;
+      TC_CK(cudaMemsetAsync(bar.p, 0, sizeof(GridBar), st));
+      TC_CK(cudaStreamSynchronize(st));
+      throw TcError(TC_ERR_TIMEOUT, "a grid barrier of the persistent solver timed out; the frame is incomplete");
+    }
+  }
   void step(float dt, uint32_t substeps) {
     launch_frame(dt, substeps);
     TC_CK(cudaStreamSynchronize(st));
     TC_CK(cudaGetLastError());
+    check_barrier_status();
   }
 
   void get_positions(float* out) {
@@ -669,7 +750,10 @@ void Sim::encode_residual(const SubstepParams& sp) {
 // ===================================================================
 // C ABI
 // ===================================================================
+using tcloth::GridBar;
 using tcloth::Sim;
+using tcloth::SolverArgs;
+using tcloth::SubstepParams;
 using tcloth::TcError;
 
 struct tc_sim {
@@ -797,6 +881,7 @@ tc_status tc_fetch_positions(tc_sim* s, float* out, size_t out_len, int* ok) {
     need(out != nullptr && out_len >= size_t(m.n) * 3, "out_array too small");
     m.get_positions(out);
     m.async_pending = false;
+    m.check_barrier_status();
     float md = 0.f;
     for (size_t i = 0; i < size_t(m.n) * 3; ++i) md = std::fmax(md, std::fabs(out[i] - m.prev_frame_pos[i]));
     std::memcpy(m.prev_frame_pos.data(), out, size_t(m.n) * 3 * sizeof(float));
@@ -1220,6 +1305,40 @@ tc_status tc_take_profile(tc_sim* s, char* names, size_t names_len, float* ms, u
     if (names && names_len) std::snprintf(names, names_len, "%s", joined.c_str());
     *n_entries = k;
     m.prof_names.clear(); m.prof_ms.clear(); m.prof_cnt.clear();
+  });
+}
+
+tc_status tc_set_persistent_solver(tc_sim* s, int enable) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (enable && !m.persist_blocks) throw TcError(TC_ERR_CUDA, "cooperative launch is not available on this device");
+    m.persistent = enable != 0;
+    m.mark();
+  });
+}
+
+// Runs the persistent solver's barrier once with one more expected arrival
+// than there are blocks, so it can never be released, and with the given
+// poll limit: every wait ends by the limit and the launch reports
+// TC_ERR_TIMEOUT.  No vertex or constraint is touched (zero-size phases).
+tc_status tc_check_barrier_timeout(tc_sim* s, uint32_t spin_limit) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(m.persist_blocks > 0, "cooperative launch is not available on this device");
+    need(spin_limit > 0 && spin_limit <= (1u << 22), "spin_limit must be in [1, 4194304]");
+    const SubstepParams sp{1e-3f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    SolverArgs a = m.solver_args(sp, 1, false, false);
+    a.n = 0; a.nd = 0; a.nb = 0; a.npins = 0; a.ndc = 0; a.nbc = 0; a.hascol = false;
+    a.bar = m.bar.p + 1;
+    a.expected = m.persist_blocks + 1;
+    a.spin_limit = spin_limit;
+    m.launch_persistent(a);
+    int err = 0;
+    TC_CK(cudaMemcpyAsync(&err, &a.bar->err, sizeof(int), cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    TC_CK(cudaMemsetAsync(a.bar, 0, sizeof(GridBar), m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    if (err) throw TcError(TC_ERR_TIMEOUT, "grid barrier wait reached its poll limit");
   });
 }
 

@@ -12,6 +12,17 @@
 
 namespace tcloth {
 
+// Loads of data that other blocks of a persistent launch write between two
+// grid barriers go through L2 (ld.global.cg) so no SM reads a stale L1 line.
+template <bool kCg>
+__device__ __forceinline__ float4 ld4(const float4* p) {
+  if constexpr (kCg) return __ldcg(p); else return *p;
+}
+template <bool kCg>
+__device__ __forceinline__ float ld1(const float* p) {
+  if constexpr (kCg) return __ldcg(p); else return *p;
+}
+
 struct SubstepParams {
   float dt;       // substep dt (already max(dt, 1e-8) where the shaders do so)
   float gx, gy, gz;
@@ -20,11 +31,10 @@ struct SubstepParams {
 };
 
 // shaders/predict.wgsl:33-55
-__global__ void k_predict(uint32_t n, const float4* __restrict__ x4, float4* __restrict__ p4,
-                          float4* __restrict__ v4, SubstepParams sp) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float4 x = x4[i], p = p4[i], v = v4[i];
+template <bool kCg>
+__device__ __forceinline__ void predict_vertex(uint32_t i, const float4* __restrict__ x4, float4* __restrict__ p4,
+                                               float4* __restrict__ v4, const SubstepParams& sp) {
+  float4 x = ld4<kCg>(x4 + i), p = ld4<kCg>(p4 + i), v = ld4<kCg>(v4 + i);
   const float dt = fmaxf(sp.dt, 1e-8f);
   if (x.w <= 0.0f) {
     v.x = 0.f; v.y = 0.f; v.z = 0.f;
@@ -39,18 +49,24 @@ __global__ void k_predict(uint32_t n, const float4* __restrict__ x4, float4* __r
   p4[i] = p;
   v4[i] = v;
 }
+__global__ void k_predict(uint32_t n, const float4* __restrict__ x4, float4* __restrict__ p4,
+                          float4* __restrict__ v4, SubstepParams sp) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  predict_vertex<false>(i, x4, p4, v4, sp);
+}
 
 // shaders/pin.wgsl:56-92; pins are on distinct vertices, so order is free
-__global__ void k_pin(uint32_t npins, const uint32_t* __restrict__ pin_v, const float4* __restrict__ pin_t,
-                      const float4* __restrict__ x4, float4* __restrict__ p4, float dt_sub) {
-  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= npins) return;
+template <bool kCg>
+__device__ __forceinline__ void pin_one(uint32_t k, const uint32_t* __restrict__ pin_v,
+                                        const float4* __restrict__ pin_t, const float4* __restrict__ x4,
+                                        float4* __restrict__ p4, float dt_sub) {
   const uint32_t vi = pin_v[k];
   const float4 t = pin_t[k];  // target xyz, weight
   const float w = clampf(t.w, 0.0f, 1.0f);
   if (w <= 0.0f) return;
-  const float im = x4[vi].w;
-  float4 p = p4[vi];
+  const float im = ld4<kCg>(x4 + vi).w;
+  float4 p = ld4<kCg>(p4 + vi);
   if (im <= 0.0f) {
     p.x = t.x; p.y = t.y; p.z = t.z;
     p4[vi] = p;
@@ -68,19 +84,26 @@ __global__ void k_pin(uint32_t npins, const uint32_t* __restrict__ pin_v, const 
   p.x = np.x; p.y = np.y; p.z = np.z;
   p4[vi] = p;
 }
+__global__ void k_pin(uint32_t npins, const uint32_t* __restrict__ pin_v, const float4* __restrict__ pin_t,
+                      const float4* __restrict__ x4, float4* __restrict__ p4, float dt_sub) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npins) return;
+  pin_one<false>(k, pin_v, pin_t, x4, p4, dt_sub);
+}
 
 // One distance constraint (shaders/distance.wgsl:60-124).  dist_par =
 // (rest, tension compliance, compression compliance, shear flag).
+template <bool kCg>
 __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __restrict__ ids,
                                                  const float4* __restrict__ par, float4* __restrict__ x4,
                                                  float4* __restrict__ p4, float* __restrict__ lam,
                                                  const SubstepParams& sp, bool damped) {
   const uint2 e = ids[ci];
   const float4 c = par[ci];
-  const float w0 = x4[e.x].w, w1 = x4[e.y].w;
+  const float w0 = ld4<kCg>(x4 + e.x).w, w1 = ld4<kCg>(x4 + e.y).w;
   const float ws = w0 + w1;
   if (ws <= kEps) return;
-  const float4 q0 = p4[e.x], q1 = p4[e.y];
+  const float4 q0 = ld4<kCg>(p4 + e.x), q1 = ld4<kCg>(p4 + e.y);
   const V3 p0 = mk(q0), p1 = mk(q1);
   const V3 delta = p0 - p1;
   const float dist = length(delta);
@@ -95,9 +118,9 @@ __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __res
     const float damp = c.w != 0.0f ? sp.sd : (cv >= 0.0f ? sp.td : sp.cd);
     const float tau = damp * 1e-5f;
     const float gamma = fminf(tau / dt, 1e4f);
-    const V3 rel = (p0 - mk(x4[e.x])) - (p1 - mk(x4[e.y]));
+    const V3 rel = (p0 - mk(ld4<kCg>(x4 + e.x))) - (p1 - mk(ld4<kCg>(x4 + e.y)));
     const float vp = dot(dir, rel);
-    const float l = lam[ci];
+    const float l = ld1<kCg>(lam + ci);
     const float dl = (-cv - alpha * l - gamma * vp) / ((1.0f + gamma) * ws + alpha);
     lam[ci] = l + dl;
     const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
@@ -105,7 +128,7 @@ __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __res
     p4[e.y] = make_float4(n1.x, n1.y, n1.z, q1.w);
     return;
   }
-  const float l = lam[ci];
+  const float l = ld1<kCg>(lam + ci);
   // gamma == 0: (-cv - alpha*l - 0*vp) / (1*ws + alpha)
   const float dl = (-cv - alpha * l) / (1.0f * ws + alpha);
   lam[ci] = l + dl;
@@ -119,11 +142,12 @@ __global__ void k_distance(uint32_t off, uint32_t cnt, const uint2* __restrict__
                            SubstepParams sp, bool damped) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= cnt) return;
-  project_distance(off + k, ids, par, x4, p4, lam, sp, damped);
+  project_distance<false>(off + k, ids, par, x4, p4, lam, sp, damped);
 }
 
 // One bending constraint (shaders/bending.wgsl:59-126).  bend_par =
 // (rest, compliance, kind, seam gap).
+template <bool kCg>
 __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __restrict__ ids,
                                                 const float4* __restrict__ par, float4* __restrict__ x4,
                                                 float4* __restrict__ p4, float* __restrict__ lam,
@@ -131,29 +155,29 @@ __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __rest
   const float4 c = par[ci];
   if (c.y >= 1e9f) return;
   const uint4 e = ids[ci];
-  const float w2 = x4[e.z].w, w3 = x4[e.w].w;
+  const float w2 = ld4<kCg>(x4 + e.z).w, w3 = ld4<kCg>(x4 + e.w).w;
   const float ws = w2 + w3;
   if (ws <= kEps) return;
-  const float4 q2 = p4[e.z], q3 = p4[e.w];
+  const float4 q2 = ld4<kCg>(p4 + e.z), q3 = ld4<kCg>(p4 + e.w);
   const V3 p2 = mk(q2), p3 = mk(q3);
   const V3 delta = p2 - p3;
   const float dist = length(delta);
   if (dist <= kEps) return;
   if (c.z > 0.5f && c.z < 1.5f) {
     if (dist >= c.x) return;
-    float gap = length(mk(p4[e.x]) - mk(p4[e.y]));
+    float gap = length(mk(ld4<kCg>(p4 + e.x)) - mk(ld4<kCg>(p4 + e.y)));
     if (gap > c.w) return;
   }
   const V3 dir = delta / dist;
   const float dt = fmaxf(sp.dt, 1e-8f);
   const float alpha = c.y / (dt * dt);
   const float cv = dist - c.x;
-  const float l = lam[ci];
+  const float l = ld1<kCg>(lam + ci);
   float dl;
   if (damped) {
     const float tau = sp.bd * 1e-5f;
     const float gamma = fminf(tau / dt, 1e4f);
-    const V3 rel = (p2 - mk(x4[e.z])) - (p3 - mk(x4[e.w]));
+    const V3 rel = (p2 - mk(ld4<kCg>(x4 + e.z))) - (p3 - mk(ld4<kCg>(x4 + e.w)));
     const float vp = dot(dir, rel);
     dl = (-cv - alpha * l - gamma * vp) / ((1.0f + gamma) * ws + alpha);
   } else {
@@ -170,17 +194,16 @@ __global__ void k_bending(uint32_t off, uint32_t cnt, const uint4* __restrict__ 
                           SubstepParams sp, bool damped) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= cnt) return;
-  project_bending(off + k, ids, par, x4, p4, lam, sp, damped);
+  project_bending<false>(off + k, ids, par, x4, p4, lam, sp, damped);
 }
 
 // shaders/update_vel.wgsl:33-53
-__global__ void k_update_vel(uint32_t n, float4* __restrict__ x4, const float4* __restrict__ p4,
-                             float4* __restrict__ v4, float dt_sub) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float4 x = x4[i];
-  const float4 p = p4[i];
-  float4 v = v4[i];
+template <bool kCg>
+__device__ __forceinline__ void update_vertex(uint32_t i, float4* __restrict__ x4, const float4* __restrict__ p4,
+                                              float4* __restrict__ v4, float dt_sub) {
+  float4 x = ld4<kCg>(x4 + i);
+  const float4 p = ld4<kCg>(p4 + i);
+  float4 v = ld4<kCg>(v4 + i);
   const float dt = fmaxf(dt_sub, 1e-8f);
   if (x.w > 0.0f) {
     V3 vv = (mk(p) - mk(x)) / dt;
@@ -191,6 +214,12 @@ __global__ void k_update_vel(uint32_t n, float4* __restrict__ x4, const float4* 
   x.x = p.x; x.y = p.y; x.z = p.z;
   x4[i] = x;
   v4[i] = v;
+}
+__global__ void k_update_vel(uint32_t n, float4* __restrict__ x4, const float4* __restrict__ p4,
+                             float4* __restrict__ v4, float dt_sub) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  update_vertex<false>(i, x4, p4, v4, dt_sub);
 }
 
 // ---------------------------------------------------------------------
@@ -311,13 +340,12 @@ __device__ __forceinline__ bool group_far(V3 a, V3 b, float4 g, float th) {
 // exactly like the reference; two levels of conservative bounding spheres
 // skip runs of triangles none of which could pass the per-triangle test, so
 // the sequence of applied contacts is unchanged.
-__global__ void k_collision(uint32_t n, float4* __restrict__ x4, float4* __restrict__ p4, ColliderArgs ca,
-                            float dt) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float4 x = x4[i];
+template <bool kCg>
+__device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ x4, float4* __restrict__ p4,
+                                               const ColliderArgs& ca, float dt) {
+  float4 x = ld4<kCg>(x4 + i);
   if (x.w <= 0.0f) return;
-  float4 pr = p4[i];
+  float4 pr = ld4<kCg>(p4 + i);
   V3 p = mk(pr), pinit = p, xn = mk(x);
   const V3 xpos = mk(x);
   const float th = pr.w;
@@ -378,6 +406,134 @@ __global__ void k_collision(uint32_t n, float4* __restrict__ x4, float4* __restr
   }
   p4[i] = make_float4(p.x, p.y, p.z, pr.w);
   x4[i] = make_float4(xn.x, xn.y, xn.z, x.w);
+}
+__global__ void k_collision(uint32_t n, float4* __restrict__ x4, float4* __restrict__ p4, ColliderArgs ca,
+                            float dt) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  collide_vertex<false>(i, x4, p4, ca, dt);
+}
+
+// ---------------------------------------------------------------------
+// persistent solver kernel
+// ---------------------------------------------------------------------
+// Grid barrier for a cooperative launch (all blocks resident).  Waits are
+// bounded: after spin_limit polls a block records an error and every block
+// leaves the kernel at its next barrier, so a stuck barrier ends with a status
+// instead of a hang.  `expected` is the number of arrivals that releases the
+// barrier (gridDim.x in normal operation).
+struct GridBar {
+  unsigned int count;
+  unsigned int gen;
+  int err;
+  unsigned int pad;
+};
+__device__ __forceinline__ bool grid_sync(GridBar* b, unsigned int expected, unsigned int spin_limit) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = &b->gen;
+    volatile int* verr = &b->err;
+    const unsigned int g = *vgen;
+    __threadfence();
+    if (*verr == 0) {
+      if (atomicAdd(&b->count, 1u) == expected - 1u) {
+        atomicExch(&b->count, 0u);
+        __threadfence();
+        atomicAdd(&b->gen, 1u);
+      } else {
+        unsigned int spins = 0;
+        while (*vgen == g && *verr == 0) {
+          if (++spins > spin_limit) {
+            atomicExch(&b->err, 1);
+            break;
+          }
+          __nanosleep(100);
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *((volatile int*)&b->err) == 0;
+}
+
+struct SolverArgs {
+  uint32_t n, nsub, iters, npins, ndc, nbc;
+  bool hascol, coupled, ddamp, bdamp, with_update;
+  SubstepParams sp;
+  float4 *x4, *p4, *v4;
+  const uint2* dist_ids;
+  const float4* dist_par;
+  float* dlam;
+  uint32_t nd;
+  const uint4* bend_ids;
+  const float4* bend_par;
+  float* blam;
+  uint32_t nb;
+  const uint32_t* dist_off;  // per colour
+  const uint32_t* dist_cnt;
+  const uint32_t* bend_off;
+  const uint32_t* bend_cnt;
+  const uint32_t* pin_v;
+  const float4* pin_t;
+  ColliderArgs ca;
+  GridBar* bar;
+  unsigned int expected;  // arrivals per barrier
+  unsigned int spin_limit;
+};
+
+// One cooperative launch runs `nsub` substeps of the constraint phase
+// (dispatch.rs:104-250: lambda clear, predict, iterations of pins / distance
+// colours / bending colours / coupled collision, decoupled collision, final
+// pin) and, with_update set, the velocity update; colours are separated by
+// grid barriers instead of kernel launches.  Same per-element functions, so
+// the same bits as the launch-per-colour path.
+__global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const float dts = a.sp.dt;
+  for (uint32_t sub = 0; sub < a.nsub; ++sub) {
+    for (uint32_t i = tid; i < a.nd; i += stride) a.dlam[i] = 0.f;
+    for (uint32_t i = tid; i < a.nb; i += stride) a.blam[i] = 0.f;
+    for (uint32_t i = tid; i < a.n; i += stride) predict_vertex<true>(i, a.x4, a.p4, a.v4, a.sp);
+    if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+    for (uint32_t it = 0; it < a.iters; ++it) {
+      if (a.npins) {
+        for (uint32_t k = tid; k < a.npins; k += stride) pin_one<true>(k, a.pin_v, a.pin_t, a.x4, a.p4, dts);
+        if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+      }
+      for (uint32_t c = 0; c < a.ndc; ++c) {
+        const uint32_t off = a.dist_off[c], cnt = a.dist_cnt[c];
+        if (!cnt) continue;
+        for (uint32_t k = tid; k < cnt; k += stride)
+          project_distance<true>(off + k, a.dist_ids, a.dist_par, a.x4, a.p4, a.dlam, a.sp, a.ddamp);
+        if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+      }
+      for (uint32_t c = 0; c < a.nbc; ++c) {
+        const uint32_t off = a.bend_off[c], cnt = a.bend_cnt[c];
+        if (!cnt) continue;
+        for (uint32_t k = tid; k < cnt; k += stride)
+          project_bending<true>(off + k, a.bend_ids, a.bend_par, a.x4, a.p4, a.blam, a.sp, a.bdamp);
+        if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+      }
+      if (a.hascol && a.coupled) {
+        for (uint32_t i = tid; i < a.n; i += stride) collide_vertex<true>(i, a.x4, a.p4, a.ca, dts);
+        if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+      }
+    }
+    if (a.hascol && !a.coupled) {
+      for (uint32_t i = tid; i < a.n; i += stride) collide_vertex<true>(i, a.x4, a.p4, a.ca, dts);
+      if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+    }
+    if (a.npins) {
+      for (uint32_t k = tid; k < a.npins; k += stride) pin_one<true>(k, a.pin_v, a.pin_t, a.x4, a.p4, dts);
+      if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+    }
+    if (a.with_update) {
+      for (uint32_t i = tid; i < a.n; i += stride) update_vertex<true>(i, a.x4, a.p4, a.v4, dts);
+      if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+    }
+  }
 }
 
 }  // namespace tcloth

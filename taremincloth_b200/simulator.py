@@ -346,6 +346,15 @@ class ClothSimulator:
         names = buf.value.decode().split("\n")[:k.value]
         return [(nm, float(ms[i]), int(cnt[i])) for i, nm in enumerate(names)]
 
+    def set_persistent_solver(self, enable=True):
+        """One cooperative launch per substep (per frame without self-collision)
+        with bounded grid barriers between colours; off = one launch per colour."""
+        self._c(self._L.tc_set_persistent_solver(self._h, int(bool(enable))))
+
+    def check_barrier_timeout(self, spin_limit=1000):
+        """Run a barrier that can never be released; raises BarrierTimeout."""
+        self._c(self._L.tc_check_barrier_timeout(self._h, int(spin_limit)))
+
     def frame_kernel_count(self):
         """Kernel launches in the recorded frame graph."""
         v = C.c_uint32()

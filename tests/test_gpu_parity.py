@@ -140,3 +140,29 @@ def test_invalid_inputs_raise():
     s = ClothSimulator(np.zeros((3, 3), np.float32), np.array([[0, 1]], np.uint32))
     with pytest.raises(ValueError):
         s.get_positions(np.empty(2, np.float32))
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_solver_paths_match_oracle(oracle_lib, persistent):
+    """Persistent cooperative solver and launch-per-colour path, config 1
+    (whole frame in one launch) and reduced config 2 (self-collision between
+    persistent launches)."""
+    for sc, frames in ((scenes.config1(), 20), (scenes.config2(n=32, subdiv=3), 6)):
+        g = scenes.build(ClothSimulator, sc)
+        g.set_persistent_solver(persistent)
+        o = scenes.build(oracle_lib.OracleSim, sc)
+        worst, same = compare_frames(g, o, frames, sc["dt"], sc["substeps"], extent(sc["positions"]))
+        assert worst.max() <= 1e-5, (persistent, worst, same)
+
+
+def test_barrier_timeout_reports_status_and_context_survives(oracle_lib):
+    """A grid barrier that can never be released ends by its poll limit with
+    TC_ERR_TIMEOUT; the context stays usable and the next frame is exact."""
+    from taremincloth_b200._lib import BarrierTimeout
+    sc = scenes.config1()
+    g = scenes.build(ClothSimulator, sc)
+    with pytest.raises(BarrierTimeout):
+        g.check_barrier_timeout(2000)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    worst, _ = compare_frames(g, o, 2, sc["dt"], sc["substeps"], extent(sc["positions"]))
+    assert worst.max() <= 1e-5
