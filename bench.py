@@ -171,6 +171,40 @@ def cpu_baseline_sample():
             "sample": f"1 timed substep of the full workload after 1 warm-up substep, OpenMP over {cores} threads"}
 
 
+def batch_extra(steps):
+    """Config 4 (64 uneven instances, 657,683 vertices): the batched simulator
+    (one persistent launch per frame, autotuned launch shape) against the same
+    64 cloths as separate simulators, device time per frame."""
+    from taremincloth_b200 import ClothSimulator, scenes
+    from taremincloth_b200.autotune import autotune
+    sc = scenes.config4()
+    n = sum(len(i["positions"]) for i in sc["instances"])
+    b = scenes.build_batch(sc)
+    tune = autotune(b, sc["dt"], sc["substeps"], frames=2)
+    for _ in range(2):
+        b.step(sc["dt"], sc["substeps"])
+    tb = 0.0
+    for _ in range(steps):
+        b.step(sc["dt"], sc["substeps"])
+        tb += b.last_frame_ms()
+    singles = [scenes.build_instance(ClothSimulator, sc, k) for k in range(len(sc["instances"]))]
+    for s in singles:
+        s.step(sc["dt"], sc["substeps"])
+    import time
+    t0 = time.perf_counter()
+    ts = 0.0
+    for _ in range(steps):
+        for s in singles:
+            s.step(sc["dt"], sc["substeps"])
+            ts += s.last_frame_ms()
+    wall = time.perf_counter() - t0
+    vs = n * sc["substeps"] * steps
+    return {"workload": "64 uneven cloths (sides log-uniform 32..192, 657683 vertices), 10 substeps x 5 iterations",
+            "batched_vertex_substeps_per_s": vs / (tb / 1e3), "separate_vertex_substeps_per_s": vs / (ts / 1e3),
+            "separate_wall_vertex_substeps_per_s": vs / wall, "speedup_device": ts / tb,
+            "batched_ms_per_frame": tb / steps, "launch_config": {k: tune[k] for k in ("persistent", "blocks_per_sm")}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -178,6 +212,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -288,6 +323,8 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0 and world == 1 and not args.no_extras:
+        line["batched_config4"] = batch_extra(3)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -47,6 +47,22 @@ tc_status tc_create(tc_sim **out, const float *positions, uint32_t n, const uint
                     float compression_stiffness, float shear_stiffness, float bending_stiffness, int device);
 tc_status tc_destroy(tc_sim *s);
 
+/* Batched instances (new; the reference runs one cloth per simulator): one
+ * simulator over `ninst` independent cloths.  Per instance k: vcount[k]
+ * vertices, ecount[k] edges, fcount[k] faces (arrays concatenated, indices
+ * local to the instance), compliance[4k..4k+3] = tension, compression,
+ * shear, bending compliance, prim_count[k] primitive colliders of 10 floats
+ * each in `prims` (type 0 sphere / 1 capsule / 2 plane, friction,
+ * restitution, radius, a.xyz, b.xyz).  Vertex v of instance k is simulator
+ * vertex offsets[k] + v (tc_batch_instance_offsets); pins use these indices.
+ * Each instance evolves bit for bit as it would in its own simulator.
+ * Self-collision is off. */
+tc_status tc_batch_create(tc_sim **out, uint32_t ninst, const uint32_t *vcount, const uint32_t *ecount,
+                          const uint32_t *fcount, const float *positions, const uint32_t *edges, const uint32_t *faces,
+                          const float *inv_masses, float thickness, const float *compliance,
+                          const uint32_t *prim_count, const float *prims, int device);
+tc_status tc_batch_instance_offsets(tc_sim *s, uint32_t *offsets, uint32_t max_entries, uint32_t *n_instances);
+
 /* GpuClothSimulator::step (crates/cloth_core/src/simulation/dispatch.rs:610-671):
  * one frame of `substeps` substeps (0 -> 20), synchronous.  The frame is
  * recorded once into a CUDA graph and replayed while parameters are unchanged. */
@@ -161,6 +177,10 @@ tc_status tc_take_profile(tc_sim *s, char *names, size_t names_len, float *ms, u
  * return TC_ERR_TIMEOUT.  New; the reference dispatches one pass per colour
  * (dispatch.rs:1449-1455). */
 tc_status tc_set_persistent_solver(tc_sim *s, int enable);
+/* Launch shape of the persistent solver (blocks per SM, 1..limit) or the
+ * launch-per-colour path; used by the autotuner.  Results do not change. */
+tc_status tc_set_launch_config(tc_sim *s, int persistent, uint32_t blocks_per_sm);
+tc_status tc_get_launch_limits(tc_sim *s, uint32_t *max_blocks_per_sm, uint32_t *num_sms);
 /* Diagnostics for the failure path: runs one barrier that can never be
  * released, with the given poll limit (1..4194304), and returns
  * TC_ERR_TIMEOUT when every wait ended by the limit.  Touches no state. */

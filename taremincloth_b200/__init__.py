@@ -3,6 +3,6 @@
 ``ClothSimulator`` mirrors the reference's ``taremin_cloth_core.ClothSimulator``;
 all computation runs in the in-tree CUDA library ``libtcloth.so``.
 """
-from .simulator import ClothSimulator, get_gpu_device_name, is_gpu_available  # noqa: F401
+from .simulator import BatchedClothSimulator, ClothSimulator, get_gpu_device_name, is_gpu_available  # noqa: F401
 
-__all__ = ["ClothSimulator", "is_gpu_available", "get_gpu_device_name"]
+__all__ = ["ClothSimulator", "BatchedClothSimulator", "is_gpu_available", "get_gpu_device_name"]

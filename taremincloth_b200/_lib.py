@@ -26,6 +26,8 @@ SIGNATURES = {
     "tc_device_name": [_I, C.c_char_p, C.c_size_t],
     "tc_create": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F, _I],
     "tc_destroy": [_P],
+    "tc_batch_create": [C.POINTER(_P), _U, _P, _P, _P, _P, _P, _P, _P, _F, _P, _P, _P, _I],
+    "tc_batch_instance_offsets": [_P, _P, _U, C.POINTER(_U)],
     "tc_step": [_P, _F, _U, C.POINTER(_U)],
     "tc_step_async": [_P, _F, _U],
     "tc_fetch_positions": [_P, _P, C.c_size_t, C.POINTER(_I)],
@@ -68,6 +70,8 @@ SIGNATURES = {
     "tc_set_profiling_enabled": [_P, _I],
     "tc_frame_kernel_count": [_P, C.POINTER(_U)],
     "tc_set_persistent_solver": [_P, _I],
+    "tc_set_launch_config": [_P, _I, _U],
+    "tc_get_launch_limits": [_P, C.POINTER(_U), C.POINTER(_U)],
     "tc_check_barrier_timeout": [_P, _U],
     "tc_hash_build_static": [_P, _U, _F, _U, _P, _P, _P],
     "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],

@@ -103,13 +103,18 @@ struct Sim {
   DBuf<Prim> prims;
   DBuf<MeshTri> tris;
   DBuf<float4> bounds, cl16, cl256;
+  // batched instances (empty for a single cloth)
+  std::vector<uint32_t> inst_vert_off;  // n_instances + 1
+  std::vector<uint2> inst_prims_h;
+  DBuf<uint32_t> vinst;
+  DBuf<uint2> inst_prims;
   // pins
   std::map<uint32_t, PinH> pins;
   DBuf<uint32_t> pin_v;
   DBuf<float4> pin_t;
   // persistent solver (one cooperative launch per substep / frame)
   bool persistent = true;
-  unsigned int persist_blocks = 0;
+  unsigned int persist_blocks = 0, persist_max_per_sm = 0, num_sms = 0;
   unsigned int spin_limit = 1u << 22;  // ~0.5 s of polling per barrier
   DBuf<GridBar> bar;
   DBuf<uint32_t> dist_offc, dist_cntc, bend_offc, bend_cntc;
@@ -302,6 +307,8 @@ struct Sim {
       TC_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
       TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solver_persistent, 256, 0));
       persist_blocks = coop && per_sm > 0 ? unsigned(nsm * std::min(per_sm, 4)) : 0u;
+      persist_max_per_sm = unsigned(per_sm);
+      num_sms = unsigned(nsm);
       if (!persist_blocks) persistent = false;
     }
     pin_v.alloc(1); pin_t.alloc(1);
@@ -503,6 +510,8 @@ struct Sim {
     c.prims = prims.p; c.nprims = uint32_t(prims_h.size());
     c.tris = tris.p; c.bounds = bounds.p; c.cl16 = cl16.p; c.cl256 = cl256.p; c.ntris = uint32_t(tris_h.size());
     c.recovery = recovery;
+    c.vinst = inst_prims_h.empty() ? nullptr : vinst.p;
+    c.inst_prims = inst_prims_h.empty() ? nullptr : inst_prims.p;
     return c;
   }
 
@@ -759,6 +768,13 @@ using tcloth::TcError;
 struct tc_sim {
   Sim s;
 };
+static tcloth::Prim make_prim(uint32_t type, const float* a, const float* b, float r, float f, float rest) {
+  float tf;
+  std::memcpy(&tf, &type, 4);
+  return tcloth::Prim{make_float4(f, rest, r, tf), make_float4(a[0], a[1], a[2], 0.f),
+                      make_float4(b ? b[0] : 0.f, b ? b[1] : 0.f, b ? b[2] : 0.f, 0.f)};
+}
+
 
 static thread_local std::string g_err;
 
@@ -842,6 +858,98 @@ tc_status tc_create(tc_sim** out, const float* positions, uint32_t n, const uint
     std::unique_ptr<tc_sim> h(new tc_sim);
     h->s.init(in, device);
     *out = h.release();
+  });
+}
+
+// Batched instances: one simulator over the disjoint union of the instance
+// meshes.  Each constraint keeps its standalone colour (Welsh-Powell order
+// restricted to one instance is that instance's own order), so a batch
+// colour is the union of the instances' colours and every instance evolves
+// exactly as it would alone.  Each instance has its own compliances and
+// primitive colliders.
+tc_status tc_batch_create(tc_sim** out, uint32_t ninst, const uint32_t* vcount, const uint32_t* ecount,
+                          const uint32_t* fcount, const float* positions, const uint32_t* edges, const uint32_t* faces,
+                          const float* inv_masses, float thickness, const float* compliance,
+                          const uint32_t* prim_count, const float* prims, int device) {
+  return guard([&] {
+    need(out != nullptr && ninst > 0, "at least one instance");
+    need(vcount && ecount && fcount && positions && edges && compliance && prim_count, "instance arrays required");
+    *out = nullptr;
+    std::vector<uint32_t> voff(ninst + 1, 0);
+    uint64_t NE = 0, NF = 0, NP = 0;
+    for (uint32_t k = 0; k < ninst; ++k) {
+      voff[k + 1] = voff[k] + vcount[k];
+      NE += ecount[k]; NF += fcount[k]; NP += prim_count[k];
+    }
+    const uint32_t N = voff[ninst];
+    std::vector<uint32_t> ge(2 * NE), gf(3 * NF);
+    uint64_t eo = 0, fo = 0;
+    for (uint32_t k = 0; k < ninst; ++k) {
+      for (uint32_t e = 0; e < 2 * ecount[k]; ++e, ++eo) {
+        need(edges[eo] < vcount[k], "edge index >= instance vertex count");
+        ge[eo] = edges[eo] + voff[k];
+      }
+      for (uint32_t f = 0; f < 3 * fcount[k]; ++f, ++fo) {
+        need(faces[fo] < vcount[k], "face index >= instance vertex count");
+        gf[fo] = faces[fo] + voff[k];
+      }
+    }
+    std::vector<uint32_t> layers(N, 0u);
+    tcloth::MeshInput in;
+    in.pos = positions; in.n = N; in.edges = ge.data(); in.ne = uint32_t(NE);
+    in.faces = NF ? gf.data() : nullptr; in.nf = uint32_t(NF);
+    in.inv_masses = inv_masses; in.layer_ids = layers.data(); in.thickness = thickness;
+    in.tension_k = in.compression_k = in.shear_k = in.bending_k = 1000.f;
+    std::unique_ptr<tc_sim> h(new tc_sim);
+    Sim& m = h->s;
+    m.init(in, device);
+    m.self_collision = false;
+    // per-instance compliances (tension, compression, shear, bending)
+    std::vector<uint32_t> vi(N);
+    for (uint32_t k = 0; k < ninst; ++k)
+      for (uint32_t v = voff[k]; v < voff[k + 1]; ++v) vi[v] = k;
+    for (auto& c : m.dist_h) {
+      const float* cp = compliance + 4 * size_t(vi[c.v0]);
+      if (c.type == 1) c.tc = c.cc = cp[2];
+      else { c.tc = cp[0]; c.cc = cp[1]; }
+    }
+    for (auto& c : m.bend_h) {
+      const float b = compliance[4 * size_t(vi[c.v2]) + 3];
+      c.comp = c.pad0 > 1.5f ? std::fmax(b * 10.f, 0.5f) : b;
+    }
+    m.upload_dist();
+    m.upload_bend();
+    // per-instance primitives: 10 floats each (type, friction, restitution,
+    // radius, a.xyz, b.xyz); type 0 sphere, 1 capsule, 2 plane
+    m.inst_vert_off = voff;
+    m.inst_prims_h.resize(ninst);
+    uint32_t po = 0;
+    for (uint32_t k = 0; k < ninst; ++k) {
+      m.inst_prims_h[k] = make_uint2(po, prim_count[k]);
+      for (uint32_t q = 0; q < prim_count[k]; ++q, ++po) {
+        const float* f = prims + 10 * size_t(po);
+        const uint32_t type = uint32_t(f[0]);
+        need(type <= 2, "primitive type must be 0 (sphere), 1 (capsule) or 2 (plane)");
+        m.prims_h.push_back(make_prim(type, f + 4, f + 7, f[3], f[1], f[2]));
+      }
+    }
+    m.vinst.upload(vi, m.st);
+    m.inst_prims.upload(m.inst_prims_h, m.st);
+    m.upload_prims();
+    *out = h.release();
+  });
+}
+
+tc_status tc_batch_instance_offsets(tc_sim* s, uint32_t* offsets, uint32_t max_entries, uint32_t* n_instances) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(n_instances != nullptr, "n_instances required");
+    const uint32_t k = m.inst_vert_off.empty() ? 1u : uint32_t(m.inst_vert_off.size() - 1);
+    *n_instances = k;
+    if (offsets) {
+      for (uint32_t i = 0; i <= k && i < max_entries; ++i)
+        offsets[i] = m.inst_vert_off.empty() ? (i == 0 ? 0u : m.n) : m.inst_vert_off[i];
+    }
   });
 }
 
@@ -1013,12 +1121,6 @@ tc_status tc_set_collider_options(tc_sim* s, int cluster, int recovery, float sw
   });
 }
 
-static tcloth::Prim make_prim(uint32_t type, const float* a, const float* b, float r, float f, float rest) {
-  float tf;
-  std::memcpy(&tf, &type, 4);
-  return tcloth::Prim{make_float4(f, rest, r, tf), make_float4(a[0], a[1], a[2], 0.f),
-                      make_float4(b ? b[0] : 0.f, b ? b[1] : 0.f, b ? b[2] : 0.f, 0.f)};
-}
 tc_status tc_add_sphere_collider(tc_sim* s, const float c[3], float r, float f, float rest) {
   return guard([&] { Sim& m = S(s); need(c, "center required"); m.prims_h.push_back(make_prim(0, c, nullptr, r, f, rest)); m.upload_prims(); });
 }
@@ -1305,6 +1407,28 @@ tc_status tc_take_profile(tc_sim* s, char* names, size_t names_len, float* ms, u
     if (names && names_len) std::snprintf(names, names_len, "%s", joined.c_str());
     *n_entries = k;
     m.prof_names.clear(); m.prof_ms.clear(); m.prof_cnt.clear();
+  });
+}
+
+// Launch shape of the persistent solver: blocks per SM (1..occupancy limit).
+// Results do not depend on it (grid-stride loops, same per-element work).
+tc_status tc_set_launch_config(tc_sim* s, int persistent, uint32_t blocks_per_sm) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (persistent) {
+      need(m.persist_max_per_sm > 0, "cooperative launch is not available on this device");
+      need(blocks_per_sm >= 1 && blocks_per_sm <= m.persist_max_per_sm, "blocks_per_sm out of the occupancy range");
+      m.persist_blocks = m.num_sms * blocks_per_sm;
+    }
+    m.persistent = persistent != 0;
+    m.mark();
+  });
+}
+tc_status tc_get_launch_limits(tc_sim* s, uint32_t* max_blocks_per_sm, uint32_t* num_sms) {
+  return guard([&] {
+    Sim& m = S(s);
+    *max_blocks_per_sm = m.persist_max_per_sm;
+    *num_sms = m.num_sms;
   });
 }
 

@@ -319,6 +319,10 @@ __device__ __forceinline__ void mesh_triangle(const MeshTri& tri, float thicknes
 struct ColliderArgs {
   const Prim* prims;
   uint32_t nprims;
+  // batched instances: primitive range (offset, count) of each vertex's
+  // instance; null when every vertex sees every primitive
+  const uint32_t* vinst;
+  const uint2* inst_prims;
   const MeshTri* tris;
   const float4* bounds;   // per triangle: centroid, r
   const float4* cl16;     // per 16 triangles: conservative sphere for 1.5 r
@@ -349,7 +353,13 @@ __device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ 
   V3 p = mk(pr), pinit = p, xn = mk(x);
   const V3 xpos = mk(x);
   const float th = pr.w;
-  for (uint32_t k = 0; k < ca.nprims; ++k) {
+  uint32_t kb = 0, ke = ca.nprims;
+  if (ca.vinst) {
+    const uint2 r = ca.inst_prims[ca.vinst[i]];
+    kb = r.x;
+    ke = r.x + r.y;
+  }
+  for (uint32_t k = kb; k < ke; ++k) {
     const Prim c = ca.prims[k];
     const uint32_t type = __float_as_uint(c.h.w);
     const float fric = c.h.x, rest = c.h.y, r = c.h.z;

@@ -175,3 +175,71 @@ def build(sim_cls, scene, **kw):
         s.set_mesh_collider_triangles(m["triangles"], friction=m["friction"], thickness=m["thickness"],
                                       single_sided=m["single_sided"])
     return s
+
+
+def config4(n_instances=64, seed=0, side_range=(32, 192)):
+    """Uneven batch: grid sides log-uniform in side_range (1 cm spacing, two
+    triangles per quad, edges = quad edges), 2-8 pinned boundary vertices,
+    compliance log-uniform in [1e-9, 1e-5], 1-3 sphere / capsule colliders
+    below each cloth at seeded poses."""
+    rng = np.random.default_rng(seed)
+    lo, hi = side_range
+    instances = []
+    for k in range(n_instances):
+        u = rng.uniform()
+        side = int(lo * (hi / lo) ** u)
+        h = 0.01
+        L = (side - 1) * h
+        pos, edges, faces, idx = tri_grid(side, L, 0.0)
+        pos = pos.astype(F)
+        pos[:, 1] += rng.uniform(-1e-4, 1e-4, len(pos)).astype(F)
+        inv = areal_inv_masses(pos, faces, 0.15)
+        boundary = np.unique(np.concatenate([idx[0], idx[-1], idx[:, 0], idx[:, -1]]))
+        pins = rng.choice(boundary, size=int(rng.integers(2, 9)), replace=False)
+        c = float(10.0 ** rng.uniform(-9.0, -5.0))
+        cols = []
+        for _ in range(int(rng.integers(1, 4))):
+            r = float(rng.uniform(0.1, 0.3)) * L
+            ctr = (float(rng.uniform(0.3, 0.7) * L), float(-r - rng.uniform(0.01, 0.2) * L),
+                   float(rng.uniform(0.3, 0.7) * L))
+            if rng.uniform() < 0.5:
+                cols.append(("sphere", ctr, r, float(rng.uniform(0.1, 0.5))))
+            else:
+                a = (ctr[0] - 0.3 * L, ctr[1], ctr[2])
+                b = (ctr[0] + 0.3 * L, ctr[1], ctr[2] + 0.1 * L)
+                cols.append(("capsule", a, b, 0.5 * r, float(rng.uniform(0.1, 0.5))))
+        instances.append(dict(positions=pos, edges=edges, faces=faces, inv_masses=inv,
+                              compliance=(c, c, c * 100.0, 1e-5), colliders=cols,
+                              pins=[(int(v), pos[int(v)].copy()) for v in pins]))
+    return dict(name=f"config4_batch_{n_instances}", instances=instances, thickness=0.005,
+                gravity=(0.0, -9.81, 0.0), dt=1.0 / 60.0, substeps=10, iterations=5)
+
+
+def build_batch(scene, device=0):
+    from .simulator import BatchedClothSimulator
+    s = BatchedClothSimulator(scene["instances"], thickness=scene["thickness"], device=device)
+    s.set_gravity(*scene["gravity"])
+    s.set_solver_iterations(scene["iterations"])
+    for k, inst in enumerate(scene["instances"]):
+        for v, t in inst["pins"]:
+            s.set_pin(int(s.offsets[k]) + v, t, 1.0)
+    return s
+
+
+def build_instance(sim_cls, scene, k, **kw):
+    """One instance of a batch scene as its own simulator (oracle or product)."""
+    inst = scene["instances"][k]
+    s = sim_cls(inst["positions"], inst["edges"], inst["faces"], inst["inv_masses"], thickness=scene["thickness"],
+                layer_ids=np.zeros(len(inst["positions"]), np.uint32), **kw)
+    s.set_gravity(*scene["gravity"])
+    s.set_compliance_all(*inst["compliance"])
+    s.set_enable_self_collision(False)
+    s.set_solver_iterations(scene["iterations"])
+    for v, t in inst["pins"]:
+        s.set_pin(v, t, 1.0)
+    for c in inst["colliders"]:
+        if c[0] == "sphere":
+            s.add_sphere_collider(c[1], c[2], friction=c[3])
+        else:
+            s.add_capsule_collider(c[1], c[2], c[3], friction=c[4])
+    return s

@@ -351,6 +351,14 @@ class ClothSimulator:
         with bounded grid barriers between colours; off = one launch per colour."""
         self._c(self._L.tc_set_persistent_solver(self._h, int(bool(enable))))
 
+    def set_launch_config(self, persistent=True, blocks_per_sm=4):
+        self._c(self._L.tc_set_launch_config(self._h, int(bool(persistent)), int(blocks_per_sm)))
+
+    def get_launch_limits(self):
+        a, b = C.c_uint32(), C.c_uint32()
+        self._c(self._L.tc_get_launch_limits(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def check_barrier_timeout(self, spin_limit=1000):
         """Run a barrier that can never be released; raises BarrierTimeout."""
         self._c(self._L.tc_check_barrier_timeout(self._h, int(spin_limit)))
@@ -365,3 +373,58 @@ class ClothSimulator:
         v = C.c_float()
         self._c(self._L.tc_last_frame_ms(self._h, C.byref(v)))
         return v.value
+
+
+class BatchedClothSimulator(ClothSimulator):
+    """Many independent cloths in one simulator (one persistent launch per frame).
+
+    ``instances`` is a list of dicts with ``positions`` (N_k x 3), ``edges``,
+    ``faces``, optional ``inv_masses``, ``compliance`` = (tension,
+    compression, shear, bending) and ``colliders`` = list of
+    ``("sphere", center, radius, friction)`` or
+    ``("capsule", a, b, radius, friction)``.  Vertex ``v`` of instance ``k``
+    is simulator vertex ``offsets[k] + v``.  Each instance evolves exactly as
+    it would in its own ``ClothSimulator``.
+    """
+
+    def __init__(self, instances, thickness=0.005, device=0):
+        L = _lib.load()
+        self._h = None
+        pos, edges, faces, inv, comp, pcnt, prims = [], [], [], [], [], [], []
+        vc, ec, fc = [], [], []
+        for inst in instances:
+            p = _arr(inst["positions"], _f32, 3, "positions")
+            e = _arr(inst["edges"], _u32, 2, "edges")
+            f = _arr(inst.get("faces", np.zeros((0, 3), _u32)), _u32, 3, "faces")
+            pos.append(p); edges.append(e); faces.append(f)
+            vc.append(p.shape[0]); ec.append(e.shape[0]); fc.append(f.shape[0])
+            im = inst.get("inv_masses")
+            inv.append(np.ones(p.shape[0], _f32) if im is None else np.asarray(im, _f32).reshape(-1))
+            comp.append(np.asarray(inst["compliance"], _f32).reshape(4))
+            cols = inst.get("colliders", [])
+            pcnt.append(len(cols))
+            for c in cols:
+                if c[0] == "sphere":
+                    _, ctr, r, fr = c
+                    prims.append([0, fr, 0.0, r, *ctr, 0.0, 0.0, 0.0])
+                elif c[0] == "capsule":
+                    _, a, b, r, fr = c
+                    prims.append([1, fr, 0.0, r, *a, *b])
+                else:
+                    raise ValueError(f"unknown collider kind {c[0]!r}")
+        P = np.ascontiguousarray(np.concatenate(pos), _f32)
+        E = np.ascontiguousarray(np.concatenate(edges), _u32)
+        Fa = np.ascontiguousarray(np.concatenate(faces), _u32)
+        I = np.ascontiguousarray(np.concatenate(inv), _f32)
+        Cm = np.ascontiguousarray(np.stack(comp), _f32)
+        Pr = np.ascontiguousarray(np.asarray(prims, _f32).reshape(-1, 10))
+        arrs = [np.asarray(x, _u32) for x in (vc, ec, fc, pcnt)]
+        h = C.c_void_p()
+        _lib.check(L.tc_batch_create(C.byref(h), len(instances), _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]),
+                                     _ptr(P), _ptr(E), _ptr(Fa), _ptr(I), float(thickness), _ptr(Cm), _ptr(arrs[3]),
+                                     _ptr(Pr), int(device)))
+        self._h = h
+        self._L = L
+        self._n = P.shape[0]
+        self._solver_iterations = 2
+        self.offsets = np.concatenate([[0], np.cumsum(vc)]).astype(np.int64)

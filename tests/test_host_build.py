@@ -153,3 +153,22 @@ def test_invalid_index_raises_value_error():
 def test_empty_mesh():
     h = host_build(np.zeros((0, 3), np.float32), np.zeros((0, 2), np.uint32))
     assert h["n"] == 0 and h["nd"] == 0 and h["nb"] == 0
+
+
+def test_union_colouring_equals_instance_colourings():
+    """Batching relies on this: Welsh-Powell over a disjoint union of meshes
+    gives every constraint the colour it gets in its own mesh."""
+    sc = scenes.config4(n_instances=6, seed=3, side_range=(6, 20))
+    insts = sc["instances"]
+    off = np.concatenate([[0], np.cumsum([len(i["positions"]) for i in insts])])
+    union = host_build(np.concatenate([i["positions"] for i in insts]),
+                       np.concatenate([i["edges"] + off[k] for k, i in enumerate(insts)]),
+                       np.concatenate([i["faces"] + off[k] for k, i in enumerate(insts)]),
+                       layer_ids=np.zeros(off[-1], np.uint32))
+    ucol = np.repeat(np.arange(len(union["dist_cnt"])), union["dist_cnt"])
+    for k, inst in enumerate(insts):
+        h = host_build(inst["positions"], inst["edges"], inst["faces"])
+        icol = np.repeat(np.arange(len(h["dist_cnt"])), h["dist_cnt"])
+        mine = (union["dist_v"][:, 0] >= off[k]) & (union["dist_v"][:, 0] < off[k + 1])
+        np.testing.assert_array_equal(union["dist_v"][mine] - off[k], h["dist_v"])
+        np.testing.assert_array_equal(ucol[mine], icol)
