@@ -205,6 +205,50 @@ def batch_extra(steps):
             "batched_ms_per_frame": tb / steps, "launch_config": {k: tune[k] for k in ("persistent", "blocks_per_sm")}}
 
 
+def warm_start_extra(steps):
+    """Learned warm start on the config 4 batch: record plain-solver snapshots,
+    train, calibrate the residual threshold on the plain solver (RMS over all
+    constraints), then time frames with k of 5 iterations replaced.  Every
+    substep is judged; the fallback runs the full 5 iterations."""
+    from taremincloth_b200 import scenes, warmstart
+    sc = scenes.config4()
+    n = sum(len(i["positions"]) for i in sc["instances"])
+    dt, sub = sc["dt"], sc["substeps"]
+    b = scenes.build_batch(sc)
+    for _ in range(3):
+        b.step(dt, sub)
+    got, l0, l1 = warmstart.fit(b, dt, sub, frames=2, every=5, epochs=60, lr=2e-3, seed=0)
+    x0, _, v0 = b.get_state()
+    thr = warmstart.plain_residual(b, dt, sub, 2)
+
+    def timed(frames):
+        ms = 0.0
+        for _ in range(frames):
+            b.step(dt, sub)
+            ms += b.last_frame_ms()
+        return ms / frames
+
+    b.set_positions_and_velocities(x0, v0)
+    b.step(dt, sub)
+    plain_ms = timed(steps)
+    out = {"workload": "config 4 batch (64 cloths, 657683 vertices), 10 substeps x 5 iterations",
+           "snapshots": got, "train_loss_first_epoch": l0, "train_loss_last_epoch": l1,
+           "plain_rms_residual": thr, "plain_ms_per_frame": plain_ms,
+           "plain_vertex_substeps_per_s": n * sub / (plain_ms / 1e3)}
+    for k in (1, 2):
+        b.set_positions_and_velocities(x0, v0)
+        b.ws_enable(k, thr)
+        b.step(dt, sub)
+        b.ws_reset_stats()
+        ms = timed(steps)
+        st = b.ws_stats()
+        fb = st["fallbacks"] / max(st["substeps"], 1)
+        out[f"k{k}"] = {"ms_per_frame": ms, "vertex_substeps_per_s": n * sub / (ms / 1e3), "fallback_rate": fb,
+                        "iterations_saved_per_substep": k * (1.0 - fb), "last_rms_residual": st["last_residual"]}
+        b.ws_disable()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -325,6 +369,7 @@ def main():
         line["cpu_baseline"] = cpu_baseline_sample()
     if rank == 0 and world == 1 and not args.no_extras:
         line["batched_config4"] = batch_extra(3)
+        line["warm_start_config4"] = warm_start_extra(3)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

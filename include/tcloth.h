@@ -190,6 +190,44 @@ tc_status tc_frame_kernel_count(tc_sim *s, uint32_t *count);
 /* Device time of the latest frame in milliseconds (CUDA events). */
 tc_status tc_last_frame_ms(tc_sim *s, float *ms);
 
+/* Learned warm start; no counterpart in the reference.  A graph MLP (features
+ * -> 64, two message-passing rounds [self, neighbour mean] 128 -> 64, SiLU,
+ * head 64 -> 3; bf16 weights on the tensor cores, fp32 accumulation) predicts
+ * each vertex's correction p_final - p_predicted of the coming substep, in
+ * units of the vertex's local edge length.  While enabled, a substep moves p
+ * by that prediction, runs (iterations - k_replaced) plain XPBD iterations,
+ * computes the max constraint residual |C + alpha~ lambda| and, when it is
+ * above res_thresh (the plain solver's residual; +inf never falls back),
+ * runs the k_replaced remaining iterations.  Needs cooperative launch. */
+uint32_t tc_ws_param_count(void);
+tc_status tc_ws_enable(tc_sim *s, int enable, uint32_t k_replaced, float res_thresh);
+/* Record training snapshots during the following plain frames: every
+ * `every`-th substep until `capacity` snapshots are held; a new recording
+ * replaces the old snapshots, capacity 0 stops and keeps them.  Frames run
+ * without the CUDA graph while recording; results are unchanged. */
+tc_status tc_ws_record(tc_sim *s, uint32_t capacity, uint32_t every);
+tc_status tc_ws_recorded(tc_sim *s, uint32_t *count);
+/* Adam over the recorded snapshots (epochs x snapshots steps, seeded
+ * shuffle); mean MSE loss of the first and last epoch. */
+tc_status tc_ws_train(tc_sim *s, uint32_t epochs, float lr, uint64_t seed, float *loss_first, float *loss_last);
+/* fp32 parameter blob (tc_ws_param_count() floats): W0[16][64] b0[64]
+ * W1[128][64] b1[64] W2[128][64] b2[64] W3[64][3] b3[3], weights [in][out]. */
+tc_status tc_ws_get_params(tc_sim *s, float *out, size_t len);
+tc_status tc_ws_set_params(tc_sim *s, const float *params, size_t len);
+/* out = warm-started substeps, substeps that fell back, max residual of the
+ * latest substep's check, threshold */
+tc_status tc_ws_stats(tc_sim *s, double out[4]);
+tc_status tc_ws_reset_stats(tc_sim *s);
+/* Loss, parameter gradients and outputs of the warm-start network on one
+ * graph, through the same kernels as training (for gradient checks).
+ * feat n x 16 (rounded to bf16), adjacency CSR, target n x 3, mask n,
+ * loss = sum_i mask_i |y_i - target_i|^2 / (3 n).  y_infer (optional, n x 3)
+ * receives the outputs of the inference kernels (head fused into the last
+ * layer) that the warm-started substep runs. */
+tc_status tc_mlp_grad(uint32_t n, const float *feat, const uint32_t *adj_off, const uint32_t *adj_idx,
+                      const float *target, const float *mask, const float *params, float *loss, float *grads,
+                      float *y, float *y_infer, int device);
+
 /* Spatial-hash build that allocates nothing; no counterpart in the reference.
  * For callers that cannot allocate device memory: applications whose device
  * buffers all come from their own allocator, threads that must not call

@@ -75,6 +75,16 @@ SIGNATURES = {
     "tc_check_barrier_timeout": [_P, _U],
     "tc_hash_build_static": [_P, _U, _F, _U, _P, _P, _P],
     "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],
+    "tc_ws_param_count": [],
+    "tc_ws_enable": [_P, _I, _U, _F],
+    "tc_ws_record": [_P, _U, _U],
+    "tc_ws_recorded": [_P, C.POINTER(_U)],
+    "tc_ws_train": [_P, _U, _F, C.c_uint64, C.POINTER(_F), C.POINTER(_F)],
+    "tc_ws_get_params": [_P, _P, C.c_size_t],
+    "tc_ws_set_params": [_P, _P, C.c_size_t],
+    "tc_ws_stats": [_P, _P],
+    "tc_ws_reset_stats": [_P],
+    "tc_mlp_grad": [_U, _P, _P, _P, _P, _P, _P, C.POINTER(_F), _P, _P, _P, _I],
     "tc_mesh_build": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F],
     "tc_mesh_destroy": [_P],
     "tc_mesh_counts": [_P, _P, C.POINTER(_F)],
@@ -82,7 +92,7 @@ SIGNATURES = {
     "tc_mesh_topology_sizes": [_P, C.POINTER(_U), C.POINTER(_U), C.POINTER(_U)],
     "tc_mesh_topology": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
 }
-_RESTYPES = {"tc_last_error": C.c_char_p, "tc_gpu_available": _I}
+_RESTYPES = {"tc_last_error": C.c_char_p, "tc_gpu_available": _I, "tc_ws_param_count": _U}
 
 _lib = None
 

@@ -24,6 +24,7 @@
 #include "mesh.hpp"
 #include "selfcol_kernels.cuh"
 #include "solver_kernels.cuh"
+#include "warmstart.cuh"
 
 namespace tcloth {
 
@@ -64,6 +65,142 @@ struct DBuf {
 struct PinH {
   float target[3];
   float weight;
+};
+
+// The warm-start graph MLP: fp32 master parameters with Adam moments, bf16
+// copies for the tensor cores, inference activations and (allocated on first
+// use) the training buffers.  Forward and backward run over one graph (the
+// adjacency CSR of the cloth) on the owner's stream.
+struct Mlp {
+  cudaStream_t st = nullptr;
+  uint32_t n = 0;
+  const uint32_t* adj_off = nullptr;
+  const uint32_t* adj_idx = nullptr;
+  DBuf<float> w, gw, am, av;
+  DBuf<__nv_bfloat16> wb, wbt;
+  DBuf<__nv_bfloat16> h0, h1, h2;
+  DBuf<float> y;
+  DBuf<__nv_bfloat16> x1, x2, dz;
+  DBuf<float> z0, z1, z2, dy, dh, dx;
+  uint32_t adam_t = 0;
+
+  static unsigned grid(size_t cnt, unsigned b) { return unsigned((cnt + b - 1) / b); }
+  void setup(cudaStream_t s_, uint32_t n_, const uint32_t* ao, const uint32_t* ai) {
+    st = s_; n = n_; adj_off = ao; adj_idx = ai;
+    w.alloc(kP_N); gw.alloc(kP_N); am.alloc(kP_N); av.alloc(kP_N);
+    wb.alloc(kP_N); wbt.alloc(kT_N);
+    h0.alloc(size_t(n) * kWsH); h1.alloc(size_t(n) * kWsH); h2.alloc(size_t(n) * kWsH);
+    y.alloc(size_t(n) * 3);
+  }
+  void alloc_train() {
+    x1.alloc(size_t(n) * 128); x2.alloc(size_t(n) * 128); dz.alloc(size_t(n) * kWsH);
+    z0.alloc(size_t(n) * kWsH); z1.alloc(size_t(n) * kWsH); z2.alloc(size_t(n) * kWsH);
+    dy.alloc(size_t(n) * 3); dh.alloc(size_t(n) * kWsH); dx.alloc(size_t(n) * 128);
+  }
+  // seeded init: uniform(-1/sqrt(in), 1/sqrt(in)), the head scaled by 0.1 so
+  // that an untrained network moves vertices by little; zero biases
+  static std::vector<float> init_blob(uint64_t seed) {
+    std::vector<float> h(kP_N, 0.f);
+    uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
+    auto uni = [&]() {
+      x = x * 6364136223846793005ull + 1442695040888963407ull;
+      return float((x >> 40) & 0xFFFFFF) / float(1 << 24) * 2.f - 1.f;
+    };
+    auto fill = [&](uint32_t off, uint32_t cnt, float sc) { for (uint32_t e = 0; e < cnt; ++e) h[off + e] = uni() * sc; };
+    fill(kP_W0, kP_b0 - kP_W0, 1.f / std::sqrt(16.f));
+    fill(kP_W1, kP_b1 - kP_W1, 1.f / std::sqrt(128.f));
+    fill(kP_W2, kP_b2 - kP_W2, 1.f / std::sqrt(128.f));
+    fill(kP_W3, kP_b3 - kP_W3, 0.1f / std::sqrt(64.f));
+    return h;
+  }
+  void set_params(const float* h) {
+    TC_CK(cudaMemcpyAsync(w.p, h, kP_N * sizeof(float), cudaMemcpyHostToDevice, st));
+    TC_CK(cudaMemsetAsync(am.p, 0, kP_N * sizeof(float), st));
+    TC_CK(cudaMemsetAsync(av.p, 0, kP_N * sizeof(float), st));
+    adam_t = 0;
+    refresh();
+    TC_CK(cudaStreamSynchronize(st));
+  }
+  void get_params(float* h) {
+    TC_CK(cudaMemcpyAsync(h, w.p, kP_N * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaStreamSynchronize(st));
+  }
+  void refresh() { k_ws_refresh<<<grid(kP_N, 256), 256, 0, st>>>(w.p, wb.p, wbt.p); }
+
+  // Y = MLP(feat); with train, keeps X1, X2, Z0..Z2 and (with target) writes
+  // dY and adds the loss to *loss.
+  void forward(const __nv_bfloat16* feat, bool train, const float* target, const float* mask, float* loss) {
+    if (!n) return;
+    MlpLayerArgs a{};
+    a.n = n; a.adj_off = adj_off; a.adj_idx = adj_idx;
+    a.kin = kWsF; a.x_feat = feat; a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0;
+    a.z_out = train ? z0.p : nullptr; a.h_out = h0.p;
+    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    a.kin = 128; a.x_feat = nullptr; a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1;
+    a.x_out = train ? x1.p : nullptr; a.z_out = train ? z1.p : nullptr; a.h_out = h1.p;
+    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    a.h_prev = h1.p; a.wt = wbt.p + kT_W2; a.bias = w.p + kP_b2;
+    a.x_out = train ? x2.p : nullptr; a.z_out = train ? z2.p : nullptr; a.h_out = h2.p;
+    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    k_mlp_head<<<grid(n, 256), 256, 0, st>>>(n, h2.p, wb.p + kP_W3, w.p + kP_b3, y.p, target, mask,
+                                             1.0f / float(n), target ? dy.p : nullptr, loss);
+  }
+  // inference: the head is fused into the last layer, which either writes Y
+  // (y_out) or moves p by Y L on free vertices
+  void infer(const __nv_bfloat16* feat, float* y_out, const float4* x4, float4* p4, const float* local_len) {
+    if (!n) return;
+    MlpLayerArgs a{};
+    a.n = n; a.adj_off = adj_off; a.adj_idx = adj_idx;
+    a.kin = kWsF; a.x_feat = feat; a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0; a.h_out = h0.p;
+    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    a.kin = 128; a.x_feat = nullptr; a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1; a.h_out = h1.p;
+    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    a.h_prev = h1.p; a.wt = wbt.p + kT_W2; a.bias = w.p + kP_b2; a.h_out = nullptr;
+    a.w3 = wb.p + kP_W3; a.b3 = w.p + kP_b3; a.y_out = y_out; a.x4 = x4; a.p4 = p4; a.local_len = local_len;
+    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+  }
+  // gradients of the loss of the last forward(train, target) into gw
+  void backward(const __nv_bfloat16* feat) {
+    TC_CK(cudaMemsetAsync(gw.p, 0, kP_N * sizeof(float), st));
+    if (!n) return;
+    const unsigned gh = grid(size_t(n) * kWsH, 256), gt = grid(n, kWsRows);
+    k_mlp_head_bwd<<<grid(n, 256), 256, 0, st>>>(n, h2.p, wb.p + kP_W3, dy.p, dh.p, gw.p + kP_W3, gw.p + kP_b3);
+    k_mlp_act_bwd<<<gh, 256, 0, st>>>(n, dh.p, z2.p, dz.p, gw.p + kP_b2);
+    k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, 128, x2.p, dz.p, wb.p + kP_W2, gw.p + kP_W2, dx.p});
+    k_mlp_agg_bwd<<<gh, 256, 0, st>>>(n, dx.p, adj_off, adj_idx, dh.p);
+    k_mlp_act_bwd<<<gh, 256, 0, st>>>(n, dh.p, z1.p, dz.p, gw.p + kP_b1);
+    k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, 128, x1.p, dz.p, wb.p + kP_W1, gw.p + kP_W1, dx.p});
+    k_mlp_agg_bwd<<<gh, 256, 0, st>>>(n, dx.p, adj_off, adj_idx, dh.p);
+    k_mlp_act_bwd<<<gh, 256, 0, st>>>(n, dh.p, z0.p, dz.p, gw.p + kP_b0);
+    k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, kWsF, feat, dz.p, wb.p + kP_W0, gw.p + kP_W0, nullptr});
+  }
+  void adam(float lr) {
+    ++adam_t;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, float(adam_t)), c2 = 1.f - std::pow(b2, float(adam_t));
+    k_adam<<<grid(kP_N, 256), 256, 0, st>>>(kP_N, w.p, gw.p, am.p, av.p, lr, b1, b2, 1e-8f, c1, c2, nullptr, nullptr, 0, 0);
+    refresh();
+  }
+};
+
+// Learned warm start state of one simulator: the network, the correction of
+// the previous substep, the in-kernel residual judge and the recorded
+// training snapshots (features, target correction / L, free mask).
+struct WarmStart {
+  Mlp net;
+  bool ready = false;  // buffers allocated
+  bool on = false;
+  uint32_t k = 1;
+  float res_thresh = 0.f;
+  DBuf<float4> ppred, dprev;
+  DBuf<__nv_bfloat16> feat;
+  DBuf<float> adj_rest, res_max, res_part;
+  DBuf<unsigned int> fallbacks;
+  uint64_t substeps_run = 0;
+  // recording
+  uint32_t rec_cap = 0, rec_count = 0, rec_every = 1, rec_phase = 0;
+  DBuf<__nv_bfloat16> rec_feat;
+  DBuf<float> rec_target, rec_mask, losses;
 };
 
 struct Sim {
@@ -119,6 +256,7 @@ struct Sim {
   DBuf<GridBar> bar;
   DBuf<uint32_t> dist_offc, dist_cntc, bend_offc, bend_cntc;
   int* h_err = nullptr;  // pinned
+  WarmStart ws;
   // residual instrumentation
   bool track_residual = false;
   DBuf<float> res_sum, res_max;  // [ndc + nbc] each
@@ -210,6 +348,7 @@ struct Sim {
     x4.upload(hx, st);
     p4.upload(hp, st);
     v4.upload(hv, st);
+    if (ws.ready) TC_CK(cudaMemsetAsync(ws.dprev.p, 0, size_t(n) * sizeof(float4), st));
     TC_CK(cudaStreamSynchronize(st));
   }
 
@@ -536,6 +675,14 @@ struct Sim {
     a.bar = bar.p;
     a.expected = persist_blocks;
     a.spin_limit = spin_limit;
+    a.skip_predict = false;
+    a.ppred = nullptr;
+    a.dprev = nullptr;
+    a.iters_extra = 0;
+    a.res_thresh = 0.f;
+    a.res_part = nullptr;
+    a.res_out = nullptr;
+    a.fallbacks = nullptr;
     return a;
   }
   void launch_persistent(const SolverArgs& a) {
@@ -552,9 +699,123 @@ struct Sim {
     TC_CK(cudaLaunchKernelEx(&cfg, k_solver_persistent, a));
   }
 
+  // ---- learned warm start
+  void ws_setup() {
+    if (ws.ready) return;
+    ws.net.setup(st, n, adj_off.p, adj_idx.p);
+    const std::vector<float> blob = Mlp::init_blob(1);
+    ws.net.set_params(blob.data());
+    ws.ppred.alloc(n);
+    ws.dprev.alloc(n);
+    ws.feat.alloc(size_t(n) * kWsF);
+    std::vector<float> rest(m.adj_idx.size());
+    for (uint32_t i = 0; i < n; ++i)
+      for (uint32_t q = m.adj_off[i]; q < m.adj_off[i + 1]; ++q) {
+        const uint32_t j = m.adj_idx[q];
+        const float dx = init_pos[3 * i] - init_pos[3 * j], dy = init_pos[3 * i + 1] - init_pos[3 * j + 1],
+                    dz = init_pos[3 * i + 2] - init_pos[3 * j + 2];
+        rest[q] = std::sqrt(dx * dx + dy * dy + dz * dz);
+      }
+    ws.adj_rest.upload(rest, st);
+    ws.res_max.alloc(1);
+    ws.res_part.alloc(size_t(num_sms) * std::max(persist_max_per_sm, 4u));
+    ws.fallbacks.alloc(1);
+    TC_CK(cudaMemsetAsync(ws.dprev.p, 0, size_t(n) * sizeof(float4), st));
+    TC_CK(cudaMemsetAsync(ws.res_max.p, 0, sizeof(float), st));
+    TC_CK(cudaMemsetAsync(ws.fallbacks.p, 0, sizeof(unsigned int), st));
+    TC_CK(cudaStreamSynchronize(st));
+    ws.ready = true;
+  }
+  WsFeatArgs ws_feat_args(const SubstepParams& sp, __nv_bfloat16* feat) {
+    WsFeatArgs f;
+    f.n = n; f.x4 = x4.p; f.p4 = p4.p; f.v4 = v4.p; f.dprev = ws.dprev.p; f.local_len = local_len.p;
+    f.adj_off = adj_off.p; f.adj_idx = adj_idx.p; f.adj_rest = ws.adj_rest.p;
+    f.prims = prims.p; f.nprims = uint32_t(prims_h.size());
+    f.vinst = inst_prims_h.empty() ? nullptr : vinst.p;
+    f.inst_prims = inst_prims_h.empty() ? nullptr : inst_prims.p;
+    f.dt = sp.dt;
+    f.g_dt2 = std::sqrt(sp.gx * sp.gx + sp.gy * sp.gy + sp.gz * sp.gz) * sp.dt * sp.dt;
+    f.feat = feat;
+    return f;
+  }
+  bool ws_recording() const { return ws.ready && ws.rec_count < ws.rec_cap; }
+  // One frame with the warm start: per substep predict, features, MLP, move
+  // p by the predicted correction, then one persistent launch of iters - k
+  // iterations that judges the max residual against the plain solver's and
+  // runs k more when it misses.
+  void encode_frame_ws(float dt, uint32_t substeps, bool use_coupled) {
+    const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
+    const uint32_t kk = std::min(ws.k, iters > 1 ? iters - 1 : 0u);
+    const WsFeatArgs fa = ws_feat_args(sp, ws.feat.p);
+    for (uint32_t s = 0; s < substeps; ++s) {
+      timed("predict", [&] { k_predict<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp); });
+      timed("ws_mlp", [&] {
+        k_copy4<<<grid(n, 256), 256, 0, st>>>(n, p4.p, ws.ppred.p);
+        k_ws_features<<<grid(n, 128), 128, 0, st>>>(fa);
+        ws.net.infer(ws.feat.p, nullptr, x4.p, p4.p, local_len.p);
+      });
+      SolverArgs a = solver_args(sp, 1, use_coupled, !self_collision);
+      a.skip_predict = true;
+      a.iters = iters - kk;
+      a.iters_extra = kk;
+      a.ppred = ws.ppred.p;
+      a.dprev = ws.dprev.p;
+      a.res_thresh = ws.res_thresh;
+      a.res_part = ws.res_part.p;
+      a.res_out = ws.res_max.p;
+      a.fallbacks = ws.fallbacks.p;
+      timed("solver", [&] { launch_persistent(a); });
+      if (self_collision) {
+        encode_self_collision();
+        timed("update_vel", [&] { k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp.dt); });
+      }
+    }
+    TC_CK(cudaMemcpyAsync(h_err, &bar.p->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaGetLastError());
+  }
+  // train on the recorded snapshots: epochs x snapshots Adam steps in a
+  // seeded shuffled order; returns the mean loss of the first and last epoch
+  void ws_train(uint32_t epochs, float lr, uint64_t seed, float* first, float* last) {
+    if (!ws.ready || ws.rec_count == 0) throw TcError(TC_ERR_INVALID, "no recorded snapshots to train on");
+    if (epochs == 0) throw TcError(TC_ERR_INVALID, "epochs must be positive");
+    const uint32_t cnt = ws.rec_count;
+    ws.net.alloc_train();
+    ws.losses.alloc(size_t(epochs) * cnt);
+    TC_CK(cudaMemsetAsync(ws.losses.p, 0, size_t(epochs) * cnt * sizeof(float), st));
+    std::vector<uint32_t> order(cnt);
+    for (uint32_t i = 0; i < cnt; ++i) order[i] = i;
+    uint64_t x = seed * 2862933555777941757ull + 3037000493ull;
+    for (uint32_t ep = 0; ep < epochs; ++ep) {
+      for (uint32_t i = cnt; i > 1; --i) {
+        x = x * 6364136223846793005ull + 1442695040888963407ull;
+        std::swap(order[i - 1], order[uint32_t((x >> 33) % i)]);
+      }
+      for (uint32_t j = 0; j < cnt; ++j) {
+        const uint32_t sidx = order[j];
+        const __nv_bfloat16* f = ws.rec_feat.p + size_t(sidx) * n * kWsF;
+        ws.net.forward(f, true, ws.rec_target.p + size_t(sidx) * n * 3, ws.rec_mask.p + size_t(sidx) * n,
+                       ws.losses.p + size_t(ep) * cnt + j);
+        ws.net.backward(f);
+        ws.net.adam(lr);
+      }
+    }
+    std::vector<float> h(size_t(epochs) * cnt);
+    TC_CK(cudaMemcpyAsync(h.data(), ws.losses.p, h.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaStreamSynchronize(st));
+    TC_CK(cudaGetLastError());
+    double a = 0, b = 0;
+    for (uint32_t j = 0; j < cnt; ++j) { a += h[j]; b += h[size_t(epochs - 1) * cnt + j]; }
+    if (first) *first = float(a / cnt);
+    if (last) *last = float(b / cnt);
+  }
+
   // encode_simulation_steps (dispatch.rs:7-354) for one frame
   void encode_frame(float dt, uint32_t substeps, bool use_coupled) {
-    if (persistent && !profiling && !track_residual) {
+    if (ws.on && !ws_recording()) {
+      encode_frame_ws(dt, substeps, use_coupled);
+      return;
+    }
+    if (persistent && !profiling && !track_residual && !ws_recording()) {
       const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
       if (!self_collision) {
         launch_persistent(solver_args(sp, substeps, use_coupled, true));
@@ -580,6 +841,16 @@ struct Sim {
       if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
       if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
       timed("predict", [&] { k_predict<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp); });
+      // recording for the warm start: features after predict, the
+      // iterations' correction as the target
+      const bool rec = ws_recording();
+      const bool rec_this = rec && (ws.rec_phase++ % ws.rec_every) == 0;
+      const uint32_t slot = ws.rec_count;
+      if (rec) {
+        k_copy4<<<grid(n, 256), 256, 0, st>>>(n, p4.p, ws.ppred.p);
+        if (rec_this)
+          k_ws_features<<<grid(n, 128), 128, 0, st>>>(ws_feat_args(sp, ws.rec_feat.p + size_t(slot) * n * kWsF));
+      }
       for (uint32_t it = 0; it < iters; ++it) {
         if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
         timed("distance", [&] {
@@ -597,6 +868,12 @@ struct Sim {
         if (hascol && use_coupled) timed("collision", [&] { k_collision<<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts); });
       }
       if (track_residual && s + 1 == substeps) encode_residual(sp);
+      if (rec) {
+        k_ws_correction<<<grid(n, 256), 256, 0, st>>>(n, p4.p, ws.ppred.p, x4.p, local_len.p, ws.dprev.p,
+                                                      rec_this ? ws.rec_target.p + size_t(slot) * n * 3 : nullptr,
+                                                      rec_this ? ws.rec_mask.p + size_t(slot) * n : nullptr);
+        if (rec_this) ++ws.rec_count;
+      }
       if (hascol && !use_coupled) timed("collision", [&] { k_collision<<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts); });
       if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
       if (self_collision) encode_self_collision();
@@ -619,12 +896,13 @@ struct Sim {
   void launch_frame(float dt, uint32_t substeps) {
     if (n == 0) return;
     const bool use_coupled = coupled_for(dt, substeps);
-    if (profiling) {
+    if (ws.on && !ws_recording()) ws.substeps_run += substeps;
+    if (profiling || ws_recording()) {
       TC_CK(cudaEventRecord(ev0, st));
       encode_frame(dt, substeps, use_coupled);
       TC_CK(cudaEventRecord(ev1, st));
       TC_CK(cudaStreamSynchronize(st));
-      collect_marks();
+      if (profiling) collect_marks();
       return;
     }
     if (graph_dirty || !gexec || g_dt != dt || g_sub != substeps || g_coupled != use_coupled) {
@@ -1475,6 +1753,155 @@ tc_status tc_last_frame_ms(tc_sim* s, float* ms) {
     Sim& m = S(s);
     TC_CK(cudaEventSynchronize(m.ev1));
     TC_CK(cudaEventElapsedTime(ms, m.ev0, m.ev1));
+  });
+}
+
+// ---- learned warm start
+uint32_t tc_ws_param_count(void) { return tcloth::kP_N; }
+
+tc_status tc_ws_enable(tc_sim* s, int enable, uint32_t k_replaced, float res_thresh) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (!enable) { if (m.ws.on) m.mark(); m.ws.on = false; return; }
+    need(m.persist_blocks > 0, "the warm start needs cooperative launch (persistent solver)");
+    need(k_replaced >= 1 && k_replaced < m.iters, "k_replaced must be in [1, solver iterations - 1]");
+    need(std::isfinite(res_thresh) || res_thresh > 0.f, "res_thresh must be a number or +inf");
+    m.ws_setup();
+    m.ws.on = true;
+    m.ws.k = k_replaced;
+    m.ws.res_thresh = res_thresh;
+    m.mark();
+  });
+}
+
+tc_status tc_ws_record(tc_sim* s, uint32_t capacity, uint32_t every) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(every >= 1, "every must be >= 1");
+    m.ws_setup();
+    const size_t n = m.n;
+    if (capacity == 0) {  // stop recording, keep the snapshots
+      m.ws.rec_cap = m.ws.rec_count;
+      return;
+    }
+    {
+      m.ws.rec_feat.alloc(size_t(capacity) * n * tcloth::kWsF);
+      m.ws.rec_target.alloc(size_t(capacity) * n * 3);
+      m.ws.rec_mask.alloc(size_t(capacity) * n);
+    }
+    m.ws.rec_cap = capacity;
+    m.ws.rec_count = 0;
+    m.ws.rec_every = every;
+    m.ws.rec_phase = 0;
+    TC_CK(cudaMemsetAsync(m.ws.dprev.p, 0, n * sizeof(float4), m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+  });
+}
+
+tc_status tc_ws_recorded(tc_sim* s, uint32_t* count) {
+  return guard([&] { Sim& m = S(s); need(count != nullptr, "count required"); *count = m.ws.rec_count; });
+}
+
+tc_status tc_ws_train(tc_sim* s, uint32_t epochs, float lr, uint64_t seed, float* loss_first, float* loss_last) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(lr > 0.f && std::isfinite(lr), "lr must be positive");
+    m.ws_train(epochs, lr, seed, loss_first, loss_last);
+  });
+}
+
+tc_status tc_ws_get_params(tc_sim* s, float* out, size_t len) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr && len >= tcloth::kP_N, "output array too small");
+    m.ws_setup();
+    m.ws.net.get_params(out);
+  });
+}
+
+tc_status tc_ws_set_params(tc_sim* s, const float* params, size_t len) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(params != nullptr && len == tcloth::kP_N, "params must hold tc_ws_param_count() floats");
+    for (size_t i = 0; i < len; ++i) need(std::isfinite(params[i]), "params must be finite");
+    m.ws_setup();
+    m.ws.net.set_params(params);
+  });
+}
+
+tc_status tc_ws_stats(tc_sim* s, double out[4]) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr, "out required");
+    unsigned int fb = 0;
+    float rm = 0.f;
+    if (m.ws.ready) {
+      TC_CK(cudaMemcpyAsync(&fb, m.ws.fallbacks.p, sizeof fb, cudaMemcpyDeviceToHost, m.st));
+      TC_CK(cudaMemcpyAsync(&rm, m.ws.res_max.p, sizeof rm, cudaMemcpyDeviceToHost, m.st));
+      TC_CK(cudaStreamSynchronize(m.st));
+    }
+    out[0] = double(m.ws.substeps_run);
+    out[1] = double(fb);
+    out[2] = double(rm);
+    out[3] = double(m.ws.res_thresh);
+  });
+}
+
+tc_status tc_ws_reset_stats(tc_sim* s) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.ws.substeps_run = 0;
+    if (m.ws.ready) {
+      TC_CK(cudaMemsetAsync(m.ws.fallbacks.p, 0, sizeof(unsigned int), m.st));
+      TC_CK(cudaStreamSynchronize(m.st));
+    }
+  });
+}
+
+tc_status tc_mlp_grad(uint32_t n, const float* feat, const uint32_t* adj_off, const uint32_t* adj_idx,
+                      const float* target, const float* mask, const float* params, float* loss, float* grads,
+                      float* y, float* y_infer, int device) {
+  return guard([&] {
+    need(n > 0 && feat && adj_off && target && mask && params && loss && grads && y, "all arrays are required");
+    const uint32_t na = adj_off[n];
+    need(na == 0 || adj_idx != nullptr, "adj_idx required");
+    need(adj_off[0] == 0, "adj_off[0] must be 0");
+    for (uint32_t i = 0; i < n; ++i) need(adj_off[i + 1] >= adj_off[i], "adj_off must be non-decreasing");
+    for (uint32_t q = 0; q < na; ++q) need(adj_idx[q] < n, "adjacency index out of range");
+    TC_CK(cudaSetDevice(device));
+    cudaStream_t st = nullptr;
+    TC_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); } } sg{st};
+    tcloth::DBuf<uint32_t> d_off, d_idx;
+    tcloth::DBuf<float> d_t, d_m, d_loss;
+    tcloth::DBuf<__nv_bfloat16> d_f;
+    std::vector<__nv_bfloat16> hf(size_t(n) * tcloth::kWsF);
+    for (size_t e = 0; e < hf.size(); ++e) hf[e] = __float2bfloat16(feat[e]);
+    d_off.upload(adj_off, n + 1, st);
+    d_idx.upload(adj_idx, na, st);
+    d_t.upload(target, size_t(n) * 3, st);
+    d_m.upload(mask, n, st);
+    d_f.upload(hf, st);
+    d_loss.alloc(1);
+    TC_CK(cudaMemsetAsync(d_loss.p, 0, sizeof(float), st));
+    tcloth::Mlp net;
+    net.setup(st, n, d_off.p, d_idx.p);
+    net.alloc_train();
+    net.set_params(params);
+    net.forward(d_f.p, true, d_t.p, d_m.p, d_loss.p);
+    net.backward(d_f.p);
+    TC_CK(cudaMemcpyAsync(loss, d_loss.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaMemcpyAsync(grads, net.gw.p, tcloth::kP_N * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaMemcpyAsync(y, net.y.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (y_infer) {
+      tcloth::DBuf<float> d_yi;
+      d_yi.alloc(size_t(n) * 3);
+      net.infer(d_f.p, d_yi.p, nullptr, nullptr, nullptr);
+      TC_CK(cudaMemcpyAsync(y_infer, d_yi.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+      TC_CK(cudaStreamSynchronize(st));
+    }
+    TC_CK(cudaStreamSynchronize(st));
+    TC_CK(cudaGetLastError());
   });
 }
 

@@ -490,7 +490,39 @@ struct SolverArgs {
   GridBar* bar;
   unsigned int expected;  // arrivals per barrier
   unsigned int spin_limit;
+  // learned warm start: predict ran outside (skip_predict), the iteration
+  // correction p - p_pred goes to dprev, and after iters (the reduced count)
+  // the RMS residual |C + alpha~ lambda| over all distance and bending
+  // constraints decides whether iters_extra more iterations run
+  // (res_thresh: the plain solver's residual).  The sum is reduced in a
+  // fixed order (per block, then over res_part[] by every block), so every
+  // block takes the same decision and runs are bit-reproducible.
+  bool skip_predict;
+  const float4* ppred;
+  float4* dprev;
+  uint32_t iters_extra;
+  float res_thresh;
+  float* res_part;            // [gridDim.x] per-block sums of squares
+  float* res_out;             // RMS of the latest check
+  unsigned int* fallbacks;    // count of substeps that ran the extra iterations
 };
+
+__device__ __forceinline__ float residual_dist(uint32_t ci, const uint2* ids, const float4* par, const float4* p4,
+                                               const float* lam, float dt) {
+  const uint2 e = ids[ci];
+  const float4 c = par[ci];
+  const float cv = length(mk(__ldcg(p4 + e.x)) - mk(__ldcg(p4 + e.y))) - c.x;
+  const float comp = cv >= 0.f ? c.y : c.z;
+  return comp < 1e9f ? fabsf(cv + comp / (dt * dt) * __ldcg(lam + ci)) : 0.f;
+}
+__device__ __forceinline__ float residual_bend(uint32_t ci, const uint4* ids, const float4* par, const float4* p4,
+                                               const float* lam, float dt) {
+  const uint4 e = ids[ci];
+  const float4 c = par[ci];
+  if (c.y >= 1e9f) return 0.f;
+  const float cv = length(mk(__ldcg(p4 + e.z)) - mk(__ldcg(p4 + e.w))) - c.x;
+  return fabsf(cv + c.y / (dt * dt) * __ldcg(lam + ci));
+}
 
 // One cooperative launch runs `nsub` substeps of the constraint phase
 // (dispatch.rs:104-250: lambda clear, predict, iterations of pins / distance
@@ -505,9 +537,11 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
   for (uint32_t sub = 0; sub < a.nsub; ++sub) {
     for (uint32_t i = tid; i < a.nd; i += stride) a.dlam[i] = 0.f;
     for (uint32_t i = tid; i < a.nb; i += stride) a.blam[i] = 0.f;
-    for (uint32_t i = tid; i < a.n; i += stride) predict_vertex<true>(i, a.x4, a.p4, a.v4, a.sp);
+    if (!a.skip_predict)
+      for (uint32_t i = tid; i < a.n; i += stride) predict_vertex<true>(i, a.x4, a.p4, a.v4, a.sp);
     if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
-    for (uint32_t it = 0; it < a.iters; ++it) {
+    uint32_t n_it = a.iters;
+    for (uint32_t it = 0; it < n_it; ++it) {
       if (a.npins) {
         for (uint32_t k = tid; k < a.npins; k += stride) pin_one<true>(k, a.pin_v, a.pin_t, a.x4, a.p4, dts);
         if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
@@ -530,7 +564,51 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
         for (uint32_t i = tid; i < a.n; i += stride) collide_vertex<true>(i, a.x4, a.p4, a.ca, dts);
         if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
       }
+      if (it + 1 == a.iters && a.iters_extra > 0) {
+        __shared__ float red[8];
+        __shared__ int extra;
+        const float dt = fmaxf(dts, 1e-8f);
+        float r2 = 0.f;
+        for (uint32_t k = tid; k < a.nd; k += stride) {
+          const float r = residual_dist(k, a.dist_ids, a.dist_par, a.p4, a.dlam, dt);
+          r2 += r * r;
+        }
+        for (uint32_t k = tid; k < a.nb; k += stride) {
+          const float r = residual_bend(k, a.bend_ids, a.bend_par, a.p4, a.blam, dt);
+          r2 += r * r;
+        }
+        for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          float b = 0.f;
+          for (int w = 0; w < int(blockDim.x >> 5); ++w) b += red[w];
+          __stcg(a.res_part + blockIdx.x, b);
+        }
+        if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+        if (threadIdx.x < 32) {
+          float t = 0.f;
+          for (uint32_t q = threadIdx.x; q < gridDim.x; q += 32) t += __ldcg(a.res_part + q);
+          for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+          if (threadIdx.x == 0) {
+            const float rms = sqrtf(t / float(max(a.nd + a.nb, 1u)));
+            extra = rms > a.res_thresh ? 1 : 0;
+            if (blockIdx.x == 0) {
+              *a.res_out = rms;
+              if (extra) atomicAdd(a.fallbacks, 1u);
+            }
+          }
+        }
+        __syncthreads();
+        if (extra) n_it = a.iters + a.iters_extra;
+        // res_part is rewritten at the next check only after further barriers
+      }
     }
+    if (a.dprev)
+      for (uint32_t i = tid; i < a.n; i += stride) {
+        const float4 p = __ldcg(a.p4 + i), q = a.ppred[i];
+        a.dprev[i] = make_float4(p.x - q.x, p.y - q.y, p.z - q.z, 0.f);
+      }
     if (a.hascol && !a.coupled) {
       for (uint32_t i = tid; i < a.n; i += stride) collide_vertex<true>(i, a.x4, a.p4, a.ca, dts);
       if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;

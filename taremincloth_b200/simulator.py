@@ -374,6 +374,51 @@ class ClothSimulator:
         self._c(self._L.tc_last_frame_ms(self._h, C.byref(v)))
         return v.value
 
+    # ---- learned warm start (new; no counterpart in the reference)
+    def ws_enable(self, k_replaced=1, res_thresh=float("inf")):
+        """Warm-start every substep with the graph MLP, run iterations - k
+        plain iterations, and the k others when the max residual is above
+        res_thresh (the plain solver's residual)."""
+        self._c(self._L.tc_ws_enable(self._h, 1, int(k_replaced), float(res_thresh)))
+
+    def ws_disable(self):
+        self._c(self._L.tc_ws_enable(self._h, 0, 0, 0.0))
+
+    def ws_record(self, capacity, every=1):
+        """Record `capacity` training snapshots, one every `every` substeps,
+        during the following plain frames."""
+        self._c(self._L.tc_ws_record(self._h, int(capacity), int(every)))
+
+    def ws_recorded(self):
+        v = C.c_uint32()
+        self._c(self._L.tc_ws_recorded(self._h, C.byref(v)))
+        return v.value
+
+    def ws_train(self, epochs=50, lr=1e-3, seed=0):
+        """Adam on the recorded snapshots; (mean loss of the first epoch, of the last)."""
+        a, b = C.c_float(), C.c_float()
+        self._c(self._L.tc_ws_train(self._h, int(epochs), float(lr), int(seed), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def ws_params(self):
+        out = np.zeros(self._L.tc_ws_param_count(), _f32)
+        self._c(self._L.tc_ws_get_params(self._h, _ptr(out), out.size))
+        return out
+
+    def ws_set_params(self, params):
+        p = _arr(params, _f32).ravel()
+        self._c(self._L.tc_ws_set_params(self._h, _ptr(p), p.size))
+
+    def ws_stats(self):
+        """{'substeps', 'fallbacks', 'last_residual', 'threshold'}"""
+        out = np.zeros(4, np.float64)
+        self._c(self._L.tc_ws_stats(self._h, _ptr(out)))
+        return {"substeps": int(out[0]), "fallbacks": int(out[1]), "last_residual": float(out[2]),
+                "threshold": float(out[3])}
+
+    def ws_reset_stats(self):
+        self._c(self._L.tc_ws_reset_stats(self._h))
+
 
 class BatchedClothSimulator(ClothSimulator):
     """Many independent cloths in one simulator (one persistent launch per frame).

@@ -1,0 +1,129 @@
+"""Learned warm start on the GPU.
+
+* The tensor-core forward/backward kernels against the numpy reference of
+  the network (loss, outputs, every parameter gradient; bf16 rounding points
+  emulated, tolerance 2e-2 of each tensor's norm).
+* With an all-zero network the warm-started substep is the plain solver:
+  threshold +inf gives the bits of (iterations - k) plain iterations,
+  threshold -1 (always fall back) the bits of the full iteration count.
+* Trained on plain-solver snapshots, the network lowers the RMS constraint
+  residual that (iterations - k) iterations leave, against no warm start.
+"""
+import numpy as np
+import pytest
+
+from oracle import warmstart_ref as W
+from taremincloth_b200 import ClothSimulator, scenes, warmstart
+
+pytestmark = pytest.mark.gpu
+
+
+def _nrel(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_mlp_grad_matches_reference(seed):
+    rng = np.random.default_rng(seed)
+    off, idx = W.grid_graph(20, 21)  # 420 vertices: 7 tiles of 64 rows, the last one ragged
+    n = 420
+    feat = rng.normal(0, 1, (n, 16)).astype(np.float32)
+    target = rng.normal(0, 0.3, (n, 3)).astype(np.float32)
+    mask = (rng.random(n) > 0.1).astype(np.float32)
+    blob = W.random_params(rng)
+    loss_g, grad_g, y_g, y_inf = warmstart.mlp_grad(feat, off, idx, target, mask, blob, with_inference=True)
+    loss_r, grad_r, y_r = W.forward_backward(feat, off, idx, target, mask, blob)
+    assert abs(loss_g - loss_r) <= 1e-3 * abs(loss_r)
+    assert _nrel(y_g, y_r) <= 5e-3
+    assert _nrel(y_inf, y_r) <= 5e-3  # fused inference head
+    for name, o, shape in W.LAYOUT:
+        k = int(np.prod(shape))
+        e = _nrel(grad_g[o:o + k], grad_r[o:o + k])
+        assert e <= 2e-2, (name, e)
+
+
+def _state(sim):
+    x, _, v = sim.get_state()
+    return x.copy(), v.copy()
+
+
+def _restore(sim, st):
+    sim.set_positions_and_velocities(st[0], st[1])
+
+
+def _scene_sims(scene, n_sims):
+    return [scenes.build(ClothSimulator, scene) for _ in range(n_sims)]
+
+
+@pytest.mark.parametrize("which", ["config1", "config2_small"])
+def test_zero_network_is_the_plain_solver(which):
+    sc = scenes.config1() if which == "config1" else scenes.config2(n=24, subdiv=2)
+    it, k = sc["iterations"], 2
+    a, b, c, d = _scene_sims(sc, 4)
+    zeros = np.zeros(warmstart.PARAM_COUNT, np.float32)
+    for s in (a, c):
+        s.ws_set_params(zeros)
+    a.ws_enable(k, float("inf"))
+    b.set_solver_iterations(it - k)
+    c.ws_enable(k, -1.0)
+    frames = 3
+    for _ in range(frames):
+        for s in (a, b, c, d):
+            s.step(sc["dt"], sc["substeps"])
+    xa, xb, xc, xd = (_state(s)[0] for s in (a, b, c, d))
+    assert np.array_equal(xa, xb)
+    assert np.array_equal(xc, xd)
+    st_a, st_c = a.ws_stats(), c.ws_stats()
+    assert st_a["substeps"] == st_c["substeps"] == frames * sc["substeps"]
+    assert st_a["fallbacks"] == 0 and st_c["fallbacks"] == frames * sc["substeps"]
+    assert st_a["last_residual"] > 0.0
+
+
+def test_invalid_warm_start_arguments():
+    sc = scenes.config1()
+    s = scenes.build(ClothSimulator, sc)
+    with pytest.raises(ValueError):
+        s.ws_enable(sc["iterations"], 1.0)  # k must leave at least one plain iteration
+    with pytest.raises(ValueError):
+        s.ws_enable(0, 1.0)
+    with pytest.raises(ValueError):
+        s.ws_set_params(np.zeros(10, np.float32))
+    with pytest.raises(ValueError):
+        s.ws_train(10, 1e-3)  # nothing recorded
+
+
+def test_trained_warm_start_gains_over_no_warm_start():
+    sc = scenes.config1()
+    dt, sub, it, k = sc["dt"], sc["substeps"], sc["iterations"], 2
+    s = scenes.build(ClothSimulator, sc)
+    for _ in range(4):
+        s.step(dt, sub)
+    got, l0, l1 = warmstart.fit(s, dt, sub, frames=10, every=2, epochs=60, lr=2e-3, seed=0)
+    assert got == 50
+    assert l1 < 0.5 * l0, (l0, l1)
+    trained = s.ws_params()
+    start = _state(s)
+
+    def run(params, enable):
+        _restore(s, start)
+        if enable:
+            s.ws_set_params(params)
+            s.ws_enable(k, float("inf"))
+        else:
+            s.ws_disable()
+        s.step(dt, sub)
+        out = _state(s)[0].astype(np.float64)
+        res = s.ws_stats()["last_residual"] if enable else None
+        s.ws_disable()
+        return out, res
+
+    full, _ = run(None, False)
+    x_zero, r_zero = run(np.zeros_like(trained), True)
+    x_ws, r_ws = run(trained, True)
+    e_zero = float(np.sqrt(np.mean((x_zero - full) ** 2)))
+    e_ws = float(np.sqrt(np.mean((x_ws - full) ** 2)))
+    print(f"after {it - k} of {it} iterations: RMS residual no warm start {r_zero:.3e}, learned {r_ws:.3e}; "
+          f"rms distance to the {it}-iteration positions {e_zero:.3e} vs {e_ws:.3e}")
+    assert r_ws < r_zero
