@@ -205,6 +205,40 @@ def batch_extra(steps):
             "batched_ms_per_frame": tb / steps, "launch_config": {k: tune[k] for k in ("persistent", "blocks_per_sm")}}
 
 
+def bone_sdf_extra(steps):
+    """Config 3: ~100k-vertex tube garment on a 20-bone capsule mannequin
+    (~30k body vertices, 4 weights each) with the dynamic bone SDF: every
+    frame the pose advances (+-40 degrees over 120 frames), the body is
+    skinned, every bone's 64^3 tile is rebaked, then 10 substeps x 4
+    iterations run.  Device time per frame includes the rebake."""
+    from taremincloth_b200 import ClothSimulator, scenes
+    sc = scenes.config3()
+    s, bake, order = scenes.build_config3(ClothSimulator, sc)
+    body = sc["body"]
+    n = len(sc["positions"])
+    dt, sub = sc["dt"], sc["substeps"]
+
+    def frame(f):
+        w, iw = scenes.shader_mats(scenes.pose(body, f)[order])
+        s.update_bone_transforms(w, iw)
+        s.step(dt, sub)
+        return s.last_frame_ms()
+
+    for f in range(3):
+        frame(f)
+    ms = sum(frame(3 + f) for f in range(steps)) / steps
+    s.set_profiling_enabled(True)
+    frame(3 + steps)
+    prof = {k: round(v, 3) for k, v, _ in s.take_profile()}
+    s.set_profiling_enabled(False)
+    x, _, _ = s.get_state()
+    return {"workload": f"tube garment {n} vertices, mannequin {len(body['verts'])} vertices / 20 bones, "
+                        f"atlas {bake['width']}x{bake['height']}x{bake['depth']} fp16x2, rebake every frame, "
+                        f"{sub} substeps x {sc['iterations']} iterations",
+            "ms_per_frame": ms, "vertex_substeps_per_s": n * sub / (ms / 1e3),
+            "profile_ms_per_frame": prof, "finite": bool(np.isfinite(x).all())}
+
+
 def warm_start_extra(steps):
     """Learned warm start on the config 4 batch: record plain-solver snapshots,
     train, calibrate the residual threshold on the plain solver (RMS over all
@@ -379,6 +413,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         line["batched_config4"] = batch_extra(3)
         line["warm_start_config4"] = warm_start_extra(3)
+        line["bone_sdf_config3"] = bone_sdf_extra(3)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

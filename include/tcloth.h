@@ -109,6 +109,58 @@ tc_status tc_set_mesh_collider_triangles(tc_sim *s, const float *triangles, uint
                                          float thickness, float restitution, int single_sided, const float *attributes);
 tc_status tc_clear_colliders(tc_sim *s);
 
+/* Bone SDF colliders (lib.rs:2245-2600, simulation/mod.rs:1630-2464).  The
+ * atlas is width x height x depth texels of packed half2 (distance in the low
+ * 16 bits, alpha in the high 16), z-major then y then x: the reference's
+ * Rg16Float texture bytes read as uint32.  bone_infos: n_bones rows of 20
+ * floats (aabb_min 4, aabb_max 4, uvw_scale 4, uvw_offset 4, friction,
+ * thickness, restitution, weight threshold).  Matrices: 16 floats per bone in
+ * the reference's GpuBoneTransform order (column-major: row j, column k at
+ * [k*4 + j]).  Sampling is trilinear with clamp-to-edge in fp32. */
+tc_status tc_set_bone_sdf_colliders(tc_sim *s, uint32_t width, uint32_t height, uint32_t depth,
+                                    const uint32_t *texels, size_t n_texels, const float *bone_infos,
+                                    uint32_t n_bones);
+/* dirty: bones to rebake at the next dynamic update; n_dirty < 0 = all
+ * (None), 0 = none (the reference skips the rebake) */
+tc_status tc_update_bone_transforms(tc_sim *s, const float *world, const float *inv_world, uint32_t n_bones,
+                                    const uint32_t *dirty, int64_t n_dirty);
+tc_status tc_set_dynamic_bone_sdf_dirty_bones(tc_sim *s, const uint32_t *dirty, int64_t n_dirty);
+tc_status tc_clear_bone_sdf_colliders(tc_sim *s);
+/* Dynamic bone SDF: before a frame (every update_interval frames) skin the
+ * body (4 bone indices / weights per vertex, rest_cols >= 3 floats per rest
+ * vertex), move each source triangle (i0, i1, i2, bone; weights w0, w1, w2)
+ * into its bone's frame and rebake the bones' res^3 tiles on the GPU.
+ * bind_inv: row-major, as lib.rs:2550-2562.  Indices must be in range
+ * (TC_ERR_INVALID), where the reference reads out of its buffers. */
+tc_status tc_setup_dynamic_bone_sdf(tc_sim *s, uint32_t width, uint32_t height, uint32_t depth, uint32_t res,
+                                    const float *bone_infos, uint32_t n_bones, const float *rest_verts,
+                                    uint32_t rest_cols, const uint32_t *bone_indices, const float *bone_weights,
+                                    uint32_t n_verts, const uint32_t *tri_sources, const float *tri_weights,
+                                    uint32_t n_tris, const float *bind_inv, uint32_t n_bind,
+                                    uint32_t update_interval);
+tc_status tc_set_dynamic_bone_sdf_enabled(tc_sim *s, int enable);
+tc_status tc_set_dynamic_bone_sdf_update_interval(tc_sim *s, uint32_t interval);
+/* Read back the atlas (dims = width, height, depth; out may be NULL) and the
+ * bone infos including the world bounding spheres in their .w slots. */
+tc_status tc_get_bone_sdf_atlas(tc_sim *s, uint32_t *out, size_t len, uint32_t dims[3]);
+tc_status tc_get_bone_infos(tc_sim *s, float *out, size_t len, uint32_t *n_bones);
+
+/* bake_bone_sdf_gpu (lib.rs:1186-1350, sdf_baker.rs:465-940): bone-local SDF
+ * atlas of a skinned mesh.  bone_weights: n_bones rows of n_verts;
+ * bind_matrices: n_bones row-major 4x4 (mesh -> bone local).  Fails with
+ * TC_ERR_CUDA (RuntimeError) when no bone has a weight above the threshold. */
+typedef struct tc_bake tc_bake;
+tc_status tc_bake_bone_sdf(const float *mesh_verts, uint32_t n_verts, const int32_t *mesh_tris, uint32_t n_tris,
+                           uint32_t n_bones, const float *bone_weights, const float *bind_matrices,
+                           uint32_t resolution, float margin, float weight_threshold, float blend_k, float friction,
+                           float thickness, float restitution, int close_open_boundaries, int device, tc_bake **out);
+/* out = width, height, depth, number of active bones */
+tc_status tc_bake_dims(tc_bake *b, uint32_t out[4]);
+/* texels (w*h*d), infos (n_active x 20), active (source bone index per
+ * active bone), bind (n_active x 16); any may be NULL */
+tc_status tc_bake_get(tc_bake *b, uint32_t *texels, float *infos, uint32_t *active, float *bind);
+tc_status tc_bake_destroy(tc_bake *b);
+
 /* pins (simulation/mod.rs:2768-2860) */
 tc_status tc_set_pin(tc_sim *s, uint32_t vertex, const float target[3], float weight);
 tc_status tc_set_pins_batch(tc_sim *s, const uint32_t *idx, const float *targets, const float *weights, uint32_t count);

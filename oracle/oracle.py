@@ -75,6 +75,12 @@ def lib():
         L.ocl_cell_size.restype = C.c_float
         L.ocl_build_hash.argtypes = [P, C.c_int, up, up]
         L.ocl_get_mesh_triangles.argtypes = [P, fp]
+        L.ocl_half_roundtrip.argtypes = [P, C.c_int, P, P]
+        L.ocl_bone_skin_mats.argtypes = [C.c_int, P, P, P]
+        L.ocl_bone_skin.argtypes = [C.c_int, P, P, P, P, P]
+        L.ocl_bone_prep.argtypes = [C.c_int, P, P, P, P, P]
+        L.ocl_bone_bake.argtypes = [C.c_int, P, P, P]
+        L.ocl_set_bone_sdf.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, P, C.c_int, P, P]
         _lib = L
     return _lib
 
@@ -261,3 +267,74 @@ class OracleSim:
         srt = np.zeros(max(cnt, 1), _u)
         lib().ocl_build_hash(self._h, which, cs, srt)
         return cs, srt[:cnt]
+
+
+# --- bone SDF (skinning.wgsl, prep_bone_triangles.wgsl, bake_sdf.wgsl) -----
+def half_roundtrip(x):
+    """(binary16 bits, value back in float32) with round to nearest even."""
+    x = np.ascontiguousarray(x, _f).ravel()
+    bits = np.zeros(x.size, np.uint16)
+    out = np.zeros(x.size, _f)
+    lib().ocl_half_roundtrip(_ptr(x), x.size, _ptr(bits), _ptr(out))
+    return bits, out
+
+
+def bone_skin_mats(world, bind_inv):
+    """S = M_world B_bind per bone (column-major out), as the host does before skinning.
+    world: (N, 4, 4) as stored for the shaders; bind_inv: (N, 4, 4) row-major."""
+    w = np.ascontiguousarray(world, _f).reshape(-1, 16)
+    x = np.zeros((w.shape[0], 32), _f)
+    x[:, :16] = w
+    b = np.ascontiguousarray(bind_inv, _f).reshape(-1, 16)
+    out = np.zeros((w.shape[0], 16), _f)
+    lib().ocl_bone_skin_mats(w.shape[0], _ptr(x), _ptr(b), _ptr(out))
+    return out
+
+
+def bone_skin(rest, bidx, bw, skin_mats):
+    nv = rest.shape[0]
+    r4 = np.zeros((nv, 4), _f)
+    r4[:, :3] = rest[:, :3]
+    out = np.zeros((nv, 4), _f)
+    lib().ocl_bone_skin(nv, _ptr(r4), _ptr(np.ascontiguousarray(bidx, _u)), _ptr(np.ascontiguousarray(bw, _f)),
+                        _ptr(np.ascontiguousarray(skin_mats, _f)), _ptr(out))
+    return out
+
+
+def bone_prep(skinned4, inv_mats, src4, srcw4):
+    nt = src4.shape[0]
+    out = np.zeros((nt, 16), _f)
+    lib().ocl_bone_prep(nt, _ptr(np.ascontiguousarray(skinned4, _f)), _ptr(np.ascontiguousarray(inv_mats, _f)),
+                        _ptr(np.ascontiguousarray(src4, _u)), _ptr(np.ascontiguousarray(srcw4, _f)), _ptr(out))
+    return out
+
+
+def bone_bake(params16, tris16, dims):
+    """params16: (P, 16) uint32 words of the bake parameters; returns the atlas texels."""
+    W, H, D = dims
+    atlas = np.zeros(W * H * D, _u)
+    p = np.ascontiguousarray(params16, _u)
+    lib().ocl_bone_bake(p.shape[0], _ptr(p), _ptr(np.ascontiguousarray(tris16, _f)), _ptr(atlas))
+    return atlas
+
+
+def bake_params_words(lmin, tri_start, lmax, tri_count, col, row, layer, res, W, H, D, pitch=0):
+    w = np.zeros(16, _u)
+    w[0:3] = np.asarray(lmin, _f).view(_u)
+    w[3] = tri_start
+    w[4:7] = np.asarray(lmax, _f).view(_u)
+    w[7] = tri_count
+    w[8:16] = [col, row, layer, res, W, H, D, pitch]
+    return w
+
+
+def _set_bone_sdf(self, dims, atlas, infos, xforms32):
+    W, H, D = dims
+    a = np.ascontiguousarray(atlas, _u)
+    i = np.ascontiguousarray(infos, _f).reshape(-1, 20)
+    x = np.ascontiguousarray(xforms32, _f).reshape(-1, 32)
+    self._keep_bone = (a, i, x)
+    lib().ocl_set_bone_sdf(self._h, W, H, D, _ptr(a), i.shape[0], _ptr(i), _ptr(x))
+
+
+OracleSim.set_bone_sdf = _set_bone_sdf

@@ -164,6 +164,10 @@ struct OSim {
     float last_max_disp, last_eff_disp;
     float cloth_thickness;
     int single_sided_recovery;
+    /* bone SDF colliders (collision.wgsl:116-265) */
+    uint32_t *atlas; uint32_t aw, ah, ad; int nbones;
+    float *binfo;   /* nbones x 20 */
+    float *bxf;     /* nbones x 32: world, inverse world (column-major) */
     /* colliders */
     OCol *cols; int ncols;
     OTri *tris; float *bounds; int ntris;
@@ -782,7 +786,8 @@ void ocl_destroy(OSim *s) {
                     s->dc_off, s->dc_cnt, s->dlam, s->bend, s->bc_off, s->bc_cnt, s->blam,
                     s->adj_off, s->adj_idx, s->th_off, s->th_idx, s->th_rest, s->local_len,
                     s->star_off, s->star_idx, s->edges, s->ebits, s->island, s->cols, s->tris,
-                    s->bounds, s->pins, s->acc, s->nrm, s->cs, s->srt, s->ecs, s->esrt};
+                    s->bounds, s->pins, s->acc, s->nrm, s->cs, s->srt, s->ecs, s->esrt,
+                    s->atlas, s->binfo, s->bxf};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(s);
 }
@@ -1147,6 +1152,324 @@ static void mesh_tri(const OTri *tri, float thickness, v3 xpos, v3 *p, v3 *xn, f
     }
 }
 /* shaders/collision.wgsl:378-652 (cluster culling OFF, the default) */
+/* ------------------------------------------------------------------ */
+/* Bone SDF: skinning.wgsl:16-43, prep_bone_triangles.wgsl:30-67,       */
+/* bake_sdf.wgsl:33-196, collision.wgsl:116-265.  Matrices column-major  */
+/* (row j, column k at [k*4 + j]) as GpuBoneTransform.                   */
+/* ------------------------------------------------------------------ */
+static inline v3 xf_point(const float *m, v3 p) {
+    return V3(((m[0] * p.x + m[4] * p.y) + m[8] * p.z) + m[12], ((m[1] * p.x + m[5] * p.y) + m[9] * p.z) + m[13],
+              ((m[2] * p.x + m[6] * p.y) + m[10] * p.z) + m[14]);
+}
+static inline v3 xf_dir(const float *m, v3 p) {
+    return V3((m[0] * p.x + m[4] * p.y) + m[8] * p.z, (m[1] * p.x + m[5] * p.y) + m[9] * p.z,
+              (m[2] * p.x + m[6] * p.y) + m[10] * p.z);
+}
+/* IEEE binary16, round to nearest even (pack2x16float) */
+static uint16_t f2h(float f) {
+    uint32_t x;
+    memcpy(&x, &f, 4);
+    uint32_t sign = (x >> 16) & 0x8000u;
+    uint32_t ax = x & 0x7FFFFFFFu;
+    if (ax >= 0x7F800000u) return (uint16_t)(sign | 0x7C00u | (ax > 0x7F800000u ? 0x200u : 0u));
+    if (ax >= 0x477FF000u) return (uint16_t)(sign | 0x7C00u); /* rounds to >= 65520: inf */
+    if (ax < 0x38800000u) { /* subnormal half or zero */
+        if (ax < 0x33000000u) return (uint16_t)sign; /* < 2^-25: rounds to 0 */
+        uint32_t e = ax >> 23, m = (ax & 0x7FFFFFu) | 0x800000u;
+        uint32_t shift = 126u - e; /* value = m 2^(e-150), half unit 2^-24: q = m 2^(e-126) */
+        uint32_t q = m >> shift, rem = m & ((1u << shift) - 1u), half = 1u << (shift - 1u);
+        if (rem > half || (rem == half && (q & 1u))) q++;
+        return (uint16_t)(sign | q);
+    }
+    uint32_t e = (ax >> 23) - 112u, m = ax & 0x7FFFFFu;
+    uint32_t q = (e << 10) | (m >> 13), rem = m & 0x1FFFu;
+    if (rem > 0x1000u || (rem == 0x1000u && (q & 1u))) q++;
+    return (uint16_t)(sign | q);
+}
+static float h2f(uint16_t h) {
+    uint32_t sign = (uint32_t)(h & 0x8000u) << 16, e = (h >> 10) & 0x1Fu, m = h & 0x3FFu, x;
+    if (e == 0) {
+        if (m == 0) x = sign;
+        else { float f = ldexpf((float)m, -24); memcpy(&x, &f, 4); x |= sign; }
+    } else if (e == 31) x = sign | 0x7F800000u | (m << 13);
+    else x = sign | ((e + 112u) << 23) | (m << 13);
+    float f;
+    memcpy(&f, &x, 4);
+    return f;
+}
+void ocl_half_roundtrip(const float *in, int n, uint16_t *bits, float *out) {
+    for (int i = 0; i < n; i++) { bits[i] = f2h(in[i]); out[i] = h2f(bits[i]); }
+}
+
+/* Host product of mod.rs:2339-2345: S = transpose(transpose(W) * B), W column-major, B row-major */
+void ocl_bone_skin_mats(int nb, const float *world, const float *bind_inv, float *out) {
+    for (int b = 0; b < nb; b++) {
+        float wr[4][4], bb[4][4], sr[4][4];
+        for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++) { wr[i][j] = world[32 * b + j * 4 + i]; bb[i][j] = bind_inv[16 * b + i * 4 + j]; }
+        for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++)
+                sr[i][j] = ((wr[i][0] * bb[0][j] + wr[i][1] * bb[1][j]) + wr[i][2] * bb[2][j]) + wr[i][3] * bb[3][j];
+        for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++) out[16 * b + i * 4 + j] = sr[j][i];
+    }
+}
+void ocl_bone_skin(int nv, const float *rest4, const uint32_t *bidx, const float *bw, const float *skin_mats,
+                   float *out4) {
+    for (int i = 0; i < nv; i++) {
+        v3 pos = V3(rest4[4 * i], rest4[4 * i + 1], rest4[4 * i + 2]);
+        v3 p = V3(0, 0, 0);
+        float ws = 0.0f;
+        for (int k = 0; k < 4; k++) {
+            float w = bw[4 * i + k];
+            if (w > 0.0f) {
+                p = vadd(p, vmul(xf_point(skin_mats + 16 * (size_t)bidx[4 * i + k], pos), w));
+                ws += w;
+            }
+        }
+        if (ws <= 1e-6f) p = pos;
+        out4[4 * i] = p.x; out4[4 * i + 1] = p.y; out4[4 * i + 2] = p.z; out4[4 * i + 3] = 1.0f;
+    }
+}
+void ocl_bone_prep(int nt, const float *skinned4, const float *inv_mats, const uint32_t *src, const float *srcw,
+                   float *out16) {
+    for (int t = 0; t < nt; t++) {
+        const uint32_t *q = src + 4 * t;
+        const float *inv = inv_mats + 16 * (size_t)q[3];
+        v3 p0 = xf_point(inv, V3(skinned4[4 * q[0]], skinned4[4 * q[0] + 1], skinned4[4 * q[0] + 2]));
+        v3 p1 = xf_point(inv, V3(skinned4[4 * q[1]], skinned4[4 * q[1] + 1], skinned4[4 * q[1] + 2]));
+        v3 p2 = xf_point(inv, V3(skinned4[4 * q[2]], skinned4[4 * q[2] + 1], skinned4[4 * q[2] + 2]));
+        v3 cr = vcross(vsub(p1, p0), vsub(p2, p0));
+        float l2 = vdot(cr, cr);
+        v3 nrm = V3(0.0f, 1.0f, 0.0f);
+        if (l2 > 1e-12f) nrm = vmul(cr, 1.0f / sqrtf(l2));
+        float *o = out16 + 16 * t;
+        o[0] = p0.x; o[1] = p0.y; o[2] = p0.z; o[3] = srcw[4 * t];
+        o[4] = p1.x; o[5] = p1.y; o[6] = p1.z; o[7] = srcw[4 * t + 1];
+        o[8] = p2.x; o[9] = p2.y; o[10] = p2.z; o[11] = srcw[4 * t + 2];
+        o[12] = nrm.x; o[13] = nrm.y; o[14] = nrm.z; o[15] = srcw[4 * t + 3];
+    }
+}
+/* params: 16 words per bone (GpuBakeParams); every triangle of the bone in order */
+void ocl_bone_bake(int np, const uint32_t *params, const float *tris16, uint32_t *atlas) {
+    for (int bi = 0; bi < np; bi++) {
+        const uint32_t *P = params + 16 * bi;
+        float lmin[3], lmax[3];
+        memcpy(lmin, P, 12);
+        memcpy(lmax, P + 4, 12);
+        uint32_t tri_start = P[3], tri_count = P[7], col = P[8], row = P[9], layer = P[10], res = P[11];
+        uint32_t tw = P[12], th = P[13], pitch_w = P[15] > 0 ? P[15] : tw;
+        float fr = (float)res;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (uint32_t vz = 0; vz < res; vz++)
+            for (uint32_t vy = 0; vy < res; vy++)
+                for (uint32_t vx = 0; vx < res; vx++) {
+                    v3 uvw = V3(((float)vx + 0.5f) / fr, ((float)vy + 0.5f) / fr, ((float)vz + 0.5f) / fr);
+                    v3 p = V3(lmin[0] + uvw.x * (lmax[0] - lmin[0]), lmin[1] + uvw.y * (lmax[1] - lmin[1]),
+                              lmin[2] + uvw.z * (lmax[2] - lmin[2]));
+                    float min_d2 = 1e10f, bap = -1.0f, bsd = 10.0f, bal = 0.0f;
+                    for (uint32_t i = 0; i < tri_count; i++) {
+                        const float *T = tris16 + 16 * (size_t)(tri_start + i);
+                        v3 a = V3(T[0], T[1], T[2]), b = V3(T[4], T[5], T[6]), c = V3(T[8], T[9], T[10]);
+                        v3 nrm = V3(T[12], T[13], T[14]);
+                        v3 ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a);
+                        float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+                        v3 cp = a, bary = V3(1, 0, 0);
+                        if (d1 <= 0.0f && d2 <= 0.0f) {
+                        } else {
+                            v3 bp = vsub(p, b);
+                            float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+                            if (d3 >= 0.0f && d4 <= d3) { cp = b; bary = V3(0, 1, 0); }
+                            else {
+                                float vc = d1 * d4 - d3 * d2;
+                                if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+                                    float v = d1 / (d1 - d3);
+                                    cp = vadd(a, vmul(ab, v)); bary = V3(1.0f - v, v, 0);
+                                } else {
+                                    v3 cpv = vsub(p, c);
+                                    float d5 = vdot(ab, cpv), d6 = vdot(ac, cpv);
+                                    if (d6 >= 0.0f && d5 <= d6) { cp = c; bary = V3(0, 0, 1); }
+                                    else {
+                                        float vb = d5 * d2 - d1 * d6;
+                                        if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+                                            float w = d2 / (d2 - d6);
+                                            cp = vadd(a, vmul(ac, w)); bary = V3(1.0f - w, 0, w);
+                                        } else {
+                                            float va = d3 * d6 - d5 * d4;
+                                            if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+                                                float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+                                                cp = vadd(b, vmul(vsub(c, b), w)); bary = V3(0, 1.0f - w, w);
+                                            } else {
+                                                float denom = 1.0f / ((va + vb) + vc);
+                                                float v = vb * denom, w = vc * denom;
+                                                float u = (1.0f - v) - w;
+                                                cp = vadd(vadd(a, vmul(ab, v)), vmul(ac, w));
+                                                bary = V3(u, v, w);
+                                            }
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                        v3 diff = vsub(p, cp);
+                        float d_sq = vdot(diff, diff);
+                        float proj = vdot(diff, nrm), aproj = fabsf(proj);
+                        float eps_sq = 1e-7f * fmaxf(1.0f, min_d2);
+                        int closer = d_sq + eps_sq < min_d2;
+                        int tie = fabsf(d_sq - min_d2) <= eps_sq && aproj > bap;
+                        if (closer || tie) {
+                            if (d_sq < min_d2) min_d2 = d_sq;
+                            bap = aproj;
+                            float d = sqrtf(d_sq);
+                            float sign = proj >= 0.0f ? 1.0f : -1.0f;
+                            uint32_t bmask = (uint32_t)(T[15] + 0.5f);
+                            if (bmask != 0u && sign < 0.0f) {
+                                float op = -1.0f;
+                                if ((bmask & 1u) && bary.z <= 1e-5f) {
+                                    v3 e = vcross(vsub(b, a), nrm);
+                                    op = fmaxf(op, vdot(diff, vdiv(e, vlen(e))));
+                                }
+                                if ((bmask & 2u) && bary.x <= 1e-5f) {
+                                    v3 e = vcross(vsub(c, b), nrm);
+                                    op = fmaxf(op, vdot(diff, vdiv(e, vlen(e))));
+                                }
+                                if ((bmask & 4u) && bary.y <= 1e-5f) {
+                                    v3 e = vcross(vsub(a, c), nrm);
+                                    op = fmaxf(op, vdot(diff, vdiv(e, vlen(e))));
+                                }
+                                if (op > 0.0f && op >= aproj * 0.25f) sign = 1.0f;
+                            }
+                            bsd = d * sign;
+                            bal = (bary.x * T[3] + bary.y * T[7]) + bary.z * T[11];
+                        }
+                    }
+                    uint32_t gx = col * res + vx, gy = row * res + vy, gz = layer * res + vz;
+                    atlas[((size_t)gz * th + gy) * pitch_w + gx] = (uint32_t)f2h(bsd) | ((uint32_t)f2h(bal) << 16);
+                }
+    }
+}
+void ocl_set_bone_sdf(OSim *s, uint32_t w, uint32_t h, uint32_t d, const uint32_t *atlas, int nbones,
+                      const float *infos20, const float *xforms32) {
+    free(s->atlas); free(s->binfo); free(s->bxf);
+    s->atlas = NULL; s->binfo = NULL; s->bxf = NULL; s->nbones = 0;
+    if (nbones <= 0) return;
+    size_t nvox = (size_t)w * h * d;
+    s->atlas = malloc(nvox * 4); memcpy(s->atlas, atlas, nvox * 4);
+    s->binfo = malloc((size_t)nbones * 20 * 4); memcpy(s->binfo, infos20, (size_t)nbones * 20 * 4);
+    s->bxf = malloc((size_t)nbones * 32 * 4); memcpy(s->bxf, xforms32, (size_t)nbones * 32 * 4);
+    s->aw = w; s->ah = h; s->ad = d; s->nbones = nbones;
+}
+static void atlas_at(const OSim *s, int x, int y, int z, float *dv, float *av) {
+    uint32_t u = s->atlas[((size_t)z * s->ah + y) * s->aw + x];
+    *dv = h2f((uint16_t)(u & 0xFFFFu));
+    *av = h2f((uint16_t)(u >> 16));
+}
+static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+/* trilinear, clamp to edge, fp32 weights */
+static void sample_atlas(const OSim *s, v3 uvw, float *dist, float *alpha) {
+    float fx = uvw.x * (float)s->aw - 0.5f, fy = uvw.y * (float)s->ah - 0.5f, fz = uvw.z * (float)s->ad - 0.5f;
+    float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
+    float tx = fx - flx, ty = fy - fly, tz = fz - flz;
+    int ix = (int)flx, iy = (int)fly, iz = (int)flz;
+    int x0 = clampi(ix, 0, (int)s->aw - 1), x1 = clampi(ix + 1, 0, (int)s->aw - 1);
+    int y0 = clampi(iy, 0, (int)s->ah - 1), y1 = clampi(iy + 1, 0, (int)s->ah - 1);
+    int z0 = clampi(iz, 0, (int)s->ad - 1), z1 = clampi(iz + 1, 0, (int)s->ad - 1);
+    float rz[2][2];
+    for (int zi = 0; zi < 2; zi++) {
+        int z = zi ? z1 : z0;
+        float ry[2][2];
+        for (int yi = 0; yi < 2; yi++) {
+            int y = yi ? y1 : y0;
+            float pd, pa, qd, qa;
+            atlas_at(s, x0, y, z, &pd, &pa);
+            atlas_at(s, x1, y, z, &qd, &qa);
+            ry[yi][0] = pd * (1.0f - tx) + qd * tx;
+            ry[yi][1] = pa * (1.0f - tx) + qa * tx;
+        }
+        rz[zi][0] = ry[0][0] * (1.0f - ty) + ry[1][0] * ty;
+        rz[zi][1] = ry[0][1] * (1.0f - ty) + ry[1][1] * ty;
+    }
+    *dist = rz[0][0] * (1.0f - tz) + rz[1][0] * tz;
+    *alpha = rz[0][1] * (1.0f - tz) + rz[1][1] * tz;
+}
+static float sample_d(const OSim *s, v3 uvw) { float d, a; sample_atlas(s, uvw, &d, &a); return d; }
+static float smoothstep_f(float e0, float e1, float x) {
+    float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return (t * t) * (3.0f - 2.0f * t);
+}
+static int bone_sdf_contact(const OSim *s, v3 p, float vth, v3 *target, v3 *nrm_out, float *fric, float *rest) {
+    float best = 1e6f, best_target = 0.0f, bf = 0.0f, br = 0.0f;
+    v3 best_n = V3(0, 0, 0);
+    unsigned hits = 0;
+    int has_mesh = s->ntris > 0;
+    for (int b = 0; b < s->nbones; b++) {
+        const float *I = s->binfo + 20 * b;
+        const float *X = s->bxf + 32 * b;
+        float wr = I[15];
+        if (wr > 0.0f) {
+            v3 dw = vsub(p, V3(I[3], I[7], I[11]));
+            float rt = wr + vth;
+            if (vdot(dw, dw) > rt * rt) continue;
+        }
+        v3 pl = xf_point(X + 16, p);
+        float target_dist = vth + I[17];
+        float margin = target_dist + 0.05f;
+        if (pl.x < I[0] - margin || pl.x > I[4] + margin || pl.y < I[1] - margin || pl.y > I[5] + margin ||
+            pl.z < I[2] - margin || pl.z > I[6] + margin)
+            continue;
+        v3 sc = V3(I[8], I[9], I[10]), of = V3(I[12], I[13], I[14]);
+        v3 uvw = V3(pl.x * sc.x + of.x, pl.y * sc.y + of.y, pl.z * sc.z + of.z);
+        v3 umin = V3(I[0] * sc.x + of.x, I[1] * sc.y + of.y, I[2] * sc.z + of.z);
+        v3 umax = V3(I[4] * sc.x + of.x, I[5] * sc.y + of.y, I[6] * sc.z + of.z);
+        if (uvw.x < umin.x || uvw.x > umax.x || uvw.y < umin.y || uvw.y > umax.y || uvw.z < umin.z || uvw.z > umax.z)
+            continue;
+        v3 es = vmul(vsub(umax, umin), s->nbones == 1 ? 0.002f : 0.015f);
+        v3 lo = vadd(umin, es), hi = vsub(umax, es);
+        v3 us = V3(clampf(uvw.x, lo.x, hi.x), clampf(uvw.y, lo.y, hi.y), clampf(uvw.z, lo.z, hi.z));
+        float raw, alpha;
+        sample_atlas(s, us, &raw, &alpha);
+        float thr = fmaxf(I[19], 0.01f);
+        float retract = 0.0f;
+        if (has_mesh) retract = (1.0f - smoothstep_f(thr, 0.7f, alpha)) * 0.06f;
+        float eff = alpha > thr ? raw + retract : 10.0f;
+        if (eff < target_dist) {
+            v3 eu = vmul(sc, 0.005f);
+            float dxp = sample_d(s, V3(clampf(uvw.x + eu.x, lo.x, hi.x), us.y, us.z));
+            float dxn = sample_d(s, V3(clampf(uvw.x - eu.x, lo.x, hi.x), us.y, us.z));
+            float dyp = sample_d(s, V3(us.x, clampf(uvw.y + eu.y, lo.y, hi.y), us.z));
+            float dyn = sample_d(s, V3(us.x, clampf(uvw.y - eu.y, lo.y, hi.y), us.z));
+            float dzp = sample_d(s, V3(us.x, us.y, clampf(uvw.z + eu.z, lo.z, hi.z)));
+            float dzn = sample_d(s, V3(us.x, us.y, clampf(uvw.z - eu.z, lo.z, hi.z)));
+            float dx = dxp - dxn, dy = dyp - dyn, dz = dzp - dzn;
+            if (fabsf(dx) < 1e-6f) dx = uvw.x < (lo.x + hi.x) * 0.5f ? dxp - raw : raw - dxn;
+            if (fabsf(dy) < 1e-6f) dy = uvw.y < (lo.y + hi.y) * 0.5f ? dyp - raw : raw - dyn;
+            if (fabsf(dz) < 1e-6f) dz = uvw.z < (lo.z + hi.z) * 0.5f ? dzp - raw : raw - dzn;
+            v3 g = V3(dx, dy, dz);
+            float gl = vlen(g);
+            v3 nl = V3(0, 0, 1);
+            if (gl > 1e-6f) nl = vdiv(g, gl);
+            else {
+                v3 cl = vmul(vadd(V3(I[0], I[1], I[2]), V3(I[4], I[5], I[6])), 0.5f);
+                v3 dc = vsub(pl, cl);
+                float lc = vlen(dc);
+                if (lc > 1e-6f) nl = vdiv(dc, lc);
+            }
+            v3 nwr = xf_dir(X, nl);
+            v3 nw = vdiv(nwr, vlen(nwr));
+            if (hits == 0 || eff < best) { best = eff; best_n = nw; bf = I[16]; br = I[18]; best_target = target_dist; }
+            hits++;
+        }
+    }
+    if (hits > 0 && best < best_target) {
+        *target = vadd(p, vmul(best_n, best_target - best));
+        *nrm_out = best_n;
+        *fric = bf;
+        *rest = br;
+        return 1;
+    }
+    return 0;
+}
+
 static void k_collision(OSim *s, float dt) {
 #pragma omp parallel for schedule(dynamic, 64)
     for (int i = 0; i < s->n; i++) {
@@ -1203,6 +1526,14 @@ static void k_collision(OSim *s, float dt) {
                      &bpos, &bn, &bf, &br, &hasrec);
         }
         if (!front && hasrec) contact(bpos, bn, bf, br, dt, pinit, &xn, &p);
+        if (s->nbones > 0) {
+            v3 tgt, bnn;
+            float bfr, brs;
+            if (bone_sdf_contact(s, p, th, &tgt, &bnn, &bfr, &brs)) {
+                v3 pb = p;
+                contact(tgt, bnn, bfr, brs, dt, pb, &xn, &p);
+            }
+        }
         s->p[i] = p;
         s->x[i] = xn;
     }
@@ -2059,7 +2390,7 @@ void ocl_step(OSim *s, float dt, int substeps) {
     float sm = fmaxf(s->cloth_thickness * 0.8f, 0.002f);
     int risk = sd > sm * 0.25f;
     int coupled = s->coupled || (s->auto_coupled && risk);
-    int hascol = s->ncols > 0 || s->ntris > 0;
+    int hascol = s->ncols > 0 || s->ntris > 0 || s->nbones > 0;
     for (int sub = 0; sub < substeps; sub++) {
         memset(s->dlam, 0, 4 * ((size_t)s->nd + 1));
         memset(s->blam, 0, 4 * ((size_t)s->nb + 1));

@@ -86,6 +86,19 @@ float ocl_cell_size(const OSim *s);
 void ocl_build_hash(OSim *s, int which, uint32_t *cell_starts, uint32_t *sorted);
 void ocl_get_mesh_triangles(const OSim *s, float *tris16);  /* T x 16 floats (sorted) */
 
+/* Bone SDF (skinning.wgsl, prep_bone_triangles.wgsl, bake_sdf.wgsl,
+ * collision.wgsl:116-265).  Matrices: 16 floats, column-major
+ * (row j, column k at [k*4 + j]); bind_inv row-major as mod.rs:2339-2345. */
+void ocl_half_roundtrip(const float *in, int n, uint16_t *bits, float *out);
+void ocl_bone_skin_mats(int nb, const float *world32, const float *bind_inv16, float *out16);
+void ocl_bone_skin(int nv, const float *rest4, const uint32_t *bidx4, const float *bw4, const float *skin_mats,
+                   float *out4);
+void ocl_bone_prep(int nt, const float *skinned4, const float *inv_mats16, const uint32_t *src4,
+                   const float *srcw4, float *out16);
+void ocl_bone_bake(int nparams, const uint32_t *params16, const float *tris16, uint32_t *atlas);
+void ocl_set_bone_sdf(OSim *s, uint32_t w, uint32_t h, uint32_t d, const uint32_t *atlas, int nbones,
+                      const float *infos20, const float *xforms32);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,19 @@ SIGNATURES = {
     "tc_check_barrier_timeout": [_P, _U],
     "tc_hash_build_static": [_P, _U, _F, _U, _P, _P, _P],
     "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],
+    "tc_set_bone_sdf_colliders": [_P, _U, _U, _U, _P, C.c_size_t, _P, _U],
+    "tc_update_bone_transforms": [_P, _P, _P, _U, _P, C.c_int64],
+    "tc_set_dynamic_bone_sdf_dirty_bones": [_P, _P, C.c_int64],
+    "tc_clear_bone_sdf_colliders": [_P],
+    "tc_setup_dynamic_bone_sdf": [_P, _U, _U, _U, _U, _P, _U, _P, _U, _P, _P, _U, _P, _P, _U, _P, _U, _U],
+    "tc_set_dynamic_bone_sdf_enabled": [_P, _I],
+    "tc_set_dynamic_bone_sdf_update_interval": [_P, _U],
+    "tc_get_bone_sdf_atlas": [_P, _P, C.c_size_t, _P],
+    "tc_get_bone_infos": [_P, _P, C.c_size_t, C.POINTER(_U)],
+    "tc_bake_bone_sdf": [_P, _U, _P, _U, _U, _P, _P, _U, _F, _F, _F, _F, _F, _F, _I, _I, C.POINTER(_P)],
+    "tc_bake_dims": [_P, _P],
+    "tc_bake_get": [_P, _P, _P, _P, _P],
+    "tc_bake_destroy": [_P],
     "tc_ws_param_count": [],
     "tc_ws_enable": [_P, _I, _U, _F],
     "tc_ws_record": [_P, _U, _U],

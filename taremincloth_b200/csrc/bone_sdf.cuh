@@ -1,0 +1,403 @@
+// Bone SDF collider: linear-blend skinning, bone-local triangle preparation,
+// the per-bone signed-distance bake into an fp16 x 2 atlas, and the collision
+// phase that samples it.
+//
+// Restates skinning.wgsl:16-43, prep_bone_triangles.wgsl:30-67,
+// bake_sdf.wgsl:33-196 and collision.wgsl:116-265 (crates/cloth_core/src/shaders).
+// Matrices are stored as the reference's GpuBoneTransform: 16 floats,
+// column-major (element (row j, column k) at [k * 4 + j]).
+//
+// The atlas is a plain device array [depth][height][width] of packed half2
+// (distance in the low half, alpha in the high half), the reference's
+// Rg16Float texture layout.  Sampling is trilinear with clamp-to-edge in fp32
+// (the reference's hardware sampler filters with 8-bit weights; no fixture
+// pins either, so this row is parity unpinned against the reference and
+// bit-exact against the oracle).
+//
+// The bake visits each bone's triangles in the reference's order for every
+// voxel.  A triangle, or a tile of 32, is skipped only when a conservative
+// bounding-sphere lower bound on its squared distance exceeds the voxel's
+// running minimum plus the tie tolerance: such a triangle cannot be accepted
+// by the sequential rule, so the state after it is unchanged and the result
+// equals the full scan.
+#pragma once
+#include <cuda_fp16.h>
+
+#include "vmath.cuh"
+
+namespace tcloth {
+
+struct BoneInfo {    // the reference's GpuBoneInfo (collision.wgsl:50-56), 80 B
+  float4 aabb_min;   // .w: world bounding-sphere centre x
+  float4 aabb_max;   // .w: centre y
+  float4 uvw_scale;  // .w: centre z (the bake writes blend_k here)
+  float4 uvw_offset; // .w: world bounding-sphere radius
+  float4 params;     // friction, thickness, restitution, weight threshold
+};
+struct BoneXform {   // world and inverse world, column-major
+  float m[16];
+  float inv[16];
+};
+struct BakeParams {  // GpuBakeParams (sdf_baker.rs:12-25), 64 B
+  float lmin[3];
+  uint32_t tri_start;
+  float lmax[3];
+  uint32_t tri_count;
+  uint32_t tile_col, tile_row, tile_layer, res;
+  uint32_t total_w, total_h, total_d, row_pitch;
+};
+struct BakeTri {     // GpuBakeTriangle (sdf_baker.rs:29-38), 64 B
+  float4 p0w0, p1w1, p2w2;
+  float4 n_bmask;    // normal, open-boundary bit mask (as float)
+};
+
+// ((m0 x + m4 y) + m8 z) + m12: column-major matrix times (x, y, z, 1)
+__device__ __forceinline__ V3 xform_point(const float* m, V3 p) {
+  return mk(((m[0] * p.x + m[4] * p.y) + m[8] * p.z) + m[12], ((m[1] * p.x + m[5] * p.y) + m[9] * p.z) + m[13],
+            ((m[2] * p.x + m[6] * p.y) + m[10] * p.z) + m[14]);
+}
+__device__ __forceinline__ V3 xform_dir(const float* m, V3 p) {
+  return mk((m[0] * p.x + m[4] * p.y) + m[8] * p.z, (m[1] * p.x + m[5] * p.y) + m[9] * p.z,
+            (m[2] * p.x + m[6] * p.y) + m[10] * p.z);
+}
+
+// ---- skinning.wgsl:16-43: rest (pos, normal) + 4 bone indices / weights
+__global__ void k_bone_skin(uint32_t nv, const float4* __restrict__ rest_pos, const uint4* __restrict__ bidx,
+                            const float4* __restrict__ bw, const float* __restrict__ skin_mats,
+                            float4* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const V3 pos = mk(rest_pos[i]);
+  const uint4 bi = bidx[i];
+  const float4 w4 = bw[i];
+  const uint32_t ids[4] = {bi.x, bi.y, bi.z, bi.w};
+  const float ws[4] = {w4.x, w4.y, w4.z, w4.w};
+  V3 p = mk(0.f, 0.f, 0.f);
+  float wsum = 0.f;
+  for (int k = 0; k < 4; ++k) {
+    const float w = ws[k];
+    if (w > 0.f) {
+      p = p + xform_point(skin_mats + 16 * size_t(ids[k]), pos) * w;
+      wsum += w;
+    }
+  }
+  if (wsum <= 1e-6f) p = pos;
+  out[i] = make_float4(p.x, p.y, p.z, 1.f);
+}
+
+// ---- prep_bone_triangles.wgsl:30-67: world triangle -> bone-local BakeTri
+// src = (i0, i1, i2, bone), srcw = (w0, w1, w2, open-boundary mask)
+__global__ void k_bone_prep(uint32_t nt, const float4* __restrict__ skinned, const float* __restrict__ inv_mats,
+                            const uint4* __restrict__ src, const float4* __restrict__ srcw,
+                            BakeTri* __restrict__ out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const uint4 s = src[t];
+  const float4 w = srcw[t];
+  const float* inv = inv_mats + 16 * size_t(s.w);
+  const V3 p0 = xform_point(inv, mk(skinned[s.x]));
+  const V3 p1 = xform_point(inv, mk(skinned[s.y]));
+  const V3 p2 = xform_point(inv, mk(skinned[s.z]));
+  const V3 cr = cross(p1 - p0, p2 - p0);
+  const float l2 = dot(cr, cr);
+  V3 n = mk(0.f, 1.f, 0.f);
+  if (l2 > 1e-12f) n = cr * (1.0f / sqrtf(l2));
+  out[t] = BakeTri{make_float4(p0.x, p0.y, p0.z, w.x), make_float4(p1.x, p1.y, p1.z, w.y),
+                   make_float4(p2.x, p2.y, p2.z, w.z), make_float4(n.x, n.y, n.z, w.w)};
+}
+
+// Conservative bounding spheres: per triangle (centroid, max vertex distance),
+// and per tile of 32 consecutive triangles of one bone (tiles listed by the
+// host: tile k covers [tile_first[k], tile_first[k] + tile_cnt[k])).  Radii are
+// widened (x 1.001 + 1e-5) so that fp32 rounding cannot make a bound exceed a
+// computed distance.
+__global__ void k_bone_tri_spheres(uint32_t nt, const BakeTri* __restrict__ tris, float4* __restrict__ sph) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const BakeTri q = tris[t];
+  const V3 a = mk(q.p0w0), b = mk(q.p1w1), c = mk(q.p2w2);
+  const V3 m = (a + b + c) / 3.0f;
+  const float r = sqrtf(fmaxf(fmaxf(dot(a - m, a - m), dot(b - m, b - m)), dot(c - m, c - m)));
+  sph[t] = make_float4(m.x, m.y, m.z, r * 1.001f + 1e-5f);
+}
+__global__ void k_bone_tile_spheres(uint32_t ntiles, const uint32_t* __restrict__ tile_first,
+                                    const uint32_t* __restrict__ tile_cnt, const float4* __restrict__ sph,
+                                    float4* __restrict__ tsph) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ntiles) return;
+  const uint32_t f = tile_first[k], c = tile_cnt[k];
+  V3 m = mk(0.f, 0.f, 0.f);
+  for (uint32_t i = 0; i < c; ++i) m = m + mk(sph[f + i]);
+  m = m / float(max(c, 1u));
+  float r = 0.f;
+  for (uint32_t i = 0; i < c; ++i) {
+    const float4 s = sph[f + i];
+    r = fmaxf(r, length(mk(s) - m) + s.w);
+  }
+  tsph[k] = make_float4(m.x, m.y, m.z, r * 1.001f + 1e-5f);
+}
+
+__device__ __forceinline__ uint32_t pack_half2(float lo, float hi) {
+  return (uint32_t)__half_as_ushort(__float2half_rn(lo)) | ((uint32_t)__half_as_ushort(__float2half_rn(hi)) << 16);
+}
+
+// Voxel state of the sequential nearest-triangle rule (bake_sdf.wgsl:71-183)
+struct BakeState {
+  float min_d2, best_abs_proj, best_signed, best_alpha;
+};
+__device__ __forceinline__ void bake_visit(BakeState& s, V3 p, const BakeTri& tri) {
+  const V3 a = mk(tri.p0w0), b = mk(tri.p1w1), c = mk(tri.p2w2);
+  const V3 ab = b - a, ac = c - a, ap = p - a;
+  const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+  V3 cp = a;
+  V3 bary = mk(1.f, 0.f, 0.f);
+  if (d1 <= 0.f && d2 <= 0.f) {
+  } else {
+    const V3 bp = p - b;
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.f && d4 <= d3) {
+      cp = b;
+      bary = mk(0.f, 1.f, 0.f);
+    } else {
+      const float vc = d1 * d4 - d3 * d2;
+      if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+        const float v = d1 / (d1 - d3);
+        cp = a + ab * v;
+        bary = mk(1.f - v, v, 0.f);
+      } else {
+        const V3 cpv = p - c;
+        const float d5 = dot(ab, cpv), d6 = dot(ac, cpv);
+        if (d6 >= 0.f && d5 <= d6) {
+          cp = c;
+          bary = mk(0.f, 0.f, 1.f);
+        } else {
+          const float vb = d5 * d2 - d1 * d6;
+          if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+            const float w = d2 / (d2 - d6);
+            cp = a + ac * w;
+            bary = mk(1.f - w, 0.f, w);
+          } else {
+            const float va = d3 * d6 - d5 * d4;
+            if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
+              const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+              cp = b + (c - b) * w;
+              bary = mk(0.f, 1.f - w, w);
+            } else {
+              const float denom = 1.0f / ((va + vb) + vc);
+              const float v = vb * denom, w = vc * denom;
+              const float u = (1.0f - v) - w;
+              cp = (a + ab * v) + ac * w;
+              bary = mk(u, v, w);
+            }
+          }
+        }
+      }
+    }
+  }
+  const V3 diff = p - cp;
+  const float d_sq = dot(diff, diff);
+  const V3 nrm = mk(tri.n_bmask);
+  const float proj = dot(diff, nrm);
+  const float aproj = fabsf(proj);
+  const float eps_sq = 1e-7f * fmaxf(1.0f, s.min_d2);
+  const bool closer = d_sq + eps_sq < s.min_d2;
+  const bool tie = fabsf(d_sq - s.min_d2) <= eps_sq && aproj > s.best_abs_proj;
+  if (closer || tie) {
+    if (d_sq < s.min_d2) s.min_d2 = d_sq;
+    s.best_abs_proj = aproj;
+    const float d = sqrtf(d_sq);
+    float sign = proj >= 0.f ? 1.f : -1.f;
+    const uint32_t bmask = uint32_t(tri.n_bmask.w + 0.5f);
+    if (bmask != 0u && sign < 0.f) {
+      float out_proj = -1.f;
+      if ((bmask & 1u) && bary.z <= 1e-5f) {
+        const V3 e = cross(b - a, nrm);
+        out_proj = fmaxf(out_proj, dot(diff, e / length(e)));
+      }
+      if ((bmask & 2u) && bary.x <= 1e-5f) {
+        const V3 e = cross(c - b, nrm);
+        out_proj = fmaxf(out_proj, dot(diff, e / length(e)));
+      }
+      if ((bmask & 4u) && bary.y <= 1e-5f) {
+        const V3 e = cross(a - c, nrm);
+        out_proj = fmaxf(out_proj, dot(diff, e / length(e)));
+      }
+      if (out_proj > 0.f && out_proj >= aproj * 0.25f) sign = 1.f;
+    }
+    s.best_signed = d * sign;
+    s.best_alpha = (bary.x * tri.p0w0.w + bary.y * tri.p1w1.w) + bary.z * tri.p2w2.w;
+  }
+}
+// true when nothing in the sphere can be accepted for this voxel state
+__device__ __forceinline__ bool bake_far(const BakeState& s, V3 p, float4 sph) {
+  const float dc = length(p - mk(sph)) - sph.w;
+  if (dc <= 0.f) return false;
+  const float lim = s.min_d2 + 1e-7f * fmaxf(1.0f, s.min_d2);
+  return dc * dc > lim * 1.0001f;
+}
+
+// ---- bake_sdf.wgsl:33-196.  Block = 8 warps = an 8 x 8 x 4 voxel region of
+// one bone; each warp owns a 4 x 4 x 2 brick.  blockIdx.y = entry of `params`.
+__global__ void __launch_bounds__(256) k_bone_bake(const BakeParams* __restrict__ params, const BakeTri* __restrict__ tris,
+                                                   const float4* __restrict__ sph, const float4* __restrict__ tsph,
+                                                   const uint32_t* __restrict__ bone_tile_off,
+                                                   const uint32_t* __restrict__ param_bone,
+                                                   uint32_t* __restrict__ atlas) {
+  const BakeParams P = params[blockIdx.y];
+  const uint32_t res = P.res;
+  const uint32_t bx = (res + 7) / 8, by = (res + 7) / 8;
+  const uint32_t blk = blockIdx.x;
+  const uint32_t ox = (blk % bx) * 8, oy = ((blk / bx) % by) * 8, oz = (blk / (bx * by)) * 4;
+  if (oz >= res) return;  // whole block
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t vx = ox + (warp & 1) * 4 + (lane & 3);
+  const uint32_t vy = oy + ((warp >> 1) & 1) * 4 + ((lane >> 2) & 3);
+  const uint32_t vz = oz + (warp >> 2) * 2 + (lane >> 4);
+  const bool valid = vx < res && vy < res && vz < res;
+  const float fr = float(res);
+  const V3 uvw = mk((float(vx) + 0.5f) / fr, (float(vy) + 0.5f) / fr, (float(vz) + 0.5f) / fr);
+  const V3 p = mk(P.lmin[0] + uvw.x * (P.lmax[0] - P.lmin[0]), P.lmin[1] + uvw.y * (P.lmax[1] - P.lmin[1]),
+                  P.lmin[2] + uvw.z * (P.lmax[2] - P.lmin[2]));
+  BakeState s{1e10f, -1.0f, 10.0f, 0.0f};
+  const uint32_t t0 = P.tri_start, tn = P.tri_count;
+  const uint32_t tile0 = bone_tile_off[param_bone[blockIdx.y]];
+  for (uint32_t k = 0; k * 32u < tn; ++k) {
+    const bool skip_tile = !valid || bake_far(s, p, __ldg(tsph + tile0 + k));
+    if (__all_sync(0xffffffffu, skip_tile)) continue;
+    const uint32_t e = min(32u, tn - k * 32u);
+    for (uint32_t q = 0; q < e; ++q) {
+      const uint32_t t = t0 + k * 32u + q;
+      if (skip_tile || bake_far(s, p, __ldg(sph + t))) continue;
+      const BakeTri tri{__ldg(&tris[t].p0w0), __ldg(&tris[t].p1w1), __ldg(&tris[t].p2w2), __ldg(&tris[t].n_bmask)};
+      bake_visit(s, p, tri);
+    }
+  }
+  if (!valid) return;
+  const uint32_t gx = P.tile_col * res + vx, gy = P.tile_row * res + vy, gz = P.tile_layer * res + vz;
+  const uint32_t pitch = P.row_pitch > 0u ? P.row_pitch : P.total_w;
+  atlas[(size_t(gz) * P.total_h + gy) * pitch + gx] = pack_half2(s.best_signed, s.best_alpha);
+}
+
+// ---- sampling: trilinear, clamp to edge, texel centres at (i + 0.5) / size
+__device__ __forceinline__ float2 unpack_half2(uint32_t u) {
+  return make_float2(__half2float(__ushort_as_half((unsigned short)(u & 0xFFFFu))),
+                     __half2float(__ushort_as_half((unsigned short)(u >> 16))));
+}
+struct BoneSdfArgs {
+  const BoneInfo* info;
+  const BoneXform* xf;
+  const uint32_t* atlas;
+  uint32_t nbones, w, h, d;
+};
+__device__ __forceinline__ float2 atlas_fetch(const BoneSdfArgs& a, int x, int y, int z) {
+  return unpack_half2(__ldg(a.atlas + (size_t(z) * a.h + y) * a.w + x));
+}
+__device__ __forceinline__ float2 sample_atlas(const BoneSdfArgs& a, V3 uvw) {
+  const float fx = uvw.x * float(a.w) - 0.5f, fy = uvw.y * float(a.h) - 0.5f, fz = uvw.z * float(a.d) - 0.5f;
+  const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
+  const float tx = fx - flx, ty = fy - fly, tz = fz - flz;
+  const int ix = int(flx), iy = int(fly), iz = int(flz);
+  const int x0 = min(max(ix, 0), int(a.w) - 1), x1 = min(max(ix + 1, 0), int(a.w) - 1);
+  const int y0 = min(max(iy, 0), int(a.h) - 1), y1 = min(max(iy + 1, 0), int(a.h) - 1);
+  const int z0 = min(max(iz, 0), int(a.d) - 1), z1 = min(max(iz + 1, 0), int(a.d) - 1);
+  auto lx = [&](int y, int z) {
+    const float2 p = atlas_fetch(a, x0, y, z), q = atlas_fetch(a, x1, y, z);
+    return make_float2(p.x * (1.f - tx) + q.x * tx, p.y * (1.f - tx) + q.y * tx);
+  };
+  auto ly = [&](int z) {
+    const float2 p = lx(y0, z), q = lx(y1, z);
+    return make_float2(p.x * (1.f - ty) + q.x * ty, p.y * (1.f - ty) + q.y * ty);
+  };
+  const float2 p = ly(z0), q = ly(z1);
+  return make_float2(p.x * (1.f - tz) + q.x * tz, p.y * (1.f - tz) + q.y * tz);
+}
+__device__ __forceinline__ float smoothstep_f(float e0, float e1, float x) {
+  const float t = clampf((x - e0) / (e1 - e0), 0.f, 1.f);
+  return (t * t) * (3.0f - 2.0f * t);
+}
+
+// collision.wgsl:123-265 (solve_bone_sdf_collision).  Returns true with the
+// best contact (target position, normal, friction, restitution) when the
+// vertex penetrates target_dist of some bone.
+__device__ __noinline__ bool bone_sdf_contact(const BoneSdfArgs& a, V3 p, float vth, bool has_mesh, V3& target,
+                                              V3& nrm_out, float& fric, float& rest) {
+  float best = 1e6f, best_target = 0.f;
+  V3 best_n = mk(0.f, 0.f, 0.f);
+  float bf = 0.f, br = 0.f;
+  uint32_t hits = 0;
+  for (uint32_t b = 0; b < a.nbones; ++b) {
+    const BoneInfo info = a.info[b];
+    const float wr = info.uvw_offset.w;
+    if (wr > 0.f) {
+      const V3 dw = p - mk(info.aabb_min.w, info.aabb_max.w, info.uvw_scale.w);
+      const float rt = wr + vth;
+      if (dot(dw, dw) > rt * rt) continue;
+    }
+    const BoneXform& X = a.xf[b];
+    const V3 pl = xform_point(X.inv, p);
+    const float target_dist = vth + info.params.y;
+    const float margin = target_dist + 0.05f;
+    if (pl.x < info.aabb_min.x - margin || pl.x > info.aabb_max.x + margin || pl.y < info.aabb_min.y - margin ||
+        pl.y > info.aabb_max.y + margin || pl.z < info.aabb_min.z - margin || pl.z > info.aabb_max.z + margin)
+      continue;
+    const V3 sc = mk(info.uvw_scale), of = mk(info.uvw_offset);
+    const V3 uvw = mk(pl.x * sc.x + of.x, pl.y * sc.y + of.y, pl.z * sc.z + of.z);
+    const V3 umin = mk(info.aabb_min.x * sc.x + of.x, info.aabb_min.y * sc.y + of.y, info.aabb_min.z * sc.z + of.z);
+    const V3 umax = mk(info.aabb_max.x * sc.x + of.x, info.aabb_max.y * sc.y + of.y, info.aabb_max.z * sc.z + of.z);
+    if (uvw.x < umin.x || uvw.x > umax.x || uvw.y < umin.y || uvw.y > umax.y || uvw.z < umin.z || uvw.z > umax.z)
+      continue;
+    const V3 es = (umax - umin) * (a.nbones == 1u ? 0.002f : 0.015f);
+    const V3 lo = umin + es, hi = umax - es;
+    const V3 us = mk(clampf(uvw.x, lo.x, hi.x), clampf(uvw.y, lo.y, hi.y), clampf(uvw.z, lo.z, hi.z));
+    const float2 sv = sample_atlas(a, us);
+    const float raw = sv.x, alpha = sv.y;
+    const float thr = fmaxf(info.params.w, 0.01f);
+    float retract = 0.f;
+    if (has_mesh) retract = (1.0f - smoothstep_f(thr, 0.7f, alpha)) * 0.06f;
+    const float eff = alpha > thr ? raw + retract : 10.0f;
+    if (eff < target_dist) {
+      const V3 eu = sc * 0.005f;
+      const float dxp = sample_atlas(a, mk(clampf(uvw.x + eu.x, lo.x, hi.x), us.y, us.z)).x;
+      const float dxn = sample_atlas(a, mk(clampf(uvw.x - eu.x, lo.x, hi.x), us.y, us.z)).x;
+      const float dyp = sample_atlas(a, mk(us.x, clampf(uvw.y + eu.y, lo.y, hi.y), us.z)).x;
+      const float dyn = sample_atlas(a, mk(us.x, clampf(uvw.y - eu.y, lo.y, hi.y), us.z)).x;
+      const float dzp = sample_atlas(a, mk(us.x, us.y, clampf(uvw.z + eu.z, lo.z, hi.z))).x;
+      const float dzn = sample_atlas(a, mk(us.x, us.y, clampf(uvw.z - eu.z, lo.z, hi.z))).x;
+      float dx = dxp - dxn, dy = dyp - dyn, dz = dzp - dzn;
+      if (fabsf(dx) < 1e-6f) dx = uvw.x < (lo.x + hi.x) * 0.5f ? dxp - raw : raw - dxn;
+      if (fabsf(dy) < 1e-6f) dy = uvw.y < (lo.y + hi.y) * 0.5f ? dyp - raw : raw - dyn;
+      if (fabsf(dz) < 1e-6f) dz = uvw.z < (lo.z + hi.z) * 0.5f ? dzp - raw : raw - dzn;
+      const V3 g = mk(dx, dy, dz);
+      const float gl = length(g);
+      V3 nl = mk(0.f, 0.f, 1.f);
+      if (gl > 1e-6f) {
+        nl = g / gl;
+      } else {
+        const V3 cl = (mk(info.aabb_min) + mk(info.aabb_max)) * 0.5f;
+        const V3 dc = pl - cl;
+        const float lc = length(dc);
+        if (lc > 1e-6f) nl = dc / lc;
+      }
+      const V3 nwr = xform_dir(X.m, nl);
+      const V3 nw = nwr / length(nwr);
+      if (hits == 0u || eff < best) {
+        best = eff;
+        best_n = nw;
+        bf = info.params.x;
+        br = info.params.z;
+        best_target = target_dist;
+      }
+      ++hits;
+    }
+  }
+  if (hits > 0u && best < best_target) {
+    target = p + best_n * (best_target - best);
+    nrm_out = best_n;
+    fric = bf;
+    rest = br;
+    return true;
+  }
+  return false;
+}
+
+}  // namespace tcloth

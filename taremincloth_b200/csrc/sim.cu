@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -183,6 +184,80 @@ struct Mlp {
   }
 };
 
+// Tiles of 32 consecutive triangles per bone for the bake's sphere culling.
+struct BakeTiles {
+  std::vector<uint32_t> first, cnt, bone_off;  // per tile; per bone: first tile
+};
+static BakeTiles make_bake_tiles(const std::vector<uint32_t>& start, const std::vector<uint32_t>& count) {
+  BakeTiles t;
+  t.bone_off.resize(start.size() + 1);
+  for (size_t b = 0; b < start.size(); ++b) {
+    t.bone_off[b] = uint32_t(t.first.size());
+    for (uint32_t k = 0; k < count[b]; k += 32) {
+      t.first.push_back(start[b] + k);
+      t.cnt.push_back(std::min(32u, count[b] - k));
+    }
+  }
+  t.bone_off[start.size()] = uint32_t(t.first.size());
+  return t;
+}
+
+// Device side of a bake: triangles, spheres, tiles, parameters.
+struct BakeGpu {
+  DBuf<BakeTri> tris;
+  DBuf<float4> sph, tsph;
+  DBuf<uint32_t> tile_first, tile_cnt, tile_off, param_bone;
+  DBuf<BakeParams> params;
+  uint32_t nt = 0, ntiles = 0;
+  void setup_tiles(const BakeTiles& t, cudaStream_t st) {
+    ntiles = uint32_t(t.first.size());
+    tile_first.upload(t.first, st);
+    tile_cnt.upload(t.cnt, st);
+    tile_off.upload(t.bone_off, st);
+    sph.alloc(std::max<uint32_t>(nt, 1));
+    tsph.alloc(std::max<uint32_t>(ntiles, 1));
+  }
+  // spheres of the current triangles, then the bake of the listed entries
+  void bake(const std::vector<BakeParams>& ps, const std::vector<uint32_t>& bones, uint32_t* atlas, cudaStream_t st) {
+    if (ps.empty()) return;
+    if (nt) k_bone_tri_spheres<<<(nt + 255) / 256, 256, 0, st>>>(nt, tris.p, sph.p);
+    if (ntiles) k_bone_tile_spheres<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, tile_first.p, tile_cnt.p, sph.p, tsph.p);
+    params.upload(ps, st);
+    param_bone.upload(bones, st);
+    uint32_t res = 0;
+    for (const auto& q : ps) res = std::max(res, q.res);
+    const uint32_t nblk = ((res + 7) / 8) * ((res + 7) / 8) * ((res + 3) / 4);
+    k_bone_bake<<<dim3(nblk, uint32_t(ps.size())), 256, 0, st>>>(params.p, tris.p, sph.p, tsph.p, tile_off.p,
+                                                                 param_bone.p, atlas);
+  }
+};
+
+// Bone SDF colliders (simulation/mod.rs:1630-1960, :1998-2464): atlas,
+// per-bone infos and transforms, and the dynamic path (skinning, triangle
+// preparation and rebake of dirty bones before a frame).
+struct BoneSdfState {
+  std::vector<BoneInfo> info_h;
+  std::vector<BoneXform> xf_h;
+  DBuf<BoneInfo> info;
+  DBuf<BoneXform> xf;
+  DBuf<uint32_t> atlas;
+  uint32_t w = 0, h = 0, d = 0;
+  bool enabled = false;
+  // dynamic
+  bool dyn = false, dyn_on = false, baked = false;
+  uint32_t interval = 1, res = 0, nv = 0, nb = 0;
+  uint64_t counter = 0;
+  bool dirty_set = false;
+  std::vector<uint32_t> dirty;
+  std::vector<float> bind_inv;  // nb x 16, row-major
+  std::vector<BakeParams> params_h;
+  DBuf<float4> rest, bw, skinned;
+  DBuf<uint4> bidx, tsrc;
+  DBuf<float4> tsrcw;
+  DBuf<float> skin_m, inv_m;
+  BakeGpu bake;
+};
+
 // Learned warm start state of one simulator: the network, the correction of
 // the previous substep, the in-kernel residual judge and the recorded
 // training snapshots (features, target correction / L, free mask).
@@ -251,12 +326,13 @@ struct Sim {
   DBuf<float4> pin_t;
   // persistent solver (one cooperative launch per substep / frame)
   bool persistent = true;
-  unsigned int persist_blocks = 0, persist_max_per_sm = 0, num_sms = 0;
+  unsigned int persist_blocks = 0, persist_max_per_sm = 0, num_sms = 0, persist_bone_per_sm = 0;
   unsigned int spin_limit = 1u << 22;  // ~0.5 s of polling per barrier
   DBuf<GridBar> bar;
   DBuf<uint32_t> dist_offc, dist_cntc, bend_offc, bend_cntc;
   int* h_err = nullptr;  // pinned
   WarmStart ws;
+  BoneSdfState bone;
   // residual instrumentation
   bool track_residual = false;
   DBuf<float> res_sum, res_max;  // [ndc + nbc] each
@@ -444,9 +520,12 @@ struct Sim {
       int coop = 0, nsm = 0, per_sm = 0;
       TC_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
       TC_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-      TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solver_persistent, 256, 0));
+      TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solver_persistent<false>, 256, 0));
       persist_blocks = coop && per_sm > 0 ? unsigned(nsm * std::min(per_sm, 4)) : 0u;
       persist_max_per_sm = unsigned(per_sm);
+      int per_sm_bone = 0;
+      TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_bone, k_solver_persistent<true>, 256, 0));
+      persist_bone_per_sm = coop ? unsigned(per_sm_bone) : 0u;
       num_sms = unsigned(nsm);
       if (!persist_blocks) persistent = false;
     }
@@ -651,7 +730,104 @@ struct Sim {
     c.recovery = recovery;
     c.vinst = inst_prims_h.empty() ? nullptr : vinst.p;
     c.inst_prims = inst_prims_h.empty() ? nullptr : inst_prims.p;
+    c.bone = BoneSdfArgs{bone.info.p, bone.xf.p, bone.atlas.p,
+                         bone.enabled ? uint32_t(std::min(bone.info_h.size(), bone.xf_h.size())) : 0u,
+                         bone.w, bone.h, bone.d};
     return c;
+  }
+  bool has_colliders() const { return !prims_h.empty() || !tris_h.empty() || bone.enabled; }
+
+  // ---- bone SDF
+  // update_bone_transforms (simulation/mod.rs:1865-1935): store the
+  // transforms and the world bounding sphere of each bone in the infos' .w
+  void set_bone_transforms(const float* world, const float* inv, uint32_t nbt) {
+    bone.xf_h.resize(nbt);
+    for (uint32_t b = 0; b < nbt; ++b) {
+      std::memcpy(bone.xf_h[b].m, world + 16 * size_t(b), 64);
+      std::memcpy(bone.xf_h[b].inv, inv + 16 * size_t(b), 64);
+    }
+    const uint32_t nn = uint32_t(std::min(bone.info_h.size(), bone.xf_h.size()));
+    for (uint32_t b = 0; b < nn; ++b) {
+      BoneInfo& I = bone.info_h[b];
+      const float* m = bone.xf_h[b].m;
+      const float c[3] = {(I.aabb_min.x + I.aabb_max.x) * 0.5f, (I.aabb_min.y + I.aabb_max.y) * 0.5f,
+                          (I.aabb_min.z + I.aabb_max.z) * 0.5f};
+      const float ex = I.aabb_max.x - I.aabb_min.x, ey = I.aabb_max.y - I.aabb_min.y, ez = I.aabb_max.z - I.aabb_min.z;
+      const float rl = 0.5f * std::sqrt((ex * ex + ey * ey) + ez * ez);
+      float cw[3];
+      for (int j = 0; j < 3; ++j) cw[j] = ((m[0 + j] * c[0] + m[4 + j] * c[1]) + m[8 + j] * c[2]) + m[12 + j];
+      const float sx = std::sqrt((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2]);
+      const float sy = std::sqrt((m[4] * m[4] + m[5] * m[5]) + m[6] * m[6]);
+      const float sz = std::sqrt((m[8] * m[8] + m[9] * m[9]) + m[10] * m[10]);
+      const float rw = rl * std::fmax(std::fmax(sx, sy), sz) + 0.1f;
+      I.aabb_min.w = cw[0];
+      I.aabb_max.w = cw[1];
+      I.uvw_scale.w = cw[2];
+      I.uvw_offset.w = rw;
+    }
+    const void* before[2] = {bone.info.p, bone.xf.p};
+    if (!bone.info_h.empty()) bone.info.upload(bone.info_h, st);
+    if (!bone.xf_h.empty()) bone.xf.upload(bone.xf_h, st);
+    TC_CK(cudaStreamSynchronize(st));
+    const void* after[2] = {bone.info.p, bone.xf.p};
+    if (std::memcmp(before, after, sizeof before) != 0) mark();
+  }
+  void set_identity_transforms(uint32_t nbt) {
+    std::vector<float> id(16 * size_t(nbt), 0.f);
+    for (uint32_t b = 0; b < nbt; ++b)
+      for (int k = 0; k < 4; ++k) id[16 * size_t(b) + 5 * k] = 1.f;
+    set_bone_transforms(id.data(), id.data(), nbt);
+  }
+  void clear_bone() {
+    bone.info_h.clear();
+    bone.xf_h.clear();
+    bone.enabled = false;
+    bone.dyn = bone.dyn_on = false;
+    mark();
+  }
+  // dispatch_dynamic_bone_sdf_update (simulation/mod.rs:2320-2464), before a frame
+  void dynamic_bone_update() {
+    BoneSdfState& B = bone;
+    if (!B.dyn || !B.dyn_on) return;
+    B.counter += 1;
+    if ((B.counter - 1) % B.interval != 0) return;
+    if (B.xf_h.size() < B.nb) return;
+    std::vector<uint32_t> list;
+    if (!B.baked || !B.dirty_set) {
+      list.resize(B.nb);
+      for (uint32_t b = 0; b < B.nb; ++b) list[b] = b;
+    } else {
+      if (B.dirty.empty()) return;  // no pose change: nothing to do
+      for (uint32_t b : B.dirty)
+        if (b < B.nb) list.push_back(b);
+    }
+    std::vector<float> skin(16 * size_t(B.nb)), inv(16 * size_t(B.nb));
+    for (uint32_t b = 0; b < B.nb; ++b) {
+      float wr[4][4], bb[4][4], sr[4][4];
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) { wr[i][j] = B.xf_h[b].m[j * 4 + i]; bb[i][j] = B.bind_inv[16 * size_t(b) + i * 4 + j]; }
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+          sr[i][j] = ((wr[i][0] * bb[0][j] + wr[i][1] * bb[1][j]) + wr[i][2] * bb[2][j]) + wr[i][3] * bb[3][j];
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) skin[16 * size_t(b) + i * 4 + j] = sr[j][i];
+      std::memcpy(&inv[16 * size_t(b)], B.xf_h[b].inv, 64);
+    }
+    B.skin_m.upload(skin, st);
+    B.inv_m.upload(inv, st);
+    timed("bone_skin", [&] {
+      k_bone_skin<<<(B.nv + 127) / 128, 128, 0, st>>>(B.nv, B.rest.p, B.bidx.p, B.bw.p, B.skin_m.p, B.skinned.p);
+    });
+    timed("bone_prep", [&] {
+      if (B.bake.nt)
+        k_bone_prep<<<(B.bake.nt + 127) / 128, 128, 0, st>>>(B.bake.nt, B.skinned.p, B.inv_m.p, B.tsrc.p, B.tsrcw.p,
+                                                              B.bake.tris.p);
+    });
+    std::vector<BakeParams> ps;
+    for (uint32_t b : list) ps.push_back(B.params_h[b]);
+    timed("bone_bake", [&] { B.bake.bake(ps, list, B.atlas.p, st); });
+    TC_CK(cudaGetLastError());
+    B.baked = true;
   }
 
   void encode_residual(const SubstepParams& sp);
@@ -660,7 +836,7 @@ struct Sim {
     SolverArgs a;
     a.n = n; a.nsub = nsub; a.iters = iters; a.npins = uint32_t(pins.size());
     a.ndc = uint32_t(m.dist_cnt.size()); a.nbc = uint32_t(m.bend_cnt.size());
-    a.hascol = !prims_h.empty() || !tris_h.empty();
+    a.hascol = has_colliders();
     a.coupled = use_coupled;
     a.ddamp = td != 0.f || cd != 0.f || sd != 0.f;
     a.bdamp = bd != 0.f;
@@ -673,7 +849,7 @@ struct Sim {
     a.pin_v = pin_v.p; a.pin_t = pin_t.p;
     a.ca = collider_args();
     a.bar = bar.p;
-    a.expected = persist_blocks;
+    a.expected = 0;  // the launch fills in its grid size
     a.spin_limit = spin_limit;
     a.skip_predict = false;
     a.ppred = nullptr;
@@ -685,10 +861,21 @@ struct Sim {
     a.fallbacks = nullptr;
     return a;
   }
-  void launch_persistent(const SolverArgs& a) {
+  // the persistent path is available: cooperative launch, and with bone
+  // colliders the bone instantiation fits on an SM
+  bool can_persist() const { return persist_blocks > 0 && (!bone.enabled || persist_bone_per_sm > 0); }
+  unsigned persist_grid(bool with_bone) const {
+    if (!with_bone) return persist_blocks;
+    return num_sms * std::min(persist_blocks / std::max(num_sms, 1u), persist_bone_per_sm);
+  }
+  void launch_persistent(const SolverArgs& args) {
+    SolverArgs a = args;
+    const bool with_bone = a.ca.bone.nbones > 0;
+    const unsigned blocks = persist_grid(with_bone);
+    if (a.expected == 0) a.expected = blocks;
     TC_CK(cudaMemsetAsync(a.bar, 0, sizeof(GridBar), st));
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(persist_blocks);
+    cfg.gridDim = dim3(blocks);
     cfg.blockDim = dim3(256);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
@@ -696,7 +883,8 @@ struct Sim {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    TC_CK(cudaLaunchKernelEx(&cfg, k_solver_persistent, a));
+    if (with_bone) TC_CK(cudaLaunchKernelEx(&cfg, k_solver_persistent<true>, a));
+    else TC_CK(cudaLaunchKernelEx(&cfg, k_solver_persistent<false>, a));
   }
 
   // ---- learned warm start
@@ -809,13 +997,18 @@ struct Sim {
     if (last) *last = float(b / cnt);
   }
 
+  void launch_collision(const ColliderArgs& ca, float dts) {
+    if (ca.bone.nbones > 0) k_collision<true><<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts);
+    else k_collision<false><<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts);
+  }
+
   // encode_simulation_steps (dispatch.rs:7-354) for one frame
   void encode_frame(float dt, uint32_t substeps, bool use_coupled) {
     if (ws.on && !ws_recording()) {
       encode_frame_ws(dt, substeps, use_coupled);
       return;
     }
-    if (persistent && !profiling && !track_residual && !ws_recording()) {
+    if (persistent && can_persist() && !profiling && !track_residual && !ws_recording()) {
       const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
       if (!self_collision) {
         launch_persistent(solver_args(sp, substeps, use_coupled, true));
@@ -834,7 +1027,7 @@ struct Sim {
     SubstepParams sp{dts, g[0], g[1], g[2], damping, td, cd, sd, bd};
     const bool ddamp = td != 0.f || cd != 0.f || sd != 0.f;
     const bool bdamp = bd != 0.f;
-    const bool hascol = !prims_h.empty() || !tris_h.empty();
+    const bool hascol = has_colliders();
     const uint32_t npins = uint32_t(pins.size());
     ColliderArgs ca = collider_args();
     for (uint32_t s = 0; s < substeps; ++s) {
@@ -865,7 +1058,7 @@ struct Sim {
               k_bending<<<grid(m.bend_cnt[c], 256), 256, 0, st>>>(m.bend_off[c], m.bend_cnt[c], bend_ids.p,
                                                                    bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
         });
-        if (hascol && use_coupled) timed("collision", [&] { k_collision<<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts); });
+        if (hascol && use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
       }
       if (track_residual && s + 1 == substeps) encode_residual(sp);
       if (rec) {
@@ -874,7 +1067,7 @@ struct Sim {
                                                       rec_this ? ws.rec_mask.p + size_t(slot) * n : nullptr);
         if (rec_this) ++ws.rec_count;
       }
-      if (hascol && !use_coupled) timed("collision", [&] { k_collision<<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts); });
+      if (hascol && !use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
       if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
       if (self_collision) encode_self_collision();
       timed("update_vel", [&] { k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, dts); });
@@ -895,10 +1088,12 @@ struct Sim {
 
   void launch_frame(float dt, uint32_t substeps) {
     if (n == 0) return;
+    // the frame's device time (last_frame_ms) includes the dynamic bone SDF rebake
+    TC_CK(cudaEventRecord(ev0, st));
+    dynamic_bone_update();
     const bool use_coupled = coupled_for(dt, substeps);
     if (ws.on && !ws_recording()) ws.substeps_run += substeps;
     if (profiling || ws_recording()) {
-      TC_CK(cudaEventRecord(ev0, st));
       encode_frame(dt, substeps, use_coupled);
       TC_CK(cudaEventRecord(ev1, st));
       TC_CK(cudaStreamSynchronize(st));
@@ -940,7 +1135,6 @@ struct Sim {
       TC_CK(cudaMemsetAsync(res_sum.p, 0, (k + 1) * sizeof(float), st));
       TC_CK(cudaMemsetAsync(res_max.p, 0, (k + 1) * sizeof(float), st));
     }
-    TC_CK(cudaEventRecord(ev0, st));
     TC_CK(cudaGraphLaunch(gexec, st));
     TC_CK(cudaEventRecord(ev1, st));
   }
@@ -1731,6 +1925,7 @@ tc_status tc_check_barrier_timeout(tc_sim* s, uint32_t spin_limit) {
     const SubstepParams sp{1e-3f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     SolverArgs a = m.solver_args(sp, 1, false, false);
     a.n = 0; a.nd = 0; a.nb = 0; a.npins = 0; a.ndc = 0; a.nbc = 0; a.hascol = false;
+    a.ca.bone.nbones = 0;
     a.bar = m.bar.p + 1;
     a.expected = m.persist_blocks + 1;
     a.spin_limit = spin_limit;
@@ -1756,6 +1951,558 @@ tc_status tc_last_frame_ms(tc_sim* s, float* ms) {
   });
 }
 
+// ---- bone SDF colliders
+using tcloth::BakeParams;
+using tcloth::BakeTri;
+using tcloth::BoneInfo;
+using tcloth::BoneSdfState;
+
+static BoneInfo info_from_row(const float* r) {
+  return BoneInfo{make_float4(r[0], r[1], r[2], r[3]), make_float4(r[4], r[5], r[6], r[7]),
+                  make_float4(r[8], r[9], r[10], r[11]), make_float4(r[12], r[13], r[14], r[15]),
+                  make_float4(r[16], r[17], r[18], r[19])};
+}
+
+tc_status tc_set_bone_sdf_colliders(tc_sim* s, uint32_t width, uint32_t height, uint32_t depth,
+                                    const uint32_t* texels, size_t n_texels, const float* infos, uint32_t n_bones) {
+  return guard([&] {
+    Sim& m = S(s);
+    const size_t nvox = size_t(width) * height * depth;
+    need(n_texels == nvox && (nvox == 0 || texels != nullptr), "texture size must be width*height*depth texels");
+    need(n_bones == 0 || infos != nullptr, "bone_infos required");
+    m.bone.w = width; m.bone.h = height; m.bone.d = depth;
+    if (nvox) m.bone.atlas.upload(texels, nvox, m.st);
+    m.bone.info_h.resize(n_bones);
+    for (uint32_t b = 0; b < n_bones; ++b) m.bone.info_h[b] = info_from_row(infos + 20 * size_t(b));
+    m.bone.enabled = n_bones > 0 && nvox > 0;
+    m.mark();
+    if (n_bones) m.set_identity_transforms(n_bones);
+    TC_CK(cudaStreamSynchronize(m.st));
+  });
+}
+
+static void set_dirty(Sim& m, const uint32_t* dirty, int64_t ndirty) {
+  if (ndirty < 0) { m.bone.dirty_set = false; m.bone.dirty.clear(); return; }
+  m.bone.dirty_set = true;
+  m.bone.dirty.assign(dirty, dirty + ndirty);
+}
+
+tc_status tc_update_bone_transforms(tc_sim* s, const float* world, const float* inv_world, uint32_t n_bones,
+                                    const uint32_t* dirty, int64_t n_dirty) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(n_bones == 0 || (world && inv_world), "world and inverse matrices required");
+    need(n_dirty <= 0 || dirty != nullptr, "dirty list required");
+    if (n_bones) m.set_bone_transforms(world, inv_world, n_bones);
+    set_dirty(m, dirty, n_dirty);
+  });
+}
+
+tc_status tc_set_dynamic_bone_sdf_dirty_bones(tc_sim* s, const uint32_t* dirty, int64_t n_dirty) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(n_dirty <= 0 || dirty != nullptr, "dirty list required");
+    set_dirty(m, dirty, n_dirty);
+  });
+}
+
+tc_status tc_clear_bone_sdf_colliders(tc_sim* s) {
+  return guard([&] { S(s).clear_bone(); });
+}
+
+tc_status tc_set_dynamic_bone_sdf_enabled(tc_sim* s, int enable) {
+  return guard([&] { Sim& m = S(s); m.bone.dyn_on = enable != 0 && m.bone.dyn; });
+}
+
+tc_status tc_set_dynamic_bone_sdf_update_interval(tc_sim* s, uint32_t interval) {
+  return guard([&] { S(s).bone.interval = std::max(interval, 1u); });
+}
+
+// open boundary edges: undirected edges used by exactly one valid triangle
+// (sdf_baker.rs:203-240)
+static std::vector<uint64_t> open_boundary_edges(const int32_t* tris, size_t nt, size_t nv) {
+  std::vector<uint64_t> keys;
+  keys.reserve(nt * 3);
+  for (size_t t = 0; t < nt; ++t) {
+    const int32_t i0 = tris[3 * t], i1 = tris[3 * t + 1], i2 = tris[3 * t + 2];
+    if (i0 < 0 || i1 < 0 || i2 < 0 || size_t(i0) >= nv || size_t(i1) >= nv || size_t(i2) >= nv || i0 == i1 ||
+        i1 == i2 || i2 == i0)
+      continue;
+    const int32_t e[3][2] = {{i0, i1}, {i1, i2}, {i2, i0}};
+    for (auto& q : e)
+      keys.push_back((uint64_t(uint32_t(std::min(q[0], q[1]))) << 32) | uint32_t(std::max(q[0], q[1])));
+  }
+  std::sort(keys.begin(), keys.end());
+  std::vector<uint64_t> once;
+  for (size_t i = 0; i < keys.size();) {
+    size_t j = i;
+    while (j < keys.size() && keys[j] == keys[i]) ++j;
+    if (j - i == 1) once.push_back(keys[i]);
+    i = j;
+  }
+  return once;
+}
+static bool has_edge(const std::vector<uint64_t>& sorted, int32_t a, int32_t b) {
+  const uint64_t k = (uint64_t(uint32_t(std::min(a, b))) << 32) | uint32_t(std::max(a, b));
+  return std::binary_search(sorted.begin(), sorted.end(), k);
+}
+static uint32_t bmask_of(const std::vector<uint64_t>& open, int32_t i0, int32_t i1, int32_t i2) {
+  uint32_t m = 0;
+  if (has_edge(open, i0, i1)) m |= 1u;
+  if (has_edge(open, i1, i2)) m |= 2u;
+  if (has_edge(open, i2, i0)) m |= 4u;
+  return m;
+}
+
+tc_status tc_setup_dynamic_bone_sdf(tc_sim* s, uint32_t width, uint32_t height, uint32_t depth, uint32_t res,
+                                    const float* infos, uint32_t n_bones, const float* rest_verts,
+                                    uint32_t rest_cols, const uint32_t* bone_indices, const float* bone_weights,
+                                    uint32_t nv, const uint32_t* tri_sources, const float* tri_weights, uint32_t nt,
+                                    const float* bind_inv, uint32_t n_bind, uint32_t update_interval) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(res > 0 && width > 0 && height > 0 && depth > 0, "width, height, depth and res must be >= 1");
+    need(rest_cols >= 3, "rest_verts needs at least 3 columns");
+    need(n_bind >= n_bones, "bone_bind_inv_matrices must hold one matrix per bone");
+    need((nv == 0 || (rest_verts && bone_indices && bone_weights)) && (nt == 0 || (tri_sources && tri_weights)) &&
+             (n_bones == 0 || (infos && bind_inv)),
+         "arrays required");
+    // the reference's setup is a no-op without vertices, triangles or bones
+    if (nv == 0 || nt == 0 || n_bones == 0) return;
+    for (uint32_t i = 0; i < nv; ++i)
+      for (int k = 0; k < 4; ++k)
+        need(!(bone_weights[4 * size_t(i) + k] > 0.f) || bone_indices[4 * size_t(i) + k] < n_bones,
+             "bone index out of range for a weighted vertex");
+    for (uint32_t t = 0; t < nt; ++t) {
+      const uint32_t* q = tri_sources + 4 * size_t(t);
+      need(q[0] < nv && q[1] < nv && q[2] < nv && q[3] < n_bones, "triangle source index out of range");
+    }
+    BoneSdfState& B = m.bone;
+    B.info_h.resize(n_bones);
+    for (uint32_t b = 0; b < n_bones; ++b) B.info_h[b] = info_from_row(infos + 20 * size_t(b));
+    // open-boundary mask from the first occurrence of each distinct triangle (lib.rs:2490-2540)
+    std::vector<int32_t> uniq;
+    {
+      // (sorted triangle, index) pairs: the first index of each distinct key
+      std::vector<std::pair<std::array<uint32_t, 3>, uint32_t>> seen(nt);
+      for (uint32_t t = 0; t < nt; ++t) {
+        const uint32_t* q = tri_sources + 4 * size_t(t);
+        std::array<uint32_t, 3> k{q[0], q[1], q[2]};
+        std::sort(k.begin(), k.end());
+        seen[t] = std::make_pair(k, t);
+      }
+      std::sort(seen.begin(), seen.end());
+      std::vector<char> first(nt, 0);
+      for (uint32_t i = 0; i < nt; ++i)
+        if (i == 0 || seen[i].first != seen[i - 1].first) first[seen[i].second] = 1;
+      for (uint32_t t = 0; t < nt; ++t)
+        if (first[t]) {
+          const uint32_t* q = tri_sources + 4 * size_t(t);
+          uniq.push_back(int32_t(q[0])); uniq.push_back(int32_t(q[1])); uniq.push_back(int32_t(q[2]));
+        }
+    }
+    const std::vector<uint64_t> open = open_boundary_edges(uniq.data(), uniq.size() / 3, nv);
+    std::vector<uint4> src(nt);
+    std::vector<float4> srcw(nt);
+    std::vector<uint32_t> start(n_bones, 0), count(n_bones, 0);
+    for (uint32_t t = 0; t < nt; ++t) {
+      const uint32_t* q = tri_sources + 4 * size_t(t);
+      const float* w = tri_weights + 3 * size_t(t);
+      float bm = 0.f;
+      if (q[0] != q[1] && q[1] != q[2] && q[2] != q[0]) bm = float(bmask_of(open, int32_t(q[0]), int32_t(q[1]), int32_t(q[2])));
+      src[t] = make_uint4(q[0], q[1], q[2], q[3]);
+      srcw[t] = make_float4(w[0], w[1], w[2], bm);
+      if (count[q[3]] == 0) start[q[3]] = t;
+      count[q[3]] += 1;
+    }
+    const uint32_t ncols = std::max(width / res, 1u), nrows = std::max(height / res, 1u);
+    B.params_h.resize(n_bones);
+    for (uint32_t b = 0; b < n_bones; ++b) {
+      const uint32_t l = b / (ncols * nrows), rem = b % (ncols * nrows);
+      const BoneInfo& I = B.info_h[b];
+      B.params_h[b] = BakeParams{{I.aabb_min.x, I.aabb_min.y, I.aabb_min.z}, start[b],
+                                 {I.aabb_max.x, I.aabb_max.y, I.aabb_max.z}, count[b], rem % ncols, rem / ncols, l,
+                                 res, width, height, depth, 0u};
+      need(uint64_t(rem % ncols + 1) * res <= width && uint64_t(rem / ncols + 1) * res <= height &&
+               uint64_t(l + 1) * res <= depth,
+           "atlas too small for the bone tiles");
+    }
+    std::vector<float4> rp(nv), bwv(nv);
+    std::vector<uint4> bi(nv);
+    for (uint32_t i = 0; i < nv; ++i) {
+      const float* r = rest_verts + size_t(rest_cols) * i;
+      rp[i] = make_float4(r[0], r[1], r[2], 0.f);
+      const uint32_t* x = bone_indices + 4 * size_t(i);
+      const float* w = bone_weights + 4 * size_t(i);
+      bi[i] = make_uint4(x[0], x[1], x[2], x[3]);
+      bwv[i] = make_float4(w[0], w[1], w[2], w[3]);
+    }
+    B.rest.upload(rp, m.st); B.bidx.upload(bi, m.st); B.bw.upload(bwv, m.st); B.skinned.alloc(nv);
+    B.tsrc.upload(src, m.st); B.tsrcw.upload(srcw, m.st);
+    B.bake.nt = nt;
+    B.bake.tris.alloc(nt);
+    B.bake.setup_tiles(tcloth::make_bake_tiles(start, count), m.st);
+    B.bind_inv.assign(bind_inv, bind_inv + 16 * size_t(n_bones));
+    B.nv = nv; B.nb = n_bones; B.res = res;
+    B.w = width; B.h = height; B.d = depth;
+    const size_t nvox = size_t(width) * height * depth;
+    B.atlas.alloc(nvox);
+    TC_CK(cudaMemsetAsync(B.atlas.p, 0, nvox * 4, m.st));
+    // transforms: identity for bones without one yet (mod.rs:2055-2075); the
+    // infos' world bounding spheres follow the current transforms
+    {
+      const size_t nx = std::max<size_t>(B.xf_h.size(), n_bones);
+      std::vector<float> wm(16 * nx), im(16 * nx);
+      for (size_t b = 0; b < nx; ++b) {
+        if (b < B.xf_h.size()) {
+          std::memcpy(&wm[16 * b], B.xf_h[b].m, 64);
+          std::memcpy(&im[16 * b], B.xf_h[b].inv, 64);
+        } else {
+          for (int k = 0; k < 16; ++k) wm[16 * b + k] = im[16 * b + k] = (k % 5 == 0) ? 1.f : 0.f;
+        }
+      }
+      m.set_bone_transforms(wm.data(), im.data(), uint32_t(nx));
+    }
+    B.enabled = true;
+    B.dyn = true;
+    B.dyn_on = true;
+    B.baked = false;
+    B.dirty_set = false;
+    B.dirty.clear();
+    B.counter = 0;
+    B.interval = std::max(update_interval, 1u);
+    m.mark();
+    TC_CK(cudaStreamSynchronize(m.st));
+  });
+}
+
+tc_status tc_get_bone_sdf_atlas(tc_sim* s, uint32_t* out, size_t len, uint32_t dims[3]) {
+  return guard([&] {
+    Sim& m = S(s);
+    const size_t nvox = size_t(m.bone.w) * m.bone.h * m.bone.d;
+    if (dims) { dims[0] = m.bone.w; dims[1] = m.bone.h; dims[2] = m.bone.d; }
+    if (!out) return;
+    need(len >= nvox, "output array too small");
+    if (nvox) TC_CK(cudaMemcpyAsync(out, m.bone.atlas.p, nvox * 4, cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+  });
+}
+
+tc_status tc_get_bone_infos(tc_sim* s, float* out, size_t len, uint32_t* n_bones) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (n_bones) *n_bones = uint32_t(m.bone.info_h.size());
+    if (!out) return;
+    need(len >= m.bone.info_h.size() * 20, "output array too small");
+    std::memcpy(out, m.bone.info_h.data(), m.bone.info_h.size() * sizeof(BoneInfo));
+  });
+}
+
+// ---- bake_bone_sdf_gpu (sdf_baker.rs:465-940): host preparation, GPU bake
+struct tc_bake {
+  std::vector<uint32_t> texels;
+  uint32_t w = 0, h = 0, d = 0;
+  std::vector<float> infos;        // n_active x 20
+  std::vector<uint32_t> active;    // source bone index per active bone
+  std::vector<float> bind;         // n_active x 16 (row-major, as given)
+};
+
+namespace {
+// row-major 4x4 point transform with the projective divide (sdf_baker.rs:167-177)
+void tp_rowmajor(const float* m, const float* p, float* o) {
+  const float x = ((m[0] * p[0] + m[1] * p[1]) + m[2] * p[2]) + m[3];
+  const float y = ((m[4] * p[0] + m[5] * p[1]) + m[6] * p[2]) + m[7];
+  const float z = ((m[8] * p[0] + m[9] * p[1]) + m[10] * p[2]) + m[11];
+  const float w = ((m[12] * p[0] + m[13] * p[1]) + m[14] * p[2]) + m[15];
+  if (std::fabs(w) > 1e-7f && std::fabs(w - 1.0f) > 1e-5f) {
+    const float iw = 1.0f / w;
+    o[0] = x * iw; o[1] = y * iw; o[2] = z * iw;
+  } else {
+    o[0] = x; o[1] = y; o[2] = z;
+  }
+}
+void h_cross(const float* a, const float* b, float* o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+void h_normalize(const float* v, float* o) {
+  const float l2 = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
+  if (l2 > 1e-12f) {
+    const float inv = 1.0f / std::sqrt(l2);
+    o[0] = v[0] * inv; o[1] = v[1] * inv; o[2] = v[2] * inv;
+  } else {
+    o[0] = 0.f; o[1] = 1.f; o[2] = 0.f;
+  }
+}
+bool valid_tri(const int32_t* t, size_t nv) {
+  return !(t[0] < 0 || t[1] < 0 || t[2] < 0 || size_t(t[0]) >= nv || size_t(t[1]) >= nv || size_t(t[2]) >= nv ||
+           t[0] == t[1] || t[1] == t[2] || t[2] == t[0]);
+}
+// close_open_boundary_loops (sdf_baker.rs:242-453): fan caps over closed
+// boundary loops of solid meshes; the cap centre's bone weights are the loop
+// average.  weights: n_bones rows of `nv` (grown by one per added centre).
+void close_open_loops(std::vector<float>& verts, std::vector<int32_t>& tris, std::vector<std::vector<float>>& weights) {
+  const size_t nv = verts.size() / 3, nt = tris.size() / 3;
+  if (nt < 4 || nv < 4) return;
+  std::map<std::pair<int32_t, int32_t>, uint32_t> ecount;
+  std::vector<std::array<int32_t, 3>> existing;
+  for (size_t t = 0; t < nt; ++t) {
+    const int32_t* q = &tris[3 * t];
+    if (!valid_tri(q, nv)) continue;
+    std::array<int32_t, 3> k{q[0], q[1], q[2]};
+    std::sort(k.begin(), k.end());
+    existing.push_back(k);
+    const int32_t e[3][2] = {{q[0], q[1]}, {q[1], q[2]}, {q[2], q[0]}};
+    for (auto& x : e) ecount[{std::min(x[0], x[1]), std::max(x[0], x[1])}] += 1;
+  }
+  std::sort(existing.begin(), existing.end());
+  std::vector<std::pair<int32_t, int32_t>> bedges;
+  std::vector<std::array<float, 3>> bnormal;
+  std::map<int32_t, std::vector<size_t>> next;
+  for (size_t t = 0; t < nt; ++t) {
+    const int32_t* q = &tris[3 * t];
+    if (!valid_tri(q, nv)) continue;
+    const float* p0 = &verts[3 * size_t(q[0])];
+    const float* p1 = &verts[3 * size_t(q[1])];
+    const float* p2 = &verts[3 * size_t(q[2])];
+    const float e01[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    const float e02[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+    float cr[3], tn[3];
+    h_cross(e01, e02, cr);
+    h_normalize(cr, tn);
+    const int32_t e[3][2] = {{q[0], q[1]}, {q[1], q[2]}, {q[2], q[0]}};
+    for (auto& x : e) {
+      if (ecount[{std::min(x[0], x[1]), std::max(x[0], x[1])}] == 1) {
+        next[x[0]].push_back(bedges.size());
+        bedges.push_back({x[0], x[1]});
+        bnormal.push_back({tn[0], tn[1], tn[2]});
+      }
+    }
+  }
+  if (bedges.empty()) return;
+  std::vector<char> used(bedges.size(), 0);
+  for (size_t s0 = 0; s0 < bedges.size(); ++s0) {
+    if (used[s0]) continue;
+    used[s0] = 1;
+    const int32_t su = bedges[s0].first, sv = bedges[s0].second;
+    std::vector<int32_t> lv{su, sv};
+    std::vector<size_t> le{s0};
+    int32_t cur = sv;
+    bool closed = false;
+    while (lv.size() <= nv) {
+      if (cur == su) { lv.pop_back(); closed = true; break; }
+      bool found = false;
+      auto it = next.find(cur);
+      if (it != next.end())
+        for (size_t ei : it->second)
+          if (!used[ei]) {
+            used[ei] = 1;
+            le.push_back(ei);
+            cur = bedges[ei].second;
+            lv.push_back(cur);
+            found = true;
+            break;
+          }
+      if (!found) break;
+    }
+    const size_t k = lv.size();
+    if (!closed || k < 3 || k >= nv) continue;
+    const float invk = 1.0f / float(k);
+    float c[3] = {0.f, 0.f, 0.f};
+    for (int32_t v : lv)
+      for (int j = 0; j < 3; ++j) c[j] += verts[3 * size_t(v) + j];
+    for (int j = 0; j < 3; ++j) c[j] *= invk;
+    float cs[3] = {0.f, 0.f, 0.f};
+    for (size_t i = 0; i < k; ++i) {
+      const float* pu = &verts[3 * size_t(lv[i])];
+      const float* pv = &verts[3 * size_t(lv[(i + 1) % k])];
+      const float d1[3] = {pu[0] - pv[0], pu[1] - pv[1], pu[2] - pv[2]};
+      const float d2[3] = {c[0] - pv[0], c[1] - pv[1], c[2] - pv[2]};
+      float cn[3];
+      h_cross(d1, d2, cn);
+      for (int j = 0; j < 3; ++j) cs[j] += cn[j];
+    }
+    float capn[3];
+    h_normalize(cs, capn);
+    float ds = 0.f;
+    for (size_t ei : le) ds += (bnormal[ei][0] * capn[0] + bnormal[ei][1] * capn[1]) + bnormal[ei][2] * capn[2];
+    if (ds / float(std::max<size_t>(le.size(), 1)) <= -0.85f) continue;
+    if (k == 3) {
+      std::array<int32_t, 3> key{lv[0], lv[1], lv[2]};
+      std::sort(key.begin(), key.end());
+      if (std::binary_search(existing.begin(), existing.end(), key)) continue;
+      tris.insert(tris.end(), {lv[0], lv[2], lv[1]});
+      existing.insert(std::upper_bound(existing.begin(), existing.end(), key), key);
+      continue;
+    }
+    const int32_t ci = int32_t(verts.size() / 3);
+    verts.insert(verts.end(), {c[0], c[1], c[2]});
+    for (auto& w : weights) {
+      float ws = 0.f;
+      for (int32_t v : lv)
+        if (size_t(v) < w.size()) ws += w[size_t(v)];
+      while (w.size() < size_t(ci)) w.push_back(0.f);
+      w.push_back(ws * invk);
+    }
+    for (size_t i = 0; i < k; ++i) tris.insert(tris.end(), {lv[(i + 1) % k], lv[i], ci});
+  }
+}
+}  // namespace
+
+tc_status tc_bake_bone_sdf(const float* mesh_verts, uint32_t nv, const int32_t* mesh_tris, uint32_t nt,
+                           uint32_t n_bones, const float* bone_weights, const float* bind_matrices,
+                           uint32_t resolution, float margin, float weight_threshold, float blend_k, float friction,
+                           float thickness, float restitution, int close_open_boundaries, int device, tc_bake** out) {
+  return guard([&] {
+    need(out != nullptr, "out required");
+    *out = nullptr;
+    need(resolution >= 1, "resolution must be >= 1");
+    need((nv == 0 || mesh_verts) && (nt == 0 || mesh_tris) && (n_bones == 0 || (bone_weights && bind_matrices)),
+         "arrays required");
+    std::vector<float> verts(mesh_verts, mesh_verts + 3 * size_t(nv));
+    std::vector<int32_t> tris(mesh_tris, mesh_tris + 3 * size_t(nt));
+    std::vector<std::vector<float>> weights(n_bones);
+    for (uint32_t b = 0; b < n_bones; ++b) weights[b].assign(bone_weights + size_t(b) * nv, bone_weights + size_t(b + 1) * nv);
+    if (close_open_boundaries) close_open_loops(verts, tris, weights);
+    const size_t NV = verts.size() / 3, NT = tris.size() / 3;
+    const std::vector<uint64_t> open = open_boundary_edges(tris.data(), NT, NV);
+    std::vector<uint32_t> active;
+    for (uint32_t b = 0; b < n_bones; ++b) {
+      float mx = 0.f;
+      for (float w : weights[b]) mx = std::fmax(mx, w);
+      if (mx > weight_threshold) active.push_back(b);
+    }
+    if (active.empty()) throw TcError(TC_ERR_CUDA, "GPU SDF bake failed: no bone has skin weights above the threshold");
+    // compute_3d_atlas_layout (sdf_baker.rs:137-164)
+    const size_t na = active.size();
+    const size_t ncols = std::max<size_t>(size_t(std::ceil(std::pow(double(na), 1.0 / 3.0))), 1);
+    const size_t nrows = std::max<size_t>(size_t(std::ceil(std::sqrt(double((na + ncols - 1) / ncols)))), 1);
+    const size_t nlay = std::max<size_t>((na + ncols * nrows - 1) / (ncols * nrows), 1);
+    const size_t max_tile = std::max(std::max(ncols, nrows), nlay);
+    const size_t res = max_tile * resolution > 2048 ? std::max<size_t>(2048 / max_tile, 16) : resolution;
+    tc_bake* R = new tc_bake();
+    std::unique_ptr<tc_bake> guard_r(R);
+    R->w = uint32_t(ncols * res); R->h = uint32_t(nrows * res); R->d = uint32_t(nlay * res);
+    std::vector<BakeTri> all;
+    std::vector<BakeParams> params;
+    std::vector<uint32_t> starts, counts, pbone;
+    for (size_t ob = 0; ob < na; ++ob) {
+      const uint32_t sb = active[ob];
+      const float* M = bind_matrices + 16 * size_t(sb);
+      R->active.push_back(sb);
+      R->bind.insert(R->bind.end(), M, M + 16);
+      float mn[3] = {INFINITY, INFINITY, INFINITY}, mxp[3] = {-INFINITY, -INFINITY, -INFINITY};
+      size_t valid = 0;
+      for (size_t v = 0; v < weights[sb].size(); ++v)
+        if (weights[sb][v] > weight_threshold && v < NV) {
+          float pl[3];
+          tp_rowmajor(M, &verts[3 * v], pl);
+          for (int k = 0; k < 3; ++k) { mn[k] = std::fmin(mn[k], pl[k]); mxp[k] = std::fmax(mxp[k], pl[k]); }
+          ++valid;
+        }
+      if (!valid) for (int k = 0; k < 3; ++k) { mn[k] = -0.1f; mxp[k] = 0.1f; }
+      float size[3];
+      for (int k = 0; k < 3; ++k) size[k] = std::fmax(mxp[k] - mn[k], 0.05f);
+      for (int k = 0; k < 3; ++k) {
+        const float pad = size[k] * margin + std::fmax(thickness, 0.f);
+        mn[k] -= pad;
+        mxp[k] += pad;
+        size[k] = mxp[k] - mn[k];
+      }
+      const size_t bpl = ncols * nrows;
+      const uint32_t l = uint32_t(ob / bpl), rem = uint32_t(ob % bpl), r = uint32_t(rem / ncols), c = uint32_t(rem % ncols);
+      const float sl[3] = {1.0f / size[0], 1.0f / size[1], 1.0f / size[2]};
+      const float ol[3] = {-mn[0] / size[0], -mn[1] / size[1], -mn[2] / size[2]};
+      float row[20];
+      row[0] = mn[0]; row[1] = mn[1]; row[2] = mn[2]; row[3] = float(ob);
+      row[4] = mxp[0]; row[5] = mxp[1]; row[6] = mxp[2]; row[7] = float(res);
+      row[8] = sl[0] / float(ncols); row[9] = sl[1] / float(nrows); row[10] = sl[2] / float(nlay); row[11] = blend_k;
+      row[12] = (ol[0] + float(c)) / float(ncols); row[13] = (ol[1] + float(r)) / float(nrows);
+      row[14] = (ol[2] + float(l)) / float(nlay); row[15] = 0.f;
+      row[16] = friction; row[17] = thickness; row[18] = restitution; row[19] = weight_threshold;
+      R->infos.insert(R->infos.end(), row, row + 20);
+      const uint32_t ts = uint32_t(all.size());
+      for (size_t t = 0; t < NT; ++t) {
+        const int32_t* q = &tris[3 * t];
+        if (q[0] < 0 || q[1] < 0 || q[2] < 0 || size_t(q[0]) >= NV || size_t(q[1]) >= NV || size_t(q[2]) >= NV) continue;
+        const float w0 = size_t(q[0]) < weights[sb].size() ? weights[sb][size_t(q[0])] : 0.f;
+        const float w1 = size_t(q[1]) < weights[sb].size() ? weights[sb][size_t(q[1])] : 0.f;
+        const float w2 = size_t(q[2]) < weights[sb].size() ? weights[sb][size_t(q[2])] : 0.f;
+        if (!(w0 > 0.f || w1 > 0.f || w2 > 0.f)) continue;
+        float p0[3], p1[3], p2[3];
+        tp_rowmajor(M, &verts[3 * size_t(q[0])], p0);
+        tp_rowmajor(M, &verts[3 * size_t(q[1])], p1);
+        tp_rowmajor(M, &verts[3 * size_t(q[2])], p2);
+        float tmin[3], tmax[3];
+        for (int k = 0; k < 3; ++k) {
+          tmin[k] = std::fmin(std::fmin(p0[k], p1[k]), p2[k]);
+          tmax[k] = std::fmax(std::fmax(p0[k], p1[k]), p2[k]);
+        }
+        const bool overlap = tmin[0] <= mxp[0] && tmax[0] >= mn[0] && tmin[1] <= mxp[1] && tmax[1] >= mn[1] &&
+                             tmin[2] <= mxp[2] && tmax[2] >= mn[2];
+        if (!overlap) continue;
+        const float e01[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+        const float e02[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+        float cr[3], nn[3];
+        h_cross(e01, e02, cr);
+        h_normalize(cr, nn);
+        const uint32_t bm = bmask_of(open, q[0], q[1], q[2]);
+        all.push_back(BakeTri{make_float4(p0[0], p0[1], p0[2], w0), make_float4(p1[0], p1[1], p1[2], w1),
+                              make_float4(p2[0], p2[1], p2[2], w2), make_float4(nn[0], nn[1], nn[2], float(bm))});
+      }
+      const uint32_t tc = uint32_t(all.size()) - ts;
+      params.push_back(BakeParams{{mn[0], mn[1], mn[2]}, ts, {mxp[0], mxp[1], mxp[2]}, tc, c, r, l, uint32_t(res),
+                                  R->w, R->h, R->d, 0u});
+      starts.push_back(ts);
+      counts.push_back(tc);
+      pbone.push_back(uint32_t(ob));
+    }
+    if (all.empty())
+      all.push_back(BakeTri{make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 1, 0, 0)});
+    TC_CK(cudaSetDevice(device));
+    cudaStream_t st = nullptr;
+    TC_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); } } sg{st};
+    tcloth::BakeGpu G;
+    G.nt = uint32_t(all.size());
+    G.tris.upload(all, st);
+    G.setup_tiles(tcloth::make_bake_tiles(starts, counts), st);
+    tcloth::DBuf<uint32_t> atlas;
+    const size_t nvox = size_t(R->w) * R->h * R->d;
+    atlas.alloc(nvox);
+    TC_CK(cudaMemsetAsync(atlas.p, 0, nvox * 4, st));
+    G.bake(params, pbone, atlas.p, st);
+    R->texels.resize(nvox);
+    TC_CK(cudaMemcpyAsync(R->texels.data(), atlas.p, nvox * 4, cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaStreamSynchronize(st));
+    TC_CK(cudaGetLastError());
+    *out = guard_r.release();
+  });
+}
+
+tc_status tc_bake_dims(tc_bake* b, uint32_t out[4]) {
+  return guard([&] {
+    need(b && out, "bake result and output required");
+    out[0] = b->w; out[1] = b->h; out[2] = b->d; out[3] = uint32_t(b->active.size());
+  });
+}
+
+tc_status tc_bake_get(tc_bake* b, uint32_t* texels, float* infos, uint32_t* active, float* bind) {
+  return guard([&] {
+    need(b != nullptr, "bake result required");
+    if (texels) std::memcpy(texels, b->texels.data(), b->texels.size() * 4);
+    if (infos) std::memcpy(infos, b->infos.data(), b->infos.size() * 4);
+    if (active) std::memcpy(active, b->active.data(), b->active.size() * 4);
+    if (bind) std::memcpy(bind, b->bind.data(), b->bind.size() * 4);
+  });
+}
+
+tc_status tc_bake_destroy(tc_bake* b) {
+  delete b;
+  return TC_OK;
+}
+
 // ---- learned warm start
 uint32_t tc_ws_param_count(void) { return tcloth::kP_N; }
 
@@ -1763,7 +2510,7 @@ tc_status tc_ws_enable(tc_sim* s, int enable, uint32_t k_replaced, float res_thr
   return guard([&] {
     Sim& m = S(s);
     if (!enable) { if (m.ws.on) m.mark(); m.ws.on = false; return; }
-    need(m.persist_blocks > 0, "the warm start needs cooperative launch (persistent solver)");
+    need(m.can_persist(), "the warm start needs cooperative launch (persistent solver)");
     need(k_replaced >= 1 && k_replaced < m.iters, "k_replaced must be in [1, solver iterations - 1]");
     need(std::isfinite(res_thresh) || res_thresh > 0.f, "res_thresh must be a number or +inf");
     m.ws_setup();

@@ -8,6 +8,7 @@
 // One thread per vertex / constraint; each kernel restates one WGSL entry
 // point of crates/cloth_core/src/shaders/.
 #pragma once
+#include "bone_sdf.cuh"
 #include "vmath.cuh"
 
 namespace tcloth {
@@ -329,6 +330,7 @@ struct ColliderArgs {
   const float4* cl256;    // per 256 triangles
   uint32_t ntris;
   bool recovery;
+  BoneSdfArgs bone;       // bone SDF colliders (nbones == 0: off)
 };
 
 // Conservative skip test for a group of triangles: true only when every
@@ -344,7 +346,7 @@ __device__ __forceinline__ bool group_far(V3 a, V3 b, float4 g, float th) {
 // exactly like the reference; two levels of conservative bounding spheres
 // skip runs of triangles none of which could pass the per-triangle test, so
 // the sequence of applied contacts is unchanged.
-template <bool kCg>
+template <bool kCg, bool kBone = false>
 __device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ x4, float4* __restrict__ p4,
                                                const ColliderArgs& ca, float dt) {
   float4 x = ld4<kCg>(x4 + i);
@@ -414,14 +416,26 @@ __device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ 
     }
     if (!st.front && st.has_rec) contact(st.bpos, st.bn, st.bf, st.br, dt, pinit, xn, p);
   }
+  // phase 3: bone SDF, judged at the current p (collision.wgsl:648)
+  if (kBone && ca.bone.nbones > 0u) {
+    V3 tgt, bn;
+    float bf, br;
+    if (bone_sdf_contact(ca.bone, p, th, ca.ntris > 0u, tgt, bn, bf, br)) {
+      const V3 pb = p;
+      contact(tgt, bn, bf, br, dt, pb, xn, p);
+    }
+  }
   p4[i] = make_float4(p.x, p.y, p.z, pr.w);
   x4[i] = make_float4(xn.x, xn.y, xn.z, x.w);
 }
+// kBone: with the bone SDF phase (a separate instantiation, so that kernels
+// without bone colliders keep their register budget)
+template <bool kBone>
 __global__ void k_collision(uint32_t n, float4* __restrict__ x4, float4* __restrict__ p4, ColliderArgs ca,
                             float dt) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  collide_vertex<false>(i, x4, p4, ca, dt);
+  collide_vertex<false, kBone>(i, x4, p4, ca, dt);
 }
 
 // ---------------------------------------------------------------------
@@ -530,6 +544,7 @@ __device__ __forceinline__ float residual_bend(uint32_t ci, const uint4* ids, co
 // pin) and, with_update set, the velocity update; colours are separated by
 // grid barriers instead of kernel launches.  Same per-element functions, so
 // the same bits as the launch-per-colour path.
+template <bool kBone>
 __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -561,7 +576,7 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
         if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
       }
       if (a.hascol && a.coupled) {
-        for (uint32_t i = tid; i < a.n; i += stride) collide_vertex<true>(i, a.x4, a.p4, a.ca, dts);
+        for (uint32_t i = tid; i < a.n; i += stride) collide_vertex<true, kBone>(i, a.x4, a.p4, a.ca, dts);
         if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
       }
       if (it + 1 == a.iters && a.iters_extra > 0) {
@@ -610,7 +625,7 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
         a.dprev[i] = make_float4(p.x - q.x, p.y - q.y, p.z - q.z, 0.f);
       }
     if (a.hascol && !a.coupled) {
-      for (uint32_t i = tid; i < a.n; i += stride) collide_vertex<true>(i, a.x4, a.p4, a.ca, dts);
+      for (uint32_t i = tid; i < a.n; i += stride) collide_vertex<true, kBone>(i, a.x4, a.p4, a.ca, dts);
       if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
     }
     if (a.npins) {

@@ -32,6 +32,55 @@ def _arr(a, dtype, cols=None, name="array"):
     return x
 
 
+def bake_bone_sdf_gpu(mesh_verts, mesh_tris, bone_names, bone_weights, bone_bind_matrices, resolution=64,
+                      margin=0.2, weight_threshold=0.02, blend_k=0.05, friction=0.5, thickness=0.005,
+                      restitution=0.0, close_open_boundaries=True, device=0):
+    """Bone-local SDF atlas of a skinned mesh on the GPU (lib.rs:1186-1350).
+    Returns dict(texture_bytes, width, height, depth, bone_infos (N, 20),
+    active_bones, bind_matrices (N, 4, 4))."""
+    if resolution == 0:
+        raise ValueError("resolution must be >= 1")
+    v = np.ascontiguousarray(np.asarray(mesh_verts, _f32))
+    if v.ndim != 2 or v.shape[1] < 3:
+        raise ValueError("mesh_verts must have shape (N, 3)")
+    v = np.ascontiguousarray(v[:, :3])
+    t = np.ascontiguousarray(np.asarray(mesh_tris, np.int32))
+    if t.ndim != 2 or t.shape[1] < 3:
+        raise ValueError("mesh_tris must have shape (M, 3)")
+    t = np.ascontiguousarray(t[:, :3])
+    names = list(bone_names)
+    if len(bone_weights) != len(names):
+        raise ValueError("bone_names and bone_weights differ in length")
+    w = np.zeros((len(names), v.shape[0]), _f32)
+    for b, wb in enumerate(bone_weights):
+        wb = np.asarray(wb, _f32).ravel()
+        if wb.size != v.shape[0]:
+            raise ValueError(f"bone_weights[{b}] has {wb.size} entries for {v.shape[0]} vertices")
+        w[b] = wb
+    m = np.ascontiguousarray(np.asarray(bone_bind_matrices, _f32))
+    if m.ndim != 3 or m.shape[0] < len(names) or m.shape[1:] != (4, 4):
+        raise ValueError("bone_bind_matrices must have shape (N_bones, 4, 4)")
+    L = _lib.load()
+    h = C.c_void_p()
+    _lib.check(L.tc_bake_bone_sdf(_ptr(v), v.shape[0], _ptr(t), t.shape[0], len(names), _ptr(w), _ptr(m),
+                                  int(resolution), float(margin), float(weight_threshold), float(blend_k),
+                                  float(friction), float(thickness), float(restitution),
+                                  int(bool(close_open_boundaries)), int(device), C.byref(h)))
+    try:
+        dims = np.zeros(4, _u32)
+        _lib.check(L.tc_bake_dims(h, _ptr(dims)))
+        W, H, D, na = (int(x) for x in dims)
+        tex = np.zeros(W * H * D, _u32)
+        infos = np.zeros((na, 20), _f32)
+        active = np.zeros(na, _u32)
+        bind = np.zeros((na, 4, 4), _f32)
+        _lib.check(L.tc_bake_get(h, _ptr(tex), _ptr(infos), _ptr(active), _ptr(bind)))
+    finally:
+        L.tc_bake_destroy(h)
+    return {"texture_bytes": tex.tobytes(), "width": W, "height": H, "depth": D, "bone_infos": infos,
+            "active_bones": [names[int(i)] for i in active], "bind_matrices": bind}
+
+
 def is_gpu_available() -> bool:
     try:
         return bool(_lib.load().tc_gpu_available())
@@ -373,6 +422,97 @@ class ClothSimulator:
         v = C.c_float()
         self._c(self._L.tc_last_frame_ms(self._h, C.byref(v)))
         return v.value
+
+    # ---- bone SDF colliders (lib.rs:2245-2600)
+    @staticmethod
+    def _mats(a, name):
+        m = np.ascontiguousarray(np.asarray(a, _f32))
+        if m.ndim != 3 or m.shape[1:] != (4, 4):
+            raise ValueError(f"{name} must have shape (N, 4, 4)")
+        return m
+
+    @staticmethod
+    def _dirty(d):
+        if d is None:
+            return None, -1
+        x = np.ascontiguousarray(np.asarray(d, _u32).ravel())
+        return x, x.size
+
+    def set_bone_sdf_colliders(self, width, height, depth, texture_bytes, bone_infos):
+        """Static atlas: Rg16Float texture bytes (width x height x depth x 4) and
+        bone_infos of shape (N, 20)."""
+        tex = np.frombuffer(bytes(texture_bytes), dtype=np.uint32)
+        info = np.ascontiguousarray(np.asarray(bone_infos, _f32))
+        if info.ndim != 2 or (info.size and info.shape[1] < 20):
+            raise ValueError("bone_infos rows need at least 20 elements")
+        info = np.ascontiguousarray(info[:, :20]) if info.size else np.zeros((0, 20), _f32)
+        self._c(self._L.tc_set_bone_sdf_colliders(self._h, int(width), int(height), int(depth), _ptr(tex),
+                                                  tex.size, _ptr(info), info.shape[0]))
+
+    def update_bone_transforms(self, world_matrices, inv_world_matrices, dirty_bone_indices=None):
+        w = self._mats(world_matrices, "world_matrices")
+        iw = self._mats(inv_world_matrices, "inv_world_matrices")
+        if iw.shape[0] != w.shape[0]:
+            raise ValueError("world_matrices and inv_world_matrices need the same shape (N, 4, 4)")
+        d, nd = self._dirty(dirty_bone_indices)
+        self._c(self._L.tc_update_bone_transforms(self._h, _ptr(w), _ptr(iw), w.shape[0], _ptr(d), nd))
+
+    def set_dynamic_bone_sdf_dirty_bones(self, dirty_bone_indices=None):
+        d, nd = self._dirty(dirty_bone_indices)
+        self._c(self._L.tc_set_dynamic_bone_sdf_dirty_bones(self._h, _ptr(d), nd))
+
+    def clear_bone_sdf_colliders(self):
+        self._c(self._L.tc_clear_bone_sdf_colliders(self._h))
+
+    def setup_dynamic_bone_sdf(self, width, height, depth, res, bone_infos, rest_verts, bone_indices, bone_weights,
+                               tri_sources, tri_weights, bone_bind_inv_matrices, update_interval=1):
+        if res == 0 or width == 0 or height == 0 or depth == 0:
+            raise ValueError("width, height, depth and res must be >= 1")
+        info = np.ascontiguousarray(np.asarray(bone_infos, _f32))
+        if info.ndim != 2 or info.shape[1] < 20:
+            raise ValueError("bone_infos rows need at least 20 elements")
+        info = np.ascontiguousarray(info[:, :20])
+        rv = np.ascontiguousarray(np.asarray(rest_verts, _f32))
+        bi = np.ascontiguousarray(np.asarray(bone_indices, _u32))
+        bw = np.ascontiguousarray(np.asarray(bone_weights, _f32))
+        if rv.ndim != 2 or rv.shape[1] < 3 or bi.ndim != 2 or bi.shape[1] < 4 or bw.ndim != 2 or bw.shape[1] < 4:
+            raise ValueError("rest_verts needs >= 3 columns, bone_indices / bone_weights >= 4")
+        if bi.shape[0] != rv.shape[0] or bw.shape[0] != rv.shape[0]:
+            raise ValueError("rest_verts, bone_indices and bone_weights need the same vertex count")
+        bi = np.ascontiguousarray(bi[:, :4])
+        bw = np.ascontiguousarray(bw[:, :4])
+        ts = np.ascontiguousarray(np.asarray(tri_sources, _u32))
+        tw = np.ascontiguousarray(np.asarray(tri_weights, _f32))
+        if ts.ndim != 2 or ts.shape[1] < 4 or tw.ndim != 2 or tw.shape[1] < 3 or tw.shape[0] != ts.shape[0]:
+            raise ValueError("tri_sources (M, 4) and tri_weights (M, 3) are required")
+        ts = np.ascontiguousarray(ts[:, :4])
+        tw = np.ascontiguousarray(tw[:, :3])
+        inv = self._mats(bone_bind_inv_matrices, "bone_bind_inv_matrices")
+        self._c(self._L.tc_setup_dynamic_bone_sdf(
+            self._h, int(width), int(height), int(depth), int(res), _ptr(info), info.shape[0], _ptr(rv), rv.shape[1],
+            _ptr(bi), _ptr(bw), rv.shape[0], _ptr(ts), _ptr(tw), ts.shape[0], _ptr(inv), inv.shape[0],
+            int(update_interval)))
+
+    def set_dynamic_bone_sdf_enabled(self, enabled):
+        self._c(self._L.tc_set_dynamic_bone_sdf_enabled(self._h, int(bool(enabled))))
+
+    def set_dynamic_bone_sdf_update_interval(self, interval):
+        self._c(self._L.tc_set_dynamic_bone_sdf_update_interval(self._h, int(interval)))
+
+    def get_bone_sdf_atlas(self):
+        """(width, height, depth), uint32 texels (packed half2: distance, alpha)."""
+        dims = np.zeros(3, _u32)
+        self._c(self._L.tc_get_bone_sdf_atlas(self._h, None, 0, _ptr(dims)))
+        out = np.zeros(int(dims[0]) * int(dims[1]) * int(dims[2]), _u32)
+        self._c(self._L.tc_get_bone_sdf_atlas(self._h, _ptr(out), out.size, _ptr(dims)))
+        return tuple(int(x) for x in dims), out
+
+    def get_bone_infos(self):
+        n = C.c_uint32()
+        self._c(self._L.tc_get_bone_infos(self._h, None, 0, C.byref(n)))
+        out = np.zeros((n.value, 20), _f32)
+        self._c(self._L.tc_get_bone_infos(self._h, _ptr(out), out.size, C.byref(n)))
+        return out
 
     # ---- learned warm start (new; no counterpart in the reference)
     def ws_enable(self, k_replaced=1, res_thresh=float("inf")):
