@@ -108,6 +108,13 @@ tc_status tc_add_plane_collider(tc_sim *s, const float point[3], const float nor
 tc_status tc_set_mesh_collider_triangles(tc_sim *s, const float *triangles, uint32_t T, float friction,
                                          float thickness, float restitution, int single_sided, const float *attributes);
 tc_status tc_clear_colliders(tc_sim *s);
+/* Self-collision every `interval` substeps and on the last (>= 1), and the
+ * edge-edge pass every `interval` substeps and on the last (0 = never,
+ * 1 = always): dispatch.rs:105-114, mod.rs:1071-1088.  Defaults 1 / 1.
+ * out = (self-collision interval, E-E interval). */
+tc_status tc_set_self_collision_substep_interval(tc_sim *s, uint32_t interval);
+tc_status tc_set_self_collision_ee_substep_interval(tc_sim *s, uint32_t interval);
+tc_status tc_get_self_collision_intervals(tc_sim *s, uint32_t out[2]);
 
 /* Bone SDF colliders (lib.rs:2245-2600, simulation/mod.rs:1630-2464).  The
  * atlas is width x height x depth texels of packed half2 (distance in the low

@@ -76,6 +76,7 @@ def lib():
         L.ocl_build_hash.argtypes = [P, C.c_int, up, up]
         L.ocl_get_mesh_triangles.argtypes = [P, fp]
         L.ocl_half_roundtrip.argtypes = [P, C.c_int, P, P]
+        L.ocl_set_self_collision_intervals.argtypes = [P, C.c_int, C.c_int]
         L.ocl_bone_skin_mats.argtypes = [C.c_int, P, P, P]
         L.ocl_bone_skin.argtypes = [C.c_int, P, P, P, P, P]
         L.ocl_bone_prep.argtypes = [C.c_int, P, P, P, P, P]
@@ -338,3 +339,17 @@ def _set_bone_sdf(self, dims, atlas, infos, xforms32):
 
 
 OracleSim.set_bone_sdf = _set_bone_sdf
+
+
+def _set_sc_interval(self, interval):
+    self._sc_iv = max(int(interval), 1)
+    lib().ocl_set_self_collision_intervals(self._h, self._sc_iv, getattr(self, "_ee_iv", 1))
+
+
+def _set_ee_interval(self, interval):
+    self._ee_iv = int(interval)
+    lib().ocl_set_self_collision_intervals(self._h, getattr(self, "_sc_iv", 1), self._ee_iv)
+
+
+OracleSim.set_self_collision_substep_interval = _set_sc_interval
+OracleSim.set_self_collision_ee_substep_interval = _set_ee_interval

@@ -164,6 +164,7 @@ struct OSim {
     float last_max_disp, last_eff_disp;
     float cloth_thickness;
     int single_sided_recovery;
+    int sc_interval, ee_interval; /* self-collision / E-E substep intervals (dispatch.rs:105-114) */
     /* bone SDF colliders (collision.wgsl:116-265) */
     uint32_t *atlas; uint32_t aw, ah, ad; int nbones;
     float *binfo;   /* nbones x 20 */
@@ -317,6 +318,8 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, cons
                  const float *thicknesses, uint32_t layer_id, float thickness, float tension_k,
                  float compression_k, float shear_k, float bending_k) {
     OSim *s = (OSim *)calloc(1, sizeof(OSim));
+    s->sc_interval = 1;
+    s->ee_interval = 1;
     s->n = n;
     size_t N = (size_t)(n > 0 ? n : 1);
     s->x = (v3 *)calloc(N, sizeof(v3)); s->p = (v3 *)calloc(N, sizeof(v3));
@@ -2366,15 +2369,19 @@ static void k_apply(OSim *s) {
 
 /* dispatch_self_collision_passes, simulation/dispatch.rs:1460-1717
  * (DIRECT algorithm, pair cache off) */
-static void self_collision(OSim *s) {
+static void self_collision(OSim *s, int run_ee) {
     int untangle = s->untangle_opt && s->multi_layer;
     if (untangle) k_normals(s);
     build_hash(s, 0);
-    if (s->ne > 0) build_hash(s, 1);
+    if (run_ee && s->ne > 0) build_hash(s, 1);
     k_sc_solve(s, untangle);
     if (untangle) k_untangle(s);
-    if (s->ne > 0) k_ee(s, untangle);
+    if (run_ee && s->ne > 0) k_ee(s, untangle);
     k_apply(s);
+}
+void ocl_set_self_collision_intervals(OSim *s, int sc_interval, int ee_interval) {
+    s->sc_interval = sc_interval < 1 ? 1 : sc_interval;
+    s->ee_interval = ee_interval < 0 ? 0 : ee_interval;
 }
 
 /* encode_simulation_steps, simulation/dispatch.rs:7-354 (default modes:
@@ -2392,6 +2399,9 @@ void ocl_step(OSim *s, float dt, int substeps) {
     int coupled = s->coupled || (s->auto_coupled && risk);
     int hascol = s->ncols > 0 || s->ntris > 0 || s->nbones > 0;
     for (int sub = 0; sub < substeps; sub++) {
+        int last = sub + 1 == substeps;
+        int do_sc = s->self_collision && (s->sc_interval <= 1 || sub % s->sc_interval == 0 || last);
+        int run_ee = s->ee_interval == 0 ? 0 : (s->ee_interval == 1 ? 1 : (sub % s->ee_interval == 0 || last));
         memset(s->dlam, 0, 4 * ((size_t)s->nd + 1));
         memset(s->blam, 0, 4 * ((size_t)s->nb + 1));
         k_predict(s, dts);
@@ -2403,7 +2413,7 @@ void ocl_step(OSim *s, float dt, int substeps) {
         }
         if (hascol && !coupled) k_collision(s, dts);
         if (s->npins > 0) k_pin(s, dts);
-        if (s->self_collision) self_collision(s);
+        if (do_sc) self_collision(s, run_ee);
         k_update_vel(s, dts);
     }
 }

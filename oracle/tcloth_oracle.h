@@ -85,6 +85,8 @@ float ocl_cell_size(const OSim *s);
  * predicted positions; outputs cell_starts (table+1) and sorted (n). */
 void ocl_build_hash(OSim *s, int which, uint32_t *cell_starts, uint32_t *sorted);
 void ocl_get_mesh_triangles(const OSim *s, float *tris16);  /* T x 16 floats (sorted) */
+/* self-collision / E-E substep intervals (dispatch.rs:105-114); defaults 1 / 1 */
+void ocl_set_self_collision_intervals(OSim *s, int sc_interval, int ee_interval);
 
 /* Bone SDF (skinning.wgsl, prep_bone_triangles.wgsl, bake_sdf.wgsl,
  * collision.wgsl:116-265).  Matrices: 16 floats, column-major

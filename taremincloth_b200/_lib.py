@@ -75,6 +75,9 @@ SIGNATURES = {
     "tc_check_barrier_timeout": [_P, _U],
     "tc_hash_build_static": [_P, _U, _F, _U, _P, _P, _P],
     "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],
+    "tc_set_self_collision_substep_interval": [_P, _U],
+    "tc_set_self_collision_ee_substep_interval": [_P, _U],
+    "tc_get_self_collision_intervals": [_P, _P],
     "tc_set_bone_sdf_colliders": [_P, _U, _U, _U, _P, C.c_size_t, _P, _U],
     "tc_update_bone_transforms": [_P, _P, _P, _U, _P, C.c_int64],
     "tc_set_dynamic_bone_sdf_dirty_bones": [_P, _P, C.c_int64],

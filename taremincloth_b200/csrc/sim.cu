@@ -344,6 +344,14 @@ struct Sim {
   float relief = 0.2f, max_disp_ratio = 0.2f;
   bool enable_relief = true, exclude_neighbors = true, untangle_opt = true;
   uint32_t max_search = 256;
+  // self-collision / E-E substep intervals (dispatch.rs:105-114, defaults mod.rs:624-625)
+  uint32_t sc_interval = 1, ee_interval = 1;
+  bool sc_due(uint32_t s, uint32_t substeps) const {
+    return self_collision && (sc_interval <= 1 || s % sc_interval == 0 || s + 1 == substeps);
+  }
+  bool ee_due(uint32_t s, uint32_t substeps) const {
+    return ee_interval == 0 ? false : (ee_interval == 1 ? true : (s % ee_interval == 0 || s + 1 == substeps));
+  }
   bool coupled = false, auto_coupled = true, recovery = true;
   float cloth_thickness = 0.005f;
   float last_max_disp = 0.f, last_eff_disp = 0.f;
@@ -703,14 +711,14 @@ struct Sim {
     });
   }
 
-  void encode_self_collision() {
+  void encode_self_collision(bool run_ee = true) {
     SCArgs a = sc_args();
     if (a.untangle) timed("sc_normals", [&] { k_normals<<<grid(n, 256), 256, 0, st>>>(n, x4.p, star_off.p, star_idx.p, nrm.p); });
     encode_hash(0);
-    if (ne > 0) encode_hash(1);
+    if (run_ee && ne > 0) encode_hash(1);
     timed("sc_solve", [&] { k_sc_solve<<<grid(n, 8), 256, 0, st>>>(a); });
     if (a.untangle) timed("sc_untangle", [&] { k_untangle<<<grid(n, 128), 128, 0, st>>>(a); });
-    if (ne > 0) {
+    if (run_ee && ne > 0) {
       timed("sc_solve_ee", [&] {
         TC_CK(cudaMemsetAsync(ccd_n.p, 0, sizeof(uint32_t), st));
         k_ee<<<grid(ne, 8), 256, 0, st>>>(a);
@@ -954,7 +962,7 @@ struct Sim {
       a.fallbacks = ws.fallbacks.p;
       timed("solver", [&] { launch_persistent(a); });
       if (self_collision) {
-        encode_self_collision();
+        if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
         timed("update_vel", [&] { k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp.dt); });
       }
     }
@@ -1015,7 +1023,7 @@ struct Sim {
       } else {
         for (uint32_t s = 0; s < substeps; ++s) {
           launch_persistent(solver_args(sp, 1, use_coupled, false));
-          encode_self_collision();
+          if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
           k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp.dt);
         }
       }
@@ -1069,7 +1077,7 @@ struct Sim {
       }
       if (hascol && !use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
       if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
-      if (self_collision) encode_self_collision();
+      if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
       timed("update_vel", [&] { k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, dts); });
     }
     TC_CK(cudaGetLastError());
@@ -2501,6 +2509,22 @@ tc_status tc_bake_get(tc_bake* b, uint32_t* texels, float* infos, uint32_t* acti
 tc_status tc_bake_destroy(tc_bake* b) {
   delete b;
   return TC_OK;
+}
+
+// ---- self-collision substep intervals (mod.rs:1071-1088)
+tc_status tc_set_self_collision_substep_interval(tc_sim* s, uint32_t interval) {
+  return guard([&] { Sim& m = S(s); m.sc_interval = std::max(interval, 1u); m.mark(); });
+}
+tc_status tc_set_self_collision_ee_substep_interval(tc_sim* s, uint32_t interval) {
+  return guard([&] { Sim& m = S(s); m.ee_interval = interval; m.mark(); });
+}
+tc_status tc_get_self_collision_intervals(tc_sim* s, uint32_t out[2]) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr, "out required");
+    out[0] = m.sc_interval;
+    out[1] = m.ee_interval;
+  });
 }
 
 // ---- learned warm start

@@ -423,6 +423,24 @@ class ClothSimulator:
         self._c(self._L.tc_last_frame_ms(self._h, C.byref(v)))
         return v.value
 
+    # ---- self-collision substep intervals (lib.rs:1966-2000)
+    def set_self_collision_substep_interval(self, interval):
+        self._c(self._L.tc_set_self_collision_substep_interval(self._h, int(interval)))
+
+    def set_self_collision_ee_substep_interval(self, interval):
+        self._c(self._L.tc_set_self_collision_ee_substep_interval(self._h, int(interval)))
+
+    def _intervals(self):
+        out = np.zeros(2, _u32)
+        self._c(self._L.tc_get_self_collision_intervals(self._h, _ptr(out)))
+        return out
+
+    def get_self_collision_substep_interval(self):
+        return int(self._intervals()[0])
+
+    def get_self_collision_ee_substep_interval(self):
+        return int(self._intervals()[1])
+
     # ---- bone SDF colliders (lib.rs:2245-2600)
     @staticmethod
     def _mats(a, name):
