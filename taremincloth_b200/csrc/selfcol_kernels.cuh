@@ -408,16 +408,18 @@ __device__ __forceinline__ bool sc_filter(const SCArgs& s, const VertCtx& c, con
 }
 
 // Contact work for one candidate that passed sc_filter
-// (shaders/self_collision.wgsl:392-670).
-__device__ __forceinline__ void sc_work(const SCArgs& s, const VertCtx& c, const TwoHop& th, uint32_t slot) {
+// (shaders/self_collision.wgsl:392-670), part 1: the vertex-vertex contact
+// and the vertex-triangle gate.  Returns true with the star range of j when
+// j's incident triangles must be tested (part 2, vt_entry).
+__device__ __forceinline__ bool sc_work_vv(const SCArgs& s, const VertCtx& c, const TwoHop& th, uint32_t slot,
+                                           uint32_t& st_b, uint32_t& st_e, float4& rec0, float4& rec1) {
   const uint32_t index = c.index;
   const int4 jc = s.vs_c[slot];
   const uint32_t j = (uint32_t)jc.w;
   const float wi = c.wi;
   const bool pin_i = c.pin_i;
-  const V3 xi = c.xi, pi = c.pi;
+  const V3 pi = c.pi;
   const float mli = c.mli, thi = c.thi, lli = c.lli;
-  const I3 cell = c.cell;
   const uint32_t li = c.li;
   const bool untangle = c.untangle;
   int32_t* acc = s.acc;
@@ -430,7 +432,7 @@ __device__ __forceinline__ void sc_work(const SCArgs& s, const VertCtx& c, const
   const float eth = fmaxf(thi + thj, fminf(lli, llj) * 0.06f);
   const uint32_t lj = __float_as_uint(q.y);
   const float dvl = sqrtf(fmaxf(d2, 0.0f));
-  if (near_folded_t(th, index, j, dvl)) return;
+  if (near_folded_t(th, index, j, dvl)) return false;
   const V3 pjo = mk(s.x4[j]);
   const float wj = q.z;
   const bool both = wj > 0.0f;
@@ -473,145 +475,195 @@ __device__ __forceinline__ void sc_work(const SCArgs& s, const VertCtx& c, const
   // 2. vertex-triangle
   const float mlj = q.w;
   const float vtb = eth + llj * 1.3f + mli + mlj;
-  if (!(d2 <= vtb * vtb) || within2_t(th, index, j)) return;
-  for (uint32_t st = s.star_off[j]; st < s.star_off[j + 1]; ++st) {
-    const uint2 pr = s.star_idx[st];
-    const uint32_t v0 = pr.x, v1 = pr.y;
-    if (v0 == index || v1 == index) continue;
-    const float4 q0 = s.p4[v0], q1 = s.p4[v1];
-    const float4 o0 = s.x4[v0], o1 = s.x4[v1];
-    const V3 pv0 = mk(q0), pv1 = mk(q1), pv0o = mk(o0), pv1o = mk(o1);
-    const float wv0 = o0.w, wv1 = o1.w;
-    const V3 d0 = pi - pv0;
-    const float ll0 = s.local_len[v0];
-    const float et0 = fmaxf(thi + q0.w, fminf(lli, ll0) * 0.06f);
-    const float b0 = et0 + ll0 * 1.3f + mli + s.mlen[v0];
-    const int4 c0 = s.vcell[v0];
-    const bool in0 = abs(c0.x - cell.x) <= 1 && abs(c0.y - cell.y) <= 1 && abs(c0.z - cell.z) <= 1 &&
-                     (dot(d0, d0) <= b0 * b0);
-    const V3 d1 = pi - pv1;
-    const float ll1 = s.local_len[v1];
-    const float et1 = fmaxf(thi + q1.w, fminf(lli, ll1) * 0.06f);
-    const float b1 = et1 + ll1 * 1.3f + mli + s.mlen[v1];
-    const int4 c1 = s.vcell[v1];
-    const bool in1 = abs(c1.x - cell.x) <= 1 && abs(c1.y - cell.y) <= 1 && abs(c1.z - cell.z) <= 1 &&
-                     (dot(d1, d1) <= b1 * b1);
-    if ((in0 && j > v0) || (in1 && j > v1)) continue;
-    const V3 tmove = (((pj - pjo) + (pv0 - pv0o)) + (pv1 - pv1o)) / 3.0f;
-    const bool tpin = (wj <= 0.0f) || (wv0 <= 0.0f) || (wv1 <= 0.0f);
-    const V3 rel = xi + tmove;
-    const V3 E = mk(eth, eth, eth);
-    const V3 smin = vmin(rel, pi) - E, smax = vmax(rel, pi) + E;
-    const V3 tmin = vmin(vmin(pj, pv0), pv1), tmax = vmax(vmax(pj, pv0), pv1);
-    if (smin.x > tmax.x || smin.y > tmax.y || smin.z > tmax.z || smax.x < tmin.x || smax.y < tmin.y ||
-        smax.z < tmin.z)
-      continue;
-    if (within2_t(th, index, v0) || within2_t(th, index, v1)) continue;
-    const V3 mv = pi - rel;
-    const float msq = dot(mv, mv);
-    float ht = 1.0f, hu = 0.0f, hv = 0.0f;
-    bool hit = false;
-    if (msq > 1e-12f) hit = seg_tri(rel, pi, pj, pv0, pv1, ht, hu, hv);
-    if (hit) {
-      const V3 hp = rel + mv * ht;
-      const V3 tc = cross(pv0 - pj, pv1 - pj);
-      const float tl = length(tc);
-      const V3 tn = tl > 1e-12f ? tc / tl : mk(0.0f, 1.0f, 0.0f);
-      const float hor = dot(rel - pj, tn);
-      bool utc = false;
-      if (untangle && !pin_i && (li > lj) && tl > 1e-12f) {
-        const V3 ni = mk(s.nrm[index]);
-        const float nil = length(ni);
-        const bool allow = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
-        const bool ret = (hor < 0.0f) && (dot(mv, tn) > 0.0f);
-        utc = allow && ret;
-      }
-      if (!utc) {
-        const float ss = fabsf(hor) > 1e-6f ? hor : dot(-mv, tn);
-        const V3 ns = ss >= 0.0f ? tn : -tn;
-        const float ho = fmaxf(dot(rel - hp, ns), 0.0f);
-        const float hs = fmaxf(ho, eth * 0.25f);
-        const V3 psafe = hp + ns * hs;
-        const V3 tccd = psafe - pi;
-        const float pcs = fmaxf(0.0f, eth - hs);
-        if (tpin) {
-          if (!pin_i) add_ccd(acc, index, tccd + ns * pcs, false);
-        } else if (pin_i) {
-          const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
-          const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
-          if (wt > kEps) {
-            const V3 full = tccd + ns * pcs;
-            if (wj > 0.0f) add_ccd(acc, j, (-full) * (bc.x * wj / wt), false);
-            if (wv0 > 0.0f) add_ccd(acc, v0, (-full) * (bc.y * wv0 / wt), false);
-            if (wv1 > 0.0f) add_ccd(acc, v1, (-full) * (bc.z * wv1 / wt), false);
+  if (!(d2 <= vtb * vtb) || within2_t(th, index, j)) return false;
+  st_b = s.star_off[j];
+  st_e = s.star_off[j + 1];
+  // what the triangle filter needs of j: p, contact thickness, x, index
+  rec0 = make_float4(pj.x, pj.y, pj.z, eth);
+  rec1 = make_float4(pjo.x, pjo.y, pjo.z, __uint_as_float(j));
+  return st_e > st_b;
+}
+
+// Part 2: one (candidate j, incident triangle) pair, star entry `st` of j
+// (shaders/self_collision.wgsl:477-667).  kHeavy = false runs the cheap tests
+// (ownership, swept bounds, two-hop exclusion) on j's values cached by
+// sc_work_vv (rec0 = p_j, contact thickness; rec1 = x_j, j) and returns
+// whether the pair needs the contact math; kHeavy = true reloads j and runs
+// the whole pair.  Each pair is independent (its output goes through the
+// order-free integer accumulators).
+template <bool kHeavy>
+__device__ __forceinline__ bool vt_entry(const SCArgs& s, const VertCtx& c, const TwoHop& th, uint32_t slot,
+                                         uint32_t st, float4 rec0 = float4(), float4 rec1 = float4()) {
+  const uint32_t index = c.index;
+  const float wi = c.wi;
+  const bool pin_i = c.pin_i;
+  const V3 xi = c.xi, pi = c.pi;
+  const float mli = c.mli, thi = c.thi, lli = c.lli;
+  const I3 cell = c.cell;
+  const uint32_t li = c.li;
+  const bool untangle = c.untangle;
+  int32_t* acc = s.acc;
+  V3 pj, pjo;
+  uint32_t j, lj = 0u;
+  float eth, wj = 0.f;
+  if (kHeavy) {
+    j = (uint32_t)s.vs_c[slot].w;
+    const float4 pj4 = s.vs_p[slot];
+    const float4 q = s.vs_q[slot];
+    pj = mk(pj4);
+    eth = fmaxf(thi + pj4.w, fminf(lli, q.x) * 0.06f);
+    lj = __float_as_uint(q.y);
+    pjo = mk(s.x4[j]);
+    wj = q.z;
+  } else {
+    pj = mk(rec0);
+    eth = rec0.w;
+    pjo = mk(rec1);
+    j = __float_as_uint(rec1.w);
+  }
+  const float eth2 = eth * eth;
+
+  const uint2 pr = s.star_idx[st];
+  const uint32_t v0 = pr.x, v1 = pr.y;
+  if (v0 == index || v1 == index) return false;
+  const float4 q0 = s.p4[v0], q1 = s.p4[v1];
+  const float4 o0 = s.x4[v0], o1 = s.x4[v1];
+  const V3 pv0 = mk(q0), pv1 = mk(q1), pv0o = mk(o0), pv1o = mk(o1);
+  const float wv0 = o0.w, wv1 = o1.w;
+  const V3 d0 = pi - pv0;
+  const float ll0 = s.local_len[v0];
+  const float et0 = fmaxf(thi + q0.w, fminf(lli, ll0) * 0.06f);
+  const float b0 = et0 + ll0 * 1.3f + mli + s.mlen[v0];
+  const int4 c0 = s.vcell[v0];
+  const bool in0 = abs(c0.x - cell.x) <= 1 && abs(c0.y - cell.y) <= 1 && abs(c0.z - cell.z) <= 1 &&
+                   (dot(d0, d0) <= b0 * b0);
+  const V3 d1 = pi - pv1;
+  const float ll1 = s.local_len[v1];
+  const float et1 = fmaxf(thi + q1.w, fminf(lli, ll1) * 0.06f);
+  const float b1 = et1 + ll1 * 1.3f + mli + s.mlen[v1];
+  const int4 c1 = s.vcell[v1];
+  const bool in1 = abs(c1.x - cell.x) <= 1 && abs(c1.y - cell.y) <= 1 && abs(c1.z - cell.z) <= 1 &&
+                   (dot(d1, d1) <= b1 * b1);
+  if ((in0 && j > v0) || (in1 && j > v1)) return false;
+  const V3 tmove = (((pj - pjo) + (pv0 - pv0o)) + (pv1 - pv1o)) / 3.0f;
+  const bool tpin = (wj <= 0.0f) || (wv0 <= 0.0f) || (wv1 <= 0.0f);
+  const V3 rel = xi + tmove;
+  const V3 E = mk(eth, eth, eth);
+  const V3 smin = vmin(rel, pi) - E, smax = vmax(rel, pi) + E;
+  const V3 tmin = vmin(vmin(pj, pv0), pv1), tmax = vmax(vmax(pj, pv0), pv1);
+  if (smin.x > tmax.x || smin.y > tmax.y || smin.z > tmax.z || smax.x < tmin.x || smax.y < tmin.y ||
+      smax.z < tmin.z)
+    return false;
+  if (within2_t(th, index, v0) || within2_t(th, index, v1)) return false;
+  if (!kHeavy) return true;
+  const V3 mv = pi - rel;
+  const float msq = dot(mv, mv);
+  float ht = 1.0f, hu = 0.0f, hv = 0.0f;
+  bool hit = false;
+  if (msq > 1e-12f) hit = seg_tri(rel, pi, pj, pv0, pv1, ht, hu, hv);
+  if (hit) {
+    const V3 hp = rel + mv * ht;
+    const V3 tc = cross(pv0 - pj, pv1 - pj);
+    const float tl = length(tc);
+    const V3 tn = tl > 1e-12f ? tc / tl : mk(0.0f, 1.0f, 0.0f);
+    const float hor = dot(rel - pj, tn);
+    bool utc = false;
+    if (untangle && !pin_i && (li > lj) && tl > 1e-12f) {
+      const V3 ni = mk(s.nrm[index]);
+      const float nil = length(ni);
+      const bool allow = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
+      const bool ret = (hor < 0.0f) && (dot(mv, tn) > 0.0f);
+      utc = allow && ret;
+    }
+    if (!utc) {
+      const float ss = fabsf(hor) > 1e-6f ? hor : dot(-mv, tn);
+      const V3 ns = ss >= 0.0f ? tn : -tn;
+      const float ho = fmaxf(dot(rel - hp, ns), 0.0f);
+      const float hs = fmaxf(ho, eth * 0.25f);
+      const V3 psafe = hp + ns * hs;
+      const V3 tccd = psafe - pi;
+      const float pcs = fmaxf(0.0f, eth - hs);
+      if (tpin) {
+        if (!pin_i) add_ccd(acc, index, tccd + ns * pcs, false);
+      } else if (pin_i) {
+        const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
+        const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
+        if (wt > kEps) {
+          const V3 full = tccd + ns * pcs;
+          if (wj > 0.0f) add_ccd(acc, j, (-full) * (bc.x * wj / wt), false);
+          if (wv0 > 0.0f) add_ccd(acc, v0, (-full) * (bc.y * wv0 / wt), false);
+          if (wv1 > 0.0f) add_ccd(acc, v1, (-full) * (bc.z * wv1 / wt), false);
+        }
+      } else {
+        const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
+        const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
+        const float wtot = wi + wt;
+        if (wtot > kEps) {
+          add_ccd(acc, index, tccd * (wi / wtot), false);
+          if (wj > 0.0f) add_ccd(acc, j, (-tccd) * (bc.x * wj / wtot), false);
+          if (wv0 > 0.0f) add_ccd(acc, v0, (-tccd) * (bc.y * wv0 / wtot), false);
+          if (wv1 > 0.0f) add_ccd(acc, v1, (-tccd) * (bc.z * wv1 / wtot), false);
+          if (pcs > kEps) {
+            const V3 tp = ns * (pcs * 0.6f);
+            add_disp(acc, index, tp * (wi / wtot));
+            if (wj > 0.0f) add_disp(acc, j, (-tp) * (bc.x * wj / wtot));
+            if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bc.y * wv0 / wtot));
+            if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bc.z * wv1 / wtot));
           }
+        }
+      }
+    }
+  } else {
+    bool isf;
+    V3 bary;
+    const V3 cp = closest_tri(pi, pj, pv0, pv1, isf, bary);
+    const V3 dvt = pi - cp;
+    const float d2vt = dot(dvt, dvt);
+    if (!pin_i && d2vt < eth2 && d2vt > kEps * kEps) {
+      const float dvtl = sqrtf(d2vt);
+      bool utv = false;
+      if (untangle && li > lj) {
+        const V3 tc = cross(pv0 - pj, pv1 - pj);
+        const float tl = length(tc);
+        if (tl > kEps) {
+          const V3 tn = tc / tl;
+          if (dot(dvt, tn) < 0.0f) {
+            const V3 ni = mk(s.nrm[index]);
+            const float nil = length(ni);
+            utv = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
+          }
+        }
+      }
+      if (!utv) {
+        const V3 nvt = dvt / dvtl;
+        const float pvt = eth - dvtl;
+        if (tpin) {
+          add_pin(acc, index, nvt * pvt + tmove * 0.5f);
         } else {
-          const V3 bc = mk(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
-          const float wt = bc.x * bc.x * wj + bc.y * bc.y * wv0 + bc.z * bc.z * wv1;
+          const float wt = bary.x * bary.x * wj + bary.y * bary.y * wv0 + bary.z * bary.z * wv1;
           const float wtot = wi + wt;
           if (wtot > kEps) {
-            add_ccd(acc, index, tccd * (wi / wtot), false);
-            if (wj > 0.0f) add_ccd(acc, j, (-tccd) * (bc.x * wj / wtot), false);
-            if (wv0 > 0.0f) add_ccd(acc, v0, (-tccd) * (bc.y * wv0 / wtot), false);
-            if (wv1 > 0.0f) add_ccd(acc, v1, (-tccd) * (bc.z * wv1 / wtot), false);
-            if (pcs > kEps) {
-              const V3 tp = ns * (pcs * 0.6f);
-              add_disp(acc, index, tp * (wi / wtot));
-              if (wj > 0.0f) add_disp(acc, j, (-tp) * (bc.x * wj / wtot));
-              if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bc.y * wv0 / wtot));
-              if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bc.z * wv1 / wtot));
-            }
-          }
-        }
-      }
-    } else {
-      bool isf;
-      V3 bary;
-      const V3 cp = closest_tri(pi, pj, pv0, pv1, isf, bary);
-      const V3 dvt = pi - cp;
-      const float d2vt = dot(dvt, dvt);
-      if (!pin_i && d2vt < eth2 && d2vt > kEps * kEps) {
-        const float dvtl = sqrtf(d2vt);
-        bool utv = false;
-        if (untangle && li > lj) {
-          const V3 tc = cross(pv0 - pj, pv1 - pj);
-          const float tl = length(tc);
-          if (tl > kEps) {
-            const V3 tn = tc / tl;
-            if (dot(dvt, tn) < 0.0f) {
-              const V3 ni = mk(s.nrm[index]);
-              const float nil = length(ni);
-              utv = tpin || (nil <= 0.5f) || (dot(ni / fmaxf(nil, kEps), tn) > 0.0f);
-            }
-          }
-        }
-        if (!utv) {
-          const V3 nvt = dvt / dvtl;
-          const float pvt = eth - dvtl;
-          if (tpin) {
-            add_pin(acc, index, nvt * pvt + tmove * 0.5f);
-          } else {
-            const float wt = bary.x * bary.x * wj + bary.y * bary.y * wv0 + bary.z * bary.z * wv1;
-            const float wtot = wi + wt;
-            if (wtot > kEps) {
-              const V3 tp = nvt * (pvt * 0.6f);
-              add_disp(acc, index, tp * (wi / wtot));
-              if (wj > 0.0f) add_disp(acc, j, (-tp) * (bary.x * wj / wtot));
-              if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bary.y * wv0 / wtot));
-              if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bary.z * wv1 / wtot));
-            }
+            const V3 tp = nvt * (pvt * 0.6f);
+            add_disp(acc, index, tp * (wi / wtot));
+            if (wj > 0.0f) add_disp(acc, j, (-tp) * (bary.x * wj / wtot));
+            if (wv0 > 0.0f) add_disp(acc, v0, (-tp) * (bary.y * wv0 / wtot));
+            if (wv1 > 0.0f) add_disp(acc, v1, (-tp) * (bary.z * wv1 / wtot));
           }
         }
       }
     }
   }
+  return true;
 }
 
-__global__ void __launch_bounds__(256, 4) k_sc_solve(SCArgs s) {
+__global__ void __launch_bounds__(256, 3) k_sc_solve(SCArgs s) {
   __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
   __shared__ uint32_t sh_th[8][kTwoHopCache];
   __shared__ float sh_thr[8][kTwoHopCache];
   __shared__ uint32_t sh_q[8][32 * kRounds];
+  __shared__ uint32_t pr_slot[8][32], pr_sb[8][32], pr_ex[8][32];  // survivors' star ranges
+  __shared__ uint32_t tq_slot[8][64], tq_st[8][64];                 // (candidate, triangle) pairs
+  __shared__ float4 pr_rec0[8][32], pr_rec1[8][32];                 // survivors' cached values
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t index = blockIdx.x * 8u + warp;
   if (index >= s.n) return;  // whole warp
@@ -658,6 +710,7 @@ __global__ void __launch_bounds__(256, 4) k_sc_solve(SCArgs s) {
   int k = 0;
   uint32_t* queue = sh_q[warp];
   const uint32_t lt_mask = (1u << lane) - 1u;
+  uint32_t tqn = 0;
   for (uint32_t chunk = 0; chunk < total; chunk += 32u * kRounds) {
     // phase 1: cheap filters on 32 x kRounds candidates, survivors compacted
     uint32_t qn = 0;
@@ -676,10 +729,66 @@ __global__ void __launch_bounds__(256, 4) k_sc_solve(SCArgs s) {
       qn += __popc(b);
     }
     __syncwarp();
-    // phase 2: contact work on the survivors, all lanes busy
-    for (uint32_t q = lane; q < qn; q += 32u) sc_work(s, c, th, queue[q]);
-    __syncwarp();
+    // phase 2: vertex-vertex work on the survivors, 32 at a time; each
+    // survivor's incident triangles become (survivor, star entry) pairs
+    for (uint32_t base = 0; base < qn; base += 32u) {
+      const uint32_t q = base + lane;
+      uint32_t sb = 0, se = 0;
+      float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
+      const uint32_t slot = q < qn ? queue[q] : 0u;
+      const bool vt = q < qn && sc_work_vv(s, c, th, slot, sb, se, r0, r1);
+      const uint32_t cnt = vt ? se - sb : 0u;
+      uint32_t incl = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t npairs = __shfl_sync(0xffffffffu, incl, 31);
+      pr_slot[warp][lane] = slot;
+      pr_sb[warp][lane] = sb;
+      pr_ex[warp][lane] = incl - cnt;
+      pr_rec0[warp][lane] = r0;
+      pr_rec1[warp][lane] = r1;
+      __syncwarp();
+      // phase 3: cheap tests of each pair; passing pairs are compacted into
+      // tq and the contact math runs on full batches of 32
+      for (uint32_t eb = 0; eb < npairs; eb += 32u) {
+        const uint32_t e = eb + uint32_t(lane);
+        bool pass = false;
+        uint32_t ps = 0, pst = 0;
+        if (e < npairs) {
+          uint32_t lo = 0, hi = 31;  // owner: the last lane whose range starts at or before e
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1u) >> 1;
+            if (pr_ex[warp][mid] <= e) lo = mid; else hi = mid - 1u;
+          }
+          ps = pr_slot[warp][lo];
+          pst = pr_sb[warp][lo] + (e - pr_ex[warp][lo]);
+          pass = vt_entry<false>(s, c, th, ps, pst, pr_rec0[warp][lo], pr_rec1[warp][lo]);
+        }
+        const uint32_t b = __ballot_sync(0xffffffffu, pass);
+        if (pass) {
+          const uint32_t kq = tqn + __popc(b & lt_mask);
+          tq_slot[warp][kq] = ps;
+          tq_st[warp][kq] = pst;
+        }
+        tqn += __popc(b);
+        __syncwarp();
+        if (tqn >= 32u) {
+          vt_entry<true>(s, c, th, tq_slot[warp][lane], tq_st[warp][lane]);
+          __syncwarp();
+          tqn -= 32u;
+          if (uint32_t(lane) < tqn) {
+            tq_slot[warp][lane] = tq_slot[warp][32 + lane];
+            tq_st[warp][lane] = tq_st[warp][32 + lane];
+          }
+          __syncwarp();
+        }
+      }
+      __syncwarp();
+    }
   }
+  if (uint32_t(lane) < tqn) vt_entry<true>(s, c, th, tq_slot[warp][lane], tq_st[warp][lane]);
   if (c.track) {
     for (int o = 16; o > 0; o >>= 1) {
       const float ob = __shfl_xor_sync(0xffffffffu, best_in, o);
