@@ -115,6 +115,27 @@ tc_status tc_clear_colliders(tc_sim *s);
 tc_status tc_set_self_collision_substep_interval(tc_sim *s, uint32_t interval);
 tc_status tc_set_self_collision_ee_substep_interval(tc_sim *s, uint32_t interval);
 tc_status tc_get_self_collision_intervals(tc_sim *s, uint32_t out[2]);
+/* Adaptive substeps and iterations (set_adaptive_substep_options etc.,
+ * simulation/mod.rs:723-790; decisions dispatch.rs:477-607).  Off by default.
+ * When on, tc_step's substep count is chosen from the previous frames'
+ * maximum vertex displacement (CFL), the free-fall floor and the P95 tensile
+ * strain of a 2048-constraint sample, with hysteresis; iterations are
+ * compensated toward a propagation budget.  The feedback is reduced on the
+ * GPU after each frame (no position readback).
+ * out = effective substeps, effective iterations, last P95 strain, last max
+ * displacement, CFL characteristic length, mesh diameter in hops. */
+tc_status tc_set_adaptive_substep_options(tc_sim *s, int enabled, uint32_t min_substeps, uint32_t max_substeps);
+tc_status tc_set_auto_compensate_iterations(tc_sim *s, int enabled);
+tc_status tc_set_strain_adaptive_options(tc_sim *s, int enabled, float tolerance);
+tc_status tc_note_external_displacement(tc_sim *s, float disp);
+tc_status tc_get_adaptive_state(tc_sim *s, float out[6]);
+/* The decision rules alone (no simulator), for tests; in[18] is documented
+ * beside the definition order: enabled, min, max, base substeps, previous
+ * effective substeps, characteristic length, thickness, gx, gy, gz, max
+ * displacement, external displacement, strain adaptive, tolerance, last
+ * strain, auto compensate, solver iterations, diameter hops.  out = substeps,
+ * iterations for iter_substeps substeps (0 = for the substeps chosen). */
+tc_status tc_adaptive_eval(float dt, uint32_t requested, uint32_t iter_substeps, const float in[18], uint32_t out[2]);
 
 /* Bone SDF colliders (lib.rs:2245-2600, simulation/mod.rs:1630-2464).  The
  * atlas is width x height x depth texels of packed half2 (distance in the low

@@ -75,6 +75,12 @@ SIGNATURES = {
     "tc_check_barrier_timeout": [_P, _U],
     "tc_hash_build_static": [_P, _U, _F, _U, _P, _P, _P],
     "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],
+    "tc_set_adaptive_substep_options": [_P, _I, _U, _U],
+    "tc_set_auto_compensate_iterations": [_P, _I],
+    "tc_set_strain_adaptive_options": [_P, _I, _F],
+    "tc_note_external_displacement": [_P, _F],
+    "tc_get_adaptive_state": [_P, _P],
+    "tc_adaptive_eval": [_F, _U, _U, _P, _P],
     "tc_set_self_collision_substep_interval": [_P, _U],
     "tc_set_self_collision_ee_substep_interval": [_P, _U],
     "tc_get_self_collision_intervals": [_P, _P],

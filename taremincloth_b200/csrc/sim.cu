@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/tcloth.h"
+#include "adaptive.hpp"
 #include "mesh.hpp"
 #include "selfcol_kernels.cuh"
 #include "solver_kernels.cuh"
@@ -62,6 +63,42 @@ struct DBuf {
   }
   void upload(const std::vector<T>& v, cudaStream_t st) { upload(v.data(), v.size(), st); }
 };
+
+// Adaptive feedback (update_feedback_from_floats, dispatch.rs:356-429): the
+// largest per-axis displacement since the previous frame (max is order-free:
+// atomicMax on the bits of non-negative floats), then prev = x.
+__global__ void k_fb_disp(uint32_t n, const float4* __restrict__ x4, float4* __restrict__ prev, float* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  float d = 0.f;
+  if (i < n) {
+    const float4 x = x4[i], q = prev[i];
+    d = fmaxf(fmaxf(fabsf(x.x - q.x), fabsf(x.y - q.y)), fabsf(x.z - q.z));
+    prev[i] = x;
+  }
+  for (int o = 16; o > 0; o >>= 1) d = fmaxf(d, __shfl_down_sync(0xffffffffu, d, o));
+  if ((threadIdx.x & 31) == 0 && d > 0.f) atomicMax(reinterpret_cast<int*>(out), __float_as_int(d));
+}
+// Tensile strain of every `stride`-th distance constraint against its
+// initial rest length, or -1 when not stretched.
+__global__ void k_fb_strain(uint32_t ns, uint32_t stride, const uint2* __restrict__ ids, const float* __restrict__ rest0,
+                            const float4* __restrict__ x4, float min_ref, float* __restrict__ out) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  const uint32_t c = k * stride;
+  const float l0 = rest0[c];
+  float r = -1.f;
+  if (l0 > 1e-6f) {
+    const uint2 e = ids[c];
+    const float4 a = x4[e.x], b = x4[e.y];
+    const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    const float d2 = (dx * dx + dy * dy) + dz * dz;
+    if (d2 > l0 * l0) {
+      const float st = (sqrtf(d2) - l0) / fmaxf(l0, min_ref);
+      if (st > 0.f) r = st;
+    }
+  }
+  out[k] = r;
+}
 
 struct PinH {
   float target[3];
@@ -333,6 +370,14 @@ struct Sim {
   int* h_err = nullptr;  // pinned
   WarmStart ws;
   BoneSdfState bone;
+  // adaptive substeps / iterations with their GPU feedback (max displacement,
+  // strided strain sample), read after each frame
+  AdaptiveCtl ad;
+  DBuf<float4> fb_prev;
+  DBuf<float> fb_out, rest0;
+  float* h_fb = nullptr;  // pinned: [0] = max displacement, [1 .. ] strain sample
+  uint32_t fb_nsamp = 0, fb_stride = 1;
+  uint32_t run_iters() const { return ad.enabled ? std::max(ad.effective_iterations, 1u) : iters; }
   // residual instrumentation
   bool track_residual = false;
   DBuf<float> res_sum, res_max;  // [ndc + nbc] each
@@ -362,6 +407,7 @@ struct Sim {
   float g_dt = -1.f;
   uint32_t g_sub = 0;
   bool g_coupled = false;
+  uint32_t g_iters = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool async_pending = false;
   // per-pass profiling (GpuProfiler / take_profile, simulation/profile.rs:38-252):
@@ -413,6 +459,7 @@ struct Sim {
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
     if (h_err) cudaFreeHost(h_err);
+    if (h_fb) cudaFreeHost(h_fb);
   }
 
   void mark() { graph_dirty = true; }
@@ -490,6 +537,27 @@ struct Sim {
     init_w = m.inv_mass;
     init_pos = m.pos;
     prev_frame_pos = m.pos;
+    {  // CFL characteristic length, mean rest length, diameter in hops (mod.rs:380-420)
+      float min_d2 = 3.4028235e38f;
+      for (const auto& c : dist_h) {
+        const float* a = &m.pos[3 * size_t(c.v0)];
+        const float* b = &m.pos[3 * size_t(c.v1)];
+        const float dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+        const float d2 = (dx * dx + dy * dy) + dz * dz;
+        if (d2 > 1e-8f && d2 < min_d2) min_d2 = d2;
+      }
+      const float min_edge = min_d2 < 3.4028235e38f ? std::sqrt(min_d2) : 0.02f;
+      ad.mesh_char_len = std::fmax(std::fmin(0.005f * 2.0f, min_edge), 0.001f);
+      float lo[3] = {3.4028235e38f, 3.4028235e38f, 3.4028235e38f}, hi[3] = {-3.4028235e38f, -3.4028235e38f, -3.4028235e38f};
+      for (uint32_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) { lo[k] = std::fmin(lo[k], m.pos[3 * i + k]); hi[k] = std::fmax(hi[k], m.pos[3 * i + k]); }
+      const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+      const float diag = n ? std::sqrt((ex * ex + ey * ey) + ez * ez) : 0.f;
+      float tot = 0.f;
+      for (const auto& c : dist_h) tot += c.rest;
+      ad.mesh_avg_edge_len = nd ? std::fmax(tot / float(nd), 1e-4f) : 0.02f;
+      ad.mesh_diameter_hops = std::min(std::max(uint32_t(std::ceil(diag / ad.mesh_avg_edge_len)), 10u), 60u);
+    }
     upload_vertices(m.pos.data(), nullptr, m.inv_mass.data());
     local_len.upload(m.local_len, st);
     upload_dist();
@@ -842,7 +910,7 @@ struct Sim {
 
   SolverArgs solver_args(const SubstepParams& sp, uint32_t nsub, bool use_coupled, bool with_update) {
     SolverArgs a;
-    a.n = n; a.nsub = nsub; a.iters = iters; a.npins = uint32_t(pins.size());
+    a.n = n; a.nsub = nsub; a.iters = run_iters(); a.npins = uint32_t(pins.size());
     a.ndc = uint32_t(m.dist_cnt.size()); a.nbc = uint32_t(m.bend_cnt.size());
     a.hascol = has_colliders();
     a.coupled = use_coupled;
@@ -941,7 +1009,8 @@ struct Sim {
   // runs k more when it misses.
   void encode_frame_ws(float dt, uint32_t substeps, bool use_coupled) {
     const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
-    const uint32_t kk = std::min(ws.k, iters > 1 ? iters - 1 : 0u);
+    const uint32_t itn = run_iters();
+    const uint32_t kk = std::min(ws.k, itn > 1 ? itn - 1 : 0u);
     const WsFeatArgs fa = ws_feat_args(sp, ws.feat.p);
     for (uint32_t s = 0; s < substeps; ++s) {
       timed("predict", [&] { k_predict<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp); });
@@ -952,7 +1021,7 @@ struct Sim {
       });
       SolverArgs a = solver_args(sp, 1, use_coupled, !self_collision);
       a.skip_predict = true;
-      a.iters = iters - kk;
+      a.iters = itn - kk;
       a.iters_extra = kk;
       a.ppred = ws.ppred.p;
       a.dprev = ws.dprev.p;
@@ -1052,7 +1121,7 @@ struct Sim {
         if (rec_this)
           k_ws_features<<<grid(n, 128), 128, 0, st>>>(ws_feat_args(sp, ws.rec_feat.p + size_t(slot) * n * kWsF));
       }
-      for (uint32_t it = 0; it < iters; ++it) {
+      for (uint32_t it = 0, itn = run_iters(); it < itn; ++it) {
         if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
         timed("distance", [&] {
           for (size_t c = 0; c < m.dist_cnt.size(); ++c)
@@ -1108,7 +1177,8 @@ struct Sim {
       if (profiling) collect_marks();
       return;
     }
-    if (graph_dirty || !gexec || g_dt != dt || g_sub != substeps || g_coupled != use_coupled) {
+    if (graph_dirty || !gexec || g_dt != dt || g_sub != substeps || g_coupled != use_coupled ||
+        g_iters != run_iters()) {
       if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
       cudaGraph_t graph = nullptr;
       TC_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -1137,6 +1207,7 @@ struct Sim {
       g_dt = dt;
       g_sub = substeps;
       g_coupled = use_coupled;
+      g_iters = run_iters();
     }
     if (track_residual) {
       const size_t k = m.dist_cnt.size() + m.bend_cnt.size();
@@ -1156,11 +1227,50 @@ struct Sim {
       throw TcError(TC_ERR_TIMEOUT, "a grid barrier of the persistent solver timed out; the frame is incomplete");
     }
   }
+  // ---- adaptive substeps: plan before a frame, GPU feedback after it
+  void adaptive_enable_buffers() {
+    if (h_fb) return;
+    const uint32_t total = nd;
+    fb_stride = std::max(total / 2048u, 1u);
+    fb_nsamp = total ? (total + fb_stride - 1) / fb_stride : 0u;
+    fb_prev.alloc(n);
+    fb_out.alloc(1 + std::max(fb_nsamp, 1u));
+    rest0.upload(base_rest, st);
+    TC_CK(cudaMemcpyAsync(fb_prev.p, x4.p, size_t(n) * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    TC_CK(cudaHostAlloc(&h_fb, (2 + size_t(fb_nsamp)) * sizeof(float), cudaHostAllocDefault));
+    TC_CK(cudaStreamSynchronize(st));
+  }
+  uint32_t plan_frame(float dt, uint32_t requested) {
+    const uint32_t sub = ad.substeps(dt, requested, g, n);
+    ad.iterations(iters, sub);
+    return sub;
+  }
+  void encode_feedback() {
+    if (!ad.enabled || !h_fb) return;
+    TC_CK(cudaMemsetAsync(fb_out.p, 0, sizeof(float), st));
+    k_fb_disp<<<grid(n, 256), 256, 0, st>>>(n, x4.p, fb_prev.p, fb_out.p);
+    const float min_ref = std::fmax(0.5f * ad.mesh_avg_edge_len, 0.002f);
+    if (fb_nsamp)
+      k_fb_strain<<<grid(fb_nsamp, 256), 256, 0, st>>>(fb_nsamp, fb_stride, dist_ids.p, rest0.p, x4.p, min_ref,
+                                                       fb_out.p + 1);
+    TC_CK(cudaMemcpyAsync(h_fb, fb_out.p, (1 + size_t(fb_nsamp)) * sizeof(float), cudaMemcpyDeviceToHost, st));
+  }
+  void consume_feedback() {  // after the stream is synchronised
+    if (!ad.enabled || !h_fb) return;
+    ad.last_max_disp = h_fb[0];
+    last_max_disp = h_fb[0];
+    std::vector<float> pos;
+    for (uint32_t k = 0; k < fb_nsamp; ++k)
+      if (h_fb[1 + k] > 0.f) pos.push_back(h_fb[1 + k]);
+    ad.last_strain = AdaptiveCtl::p95(std::move(pos));
+  }
   void step(float dt, uint32_t substeps) {
     launch_frame(dt, substeps);
+    encode_feedback();
     TC_CK(cudaStreamSynchronize(st));
     TC_CK(cudaGetLastError());
     check_barrier_status();
+    consume_feedback();
   }
 
   void get_positions(float* out) {
@@ -1445,7 +1555,7 @@ tc_status tc_destroy(tc_sim* s) {
 tc_status tc_step(tc_sim* s, float dt, uint32_t substeps, uint32_t* eff) {
   return guard([&] {
     Sim& m = S(s);
-    const uint32_t sub = substeps ? substeps : 20u;
+    const uint32_t sub = m.plan_frame(dt, substeps);
     m.step(dt, sub);
     if (eff) *eff = sub;
   });
@@ -1454,7 +1564,8 @@ tc_status tc_step(tc_sim* s, float dt, uint32_t substeps, uint32_t* eff) {
 tc_status tc_step_async(tc_sim* s, float dt, uint32_t substeps) {
   return guard([&] {
     Sim& m = S(s);
-    m.launch_frame(dt, substeps ? substeps : 20u);
+    m.launch_frame(dt, m.plan_frame(dt, substeps));
+    m.encode_feedback();
     m.async_pending = true;
   });
 }
@@ -1470,6 +1581,7 @@ tc_status tc_fetch_positions(tc_sim* s, float* out, size_t out_len, int* ok) {
     m.get_positions(out);
     m.async_pending = false;
     m.check_barrier_status();
+    m.consume_feedback();
     float md = 0.f;
     for (size_t i = 0; i < size_t(m.n) * 3; ++i) md = std::fmax(md, std::fabs(out[i] - m.prev_frame_pos[i]));
     std::memcpy(m.prev_frame_pos.data(), out, size_t(m.n) * 3 * sizeof(float));
@@ -2509,6 +2621,66 @@ tc_status tc_bake_get(tc_bake* b, uint32_t* texels, float* infos, uint32_t* acti
 tc_status tc_bake_destroy(tc_bake* b) {
   delete b;
   return TC_OK;
+}
+
+// ---- adaptive substeps and iterations (mod.rs:723-790, dispatch.rs:477-607)
+tc_status tc_set_adaptive_substep_options(tc_sim* s, int enabled, uint32_t min_substeps, uint32_t max_substeps) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (enabled) m.adaptive_enable_buffers();
+    m.ad.set_options(enabled != 0, min_substeps, max_substeps);
+    m.mark();
+  });
+}
+tc_status tc_set_auto_compensate_iterations(tc_sim* s, int enabled) {
+  return guard([&] { S(s).ad.auto_compensate = enabled != 0; });
+}
+tc_status tc_set_strain_adaptive_options(tc_sim* s, int enabled, float tolerance) {
+  return guard([&] { S(s).ad.set_strain_options(enabled != 0, tolerance); });
+}
+tc_status tc_note_external_displacement(tc_sim* s, float disp) {
+  return guard([&] { S(s).ad.note_external(disp); });
+}
+tc_status tc_get_adaptive_state(tc_sim* s, float out[6]) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr, "out required");
+    out[0] = float(m.ad.effective_substeps);
+    out[1] = float(m.ad.effective_iterations > 0 ? m.ad.effective_iterations : m.iters);
+    out[2] = m.ad.last_strain;
+    out[3] = m.ad.last_max_disp;
+    out[4] = m.ad.mesh_char_len;
+    out[5] = float(m.ad.mesh_diameter_hops);
+  });
+}
+// Pure evaluation of the decision rules, for tests: in = {enabled, min, max,
+// base, previous effective substeps (0 = none), char length, thickness, gx,
+// gy, gz, max displacement, external displacement, strain adaptive,
+// tolerance, last strain, auto compensate, solver iterations, diameter hops};
+// out = {effective substeps, effective iterations for iter_substeps substeps
+// (0 = for the substeps just chosen)}.
+tc_status tc_adaptive_eval(float dt, uint32_t requested, uint32_t iter_substeps, const float in[18], uint32_t out[2]) {
+  return guard([&] {
+    need(in != nullptr && out != nullptr, "in and out required");
+    tcloth::AdaptiveCtl a;
+    a.enabled = in[0] != 0.f;
+    a.min_substeps = uint32_t(in[1]);
+    a.max_substeps = uint32_t(in[2]);
+    a.base_substeps = uint32_t(in[3]);
+    a.effective_substeps = uint32_t(in[4]);
+    a.mesh_char_len = in[5];
+    a.cloth_thickness = in[6];
+    const float g[3] = {in[7], in[8], in[9]};
+    a.last_max_disp = in[10];
+    a.pending_external = in[11];
+    a.strain_adaptive = in[12] != 0.f;
+    a.strain_tolerance = in[13];
+    a.last_strain = in[14];
+    a.auto_compensate = in[15] != 0.f;
+    a.mesh_diameter_hops = uint32_t(in[17]);
+    out[0] = a.substeps(dt, requested, g, 3);
+    out[1] = a.iterations(uint32_t(in[16]), iter_substeps ? iter_substeps : out[0]);
+  });
 }
 
 // ---- self-collision substep intervals (mod.rs:1071-1088)

@@ -423,6 +423,34 @@ class ClothSimulator:
         self._c(self._L.tc_last_frame_ms(self._h, C.byref(v)))
         return v.value
 
+    # ---- adaptive substeps and iterations (lib.rs:1788-1805, :1950-1965)
+    def set_adaptive_substep_options(self, enabled, min_substeps=4, max_substeps=64):
+        self._c(self._L.tc_set_adaptive_substep_options(self._h, int(bool(enabled)), int(min_substeps),
+                                                        int(max_substeps)))
+
+    def set_auto_compensate_iterations(self, enabled):
+        self._c(self._L.tc_set_auto_compensate_iterations(self._h, int(bool(enabled))))
+
+    def set_strain_adaptive_options(self, enabled, tolerance=0.008):
+        self._c(self._L.tc_set_strain_adaptive_options(self._h, int(bool(enabled)), float(tolerance)))
+
+    def note_external_displacement(self, disp):
+        self._c(self._L.tc_note_external_displacement(self._h, float(disp)))
+
+    def _adaptive(self):
+        out = np.zeros(6, _f32)
+        self._c(self._L.tc_get_adaptive_state(self._h, _ptr(out)))
+        return out
+
+    def get_effective_substeps(self):
+        return int(self._adaptive()[0])
+
+    def get_effective_solver_iterations(self):
+        return int(self._adaptive()[1])
+
+    def get_last_step_max_strain(self):
+        return float(self._adaptive()[2])
+
     # ---- self-collision substep intervals (lib.rs:1966-2000)
     def set_self_collision_substep_interval(self, interval):
         self._c(self._L.tc_set_self_collision_substep_interval(self._h, int(interval)))
