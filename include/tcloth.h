@@ -257,8 +257,12 @@ tc_status tc_take_profile(tc_sim *s, char *names, size_t names_len, float *ms, u
  * return TC_ERR_TIMEOUT.  New; the reference dispatches one pass per colour
  * (dispatch.rs:1449-1455). */
 tc_status tc_set_persistent_solver(tc_sim *s, int enable);
-/* Launch shape of the persistent solver (blocks per SM, 1..limit) or the
- * launch-per-colour path; used by the autotuner.  Results do not change. */
+/* Launch shape: persistent = 0 one launch per colour; 1 the persistent
+ * solver with blocks_per_sm (1..limit); 2 the cluster solver for batched
+ * instances without self-collision (each thread-block cluster of 8 CTAs runs
+ * a bin of whole instances through the frame, colour steps separated by the
+ * cluster barrier; TC_ERR_INVALID when not applicable).  Used by the
+ * autotuner.  Results do not change. */
 tc_status tc_set_launch_config(tc_sim *s, int persistent, uint32_t blocks_per_sm);
 tc_status tc_get_launch_limits(tc_sim *s, uint32_t *max_blocks_per_sm, uint32_t *num_sms);
 /* Diagnostics for the failure path: runs one barrier that can never be

@@ -354,6 +354,13 @@ struct Sim {
   DBuf<float4> bounds, cl16, cl256;
   // batched instances (empty for a single cloth)
   std::vector<uint32_t> inst_vert_off;  // n_instances + 1
+  // cluster solver: bins of whole instances, one thread-block cluster each
+  static constexpr uint32_t kClusterCtas = 8;
+  bool cluster_mode = false, cl_stale = true;
+  int cl_max_active = 0;
+  uint32_t cl_bins = 0;
+  DBuf<uint2> cl_vrange, cl_pins, cl_dist, cl_bend;
+  DBuf<uint32_t> cl_dperm, cl_bperm;
   std::vector<uint2> inst_prims_h;
   DBuf<uint32_t> vinst;
   DBuf<uint2> inst_prims;
@@ -602,6 +609,24 @@ struct Sim {
       int per_sm_bone = 0;
       TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_bone, k_solver_persistent<true>, 256, 0));
       persist_bone_per_sm = coop ? unsigned(per_sm_bone) : 0u;
+      {  // co-resident clusters of the cluster solver (0 when clusters cannot launch)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kClusterCtas * 64);
+        cfg.blockDim = dim3(256);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kClusterCtas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, k_solver_cluster<false>, &cfg) != cudaSuccess) {
+          cudaGetLastError();
+          ncl = 0;
+        }
+        cl_max_active = ncl;
+      }
       num_sms = unsigned(nsm);
       if (!persist_blocks) persistent = false;
     }
@@ -701,6 +726,7 @@ struct Sim {
 
   // ---- pins
   void upload_pins() {
+    cl_stale = true;
     std::vector<uint32_t> v;
     std::vector<float4> t;
     for (const auto& kv : pins) {
@@ -937,6 +963,81 @@ struct Sim {
     a.fallbacks = nullptr;
     return a;
   }
+  bool can_cluster() const { return !inst_vert_off.empty() && cl_max_active > 0 && !self_collision; }
+  // bins: contiguous runs of instances, balanced by vertex count; the
+  // constraint permutations are sorted by (bin, colour, original index)
+  void build_cluster_tables() {
+    const uint32_t ninst = uint32_t(inst_vert_off.size() - 1);
+    const uint32_t B = std::max(1u, std::min(ninst, uint32_t(cl_max_active)));
+    const uint64_t target = (uint64_t(n) + B - 1) / B;
+    std::vector<uint32_t> bin_of_inst(ninst);
+    for (uint32_t k = 0; k < ninst; ++k) {
+      const uint64_t mid = uint64_t(inst_vert_off[k]) + (inst_vert_off[k + 1] - inst_vert_off[k]) / 2;
+      bin_of_inst[k] = uint32_t(std::min<uint64_t>(B - 1, mid / std::max<uint64_t>(target, 1)));
+    }
+    std::vector<uint2> vr(B, make_uint2(0, 0));
+    std::vector<char> seen(B, 0);
+    for (uint32_t k = 0; k < ninst; ++k) {
+      const uint32_t b = bin_of_inst[k];
+      if (!seen[b]) { vr[b] = make_uint2(inst_vert_off[k], inst_vert_off[k + 1]); seen[b] = 1; }
+      else vr[b].y = inst_vert_off[k + 1];
+    }
+    for (uint32_t b = 0; b < B; ++b)  // empty bins: an empty range
+      if (!seen[b]) vr[b] = make_uint2(b ? vr[b - 1].y : 0u, b ? vr[b - 1].y : 0u);
+    std::vector<uint32_t> bin_of_v(n);
+    for (uint32_t k = 0; k < ninst; ++k)
+      for (uint32_t v = inst_vert_off[k]; v < inst_vert_off[k + 1]; ++v) bin_of_v[v] = bin_of_inst[k];
+    std::vector<uint32_t> pv;
+    for (const auto& kv : pins) pv.push_back(kv.first);
+    std::vector<uint2> pr(B);
+    for (uint32_t b = 0; b < B; ++b) {
+      const uint32_t lo = uint32_t(std::lower_bound(pv.begin(), pv.end(), vr[b].x) - pv.begin());
+      const uint32_t hi = uint32_t(std::lower_bound(pv.begin(), pv.end(), vr[b].y) - pv.begin());
+      pr[b] = make_uint2(lo, hi - lo);
+    }
+    auto perm_of = [&](const std::vector<uint32_t>& off, const std::vector<uint32_t>& cnt, auto vert_of,
+                       std::vector<uint32_t>& perm, std::vector<uint2>& tab) {
+      const uint32_t nc = uint32_t(off.size());
+      std::vector<std::vector<uint32_t>> bucket(size_t(B) * std::max(nc, 1u));
+      for (uint32_t c = 0; c < nc; ++c)
+        for (uint32_t k = off[c]; k < off[c] + cnt[c]; ++k) bucket[size_t(bin_of_v[vert_of(k)]) * nc + c].push_back(k);
+      perm.clear();
+      tab.assign(size_t(B) * nc, make_uint2(0, 0));
+      for (size_t q = 0; q < size_t(B) * nc; ++q) {
+        tab[q] = make_uint2(uint32_t(perm.size()), uint32_t(bucket[q].size()));
+        perm.insert(perm.end(), bucket[q].begin(), bucket[q].end());
+      }
+    };
+    std::vector<uint32_t> dperm, bperm;
+    std::vector<uint2> dtab, btab;
+    perm_of(m.dist_off, m.dist_cnt, [&](uint32_t k) { return dist_h[k].v0; }, dperm, dtab);
+    perm_of(m.bend_off, m.bend_cnt, [&](uint32_t k) { return bend_h[k].v0; }, bperm, btab);
+    cl_vrange.upload(vr, st);
+    cl_pins.upload(pr, st);
+    cl_dist.upload(dtab, st);
+    cl_bend.upload(btab, st);
+    cl_dperm.upload(dperm, st);
+    cl_bperm.upload(bperm, st);
+    TC_CK(cudaStreamSynchronize(st));
+    cl_bins = B;
+    cl_stale = false;
+  }
+  void launch_cluster(const SolverArgs& a) {
+    const ClusterTables t{cl_vrange.p, cl_pins.p, cl_dist.p, cl_bend.p, cl_dperm.p, cl_bperm.p};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl_bins * kClusterCtas);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClusterCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (a.ca.bone.nbones > 0) TC_CK(cudaLaunchKernelEx(&cfg, k_solver_cluster<true>, a, t));
+    else TC_CK(cudaLaunchKernelEx(&cfg, k_solver_cluster<false>, a, t));
+  }
   // the persistent path is available: cooperative launch, and with bone
   // colliders the bone instantiation fits on an SM
   bool can_persist() const { return persist_blocks > 0 && (!bone.enabled || persist_bone_per_sm > 0); }
@@ -1074,15 +1175,42 @@ struct Sim {
     if (last) *last = float(b / cnt);
   }
 
+  // Launch of a per-colour-path kernel; with pdl (not while profiling) the
+  // launch carries programmatic stream serialization, so the kernel's launch
+  // overlaps the tail of the previous one (the kernel waits for its data).
+  bool pdl = true;
+  template <typename... KArgs, typename... Args>
+  void launch_k(void (*kern)(KArgs...), unsigned gx, unsigned block, Args... args) {
+    if (!pdl || profiling) {
+      kern<<<gx, block, 0, st>>>(args...);
+      return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(gx);
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    TC_CK(cudaLaunchKernelEx(&cfg, kern, args...));
+  }
   void launch_collision(const ColliderArgs& ca, float dts) {
-    if (ca.bone.nbones > 0) k_collision<true><<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts);
-    else k_collision<false><<<grid(n, 128), 128, 0, st>>>(n, x4.p, p4.p, ca, dts);
+    if (ca.bone.nbones > 0) launch_k(k_collision<true>, grid(n, 128), 128, n, x4.p, p4.p, ca, dts);
+    else launch_k(k_collision<false>, grid(n, 128), 128, n, x4.p, p4.p, ca, dts);
   }
 
   // encode_simulation_steps (dispatch.rs:7-354) for one frame
   void encode_frame(float dt, uint32_t substeps, bool use_coupled) {
     if (ws.on && !ws_recording()) {
       encode_frame_ws(dt, substeps, use_coupled);
+      return;
+    }
+    if (cluster_mode && can_cluster() && !cl_stale && !profiling && !track_residual && !ws_recording()) {
+      const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
+      launch_cluster(solver_args(sp, substeps, use_coupled, true));
+      TC_CK(cudaGetLastError());
       return;
     }
     if (persistent && can_persist() && !profiling && !track_residual && !ws_recording()) {
@@ -1110,7 +1238,7 @@ struct Sim {
     for (uint32_t s = 0; s < substeps; ++s) {
       if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
       if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
-      timed("predict", [&] { k_predict<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp); });
+      timed("predict", [&] { launch_k(k_predict, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp); });
       // recording for the warm start: features after predict, the
       // iterations' correction as the target
       const bool rec = ws_recording();
@@ -1122,18 +1250,18 @@ struct Sim {
           k_ws_features<<<grid(n, 128), 128, 0, st>>>(ws_feat_args(sp, ws.rec_feat.p + size_t(slot) * n * kWsF));
       }
       for (uint32_t it = 0, itn = run_iters(); it < itn; ++it) {
-        if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
+        if (npins) timed("pin", [&] { launch_k(k_pin, grid(npins, 128), 128, npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
         timed("distance", [&] {
           for (size_t c = 0; c < m.dist_cnt.size(); ++c)
             if (m.dist_cnt[c])
-              k_distance<<<grid(m.dist_cnt[c], 256), 256, 0, st>>>(m.dist_off[c], m.dist_cnt[c], dist_ids.p,
-                                                                    dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
+              launch_k(k_distance, grid(m.dist_cnt[c], 256), 256, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
+                       dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
         });
         timed("bending", [&] {
           for (size_t c = 0; c < m.bend_cnt.size(); ++c)
             if (m.bend_cnt[c])
-              k_bending<<<grid(m.bend_cnt[c], 256), 256, 0, st>>>(m.bend_off[c], m.bend_cnt[c], bend_ids.p,
-                                                                   bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
+              launch_k(k_bending, grid(m.bend_cnt[c], 256), 256, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
+                       bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
         });
         if (hascol && use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
       }
@@ -1145,9 +1273,9 @@ struct Sim {
         if (rec_this) ++ws.rec_count;
       }
       if (hascol && !use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
-      if (npins) timed("pin", [&] { k_pin<<<grid(npins, 128), 128, 0, st>>>(npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
+      if (npins) timed("pin", [&] { launch_k(k_pin, grid(npins, 128), 128, npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
       if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
-      timed("update_vel", [&] { k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, dts); });
+      timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, dts); });
     }
     TC_CK(cudaGetLastError());
   }
@@ -1165,6 +1293,7 @@ struct Sim {
 
   void launch_frame(float dt, uint32_t substeps) {
     if (n == 0) return;
+    if (cluster_mode && can_cluster() && cl_stale) build_cluster_tables();  // before any capture
     // the frame's device time (last_frame_ms) includes the dynamic bone SDF rebake
     TC_CK(cudaEventRecord(ev0, st));
     dynamic_bone_update();
@@ -2007,11 +2136,19 @@ tc_status tc_take_profile(tc_sim* s, char* names, size_t names_len, float* ms, u
 tc_status tc_set_launch_config(tc_sim* s, int persistent, uint32_t blocks_per_sm) {
   return guard([&] {
     Sim& m = S(s);
+    if (persistent == 2) {  // cluster solver (batched instances without self-collision)
+      need(m.can_cluster(), "the cluster solver needs batched instances, no self-collision and cluster launch");
+      m.cluster_mode = true;
+      m.cl_stale = true;
+      m.mark();
+      return;
+    }
     if (persistent) {
       need(m.persist_max_per_sm > 0, "cooperative launch is not available on this device");
       need(blocks_per_sm >= 1 && blocks_per_sm <= m.persist_max_per_sm, "blocks_per_sm out of the occupancy range");
       m.persist_blocks = m.num_sms * blocks_per_sm;
     }
+    m.cluster_mode = false;
     m.persistent = persistent != 0;
     m.mark();
   });

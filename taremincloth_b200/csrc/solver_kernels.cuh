@@ -8,10 +8,22 @@
 // One thread per vertex / constraint; each kernel restates one WGSL entry
 // point of crates/cloth_core/src/shaders/.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "bone_sdf.cuh"
 #include "vmath.cuh"
 
 namespace tcloth {
+
+// Programmatic dependent launch: wait until the preceding kernel of the stream
+// has finished and its writes are visible (a no-op for a launch without the
+// attribute), then allow the next kernel to begin launching.  The per-colour
+// kernels call it first, so only launch latency overlaps, never data.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" :::);
+}
+
 
 // Loads of data that other blocks of a persistent launch write between two
 // grid barriers go through L2 (ld.global.cg) so no SM reads a stale L1 line.
@@ -52,6 +64,7 @@ __device__ __forceinline__ void predict_vertex(uint32_t i, const float4* __restr
 }
 __global__ void k_predict(uint32_t n, const float4* __restrict__ x4, float4* __restrict__ p4,
                           float4* __restrict__ v4, SubstepParams sp) {
+  pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   predict_vertex<false>(i, x4, p4, v4, sp);
@@ -87,6 +100,7 @@ __device__ __forceinline__ void pin_one(uint32_t k, const uint32_t* __restrict__
 }
 __global__ void k_pin(uint32_t npins, const uint32_t* __restrict__ pin_v, const float4* __restrict__ pin_t,
                       const float4* __restrict__ x4, float4* __restrict__ p4, float dt_sub) {
+  pdl_enter();
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= npins) return;
   pin_one<false>(k, pin_v, pin_t, x4, p4, dt_sub);
@@ -101,10 +115,14 @@ __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __res
                                                  const SubstepParams& sp, bool damped) {
   const uint2 e = ids[ci];
   const float4 c = par[ci];
-  const float w0 = ld4<kCg>(x4 + e.x).w, w1 = ld4<kCg>(x4 + e.y).w;
+  // every load of the constraint issued together: within a colour no other
+  // thread writes these addresses, so this changes latency, not results
+  const float4 xa = ld4<kCg>(x4 + e.x), xb = ld4<kCg>(x4 + e.y);
+  const float4 q0 = ld4<kCg>(p4 + e.x), q1 = ld4<kCg>(p4 + e.y);
+  const float l = ld1<kCg>(lam + ci);
+  const float w0 = xa.w, w1 = xb.w;
   const float ws = w0 + w1;
   if (ws <= kEps) return;
-  const float4 q0 = ld4<kCg>(p4 + e.x), q1 = ld4<kCg>(p4 + e.y);
   const V3 p0 = mk(q0), p1 = mk(q1);
   const V3 delta = p0 - p1;
   const float dist = length(delta);
@@ -119,9 +137,8 @@ __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __res
     const float damp = c.w != 0.0f ? sp.sd : (cv >= 0.0f ? sp.td : sp.cd);
     const float tau = damp * 1e-5f;
     const float gamma = fminf(tau / dt, 1e4f);
-    const V3 rel = (p0 - mk(ld4<kCg>(x4 + e.x))) - (p1 - mk(ld4<kCg>(x4 + e.y)));
+    const V3 rel = (p0 - mk(xa)) - (p1 - mk(xb));
     const float vp = dot(dir, rel);
-    const float l = ld1<kCg>(lam + ci);
     const float dl = (-cv - alpha * l - gamma * vp) / ((1.0f + gamma) * ws + alpha);
     lam[ci] = l + dl;
     const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
@@ -129,7 +146,6 @@ __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __res
     p4[e.y] = make_float4(n1.x, n1.y, n1.z, q1.w);
     return;
   }
-  const float l = ld1<kCg>(lam + ci);
   // gamma == 0: (-cv - alpha*l - 0*vp) / (1*ws + alpha)
   const float dl = (-cv - alpha * l) / (1.0f * ws + alpha);
   lam[ci] = l + dl;
@@ -141,6 +157,7 @@ __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __res
 __global__ void k_distance(uint32_t off, uint32_t cnt, const uint2* __restrict__ ids, const float4* __restrict__ par,
                            float4* __restrict__ x4, float4* __restrict__ p4, float* __restrict__ lam,
                            SubstepParams sp, bool damped) {
+  pdl_enter();
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= cnt) return;
   project_distance<false>(off + k, ids, par, x4, p4, lam, sp, damped);
@@ -154,12 +171,15 @@ __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __rest
                                                 float4* __restrict__ p4, float* __restrict__ lam,
                                                 const SubstepParams& sp, bool damped) {
   const float4 c = par[ci];
-  if (c.y >= 1e9f) return;
   const uint4 e = ids[ci];
-  const float w2 = ld4<kCg>(x4 + e.z).w, w3 = ld4<kCg>(x4 + e.w).w;
+  if (c.y >= 1e9f) return;
+  // loads of the written pair issued together (see project_distance)
+  const float4 xc = ld4<kCg>(x4 + e.z), xd = ld4<kCg>(x4 + e.w);
+  const float4 q2 = ld4<kCg>(p4 + e.z), q3 = ld4<kCg>(p4 + e.w);
+  const float l = ld1<kCg>(lam + ci);
+  const float w2 = xc.w, w3 = xd.w;
   const float ws = w2 + w3;
   if (ws <= kEps) return;
-  const float4 q2 = ld4<kCg>(p4 + e.z), q3 = ld4<kCg>(p4 + e.w);
   const V3 p2 = mk(q2), p3 = mk(q3);
   const V3 delta = p2 - p3;
   const float dist = length(delta);
@@ -173,12 +193,11 @@ __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __rest
   const float dt = fmaxf(sp.dt, 1e-8f);
   const float alpha = c.y / (dt * dt);
   const float cv = dist - c.x;
-  const float l = ld1<kCg>(lam + ci);
   float dl;
   if (damped) {
     const float tau = sp.bd * 1e-5f;
     const float gamma = fminf(tau / dt, 1e4f);
-    const V3 rel = (p2 - mk(ld4<kCg>(x4 + e.z))) - (p3 - mk(ld4<kCg>(x4 + e.w)));
+    const V3 rel = (p2 - mk(xc)) - (p3 - mk(xd));
     const float vp = dot(dir, rel);
     dl = (-cv - alpha * l - gamma * vp) / ((1.0f + gamma) * ws + alpha);
   } else {
@@ -193,6 +212,7 @@ __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __rest
 __global__ void k_bending(uint32_t off, uint32_t cnt, const uint4* __restrict__ ids, const float4* __restrict__ par,
                           float4* __restrict__ x4, float4* __restrict__ p4, float* __restrict__ lam,
                           SubstepParams sp, bool damped) {
+  pdl_enter();
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= cnt) return;
   project_bending<false>(off + k, ids, par, x4, p4, lam, sp, damped);
@@ -218,6 +238,7 @@ __device__ __forceinline__ void update_vertex(uint32_t i, float4* __restrict__ x
 }
 __global__ void k_update_vel(uint32_t n, float4* __restrict__ x4, const float4* __restrict__ p4,
                              float4* __restrict__ v4, float dt_sub) {
+  pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   update_vertex<false>(i, x4, p4, v4, dt_sub);
@@ -433,6 +454,7 @@ __device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ 
 template <bool kBone>
 __global__ void k_collision(uint32_t n, float4* __restrict__ x4, float4* __restrict__ p4, ColliderArgs ca,
                             float dt) {
+  pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   collide_vertex<false, kBone>(i, x4, p4, ca, dt);
@@ -636,6 +658,80 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
       for (uint32_t i = tid; i < a.n; i += stride) update_vertex<true>(i, a.x4, a.p4, a.v4, dts);
       if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
     }
+  }
+}
+
+// ---------------------------------------------------------------------
+// cluster solver for batched instances
+// ---------------------------------------------------------------------
+// Instances share no vertex, so a thread-block cluster can own a bin of
+// whole instances (a contiguous vertex range) and run the complete frame on
+// it, separating colour steps with the cluster barrier instead of a grid
+// barrier or a kernel launch.  Constraints are visited through a permutation
+// sorted by (bin, colour): every constraint still runs the same device
+// function in its colour step, and constraints of one colour share no vertex,
+// so the results are the bits of the one-launch-per-colour path.  Loads of
+// data that other CTAs write go around L1 (ld.global.cg).
+struct ClusterTables {
+  const uint2* vrange;     // [bins] vertex range [x, y)
+  const uint2* pins;       // [bins] (first, count) into pin_v / pin_t
+  const uint2* dist;       // [bins * ndc] (first, count) into dist_perm
+  const uint2* bend;       // [bins * nbc] (first, count) into bend_perm
+  const uint32_t* dist_perm;
+  const uint32_t* bend_perm;
+};
+template <bool kBone>
+__global__ void __launch_bounds__(256) k_solver_cluster(SolverArgs a, ClusterTables t) {
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  const uint32_t bin = blockIdx.x / cl.dim_blocks().x;
+  const uint32_t tid = cl.block_rank() * blockDim.x + threadIdx.x;
+  const uint32_t stride = cl.num_blocks() * blockDim.x;
+  const float dts = a.sp.dt;
+  const uint2 vr = t.vrange[bin], pr = t.pins[bin];
+  // the bin's constraints are contiguous in the permutations across colours
+  const uint32_t d0 = a.ndc ? t.dist[bin * a.ndc].x : 0u;
+  const uint32_t d1 = a.ndc ? t.dist[bin * a.ndc + a.ndc - 1].x + t.dist[bin * a.ndc + a.ndc - 1].y : 0u;
+  const uint32_t b0 = a.nbc ? t.bend[bin * a.nbc].x : 0u;
+  const uint32_t b1 = a.nbc ? t.bend[bin * a.nbc + a.nbc - 1].x + t.bend[bin * a.nbc + a.nbc - 1].y : 0u;
+  for (uint32_t sub = 0; sub < a.nsub; ++sub) {
+    for (uint32_t k = d0 + tid; k < d1; k += stride) a.dlam[t.dist_perm[k]] = 0.f;
+    for (uint32_t k = b0 + tid; k < b1; k += stride) a.blam[t.bend_perm[k]] = 0.f;
+    for (uint32_t i = vr.x + tid; i < vr.y; i += stride) predict_vertex<true>(i, a.x4, a.p4, a.v4, a.sp);
+    cl.sync();
+    for (uint32_t it = 0; it < a.iters; ++it) {
+      if (pr.y) {
+        for (uint32_t k = pr.x + tid; k < pr.x + pr.y; k += stride) pin_one<true>(k, a.pin_v, a.pin_t, a.x4, a.p4, dts);
+        cl.sync();
+      }
+      for (uint32_t c = 0; c < a.ndc; ++c) {
+        const uint2 r = t.dist[bin * a.ndc + c];
+        if (!r.y) continue;
+        for (uint32_t k = r.x + tid; k < r.x + r.y; k += stride)
+          project_distance<true>(t.dist_perm[k], a.dist_ids, a.dist_par, a.x4, a.p4, a.dlam, a.sp, a.ddamp);
+        cl.sync();
+      }
+      for (uint32_t c = 0; c < a.nbc; ++c) {
+        const uint2 r = t.bend[bin * a.nbc + c];
+        if (!r.y) continue;
+        for (uint32_t k = r.x + tid; k < r.x + r.y; k += stride)
+          project_bending<true>(t.bend_perm[k], a.bend_ids, a.bend_par, a.x4, a.p4, a.blam, a.sp, a.bdamp);
+        cl.sync();
+      }
+      if (a.hascol && a.coupled) {
+        for (uint32_t i = vr.x + tid; i < vr.y; i += stride) collide_vertex<true, kBone>(i, a.x4, a.p4, a.ca, dts);
+        cl.sync();
+      }
+    }
+    if (a.hascol && !a.coupled) {
+      for (uint32_t i = vr.x + tid; i < vr.y; i += stride) collide_vertex<true, kBone>(i, a.x4, a.p4, a.ca, dts);
+      cl.sync();
+    }
+    if (pr.y) {
+      for (uint32_t k = pr.x + tid; k < pr.x + pr.y; k += stride) pin_one<true>(k, a.pin_v, a.pin_t, a.x4, a.p4, dts);
+      cl.sync();
+    }
+    for (uint32_t i = vr.x + tid; i < vr.y; i += stride) update_vertex<true>(i, a.x4, a.p4, a.v4, dts);
+    cl.sync();
   }
 }
 

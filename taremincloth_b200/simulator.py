@@ -401,7 +401,10 @@ class ClothSimulator:
         self._c(self._L.tc_set_persistent_solver(self._h, int(bool(enable))))
 
     def set_launch_config(self, persistent=True, blocks_per_sm=4):
-        self._c(self._L.tc_set_launch_config(self._h, int(bool(persistent)), int(blocks_per_sm)))
+        """persistent: False = one launch per colour, True = persistent cooperative
+        solver with `blocks_per_sm`, 2 = cluster solver (batched instances)."""
+        mode = 2 if persistent == 2 else int(bool(persistent))
+        self._c(self._L.tc_set_launch_config(self._h, mode, int(blocks_per_sm)))
 
     def get_launch_limits(self):
         a, b = C.c_uint32(), C.c_uint32()
