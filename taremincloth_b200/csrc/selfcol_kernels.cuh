@@ -656,7 +656,7 @@ __device__ __forceinline__ bool vt_entry(const SCArgs& s, const VertCtx& c, cons
   return true;
 }
 
-__global__ void __launch_bounds__(256, 3) k_sc_solve(SCArgs s) {
+__global__ void __launch_bounds__(256, 4) k_sc_solve(SCArgs s) {
   __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
   __shared__ uint32_t sh_th[8][kTwoHopCache];
   __shared__ float sh_thr[8][kTwoHopCache];
@@ -1244,7 +1244,7 @@ __global__ void __launch_bounds__(256) k_ee_ccd(SCArgs s) {
 // round.  The per-edge cap on counted candidates (search_count >
 // max_search_iterations, :356-359) is applied with a ballot prefix count, so
 // exactly the reference's first max_search counted pairs are processed.
-__global__ void __launch_bounds__(256, 3) k_ee(SCArgs s) {
+__global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
   __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
   __shared__ uint32_t sh_th[8][2][kTwoHopCache];
   __shared__ float sh_thr[8][2][kTwoHopCache];
