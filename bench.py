@@ -121,6 +121,10 @@ def algorithmic_bytes(pass_name, sim_counts, n_tris):
     return 0
 
 
+WORKLOAD = ("two 256x256 sheets (131072 vertices) on a 20480-triangle icosphere mesh collider, "
+            "self-collision on, 20 substeps x 4 iterations per step")
+
+
 def run_reference(args, rank):
     """CPU implementation of the reference algorithm (the oracle, OpenMP over
     the host's cores) on the same workload; each step is a bounded sample of
@@ -146,8 +150,9 @@ def run_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": sc["name"] + " (one substep per step)", "vertices": n, "substeps_per_step": 1,
-                   "iterations": sc["iterations"]},
+        "config": {"workload": WORKLOAD, "vertices": n, "substeps": sc["substeps"], "iterations": sc["iterations"],
+                   "parallelism": "replicas x1",
+                   "path": "CPU restatement of the reference algorithm (OpenMP); each step is one substep"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{args.steps} substeps of the full workload, OpenMP over {cores} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -393,8 +398,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "two 256x256 sheets (131072 vertices) on a 20480-triangle icosphere mesh collider, "
-                               "self-collision on, 20 substeps x 4 iterations per step",
+        "config": {"workload": WORKLOAD,
                    "vertices": n, "substeps": sub, "iterations": sc["iterations"],
                    "distance_constraints": counts["nd"], "bending_constraints": counts["nb"],
                    "l2": "256 MB buffer written before every timed step", "parallelism": f"replicas x{world}",

@@ -335,7 +335,9 @@ struct Sim {
   DBuf<float4> dist_par, bend_par;
   DBuf<uint4> bend_ids;
   DBuf<uint32_t> adj_off, adj_idx, th_off, th_idx, star_off, edge_bits;
-  DBuf<uint32_t> keys, counts, cursor, cs, srt, ekeys, ecs, esrt;
+  DBuf<uint32_t> keys, counts, cursor, cs, srt, ekeys, ecs, esrt, ecounts, ecursor, etile_sum;
+  cudaStream_t st2 = nullptr;  // edge side of self-collision
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   DBuf<float4> nrm;
   DBuf<int32_t> acc;
   DBuf<int4> vcell, ecell;
@@ -464,6 +466,9 @@ struct Sim {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (auto e : ev_pool) cudaEventDestroy(e);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st2) cudaStreamDestroy(st2);
     if (st) cudaStreamDestroy(st);
     if (h_err) cudaFreeHost(h_err);
     if (h_fb) cudaFreeHost(h_fb);
@@ -583,6 +588,10 @@ struct Sim {
     const size_t T = m.table;
     keys.alloc(n); counts.alloc(T + 1); cursor.alloc(T + 1); cs.alloc(T + 1); srt.alloc(n);
     ekeys.alloc(ne); ecs.alloc(T + 1); esrt.alloc(ne);
+    ecounts.alloc(T + 1); ecursor.alloc(T + 1); etile_sum.alloc(64);
+    TC_CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    TC_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    TC_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     nrm.alloc(n);
     acc.alloc(size_t(n) * A_N);
     vcell.alloc(n); mlen.alloc(n); ecell.alloc(ne); eamin.alloc(ne); eamax.alloc(ne);
@@ -779,46 +788,69 @@ struct Sim {
 
   static unsigned grid(uint32_t cnt, unsigned b) { return (cnt + b - 1) / b; }
 
-  void encode_hash(int which) {
+  // Spatial hash of the vertices (which = 0) or edge midpoints (which = 1) on
+  // stream `ss`; the edge build has its own counting scratch so that it can
+  // run beside the vertex side.
+  void encode_hash(int which, cudaStream_t ss) {
     const uint32_t cnt = which == 0 ? n : ne;
     const uint32_t T = m.table;
     uint32_t* k = which == 0 ? keys.p : ekeys.p;
     uint32_t* start = which == 0 ? cs.p : ecs.p;
     uint32_t* sorted = which == 0 ? srt.p : esrt.p;
-    TC_CK(cudaMemsetAsync(counts.p, 0, (T + 1) * sizeof(uint32_t), st));
-    TC_CK(cudaMemsetAsync(cursor.p, 0, (T + 1) * sizeof(uint32_t), st));
+    uint32_t* cnts = which == 0 ? counts.p : ecounts.p;
+    uint32_t* curs = which == 0 ? cursor.p : ecursor.p;
+    uint32_t* tsum = which == 0 ? tile_sum.p : etile_sum.p;
+    TC_CK(cudaMemsetAsync(cnts, 0, (T + 1) * sizeof(uint32_t), ss));
+    TC_CK(cudaMemsetAsync(curs, 0, (T + 1) * sizeof(uint32_t), ss));
     timed(which == 0 ? "hash_vertices" : "hash_edges", [&] {
       if (cnt)
-        k_hash_count<<<grid(cnt, 256), 256, 0, st>>>(cnt, which, x4.p, p4.p, edges.p, m.cell, T, k, counts.p,
+        k_hash_count<<<grid(cnt, 256), 256, 0, ss>>>(cnt, which, x4.p, p4.p, edges.p, m.cell, T, k, cnts,
                                                       which == 0 ? vcell.p : ecell.p, mlen.p, eamin.p, eamax.p);
       const uint32_t ntiles = (T + 1023) / 1024;
-      k_scan_blocks<<<ntiles, 1024, 0, st>>>(T, counts.p, start, tile_sum.p);
-      k_scan_finish<<<ntiles, 1024, 0, st>>>(T, ntiles, tile_sum.p, start);
-      if (cnt) k_hash_scatter<<<grid(cnt, 256), 256, 0, st>>>(cnt, k, start, cursor.p, sorted);
-      k_hash_sort_buckets<<<grid(T, 256), 256, 0, st>>>(T, start, sorted);
+      k_scan_blocks<<<ntiles, 1024, 0, ss>>>(T, cnts, start, tsum);
+      k_scan_finish<<<ntiles, 1024, 0, ss>>>(T, ntiles, tsum, start);
+      if (cnt) k_hash_scatter<<<grid(cnt, 256), 256, 0, ss>>>(cnt, k, start, curs, sorted);
+      k_hash_sort_buckets<<<grid(T, 256), 256, 0, ss>>>(T, start, sorted);
       if (cnt && which == 0)
-        k_gather_vertices<<<grid(cnt, 256), 256, 0, st>>>(cnt, sorted, x4.p, p4.p, v4.p, local_len.p, mlen.p, vcell.p,
+        k_gather_vertices<<<grid(cnt, 256), 256, 0, ss>>>(cnt, sorted, x4.p, p4.p, v4.p, local_len.p, mlen.p, vcell.p,
                                                            vs_p.p, vs_c.p, vs_q.p);
       if (cnt && which == 1)
-        k_gather_edges<<<grid(cnt, 256), 256, 0, st>>>(cnt, sorted, edges.p, ecell.p, eamin.p, eamax.p, es_c.p, es_v.p,
+        k_gather_edges<<<grid(cnt, 256), 256, 0, ss>>>(cnt, sorted, edges.p, ecell.p, eamin.p, eamax.p, es_c.p, es_v.p,
                                                         es_lo.p, es_hi.p);
     });
   }
+  void encode_hash(int which) { encode_hash(which, st); }
+  void encode_ee(const SCArgs& a, cudaStream_t ss) {
+    timed("sc_solve_ee", [&] {
+      TC_CK(cudaMemsetAsync(ccd_n.p, 0, sizeof(uint32_t), ss));
+      k_ee<<<grid(ne, 8), 256, 0, ss>>>(a);
+    });
+    timed("sc_solve_ee_ccd", [&] { k_ee_ccd<<<148 * 8, 256, 0, ss>>>(a); });
+  }
 
+  // The edge side (edge hash, E-E, deferred CCD) reads positions, normals
+  // and its own hash, and writes the contact accumulators only through
+  // atomic add / max / min, which commute with the vertex side's; so outside
+  // profiling it runs on a second stream concurrently with the vertex side
+  // (vertex hash, V-V / V-T, untangle), joined before apply.
   void encode_self_collision(bool run_ee = true) {
     SCArgs a = sc_args();
     if (a.untangle) timed("sc_normals", [&] { k_normals<<<grid(n, 256), 256, 0, st>>>(n, x4.p, star_off.p, star_idx.p, nrm.p); });
+    const bool edges_on = run_ee && ne > 0;
+    const bool fork = edges_on && !profiling;
+    if (fork) {
+      TC_CK(cudaEventRecord(ev_fork, st));
+      TC_CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+      encode_hash(1, st2);
+      encode_ee(a, st2);
+      TC_CK(cudaEventRecord(ev_join, st2));
+    }
     encode_hash(0);
-    if (run_ee && ne > 0) encode_hash(1);
+    if (edges_on && !fork) encode_hash(1);
     timed("sc_solve", [&] { k_sc_solve<<<grid(n, 8), 256, 0, st>>>(a); });
     if (a.untangle) timed("sc_untangle", [&] { k_untangle<<<grid(n, 128), 128, 0, st>>>(a); });
-    if (run_ee && ne > 0) {
-      timed("sc_solve_ee", [&] {
-        TC_CK(cudaMemsetAsync(ccd_n.p, 0, sizeof(uint32_t), st));
-        k_ee<<<grid(ne, 8), 256, 0, st>>>(a);
-      });
-      timed("sc_solve_ee_ccd", [&] { k_ee_ccd<<<148 * 8, 256, 0, st>>>(a); });
-    }
+    if (fork) TC_CK(cudaStreamWaitEvent(st, ev_join, 0));
+    if (edges_on && !fork) encode_ee(a, st);
     timed("sc_apply", [&] {
       k_apply<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, local_len.p, acc.p, relief, enable_relief ? 1 : 0,
                                              max_disp_ratio);
