@@ -269,6 +269,10 @@ tc_status tc_get_launch_limits(tc_sim *s, uint32_t *max_blocks_per_sm, uint32_t 
  * released, with the given poll limit (1..4194304), and returns
  * TC_ERR_TIMEOUT when every wait ended by the limit.  Touches no state. */
 tc_status tc_check_barrier_timeout(tc_sim *s, uint32_t spin_limit);
+/* Diagnostics (new): out = edge pairs the latest self-collision pass handed to
+ * the deferred edge-edge CCD kernel, and the queue capacity (pairs beyond it
+ * run inline in the warp pass). */
+tc_status tc_get_ccd_queue(tc_sim *s, uint32_t out[2]);
 /* Kernel launches in the recorded frame (kernel nodes of its CUDA graph). */
 tc_status tc_frame_kernel_count(tc_sim *s, uint32_t *count);
 /* Device time of the latest frame in milliseconds (CUDA events). */

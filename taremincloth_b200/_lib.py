@@ -75,6 +75,7 @@ SIGNATURES = {
     "tc_check_barrier_timeout": [_P, _U],
     "tc_hash_build_static": [_P, _U, _F, _U, _P, _P, _P],
     "tc_take_profile": [_P, C.c_char_p, C.c_size_t, _P, _P, _U, C.POINTER(_U)],
+    "tc_get_ccd_queue": [_P, _P],
     "tc_set_adaptive_substep_options": [_P, _I, _U, _U],
     "tc_set_auto_compensate_iterations": [_P, _I],
     "tc_set_strain_adaptive_options": [_P, _I, _F],

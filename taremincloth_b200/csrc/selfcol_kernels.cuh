@@ -47,6 +47,9 @@ struct SCArgs {
   int32_t* acc;
   // per-substep caches written by the hash pass (same float operations as
   // the reference performs per candidate, done once per element)
+  // per vertex j: bounding box of p over j and its star triangles' vertices,
+  // and the range of their motion p - x: (lo, mlo.x), (hi, mlo.y), (mhi, mlo.z)
+  const float4* sbox;
   const int4* vcell;    // floor(p / cell) per vertex
   const float* mlen;    // |p - x| per vertex
   const int4* ecell;    // floor(midpoint / cell) per edge
@@ -126,6 +129,28 @@ __device__ __forceinline__ TwoHop stage_two_hop(const uint32_t* th_off, const ui
 }
 
 __device__ __forceinline__ uint32_t layer_of(const float4* v4, uint32_t i) { return __float_as_uint(v4[i].w); }
+
+// Star boxes for the vertex-triangle pass (see SCArgs::sbox): one thread per
+// vertex over its star pairs.
+__global__ void k_star_box(uint32_t n, const uint32_t* __restrict__ star_off, const uint2* __restrict__ star_idx,
+                           const float4* __restrict__ x4, const float4* __restrict__ p4, float4* __restrict__ sbox) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const V3 pj = mk(p4[j]);
+  V3 lo = pj, hi = pj, mlo = pj - mk(x4[j]), mhi = mlo;
+  for (uint32_t k = star_off[j]; k < star_off[j + 1]; ++k) {
+    const uint2 pr = star_idx[k];
+    const V3 a = mk(p4[pr.x]), b = mk(p4[pr.y]);
+    const V3 ma = a - mk(x4[pr.x]), mb = b - mk(x4[pr.y]);
+    lo = vmin(lo, vmin(a, b));
+    hi = vmax(hi, vmax(a, b));
+    mlo = vmin(mlo, vmin(ma, mb));
+    mhi = vmax(mhi, vmax(ma, mb));
+  }
+  sbox[3 * size_t(j)] = make_float4(lo.x, lo.y, lo.z, mlo.x);
+  sbox[3 * size_t(j) + 1] = make_float4(hi.x, hi.y, hi.z, mlo.y);
+  sbox[3 * size_t(j) + 2] = make_float4(mhi.x, mhi.y, mhi.z, mlo.z);
+}
 
 // ---------------- normals: shaders/compute_normals.wgsl:25-58
 __global__ void k_normals(uint32_t n, const float4* __restrict__ x4, const uint32_t* __restrict__ star_off,
@@ -476,6 +501,25 @@ __device__ __forceinline__ bool sc_work_vv(const SCArgs& s, const VertCtx& c, co
   const float mlj = q.w;
   const float vtb = eth + llj * 1.3f + mli + mlj;
   if (!(d2 <= vtb * vtb) || within2_t(th, index, j)) return false;
+  {
+    // Every triangle of j's star is skipped by its own swept-box test
+    // (smin > tmax or smax < tmin on an axis) when the widest possible swept
+    // box of i, over the star's motion range plus a 10 um rounding margin,
+    // misses the star's box: skipping the whole star is then exact.
+    const float4 b0 = s.sbox[3 * size_t(j)], b1 = s.sbox[3 * size_t(j) + 1], b2 = s.sbox[3 * size_t(j) + 2];
+    const V3 xi = c.xi;
+    const float sl = 1e-5f;
+    const float rl[3] = {xi.x + b0.w - sl, xi.y + b1.w - sl, xi.z + b2.w - sl};
+    const float rh[3] = {xi.x + b2.x + sl, xi.y + b2.y + sl, xi.z + b2.z + sl};
+    const float pa[3] = {pi.x, pi.y, pi.z};
+    const float lo[3] = {b0.x, b0.y, b0.z}, hi[3] = {b1.x, b1.y, b1.z};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      const float smin_lb = fminf(rl[ax], pa[ax]) - eth - sl;
+      const float smax_ub = fmaxf(rh[ax], pa[ax]) + eth + sl;
+      if (smin_lb > hi[ax] || smax_ub < lo[ax]) return false;
+    }
+  }
   st_b = s.star_off[j];
   st_e = s.star_off[j + 1];
   // what the triangle filter needs of j: p, contact thickness, x, index

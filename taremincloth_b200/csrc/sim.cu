@@ -341,6 +341,7 @@ struct Sim {
   DBuf<float4> nrm;
   DBuf<int32_t> acc;
   DBuf<int4> vcell, ecell;
+  DBuf<float4> sbox;
   DBuf<float> mlen;
   DBuf<float4> eamin, eamax;
   DBuf<float4> vs_p, vs_q, es_lo, es_hi;
@@ -594,7 +595,7 @@ struct Sim {
     TC_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     nrm.alloc(n);
     acc.alloc(size_t(n) * A_N);
-    vcell.alloc(n); mlen.alloc(n); ecell.alloc(ne); eamin.alloc(ne); eamax.alloc(ne);
+    vcell.alloc(n); mlen.alloc(n); sbox.alloc(3 * size_t(n)); ecell.alloc(ne); eamin.alloc(ne); eamax.alloc(ne);
     ccd_q.alloc(size_t(ne) * 4 + 1024); ccd_n.alloc(1);
     vs_p.alloc(n); vs_q.alloc(n); vs_c.alloc(n); tile_sum.alloc(64); es_c.alloc(ne); es_v.alloc(ne); es_lo.alloc(ne); es_hi.alloc(ne);
     TC_CK(cudaMemsetAsync(acc.p, 0, size_t(n) * A_N * sizeof(int32_t), st));
@@ -780,6 +781,7 @@ struct Sim {
     a.adj_off = adj_off.p; a.adj_idx = adj_idx.p; a.th_off = th_off.p; a.th_idx = th_idx.p; a.th_rest = th_rest.p;
     a.star_off = star_off.p; a.star_idx = star_idx.p; a.edges = edges.p; a.edge_bits = edge_bits.p;
     a.cs = cs.p; a.srt = srt.p; a.ecs = ecs.p; a.esrt = esrt.p; a.nrm = nrm.p; a.acc = acc.p;
+    a.sbox = sbox.p;
     a.vcell = vcell.p; a.mlen = mlen.p; a.ecell = ecell.p; a.eamin = eamin.p; a.eamax = eamax.p;
     a.ccd_q = ccd_q.p; a.ccd_n = ccd_n.p; a.ccd_cap = uint32_t(ccd_q.n);
     a.vs_p = vs_p.p; a.vs_q = vs_q.p; a.vs_c = vs_c.p; a.es_c = es_c.p; a.es_v = es_v.p; a.es_lo = es_lo.p; a.es_hi = es_hi.p;
@@ -846,6 +848,7 @@ struct Sim {
       TC_CK(cudaEventRecord(ev_join, st2));
     }
     encode_hash(0);
+    timed("sc_star_box", [&] { k_star_box<<<grid(n, 256), 256, 0, st>>>(n, star_off.p, star_idx.p, x4.p, p4.p, sbox.p); });
     if (edges_on && !fork) encode_hash(1);
     timed("sc_solve", [&] { k_sc_solve<<<grid(n, 8), 256, 0, st>>>(a); });
     if (a.untangle) timed("sc_untangle", [&] { k_untangle<<<grid(n, 128), 128, 0, st>>>(a); });
@@ -2790,6 +2793,22 @@ tc_status tc_bake_get(tc_bake* b, uint32_t* texels, float* infos, uint32_t* acti
 tc_status tc_bake_destroy(tc_bake* b) {
   delete b;
   return TC_OK;
+}
+
+// ---- diagnostics of the latest self-collision pass: pairs handed to the
+// deferred edge-edge CCD kernel, and the queue capacity
+tc_status tc_get_ccd_queue(tc_sim* s, uint32_t out[2]) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr, "out required");
+    uint32_t q = 0;
+    if (m.ccd_n.p) {
+      TC_CK(cudaMemcpyAsync(&q, m.ccd_n.p, sizeof q, cudaMemcpyDeviceToHost, m.st));
+      TC_CK(cudaStreamSynchronize(m.st));
+    }
+    out[0] = q;
+    out[1] = uint32_t(m.ccd_q.n);
+  });
 }
 
 // ---- adaptive substeps and iterations (mod.rs:723-790, dispatch.rs:477-607)

@@ -426,6 +426,12 @@ class ClothSimulator:
         self._c(self._L.tc_last_frame_ms(self._h, C.byref(v)))
         return v.value
 
+    def get_ccd_queue(self):
+        """(edge pairs deferred to the CCD kernel in the latest self-collision pass, capacity)"""
+        out = np.zeros(2, _u32)
+        self._c(self._L.tc_get_ccd_queue(self._h, _ptr(out)))
+        return int(out[0]), int(out[1])
+
     # ---- adaptive substeps and iterations (lib.rs:1788-1805, :1950-1965)
     def set_adaptive_substep_options(self, enabled, min_substeps=4, max_substeps=64):
         self._c(self._L.tc_set_adaptive_substep_options(self._h, int(bool(enabled)), int(min_substeps),
