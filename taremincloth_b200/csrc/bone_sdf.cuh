@@ -144,7 +144,11 @@ __device__ __forceinline__ uint32_t pack_half2(float lo, float hi) {
 // Voxel state of the sequential nearest-triangle rule (bake_sdf.wgsl:71-183)
 struct BakeState {
   float min_d2, best_abs_proj, best_signed, best_alpha;
+  float reach;  // sqrt((min_d2 + tolerance) * 1.0001), refreshed when min_d2 changes
 };
+__device__ __forceinline__ float bake_reach(float min_d2) {
+  return sqrtf((min_d2 + 1e-7f * fmaxf(1.0f, min_d2)) * 1.0001f);
+}
 __device__ __forceinline__ void bake_visit(BakeState& s, V3 p, const BakeTri& tri) {
   const V3 a = mk(tri.p0w0), b = mk(tri.p1w1), c = mk(tri.p2w2);
   const V3 ab = b - a, ac = c - a, ap = p - a;
@@ -203,7 +207,10 @@ __device__ __forceinline__ void bake_visit(BakeState& s, V3 p, const BakeTri& tr
   const bool closer = d_sq + eps_sq < s.min_d2;
   const bool tie = fabsf(d_sq - s.min_d2) <= eps_sq && aproj > s.best_abs_proj;
   if (closer || tie) {
-    if (d_sq < s.min_d2) s.min_d2 = d_sq;
+    if (d_sq < s.min_d2) {
+      s.min_d2 = d_sq;
+      s.reach = bake_reach(d_sq);
+    }
     s.best_abs_proj = aproj;
     const float d = sqrtf(d_sq);
     float sign = proj >= 0.f ? 1.f : -1.f;
@@ -229,11 +236,12 @@ __device__ __forceinline__ void bake_visit(BakeState& s, V3 p, const BakeTri& tr
   }
 }
 // true when nothing in the sphere can be accepted for this voxel state
+// |p - c| - r > reach, tested on squares with a 1e-5 relative margin for
+// rounding (no square root per test)
 __device__ __forceinline__ bool bake_far(const BakeState& s, V3 p, float4 sph) {
-  const float dc = length(p - mk(sph)) - sph.w;
-  if (dc <= 0.f) return false;
-  const float lim = s.min_d2 + 1e-7f * fmaxf(1.0f, s.min_d2);
-  return dc * dc > lim * 1.0001f;
+  const V3 d = p - mk(sph);
+  const float rr = sph.w + s.reach;
+  return dot(d, d) > (rr * rr) * 1.00001f;
 }
 
 // ---- bake_sdf.wgsl:33-196.  Block = 8 warps = an 8 x 8 x 4 voxel region of
@@ -258,7 +266,7 @@ __global__ void __launch_bounds__(256) k_bone_bake(const BakeParams* __restrict_
   const V3 uvw = mk((float(vx) + 0.5f) / fr, (float(vy) + 0.5f) / fr, (float(vz) + 0.5f) / fr);
   const V3 p = mk(P.lmin[0] + uvw.x * (P.lmax[0] - P.lmin[0]), P.lmin[1] + uvw.y * (P.lmax[1] - P.lmin[1]),
                   P.lmin[2] + uvw.z * (P.lmax[2] - P.lmin[2]));
-  BakeState s{1e10f, -1.0f, 10.0f, 0.0f};
+  BakeState s{1e10f, -1.0f, 10.0f, 0.0f, bake_reach(1e10f)};
   const uint32_t t0 = P.tri_start, tn = P.tri_count;
   const uint32_t tile0 = bone_tile_off[param_bone[blockIdx.y]];
   for (uint32_t k = 0; k * 32u < tn; ++k) {
