@@ -218,6 +218,10 @@ tc_status tc_get_edges(tc_sim *s, uint32_t *edges, uint32_t *bits);
  * last substep of the latest frame, when tracking is on.  rms/max arrays are
  * sized by the colour counts; totals[4] = dist rms, dist max, bend rms, bend max. */
 tc_status tc_set_residual_tracking(tc_sim *s, int enable);
+/* With residual tracking: RMS residual |C| over all distance and bending
+ * constraints at the predicted positions of the latest frame's last substep
+ * (before any iteration, lambda = 0). */
+tc_status tc_get_predicted_residual(tc_sim *s, float *rms);
 tc_status tc_get_residuals(tc_sim *s, float *dist_rms, float *dist_max, float *bend_rms, float *bend_max,
                            float totals[4]);
 /* ---- host-only topology build (no device needed) ----
@@ -284,8 +288,9 @@ tc_status tc_last_frame_ms(tc_sim *s, float *ms);
  * each vertex's correction p_final - p_predicted of the coming substep, in
  * units of the vertex's local edge length.  While enabled, a substep moves p
  * by that prediction, runs (iterations - k_replaced) plain XPBD iterations,
- * computes the max constraint residual |C + alpha~ lambda| and, when it is
- * above res_thresh (the plain solver's residual; +inf never falls back),
+ * computes the RMS constraint residual |C + alpha~ lambda| over all distance
+ * and bending constraints and, when it is above res_thresh (the plain
+ * solver's residual; +inf never falls back),
  * runs the k_replaced remaining iterations.  Needs cooperative launch. */
 uint32_t tc_ws_param_count(void);
 tc_status tc_ws_enable(tc_sim *s, int enable, uint32_t k_replaced, float res_thresh);
@@ -296,15 +301,28 @@ tc_status tc_ws_enable(tc_sim *s, int enable, uint32_t k_replaced, float res_thr
 tc_status tc_ws_record(tc_sim *s, uint32_t capacity, uint32_t every);
 tc_status tc_ws_recorded(tc_sim *s, uint32_t *count);
 /* Adam over the recorded snapshots (epochs x snapshots steps, seeded
- * shuffle); mean MSE loss of the first and last epoch. */
+ * shuffle); mean MSE loss (of the normalised target) of the first and last
+ * epoch.  The first training of a network that was not loaded with
+ * tc_ws_set_params first fits its normalizer on the recorded snapshots. */
 tc_status tc_ws_train(tc_sim *s, uint32_t epochs, float lr, uint64_t seed, float *loss_first, float *loss_last);
 /* fp32 parameter blob (tc_ws_param_count() floats): W0[16][64] b0[64]
- * W1[128][64] b1[64] W2[128][64] b2[64] W3[64][3] b3[3], weights [in][out]. */
+ * W1[128][64] b1[64] W2[128][64] b2[64] W3[64][3] b3[3], weights [in][out],
+ * then the normalizer FS[16] YS[1]: features enter as bf16(feature * FS),
+ * vertices move by Y * YS * L (YS <= 0 reads as 1).  Setting a blob keeps
+ * its normalizer for later training. */
 tc_status tc_ws_get_params(tc_sim *s, float *out, size_t len);
 tc_status tc_ws_set_params(tc_sim *s, const float *params, size_t len);
 /* out = warm-started substeps, substeps that fell back, max residual of the
  * latest substep's check, threshold */
 tc_status tc_ws_stats(tc_sim *s, double out[4]);
+/* Relative threshold (ratio > 0; 0 returns to res_thresh): a warm-started
+ * substep falls back when its residual is above ratio x the RMS residual
+ * |C| of its predicted positions (before the network moves them, lambda =
+ * 0; at least 1e-6 of the mean edge length), so the threshold follows the
+ * scene.  The ratio is the plain solver's
+ * final / predicted residual (tc_get_predicted_residual), e.g. a percentile
+ * over plain substeps.  tc_ws_stats then reports the latest threshold. */
+tc_status tc_ws_set_relative_threshold(tc_sim *s, float ratio);
 tc_status tc_ws_reset_stats(tc_sim *s);
 /* Loss, parameter gradients and outputs of the warm-start network on one
  * graph, through the same kernels as training (for gradient checks).

@@ -5,15 +5,16 @@ upstream algorithm to restate: this module restates the network that
 taremincloth_b200/csrc/warmstart.cuh computes, in numpy, as the checker for
 its forward and backward kernels.  Only tests may import it.
 
-Network (per vertex i, neighbours N(i) from an adjacency CSR):
-    X0 = bf16(features)                      16
+Network (per vertex i, neighbours N(i) from an adjacency CSR; FS, YS the
+normalizer stored after the weights, not trained):
+    X0 = bf16(bf16(features) * FS)           16
     H0 = bf16(SiLU(X0 W0 + b0))              64
     X1 = [H0_i, bf16(mean_{j in N(i)} H0_j)] 128
     H1 = bf16(SiLU(X1 W1 + b1))              64
     X2 = [H1_i, bf16(mean H1_j)]             128
     H2 = bf16(SiLU(X2 W2 + b2))              64
     Y  = H2 bf16(W3) + b3                    3
-    loss = sum_i mask_i |Y_i - T_i|^2 / (3 n)
+    loss = sum_i mask_i |Y_i - T_i / YS|^2 / (3 n)
 Weights are used as bf16, biases as fp32.  The backward pass treats the bf16
 roundings of activations as identity (straight-through) and rounds dZ to bf16
 before the weight and input gradient products, as the kernels do.  With
@@ -24,9 +25,11 @@ from __future__ import annotations
 
 import numpy as np
 
-PARAM_COUNT = 17795
+PARAM_COUNT = 17812
 LAYOUT = (("W0", 0, (16, 64)), ("b0", 1024, (64,)), ("W1", 1088, (128, 64)), ("b1", 9280, (64,)),
           ("W2", 9344, (128, 64)), ("b2", 17536, (64,)), ("W3", 17600, (64, 3)), ("b3", 17792, (3,)))
+# the normalizer (not trained): per-feature input scales and the output scale
+NORM_LAYOUT = (("fscale", 17795, (16,)), ("yscale", 17811, (1,)))
 
 
 def bf16(x):
@@ -39,13 +42,16 @@ def bf16(x):
 
 def unpack(blob, dtype=np.float32):
     blob = np.asarray(blob, dtype).ravel()
-    return {name: blob[off:off + int(np.prod(shape))].reshape(shape) for name, off, shape in LAYOUT}
+    return {name: blob[off:off + int(np.prod(shape))].reshape(shape) for name, off, shape in LAYOUT + NORM_LAYOUT}
 
 
 def pack(params):
+    """Blob of the named arrays; a missing entry is zero (the gradient of the
+    normalizer, which is not trained)."""
     out = np.zeros(PARAM_COUNT, np.float64)
-    for name, off, shape in LAYOUT:
-        out[off:off + int(np.prod(shape))] = np.asarray(params[name]).ravel()
+    for name, off, shape in LAYOUT + NORM_LAYOUT:
+        if name in params:
+            out[off:off + int(np.prod(shape))] = np.asarray(params[name]).ravel()
     return out
 
 
@@ -80,7 +86,9 @@ def forward_backward(feat, adj_off, adj_idx, target, mask, blob, round_bf16=True
     B = [P["b0"].astype(dt), P["b1"].astype(dt), P["b2"].astype(dt)]
     W3 = R(P["W3"]).astype(dt)
     b3 = P["b3"].astype(dt)
-    X = [R(feat).astype(dt)]
+    ys = P["yscale"].astype(dt)[0]
+    ys = ys if ys > 0 else dt(1)
+    X = [R(R(feat).astype(dt) * P["fscale"].astype(dt)).astype(dt)]
     Z, H = [], []
     for layer in range(3):
         if layer > 0:
@@ -91,7 +99,7 @@ def forward_backward(feat, adj_off, adj_idx, target, mask, blob, round_bf16=True
         H.append(R(_silu(z)).astype(dt))
     y = (H[2].astype(np.float64) @ W3.astype(np.float64)).astype(dt) + b3
     m = np.asarray(mask, dt).reshape(n, 1)
-    d = (y - np.asarray(target, dt).reshape(n, 3)) * m
+    d = (y - np.asarray(target, dt).reshape(n, 3) / ys) * m
     loss = float(np.sum(d.astype(np.float64) ** 2) / (3.0 * n))
     dy = (2.0 * d / (3.0 * n)).astype(dt)
     g = {"W3": H[2].astype(np.float64).T @ dy, "b3": dy.sum(0, dtype=np.float64)}
@@ -130,10 +138,15 @@ def grid_graph(w, h):
 
 
 def random_params(rng, scale_head=1.0):
+    """Uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights and biases, and a
+    normalizer of scales in [0.5, 2]."""
     blob = np.zeros(PARAM_COUNT, np.float32)
     for name, off, shape in LAYOUT:
         k = int(np.prod(shape))
         fan_in = shape[0] if len(shape) == 2 else 4.0
         sc = 1.0 / np.sqrt(fan_in) * (scale_head if name == "W3" else 1.0)
         blob[off:off + k] = rng.uniform(-sc, sc, k).astype(np.float32)
+    for name, off, shape in NORM_LAYOUT:
+        k = int(np.prod(shape))
+        blob[off:off + k] = rng.uniform(0.5, 2.0, k).astype(np.float32)
     return blob

@@ -106,6 +106,8 @@ SIGNATURES = {
     "tc_ws_get_params": [_P, _P, C.c_size_t],
     "tc_ws_set_params": [_P, _P, C.c_size_t],
     "tc_ws_stats": [_P, _P],
+    "tc_ws_set_relative_threshold": [_P, _F],
+    "tc_get_predicted_residual": [_P, _P],
     "tc_ws_reset_stats": [_P],
     "tc_mlp_grad": [_U, _P, _P, _P, _P, _P, _P, C.POINTER(_F), _P, _P, _P, _I],
     "tc_mesh_build": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F],

@@ -118,8 +118,10 @@ struct Mlp {
   DBuf<__nv_bfloat16> wb, wbt;
   DBuf<__nv_bfloat16> h0, h1, h2;
   DBuf<float> y;
-  DBuf<__nv_bfloat16> x1, x2, dz;
+  DBuf<__nv_bfloat16> x0, x1, x2, dz;
   DBuf<float> z0, z1, z2, dy, dh, dx;
+  DBuf<uint32_t> ell;  // inference: [n][16] degree, first 15 neighbours
+  unsigned mp_grid = 1;
   uint32_t adam_t = 0;
 
   static unsigned grid(size_t cnt, unsigned b) { return unsigned((cnt + b - 1) / b); }
@@ -129,9 +131,25 @@ struct Mlp {
     wb.alloc(kP_N); wbt.alloc(kT_N);
     h0.alloc(size_t(n) * kWsH); h1.alloc(size_t(n) * kWsH); h2.alloc(size_t(n) * kWsH);
     y.alloc(size_t(n) * 3);
+    int dev = 0, sms = 0, per_sm = 0;
+    TC_CK(cudaGetDevice(&dev));
+    TC_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp, 256, 0));
+    const unsigned tiles = grid(n, kWsRows);
+    mp_grid = std::max(1u, std::min(tiles, unsigned(std::max(per_sm, 1) * sms)));
+  }
+  // the ELL table of the inference kernels from the host CSR
+  void set_ell(const uint32_t* h_off, const uint32_t* h_idx) {
+    std::vector<uint32_t> e(size_t(n) * kWsEll, 0u);
+    for (uint32_t v = 0; v < n; ++v) {
+      const uint32_t b = h_off[v], d = h_off[v + 1] - b;
+      e[size_t(v) * kWsEll] = d;
+      for (uint32_t q = 0; q < std::min(d, uint32_t(kWsEll - 1)); ++q) e[size_t(v) * kWsEll + 1 + q] = h_idx[b + q];
+    }
+    ell.upload(e, st);
   }
   void alloc_train() {
-    x1.alloc(size_t(n) * 128); x2.alloc(size_t(n) * 128); dz.alloc(size_t(n) * kWsH);
+    x0.alloc(size_t(n) * kWsF); x1.alloc(size_t(n) * 128); x2.alloc(size_t(n) * 128); dz.alloc(size_t(n) * kWsH);
     z0.alloc(size_t(n) * kWsH); z1.alloc(size_t(n) * kWsH); z2.alloc(size_t(n) * kWsH);
     dy.alloc(size_t(n) * 3); dh.alloc(size_t(n) * kWsH); dx.alloc(size_t(n) * 128);
   }
@@ -149,6 +167,7 @@ struct Mlp {
     fill(kP_W1, kP_b1 - kP_W1, 1.f / std::sqrt(128.f));
     fill(kP_W2, kP_b2 - kP_W2, 1.f / std::sqrt(128.f));
     fill(kP_W3, kP_b3 - kP_W3, 0.1f / std::sqrt(64.f));
+    for (uint32_t e = kP_FS; e < kP_N; ++e) h[e] = 1.f;  // identity normalizer
     return h;
   }
   void set_params(const float* h) {
@@ -171,34 +190,39 @@ struct Mlp {
     if (!n) return;
     MlpLayerArgs a{};
     a.n = n; a.adj_off = adj_off; a.adj_idx = adj_idx;
-    a.kin = kWsF; a.x_feat = feat; a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0;
-    a.z_out = train ? z0.p : nullptr; a.h_out = h0.p;
+    a.kin = kWsF; a.x_feat = feat; a.fscale = w.p + kP_FS; a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0;
+    a.x_out = train ? x0.p : nullptr; a.z_out = train ? z0.p : nullptr; a.h_out = h0.p;
     k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
-    a.kin = 128; a.x_feat = nullptr; a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1;
+    a.kin = 128; a.x_feat = nullptr; a.fscale = nullptr; a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1;
     a.x_out = train ? x1.p : nullptr; a.z_out = train ? z1.p : nullptr; a.h_out = h1.p;
     k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
     a.h_prev = h1.p; a.wt = wbt.p + kT_W2; a.bias = w.p + kP_b2;
     a.x_out = train ? x2.p : nullptr; a.z_out = train ? z2.p : nullptr; a.h_out = h2.p;
     k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
-    k_mlp_head<<<grid(n, 256), 256, 0, st>>>(n, h2.p, wb.p + kP_W3, w.p + kP_b3, y.p, target, mask,
+    k_mlp_head<<<grid(n, 256), 256, 0, st>>>(n, h2.p, wb.p + kP_W3, w.p + kP_b3, y.p, target, mask, w.p + kP_YS,
                                              1.0f / float(n), target ? dy.p : nullptr, loss);
   }
-  // inference: the head is fused into the last layer, which either writes Y
-  // (y_out) or moves p by Y L on free vertices
-  void infer(const __nv_bfloat16* feat, float* y_out, const float4* x4, float4* p4, const float* local_len) {
+  // inference: layer 0 from the given features (feat) or computed from fa
+  // (then p is kept in ppred first); the head is fused into the last layer,
+  // which either writes Y (y_out) or moves p by Y YS L on free vertices
+  void infer(const __nv_bfloat16* feat, const WsFeatArgs* fa, float4* ppred, float* y_out, const float4* x4,
+             float4* p4, const float* local_len) {
     if (!n) return;
-    MlpLayerArgs a{};
-    a.n = n; a.adj_off = adj_off; a.adj_idx = adj_idx;
-    a.kin = kWsF; a.x_feat = feat; a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0; a.h_out = h0.p;
-    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
-    a.kin = 128; a.x_feat = nullptr; a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1; a.h_out = h1.p;
-    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    MlpInferArgs a{};
+    a.n = n; a.x_feat = feat; if (fa) a.fa = *fa; a.ppred = ppred; a.fscale = w.p + kP_FS;
+    a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0; a.h_out = h0.p;
+    k_mlp_infer_l0<<<grid(n, kWsL0Rows), kWsL0Rows, 0, st>>>(a);
+    a.h_prev = h0.p; a.ell = ell.p; a.adj_off = adj_off; a.adj_idx = adj_idx;
+    a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1; a.h_out = h1.p;
+    k_mlp_infer_mp<<<mp_grid, 256, 0, st>>>(a);
     a.h_prev = h1.p; a.wt = wbt.p + kT_W2; a.bias = w.p + kP_b2; a.h_out = nullptr;
-    a.w3 = wb.p + kP_W3; a.b3 = w.p + kP_b3; a.y_out = y_out; a.x4 = x4; a.p4 = p4; a.local_len = local_len;
-    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    a.w3 = wb.p + kP_W3; a.b3 = w.p + kP_b3; a.yscale = w.p + kP_YS; a.y_out = y_out; a.x4 = x4; a.p4 = p4;
+    a.local_len = local_len;
+    k_mlp_infer_mp<<<mp_grid, 256, 0, st>>>(a);
   }
-  // gradients of the loss of the last forward(train, target) into gw
-  void backward(const __nv_bfloat16* feat) {
+  // gradients of the loss of the last forward(train, target) into gw (layer
+  // 0's input is the scaled copy x0 that forward kept)
+  void backward() {
     TC_CK(cudaMemsetAsync(gw.p, 0, kP_N * sizeof(float), st));
     if (!n) return;
     const unsigned gh = grid(size_t(n) * kWsH, 256), gt = grid(n, kWsRows);
@@ -210,7 +234,31 @@ struct Mlp {
     k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, 128, x1.p, dz.p, wb.p + kP_W1, gw.p + kP_W1, dx.p});
     k_mlp_agg_bwd<<<gh, 256, 0, st>>>(n, dx.p, adj_off, adj_idx, dh.p);
     k_mlp_act_bwd<<<gh, 256, 0, st>>>(n, dh.p, z0.p, dz.p, gw.p + kP_b0);
-    k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, kWsF, feat, dz.p, wb.p + kP_W0, gw.p + kP_W0, nullptr});
+    k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, kWsF, x0.p, dz.p, wb.p + kP_W0, gw.p + kP_W0, nullptr});
+  }
+  // Normalizer from `rows` recorded rows (features, targets, free mask): FS =
+  // 1 / RMS of each feature, YS = RMS of the target components, over the
+  // free rows; FS clamped to [1e-4, 1e4], 1 where a feature is all zero.
+  void fit_normalizer(const __nv_bfloat16* feat, const float* target, const float* mask, size_t rows) {
+    DBuf<float> part;
+    part.alloc(size_t(kWsMomBlocks) * kWsMom);
+    k_ws_moments<<<kWsMomBlocks, 256, 0, st>>>(rows, feat, target, mask, part.p);
+    std::vector<float> h(size_t(kWsMomBlocks) * kWsMom), blob(kP_N);
+    TC_CK(cudaMemcpyAsync(h.data(), part.p, h.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaMemcpyAsync(blob.data(), w.p, kP_N * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaStreamSynchronize(st));
+    double sum[kWsMom] = {};
+    for (int b = 0; b < kWsMomBlocks; ++b)
+      for (int c = 0; c < kWsMom; ++c) sum[c] += h[size_t(b) * kWsMom + c];
+    const double cnt = sum[kWsF + 1];
+    if (cnt <= 0.0) return;
+    for (int c = 0; c < kWsF; ++c) {
+      const double rms = std::sqrt(sum[c] / cnt);
+      blob[kP_FS + c] = rms > 0.0 ? float(std::min(std::max(1.0 / rms, 1e-4), 1e4)) : 1.f;
+    }
+    const double yr = std::sqrt(sum[kWsF] / (3.0 * cnt));
+    blob[kP_YS] = yr > 0.0 && std::isfinite(yr) ? float(yr) : 1.f;
+    set_params(blob.data());
   }
   void adam(float lr) {
     ++adam_t;
@@ -301,13 +349,14 @@ struct BoneSdfState {
 struct WarmStart {
   Mlp net;
   bool ready = false;  // buffers allocated
+  bool normalized = false;  // the network's normalizer is set (fitted or loaded)
   bool on = false;
   uint32_t k = 1;
   float res_thresh = 0.f;
+  float res_ratio = 0.f;  // > 0: threshold = res_ratio x residual of the predicted positions
   DBuf<float4> ppred, dprev;
-  DBuf<__nv_bfloat16> feat;
-  DBuf<float> adj_rest, res_max, res_part;
-  DBuf<unsigned int> fallbacks;
+  DBuf<float> adj_rest, res_max, res_part, res_pred;
+  DBuf<unsigned int> fallbacks, gate;
   uint64_t substeps_run = 0;
   // recording
   uint32_t rec_cap = 0, rec_count = 0, rec_every = 1, rec_phase = 0;
@@ -1103,11 +1152,11 @@ struct Sim {
   void ws_setup() {
     if (ws.ready) return;
     ws.net.setup(st, n, adj_off.p, adj_idx.p);
+    ws.net.set_ell(m.adj_off.data(), m.adj_idx.data());
     const std::vector<float> blob = Mlp::init_blob(1);
     ws.net.set_params(blob.data());
     ws.ppred.alloc(n);
     ws.dprev.alloc(n);
-    ws.feat.alloc(size_t(n) * kWsF);
     std::vector<float> rest(m.adj_idx.size());
     for (uint32_t i = 0; i < n; ++i)
       for (uint32_t q = m.adj_off[i]; q < m.adj_off[i + 1]; ++q) {
@@ -1120,6 +1169,8 @@ struct Sim {
     ws.res_max.alloc(1);
     ws.res_part.alloc(size_t(num_sms) * std::max(persist_max_per_sm, 4u));
     ws.fallbacks.alloc(1);
+    ws.gate.alloc(1);
+    ws.res_pred.alloc(1);
     TC_CK(cudaMemsetAsync(ws.dprev.p, 0, size_t(n) * sizeof(float4), st));
     TC_CK(cudaMemsetAsync(ws.res_max.p, 0, sizeof(float), st));
     TC_CK(cudaMemsetAsync(ws.fallbacks.p, 0, sizeof(unsigned int), st));
@@ -1140,39 +1191,130 @@ struct Sim {
   }
   bool ws_recording() const { return ws.ready && ws.rec_count < ws.rec_cap; }
   // One frame with the warm start: per substep predict, features, MLP, move
-  // p by the predicted correction, then one persistent launch of iters - k
-  // iterations that judges the max residual against the plain solver's and
-  // runs k more when it misses.
+  // p by the predicted correction, then iters - k iterations, the RMS
+  // residual judged against the plain solver's, and k more iterations when
+  // it misses.  The solver part is one persistent launch per substep, or, in
+  // the per-colour launch mode, the per-colour kernels with the residual
+  // check on the device and the fallback iterations gated by its flag.
   void encode_frame_ws(float dt, uint32_t substeps, bool use_coupled) {
     const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
     const uint32_t itn = run_iters();
     const uint32_t kk = std::min(ws.k, itn > 1 ? itn - 1 : 0u);
-    const WsFeatArgs fa = ws_feat_args(sp, ws.feat.p);
+    const WsFeatArgs fa = ws_feat_args(sp, nullptr);
+    const bool colors = !persistent || cluster_mode;
     for (uint32_t s = 0; s < substeps; ++s) {
-      timed("predict", [&] { k_predict<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp); });
-      timed("ws_mlp", [&] {
-        k_copy4<<<grid(n, 256), 256, 0, st>>>(n, p4.p, ws.ppred.p);
-        k_ws_features<<<grid(n, 128), 128, 0, st>>>(fa);
-        ws.net.infer(ws.feat.p, nullptr, x4.p, p4.p, local_len.p);
-      });
-      SolverArgs a = solver_args(sp, 1, use_coupled, !self_collision);
-      a.skip_predict = true;
-      a.iters = itn - kk;
-      a.iters_extra = kk;
-      a.ppred = ws.ppred.p;
-      a.dprev = ws.dprev.p;
-      a.res_thresh = ws.res_thresh;
-      a.res_part = ws.res_part.p;
-      a.res_out = ws.res_max.p;
-      a.fallbacks = ws.fallbacks.p;
-      timed("solver", [&] { launch_persistent(a); });
+      if (colors) {
+        encode_substep_ws_colors(sp, use_coupled, itn, kk, fa);
+      } else {
+        timed("predict", [&] { k_predict<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp); });
+        SolverArgs a = solver_args(sp, 1, use_coupled, !self_collision);
+        timed("ws_check", [&] { encode_ws_res_pred(sp.dt, a.ca.bone.nbones > 0); });
+        timed("ws_mlp", [&] { ws.net.infer(nullptr, &fa, ws.ppred.p, nullptr, x4.p, p4.p, local_len.p); });
+        a.skip_predict = true;
+        a.iters = itn - kk;
+        a.iters_extra = kk;
+        a.ppred = ws.ppred.p;
+        a.dprev = ws.dprev.p;
+        a.res_thresh = ws.res_thresh;
+        a.res_ratio = ws.res_ratio;
+        a.res_floor = ws_res_floor();
+        a.res_pred = ws.res_pred.p;
+        a.res_part = ws.res_part.p;
+        a.res_out = ws.res_max.p;
+        a.fallbacks = ws.fallbacks.p;
+        timed("solver", [&] { launch_persistent(a); });
+      }
       if (self_collision) {
         if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
-        timed("update_vel", [&] { k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp.dt); });
+        timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp.dt); });
+      } else if (colors) {
+        timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp.dt); });
       }
     }
     TC_CK(cudaMemcpyAsync(h_err, &bar.p->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaGetLastError());
+  }
+  WsCheckArgs ws_check_args(float dts) {
+    return WsCheckArgs{nd, nb, dist_ids.p, dist_par.p, bend_ids.p, bend_par.p, p4.p, dlam.p, blam.p, dts,
+                       ws.res_thresh, ws.res_ratio, ws_res_floor(), ws.res_pred.p, ws.res_part.p, ws.res_max.p,
+                       ws.fallbacks.p, ws.gate.p};
+  }
+  // floor of a relative threshold: a strain of 1e-6 of the mean edge length
+  // (a rigidly moving cloth has a zero predicted residual)
+  float ws_res_floor() const { return 1e-6f * ad.mesh_avg_edge_len;
+  }
+  // with a relative threshold: the residual of the predicted positions
+  // (before the network moves them), lambdas read as zero
+  void encode_ws_res_pred(float dts, bool bone_col) {
+    if (ws.res_ratio <= 0.f) return;
+    WsCheckArgs c = ws_check_args(dts);
+    c.dlam = nullptr;
+    c.blam = nullptr;
+    const unsigned parts = persist_grid(bone_col);
+    launch_k(k_ws_res_part, parts, 256, c);
+    launch_k(k_ws_res_pred, 1, 32, c, uint32_t(parts));
+  }
+  // The constraint phase of one warm-started substep with per-colour
+  // launches (the order of k_solver_persistent: clear lambdas, predict, the
+  // network, iterations, check, gated iterations, the correction for the
+  // next substep's features, decoupled collision, final pins).
+  void encode_substep_ws_colors(const SubstepParams& sp, bool use_coupled, uint32_t itn, uint32_t kk,
+                                const WsFeatArgs& fa) {
+    const float dts = sp.dt;
+    const bool ddamp = td != 0.f || cd != 0.f || sd != 0.f;
+    const bool bdamp = bd != 0.f;
+    const bool hascol = has_colliders();
+    const uint32_t npins = uint32_t(pins.size());
+    const ColliderArgs ca = collider_args();
+    const bool bone_col = ca.bone.nbones > 0;
+    if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
+    if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
+    timed("predict", [&] { launch_k(k_predict, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp); });
+    timed("ws_check", [&] { encode_ws_res_pred(dts, bone_col); });
+    timed("ws_mlp", [&] { ws.net.infer(nullptr, &fa, ws.ppred.p, nullptr, x4.p, p4.p, local_len.p); });
+    auto iteration = [&](const unsigned int* gate) {
+      if (npins) {
+        if (gate) launch_k(k_pin_gated, grid(npins, 128), 128, gate, npins, pin_v.p, pin_t.p, x4.p, p4.p, dts);
+        else launch_k(k_pin, grid(npins, 128), 128, npins, pin_v.p, pin_t.p, x4.p, p4.p, dts);
+      }
+      for (size_t c = 0; c < m.dist_cnt.size(); ++c)
+        if (m.dist_cnt[c]) {
+          if (gate)
+            launch_k(k_distance_gated, grid(m.dist_cnt[c], 256), 256, gate, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
+                     dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
+          else
+            launch_k(k_distance, grid(m.dist_cnt[c], 256), 256, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
+                     dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
+        }
+      for (size_t c = 0; c < m.bend_cnt.size(); ++c)
+        if (m.bend_cnt[c]) {
+          if (gate)
+            launch_k(k_bending_gated, grid(m.bend_cnt[c], 256), 256, gate, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
+                     bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
+          else
+            launch_k(k_bending, grid(m.bend_cnt[c], 256), 256, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
+                     bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
+        }
+      if (hascol && use_coupled) {
+        if (!gate) launch_collision(ca, dts);
+        else if (bone_col) launch_k(k_collision_gated<true>, grid(n, 128), 128, gate, n, x4.p, p4.p, ca, dts);
+        else launch_k(k_collision_gated<false>, grid(n, 128), 128, gate, n, x4.p, p4.p, ca, dts);
+      }
+    };
+    timed("solver", [&] {
+      for (uint32_t it = 0; it < itn - kk; ++it) iteration(nullptr);
+      if (kk) {
+        const WsCheckArgs c = ws_check_args(dts);
+        const unsigned parts = persist_grid(bone_col);
+        launch_k(k_ws_res_part, parts, 256, c);
+        launch_k(k_ws_res_decide, 1, 32, c, uint32_t(parts));
+        for (uint32_t it = 0; it < kk; ++it) iteration(ws.gate.p);
+      }
+      k_ws_correction<<<grid(n, 256), 256, 0, st>>>(n, p4.p, ws.ppred.p, x4.p, local_len.p, ws.dprev.p, nullptr,
+                                                    nullptr);
+      if (hascol && !use_coupled) launch_collision(ca, dts);
+      if (npins) launch_k(k_pin, grid(npins, 128), 128, npins, pin_v.p, pin_t.p, x4.p, p4.p, dts);
+    });
   }
   // train on the recorded snapshots: epochs x snapshots Adam steps in a
   // seeded shuffled order; returns the mean loss of the first and last epoch
@@ -1181,6 +1323,10 @@ struct Sim {
     if (epochs == 0) throw TcError(TC_ERR_INVALID, "epochs must be positive");
     const uint32_t cnt = ws.rec_count;
     ws.net.alloc_train();
+    if (!ws.normalized) {
+      ws.net.fit_normalizer(ws.rec_feat.p, ws.rec_target.p, ws.rec_mask.p, size_t(cnt) * n);
+      ws.normalized = true;
+    }
     ws.losses.alloc(size_t(epochs) * cnt);
     TC_CK(cudaMemsetAsync(ws.losses.p, 0, size_t(epochs) * cnt * sizeof(float), st));
     std::vector<uint32_t> order(cnt);
@@ -1196,7 +1342,7 @@ struct Sim {
         const __nv_bfloat16* f = ws.rec_feat.p + size_t(sidx) * n * kWsF;
         ws.net.forward(f, true, ws.rec_target.p + size_t(sidx) * n * 3, ws.rec_mask.p + size_t(sidx) * n,
                        ws.losses.p + size_t(ep) * cnt + j);
-        ws.net.backward(f);
+        ws.net.backward();
         ws.net.adam(lr);
       }
     }
@@ -1274,6 +1420,10 @@ struct Sim {
       if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
       if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
       timed("predict", [&] { launch_k(k_predict, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp); });
+      if (track_residual && s + 1 == substeps && nd + nb)
+        k_residual_pred<<<grid(nd + nb, 256), 256, 0, st>>>(nd, nb, dist_ids.p, dist_par.p, bend_ids.p, bend_par.p,
+                                                           p4.p, fmaxf(dts, 1e-8f),
+                                                           res_sum.p + m.dist_cnt.size() + m.bend_cnt.size());
       // recording for the warm start: features after predict, the
       // iterations' correction as the target
       const bool rec = ws_recording();
@@ -2060,6 +2210,17 @@ tc_status tc_get_residuals(tc_sim* s, float* drms, float* dmax, float* brms, flo
       totals[2] = m.nb ? float(std::sqrt(bs / m.nb)) : 0.f;
       totals[3] = bm;
     }
+  });
+}
+tc_status tc_get_predicted_residual(tc_sim* s, float* rms) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(rms != nullptr, "rms required");
+    float sum = 0.f;
+    TC_CK(cudaMemcpyAsync(&sum, m.res_sum.p + m.m.dist_cnt.size() + m.m.bend_cnt.size(), sizeof(float),
+                          cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    *rms = m.nd + m.nb ? float(std::sqrt(double(sum) / double(m.nd + m.nb))) : 0.f;
   });
 }
 struct tc_mesh {
@@ -2957,6 +3118,16 @@ tc_status tc_ws_set_params(tc_sim* s, const float* params, size_t len) {
     for (size_t i = 0; i < len; ++i) need(std::isfinite(params[i]), "params must be finite");
     m.ws_setup();
     m.ws.net.set_params(params);
+    m.ws.normalized = true;
+  });
+}
+
+tc_status tc_ws_set_relative_threshold(tc_sim* s, float ratio) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(std::isfinite(ratio) && ratio >= 0.f, "ratio must be finite and non-negative");
+    m.ws.res_ratio = ratio;
+    m.mark();
   });
 }
 
@@ -2965,16 +3136,17 @@ tc_status tc_ws_stats(tc_sim* s, double out[4]) {
     Sim& m = S(s);
     need(out != nullptr, "out required");
     unsigned int fb = 0;
-    float rm = 0.f;
+    float rm = 0.f, rp = 0.f;
     if (m.ws.ready) {
       TC_CK(cudaMemcpyAsync(&fb, m.ws.fallbacks.p, sizeof fb, cudaMemcpyDeviceToHost, m.st));
       TC_CK(cudaMemcpyAsync(&rm, m.ws.res_max.p, sizeof rm, cudaMemcpyDeviceToHost, m.st));
+      TC_CK(cudaMemcpyAsync(&rp, m.ws.res_pred.p, sizeof rp, cudaMemcpyDeviceToHost, m.st));
       TC_CK(cudaStreamSynchronize(m.st));
     }
     out[0] = double(m.ws.substeps_run);
     out[1] = double(fb);
     out[2] = double(rm);
-    out[3] = double(m.ws.res_thresh);
+    out[3] = m.ws.res_ratio > 0.f ? double(std::fmax(m.ws.res_ratio * rp, m.ws_res_floor())) : double(m.ws.res_thresh);
   });
 }
 
@@ -3017,17 +3189,18 @@ tc_status tc_mlp_grad(uint32_t n, const float* feat, const uint32_t* adj_off, co
     TC_CK(cudaMemsetAsync(d_loss.p, 0, sizeof(float), st));
     tcloth::Mlp net;
     net.setup(st, n, d_off.p, d_idx.p);
+    net.set_ell(adj_off, adj_idx);
     net.alloc_train();
     net.set_params(params);
     net.forward(d_f.p, true, d_t.p, d_m.p, d_loss.p);
-    net.backward(d_f.p);
+    net.backward();
     TC_CK(cudaMemcpyAsync(loss, d_loss.p, sizeof(float), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaMemcpyAsync(grads, net.gw.p, tcloth::kP_N * sizeof(float), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaMemcpyAsync(y, net.y.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
     if (y_infer) {
       tcloth::DBuf<float> d_yi;
       d_yi.alloc(size_t(n) * 3);
-      net.infer(d_f.p, d_yi.p, nullptr, nullptr, nullptr);
+      net.infer(d_f.p, nullptr, nullptr, d_yi.p, nullptr, nullptr, nullptr);
       TC_CK(cudaMemcpyAsync(y_infer, d_yi.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
       TC_CK(cudaStreamSynchronize(st));
     }

@@ -538,6 +538,9 @@ struct SolverArgs {
   float4* dprev;
   uint32_t iters_extra;
   float res_thresh;
+  float res_ratio;            // > 0: the threshold is max(res_ratio * *res_pred, res_floor) instead
+  float res_floor;
+  const float* res_pred;      // RMS residual of the predicted positions (lambda = 0)
   float* res_part;            // [gridDim.x] per-block sums of squares
   float* res_out;             // RMS of the latest check
   unsigned int* fallbacks;    // count of substeps that ran the extra iterations
@@ -549,7 +552,7 @@ __device__ __forceinline__ float residual_dist(uint32_t ci, const uint2* ids, co
   const float4 c = par[ci];
   const float cv = length(mk(__ldcg(p4 + e.x)) - mk(__ldcg(p4 + e.y))) - c.x;
   const float comp = cv >= 0.f ? c.y : c.z;
-  return comp < 1e9f ? fabsf(cv + comp / (dt * dt) * __ldcg(lam + ci)) : 0.f;
+  return comp < 1e9f ? fabsf(cv + comp / (dt * dt) * (lam ? __ldcg(lam + ci) : 0.f)) : 0.f;
 }
 __device__ __forceinline__ float residual_bend(uint32_t ci, const uint4* ids, const float4* par, const float4* p4,
                                                const float* lam, float dt) {
@@ -557,7 +560,137 @@ __device__ __forceinline__ float residual_bend(uint32_t ci, const uint4* ids, co
   const float4 c = par[ci];
   if (c.y >= 1e9f) return 0.f;
   const float cv = length(mk(__ldcg(p4 + e.z)) - mk(__ldcg(p4 + e.w))) - c.x;
-  return fabsf(cv + c.y / (dt * dt) * __ldcg(lam + ci));
+  return fabsf(cv + c.y / (dt * dt) * (lam ? __ldcg(lam + ci) : 0.f));
+}
+
+// Sum of the squared residuals of this thread's grid-stride share of the
+// distance and bending constraints, reduced over the block (red: 8 floats of
+// shared memory); the block's sum is returned on thread 0.  The per-colour
+// check and the persistent solver share this and ws_total_residual, so that
+// with the same grid both take the same decision bit for bit.
+__device__ __forceinline__ float ws_block_residual(uint32_t tid, uint32_t stride, uint32_t nd, uint32_t nb,
+                                                   const uint2* dist_ids, const float4* dist_par,
+                                                   const uint4* bend_ids, const float4* bend_par, const float4* p4,
+                                                   const float* dlam, const float* blam, float dt, float* red) {
+  float r2 = 0.f;
+  for (uint32_t k = tid; k < nd; k += stride) {
+    const float r = residual_dist(k, dist_ids, dist_par, p4, dlam, dt);
+    r2 += r * r;
+  }
+  for (uint32_t k = tid; k < nb; k += stride) {
+    const float r = residual_bend(k, bend_ids, bend_par, p4, blam, dt);
+    r2 += r * r;
+  }
+  for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+  __syncthreads();
+  float b = 0.f;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) b += red[w];
+  return b;
+}
+// RMS over all constraints from the per-block sums (called by one full
+// warp; the result is valid on lane 0)
+__device__ __forceinline__ float ws_total_residual(const float* res_part, uint32_t nparts, uint32_t ncons) {
+  float t = 0.f;
+  for (uint32_t q = threadIdx.x; q < nparts; q += 32) t += __ldcg(res_part + q);
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  return sqrtf(t / float(max(ncons, 1u)));
+}
+
+// Residual check of a warm-started substep in the per-colour path: block
+// sums (launched with the persistent solver's grid), then one warp decides
+// and sets *gate, which the fallback iterations' kernels read.
+struct WsCheckArgs {
+  uint32_t nd, nb;
+  const uint2* dist_ids;
+  const float4* dist_par;
+  const uint4* bend_ids;
+  const float4* bend_par;
+  const float4* p4;
+  const float* dlam;
+  const float* blam;
+  float dt, res_thresh;
+  float res_ratio;         // > 0: the threshold is max(res_ratio * *res_pred, res_floor)
+  float res_floor;
+  float* res_pred;         // RMS residual of the predicted positions
+  float* res_part;
+  float* res_out;
+  unsigned int* fallbacks;
+  unsigned int* gate;
+};
+__global__ void __launch_bounds__(256) k_ws_res_part(WsCheckArgs a) {
+  pdl_enter();
+  __shared__ float red[8];
+  const float b = ws_block_residual(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, a.nd, a.nb,
+                                    a.dist_ids, a.dist_par, a.bend_ids, a.bend_par, a.p4, a.dlam, a.blam,
+                                    fmaxf(a.dt, 1e-8f), red);
+  if (threadIdx.x == 0) a.res_part[blockIdx.x] = b;
+}
+__global__ void k_ws_res_decide(WsCheckArgs a, uint32_t nparts) {
+  pdl_enter();
+  const float rms = ws_total_residual(a.res_part, nparts, a.nd + a.nb);
+  if (threadIdx.x == 0) {
+    const float thr = a.res_ratio > 0.f ? fmaxf(a.res_ratio * *a.res_pred, a.res_floor) : a.res_thresh;
+    const unsigned int extra = rms > thr ? 1u : 0u;
+    *a.res_out = rms;
+    *a.gate = extra;
+    if (extra) *a.fallbacks += 1u;
+  }
+}
+// RMS residual of the predicted positions (block sums of k_ws_res_part
+// launched with null lambdas): the reference level of a relative threshold
+__global__ void k_ws_res_pred(WsCheckArgs a, uint32_t nparts) {
+  pdl_enter();
+  const float rms = ws_total_residual(a.res_part, nparts, a.nd + a.nb);
+  if (threadIdx.x == 0) *a.res_pred = rms;
+}
+// Sum of squared residuals of the predicted positions (lambda = 0) into
+// *sum, for residual tracking
+__global__ void k_residual_pred(uint32_t nd, uint32_t nb, const uint2* dist_ids, const float4* dist_par,
+                                const uint4* bend_ids, const float4* bend_par, const float4* p4, float dt,
+                                float* sum) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  float r = 0.f;
+  if (k < nd) r = residual_dist(k, dist_ids, dist_par, p4, nullptr, dt);
+  else if (k < nd + nb) r = residual_bend(k - nd, bend_ids, bend_par, p4, nullptr, dt);
+  float s2 = r * r;
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_down_sync(0xffffffffu, s2, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(sum, s2);
+}
+// The fallback iterations of the per-colour path: the element functions of
+// k_pin / k_distance / k_bending / k_collision, skipped unless *gate is set.
+__global__ void k_pin_gated(const unsigned int* gate, uint32_t npins, const uint32_t* __restrict__ pin_v,
+                            const float4* __restrict__ pin_t, const float4* __restrict__ x4, float4* __restrict__ p4,
+                            float dt_sub) {
+  pdl_enter();
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npins || !*gate) return;
+  pin_one<false>(k, pin_v, pin_t, x4, p4, dt_sub);
+}
+__global__ void k_distance_gated(const unsigned int* gate, uint32_t off, uint32_t cnt, const uint2* __restrict__ ids,
+                                 const float4* __restrict__ par, float4* __restrict__ x4, float4* __restrict__ p4,
+                                 float* __restrict__ lam, SubstepParams sp, bool damped) {
+  pdl_enter();
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cnt || !*gate) return;
+  project_distance<false>(off + k, ids, par, x4, p4, lam, sp, damped);
+}
+__global__ void k_bending_gated(const unsigned int* gate, uint32_t off, uint32_t cnt, const uint4* __restrict__ ids,
+                                const float4* __restrict__ par, float4* __restrict__ x4, float4* __restrict__ p4,
+                                float* __restrict__ lam, SubstepParams sp, bool damped) {
+  pdl_enter();
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cnt || !*gate) return;
+  project_bending<false>(off + k, ids, par, x4, p4, lam, sp, damped);
+}
+template <bool kBone>
+__global__ void k_collision_gated(const unsigned int* gate, uint32_t n, float4* __restrict__ x4,
+                                  float4* __restrict__ p4, ColliderArgs ca, float dt) {
+  pdl_enter();
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !*gate) return;
+  collide_vertex<false, kBone>(i, x4, p4, ca, dt);
 }
 
 // One cooperative launch runs `nsub` substeps of the constraint phase
@@ -604,32 +737,15 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
       if (it + 1 == a.iters && a.iters_extra > 0) {
         __shared__ float red[8];
         __shared__ int extra;
-        const float dt = fmaxf(dts, 1e-8f);
-        float r2 = 0.f;
-        for (uint32_t k = tid; k < a.nd; k += stride) {
-          const float r = residual_dist(k, a.dist_ids, a.dist_par, a.p4, a.dlam, dt);
-          r2 += r * r;
-        }
-        for (uint32_t k = tid; k < a.nb; k += stride) {
-          const float r = residual_bend(k, a.bend_ids, a.bend_par, a.p4, a.blam, dt);
-          r2 += r * r;
-        }
-        for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          float b = 0.f;
-          for (int w = 0; w < int(blockDim.x >> 5); ++w) b += red[w];
-          __stcg(a.res_part + blockIdx.x, b);
-        }
+        const float b = ws_block_residual(tid, stride, a.nd, a.nb, a.dist_ids, a.dist_par, a.bend_ids, a.bend_par,
+                                          a.p4, a.dlam, a.blam, fmaxf(dts, 1e-8f), red);
+        if (threadIdx.x == 0) __stcg(a.res_part + blockIdx.x, b);
         if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
         if (threadIdx.x < 32) {
-          float t = 0.f;
-          for (uint32_t q = threadIdx.x; q < gridDim.x; q += 32) t += __ldcg(a.res_part + q);
-          for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+          const float rms = ws_total_residual(a.res_part, gridDim.x, a.nd + a.nb);
           if (threadIdx.x == 0) {
-            const float rms = sqrtf(t / float(max(a.nd + a.nb, 1u)));
-            extra = rms > a.res_thresh ? 1 : 0;
+            const float thr = a.res_ratio > 0.f ? fmaxf(a.res_ratio * __ldcg(a.res_pred), a.res_floor) : a.res_thresh;
+            extra = rms > thr ? 1 : 0;
             if (blockIdx.x == 0) {
               *a.res_out = rms;
               if (extra) atomicAdd(a.fallbacks, 1u);

@@ -25,13 +25,19 @@ constexpr int kWsF = 16;   // input features
 constexpr int kWsH = 64;   // hidden width
 constexpr int kWsRows = 64;  // vertices per block tile (4 warps x 16 rows)
 
-// fp32 parameter blob: weights row-major [in][out], then the bias
+// fp32 parameter blob: weights row-major [in][out], then the bias; then the
+// normalizer, which training does not change (its gradient is zero): the
+// per-feature input scales FS[16] and the output scale YS (features enter
+// layer 0 as bf16(feature * FS); the network predicts correction / (L YS))
 constexpr uint32_t kP_W0 = 0, kP_b0 = 1024, kP_W1 = 1088, kP_b1 = 9280, kP_W2 = 9344, kP_b2 = 17536,
-                   kP_W3 = 17600, kP_b3 = 17792, kP_N = 17795;
+                   kP_W3 = 17600, kP_b3 = 17792, kP_FS = 17795, kP_YS = 17811, kP_N = 17812;
 // transposed bf16 copies [out][in] of W0..W2 for the forward GEMM's B operand
 constexpr uint32_t kT_W0 = 0, kT_W1 = 1024, kT_W2 = 9216, kT_N = 17408;
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
+// SiLU with the fast exponential and division intrinsics (the activation is
+// rounded to bf16 next, which absorbs their few-ulp error); z below about
+// -88 gives an infinite exponential and a zero quotient.
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
   const float s = 1.0f / (1.0f + expf(-z));
   return s * (1.0f + z * (1.0f - s));
@@ -87,6 +93,7 @@ struct MlpLayerArgs {
   uint32_t n;
   int kin;                      // 16 (layer 0) or 128 (message-passing layers)
   const __nv_bfloat16* x_feat;  // layer 0 input [n][16]
+  const float* fscale;          // layer 0: per-feature scales [16], or null
   const __nv_bfloat16* h_prev;  // rounds: previous hidden [n][64]
   const uint32_t* adj_off;
   const uint32_t* adj_idx;
@@ -94,16 +101,13 @@ struct MlpLayerArgs {
   const float* bias;            // [64]
   __nv_bfloat16* x_out;         // optional: the assembled input [n][kin] (training)
   float* z_out;                 // optional: pre-activations [n][64] (training)
-  __nv_bfloat16* h_out;         // [n][64], or null when the head is fused
-  // fused head (inference, last layer): Y = H W3 + b3, then p += Y L on
-  // free vertices (x4.w > 0) when p4 is given, else Y to y_out
-  const __nv_bfloat16* w3;      // [64][3] or null
-  const float* b3;
-  float* y_out;
-  const float4* x4;
-  float4* p4;
-  const float* local_len;
+  __nv_bfloat16* h_out;         // [n][64]
 };
+
+__device__ __forceinline__ float out_scale(const float* ys) {
+  const float v = ys ? *ys : 1.f;
+  return v > 0.f ? v : 1.f;
+}
 
 __device__ __forceinline__ void bf16x8_to_f32(const uint4 u, float f[8]) {
   const uint32_t w[4] = {u.x, u.y, u.z, u.w};
@@ -136,8 +140,15 @@ __global__ void __launch_bounds__(kWsFwdThreads) k_mlp_layer_fwd(MlpLayerArgs a)
     for (int e = tid; e < kWsRows * 2; e += blockDim.x) {
       const int r = e >> 1, c = (e & 1) * 8;
       const uint32_t v = row0 + r;
-      *reinterpret_cast<uint4*>(&xs[r][c]) =
-          v < a.n ? __ldg(reinterpret_cast<const uint4*>(a.x_feat + size_t(v) * kWsF + c)) : make_uint4(0, 0, 0, 0);
+      uint4 u = v < a.n ? __ldg(reinterpret_cast<const uint4*>(a.x_feat + size_t(v) * kWsF + c)) : make_uint4(0, 0, 0, 0);
+      if (a.fscale) {
+        float f[8];
+        bf16x8_to_f32(u, f);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) f[q] *= __ldg(a.fscale + c + q);
+        u = f32_to_bf16x8(f);
+      }
+      *reinterpret_cast<uint4*>(&xs[r][c]) = u;
     }
   } else {
     // self part and neighbour mean; each thread owns (row, 8-column group)
@@ -200,7 +211,6 @@ __global__ void __launch_bounds__(kWsFwdThreads) k_mlp_layer_fwd(MlpLayerArgs a)
     }
   }
   const int g = lane >> 2, t = lane & 3;
-  float y0[3] = {0.f, 0.f, 0.f}, y1[3] = {0.f, 0.f, 0.f};  // fused head partials, rows g and g + 8
   // the epilogue overwrites this warp's own 16 rows of xs only
   __syncwarp();
 #pragma unroll
@@ -211,44 +221,9 @@ __global__ void __launch_bounds__(kWsFwdThreads) k_mlp_layer_fwd(MlpLayerArgs a)
       const uint32_t v = row0 + r;
       const float z = acc[nt][q] + __ldg(a.bias + c);
       if (a.z_out && v < a.n) a.z_out[size_t(v) * kWsH + c] = z;
-      const __nv_bfloat16 h = __float2bfloat16(silu(z));
-      xs[r][c] = h;
-      if (a.w3) {
-        const float hf = __bfloat162float(h);
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const float wv = __bfloat162float(a.w3[c * 3 + j]);
-          if (q >> 1) y1[j] += hf * wv;
-          else y0[j] += hf * wv;
-        }
-      }
+      xs[r][c] = __float2bfloat16(silu(z));
     }
   __syncwarp();
-  if (a.w3) {
-    for (int j = 0; j < 3; ++j) {
-      y0[j] += __shfl_xor_sync(0xffffffffu, y0[j], 1);
-      y0[j] += __shfl_xor_sync(0xffffffffu, y0[j], 2);
-      y1[j] += __shfl_xor_sync(0xffffffffu, y1[j], 1);
-      y1[j] += __shfl_xor_sync(0xffffffffu, y1[j], 2);
-    }
-    if (t < 2) {
-      const uint32_t v = row0 + warp * 16 + g + t * 8;
-      if (v < a.n) {
-        const float Y[3] = {(t ? y1[0] : y0[0]) + a.b3[0], (t ? y1[1] : y0[1]) + a.b3[1],
-                            (t ? y1[2] : y0[2]) + a.b3[2]};
-        if (a.y_out)
-          for (int j = 0; j < 3; ++j) a.y_out[size_t(v) * 3 + j] = Y[j];
-        if (a.p4 && a.x4[v].w > 0.f) {
-          const float L = fmaxf(a.local_len[v], 1e-6f);
-          float4 p = a.p4[v];
-          p.x += Y[0] * L;
-          p.y += Y[1] * L;
-          p.z += Y[2] * L;
-          a.p4[v] = p;
-        }
-      }
-    }
-  }
   if (a.h_out) {
     for (int e = lane; e < 16 * 8; e += 32) {
       const int r = warp * 16 + (e >> 3), c = (e & 7) * 8;
@@ -259,14 +234,15 @@ __global__ void __launch_bounds__(kWsFwdThreads) k_mlp_layer_fwd(MlpLayerArgs a)
 }
 
 // Head: Y = H2 W3 + b3 (fp32 accumulation of bf16 products).  With targets,
-// also dY = 2 (Y - T) m / (3 M) (mean squared error over the M free vertices,
-// mask m) and the loss.
+// also dY = 2 (Y - T / YS) m / (3 n) (mean squared error against the
+// normalised target, mask m of free vertices) and the loss.
 __global__ void k_mlp_head(uint32_t n, const __nv_bfloat16* __restrict__ h2, const __nv_bfloat16* __restrict__ w3,
                            const float* __restrict__ b3, float* __restrict__ y, const float* __restrict__ target,
-                           const float* __restrict__ mask, float inv_count, float* __restrict__ dy,
-                           float* __restrict__ loss) {
+                           const float* __restrict__ mask, const float* __restrict__ yscale, float inv_count,
+                           float* __restrict__ dy, float* __restrict__ loss) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   float l = 0.f;
+  const float ys = out_scale(yscale);
   if (v < n) {
     for (int c = 0; c < 3; ++c) {
       float s = 0.f;
@@ -275,7 +251,7 @@ __global__ void k_mlp_head(uint32_t n, const __nv_bfloat16* __restrict__ h2, con
       y[size_t(v) * 3 + c] = s;
       if (target) {
         const float m = mask ? mask[v] : 1.0f;
-        const float d = (s - target[size_t(v) * 3 + c]) * m;
+        const float d = (s - target[size_t(v) * 3 + c] / ys) * m;
         dy[size_t(v) * 3 + c] = 2.0f * d * inv_count / 3.0f;
         l += d * d;
       }
@@ -432,6 +408,44 @@ __global__ void k_adam(uint32_t cnt, float* __restrict__ w, const float* __restr
   if (wbt) wbt[(e % cols) * rows + e / cols] = __float2bfloat16(nw);
 }
 
+// Normalizer statistics of recorded snapshots: per block, over the rows
+// blockIdx.x, blockIdx.x + gridDim.x, ... of the free vertices (mask), the
+// sums of squares of the 16 features and of the target, and the row count;
+// a fixed grid and fixed reduction order make the result reproducible.
+constexpr int kWsMomBlocks = 296, kWsMom = kWsF + 2;
+__global__ void __launch_bounds__(256) k_ws_moments(size_t rows, const __nv_bfloat16* __restrict__ feat,
+                                                    const float* __restrict__ target, const float* __restrict__ mask,
+                                                    float* __restrict__ part) {
+  float acc[kWsMom];
+#pragma unroll
+  for (int c = 0; c < kWsMom; ++c) acc[c] = 0.f;
+  for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += size_t(gridDim.x) * blockDim.x) {
+    if (mask[r] <= 0.f) continue;
+    float f[8];
+    for (int h = 0; h < 2; ++h) {
+      bf16x8_to_f32(__ldg(reinterpret_cast<const uint4*>(feat + r * kWsF) + h), f);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc[h * 8 + q] += f[q] * f[q];
+    }
+    for (int q = 0; q < 3; ++q) acc[kWsF] += target[r * 3 + q] * target[r * 3 + q];
+    acc[kWsF + 1] += 1.f;
+  }
+  __shared__ float red[8][kWsMom];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < kWsMom; ++c) {
+    float t = acc[c];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) red[warp][c] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < kWsMom) {
+    float t = 0.f;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+    part[size_t(blockIdx.x) * kWsMom + threadIdx.x] = t;
+  }
+}
+
 // bf16 copies of the fp32 master blob (row-major, and transposed W0..W2)
 __global__ void k_ws_refresh(const float* __restrict__ w, __nv_bfloat16* __restrict__ wb,
                              __nv_bfloat16* __restrict__ wbt) {
@@ -491,9 +505,7 @@ __device__ __forceinline__ float prim_sdf(const Prim& c, V3 p, V3& nrm) {
   nrm = B / length(B);
   return dot(p - mk(c.a), nrm);
 }
-__global__ void k_ws_features(WsFeatArgs a) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
+__device__ __forceinline__ void ws_feature_row(const WsFeatArgs& a, uint32_t i, float f[kWsF]) {
   const float4 xi4 = a.x4[i], pi4 = a.p4[i], vi4 = a.v4[i];
   const V3 pi = mk(pi4);
   const float wi = xi4.w;
@@ -524,10 +536,249 @@ __global__ void k_ws_features(WsFeatArgs a) {
     if (k == kb || s < sdf) { sdf = s; n = nk; }
   }
   sdf = clampf(sdf, -4.f, 4.f);
-  float f[kWsF] = {dp.x * invL, dp.y * invL, dp.z * invL, jac.x * invL, jac.y * invL, jac.z * invL, sdf,
-                   n.x, n.y, n.z, vi4.x * a.dt * invL, vi4.y * a.dt * invL, vi4.z * a.dt * invL,
-                   a.g_dt2 * invL, wi > 0.f ? 1.f : 0.f, 1.f};
+  const float g[kWsF] = {dp.x * invL, dp.y * invL, dp.z * invL, jac.x * invL, jac.y * invL, jac.z * invL, sdf,
+                         n.x, n.y, n.z, vi4.x * a.dt * invL, vi4.y * a.dt * invL, vi4.z * a.dt * invL,
+                         a.g_dt2 * invL, wi > 0.f ? 1.f : 0.f, 1.f};
+#pragma unroll
+  for (int c = 0; c < kWsF; ++c) f[c] = g[c];
+}
+// features of every vertex (bf16) for the recorded training snapshots
+__global__ void k_ws_features(WsFeatArgs a) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  float f[kWsF];
+  ws_feature_row(a, i, f);
   for (int c = 0; c < kWsF; ++c) a.feat[size_t(i) * kWsF + c] = __float2bfloat16(f[c]);
+}
+
+// ---------------------------------------------------------------------------
+// Inference kernels.  Same products and rounding points as the training
+// forward (k_mlp_layer_fwd; the fused head sums in another order), organised
+// for throughput on large graphs: layer 0 computes the features in the
+// kernel (and keeps the predicted positions); the message-passing layers run
+// persistent over 64-row tiles with W^T staged in shared memory once per
+// block, all 8 warps on the tensor cores (two per 16 rows, 32 output columns
+// each); each row's neighbour list comes from an ELL table (degree, then the
+// first 15 neighbours in adjacency order; the CSR serves the rest), so the
+// neighbour rows of a vertex are all in flight at once.
+constexpr int kWsEll = 16;
+constexpr int kWsL0Rows = 256;  // layer 0: one vertex per thread
+
+struct MlpInferArgs {
+  uint32_t n;
+  // layer 0
+  const __nv_bfloat16* x_feat;  // given features [n][16], or null: computed from fa
+  WsFeatArgs fa;
+  float4* ppred;                // with computed features: copy of p before the move
+  const float* fscale;
+  // message-passing layers
+  const __nv_bfloat16* h_prev;
+  const uint32_t* ell;          // [n][16]
+  const uint32_t* adj_off;
+  const uint32_t* adj_idx;
+  const __nv_bfloat16* wt;      // W^T [64][kin]
+  const float* bias;
+  __nv_bfloat16* h_out;         // or null with the fused head
+  const __nv_bfloat16* w3;
+  const float* b3;
+  const float* yscale;
+  float* y_out;
+  const float4* x4;
+  float4* p4;
+  const float* local_len;
+};
+
+// Layer 0: X0 = bf16(bf16(features) * FS), H0 = bf16(SiLU(X0 W0 + b0)).
+__global__ void __launch_bounds__(kWsL0Rows) k_mlp_infer_l0(MlpInferArgs a) {
+  __shared__ __align__(16) union {
+    __nv_bfloat16 x[kWsL0Rows][kWsF + 8];
+    __nv_bfloat16 h[kWsL0Rows][kWsH + 8];
+  } sm;
+  __shared__ __align__(16) __nv_bfloat16 wt[kWsH][kWsF + 8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t row0 = blockIdx.x * kWsL0Rows, v = row0 + tid;
+  for (int e = tid; e < kWsH * 2; e += blockDim.x)
+    *reinterpret_cast<uint4*>(&wt[e >> 1][(e & 1) * 8]) = __ldg(reinterpret_cast<const uint4*>(a.wt) + e);
+  float f[kWsF];
+  if (v < a.n) {
+    if (a.x_feat) {
+      bf16x8_to_f32(__ldg(reinterpret_cast<const uint4*>(a.x_feat + size_t(v) * kWsF)), f);
+      bf16x8_to_f32(__ldg(reinterpret_cast<const uint4*>(a.x_feat + size_t(v) * kWsF) + 1), f + 8);
+    } else {
+      ws_feature_row(a.fa, v, f);
+#pragma unroll
+      for (int c = 0; c < kWsF; ++c) f[c] = __bfloat162float(__float2bfloat16(f[c]));
+      a.ppred[v] = a.fa.p4[v];
+    }
+#pragma unroll
+    for (int c = 0; c < kWsF; ++c) f[c] *= __ldg(a.fscale + c);
+  } else {
+#pragma unroll
+    for (int c = 0; c < kWsF; ++c) f[c] = 0.f;
+  }
+  *reinterpret_cast<uint4*>(&sm.x[tid][0]) = f32_to_bf16x8(f);
+  *reinterpret_cast<uint4*>(&sm.x[tid][8]) = f32_to_bf16x8(f + 8);
+  __syncthreads();
+  // each warp: rows warp*32 .. +31, two 16-row tiles, one k step
+  uint32_t af[2][4];
+  load_a_frag(af[0], &sm.x[0][0], kWsF + 8, warp * 32, 0, lane);
+  load_a_frag(af[1], &sm.x[0][0], kWsF + 8, warp * 32 + 16, 0, lane);
+  __syncthreads();  // sm.x is overwritten by the outputs below
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      float acc[4] = {0.f, 0.f, 0.f, 0.f};
+      uint32_t bf[2];
+      load_b_frag(bf, &wt[0][0], kWsF + 8, nt * 8, 0, lane);
+      mma_bf16_16816(acc, af[mt], bf);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = warp * 32 + mt * 16 + g + (q >> 1) * 8, c = nt * 8 + 2 * t + (q & 1);
+        sm.h[r][c] = __float2bfloat16(silu(acc[q] + __ldg(a.bias + c)));
+      }
+    }
+  __syncthreads();
+  for (int e = tid; e < kWsL0Rows * 8; e += blockDim.x) {
+    const int r = e >> 3, c = (e & 7) * 8;
+    if (row0 + r < a.n)
+      *reinterpret_cast<uint4*>(a.h_out + size_t(row0 + r) * kWsH + c) = *reinterpret_cast<const uint4*>(&sm.h[r][c]);
+  }
+}
+
+// Message-passing layer: X = [H_i, bf16(mean_j H_j)], H' = bf16(SiLU(X W + b)),
+// or with w3 the head Y = H' W3 + b3 and p += Y YS L on free vertices.
+__global__ void __launch_bounds__(256, 3) k_mlp_infer_mp(MlpInferArgs a) {
+  __shared__ __align__(16) __nv_bfloat16 xs[kWsRows][128 + 8];
+  __shared__ __align__(16) __nv_bfloat16 ws[kWsH][128 + 8];
+  __shared__ float ypart[2][kWsRows][3];  // fused head: partial sums of the two column halves
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < kWsH * 16; e += blockDim.x)
+    *reinterpret_cast<uint4*>(&ws[e >> 4][(e & 15) * 8]) = __ldg(reinterpret_cast<const uint4*>(a.wt) + e);
+  const uint32_t ntiles = (a.n + kWsRows - 1) / kWsRows;
+  auto row = [&](uint32_t j, int cg) { return __ldg(reinterpret_cast<const uint4*>(a.h_prev + size_t(j) * kWsH + cg)); };
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint32_t row0 = tile * kWsRows;
+#pragma unroll 1
+    for (int m = 0; m < 2; ++m) {
+      const int r = (tid >> 3) + 32 * m, cg = (tid & 7) * 8;
+      const uint32_t v = row0 + r;
+      uint4 self = make_uint4(0, 0, 0, 0), mean = make_uint4(0, 0, 0, 0);
+      if (v < a.n) {
+        self = row(v, cg);
+        const uint4* er = reinterpret_cast<const uint4*>(a.ell + size_t(v) * kWsEll);
+        const uint4 e0 = __ldg(er), e1 = __ldg(er + 1), e2 = __ldg(er + 2), e3 = __ldg(er + 3);
+        const uint32_t idx[15] = {e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w, e2.x,
+                                  e2.y, e2.z, e2.w, e3.x, e3.y, e3.z, e3.w};
+        const uint32_t deg = e0.x, d1 = min(deg, 15u);
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        auto add = [&](const uint4 u) {
+          float fv[8];
+          bf16x8_to_f32(u, fv);
+#pragma unroll
+          for (int c = 0; c < 8; ++c) acc[c] += fv[c];
+        };
+#pragma unroll
+        for (int q0 = 0; q0 < 15; q0 += 8) {
+          if (uint32_t(q0) >= d1) break;
+          uint4 u[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            if (q0 + k < 15 && uint32_t(q0 + k) < d1) u[k] = row(idx[q0 + k], cg);
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            if (q0 + k < 15 && uint32_t(q0 + k) < d1) add(u[k]);
+        }
+        if (deg > 15u) {
+          const uint32_t b = __ldg(a.adj_off + v), en = __ldg(a.adj_off + v + 1);
+          for (uint32_t q = b + 15u; q < en; ++q) add(row(__ldg(a.adj_idx + q), cg));
+        }
+        const float inv = deg ? 1.0f / float(deg) : 0.0f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[c] *= inv;
+        mean = f32_to_bf16x8(acc);
+      }
+      *reinterpret_cast<uint4*>(&xs[r][cg]) = self;
+      *reinterpret_cast<uint4*>(&xs[r][kWsH + cg]) = mean;
+    }
+    __syncthreads();
+    // warp w: rows (w % 4) * 16 .. +15, output columns (w / 4) * 32 .. +31
+    const int wr = (warp & 3) * 16, wn = (warp >> 2) * 4;
+    float acc[4][4];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
+#pragma unroll
+    for (int k0 = 0; k0 < 128; k0 += 16) {
+      uint32_t af[4];
+      load_a_frag(af, &xs[0][0], 128 + 8, wr, k0, lane);
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        uint32_t bf[2];
+        load_b_frag(bf, &ws[0][0], 128 + 8, (wn + nt) * 8, k0, lane);
+        mma_bf16_16816(acc[nt], af, bf);
+      }
+    }
+    __syncthreads();  // every warp has read its input rows before any output is written over them
+    const int g = lane >> 2, t = lane & 3;
+    float y0[3] = {0.f, 0.f, 0.f}, y1[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = wr + g + (q >> 1) * 8, c = (wn + nt) * 8 + 2 * t + (q & 1);
+        const __nv_bfloat16 h = __float2bfloat16(silu(acc[nt][q] + __ldg(a.bias + c)));
+        xs[r][c] = h;
+        if (a.w3) {
+          const float hf = __bfloat162float(h);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const float wv = __bfloat162float(a.w3[c * 3 + j]);
+            if (q >> 1) y1[j] += hf * wv;
+            else y0[j] += hf * wv;
+          }
+        }
+      }
+    if (a.w3) {
+      for (int j = 0; j < 3; ++j) {
+        y0[j] += __shfl_xor_sync(0xffffffffu, y0[j], 1);
+        y0[j] += __shfl_xor_sync(0xffffffffu, y0[j], 2);
+        y1[j] += __shfl_xor_sync(0xffffffffu, y1[j], 1);
+        y1[j] += __shfl_xor_sync(0xffffffffu, y1[j], 2);
+      }
+      if (t < 2)
+        for (int j = 0; j < 3; ++j) ypart[warp >> 2][wr + g + t * 8][j] = t ? y1[j] : y0[j];
+      __syncthreads();
+      if (tid < kWsRows) {
+        const uint32_t v = row0 + tid;
+        if (v < a.n) {
+          const float Y[3] = {ypart[0][tid][0] + ypart[1][tid][0] + a.b3[0],
+                              ypart[0][tid][1] + ypart[1][tid][1] + a.b3[1],
+                              ypart[0][tid][2] + ypart[1][tid][2] + a.b3[2]};
+          if (a.y_out)
+            for (int j = 0; j < 3; ++j) a.y_out[size_t(v) * 3 + j] = Y[j];
+          if (a.p4 && a.x4[v].w > 0.f) {
+            const float L = fmaxf(a.local_len[v], 1e-6f), ys = out_scale(a.yscale);
+            float4 p = a.p4[v];
+            p.x += Y[0] * ys * L;
+            p.y += Y[1] * ys * L;
+            p.z += Y[2] * ys * L;
+            a.p4[v] = p;
+          }
+        }
+      }
+    } else {
+      __syncthreads();
+      for (int e = tid; e < kWsRows * 8; e += blockDim.x) {
+        const int r = e >> 3, c = (e & 7) * 8;
+        if (row0 + r < a.n)
+          *reinterpret_cast<uint4*>(a.h_out + size_t(row0 + r) * kWsH + c) = *reinterpret_cast<const uint4*>(&xs[r][c]);
+      }
+    }
+    __syncthreads();  // xs is rewritten by the next tile's gather
+  }
 }
 
 __global__ void k_copy4(uint32_t n, const float4* __restrict__ src, float4* __restrict__ dst) {

@@ -381,6 +381,13 @@ class ClothSimulator:
                     dist_rms_total=float(tot[0]), dist_max_total=float(tot[1]),
                     bend_rms_total=float(tot[2]), bend_max_total=float(tot[3]))
 
+    def get_predicted_residual(self):
+        """With residual tracking: RMS |C| of the last substep's predicted
+        positions (before any iteration)."""
+        v = C.c_float()
+        self._c(self._L.tc_get_predicted_residual(self._h, C.byref(v)))
+        return v.value
+
     def set_profiling_enabled(self, enable):
         self._c(self._L.tc_set_profiling_enabled(self._h, int(bool(enable))))
         return bool(enable)
@@ -610,6 +617,12 @@ class ClothSimulator:
         self._c(self._L.tc_ws_stats(self._h, _ptr(out)))
         return {"substeps": int(out[0]), "fallbacks": int(out[1]), "last_residual": float(out[2]),
                 "threshold": float(out[3])}
+
+    def ws_set_relative_threshold(self, ratio):
+        """ratio > 0: a warm-started substep falls back when its residual is
+        above ratio x the residual of its predicted positions; 0 returns to
+        the absolute threshold of ws_enable."""
+        self._c(self._L.tc_ws_set_relative_threshold(self._h, float(ratio)))
 
     def ws_reset_stats(self):
         self._c(self._L.tc_ws_reset_stats(self._h))

@@ -2,8 +2,9 @@
 
 ``mlp_grad`` runs the warm-start network's forward and backward kernels on
 one graph and returns the loss, the parameter gradients and the outputs.
-``plain_residual`` measures the plain solver's max constraint residual, the
-threshold the warm start is judged against.  ``fit`` records plain-solver
+``plain_residual`` measures the plain solver's RMS constraint residual after
+every substep, whose percentile is the threshold the warm start is judged
+against.  ``fit`` records plain-solver
 snapshots, trains on them and leaves the network in the simulator.
 """
 from __future__ import annotations
@@ -14,23 +15,27 @@ import numpy as np
 
 from . import _lib
 
-PARAM_COUNT = 17795
+PARAM_COUNT = 17812
 # (name, offset, shape) of the fp32 parameter blob
 LAYOUT = (("W0", 0, (16, 64)), ("b0", 1024, (64,)), ("W1", 1088, (128, 64)), ("b1", 9280, (64,)),
           ("W2", 9344, (128, 64)), ("b2", 17536, (64,)), ("W3", 17600, (64, 3)), ("b3", 17792, (3,)))
+# the normalizer (not trained): per-feature input scales and the output scale
+NORM_LAYOUT = (("fscale", 17795, (16,)), ("yscale", 17811, (1,)))
 
 
 def unpack(blob):
     blob = np.asarray(blob, np.float32).ravel()
     if blob.size != PARAM_COUNT:
         raise ValueError(f"parameter blob must hold {PARAM_COUNT} floats")
-    return {name: blob[off:off + int(np.prod(shape))].reshape(shape) for name, off, shape in LAYOUT}
+    return {name: blob[off:off + int(np.prod(shape))].reshape(shape) for name, off, shape in LAYOUT + NORM_LAYOUT}
 
 
 def pack(params):
+    """Blob of the named arrays; a missing normalizer entry is the identity (1)."""
     out = np.zeros(PARAM_COUNT, np.float32)
-    for name, off, shape in LAYOUT:
-        out[off:off + int(np.prod(shape))] = np.asarray(params[name], np.float32).ravel()
+    for name, off, shape in LAYOUT + NORM_LAYOUT:
+        k = int(np.prod(shape))
+        out[off:off + k] = np.asarray(params[name], np.float32).ravel() if name in params else 1.0
     return out
 
 
@@ -59,24 +64,48 @@ def mlp_grad(feat, adj_off, adj_idx, target, mask, params, device=0, with_infere
     return (loss.value, grads, y, yi) if with_inference else (loss.value, grads, y)
 
 
-def plain_residual(sim, dt, substeps, frames):
-    """Mean over `frames` plain frames of the last substep's RMS constraint
-    residual |C + alpha~ lambda| over all distance and bending constraints,
-    the quantity the warm-started substep is judged by (advances the
-    simulation)."""
+def plain_residual(sim, dt, substeps, frames, percentile=90.0):
+    """The plain solver's RMS constraint residual |C + alpha~ lambda| over all
+    distance and bending constraints, measured after every substep of
+    `frames` frames (each substep stepped on its own, dt / substeps), as the
+    given percentile of those values: the level the warm-started substep is
+    judged against after each substep.  Advances the simulation."""
     c = sim.get_counts()
     nd, nb = c["nd"], c["nb"]
     sim.set_residual_tracking(True)
     vals = []
     try:
-        for _ in range(frames):
-            sim.step(dt, substeps)
+        for _ in range(frames * substeps):
+            sim.step(dt / substeps, 1)
             r = sim.get_residuals()
             ss = nd * r["dist_rms_total"] ** 2 + nb * r["bend_rms_total"] ** 2
             vals.append(float(np.sqrt(ss / max(nd + nb, 1))))
     finally:
         sim.set_residual_tracking(False)
-    return float(np.mean(vals))
+    return float(np.percentile(vals, percentile))
+
+
+def plain_residual_ratio(sim, dt, substeps, frames, percentile=90.0):
+    """The plain solver's final / predicted residual ratio (RMS |C + alpha~
+    lambda| after the iterations over RMS |C| of the predicted positions),
+    per substep over `frames` frames (each substep stepped on its own), as
+    the given percentile: the ratio of a relative warm-start threshold.
+    Advances the simulation."""
+    c = sim.get_counts()
+    nd, nb = c["nd"], c["nb"]
+    sim.set_residual_tracking(True)
+    vals = []
+    try:
+        for _ in range(frames * substeps):
+            sim.step(dt / substeps, 1)
+            r = sim.get_residuals()
+            ss = nd * r["dist_rms_total"] ** 2 + nb * r["bend_rms_total"] ** 2
+            r0 = sim.get_predicted_residual()
+            if r0 > 0.0:
+                vals.append(float(np.sqrt(ss / max(nd + nb, 1))) / r0)
+    finally:
+        sim.set_residual_tracking(False)
+    return float(np.percentile(vals, percentile)) if vals else float("inf")
 
 
 def fit(sim, dt, substeps, frames, every=1, capacity=None, epochs=60, lr=2e-3, seed=0):

@@ -6,8 +6,9 @@
 * With an all-zero network the warm-started substep is the plain solver:
   threshold +inf gives the bits of (iterations - k) plain iterations,
   threshold -1 (always fall back) the bits of the full iteration count.
-* Trained on plain-solver snapshots, the network lowers the RMS constraint
-  residual that (iterations - k) iterations leave, against no warm start.
+* Trained on plain-solver snapshots (the first training fits the feature
+  and output normalizer), the network lowers the RMS constraint residual
+  that (iterations - k) iterations leave, against no warm start.
 """
 import numpy as np
 import pytest
@@ -81,6 +82,62 @@ def test_zero_network_is_the_plain_solver(which):
     assert st_a["last_residual"] > 0.0
 
 
+@pytest.mark.parametrize("mode", ["absolute", "relative"])
+@pytest.mark.parametrize("which", ["config1", "config2_small"])
+def test_per_colour_warm_start_matches_persistent(which, mode):
+    """The per-colour launch mode (residual check on the device, fallback
+    iterations gated by its flag) gives the bits of the persistent solver,
+    with a threshold (absolute, or relative to the residual of the predicted
+    positions) that some substeps miss and others meet."""
+    sc = scenes.config1() if which == "config1" else scenes.config2(n=24, subdiv=2)
+    dt, sub, k = sc["dt"], sc["substeps"], 2
+    a, b = _scene_sims(sc, 2)
+    b.set_launch_config(False)
+    rng = np.random.default_rng(7)
+    blob = W.random_params(rng, scale_head=0.05)
+    probe = scenes.build(ClothSimulator, sc)
+    probe.ws_set_params(blob)
+    probe.ws_enable(k, float("inf"))
+    if mode == "relative":
+        probe.ws_set_relative_threshold(1e6)  # stats give 1e6 x the predicted residual
+    res = []
+    for _ in range(2 * sub):
+        probe.step(dt / sub, 1)
+        st = probe.ws_stats()
+        if mode == "absolute":
+            res.append(st["last_residual"])
+        elif st["threshold"] > 0.0:  # a rigidly moving cloth has a zero predicted residual
+            res.append(st["last_residual"] / (st["threshold"] / 1e6))
+    assert res
+    thr = float(np.median(res))
+    for s in (a, b):
+        s.ws_set_params(blob)
+        if mode == "relative":
+            s.ws_enable(k, float("inf"))
+            s.ws_set_relative_threshold(thr)
+        else:
+            s.ws_enable(k, thr)
+    for _ in range(3):
+        for s in (a, b):
+            s.step(dt, sub)
+    sa, sb = a.ws_stats(), b.ws_stats()
+    assert sa == sb, (sa, sb)
+    assert 0 < sa["fallbacks"] < sa["substeps"], sa
+    assert np.array_equal(_state(a)[0], _state(b)[0])
+    assert np.array_equal(_state(a)[1], _state(b)[1])
+
+
+def test_plain_residual_ratio():
+    """The plain solver's final / predicted residual ratio is a positive
+    finite number (on the pinned 64x64 sheet about 1: five Gauss-Seidel
+    iterations hardly move its global RMS residual)."""
+    sc = scenes.config1()
+    s = scenes.build(ClothSimulator, sc)
+    s.step(sc["dt"], sc["substeps"])
+    r = warmstart.plain_residual_ratio(s, sc["dt"], sc["substeps"], 1)
+    assert 0.0 < r < 4.0, r
+
+
 def test_invalid_warm_start_arguments():
     sc = scenes.config1()
     s = scenes.build(ClothSimulator, sc)
@@ -104,6 +161,11 @@ def test_trained_warm_start_gains_over_no_warm_start():
     assert got == 50
     assert l1 < 0.5 * l0, (l0, l1)
     trained = s.ws_params()
+    # the first training fitted the normalizer: motion features (about 1e-3
+    # of the edge length) are scaled up, the bias and free-flag inputs stay 1
+    P = warmstart.unpack(trained)
+    assert P["fscale"][0] > 10.0 and P["fscale"][15] == 1.0 and P["fscale"][14] == 1.0, P["fscale"]
+    assert 0.0 < P["yscale"][0] < 0.1, P["yscale"]
     start = _state(s)
 
     def run(params, enable):
@@ -127,3 +189,8 @@ def test_trained_warm_start_gains_over_no_warm_start():
     print(f"after {it - k} of {it} iterations: RMS residual no warm start {r_zero:.3e}, learned {r_ws:.3e}; "
           f"rms distance to the {it}-iteration positions {e_zero:.3e} vs {e_ws:.3e}")
     assert r_ws < r_zero
+    # a loaded network keeps its normalizer through further training
+    s.ws_set_params(trained)
+    warmstart.fit(s, dt, sub, frames=1, every=5, epochs=1, lr=1e-4, seed=1)
+    P2 = warmstart.unpack(s.ws_params())
+    assert np.array_equal(P2["fscale"], P["fscale"]) and np.array_equal(P2["yscale"], P["yscale"])

@@ -55,4 +55,5 @@ def test_blob_layout_roundtrip():
     assert blob.size == W.PARAM_COUNT
     assert np.array_equal(W.pack(W.unpack(blob)).astype(np.float32), blob)
     from taremincloth_b200 import warmstart as host
-    assert host.PARAM_COUNT == W.PARAM_COUNT and host.LAYOUT == W.LAYOUT
+    assert host.PARAM_COUNT == W.PARAM_COUNT and host.LAYOUT == W.LAYOUT and host.NORM_LAYOUT == W.NORM_LAYOUT
+    assert np.array_equal(host.pack(host.unpack(blob)), blob)
