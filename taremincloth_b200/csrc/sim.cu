@@ -134,8 +134,8 @@ struct Mlp {
     int dev = 0, sms = 0, per_sm = 0;
     TC_CK(cudaGetDevice(&dev));
     TC_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp, 256, 0));
     const unsigned tiles = grid(n, kWsRows);
+    TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp, 256, 0));
     mp_grid = std::max(1u, std::min(tiles, unsigned(std::max(per_sm, 1) * sms)));
   }
   // the ELL table of the inference kernels from the host CSR
@@ -212,8 +212,8 @@ struct Mlp {
     a.n = n; a.x_feat = feat; if (fa) a.fa = *fa; a.ppred = ppred; a.fscale = w.p + kP_FS;
     a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0; a.h_out = h0.p;
     k_mlp_infer_l0<<<grid(n, kWsL0Rows), kWsL0Rows, 0, st>>>(a);
-    a.h_prev = h0.p; a.ell = ell.p; a.adj_off = adj_off; a.adj_idx = adj_idx;
-    a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1; a.h_out = h1.p;
+    a.ell = ell.p; a.adj_off = adj_off; a.adj_idx = adj_idx;
+    a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1; a.h_out = h1.p;
     k_mlp_infer_mp<<<mp_grid, 256, 0, st>>>(a);
     a.h_prev = h1.p; a.wt = wbt.p + kT_W2; a.bias = w.p + kP_b2; a.h_out = nullptr;
     a.w3 = wb.p + kP_W3; a.b3 = w.p + kP_b3; a.yscale = w.p + kP_YS; a.y_out = y_out; a.x4 = x4; a.p4 = p4;

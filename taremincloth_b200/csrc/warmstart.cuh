@@ -73,6 +73,25 @@ __device__ __forceinline__ void load_b_frag(uint32_t b[2], const __nv_bfloat16* 
   b[0] = *reinterpret_cast<const uint32_t*>(c);
   b[1] = *reinterpret_cast<const uint32_t*>(c + 8);
 }
+// The same fragments with ldmatrix (one instruction per 16x16 A tile, one
+// per two 8-column B tiles): lane l supplies the address of row l % 8 of
+// 8x8 matrix l / 8; rows must start on 16 bytes.
+__device__ __forceinline__ void ldsm_x4(uint32_t r[4], const __nv_bfloat16* p) {
+  const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+// A fragment of rows row0..row0+15, k0..k0+15 (matrices: rows 0-7 / 8-15 x k 0-7 / 8-15)
+__device__ __forceinline__ void ldsm_a(uint32_t a[4], const __nv_bfloat16* A, int ld, int row0, int k0, int lane) {
+  const int m = lane >> 3, r = lane & 7;
+  ldsm_x4(a, A + (row0 + (m & 1) * 8 + r) * ld + k0 + (m >> 1) * 8);
+}
+// B fragments of columns n0..n0+7 (b[0..1]) and n0+8..n0+15 (b[2..3]) from Bt[n][k]
+__device__ __forceinline__ void ldsm_b2(uint32_t b[4], const __nv_bfloat16* Bt, int ld, int n0, int k0, int lane) {
+  const int m = lane >> 3, r = lane & 7;
+  ldsm_x4(b, Bt + (n0 + (m >> 1) * 8 + r) * ld + k0 + (m & 1) * 8);
+}
 // A^T fragment where the stored matrix is S[k][m] (row-major, ld): A(m, k) = S[k][m].
 __device__ __forceinline__ void load_at_frag(uint32_t a[4], const __nv_bfloat16* S, int ld, int m0, int k0, int lane) {
   const int g = lane >> 2, t = lane & 3;
@@ -647,6 +666,42 @@ __global__ void __launch_bounds__(kWsL0Rows) k_mlp_infer_l0(MlpInferArgs a) {
   }
 }
 
+// Neighbour mean of one (vertex, 8-column group): bf16(mean_{j in N(i)} H_j)
+// summed in adjacency order (as the training forward), up to eight
+// neighbour rows in flight.
+__device__ __forceinline__ uint4 ws_neighbour_mean(const MlpInferArgs& a, uint32_t v, int cg) {
+  auto row = [&](uint32_t j) { return __ldg(reinterpret_cast<const uint4*>(a.h_prev + size_t(j) * kWsH + cg)); };
+  const uint4* er = reinterpret_cast<const uint4*>(a.ell + size_t(v) * kWsEll);
+  const uint4 e0 = __ldg(er), e1 = __ldg(er + 1), e2 = __ldg(er + 2), e3 = __ldg(er + 3);
+  const uint32_t idx[15] = {e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w, e2.x, e2.y, e2.z, e2.w, e3.x, e3.y, e3.z, e3.w};
+  const uint32_t deg = e0.x, d1 = min(deg, 15u);
+  float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  auto add = [&](const uint4 u) {
+    float fv[8];
+    bf16x8_to_f32(u, fv);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] += fv[c];
+  };
+#pragma unroll
+  for (int q0 = 0; q0 < 15; q0 += 8) {
+    if (uint32_t(q0) >= d1) break;
+    uint4 u[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (q0 + k < 15 && uint32_t(q0 + k) < d1) u[k] = row(idx[q0 + k]);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (q0 + k < 15 && uint32_t(q0 + k) < d1) add(u[k]);
+  }
+  if (deg > 15u) {
+    const uint32_t b = __ldg(a.adj_off + v), en = __ldg(a.adj_off + v + 1);
+    for (uint32_t q = b + 15u; q < en; ++q) add(row(__ldg(a.adj_idx + q)));
+  }
+  const float inv = deg ? 1.0f / float(deg) : 0.0f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) acc[c] *= inv;
+  return f32_to_bf16x8(acc);
+}
 // Message-passing layer: X = [H_i, bf16(mean_j H_j)], H' = bf16(SiLU(X W + b)),
 // or with w3 the head Y = H' W3 + b3 and p += Y YS L on free vertices.
 __global__ void __launch_bounds__(256, 3) k_mlp_infer_mp(MlpInferArgs a) {
@@ -658,6 +713,8 @@ __global__ void __launch_bounds__(256, 3) k_mlp_infer_mp(MlpInferArgs a) {
     *reinterpret_cast<uint4*>(&ws[e >> 4][(e & 15) * 8]) = __ldg(reinterpret_cast<const uint4*>(a.wt) + e);
   const uint32_t ntiles = (a.n + kWsRows - 1) / kWsRows;
   auto row = [&](uint32_t j, int cg) { return __ldg(reinterpret_cast<const uint4*>(a.h_prev + size_t(j) * kWsH + cg)); };
+  const int g = lane >> 2, t = lane & 3;
+  const int wr = (warp & 3) * 16, wn = (warp >> 2) * 4;  // warp: rows wr..wr+15, columns (wn..wn+3) x 8
   for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const uint32_t row0 = tile * kWsRows;
 #pragma unroll 1
@@ -667,44 +724,12 @@ __global__ void __launch_bounds__(256, 3) k_mlp_infer_mp(MlpInferArgs a) {
       uint4 self = make_uint4(0, 0, 0, 0), mean = make_uint4(0, 0, 0, 0);
       if (v < a.n) {
         self = row(v, cg);
-        const uint4* er = reinterpret_cast<const uint4*>(a.ell + size_t(v) * kWsEll);
-        const uint4 e0 = __ldg(er), e1 = __ldg(er + 1), e2 = __ldg(er + 2), e3 = __ldg(er + 3);
-        const uint32_t idx[15] = {e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w, e2.x,
-                                  e2.y, e2.z, e2.w, e3.x, e3.y, e3.z, e3.w};
-        const uint32_t deg = e0.x, d1 = min(deg, 15u);
-        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        auto add = [&](const uint4 u) {
-          float fv[8];
-          bf16x8_to_f32(u, fv);
-#pragma unroll
-          for (int c = 0; c < 8; ++c) acc[c] += fv[c];
-        };
-#pragma unroll
-        for (int q0 = 0; q0 < 15; q0 += 8) {
-          if (uint32_t(q0) >= d1) break;
-          uint4 u[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k)
-            if (q0 + k < 15 && uint32_t(q0 + k) < d1) u[k] = row(idx[q0 + k], cg);
-#pragma unroll
-          for (int k = 0; k < 8; ++k)
-            if (q0 + k < 15 && uint32_t(q0 + k) < d1) add(u[k]);
-        }
-        if (deg > 15u) {
-          const uint32_t b = __ldg(a.adj_off + v), en = __ldg(a.adj_off + v + 1);
-          for (uint32_t q = b + 15u; q < en; ++q) add(row(__ldg(a.adj_idx + q), cg));
-        }
-        const float inv = deg ? 1.0f / float(deg) : 0.0f;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] *= inv;
-        mean = f32_to_bf16x8(acc);
+        mean = ws_neighbour_mean(a, v, cg);
       }
       *reinterpret_cast<uint4*>(&xs[r][cg]) = self;
       *reinterpret_cast<uint4*>(&xs[r][kWsH + cg]) = mean;
     }
     __syncthreads();
-    // warp w: rows (w % 4) * 16 .. +15, output columns (w / 4) * 32 .. +31
-    const int wr = (warp & 3) * 16, wn = (warp >> 2) * 4;
     float acc[4][4];
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt)
@@ -712,17 +737,14 @@ __global__ void __launch_bounds__(256, 3) k_mlp_infer_mp(MlpInferArgs a) {
       for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
 #pragma unroll
     for (int k0 = 0; k0 < 128; k0 += 16) {
-      uint32_t af[4];
-      load_a_frag(af, &xs[0][0], 128 + 8, wr, k0, lane);
+      uint32_t af[4], bf[2][4];
+      ldsm_a(af, &xs[0][0], 128 + 8, wr, k0, lane);
+      ldsm_b2(bf[0], &ws[0][0], 128 + 8, wn * 8, k0, lane);
+      ldsm_b2(bf[1], &ws[0][0], 128 + 8, wn * 8 + 16, k0, lane);
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        uint32_t bf[2];
-        load_b_frag(bf, &ws[0][0], 128 + 8, (wn + nt) * 8, k0, lane);
-        mma_bf16_16816(acc[nt], af, bf);
-      }
+      for (int nt = 0; nt < 4; ++nt) mma_bf16_16816(acc[nt], af, &bf[nt >> 1][(nt & 1) * 2]);
     }
     __syncthreads();  // every warp has read its input rows before any output is written over them
-    const int g = lane >> 2, t = lane & 3;
     float y0[3] = {0.f, 0.f, 0.f}, y1[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt)

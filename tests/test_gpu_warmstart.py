@@ -45,6 +45,22 @@ def test_mlp_grad_matches_reference(seed):
         assert e <= 2e-2, (name, e)
 
 
+def test_mlp_inference_large_graph_matches_reference():
+    """Inference on a large graph (persistent layer kernels, many tiles per
+    block): outputs against the numpy reference on a 259 x 255 grid graph
+    (66,045 vertices, a ragged last tile)."""
+    rng = np.random.default_rng(5)
+    off, idx = W.grid_graph(259, 255)
+    n = 259 * 255
+    feat = rng.normal(0, 1, (n, 16)).astype(np.float32)
+    target = rng.normal(0, 0.3, (n, 3)).astype(np.float32)
+    mask = np.ones(n, np.float32)
+    blob = W.random_params(rng)
+    _, _, _, y_inf = warmstart.mlp_grad(feat, off, idx, target, mask, blob, with_inference=True)
+    _, _, y_r = W.forward_backward(feat, off, idx, target, mask, blob)
+    assert _nrel(y_inf, y_r) <= 5e-3
+
+
 def _state(sim):
     x, _, v = sim.get_state()
     return x.copy(), v.copy()
