@@ -45,6 +45,21 @@ tc_status tc_create(tc_sim **out, const float *positions, uint32_t n, const uint
                     const uint32_t *faces, uint32_t nf, const float *inv_masses, const uint32_t *layer_ids,
                     const float *thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
                     float compression_stiffness, float shear_stiffness, float bending_stiffness, int device);
+/* tc_create with the sewing arguments of ClothSimulator::new
+ * (lib.rs:1557-1573, 1643-1665; mesh.rs:706-947): nsew sewing springs
+ * (pairs of vertices; an index out of range returns TC_ERR_INVALID),
+ * sewing_shrink_speed (m/s), sewing_stiffness (NaN: default 10000) and
+ * enable_sewing_lock, which only fill the per-constraint fields as the
+ * reference does (the solve reads tc_set_sewing_stiffness /
+ * tc_set_enable_sewing_lock, default 10000 and on), sewing_lock_distance
+ * (NaN: default 0.02 m).  The springs also add seam-gated bending across
+ * sewn boundary edges and contract the self-collision topology. */
+tc_status tc_create_sewn(tc_sim **out, const float *positions, uint32_t n, const uint32_t *edges, uint32_t ne,
+                         const uint32_t *faces, uint32_t nf, const float *inv_masses, const uint32_t *layer_ids,
+                         const float *thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
+                         float compression_stiffness, float shear_stiffness, float bending_stiffness,
+                         const uint32_t *sewing, uint32_t nsew, float sewing_shrink_speed, float sewing_stiffness,
+                         int enable_sewing_lock, float sewing_lock_distance, int device);
 tc_status tc_destroy(tc_sim *s);
 
 /* Batched instances (new; the reference runs one cloth per simulator): one
@@ -80,6 +95,34 @@ tc_status tc_reset(tc_sim *s);
 
 /* parameters (simulation/mod.rs:1091-1106, :1429-1449, lib.rs:2751-2800) */
 tc_status tc_set_gravity(tc_sim *s, float gx, float gy, float gz);
+/* Sewing (simulation/mod.rs:1211-1420, lib.rs:2798-2925).  Each substep
+ * shrinks every spring's current rest length towards 0 at the shrink speed
+ * (sewing_shrink.wgsl), projects the springs per colour after the distance
+ * constraints of every iteration and once more before the velocity update
+ * (sewing.wgsl; dispatch.rs:119-337).  Stiffness >= 5000 gives a hard
+ * constraint, else compliance 1 / max(k, 1); with the lock on, a pair
+ * closer than max(thickness sum, lock distance) latches to rest 0. */
+tc_status tc_get_num_sewing_constraints(tc_sim *s, uint32_t *count);
+tc_status tc_set_sewing_stiffness(tc_sim *s, float stiffness);
+tc_status tc_set_sewing_shrink_speed(tc_sim *s, float speed);
+tc_status tc_get_sewing_shrink_speed(tc_sim *s, float *speed);
+tc_status tc_set_enable_sewing_lock(tc_sim *s, int enabled);
+tc_status tc_set_sewing_lock_distance(tc_sim *s, float distance);
+tc_status tc_get_sewing_lock_distance(tc_sim *s, float *distance);
+/* current rest length of every spring, in the simulator's (colour) order;
+ * a set with len != the spring count is ignored, as in the reference */
+tc_status tc_get_sewing_current_rest_lengths(tc_sim *s, float *out, size_t len);
+tc_status tc_set_sewing_current_rest_lengths(tc_sim *s, const float *values, size_t len);
+/* Sewing priority: gravity is held at 0 until the share of springs closed
+ * within merge_dist reaches threshold (or max_frames pass), then ramps back
+ * with smoothstep over ramp_frames frames.  tc_update_sewing_priority takes
+ * host positions (n x 3) and returns (ratio, gravity scale, latched);
+ * tc_get_sewing_priority gives (gravity scale, ratio, held, latched). */
+tc_status tc_set_sewing_priority_options(tc_sim *s, int enabled, float threshold, float merge_dist,
+                                         uint32_t ramp_frames, uint32_t max_frames);
+tc_status tc_set_sewing_priority_state(tc_sim *s, int latched, uint32_t frame, float ramp_t, float ratio);
+tc_status tc_update_sewing_priority(tc_sim *s, const float *positions, uint32_t n, float out[3]);
+tc_status tc_get_sewing_priority(tc_sim *s, float out[4]);
 tc_status tc_set_damping(tc_sim *s, float damping);
 tc_status tc_set_damping_all(tc_sim *s, float tension, float compression, float shear, float bending);
 tc_status tc_set_solver_iterations(tc_sim *s, uint32_t iterations);
@@ -232,7 +275,20 @@ tc_status tc_mesh_build(tc_mesh **out, const float *positions, uint32_t n, const
                         const uint32_t *faces, uint32_t nf, const float *inv_masses, const uint32_t *layer_ids,
                         const float *thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
                         float compression_stiffness, float shear_stiffness, float bending_stiffness);
+/* tc_mesh_build with sewing springs (arguments as tc_create_sewn) */
+tc_status tc_mesh_build_sewn(tc_mesh **out, const float *positions, uint32_t n, const uint32_t *edges, uint32_t ne,
+                             const uint32_t *faces, uint32_t nf, const float *inv_masses, const uint32_t *layer_ids,
+                             const float *thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
+                             float compression_stiffness, float shear_stiffness, float bending_stiffness,
+                             const uint32_t *sewing, uint32_t nsew, float sewing_shrink_speed, float sewing_stiffness,
+                             int enable_sewing_lock);
 tc_status tc_mesh_destroy(tc_mesh *m);
+/* Sewing constraints (colour-sorted, coloring.rs:236-300): count, colours,
+ * vertex pairs, par[5] = current rest, target rest, shrink speed,
+ * compliance, lock flag; colour offsets / counts; rep[n] = sewing group of
+ * each vertex (its smallest member).  Any output may be NULL. */
+tc_status tc_mesh_sewing(tc_mesh *m, uint32_t *nsew, uint32_t *ncolors, uint32_t *v01, float *par, uint32_t *off,
+                         uint32_t *cnt, uint32_t *rep);
 /* out[10] = n, distance, bending, edges, distance colours, bending colours,
  * table size, multi-layer flag, virtual-particle count, adjacency length;
  * cell[1] = hash cell size */

@@ -41,6 +41,13 @@ def lib():
         L.ocl_create.restype = P
         L.ocl_create.argtypes = [P, C.c_int, P, C.c_int, P, C.c_int, P, P, P, C.c_uint32,
                                  C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]
+        L.ocl_create_sewn.restype = P
+        L.ocl_create_sewn.argtypes = [P, C.c_int, P, C.c_int, P, C.c_int, P, P, P, C.c_uint32,
+                                      C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P, C.c_int, C.c_float]
+        L.ocl_set_sewing.argtypes = [P, C.c_float, C.c_int, C.c_float, C.c_float]
+        L.ocl_get_sewing.argtypes = [P, P, P, P, P, P, P]
+        L.ocl_get_sewing.restype = C.c_int
+        L.ocl_get_bending_gate.argtypes = [P, fp]
         L.ocl_destroy.argtypes = [P]
         for name, n in [("ocl_set_gravity", 3), ("ocl_set_damping_all", 4), ("ocl_set_compliance_all", 4)]:
             getattr(L, name).argtypes = [P] + [C.c_float] * n
@@ -95,7 +102,8 @@ class OracleSim:
 
     def __init__(self, positions, edges, faces=None, inv_masses=None, layer_ids=None,
                  thicknesses=None, layer_id=0, thickness=0.005, stiffness=1000.0,
-                 bending_stiffness=10.0, compression_stiffness=None, shear_stiffness=None):
+                 bending_stiffness=10.0, compression_stiffness=None, shear_stiffness=None,
+                 sewing_springs=None, sewing_shrink_speed=1.0):
         L = lib()
         self._keep = []
         pos = np.ascontiguousarray(positions, dtype=_f).reshape(-1, 3)
@@ -107,9 +115,11 @@ class OracleSim:
         comp = stiffness if compression_stiffness is None else compression_stiffness
         shear = stiffness * 0.5 if shear_stiffness is None else shear_stiffness
         self.n = pos.shape[0]
-        self._h = L.ocl_create(_ptr(pos), pos.shape[0], _ptr(e), e.shape[0], _ptr(f),
-                               0 if f is None else f.shape[0], _ptr(im), _ptr(li), _ptr(th),
-                               layer_id, thickness, stiffness, comp, shear, bending_stiffness)
+        sew = None if sewing_springs is None else np.ascontiguousarray(sewing_springs, dtype=_u).reshape(-1, 2)
+        self._h = L.ocl_create_sewn(_ptr(pos), pos.shape[0], _ptr(e), e.shape[0], _ptr(f),
+                                    0 if f is None else f.shape[0], _ptr(im), _ptr(li), _ptr(th),
+                                    layer_id, thickness, stiffness, comp, shear, bending_stiffness,
+                                    _ptr(sew), 0 if sew is None else sew.shape[0], sewing_shrink_speed)
 
     def __del__(self):
         try:
@@ -220,9 +230,28 @@ class OracleSim:
     def bending_constraints(self):
         nb = self.counts()["nb"]
         v = np.zeros(4 * max(nb, 1), _u)
-        r, cp, p0 = (np.zeros(max(nb, 1), _f) for _ in range(3))
+        r, cp, p0, p1 = (np.zeros(max(nb, 1), _f) for _ in range(4))
         lib().ocl_get_bending(self._h, v, r, cp, p0)
-        return dict(v=v[:4 * nb].reshape(-1, 4), rest=r[:nb], comp=cp[:nb], pad0=p0[:nb])
+        lib().ocl_get_bending_gate(self._h, p1)
+        return dict(v=v[:4 * nb].reshape(-1, 4), rest=r[:nb], comp=cp[:nb], pad0=p0[:nb], pad1=p1[:nb])
+
+    # --- sewing --------------------------------------------------------
+    def set_sewing(self, stiffness=10000.0, lock=True, lock_distance=0.02, shrink_speed=1.0):
+        lib().ocl_set_sewing(self._h, stiffness, int(bool(lock)), lock_distance, shrink_speed)
+
+    def sewing(self):
+        """Sewing constraints in colour order: vertex pairs, current rest
+        lengths, colour offsets / counts and the sewing group of each vertex."""
+        L = lib()
+        nc = C.c_int()
+        k = L.ocl_get_sewing(self._h, C.byref(nc), None, None, None, None, None)
+        v = np.zeros(2 * max(k, 1), _u)
+        cur = np.zeros(max(k, 1), _f)
+        off, cnt = np.zeros(max(nc.value, 1), _u), np.zeros(max(nc.value, 1), _u)
+        rep = np.zeros(max(self.n, 1), _u)
+        L.ocl_get_sewing(self._h, None, _ptr(v), _ptr(cur), _ptr(off), _ptr(cnt), _ptr(rep))
+        return dict(v=v[:2 * k].reshape(-1, 2), cur=cur[:k], off=off[:nc.value], cnt=cnt[:nc.value],
+                    rep=rep[:self.n])
 
     def colors(self):
         c = self.counts()

@@ -13,12 +13,15 @@
  * counting-sort hash, spatial_grid_sort.wgsl:182-194) the oracle uses the
  * canonical order: ascending vertex / edge index within a hash bucket.
  *
- * Out of scope here (not reached by the workloads): sewing, seam-gated
- * bending, coarse constraints, pair-cache and virtual-particle
- * self-collision, edge colliders, bone SDF atlas.
+ * Out of scope here (not reached by the workloads): sewing priority,
+ * coarse constraints, pair-cache and virtual-particle self-collision, edge
+ * colliders.  Where the reference takes the two edges of a sewn seam in
+ * hash-map order (mesh.rs:742-765), the oracle takes them in face order;
+ * the resulting constraint acts the same either way round.
  */
 #include "tcloth_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -127,6 +130,8 @@ static int contains_u32(const uint32_t *a, size_t n, uint32_t x) {
 /* ------------------------------------------------------------------ */
 typedef struct { uint32_t v0, v1; float rest, tc, cc; uint32_t type; } ODist;
 typedef struct { uint32_t v0, v1, v2, v3; float rest, comp, pad0, pad1; } OBend;
+/* GpuSewingConstraint (mesh.rs:904-933) */
+typedef struct { uint32_t v0, v1; float cur, target, speed, comp, lock; } OSew;
 typedef struct { uint32_t type; float fric, rest; v3 a; float r; v3 b; } OCol;
 typedef struct { v3 p0; float fric; v3 p1; float thick; v3 p2; float rest; uint32_t flags; } OTri;
 typedef struct { uint32_t v; float w; v3 target; } OPin;
@@ -144,6 +149,9 @@ struct OSim {
     /* constraints */
     ODist *dist; int nd; uint32_t *dc_off, *dc_cnt; int ndc; float *dlam;
     OBend *bend; int nb; uint32_t *bc_off, *bc_cnt; int nbc; float *blam;
+    OSew *sew; int nsw; uint32_t *sc_off, *sc_cnt; int nsc; float *slam;
+    uint32_t *rep; /* sewing group of each vertex (its smallest member) */
+    float sew_stiffness, sew_speed, sew_lock_dist; int sew_lock; /* mod.rs:637-640 */
     /* topology */
     uint32_t *adj_off, *adj_idx;
     uint32_t *th_off, *th_idx; float *th_rest;
@@ -313,11 +321,87 @@ static float stiff_to_compliance(float k) {
 /* ------------------------------------------------------------------ */
 /* construction                                                        */
 /* ------------------------------------------------------------------ */
+/* unfolding about a seam edge e0->e1 (mesh.rs:795-809, :1436-1454): the
+ * position of p along the edge and its distance from the edge line */
+static int seam_frame(const float *e0, const float *e1, const float *p, float *sa, float *ha) {
+    float ev[3] = {e1[0] - e0[0], e1[1] - e0[1], e1[2] - e0[2]};
+    float len = sqrtf(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+    if (len <= 1e-6f) return 0;
+    float u[3] = {ev[0] / len, ev[1] / len, ev[2] / len};
+    float d[3] = {p[0] - e0[0], p[1] - e0[1], p[2] - e0[2]};
+    float sv = d[0] * u[0] + d[1] * u[1] + d[2] * u[2];
+    float q[3] = {d[0] - sv * u[0], d[1] - sv * u[1], d[2] - sv * u[2]};
+    *sa = sv;
+    *ha = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+    return 1;
+}
+static float seam_flat(float sa, float ha, float sb, float hb) {
+    float ds = sa - sb, dh = ha + hb;
+    return sqrtf(ds * ds + dh * dh);
+}
+/* compute_seam_two_hop_rest_length, mesh.rs:1382-1488 (oadj: the input
+ * mesh's adjacency, sorted) */
+static float seam_two_hop(int i, int nbr, const float *pos, const UVec *oadj, const uint32_t *rep) {
+    uint32_t ri = rep[i], rn = rep[nbr];
+    float best = FLT_MAX;
+    for (size_t a = 0; a < oadj[i].n; a++) {
+        uint32_t m1 = oadj[i].d[a], rm1 = rep[m1];
+        if (rm1 == ri || rm1 == rn) continue;
+        for (size_t b = 0; b < oadj[nbr].n; b++) {
+            uint32_t m2 = oadj[nbr].d[b];
+            if (rep[m2] != rm1) continue;
+            if (m1 == m2) { /* case 5a */
+                float d = dist3(pos + 3 * i, pos + 3 * nbr);
+                if (d < best) best = d;
+                continue;
+            }
+            int found = 0; /* case 5b: a seam edge from m1 and from m2 into one group */
+            for (size_t c = 0; c < oadj[m1].n; c++) {
+                uint32_t k1 = oadj[m1].d[c], rk1 = rep[k1];
+                if (rk1 == rm1) continue;
+                for (size_t e = 0; e < oadj[m2].n; e++) {
+                    uint32_t k2 = oadj[m2].d[e];
+                    if (rep[k2] != rk1) continue;
+                    float sa, ha, sb, hb;
+                    if (!seam_frame(pos + 3 * m1, pos + 3 * k1, pos + 3 * i, &sa, &ha)) continue;
+                    if (!seam_frame(pos + 3 * m2, pos + 3 * k2, pos + 3 * nbr, &sb, &hb)) continue;
+                    float fl = seam_flat(sa, ha, sb, hb);
+                    if (fl < best) { best = fl; found = 1; }
+                }
+            }
+            if (!found) { /* case 5c */
+                float sl = dist3(pos + 3 * i, pos + 3 * m1) + dist3(pos + 3 * nbr, pos + 3 * m2);
+                if (sl < best) best = sl;
+            }
+        }
+    }
+    return (best < FLT_MAX && isfinite(best) && best > 1e-5f) ? best : 0.0f;
+}
+
+typedef struct { uint64_t key; uint32_t a, b, opp, ord; } OSeam;
+static int cmp_seam(const void *x, const void *y) {
+    const OSeam *p = (const OSeam *)x, *q = (const OSeam *)y;
+    if (p->key != q->key) return p->key < q->key ? -1 : 1;
+    return (p->ord > q->ord) - (p->ord < q->ord);
+}
+
 OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, const uint32_t *faces,
                  int nf, const float *inv_masses, const uint32_t *layer_ids,
                  const float *thicknesses, uint32_t layer_id, float thickness, float tension_k,
                  float compression_k, float shear_k, float bending_k) {
+    return ocl_create_sewn(pos, n, edges, ne_in, faces, nf, inv_masses, layer_ids, thicknesses, layer_id,
+                           thickness, tension_k, compression_k, shear_k, bending_k, NULL, 0, 1.0f);
+}
+OSim *ocl_create_sewn(const float *pos, int n, const uint32_t *edges, int ne_in, const uint32_t *faces,
+                      int nf, const float *inv_masses, const uint32_t *layer_ids,
+                      const float *thicknesses, uint32_t layer_id, float thickness, float tension_k,
+                      float compression_k, float shear_k, float bending_k, const uint32_t *sew, int nsew,
+                      float shrink_speed) {
     OSim *s = (OSim *)calloc(1, sizeof(OSim));
+    s->sew_stiffness = 10000.0f;
+    s->sew_lock = 1;
+    s->sew_lock_dist = 0.02f;
+    s->sew_speed = fmaxf(shrink_speed, 0.0f);
     s->sc_interval = 1;
     s->ee_interval = 1;
     s->n = n;
@@ -430,6 +514,64 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, cons
             i = j;
         }
     }
+    /* sewing groups (mesh.rs:706-737): union-find, union into the smaller root */
+    uint32_t *rep = (uint32_t *)malloc(4 * N);
+    uint8_t *has_sew = (uint8_t *)calloc(N, 1);
+    for (int i = 0; i < n; i++) rep[i] = (uint32_t)i;
+    for (int k = 0; k < nsew; k++) {
+        uint32_t u = sew[2 * k], v = sew[2 * k + 1];
+        if ((int)u < n && (int)v < n && u != v) {
+            has_sew[u] = has_sew[v] = 1;
+            uint32_t ru = u, rv = v;
+            while (ru != rep[ru]) ru = rep[ru];
+            while (rv != rep[rv]) rv = rep[rv];
+            if (ru != rv) { if (ru < rv) rep[rv] = ru; else rep[ru] = rv; }
+        }
+    }
+    for (int i = 0; i < n; i++) { uint32_t r = (uint32_t)i; while (r != rep[r]) r = rep[r]; rep[i] = r; }
+    s->rep = rep;
+    /* seam-gated bending, mesh.rs:740-838: single-triangle edges whose ends
+     * are both sewn into two different groups, paired per group pair */
+    if (nsew > 0 && nf > 0) {
+        OSeam *se = (OSeam *)malloc(sizeof(OSeam) * ((size_t)neo + 1));
+        int nse = 0;
+        for (int i = 0; i < neo;) {
+            int j = i;
+            while (j < neo && eo[j].key == eo[i].key) j++;
+            uint32_t ea = (uint32_t)(eo[i].key >> 32), eb = (uint32_t)eo[i].key;
+            if (j - i == 1 && has_sew[ea] && has_sew[eb] && rep[ea] != rep[eb]) {
+                OSeam q;
+                q.key = ekey(rep[ea], rep[eb]);
+                q.a = rep[ea] < rep[eb] ? ea : eb; q.b = rep[ea] < rep[eb] ? eb : ea;
+                q.opp = eo[i].opp; q.ord = (uint32_t)nse;
+                se[nse++] = q;
+            }
+            i = j;
+        }
+        qsort(se, (size_t)nse, sizeof(OSeam), cmp_seam);
+        for (int i = 0; i < nse;) {
+            int j = i;
+            while (j < nse && se[j].key == se[i].key) j++;
+            if (j - i == 2) {
+                OSeam A = se[i], B = se[i + 1];
+                uint32_t v2 = A.opp, v3 = B.opp;
+                float sa, ha, sb, hb;
+                if (!(A.a == B.a || A.b == B.b || v2 == v3 || rep[v2] == rep[v3]) &&
+                    seam_frame(pos + 3 * A.a, pos + 3 * A.b, pos + 3 * v2, &sa, &ha) &&
+                    seam_frame(pos + 3 * B.a, pos + 3 * B.b, pos + 3 * v3, &sb, &hb)) {
+                    float flat = seam_flat(sa, ha, sb, hb);
+                    if (flat > 1e-5f) {
+                        if (nb == bcap) { bcap *= 2; bl = (OBend *)realloc(bl, sizeof(OBend) * (size_t)bcap); }
+                        OBend b; b.v0 = A.a; b.v1 = B.a; b.v2 = v2; b.v3 = v3; b.rest = flat; b.comp = bcomp;
+                        b.pad0 = 1.0f; b.pad1 = fmaxf(flat * 0.5f, 0.01f);
+                        bl[nb++] = b;
+                    }
+                }
+            }
+            i = j;
+        }
+        free(se);
+    }
     {
         KSet fe; kset_init(&fe, (uint32_t)(3 * nf) + 1);
         for (int f = 0; f < nf; f++) {
@@ -502,6 +644,31 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, cons
         free(vl); free(vc); free(rg); free(rc); free(col); free(perm);
     }
     free(bl);
+    /* 3. sewing constraints, mesh.rs:904-936; colouring coloring.rs:236-300 */
+    {
+        s->sew = (OSew *)malloc(sizeof(OSew) * ((size_t)nsew + 1));
+        OSew *sl = (OSew *)malloc(sizeof(OSew) * ((size_t)nsew + 1));
+        int ns = 0;
+        for (int k = 0; k < nsew; k++) {
+            uint32_t a = sew[2 * k], b = sew[2 * k + 1];
+            if ((int)a < n && (int)b < n && a != b) {
+                OSew c; c.v0 = a; c.v1 = b; c.cur = dist3(pos + 3 * a, pos + 3 * b); c.target = 0.0f;
+                c.speed = fmaxf(shrink_speed, 0.0f); c.comp = 0.0f; c.lock = 1.0f; /* stiffness 10000, lock on */
+                sl[ns++] = c;
+            }
+        }
+        uint32_t *vl = (uint32_t *)malloc(4 * (2 * (size_t)ns + 1));
+        int *vc = (int *)malloc(sizeof(int) * ((size_t)ns + 1));
+        for (int i = 0; i < ns; i++) { vl[2 * i] = sl[i].v0; vl[2 * i + 1] = sl[i].v1; vc[i] = 2; }
+        uint32_t *col = (uint32_t *)malloc(4 * ((size_t)ns + 1));
+        int ncol = ns ? wp_color(n, ns, vl, vc, 2, vl, vc, col) : 0;
+        int *perm = (int *)malloc(sizeof(int) * ((size_t)ns + 1));
+        bucket_reorder(ns, ncol, col, &s->sc_off, &s->sc_cnt, perm);
+        for (int i = 0; i < ns; i++) s->sew[i] = sl[perm[i]];
+        s->nsw = ns; s->nsc = ncol;
+        s->slam = (float *)calloc((size_t)ns + 1, 4);
+        free(sl); free(vl); free(vc); free(col); free(perm);
+    }
     /* 4. adjacency + local edge lengths, mesh.rs:949-1090 */
     UVec *adj = (UVec *)calloc(N, sizeof(UVec));
     float *lsum = (float *)calloc(N, 4);
@@ -523,6 +690,34 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, cons
     s->local_len = (float *)malloc(4 * N);
     for (int i = 0; i < n; i++)
         s->local_len[i] = lcnt[i] > 0 ? lsum[i] / (float)lcnt[i] : fmaxf(thickness, 0.01f);
+    for (int i = 0; i < n; i++) adj[i].n = sort_dedup(adj[i].d, adj[i].n);
+    /* the input mesh's adjacency, kept for two-hop rest lengths */
+    UVec *oadj = (UVec *)calloc(N, sizeof(UVec));
+    for (int i = 0; i < n; i++)
+        for (size_t k = 0; k < adj[i].n; k++) uv_push(&oadj[i], adj[i].d[k]);
+    int sewn = 0;
+    for (int i = 0; i < n; i++) if (rep[i] != (uint32_t)i) sewn = 1;
+    if (sewn) { /* mesh.rs:1026-1058: group members adjacent to each other and to all their neighbours */
+        for (int g = 0; g < n; g++) {
+            if (rep[g] != (uint32_t)g) continue;
+            UVec mem = {0}, sh = {0};
+            for (int i = g; i < n; i++) if (rep[i] == (uint32_t)g) uv_push(&mem, (uint32_t)i);
+            if (mem.n > 1) {
+                for (size_t a = 0; a < mem.n; a++)
+                    for (size_t b = 0; b < mem.n; b++)
+                        if (a != b) uv_push(&adj[mem.d[a]], mem.d[b]);
+                for (size_t a = 0; a < mem.n; a++)
+                    for (size_t k = 0; k < oadj[mem.d[a]].n; k++) {
+                        uint32_t w = oadj[mem.d[a]].d[k];
+                        if (rep[w] != (uint32_t)g) uv_push(&sh, w);
+                    }
+                sh.n = sort_dedup(sh.d, sh.n);
+                for (size_t a = 0; a < mem.n; a++)
+                    for (size_t k = 0; k < sh.n; k++) { uv_push(&adj[mem.d[a]], sh.d[k]); uv_push(&adj[sh.d[k]], mem.d[a]); }
+            }
+            free(mem.d); free(sh.d);
+        }
+    }
     s->adj_off = (uint32_t *)malloc(4 * (N + 1));
     size_t tot_adj = 0;
     for (int i = 0; i < n; i++) { adj[i].n = sort_dedup(adj[i].d, adj[i].n); tot_adj += adj[i].n; }
@@ -536,7 +731,15 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, cons
         }
         s->adj_off[n] = o;
     }
-    /* 4b. two-hop CSR, mesh.rs:1092-1199 (no sewing: contracted == original) */
+    /* 4b. two-hop CSR, mesh.rs:1092-1199: the hop sets from the sewing-
+     * extended adjacency; true two-hop pairs exclude the same group and
+     * pairs adjacent in the input or in the group-contracted mesh */
+    UVec *chop = (UVec *)calloc(N, sizeof(UVec));
+    for (int e = 0; e < ne_in; e++) {
+        uint32_t a = edges[2 * e], b = edges[2 * e + 1];
+        if ((int)a < n && (int)b < n && a != b && rep[a] != rep[b]) { uv_push(&chop[rep[a]], rep[b]); uv_push(&chop[rep[b]], rep[a]); }
+    }
+    for (int i = 0; i < n; i++) chop[i].n = sort_dedup(chop[i].d, chop[i].n);
     uint8_t *isface = (uint8_t *)calloc(N, 1);
     for (int f = 0; f < nf; f++)
         for (int k = 0; k < 3; k++) if ((int)faces[3 * f + k] < n) isface[faces[3 * f + k]] = 1;
@@ -564,9 +767,19 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, cons
             for (size_t k = 0; k < q; k++) {
                 uint32_t nbr = tmp[k];
                 uv_push(&th, nbr);
-                int true2 = nbr != (uint32_t)i && isface[i] && isface[nbr] &&
-                            !contains_u32(adj[i].d, adj[i].n, nbr);
-                float d = true2 ? dist3(pos + 3 * i, pos + 3 * nbr) : 0.0f;
+                int true2 = nbr != (uint32_t)i && isface[i] && isface[nbr] && rep[i] != rep[nbr] &&
+                            !contains_u32(oadj[i].d, oadj[i].n, nbr) &&
+                            !contains_u32(chop[rep[i]].d, chop[rep[i]].n, rep[nbr]);
+                float d = 0.0f;
+                if (true2) {
+                    /* within two hops of the input mesh: plain distance */
+                    int orig2 = contains_u32(oadj[i].d, oadj[i].n, nbr);
+                    for (size_t a = 0; a < oadj[i].n && !orig2; a++) {
+                        uint32_t u = oadj[i].d[a];
+                        orig2 = contains_u32(oadj[u].d, oadj[u].n, nbr);
+                    }
+                    d = orig2 ? dist3(pos + 3 * i, pos + 3 * nbr) : seam_two_hop(i, (int)nbr, pos, oadj, rep);
+                }
                 if (rn == rcap) { rcap = rcap ? rcap * 2 : 64; rest = (float *)realloc(rest, 4 * rcap); }
                 rest[rn++] = d;
             }
@@ -669,18 +882,38 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, cons
                 }
             }
             qsort(rc, (size_t)nrc, sizeof(EOpp), cmp_eopp);
+            /* the same counts between sewing groups (contracted mesh) */
+            EOpp *cc = (EOpp *)malloc(sizeof(EOpp) * ((size_t)nrc + 1));
+            int ncc = 0;
+            for (int q = 0; q < nrc; q++) {
+                uint32_t a = rep[(uint32_t)(rc[q].key >> 32)], b = rep[(uint32_t)rc[q].key];
+                if (a != b) { cc[ncc].key = ekey(a, b); cc[ncc].ord = (uint32_t)ncc; cc[ncc].opp = 0; ncc++; }
+            }
+            qsort(cc, (size_t)ncc, sizeof(EOpp), cmp_eopp);
             for (int e = 0; e < ng; e++) {
+                uint32_t ra = rep[ge[2 * e]], rb = rep[ge[2 * e + 1]];
+                if (ra == rb) continue;
                 uint64_t k = ekey(ge[2 * e], ge[2 * e + 1]);
                 /* binary search count */
                 int lo = 0, hi = nrc;
                 while (lo < hi) { int m = (lo + hi) / 2; if (rc[m].key < k) lo = m + 1; else hi = m; }
                 int c = 0;
                 while (lo + c < nrc && rc[lo + c].key == k) c++;
-                if (c == 0 || c == 1) s->ebits[e >> 5] |= 1u << (e & 31);
+                int open = c == 0;
+                if (c == 1) {
+                    uint64_t kc = ekey(ra, rb);
+                    lo = 0; hi = ncc;
+                    while (lo < hi) { int m = (lo + hi) / 2; if (cc[m].key < kc) lo = m + 1; else hi = m; }
+                    int c2 = 0;
+                    while (lo + c2 < ncc && cc[lo + c2].key == kc) c2++;
+                    open = c2 == 1;
+                }
+                if (open) s->ebits[e >> 5] |= 1u << (e & 31);
             }
-            free(rc);
+            free(rc); free(cc);
         } else {
-            for (int e = 0; e < ng; e++) s->ebits[e >> 5] |= 1u << (e & 31);
+            for (int e = 0; e < ng; e++)
+                if (rep[ge[2 * e]] != rep[ge[2 * e + 1]]) s->ebits[e >> 5] |= 1u << (e & 31);
         }
     }
     /* automatic layers by island mean Z, simulation/pipelines.rs:131-167 */
@@ -777,7 +1010,8 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne_in, cons
     s->srt = (uint32_t *)calloc(N, 4);
     s->ecs = (uint32_t *)calloc((size_t)s->table + 1, 4);
     s->esrt = (uint32_t *)calloc((size_t)s->ne + 1, 4);
-    for (int i = 0; i < n; i++) free(adj[i].d);
+    for (int i = 0; i < n; i++) { free(adj[i].d); free(oadj[i].d); free(chop[i].d); }
+    free(oadj); free(chop); free(has_sew);
     free(adj); free(lsum); free(lcnt); free(isface); free(eo); free(dl); free(vf);
     kset_free(&orig);
     return s;
@@ -790,7 +1024,7 @@ void ocl_destroy(OSim *s) {
                     s->adj_off, s->adj_idx, s->th_off, s->th_idx, s->th_rest, s->local_len,
                     s->star_off, s->star_idx, s->edges, s->ebits, s->island, s->cols, s->tris,
                     s->bounds, s->pins, s->acc, s->nrm, s->cs, s->srt, s->ecs, s->esrt,
-                    s->atlas, s->binfo, s->bxf};
+                    s->atlas, s->binfo, s->bxf, s->sew, s->sc_off, s->sc_cnt, s->slam, s->rep};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(s);
 }
@@ -979,6 +1213,44 @@ static void k_distance(OSim *s, int cidx, float dt_sub) {
         float a0 = w0 * dl, a1 = -w1 * dl;
         s->p[c->v0] = vadd(s->p[c->v0], vmul(dir, a0));
         s->p[c->v1] = vadd(s->p[c->v1], vmul(dir, a1));
+    }
+}
+/* shaders/sewing_shrink.wgsl:38-49 */
+static void k_sew_shrink(OSim *s, float dt_sub) {
+    float dt = fmaxf(dt_sub, 1e-8f);
+    for (int i = 0; i < s->nsw; i++) s->sew[i].cur = fmaxf(s->sew[i].target, s->sew[i].cur - s->sew_speed * dt);
+}
+/* shaders/sewing.wgsl:57-110, settings from SimParams (dispatch.rs:29-35) */
+static void k_sewing(OSim *s, int cidx, float dt_sub) {
+    float scomp = s->sew_stiffness >= 5000.0f ? 0.0f : 1.0f / fmaxf(s->sew_stiffness, 1.0f);
+    uint32_t off = s->sc_off[cidx], cnt = s->sc_cnt[cidx];
+    for (uint32_t q = 0; q < cnt; q++) {
+        uint32_t ci = off + q;
+        OSew *c = &s->sew[ci];
+        float w0 = s->w[c->v0], w1 = s->w[c->v1];
+        float ws = w0 + w1;
+        if (ws <= EPS) continue;
+        v3 p0 = s->p[c->v0], p1 = s->p[c->v1];
+        v3 delta = vsub(p0, p1);
+        float dist = vlen(delta);
+        if (dist <= EPS) continue;
+        float dt = fmaxf(dt_sub, 1e-8f);
+        v3 dir = vdiv(delta, dist);
+        float target = c->cur, comp = scomp;
+        float lock_thresh = fmaxf(s->thick[c->v0] + s->thick[c->v1], s->sew_lock_dist);
+        if (s->sew_lock && dist <= lock_thresh) {
+            comp = 0.0f;
+            target = c->target;
+            c->cur = c->target;
+        }
+        float alpha = comp / (dt * dt);
+        float cv = dist - target;
+        float lam = s->slam[ci];
+        float dl = (-cv - alpha * lam) / (ws + alpha);
+        s->slam[ci] = lam + dl;
+        float a0 = w0 * dl, a1 = -w1 * dl;
+        s->p[c->v0] = vadd(p0, vmul(dir, a0));
+        s->p[c->v1] = vadd(p1, vmul(dir, a1));
     }
 }
 /* shaders/bending.wgsl:59-126 */
@@ -2385,7 +2657,7 @@ void ocl_set_self_collision_intervals(OSim *s, int sc_interval, int ee_interval)
 }
 
 /* encode_simulation_steps, simulation/dispatch.rs:7-354 (default modes:
- * coupled self-collision mode 0, no sewing, no edge collision) */
+ * coupled self-collision mode 0, no sewing priority, no edge collision) */
 void ocl_step(OSim *s, float dt, int substeps) {
     if (s->n == 0) return;
     if (substeps <= 0) substeps = 20; /* base_substeps, simulation/mod.rs:673 */
@@ -2404,21 +2676,43 @@ void ocl_step(OSim *s, float dt, int substeps) {
         int run_ee = s->ee_interval == 0 ? 0 : (s->ee_interval == 1 ? 1 : (sub % s->ee_interval == 0 || last));
         memset(s->dlam, 0, 4 * ((size_t)s->nd + 1));
         memset(s->blam, 0, 4 * ((size_t)s->nb + 1));
+        memset(s->slam, 0, 4 * ((size_t)s->nsw + 1));
+        k_sew_shrink(s, dts);
         k_predict(s, dts);
         for (int it = 0; it < s->iters; it++) {
             if (s->npins > 0) k_pin(s, dts);
             for (int c = 0; c < s->ndc; c++) if (s->dc_cnt[c]) k_distance(s, c, dts);
+            for (int c = 0; c < s->nsc; c++) if (s->sc_cnt[c]) k_sewing(s, c, dts);
             for (int c = 0; c < s->nbc; c++) if (s->bc_cnt[c]) k_bending(s, c, dts);
             if (hascol && coupled) k_collision(s, dts);
         }
         if (hascol && !coupled) k_collision(s, dts);
         if (s->npins > 0) k_pin(s, dts);
         if (do_sc) self_collision(s, run_ee);
+        for (int c = 0; c < s->nsc; c++) if (s->sc_cnt[c]) k_sewing(s, c, dts); /* final sewing, dispatch.rs:323-337 */
         k_update_vel(s, dts);
     }
 }
 
 int ocl_num_vertices(const OSim *s) { return s->n; }
+void ocl_set_sewing(OSim *s, float stiffness, int lock, float lock_dist, float shrink_speed) {
+    s->sew_stiffness = fmaxf(stiffness, 1.0f);
+    s->sew_lock = lock != 0;
+    s->sew_lock_dist = fmaxf(lock_dist, 0.0f);
+    s->sew_speed = fmaxf(shrink_speed, 0.0f);
+}
+int ocl_get_sewing(const OSim *s, int *ncolors, uint32_t *v01, float *cur, uint32_t *off, uint32_t *cnt,
+                   uint32_t *rep) {
+    if (ncolors) *ncolors = s->nsc;
+    for (int i = 0; i < s->nsw; i++) {
+        if (v01) { v01[2 * i] = s->sew[i].v0; v01[2 * i + 1] = s->sew[i].v1; }
+        if (cur) cur[i] = s->sew[i].cur;
+    }
+    if (off) memcpy(off, s->sc_off, 4 * (size_t)s->nsc);
+    if (cnt) memcpy(cnt, s->sc_cnt, 4 * (size_t)s->nsc);
+    if (rep) memcpy(rep, s->rep, 4 * (size_t)s->n);
+    return s->nsw;
+}
 void ocl_get_positions(const OSim *s, float *out) {
     for (int i = 0; i < s->n; i++) { out[3 * i] = s->x[i].x; out[3 * i + 1] = s->x[i].y; out[3 * i + 2] = s->x[i].z; }
 }
@@ -2452,6 +2746,9 @@ void ocl_get_bending(const OSim *s, uint32_t *v, float *rest, float *comp, float
         v[4 * i] = s->bend[i].v0; v[4 * i + 1] = s->bend[i].v1; v[4 * i + 2] = s->bend[i].v2; v[4 * i + 3] = s->bend[i].v3;
         rest[i] = s->bend[i].rest; comp[i] = s->bend[i].comp; pad0[i] = s->bend[i].pad0;
     }
+}
+void ocl_get_bending_gate(const OSim *s, float *pad1) {
+    for (int i = 0; i < s->nb; i++) pad1[i] = s->bend[i].pad1;
 }
 void ocl_get_dist_colors(const OSim *s, uint32_t *off, uint32_t *cnt) {
     memcpy(off, s->dc_off, 4 * (size_t)s->ndc); memcpy(cnt, s->dc_cnt, 4 * (size_t)s->ndc);

@@ -26,8 +26,7 @@ extern "C" {
 typedef struct OSim OSim;
 
 /* Mesh + simulator construction.  Mirrors ClothMesh::from_raw_with_opts
- * (crates/cloth_core/src/mesh.rs:407-1377) without sewing / coarse
- * constraints, followed by GpuClothSimulator::with_options
+ * (crates/cloth_core/src/mesh.rs:407-1377) without coarse constraints, followed by GpuClothSimulator::with_options
  * (crates/cloth_core/src/simulation/mod.rs:363-697) and
  * build_simulation_resources (simulation/pipelines.rs:114-912). */
 OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne,
@@ -35,7 +34,20 @@ OSim *ocl_create(const float *pos, int n, const uint32_t *edges, int ne,
                  const uint32_t *layer_ids, const float *thicknesses,
                  uint32_t layer_id, float thickness, float tension_k,
                  float compression_k, float shear_k, float bending_k);
+/* ocl_create with sewing springs (nsew pairs; mesh.rs:706-947: sewing
+ * constraints, seam-gated bending, sewing-contracted topology) */
+OSim *ocl_create_sewn(const float *pos, int n, const uint32_t *edges, int ne,
+                      const uint32_t *faces, int nf, const float *inv_masses,
+                      const uint32_t *layer_ids, const float *thicknesses,
+                      uint32_t layer_id, float thickness, float tension_k,
+                      float compression_k, float shear_k, float bending_k,
+                      const uint32_t *sew, int nsew, float shrink_speed);
 void ocl_destroy(OSim *s);
+/* simulator-level sewing settings (simulation/mod.rs:1211-1255) */
+void ocl_set_sewing(OSim *s, float stiffness, int lock, float lock_dist, float shrink_speed);
+/* sewing constraints in colour order: returns the count; any output may be NULL */
+int ocl_get_sewing(const OSim *s, int *ncolors, uint32_t *v01, float *cur, uint32_t *off, uint32_t *cnt,
+                   uint32_t *rep);
 
 /* setters (simulation/mod.rs, cloth_py/src/lib.rs) */
 void ocl_set_gravity(OSim *s, float gx, float gy, float gz);
@@ -73,6 +85,8 @@ void ocl_counts(const OSim *s, int *out8);
 void ocl_get_distance(const OSim *s, uint32_t *v01, float *rest, float *tc, float *cc,
                       uint32_t *type);
 void ocl_get_bending(const OSim *s, uint32_t *v0123, float *rest, float *comp, float *pad0);
+/* pad1 of each bending constraint (the seam gate distance of seam entries) */
+void ocl_get_bending_gate(const OSim *s, float *pad1);
 void ocl_get_dist_colors(const OSim *s, uint32_t *off, uint32_t *cnt);
 void ocl_get_bend_colors(const OSim *s, uint32_t *off, uint32_t *cnt);
 void ocl_get_edges(const OSim *s, uint32_t *e2, uint32_t *bits);

@@ -25,6 +25,8 @@ SIGNATURES = {
     "tc_gpu_available": [],
     "tc_device_name": [_I, C.c_char_p, C.c_size_t],
     "tc_create": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F, _I],
+    "tc_create_sewn": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F, _P, _U, _F, _F, _I,
+                       _F, _I],
     "tc_destroy": [_P],
     "tc_batch_create": [C.POINTER(_P), _U, _P, _P, _P, _P, _P, _P, _P, _F, _P, _P, _P, _I],
     "tc_batch_instance_offsets": [_P, _P, _U, C.POINTER(_U)],
@@ -35,6 +37,19 @@ SIGNATURES = {
     "tc_set_positions_and_velocities": [_P, _P, _P, _U],
     "tc_reset": [_P],
     "tc_set_gravity": [_P, _F, _F, _F],
+    "tc_get_num_sewing_constraints": [_P, C.POINTER(_U)],
+    "tc_set_sewing_stiffness": [_P, _F],
+    "tc_set_sewing_shrink_speed": [_P, _F],
+    "tc_get_sewing_shrink_speed": [_P, C.POINTER(_F)],
+    "tc_set_enable_sewing_lock": [_P, _I],
+    "tc_set_sewing_lock_distance": [_P, _F],
+    "tc_get_sewing_lock_distance": [_P, C.POINTER(_F)],
+    "tc_get_sewing_current_rest_lengths": [_P, _P, C.c_size_t],
+    "tc_set_sewing_current_rest_lengths": [_P, _P, C.c_size_t],
+    "tc_set_sewing_priority_options": [_P, _I, _F, _F, _U, _U],
+    "tc_set_sewing_priority_state": [_P, _I, _U, _F, _F],
+    "tc_update_sewing_priority": [_P, _P, _U, _P],
+    "tc_get_sewing_priority": [_P, _P],
     "tc_set_damping": [_P, _F],
     "tc_set_damping_all": [_P, _F, _F, _F, _F],
     "tc_set_solver_iterations": [_P, _U],
@@ -111,6 +126,9 @@ SIGNATURES = {
     "tc_ws_reset_stats": [_P],
     "tc_mlp_grad": [_U, _P, _P, _P, _P, _P, _P, C.POINTER(_F), _P, _P, _P, _I],
     "tc_mesh_build": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F],
+    "tc_mesh_build_sewn": [C.POINTER(_P), _P, _U, _P, _U, _P, _U, _P, _P, _P, _U, _F, _F, _F, _F, _F, _P, _U, _F, _F,
+                           _I],
+    "tc_mesh_sewing": [_P, C.POINTER(_U), C.POINTER(_U), _P, _P, _P, _P, _P],
     "tc_mesh_destroy": [_P],
     "tc_mesh_counts": [_P, _P, C.POINTER(_F)],
     "tc_mesh_constraints": [_P, _P, _P, _P, _P, _P, _P, _P, _P],

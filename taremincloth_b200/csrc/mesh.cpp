@@ -153,6 +153,66 @@ uint32_t morton3(float px, float py, float pz, const float bmin[3], const float 
   return (expand10(x) << 2) | (expand10(y) << 1) | expand10(z);
 }
 
+// |(projection of p - e0 onto the edge e0->e1, distance from the edge line)|,
+// the in-plane coordinates used to unfold two triangles about a seam
+// (mesh.rs:795-809, :1436-1454).  ok = false for a degenerate edge.
+struct EdgeFrame { float s, h; bool ok; };
+EdgeFrame edge_frame(const float* e0, const float* e1, const float* p) {
+  const float ev[3] = {e1[0] - e0[0], e1[1] - e0[1], e1[2] - e0[2]};
+  const float len = std::sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+  if (len <= 1e-6f) return {0.f, 0.f, false};
+  const float u[3] = {ev[0] / len, ev[1] / len, ev[2] / len};
+  const float d[3] = {p[0] - e0[0], p[1] - e0[1], p[2] - e0[2]};
+  const float s = d[0] * u[0] + d[1] * u[1] + d[2] * u[2];
+  const float q[3] = {d[0] - s * u[0], d[1] - s * u[1], d[2] - s * u[2]};
+  return {s, std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]), true};
+}
+// distance of the opposite vertices with both triangles unfolded flat about
+// the seam: sqrt((sa - sb)^2 + (ha + hb)^2)
+inline float unfolded(const EdgeFrame& a, const EdgeFrame& b) {
+  const float ds = a.s - b.s, dh = a.h + b.h;
+  return std::sqrt(ds * ds + dh * dh);
+}
+
+// Rest length of a two-hop pair that is two-hop only through a sewing
+// group (mesh.rs:1382-1488): the smallest of, over relay groups reached
+// from both i and nbr, the direct distance (same relay vertex), the
+// unfolded distance across a shared seam edge, or the two edge lengths
+// summed (no shared seam edge); 0 when none is above 1e-5.
+float seam_two_hop_rest(uint32_t i, uint32_t nbr, const float* P, const std::vector<uint32_t>& off,
+                        const std::vector<uint32_t>& idx, const std::vector<uint32_t>& rep) {
+  auto pv = [&](uint32_t v) { return P + 3 * size_t(v); };
+  const uint32_t ri = rep[i], rn = rep[nbr];
+  float best = 3.4028235e38f;
+  for (uint32_t q1 = off[i]; q1 < off[i + 1]; ++q1) {
+    const uint32_t m1 = idx[q1], rm1 = rep[m1];
+    if (rm1 == ri || rm1 == rn) continue;
+    for (uint32_t q2 = off[nbr]; q2 < off[nbr + 1]; ++q2) {
+      const uint32_t m2 = idx[q2];
+      if (rep[m2] != rm1) continue;
+      if (m1 == m2) {
+        best = std::fmin(best, len3(pv(i), pv(nbr)));
+        continue;
+      }
+      bool seam = false;
+      for (uint32_t k1q = off[m1]; k1q < off[m1 + 1]; ++k1q) {
+        const uint32_t k1 = idx[k1q], rk1 = rep[k1];
+        if (rk1 == rm1) continue;
+        for (uint32_t k2q = off[m2]; k2q < off[m2 + 1]; ++k2q) {
+          const uint32_t k2 = idx[k2q];
+          if (rep[k2] != rk1) continue;
+          const EdgeFrame fa = edge_frame(pv(m1), pv(k1), pv(i)), fb = edge_frame(pv(m2), pv(k2), pv(nbr));
+          if (!fa.ok || !fb.ok) continue;
+          const float fl = unfolded(fa, fb);
+          if (fl < best) { best = fl; seam = true; }
+        }
+      }
+      if (!seam) best = std::fmin(best, len3(pv(i), pv(m1)) + len3(pv(nbr), pv(m2)));
+    }
+  }
+  return (best < 3.4028235e38f && std::isfinite(best) && best > 1e-5f) ? best : 0.f;
+}
+
 MeshData build_mesh(const MeshInput& in) {
   MeshData m;
   const uint32_t n = in.n;
@@ -258,6 +318,68 @@ MeshData build_mesh(const MeshInput& in) {
       i = j;
     }
   }
+  // ---- sewing groups (mesh.rs:706-737, :990-1024): union-find over the
+  //      springs, each group represented by its smallest vertex index
+  std::vector<uint32_t>& rep = m.sew_rep;
+  rep.resize(n);
+  std::vector<uint8_t> has_sew(n, 0);
+  for (uint32_t i = 0; i < n; ++i) rep[i] = i;
+  auto find = [&](uint32_t i) {
+    uint32_t r = i;
+    while (r != rep[r]) r = rep[r];
+    while (i != r) { const uint32_t nx = rep[i]; rep[i] = r; i = nx; }
+    return r;
+  };
+  for (uint32_t k = 0; k < in.nsew; ++k) {
+    const uint32_t u = in.sew[2 * size_t(k)], v = in.sew[2 * size_t(k) + 1];
+    if (u < n && v < n && u != v) {
+      has_sew[u] = has_sew[v] = 1;
+      const uint32_t ru = find(u), rv = find(v);
+      if (ru != rv) rep[std::max(ru, rv)] = std::min(ru, rv);
+    }
+  }
+  for (uint32_t i = 0; i < n; ++i) rep[i] = find(i);
+  // ---- seam-gated bending across sewn boundary edges (mesh.rs:706-838):
+  //      two boundary edges (one triangle each) whose endpoints fall in the
+  //      same two sewing groups get a bending constraint between their
+  //      opposite vertices, rest = the distance with both triangles unfolded
+  //      flat, gated on the seam closing to max(rest / 2, 0.01).  Within a
+  //      group pair the two edges are taken in face order (the reference
+  //      takes them in hash-map order; the constraint acts the same either
+  //      way round).
+  if (in.nsew > 0 && in.nf > 0) {
+    struct Seam { uint64_t key; uint32_t a, b, opp, ord; };
+    std::vector<Seam> se;
+    for (size_t i = 0; i < eo.size();) {
+      size_t j = i;
+      while (j < eo.size() && eo[j].key == eo[i].key) ++j;
+      const uint32_t ea = klo(eo[i].key), eb = khi(eo[i].key);
+      if (j - i == 1 && has_sew[ea] && has_sew[eb] && rep[ea] != rep[eb]) {
+        const bool fwd = rep[ea] < rep[eb];
+        se.push_back({key2(rep[ea], rep[eb]), fwd ? ea : eb, fwd ? eb : ea, eo[i].opp, uint32_t(se.size())});
+      }
+      i = j;
+    }
+    std::sort(se.begin(), se.end(), [](const Seam& x, const Seam& y) {
+      return x.key != y.key ? x.key < y.key : x.ord < y.ord;
+    });
+    for (size_t i = 0; i < se.size();) {
+      size_t j = i;
+      while (j < se.size() && se[j].key == se[i].key) ++j;
+      if (j - i == 2) {
+        const Seam &A = se[i], &B = se[i + 1];
+        const uint32_t v2 = A.opp, v3 = B.opp;
+        if (!(A.a == B.a || A.b == B.b || v2 == v3 || rep[v2] == rep[v3])) {
+          const EdgeFrame fa = edge_frame(pv(A.a), pv(A.b), pv(v2)), fb = edge_frame(pv(B.a), pv(B.b), pv(v3));
+          if (fa.ok && fb.ok) {
+            const float flat = unfolded(fa, fb);
+            if (flat > 1e-5f) bl.push_back({A.a, B.a, v2, v3, flat, bcomp, 1.f, std::fmax(flat * 0.5f, 0.01f)});
+          }
+        }
+      }
+      i = j;
+    }
+  }
   // ---- 1D strand bending (mesh.rs:840-905)
   {
     std::vector<uint64_t> fe;
@@ -315,6 +437,26 @@ MeshData build_mesh(const MeshInput& in) {
     for (size_t s = 0; s < perm.size(); ++s) m.bend[s] = bl[perm[s]];
   }
 
+  // ---- sewing constraints and their colouring (mesh.rs:904-936,
+  //      coloring.rs:236-300: Welsh-Powell as for distance constraints)
+  {
+    const float sk = in.sew_stiffness;
+    const float comp = sk >= 5000.f ? 0.f : (sk > 0.f ? 1.f / sk : 1e10f);
+    std::vector<SewC> sl;
+    for (uint32_t k = 0; k < in.nsew; ++k) {
+      const uint32_t a = in.sew[2 * size_t(k)], b = in.sew[2 * size_t(k) + 1];
+      if (a < n && b < n && a != b)
+        sl.push_back({a, b, len3(pv(a), pv(b)), 0.f, std::fmax(in.sew_shrink_speed, 0.f), comp, in.sew_lock ? 1.f : 0.f});
+    }
+    std::vector<std::vector<uint32_t>> verts(sl.size());
+    for (size_t i = 0; i < sl.size(); ++i) verts[i] = {sl[i].v0, sl[i].v1};
+    std::vector<uint32_t> color, perm;
+    const uint32_t ncol = sl.empty() ? 0 : welsh_powell(n, verts, verts, color);
+    bucket(color, ncol, m.sew_off, m.sew_cnt, perm);
+    m.sew.resize(sl.size());
+    for (size_t s2 = 0; s2 < perm.size(); ++s2) m.sew[s2] = sl[perm[s2]];
+  }
+
   // ---- adjacency and local edge length (mesh.rs:949-1090)
   std::vector<uint32_t> deg(n + 1, 0);
   std::vector<float> lsum(n, 0.f);
@@ -357,8 +499,71 @@ MeshData build_mesh(const MeshInput& in) {
     }
     m.adj_off[n] = uint32_t(m.adj_idx.size());
   }
-  // ---- two-hop CSR with rest lengths for true two-hop face pairs (mesh.rs:1092-1199)
+  // the adjacency of the input edges alone (sorted): two-hop rest lengths
+  // and the sewing contraction read it
+  const std::vector<uint32_t> orig_off = m.adj_off, orig_idx = m.adj_idx;
+  bool sewn = false;
+  for (uint32_t i = 0; i < n && !sewn; ++i) sewn = rep[i] != i;
+  // ---- sewing extends the adjacency (mesh.rs:990-1060): the members of a
+  //      group become neighbours of each other and of every neighbour of
+  //      any member, symmetrically
+  if (sewn) {
+    std::vector<std::vector<uint32_t>> lists(n), groups(n);
+    for (uint32_t i = 0; i < n; ++i) {
+      lists[i].assign(orig_idx.begin() + orig_off[i], orig_idx.begin() + orig_off[i + 1]);
+      groups[rep[i]].push_back(i);
+    }
+    for (const auto& g : groups)
+      if (g.size() > 1)
+        for (uint32_t u : g)
+          for (uint32_t v : g)
+            if (u != v) lists[u].push_back(v);
+    const std::vector<std::vector<uint32_t>> base = lists;
+    std::vector<uint32_t> shared;
+    for (const auto& g : groups) {
+      if (g.size() < 2) continue;
+      shared.clear();
+      for (uint32_t u : g)
+        for (uint32_t w : base[u])
+          if (rep[w] != rep[g[0]]) shared.push_back(w);
+      std::sort(shared.begin(), shared.end());
+      shared.erase(std::unique(shared.begin(), shared.end()), shared.end());
+      for (uint32_t u : g)
+        for (uint32_t w : shared) { lists[u].push_back(w); lists[w].push_back(u); }
+    }
+    m.adj_idx.clear();
+    for (uint32_t i = 0; i < n; ++i) {
+      auto& l = lists[i];
+      std::sort(l.begin(), l.end());
+      l.erase(std::unique(l.begin(), l.end()), l.end());
+      m.adj_off[i] = uint32_t(m.adj_idx.size());
+      m.adj_idx.insert(m.adj_idx.end(), l.begin(), l.end());
+    }
+    m.adj_off[n] = uint32_t(m.adj_idx.size());
+  }
+  // ---- two-hop CSR with rest lengths for true two-hop face pairs (mesh.rs:1092-1199).
+  //      With sewing, a pair is true two-hop when neither the same group
+  //      nor adjacent in the input mesh or in the group-contracted mesh; its
+  //      rest length is the plain distance when it is within two hops in
+  //      the input mesh, else the seam-unfolded one (seam_two_hop_rest).
   {
+    // one-hop sets of the contracted mesh, indexed by group
+    std::vector<std::vector<uint32_t>> chop;
+    if (sewn) {
+      chop.resize(n);
+      for (uint32_t e = 0; e < in.ne; ++e) {
+        const uint32_t a = in.edges[2 * size_t(e)], b = in.edges[2 * size_t(e) + 1];
+        if (a < n && b < n && a != b && rep[a] != rep[b]) {
+          chop[rep[a]].push_back(rep[b]);
+          chop[rep[b]].push_back(rep[a]);
+        }
+      }
+      for (auto& l : chop) {
+        std::sort(l.begin(), l.end());
+        l.erase(std::unique(l.begin(), l.end()), l.end());
+      }
+    }
+    std::vector<uint32_t> orig2;
     std::vector<uint8_t> isface(n, 0);
     for (uint32_t f = 0; f < in.nf; ++f)
       for (int k = 0; k < 3; ++k) {
@@ -378,12 +583,29 @@ MeshData build_mesh(const MeshInput& in) {
       std::sort(tmp.begin(), tmp.end());
       tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
       m.th_off[i] = uint32_t(m.th_idx.size());
-      const uint32_t* ab = m.adj_idx.data() + m.adj_off[i];
-      const uint32_t* ae = m.adj_idx.data() + m.adj_off[i + 1];
+      const uint32_t* ab = orig_idx.data() + orig_off[i];
+      const uint32_t* ae = orig_idx.data() + orig_off[i + 1];
+      if (sewn) {  // the input mesh's 0/1/2-hop set of i
+        orig2.assign(1, i);
+        for (const uint32_t* q = ab; q < ae; ++q) {
+          orig2.push_back(*q);
+          orig2.insert(orig2.end(), orig_idx.begin() + orig_off[*q], orig_idx.begin() + orig_off[*q + 1]);
+        }
+        std::sort(orig2.begin(), orig2.end());
+        orig2.erase(std::unique(orig2.begin(), orig2.end()), orig2.end());
+      }
       for (uint32_t nbr : tmp) {
         bool two = nbr != i && isface[i] && isface[nbr] && !std::binary_search(ab, ae, nbr);
+        if (sewn)
+          two = two && rep[i] != rep[nbr] &&
+                !std::binary_search(chop[rep[i]].begin(), chop[rep[i]].end(), rep[nbr]);
+        float rest = 0.f;
+        if (two)
+          rest = (!sewn || std::binary_search(orig2.begin(), orig2.end(), nbr))
+                     ? len3(pv(i), pv(nbr))
+                     : seam_two_hop_rest(i, nbr, P, orig_off, orig_idx, rep);
         m.th_idx.push_back(nbr);
-        m.th_rest.push_back(two ? len3(pv(i), pv(nbr)) : 0.f);
+        m.th_rest.push_back(rest);
       }
     }
     m.th_off[n] = uint32_t(m.th_idx.size());
@@ -470,12 +692,26 @@ MeshData build_mesh(const MeshInput& in) {
         }
       }
       std::sort(tk.begin(), tk.end());
+      // face edges counted between sewing groups (the contracted mesh)
+      std::vector<uint64_t> ck;
+      ck.reserve(tk.size());
+      for (uint64_t k : tk)
+        if (rep[klo(k)] != rep[khi(k)]) ck.push_back(key2(rep[klo(k)], rep[khi(k)]));
+      std::sort(ck.begin(), ck.end());
       for (size_t e = 0; e < ge.size(); ++e) {
+        const uint32_t ra = rep[klo(ge[e])], rb = rep[khi(ge[e])];
+        if (ra == rb) continue;  // an edge inside a sewing group
         auto r = std::equal_range(tk.begin(), tk.end(), ge[e]);
-        if (r.second - r.first <= 1) m.edge_bits[e >> 5] |= 1u << (e & 31);
+        bool open = r.second == r.first;  // a 1D strand edge
+        if (r.second - r.first == 1) {
+          auto c = std::equal_range(ck.begin(), ck.end(), key2(ra, rb));
+          open = c.second - c.first == 1;  // not matched by a sewn edge of another panel
+        }
+        if (open) m.edge_bits[e >> 5] |= 1u << (e & 31);
       }
     } else {
-      for (size_t e = 0; e < ge.size(); ++e) m.edge_bits[e >> 5] |= 1u << (e & 31);
+      for (size_t e = 0; e < ge.size(); ++e)
+        if (rep[klo(ge[e])] != rep[khi(ge[e])]) m.edge_bits[e >> 5] |= 1u << (e & 31);
     }
   }
   // ---- automatic layer per island by mean Z (pipelines.rs:131-167)

@@ -5,7 +5,9 @@
 // constraints, their Welsh-Powell colouring, the adjacency / two-hop / star
 // CSRs used by self-collision, the Morton-sorted unique edge list with its
 // open-boundary bits, islands and automatic layers, and the spatial-hash
-// sizing.  Semantics follow crates/cloth_core/src/mesh.rs:407-1377,
+// sizing; with sewing springs also the sewing constraints, the seam-gated
+// bending across sewn boundary edges, and the sewing-contracted adjacency,
+// two-hop and boundary data.  Semantics follow crates/cloth_core/src/mesh.rs:407-1377,
 // crates/cloth_core/src/coloring.rs:6-173 and
 // crates/cloth_core/src/simulation/pipelines.rs:131-167, :898-912.
 #pragma once
@@ -25,6 +27,14 @@ struct BendC {
   float rest, comp, pad0, pad1;  // pad0: 0 plain, 1 seam-gated, 2 strand
 };
 
+// Sewing spring (mesh.rs:904-933): pulled from its initial length towards
+// target_rest (0) at shrink_speed m/s.  compliance and lock are stored as
+// the reference stores them; the solve reads the simulator-level values.
+struct SewC {
+  uint32_t v0, v1;
+  float cur_rest, target_rest, shrink_speed, compliance, lock;
+};
+
 struct MeshInput {
   const float* pos = nullptr;  // n*3
   uint32_t n = 0;
@@ -38,6 +48,11 @@ struct MeshInput {
   uint32_t layer_id = 0;
   float thickness = 0.005f;
   float tension_k = 1000.f, compression_k = 1000.f, shear_k = 500.f, bending_k = 10.f;
+  const uint32_t* sew = nullptr;  // nsew*2 sewing springs (pairs of vertices)
+  uint32_t nsew = 0;
+  float sew_shrink_speed = 1.f;
+  float sew_stiffness = 10000.f;  // per-constraint compliance only
+  bool sew_lock = true;           // per-constraint lock flag only
 };
 
 struct MeshData {
@@ -49,6 +64,9 @@ struct MeshData {
   std::vector<int64_t> orig_edge_to_dist;  // input edge -> sorted constraint (-1 if none)
   std::vector<BendC> bend;             // colour-sorted
   std::vector<uint32_t> bend_off, bend_cnt;
+  std::vector<SewC> sew;               // colour-sorted
+  std::vector<uint32_t> sew_off, sew_cnt;
+  std::vector<uint32_t> sew_rep;       // sewing group of each vertex (its smallest index)
   std::vector<uint32_t> adj_off, adj_idx;
   std::vector<uint32_t> th_off, th_idx;
   std::vector<float> th_rest, local_len;

@@ -426,6 +426,68 @@ struct Sim {
   unsigned int spin_limit = 1u << 22;  // ~0.5 s of polling per barrier
   DBuf<GridBar> bar;
   DBuf<uint32_t> dist_offc, dist_cntc, bend_offc, bend_cntc;
+  // sewing (mesh.rs:904-936; settings dispatch.rs:29-35, simulation/mod.rs:1211-1420)
+  uint32_t nsw = 0;
+  std::vector<SewC> sew_h;              // colour-sorted, as uploaded
+  DBuf<uint2> sew_ids;
+  DBuf<float2> sew_rest;                // (current, target)
+  DBuf<float> slam;
+  DBuf<uint32_t> sew_offc, sew_cntc;
+  float sew_stiffness = 10000.f, sew_speed = 1.f, sew_lock_dist = 0.02f;
+  bool sew_lock = true;
+  // sewing priority: gravity held at 0 until the seams close, then ramped
+  // back over ramp_frames frames (simulation/mod.rs:1257-1420)
+  struct SewPriority {
+    bool enabled = false;
+    float threshold = 0.9f, merge = 0.005f;
+    uint32_t ramp_frames = 3, max_frames = 600;
+    bool latched = false;
+    uint32_t frame = 0;
+    float ramp_t = 0.f, ratio = 0.f;
+  } pri;
+  float priority_scale() const {  // sewing_priority_scale (mod.rs:1359-1371)
+    if (!pri.enabled || nsw == 0) return 1.f;
+    if (!pri.latched) return 0.f;
+    if (pri.ramp_frames == 0) return 1.f;
+    const float x = std::fmin(std::fmax(pri.ramp_t, 0.f), 1.f);
+    return x * x * (3.0f - 2.0f * x);
+  }
+  SewParams sew_params() const {
+    return SewParams{sew_stiffness >= 5000.f ? 0.f : 1.f / std::fmax(sew_stiffness, 1.f), sew_lock ? 1.f : 0.f,
+                     sew_lock_dist};
+  }
+  // substep parameters of a frame: gravity scaled by the sewing priority
+  SubstepParams make_sp(float dts) const {
+    const float k = priority_scale();
+    return SubstepParams{dts, g[0] * k, g[1] * k, g[2] * k, damping, td, cd, sd, bd};
+  }
+  void upload_sew() {
+    std::vector<uint2> ids(nsw);
+    std::vector<float2> rest(nsw);
+    for (uint32_t i = 0; i < nsw; ++i) {
+      ids[i] = make_uint2(sew_h[i].v0, sew_h[i].v1);
+      rest[i] = make_float2(sew_h[i].cur_rest, sew_h[i].target_rest);
+    }
+    sew_ids.upload(ids, st);
+    sew_rest.upload(rest, st);
+    slam.alloc(nsw);
+    sew_offc.upload(m.sew_off, st);
+    sew_cntc.upload(m.sew_cnt, st);
+  }
+  // per-colour sewing projection (the iteration's pass, or the final one)
+  void launch_sewing(float dts, const unsigned int* gate = nullptr) {
+    const SewParams sw = sew_params();
+    for (size_t c = 0; c < m.sew_cnt.size(); ++c)
+      if (m.sew_cnt[c])
+        launch_k(k_sewing, grid(m.sew_cnt[c], 256), 256, m.sew_off[c], m.sew_cnt[c], (const uint2*)sew_ids.p,
+                 sew_rest.p, (const float4*)x4.p, p4.p, slam.p, dts, sw, gate);
+  }
+  // at the start of a substep: sewing lambdas cleared, rest lengths shrunk
+  void launch_sew_start(float dts) {
+    if (!nsw) return;
+    TC_CK(cudaMemsetAsync(slam.p, 0, nsw * sizeof(float), st));
+    launch_k(k_sew_shrink, grid(nsw, 256), 256, nsw, sew_rest.p, sew_speed, dts);
+  }
   int* h_err = nullptr;  // pinned
   WarmStart ws;
   BoneSdfState bone;
@@ -654,6 +716,10 @@ struct Sim {
     prims.alloc(1); tris.alloc(1); bounds.alloc(1); cl16.alloc(1); cl256.alloc(1);
     dist_offc.upload(m.dist_off, st); dist_cntc.upload(m.dist_cnt, st);
     bend_offc.upload(m.bend_off, st); bend_cntc.upload(m.bend_cnt, st);
+    sew_h = m.sew;
+    nsw = uint32_t(sew_h.size());
+    sew_speed = std::fmax(in.sew_shrink_speed, 0.f);
+    upload_sew();
     bar.alloc(2);
     TC_CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(GridBar), st));
     TC_CK(cudaHostAlloc(&h_err, sizeof(int), cudaHostAllocDefault));
@@ -1042,12 +1108,21 @@ struct Sim {
     a.dprev = nullptr;
     a.iters_extra = 0;
     a.res_thresh = 0.f;
+    a.res_ratio = 0.f;
+    a.res_floor = 0.f;
+    a.res_pred = nullptr;
+    a.nsw = nsw;
+    a.nsc = uint32_t(m.sew_cnt.size());
+    a.sew_ids = sew_ids.p; a.sew_rest = sew_rest.p; a.slam = slam.p;
+    a.sew_off = sew_offc.p; a.sew_cnt = sew_cntc.p;
+    a.sew_speed = sew_speed;
+    a.sw = sew_params();
     a.res_part = nullptr;
     a.res_out = nullptr;
     a.fallbacks = nullptr;
     return a;
   }
-  bool can_cluster() const { return !inst_vert_off.empty() && cl_max_active > 0 && !self_collision; }
+  bool can_cluster() const { return !inst_vert_off.empty() && cl_max_active > 0 && !self_collision && nsw == 0; }
   // bins: contiguous runs of instances, balanced by vertex count; the
   // constraint permutations are sorted by (bin, colour, original index)
   void build_cluster_tables() {
@@ -1197,7 +1272,7 @@ struct Sim {
   // the per-colour launch mode, the per-colour kernels with the residual
   // check on the device and the fallback iterations gated by its flag.
   void encode_frame_ws(float dt, uint32_t substeps, bool use_coupled) {
-    const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
+    const SubstepParams sp = make_sp(dt / float(substeps));
     const uint32_t itn = run_iters();
     const uint32_t kk = std::min(ws.k, itn > 1 ? itn - 1 : 0u);
     const WsFeatArgs fa = ws_feat_args(sp, nullptr);
@@ -1226,8 +1301,10 @@ struct Sim {
       }
       if (self_collision) {
         if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
+        if (nsw) timed("final_sewing", [&] { launch_sewing(sp.dt); });
         timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp.dt); });
       } else if (colors) {
+        if (nsw) timed("final_sewing", [&] { launch_sewing(sp.dt); });
         timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp.dt); });
       }
     }
@@ -1269,6 +1346,7 @@ struct Sim {
     const bool bone_col = ca.bone.nbones > 0;
     if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
     if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
+    timed("sew_shrink", [&] { launch_sew_start(dts); });
     timed("predict", [&] { launch_k(k_predict, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp); });
     timed("ws_check", [&] { encode_ws_res_pred(dts, bone_col); });
     timed("ws_mlp", [&] { ws.net.infer(nullptr, &fa, ws.ppred.p, nullptr, x4.p, p4.p, local_len.p); });
@@ -1286,6 +1364,7 @@ struct Sim {
             launch_k(k_distance, grid(m.dist_cnt[c], 256), 256, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
                      dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
         }
+      if (nsw) launch_sewing(dts, gate);
       for (size_t c = 0; c < m.bend_cnt.size(); ++c)
         if (m.bend_cnt[c]) {
           if (gate)
@@ -1389,19 +1468,20 @@ struct Sim {
       return;
     }
     if (cluster_mode && can_cluster() && !cl_stale && !profiling && !track_residual && !ws_recording()) {
-      const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
+      const SubstepParams sp = make_sp(dt / float(substeps));
       launch_cluster(solver_args(sp, substeps, use_coupled, true));
       TC_CK(cudaGetLastError());
       return;
     }
     if (persistent && can_persist() && !profiling && !track_residual && !ws_recording()) {
-      const SubstepParams sp{dt / float(substeps), g[0], g[1], g[2], damping, td, cd, sd, bd};
+      const SubstepParams sp = make_sp(dt / float(substeps));
       if (!self_collision) {
         launch_persistent(solver_args(sp, substeps, use_coupled, true));
       } else {
         for (uint32_t s = 0; s < substeps; ++s) {
           launch_persistent(solver_args(sp, 1, use_coupled, false));
           if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
+          launch_sewing(sp.dt);  // final sewing (dispatch.rs:323-337)
           k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp.dt);
         }
       }
@@ -1410,7 +1490,7 @@ struct Sim {
       return;
     }
     const float dts = dt / float(substeps);
-    SubstepParams sp{dts, g[0], g[1], g[2], damping, td, cd, sd, bd};
+    SubstepParams sp = make_sp(dts);
     const bool ddamp = td != 0.f || cd != 0.f || sd != 0.f;
     const bool bdamp = bd != 0.f;
     const bool hascol = has_colliders();
@@ -1419,6 +1499,7 @@ struct Sim {
     for (uint32_t s = 0; s < substeps; ++s) {
       if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
       if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
+      timed("sew_shrink", [&] { launch_sew_start(dts); });
       timed("predict", [&] { launch_k(k_predict, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp); });
       if (track_residual && s + 1 == substeps && nd + nb)
         k_residual_pred<<<grid(nd + nb, 256), 256, 0, st>>>(nd, nb, dist_ids.p, dist_par.p, bend_ids.p, bend_par.p,
@@ -1442,6 +1523,7 @@ struct Sim {
               launch_k(k_distance, grid(m.dist_cnt[c], 256), 256, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
                        dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
         });
+        if (nsw) timed("sewing", [&] { launch_sewing(dts); });
         timed("bending", [&] {
           for (size_t c = 0; c < m.bend_cnt.size(); ++c)
             if (m.bend_cnt[c])
@@ -1460,6 +1542,7 @@ struct Sim {
       if (hascol && !use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
       if (npins) timed("pin", [&] { launch_k(k_pin, grid(npins, 128), 128, npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
       if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
+      if (nsw) timed("final_sewing", [&] { launch_sewing(dts); });
       timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, dts); });
     }
     TC_CK(cudaGetLastError());
@@ -1738,6 +1821,20 @@ tc_status tc_create(tc_sim** out, const float* positions, uint32_t n, const uint
                     const uint32_t* faces, uint32_t nf, const float* inv_masses, const uint32_t* layer_ids,
                     const float* thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
                     float compression_stiffness, float shear_stiffness, float bending_stiffness, int device) {
+  return tc_create_sewn(out, positions, n, edges, ne, faces, nf, inv_masses, layer_ids, thicknesses, layer_id,
+                        thickness, tension_stiffness, compression_stiffness, shear_stiffness, bending_stiffness,
+                        nullptr, 0, 1.0f, 10000.0f, 1, 0.02f, device);
+}
+static void need_sewing(const uint32_t* sewing, uint32_t nsew, uint32_t n) {
+  need(sewing != nullptr || nsew == 0, "sewing springs required");
+  for (uint32_t k = 0; k < 2 * nsew; ++k) need(sewing[k] < n, "sewing springs contain an index >= number of vertices");
+}
+tc_status tc_create_sewn(tc_sim** out, const float* positions, uint32_t n, const uint32_t* edges, uint32_t ne,
+                         const uint32_t* faces, uint32_t nf, const float* inv_masses, const uint32_t* layer_ids,
+                         const float* thicknesses, uint32_t layer_id, float thickness, float tension_stiffness,
+                         float compression_stiffness, float shear_stiffness, float bending_stiffness,
+                         const uint32_t* sewing, uint32_t nsew, float sewing_shrink_speed, float sewing_stiffness,
+                         int enable_sewing_lock, float sewing_lock_distance, int device) {
   return guard([&] {
     need(out != nullptr, "out handle required");
     *out = nullptr;
@@ -1759,8 +1856,13 @@ tc_status tc_create(tc_sim** out, const float* positions, uint32_t n, const uint
     in.layer_id = layer_id; in.thickness = thickness;
     in.tension_k = tension_stiffness; in.compression_k = compression_stiffness;
     in.shear_k = shear_stiffness; in.bending_k = bending_stiffness;
+    need_sewing(sewing, nsew, n);
+    in.sew = sewing; in.nsew = nsew; in.sew_shrink_speed = sewing_shrink_speed;
+    in.sew_stiffness = std::isnan(sewing_stiffness) ? 10000.0f : sewing_stiffness;
+    in.sew_lock = enable_sewing_lock != 0;
     std::unique_ptr<tc_sim> h(new tc_sim);
     h->s.init(in, device);
+    if (!std::isnan(sewing_lock_distance)) h->s.sew_lock_dist = std::fmax(sewing_lock_distance, 0.f);
     *out = h.release();
   });
 }
@@ -1935,7 +2037,129 @@ tc_status tc_reset(tc_sim* s) {
     std::fill(m.mult.begin(), m.mult.end(), 1.f);
     m.apply_distance_compliances();
     TC_CK(cudaMemsetAsync(m.acc.p, 0, size_t(m.n) * tcloth::A_N * sizeof(int32_t), m.st));
+    m.pri.latched = false;  // sewing priority restarts (dispatch.rs:1414-1417)
+    m.pri.frame = 0;
+    m.pri.ramp_t = 0.f;
+    m.pri.ratio = 0.f;
+    m.mark();
     TC_CK(cudaStreamSynchronize(m.st));
+  });
+}
+
+// ---- sewing settings (simulation/mod.rs:1211-1420, lib.rs:2798-2925)
+tc_status tc_get_num_sewing_constraints(tc_sim* s, uint32_t* count) {
+  return guard([&] { need(count != nullptr, "count required"); *count = S(s).nsw; });
+}
+tc_status tc_set_sewing_stiffness(tc_sim* s, float stiffness) {
+  return guard([&] { Sim& m = S(s); m.sew_stiffness = std::fmax(stiffness, 1.f); m.mark(); });
+}
+tc_status tc_set_sewing_shrink_speed(tc_sim* s, float speed) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.sew_speed = std::isfinite(speed) ? std::fmax(speed, 0.f) : 1.f;
+    m.mark();
+  });
+}
+tc_status tc_get_sewing_shrink_speed(tc_sim* s, float* speed) {
+  return guard([&] { need(speed != nullptr, "speed required"); *speed = S(s).sew_speed; });
+}
+tc_status tc_set_enable_sewing_lock(tc_sim* s, int enabled) {
+  return guard([&] { Sim& m = S(s); m.sew_lock = enabled != 0; m.mark(); });
+}
+tc_status tc_set_sewing_lock_distance(tc_sim* s, float distance) {
+  return guard([&] { Sim& m = S(s); m.sew_lock_dist = std::fmax(distance, 0.f); m.mark(); });
+}
+tc_status tc_get_sewing_lock_distance(tc_sim* s, float* distance) {
+  return guard([&] { need(distance != nullptr, "distance required"); *distance = S(s).sew_lock_dist; });
+}
+tc_status tc_get_sewing_current_rest_lengths(tc_sim* s, float* out, size_t len) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr || m.nsw == 0, "output required");
+    need(len >= m.nsw, "output array too small");
+    std::vector<float2> r(m.nsw);
+    if (m.nsw) TC_CK(cudaMemcpyAsync(r.data(), m.sew_rest.p, m.nsw * sizeof(float2), cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    for (uint32_t i = 0; i < m.nsw; ++i) out[i] = r[i].x;
+  });
+}
+tc_status tc_set_sewing_current_rest_lengths(tc_sim* s, const float* values, size_t len) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (values == nullptr || len != m.nsw || len == 0) return;  // ignored, as the reference does (dispatch.rs:928-932)
+    std::vector<float2> r(m.nsw);
+    TC_CK(cudaMemcpyAsync(r.data(), m.sew_rest.p, m.nsw * sizeof(float2), cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    for (uint32_t i = 0; i < m.nsw; ++i) r[i].x = values[i];
+    TC_CK(cudaMemcpyAsync(m.sew_rest.p, r.data(), m.nsw * sizeof(float2), cudaMemcpyHostToDevice, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+  });
+}
+tc_status tc_set_sewing_priority_options(tc_sim* s, int enabled, float threshold, float merge_dist,
+                                         uint32_t ramp_frames, uint32_t max_frames) {
+  return guard([&] {
+    Sim& m = S(s);
+    auto& p = m.pri;
+    const float th = std::fmin(std::fmax(threshold, 0.f), 1.f), md = std::fmin(std::fmax(merge_dist, 0.0005f), 0.1f);
+    const uint32_t rf = std::min(ramp_frames, 120u), mf = std::min(max_frames, 100000u);
+    if (p.enabled == (enabled != 0) && p.threshold == th && p.merge == md && p.ramp_frames == rf && p.max_frames == mf)
+      return;  // unchanged: the latch is kept
+    p.enabled = enabled != 0; p.threshold = th; p.merge = md; p.ramp_frames = rf; p.max_frames = mf;
+    p.latched = false; p.frame = 0; p.ramp_t = 0.f; p.ratio = 0.f;
+    m.mark();
+  });
+}
+tc_status tc_set_sewing_priority_state(tc_sim* s, int latched, uint32_t frame, float ramp_t, float ratio) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.pri.latched = latched != 0;
+    m.pri.frame = frame;
+    m.pri.ramp_t = std::fmin(std::fmax(ramp_t, 0.f), 1.f);
+    m.pri.ratio = std::fmin(std::fmax(ratio, 0.f), 1.f);
+    m.mark();
+  });
+}
+// update_sewing_priority_from_positions (mod.rs:1323-1356): the share of
+// sewing pairs within merge_dist in `positions` (host data, no readback),
+// then the one-way latch and the ramp.  out = (ratio, gravity scale, latched).
+tc_status tc_update_sewing_priority(tc_sim* s, const float* positions, uint32_t n, float out[3]) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr, "out required");
+    auto& p = m.pri;
+    if (!p.enabled || m.nsw == 0) { out[0] = 1.f; out[1] = 1.f; out[2] = 1.f; return; }
+    need(positions != nullptr || n == 0, "positions required");
+    const float msq = p.merge * p.merge;
+    size_t closed = 0, total = 0;
+    for (const auto& c : m.sew_h) {
+      if (c.v0 >= n || c.v1 >= n) continue;
+      ++total;
+      const float* a = positions + 3 * size_t(c.v0);
+      const float* b = positions + 3 * size_t(c.v1);
+      const float dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+      if (dx * dx + dy * dy + dz * dz <= msq) ++closed;
+    }
+    const float ratio = total ? float(closed) / float(total) : 1.f;
+    p.ratio = ratio;
+    p.frame = p.frame == UINT32_MAX ? p.frame : p.frame + 1;
+    if (!p.latched && (ratio >= p.threshold || (p.max_frames > 0 && p.frame >= p.max_frames))) p.latched = true;
+    if (p.latched && p.ramp_frames > 0) p.ramp_t = std::fmin(p.ramp_t + 1.0f / float(p.ramp_frames), 1.0f);
+    else if (p.latched) p.ramp_t = 1.f;
+    else p.ramp_t = 0.f;
+    m.mark();
+    out[0] = ratio; out[1] = m.priority_scale(); out[2] = p.latched ? 1.f : 0.f;
+  });
+}
+// (gravity scale, last closure ratio, priority active = gravity held, latched)
+tc_status tc_get_sewing_priority(tc_sim* s, float out[4]) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(out != nullptr, "out required");
+    const bool on = m.pri.enabled && m.nsw > 0;
+    out[0] = m.priority_scale();
+    out[1] = on ? m.pri.ratio : 1.f;
+    out[2] = on && !m.pri.latched ? 1.f : 0.f;
+    out[3] = m.pri.latched ? 1.f : 0.f;
   });
 }
 
@@ -2231,6 +2455,14 @@ tc_status tc_mesh_build(tc_mesh** out, const float* positions, uint32_t n, const
                         const uint32_t* faces, uint32_t nf, const float* inv_masses, const uint32_t* layer_ids,
                         const float* thicknesses, uint32_t layer_id, float thickness, float tk, float ck, float sk,
                         float bk) {
+  return tc_mesh_build_sewn(out, positions, n, edges, ne, faces, nf, inv_masses, layer_ids, thicknesses, layer_id,
+                            thickness, tk, ck, sk, bk, nullptr, 0, 1.0f, 10000.0f, 1);
+}
+tc_status tc_mesh_build_sewn(tc_mesh** out, const float* positions, uint32_t n, const uint32_t* edges, uint32_t ne,
+                             const uint32_t* faces, uint32_t nf, const float* inv_masses, const uint32_t* layer_ids,
+                             const float* thicknesses, uint32_t layer_id, float thickness, float tk, float ck,
+                             float sk, float bk, const uint32_t* sewing, uint32_t nsew, float sewing_shrink_speed,
+                             float sewing_stiffness, int enable_sewing_lock) {
   return guard([&] {
     need(out != nullptr, "out handle required");
     *out = nullptr;
@@ -2243,6 +2475,10 @@ tc_status tc_mesh_build(tc_mesh** out, const float* positions, uint32_t n, const
     in.inv_masses = inv_masses; in.layer_ids = layer_ids; in.thicknesses = thicknesses;
     in.layer_id = layer_id; in.thickness = thickness;
     in.tension_k = tk; in.compression_k = ck; in.shear_k = sk; in.bending_k = bk;
+    need_sewing(sewing, nsew, n);
+    in.sew = sewing; in.nsew = nsew; in.sew_shrink_speed = sewing_shrink_speed;
+    in.sew_stiffness = std::isnan(sewing_stiffness) ? 10000.0f : sewing_stiffness;
+    in.sew_lock = enable_sewing_lock != 0;
     std::unique_ptr<tc_mesh> h(new tc_mesh);
     h->m = tcloth::build_mesh(in);
     *out = h.release();
@@ -2280,6 +2516,26 @@ tc_status tc_mesh_constraints(tc_mesh* h, uint32_t* dv, float* dp, uint32_t* dof
     if (dcnt) std::copy(m.dist_cnt.begin(), m.dist_cnt.end(), dcnt);
     if (boff) std::copy(m.bend_off.begin(), m.bend_off.end(), boff);
     if (bcnt) std::copy(m.bend_cnt.begin(), m.bend_cnt.end(), bcnt);
+  });
+}
+tc_status tc_mesh_sewing(tc_mesh* h, uint32_t* nsew, uint32_t* ncolors, uint32_t* v01, float* par, uint32_t* off,
+                         uint32_t* cnt, uint32_t* rep) {
+  return guard([&] {
+    need(h != nullptr, "handle required");
+    const auto& m = h->m;
+    if (nsew) *nsew = uint32_t(m.sew.size());
+    if (ncolors) *ncolors = uint32_t(m.sew_cnt.size());
+    for (size_t i = 0; i < m.sew.size(); ++i) {
+      const auto& c = m.sew[i];
+      if (v01) { v01[2 * i] = c.v0; v01[2 * i + 1] = c.v1; }
+      if (par) {
+        par[5 * i] = c.cur_rest; par[5 * i + 1] = c.target_rest; par[5 * i + 2] = c.shrink_speed;
+        par[5 * i + 3] = c.compliance; par[5 * i + 4] = c.lock;
+      }
+    }
+    if (off) std::copy(m.sew_off.begin(), m.sew_off.end(), off);
+    if (cnt) std::copy(m.sew_cnt.begin(), m.sew_cnt.end(), cnt);
+    if (rep) std::copy(m.sew_rep.begin(), m.sew_rep.end(), rep);
   });
 }
 tc_status tc_mesh_topology_sizes(tc_mesh* h, uint32_t* a, uint32_t* t, uint32_t* s) {

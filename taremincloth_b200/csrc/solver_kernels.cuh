@@ -218,6 +218,70 @@ __global__ void k_bending(uint32_t off, uint32_t cnt, const uint4* __restrict__ 
   project_bending<false>(off + k, ids, par, x4, p4, lam, sp, damped);
 }
 
+// Sewing settings of a frame (dispatch.rs:29-35): compliance 0 when the
+// simulator's sewing stiffness is >= 5000, else 1 / max(stiffness, 1);
+// lock > 0.5 latches a closing seam; lock_dist its distance floor.
+struct SewParams {
+  float compliance, lock, lock_dist;
+};
+// Shrink of the sewing rest lengths, once per substep before predict
+// (shaders/sewing_shrink.wgsl:38-49).  rest = (current, target).
+__global__ void k_sew_shrink(uint32_t cnt, float2* __restrict__ rest, float speed, float dt_sub) {
+  pdl_enter();
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cnt) return;
+  float2 r = rest[k];
+  const float dt = fmaxf(dt_sub, 1e-8f);
+  r.x = fmaxf(r.y, r.x - speed * dt);
+  rest[k] = r;
+}
+// One sewing constraint (shaders/sewing.wgsl:57-110): XPBD towards the
+// current rest length; within max(thickness sum, lock distance) with the
+// lock on, a hard constraint towards the target length, which also becomes
+// the current one.
+template <bool kCg>
+__device__ __forceinline__ void project_sewing(uint32_t ci, const uint2* __restrict__ ids, float2* __restrict__ rest,
+                                               const float4* __restrict__ x4, float4* __restrict__ p4,
+                                               float* __restrict__ lam, float dt_sub, const SewParams& sw) {
+  const uint2 e = ids[ci];
+  const float4 xa = ld4<kCg>(x4 + e.x), xb = ld4<kCg>(x4 + e.y);
+  const float4 qa = ld4<kCg>(p4 + e.x), qb = ld4<kCg>(p4 + e.y);
+  const float w0 = xa.w, w1 = xb.w;
+  const float ws = w0 + w1;
+  if (ws <= kEps) return;
+  const V3 p0 = mk(qa), p1 = mk(qb);
+  const V3 delta = p0 - p1;
+  const float dist = length(delta);
+  if (dist <= kEps) return;
+  const float dt = fmaxf(dt_sub, 1e-8f);
+  const V3 dir = delta / dist;
+  const float2 r = kCg ? __ldcg(rest + ci) : rest[ci];
+  float target = r.x, comp = sw.compliance;
+  const float lock_thresh = fmaxf(qa.w + qb.w, sw.lock_dist);
+  if (sw.lock > 0.5f && dist <= lock_thresh) {
+    comp = 0.0f;
+    target = r.y;
+    rest[ci] = make_float2(r.y, r.y);
+  }
+  const float alpha = comp / (dt * dt);
+  const float cv = dist - target;
+  const float l = ld1<kCg>(lam + ci);
+  const float dl = (-cv - alpha * l) / (ws + alpha);
+  lam[ci] = l + dl;
+  const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
+  p4[e.x] = make_float4(n0.x, n0.y, n0.z, qa.w);
+  p4[e.y] = make_float4(n1.x, n1.y, n1.z, qb.w);
+}
+// gate: null, or the warm start's fallback flag (skipped unless set)
+__global__ void k_sewing(uint32_t off, uint32_t cnt, const uint2* __restrict__ ids, float2* __restrict__ rest,
+                         const float4* __restrict__ x4, float4* __restrict__ p4, float* __restrict__ lam,
+                         float dt_sub, SewParams sw, const unsigned int* gate) {
+  pdl_enter();
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cnt || (gate && !*gate)) return;
+  project_sewing<false>(off + k, ids, rest, x4, p4, lam, dt_sub, sw);
+}
+
 // shaders/update_vel.wgsl:33-53
 template <bool kCg>
 __device__ __forceinline__ void update_vertex(uint32_t i, float4* __restrict__ x4, const float4* __restrict__ p4,
@@ -523,6 +587,17 @@ struct SolverArgs {
   const uint32_t* pin_v;
   const float4* pin_t;
   ColliderArgs ca;
+  // sewing: shrink at the start of each substep, the nsc colours after the
+  // distance colours of every iteration, and, with with_update, once more
+  // after the final pins (the final sewing pass before the velocity update)
+  uint32_t nsw, nsc;
+  const uint2* sew_ids;
+  float2* sew_rest;
+  float* slam;
+  const uint32_t* sew_off;
+  const uint32_t* sew_cnt;
+  float sew_speed;
+  SewParams sw;
   GridBar* bar;
   unsigned int expected;  // arrivals per barrier
   unsigned int spin_limit;
@@ -707,6 +782,12 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
   for (uint32_t sub = 0; sub < a.nsub; ++sub) {
     for (uint32_t i = tid; i < a.nd; i += stride) a.dlam[i] = 0.f;
     for (uint32_t i = tid; i < a.nb; i += stride) a.blam[i] = 0.f;
+    for (uint32_t i = tid; i < a.nsw; i += stride) {
+      a.slam[i] = 0.f;
+      float2 r = __ldcg(a.sew_rest + i);
+      r.x = fmaxf(r.y, r.x - a.sew_speed * fmaxf(dts, 1e-8f));
+      a.sew_rest[i] = r;
+    }
     if (!a.skip_predict)
       for (uint32_t i = tid; i < a.n; i += stride) predict_vertex<true>(i, a.x4, a.p4, a.v4, a.sp);
     if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
@@ -721,6 +802,13 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
         if (!cnt) continue;
         for (uint32_t k = tid; k < cnt; k += stride)
           project_distance<true>(off + k, a.dist_ids, a.dist_par, a.x4, a.p4, a.dlam, a.sp, a.ddamp);
+        if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+      }
+      for (uint32_t c = 0; c < a.nsc; ++c) {
+        const uint32_t off = a.sew_off[c], cnt = a.sew_cnt[c];
+        if (!cnt) continue;
+        for (uint32_t k = tid; k < cnt; k += stride)
+          project_sewing<true>(off + k, a.sew_ids, a.sew_rest, a.x4, a.p4, a.slam, dts, a.sw);
         if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
       }
       for (uint32_t c = 0; c < a.nbc; ++c) {
@@ -770,6 +858,14 @@ __global__ void __launch_bounds__(256) k_solver_persistent(SolverArgs a) {
       for (uint32_t k = tid; k < a.npins; k += stride) pin_one<true>(k, a.pin_v, a.pin_t, a.x4, a.p4, dts);
       if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
     }
+    if (a.with_update)  // final sewing (dispatch.rs:323-337); with self-collision it runs after it, outside
+      for (uint32_t c = 0; c < a.nsc; ++c) {
+        const uint32_t off = a.sew_off[c], cnt = a.sew_cnt[c];
+        if (!cnt) continue;
+        for (uint32_t k = tid; k < cnt; k += stride)
+          project_sewing<true>(off + k, a.sew_ids, a.sew_rest, a.x4, a.p4, a.slam, dts, a.sw);
+        if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;
+      }
     if (a.with_update) {
       for (uint32_t i = tid; i < a.n; i += stride) update_vertex<true>(i, a.x4, a.p4, a.v4, dts);
       if (!grid_sync(a.bar, a.expected, a.spin_limit)) return;

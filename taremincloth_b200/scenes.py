@@ -158,8 +158,44 @@ def config2(n=256, seed=0, side=1.0, subdiv=5):
         self_collision=True, dt=1.0 / 60.0, substeps=20, iterations=4, frames=30)
 
 
+def sewn_garment(n=24, side=0.3, gap=0.06, seed=0):
+    """Front and back panels (n x n vertices each, two triangles per quad,
+    hanging in XY, `gap` apart in Z) sewn along both side columns into a
+    tube; the top corners of each panel pinned; self-collision on."""
+    rng = np.random.default_rng(seed)
+    ps, es, fs = [], [], []
+    for k in range(2):
+        p, e, f, idx = tri_grid(n, side, 0.0, k * n * n, flip=k == 1)
+        q = np.zeros_like(p)
+        q[:, 0] = p[:, 0]
+        q[:, 1] = 1.0 - p[:, 2]          # rows hang downwards from y = 1
+        q[:, 2] = k * gap
+        ps.append(q)
+        es.append(e)
+        fs.append(f)
+    pos = np.concatenate(ps).astype(F)
+    pos[:, 2] += rng.uniform(-1e-4, 1e-4, len(pos)).astype(F)
+    grid = np.arange(n * n).reshape(n, n)
+    sides = np.concatenate([grid[:, 0], grid[:, -1]])
+    sewing = np.stack([sides, sides + n * n], 1).astype(np.uint32)
+    faces = np.concatenate(fs)
+    inv = areal_inv_masses(pos, faces, 0.15)
+    pins = []
+    for k in range(2):
+        for v in (int(grid[0, 0]) + k * n * n, int(grid[0, -1]) + k * n * n):
+            pins.append((v, pos[v].copy()))
+    return dict(
+        name=f"sewn_garment_{n}", positions=pos, edges=np.concatenate(es), faces=faces, inv_masses=inv,
+        layer_ids=None, thickness=0.002, compliance=(1e-8, 1e-8, 1e-6, 1e-5), gravity=(0.0, -9.81, 0.0),
+        pins=pins, spheres=[], mesh=None, self_collision=True, dt=1.0 / 60.0, substeps=10, iterations=4,
+        frames=12, sewing=sewing, sewing_shrink_speed=0.5)
+
+
 def build(sim_cls, scene, **kw):
     """Construct a simulator (product or oracle) from a scene dict."""
+    if scene.get("sewing") is not None:
+        kw.setdefault("sewing_springs", scene["sewing"])
+        kw.setdefault("sewing_shrink_speed", scene.get("sewing_shrink_speed", 1.0))
     s = sim_cls(scene["positions"], scene["edges"], scene["faces"], scene["inv_masses"],
                 layer_ids=scene.get("layer_ids"), thickness=scene["thickness"], **kw)
     s.set_gravity(*scene["gravity"])

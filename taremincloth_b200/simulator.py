@@ -107,8 +107,16 @@ class ClothSimulator:
         self._h = None
         pos = _arr(positions, _f32, 3, "positions")
         e = _arr(edges, _u32, 2, "edges")
-        if sewing_springs is not None and len(np.asarray(sewing_springs)) > 0:
-            raise NotImplementedError("sewing springs are not part of this substep build")
+        sew = None
+        if sewing_springs is not None:
+            sa = np.asarray(sewing_springs)
+            if sa.ndim != 2 or sa.shape[1] != 2:
+                raise ValueError("each sewing_springs row must be a vertex pair (v0, v1)")
+            sew = np.ascontiguousarray(sa, dtype=_u32)
+            if sew.size and int(sew.max()) >= pos.shape[0]:
+                bad = sew[(sew >= pos.shape[0]).any(axis=1)][0]
+                raise ValueError(f"sewing_springs contains an index >= the vertex count ({pos.shape[0]}): "
+                                 f"[{bad[0]}, {bad[1]}]")
         if solver_mode not in (0,):
             raise NotImplementedError("only the graph-coloured solver (solver_mode=0) is built")
         f = _arr(faces, _u32, 3, "faces") if faces is not None else None
@@ -129,9 +137,15 @@ class ClothSimulator:
         shear = stiffness * 0.5 if shear_stiffness is None else shear_stiffness
         h = C.c_void_p()
         nf = 0 if f is None else f.shape[0]
-        _lib.check(L.tc_create(C.byref(h), _ptr(pos), n, _ptr(e), e.shape[0], _ptr(f), nf, _ptr(im), _ptr(li),
-                               _ptr(th), int(layer_id), float(thickness), float(stiffness), float(comp),
-                               float(shear), float(bending_stiffness), int(device)))
+        nsew = 0 if sew is None else sew.shape[0]
+        _lib.check(L.tc_create_sewn(C.byref(h), _ptr(pos), n, _ptr(e), e.shape[0], _ptr(f), nf, _ptr(im), _ptr(li),
+                                    _ptr(th), int(layer_id), float(thickness), float(stiffness), float(comp),
+                                    float(shear), float(bending_stiffness), _ptr(sew), nsew,
+                                    float(sewing_shrink_speed),
+                                    float("nan") if sewing_stiffness is None else float(sewing_stiffness),
+                                    1 if enable_sewing_lock is None else int(bool(enable_sewing_lock)),
+                                    float("nan") if sewing_lock_distance is None else float(sewing_lock_distance),
+                                    int(device)))
         self._h = h
         self._L = L
         self._n = n
@@ -178,6 +192,72 @@ class ClothSimulator:
     def get_positions(self, out_array):
         out = self._out(out_array)
         self._c(self._L.tc_get_positions(self._h, _ptr(out), out.size))
+
+    # ---------------- sewing (lib.rs:2798-2925)
+    def get_num_sewing_constraints(self):
+        v = C.c_uint32()
+        self._c(self._L.tc_get_num_sewing_constraints(self._h, C.byref(v)))
+        return v.value
+
+    def set_sewing_stiffness(self, stiffness=10000.0):
+        self._c(self._L.tc_set_sewing_stiffness(self._h, float(stiffness)))
+
+    def set_sewing_shrink_speed(self, speed=1.0):
+        self._c(self._L.tc_set_sewing_shrink_speed(self._h, float(speed)))
+
+    def get_sewing_shrink_speed(self):
+        v = C.c_float()
+        self._c(self._L.tc_get_sewing_shrink_speed(self._h, C.byref(v)))
+        return v.value
+
+    def set_enable_sewing_lock(self, enabled=True):
+        self._c(self._L.tc_set_enable_sewing_lock(self._h, int(bool(enabled))))
+
+    def set_sewing_lock_distance(self, distance=0.02):
+        self._c(self._L.tc_set_sewing_lock_distance(self._h, float(distance)))
+
+    def get_sewing_lock_distance(self):
+        v = C.c_float()
+        self._c(self._L.tc_get_sewing_lock_distance(self._h, C.byref(v)))
+        return v.value
+
+    def get_sewing_current_rest_lengths(self):
+        out = np.zeros(self.get_num_sewing_constraints(), _f32)
+        self._c(self._L.tc_get_sewing_current_rest_lengths(self._h, _ptr(out), out.size))
+        return [float(x) for x in out]
+
+    def set_sewing_current_rest_lengths(self, values):
+        v = np.ascontiguousarray(np.asarray(values, dtype=_f32).reshape(-1))
+        self._c(self._L.tc_set_sewing_current_rest_lengths(self._h, _ptr(v), v.size))
+
+    def set_sewing_priority_options(self, enabled, threshold=0.9, merge_dist=0.005, ramp_frames=3, max_frames=600):
+        self._c(self._L.tc_set_sewing_priority_options(self._h, int(bool(enabled)), float(threshold),
+                                                        float(merge_dist), int(ramp_frames), int(max_frames)))
+
+    def set_sewing_priority_state(self, latched, frame, ramp_t, ratio):
+        self._c(self._L.tc_set_sewing_priority_state(self._h, int(bool(latched)), int(frame), float(ramp_t),
+                                                      float(ratio)))
+
+    def update_sewing_priority(self, positions):
+        """(closure ratio, gravity scale, latched) from host positions (N x 3)."""
+        p = _arr(positions, _f32, 3, "positions")
+        out = np.zeros(3, _f32)
+        self._c(self._L.tc_update_sewing_priority(self._h, _ptr(p), p.shape[0], _ptr(out)))
+        return float(out[0]), float(out[1]), bool(out[2] > 0.5)
+
+    def _sewing_priority(self):
+        out = np.zeros(4, _f32)
+        self._c(self._L.tc_get_sewing_priority(self._h, _ptr(out)))
+        return out
+
+    def get_sewing_priority_scale(self):
+        return float(self._sewing_priority()[0])
+
+    def get_sewing_closure_ratio(self):
+        return float(self._sewing_priority()[1])
+
+    def is_sewing_priority_active(self):
+        return bool(self._sewing_priority()[2] > 0.5)
 
     def set_positions_and_velocities(self, positions, velocities=None):
         p = _arr(positions, _f32, 3, "positions")
@@ -316,9 +396,6 @@ class ClothSimulator:
 
     def get_num_bending_constraints(self):
         return int(self._counts()[2])
-
-    def get_num_sewing_constraints(self):
-        return 0
 
     def get_has_multiple_layers(self):
         return bool(self._counts()[7])

@@ -14,7 +14,7 @@ def _p(a):
 
 def host_build(positions, edges, faces=None, inv_masses=None, layer_ids=None, thicknesses=None, layer_id=0,
                thickness=0.005, stiffness=1000.0, bending_stiffness=10.0, compression_stiffness=None,
-               shear_stiffness=None):
+               shear_stiffness=None, sewing_springs=None, sewing_shrink_speed=1.0):
     L = _lib.load()
     pos = np.ascontiguousarray(positions, _f).reshape(-1, 3)
     e = np.ascontiguousarray(edges, _u).reshape(-1, 2)
@@ -25,9 +25,11 @@ def host_build(positions, edges, faces=None, inv_masses=None, layer_ids=None, th
     comp = stiffness if compression_stiffness is None else compression_stiffness
     shear = stiffness * 0.5 if shear_stiffness is None else shear_stiffness
     h = C.c_void_p()
-    _lib.check(L.tc_mesh_build(C.byref(h), _p(pos), pos.shape[0], _p(e), e.shape[0], _p(f),
-                               0 if f is None else f.shape[0], _p(im), _p(li), _p(th), layer_id, thickness,
-                               stiffness, comp, shear, bending_stiffness))
+    sew = None if sewing_springs is None else np.ascontiguousarray(sewing_springs, _u).reshape(-1, 2)
+    _lib.check(L.tc_mesh_build_sewn(C.byref(h), _p(pos), pos.shape[0], _p(e), e.shape[0], _p(f),
+                                    0 if f is None else f.shape[0], _p(im), _p(li), _p(th), layer_id, thickness,
+                                    stiffness, comp, shear, bending_stiffness, _p(sew),
+                                    0 if sew is None else sew.shape[0], sewing_shrink_speed, float("nan"), 1))
     try:
         c = np.zeros(10, _u)
         cell = C.c_float()
@@ -60,6 +62,13 @@ def host_build(positions, edges, faces=None, inv_masses=None, layer_ids=None, th
         topo["edges"] = topo["edges"][:ne]
         topo["edge_bits"] = topo["edge_bits"][:(ne + 31) // 32]
         out.update(topo)
+        ns, nc = C.c_uint32(), C.c_uint32()
+        _lib.check(L.tc_mesh_sewing(h, C.byref(ns), C.byref(nc), None, None, None, None, None))
+        sv, sp = np.zeros((max(ns.value, 1), 2), _u), np.zeros((max(ns.value, 1), 5), _f)
+        so, sc, rep = np.zeros(max(nc.value, 1), _u), np.zeros(max(nc.value, 1), _u), np.zeros(max(n, 1), _u)
+        _lib.check(L.tc_mesh_sewing(h, None, None, _p(sv), _p(sp), _p(so), _p(sc), _p(rep)))
+        out.update(sew_v=sv[:ns.value], sew_par=sp[:ns.value], sew_off=so[:nc.value], sew_cnt=sc[:nc.value],
+                   sew_rep=rep[:n])
         return out
     finally:
         L.tc_mesh_destroy(h)
