@@ -244,6 +244,38 @@ def bone_sdf_extra(steps):
             "profile_ms_per_frame": prof, "finite": bool(np.isfinite(x).all())}
 
 
+def sewing_extra(steps):
+    """Sewn garment: front and back panels of 128 x 128 vertices (32,768
+    vertices) sewn along both sides into a tube (256 springs), seams
+    shrinking at 0.5 m/s from 6 cm, self-collision on, 10 substeps x 4
+    iterations.  Device time per frame, frames 4.. (seams closing)."""
+    from taremincloth_b200 import ClothSimulator, scenes
+    sc = scenes.sewn_garment(n=128, side=0.6)
+    s = scenes.build(ClothSimulator, sc)
+    n = len(sc["positions"])
+    dt, sub = sc["dt"], sc["substeps"]
+    for _ in range(3):
+        s.step(dt, sub)
+    ms = 0.0
+    for _ in range(steps):
+        s.step(dt, sub)
+        ms += s.last_frame_ms()
+    ms /= steps
+    s.set_profiling_enabled(True)
+    s.step(dt, sub)
+    prof = {k: round(v, 3) for k, v, _ in s.take_profile()}
+    s.set_profiling_enabled(False)
+    x, _, _ = s.get_state()
+    pinned = {v for v, _ in sc["pins"]}
+    free = [k for k, (a, b) in enumerate(sc["sewing"]) if a not in pinned and b not in pinned]
+    gap = np.linalg.norm(x[sc["sewing"][free, 0]] - x[sc["sewing"][free, 1]], axis=1)
+    return {"workload": f"sewn garment, two 128x128 panels ({n} vertices), {len(sc['sewing'])} springs, "
+                        f"self-collision on, {sub} substeps x {sc['iterations']} iterations",
+            "ms_per_frame": ms, "vertex_substeps_per_s": n * sub / (ms / 1e3),
+            "profile_ms_per_frame": prof, "max_open_seam_m": float(gap.max()),
+            "sewing_constraints": s.get_num_sewing_constraints()}
+
+
 def _warm_start_case(sim, n, dt, sub, iters, steps, ks, rec_frames, every, workload):
     """Record plain-solver snapshots, train, calibrate the relative residual
     threshold on plain substeps (p90 of final / predicted residual), then
@@ -449,6 +481,7 @@ def main():
         line["batched_config4"] = batch_extra(3)
         line["warm_start"] = warm_start_extra(3)
         line["bone_sdf_config3"] = bone_sdf_extra(3)
+        line["sewing"] = sewing_extra(3)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
