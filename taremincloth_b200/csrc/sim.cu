@@ -1346,7 +1346,7 @@ struct Sim {
     const bool bone_col = ca.bone.nbones > 0;
     if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
     if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
-    timed("sew_shrink", [&] { launch_sew_start(dts); });
+    if (nsw) timed("sew_shrink", [&] { launch_sew_start(dts); });
     timed("predict", [&] { launch_k(k_predict, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp); });
     timed("ws_check", [&] { encode_ws_res_pred(dts, bone_col); });
     timed("ws_mlp", [&] { ws.net.infer(nullptr, &fa, ws.ppred.p, nullptr, x4.p, p4.p, local_len.p); });
@@ -1499,7 +1499,7 @@ struct Sim {
     for (uint32_t s = 0; s < substeps; ++s) {
       if (nd) TC_CK(cudaMemsetAsync(dlam.p, 0, nd * sizeof(float), st));
       if (nb) TC_CK(cudaMemsetAsync(blam.p, 0, nb * sizeof(float), st));
-      timed("sew_shrink", [&] { launch_sew_start(dts); });
+      if (nsw) timed("sew_shrink", [&] { launch_sew_start(dts); });
       timed("predict", [&] { launch_k(k_predict, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp); });
       if (track_residual && s + 1 == substeps && nd + nb)
         k_residual_pred<<<grid(nd + nb, 256), 256, 0, st>>>(nd, nb, dist_ids.p, dist_par.p, bend_ids.p, bend_par.p,
