@@ -86,6 +86,16 @@ tc_status tc_step(tc_sim *s, float dt, uint32_t substeps, uint32_t *effective_su
  * and return; fetch_positions (lib.rs:1834-1846) waits and copies. */
 tc_status tc_step_async(tc_sim *s, float dt, uint32_t substeps);
 tc_status tc_fetch_positions(tc_sim *s, float *out, size_t out_len, int *ok);
+/* step_buffered / fetch_buffered_positions / get_buffered_frame_count /
+ * clear_frame_buffer (dispatch.rs:1293-1408, lib.rs:1845-1881): a frame
+ * whose positions go to the next of 8 device slots (the last slot once all
+ * are full) with no wait, count = frames held; a fetch copies every held
+ * frame (frames x n x 3 floats, as much as fits in out) in one transfer,
+ * returns their count and empties the ring; tc_reset empties it too. */
+tc_status tc_step_buffered(tc_sim *s, float dt, uint32_t substeps, uint32_t *count);
+tc_status tc_fetch_buffered_positions(tc_sim *s, float *out, size_t out_len, uint32_t *count);
+tc_status tc_get_buffered_frame_count(tc_sim *s, uint32_t *count);
+tc_status tc_clear_frame_buffer(tc_sim *s);
 /* get_positions (lib.rs:2110-2120): out holds n*3 floats. */
 tc_status tc_get_positions(tc_sim *s, float *out, size_t out_len);
 /* set_positions_and_velocities (dispatch.rs:953-988); vel may be NULL. */

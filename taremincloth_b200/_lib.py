@@ -33,6 +33,10 @@ SIGNATURES = {
     "tc_step": [_P, _F, _U, C.POINTER(_U)],
     "tc_step_async": [_P, _F, _U],
     "tc_fetch_positions": [_P, _P, C.c_size_t, C.POINTER(_I)],
+    "tc_step_buffered": [_P, _F, _U, C.POINTER(_U)],
+    "tc_fetch_buffered_positions": [_P, _P, C.c_size_t, C.POINTER(_U)],
+    "tc_get_buffered_frame_count": [_P, C.POINTER(_U)],
+    "tc_clear_frame_buffer": [_P],
     "tc_get_positions": [_P, _P, C.c_size_t],
     "tc_set_positions_and_velocities": [_P, _P, _P, _U],
     "tc_reset": [_P],

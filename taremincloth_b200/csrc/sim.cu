@@ -64,6 +64,16 @@ struct DBuf {
   void upload(const std::vector<T>& v, cudaStream_t st) { upload(v.data(), v.size(), st); }
 };
 
+// positions x of every vertex packed as xyz (encode_extract_positions)
+__global__ void k_extract_positions(uint32_t n, const float4* __restrict__ x4, float* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 x = x4[i];
+  out[3 * size_t(i)] = x.x;
+  out[3 * size_t(i) + 1] = x.y;
+  out[3 * size_t(i) + 2] = x.z;
+}
+
 // Adaptive feedback (update_feedback_from_floats, dispatch.rs:356-429): the
 // largest per-axis displacement since the previous frame (max is order-free:
 // atomicMax on the bits of non-negative floats), then prev = x.
@@ -1670,6 +1680,22 @@ struct Sim {
     consume_feedback();
   }
 
+  // buffered frames (dispatch.rs:1293-1408): positions of up to 8 frames
+  // kept on the device, fetched in one copy
+  static constexpr uint32_t kMaxBuffered = 8;
+  DBuf<float> ring;
+  uint32_t buffered = 0;
+  uint32_t step_buffered(float dt, uint32_t substeps) {
+    if (n == 0) return 0;
+    ring.alloc(size_t(kMaxBuffered) * n * 3);
+    const uint32_t slot = std::min(buffered, kMaxBuffered - 1);
+    launch_frame(dt, substeps);
+    encode_feedback();
+    k_extract_positions<<<grid(n, 256), 256, 0, st>>>(n, x4.p, ring.p + size_t(slot) * n * 3);
+    TC_CK(cudaGetLastError());
+    if (buffered < kMaxBuffered) ++buffered;
+    return buffered;
+  }
   void get_positions(float* out) {
     std::vector<float4> h(n);
     TC_CK(cudaMemcpyAsync(h.data(), x4.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
@@ -2006,6 +2032,50 @@ tc_status tc_fetch_positions(tc_sim* s, float* out, size_t out_len, int* ok) {
   });
 }
 
+// step_buffered (dispatch.rs:1293-1340): one frame, its positions into the
+// next slot of the device ring (the last slot once 8 are held); no wait
+tc_status tc_step_buffered(tc_sim* s, float dt, uint32_t substeps, uint32_t* count) {
+  return guard([&] {
+    Sim& m = S(s);
+    const uint32_t c = m.step_buffered(dt, m.plan_frame(dt, substeps));
+    if (count) *count = c;
+  });
+}
+tc_status tc_get_buffered_frame_count(tc_sim* s, uint32_t* count) {
+  return guard([&] { need(count != nullptr, "count required"); *count = S(s).buffered; });
+}
+tc_status tc_clear_frame_buffer(tc_sim* s) {
+  return guard([&] { S(s).buffered = 0; });
+}
+// fetch_buffered_positions (dispatch.rs:1349-1403): every buffered frame
+// (frames x n x 3 floats, as much as fits in out), then the feedback of the
+// last frame and an empty ring.
+tc_status tc_fetch_buffered_positions(tc_sim* s, float* out, size_t out_len, uint32_t* count) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(count != nullptr, "count required");
+    *count = 0;
+    const uint32_t c = m.buffered;
+    if (c == 0 || m.n == 0) return;
+    need(out != nullptr || out_len == 0, "output required");
+    const size_t nv3 = size_t(m.n) * 3, total = size_t(c) * nv3, len = std::min(out_len, total);
+    if (len) TC_CK(cudaMemcpyAsync(out, m.ring.p, len * sizeof(float), cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    TC_CK(cudaGetLastError());
+    m.check_barrier_status();
+    m.consume_feedback();
+    if (len == total) {
+      const float* last = out + (size_t(c) - 1) * nv3;
+      float md = 0.f;
+      for (size_t i = 0; i < nv3; ++i) md = std::fmax(md, std::fabs(last[i] - m.prev_frame_pos[i]));
+      std::memcpy(m.prev_frame_pos.data(), last, nv3 * sizeof(float));
+      m.last_max_disp = md;
+    }
+    m.buffered = 0;
+    *count = c;
+  });
+}
+
 tc_status tc_get_positions(tc_sim* s, float* out, size_t out_len) {
   return guard([&] {
     Sim& m = S(s);
@@ -2037,6 +2107,7 @@ tc_status tc_reset(tc_sim* s) {
     std::fill(m.mult.begin(), m.mult.end(), 1.f);
     m.apply_distance_compliances();
     TC_CK(cudaMemsetAsync(m.acc.p, 0, size_t(m.n) * tcloth::A_N * sizeof(int32_t), m.st));
+    m.buffered = 0;         // dispatch.rs:1425
     m.pri.latched = false;  // sewing priority restarts (dispatch.rs:1414-1417)
     m.pri.frame = 0;
     m.pri.ramp_t = 0.f;

@@ -181,6 +181,32 @@ class ClothSimulator:
         self._c(self._L.tc_fetch_positions(self._h, _ptr(out), out.size, C.byref(ok)))
         return bool(ok.value)
 
+    def step_buffered(self, dt=0.016666667, substeps=None, solver_iterations=None):
+        """One frame into the device ring (8 slots); returns the frames held."""
+        if solver_iterations is not None:
+            self.set_solver_iterations(solver_iterations)
+        c = C.c_uint32()
+        self._c(self._L.tc_step_buffered(self._h, float(dt), 0 if substeps is None else int(substeps), C.byref(c)))
+        return c.value
+
+    def fetch_buffered_positions(self, out_array):
+        """Every held frame (frames x N x 3 floats, as much as fits) into
+        out_array in one copy; returns the frame count and empties the ring."""
+        if not isinstance(out_array, np.ndarray) or out_array.dtype != _f32 or not out_array.flags.c_contiguous \
+                or not out_array.flags.writeable:
+            raise ValueError("out_array must be a writable, contiguous float32 NumPy array")
+        c = C.c_uint32()
+        self._c(self._L.tc_fetch_buffered_positions(self._h, _ptr(out_array), out_array.size, C.byref(c)))
+        return c.value
+
+    def get_buffered_frame_count(self):
+        c = C.c_uint32()
+        self._c(self._L.tc_get_buffered_frame_count(self._h, C.byref(c)))
+        return c.value
+
+    def clear_frame_buffer(self):
+        self._c(self._L.tc_clear_frame_buffer(self._h))
+
     def _out(self, out_array):
         if not isinstance(out_array, np.ndarray) or out_array.dtype != _f32 or not out_array.flags.c_contiguous \
                 or not out_array.flags.writeable:
