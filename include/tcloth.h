@@ -105,6 +105,17 @@ tc_status tc_reset(tc_sim *s);
 
 /* parameters (simulation/mod.rs:1091-1106, :1429-1449, lib.rs:2751-2800) */
 tc_status tc_set_gravity(tc_sim *s, float gx, float gy, float gz);
+/* Edge colliders (edge_collision.wgsl; simulation/mod.rs:1007-1025,
+ * lib.rs:2736-2749), off by default: after the final pins of each substep,
+ * every cloth edge is tested against the edges of the mesh-collider
+ * triangles near its midpoint (contact distance = thickness sum x scale +
+ * offset, scale >= 1, offset >= 0) and pushed out through the pin channel
+ * of the self-collision accumulator, applied before self-collision.  The
+ * collider edges are extracted when the triangles are set. */
+tc_status tc_set_enable_edge_collision(tc_sim *s, int enable);
+tc_status tc_set_edge_margin_scale(tc_sim *s, float scale);
+tc_status tc_set_edge_margin_offset(tc_sim *s, float offset);
+tc_status tc_get_num_collider_edges(tc_sim *s, uint32_t *count);
 /* Sewing (simulation/mod.rs:1211-1420, lib.rs:2798-2925).  Each substep
  * shrinks every spring's current rest length towards 0 at the shrink speed
  * (sewing_shrink.wgsl), projects the springs per colour after the distance

@@ -48,6 +48,9 @@ def lib():
         L.ocl_get_sewing.argtypes = [P, P, P, P, P, P, P]
         L.ocl_get_sewing.restype = C.c_int
         L.ocl_get_bending_gate.argtypes = [P, fp]
+        L.ocl_set_edge_collision.argtypes = [P, C.c_int, C.c_float, C.c_float]
+        L.ocl_num_collider_edges.argtypes = [P]
+        L.ocl_num_collider_edges.restype = C.c_int
         L.ocl_destroy.argtypes = [P]
         for name, n in [("ocl_set_gravity", 3), ("ocl_set_damping_all", 4), ("ocl_set_compliance_all", 4)]:
             getattr(L, name).argtypes = [P] + [C.c_float] * n
@@ -234,6 +237,13 @@ class OracleSim:
         lib().ocl_get_bending(self._h, v, r, cp, p0)
         lib().ocl_get_bending_gate(self._h, p1)
         return dict(v=v[:4 * nb].reshape(-1, 4), rest=r[:nb], comp=cp[:nb], pad0=p0[:nb], pad1=p1[:nb])
+
+    # --- edge colliders -------------------------------------------------
+    def set_edge_collision(self, enable=True, margin_scale=1.0, margin_offset=0.0):
+        lib().ocl_set_edge_collision(self._h, int(bool(enable)), margin_scale, margin_offset)
+
+    def num_collider_edges(self):
+        return lib().ocl_num_collider_edges(self._h)
 
     # --- sewing --------------------------------------------------------
     def set_sewing(self, stiffness=10000.0, lock=True, lock_distance=0.02, shrink_speed=1.0):

@@ -135,6 +135,8 @@ typedef struct { uint32_t v0, v1; float cur, target, speed, comp, lock; } OSew;
 typedef struct { uint32_t type; float fric, rest; v3 a; float r; v3 b; } OCol;
 typedef struct { v3 p0; float fric; v3 p1; float thick; v3 p2; float rest; uint32_t flags; } OTri;
 typedef struct { uint32_t v; float w; v3 target; } OPin;
+/* GpuColliderEdge (mesh.rs:91-100) */
+typedef struct { v3 p0; float th; v3 p1; float fr; v3 nrm; uint32_t flags; } OCEdge;
 
 /* accumulator slots, SelfCollisionAccum (shaders/self_collision.wgsl:31-48) */
 enum { A_DX, A_DY, A_DZ, A_CNT, A_PDX, A_PDY, A_PDZ, A_PCNT, A_CPX, A_CPY, A_CPZ, A_CNX, A_CNY,
@@ -180,6 +182,9 @@ struct OSim {
     /* colliders */
     OCol *cols; int ncols;
     OTri *tris; float *bounds; int ntris;
+    /* edge colliders (edge_collision.wgsl), off by default (mod.rs:628-630) */
+    int edge_collision; float emscale, emoff;
+    OCEdge *ce; int nce; uint32_t *ce_cs, *ce_srt; float ce_cell;
     OPin *pins; int npins;
     /* self-collision scratch */
     int32_t *acc;  /* n * A_N */
@@ -398,6 +403,7 @@ OSim *ocl_create_sewn(const float *pos, int n, const uint32_t *edges, int ne_in,
                       float compression_k, float shear_k, float bending_k, const uint32_t *sew, int nsew,
                       float shrink_speed) {
     OSim *s = (OSim *)calloc(1, sizeof(OSim));
+    s->emscale = 1.0f;
     s->sew_stiffness = 10000.0f;
     s->sew_lock = 1;
     s->sew_lock_dist = 0.02f;
@@ -1024,7 +1030,8 @@ void ocl_destroy(OSim *s) {
                     s->adj_off, s->adj_idx, s->th_off, s->th_idx, s->th_rest, s->local_len,
                     s->star_off, s->star_idx, s->edges, s->ebits, s->island, s->cols, s->tris,
                     s->bounds, s->pins, s->acc, s->nrm, s->cs, s->srt, s->ecs, s->esrt,
-                    s->atlas, s->binfo, s->bxf, s->sew, s->sc_off, s->sc_cnt, s->slam, s->rep};
+                    s->atlas, s->binfo, s->bxf, s->sew, s->sc_off, s->sc_cnt, s->slam, s->rep,
+                    s->ce, s->ce_cs, s->ce_srt};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(s);
 }
@@ -1074,6 +1081,201 @@ void ocl_add_plane(OSim *s, const float *pt, const float *nrm, float fric, float
     k.a = V3(pt[0], pt[1], pt[2]); k.b = V3(nrm[0], nrm[1], nrm[2]); k.r = 0.0f; push_col(s, k);
 }
 /* cloth_py/src/lib.rs:2175-2234 and upload_colliders, simulation/mod.rs:2613-2670 */
+/* extract_collider_edges (mesh.rs:1503-1565): an edge per distinct
+ * endpoint pair (keyed by the endpoints' bits), oriented as in the first
+ * triangle that has it; thickness max, friction averaged, normals summed in
+ * triangle order, then normalised; flags = AND of the single-sided bits.
+ * build_collider_edge_grid (spatial_hash.rs:463-528): every cell the edge
+ * passes through at half-cell sampling, once per distinct bucket. */
+static inline uint32_t hash3(int32_t cx, int32_t cy, int32_t cz, uint32_t table);
+static inline void cell_of(v3 p, float cell, int32_t *c);
+typedef struct { uint32_t key[6]; uint32_t ord; } OEKey;
+static int cmp_ekey(const void *x, const void *y) {
+    const OEKey *p = (const OEKey *)x, *q = (const OEKey *)y;
+    for (int k = 0; k < 6; k++) if (p->key[k] != q->key[k]) return p->key[k] < q->key[k] ? -1 : 1;
+    return (p->ord > q->ord) - (p->ord < q->ord);
+}
+static int32_t sat_i32f(float f) {
+    if (!(f == f)) return 0;
+    if (f <= -2147483648.0f) return INT32_MIN;
+    if (f >= 2147483647.0f) return INT32_MAX;
+    return (int32_t)f;
+}
+static void build_collider_edges(OSim *s) {
+    free(s->ce); free(s->ce_cs); free(s->ce_srt);
+    s->ce = NULL; s->ce_cs = NULL; s->ce_srt = NULL; s->nce = 0;
+    s->ce_cell = s->cell;
+    const uint32_t T = 32768u;
+    s->ce_cs = (uint32_t *)calloc((size_t)T + 1, 4);
+    s->ce_srt = (uint32_t *)malloc(4);
+    int nt = s->ntris;
+    if (nt <= 0) return;
+    OEKey *ks = (OEKey *)malloc(sizeof(OEKey) * 3 * (size_t)nt);
+    for (int t = 0; t < nt; t++)
+        for (int k = 0; k < 3; k++) {
+            v3 a = k == 0 ? s->tris[t].p0 : (k == 1 ? s->tris[t].p1 : s->tris[t].p2);
+            v3 b = k == 0 ? s->tris[t].p1 : (k == 1 ? s->tris[t].p2 : s->tris[t].p0);
+            uint32_t ab[3], bb[3];
+            memcpy(ab, &a, 12); memcpy(bb, &b, 12);
+            int a_first = ab[0] != bb[0] ? ab[0] < bb[0] : (ab[1] != bb[1] ? ab[1] < bb[1] : ab[2] < bb[2]);
+            OEKey q;
+            memcpy(q.key, a_first ? ab : bb, 12); memcpy(q.key + 3, a_first ? bb : ab, 12);
+            q.ord = (uint32_t)(3 * t + k);
+            ks[3 * t + k] = q;
+        }
+    qsort(ks, 3 * (size_t)nt, sizeof(OEKey), cmp_ekey);
+    s->ce = (OCEdge *)malloc(sizeof(OCEdge) * 3 * (size_t)nt);
+    int ne = 0;
+    for (int i = 0; i < 3 * nt;) {
+        int j = i;
+        while (j < 3 * nt && memcmp(ks[j].key, ks[i].key, sizeof ks[i].key) == 0) j++;
+        OCEdge e;
+        for (int q = i; q < j; q++) {
+            int t = (int)(ks[q].ord / 3), k = (int)(ks[q].ord % 3);
+            OTri *o = &s->tris[t];
+            v3 e1 = vsub(o->p1, o->p0), e2 = vsub(o->p2, o->p0);
+            v3 cr = V3(e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z, e1.x * e2.y - e1.y * e2.x);
+            float cl = sqrtf(cr.x * cr.x + cr.y * cr.y + cr.z * cr.z);
+            v3 tn = cl > 1e-12f ? V3(cr.x / cl, cr.y / cl, cr.z / cl) : V3(0.0f, 0.0f, 0.0f);
+            uint32_t single = o->flags & 1u;
+            if (q == i) {
+                e.p0 = k == 0 ? o->p0 : (k == 1 ? o->p1 : o->p2);
+                e.p1 = k == 0 ? o->p1 : (k == 1 ? o->p2 : o->p0);
+                e.th = o->thick; e.fr = o->fric; e.nrm = tn; e.flags = single;
+            } else {
+                e.th = fmaxf(e.th, o->thick);
+                e.fr = (e.fr + o->fric) * 0.5f;
+                e.nrm = V3(e.nrm.x + tn.x, e.nrm.y + tn.y, e.nrm.z + tn.z);
+                e.flags &= single;
+            }
+        }
+        float nl = sqrtf(e.nrm.x * e.nrm.x + e.nrm.y * e.nrm.y + e.nrm.z * e.nrm.z);
+        e.nrm = nl > 1e-6f ? V3(e.nrm.x / nl, e.nrm.y / nl, e.nrm.z / nl) : V3(0.0f, 0.0f, 0.0f);
+        s->ce[ne++] = e;
+        i = j;
+    }
+    free(ks);
+    s->nce = ne;
+    float safe = fmaxf(s->ce_cell, 1e-4f), pitch = safe * 0.5f;
+    UVec hb = {0}, eb = {0}; /* (bucket, edge) entries */
+    uint32_t *hs = NULL; size_t hcap = 0;
+    for (int ei = 0; ei < ne; ei++) {
+        OCEdge *e = &s->ce[ei];
+        float dx = e->p1.x - e->p0.x, dy = e->p1.y - e->p0.y, dz = e->p1.z - e->p0.z;
+        float len = sqrtf(dx * dx + dy * dy + dz * dz);
+        float sf = ceilf(len / pitch);
+        size_t steps = (sf == sf && sf > 0.0f) ? (sf >= 4096.0f ? 4096 : (size_t)sf) : 0;
+        if (steps < 1) steps = 1;
+        if (steps > 4096) steps = 4096;
+        if (steps + 1 > hcap) { hcap = 2 * (steps + 1); hs = (uint32_t *)realloc(hs, 4 * hcap); }
+        for (size_t k = 0; k <= steps; k++) {
+            float t = (float)k / (float)steps;
+            float px = e->p0.x + dx * t, py = e->p0.y + dy * t, pz = e->p0.z + dz * t;
+            hs[k] = hash3(sat_i32f(floorf(px / safe)), sat_i32f(floorf(py / safe)), sat_i32f(floorf(pz / safe)), T);
+        }
+        size_t nh = sort_dedup(hs, steps + 1);
+        for (size_t k = 0; k < nh; k++) { uv_push(&hb, hs[k]); uv_push(&eb, (uint32_t)ei); }
+    }
+    free(hs);
+    for (size_t k = 0; k < hb.n; k++) s->ce_cs[hb.d[k] + 1]++;
+    for (uint32_t h = 0; h < T; h++) s->ce_cs[h + 1] += s->ce_cs[h];
+    free(s->ce_srt);
+    s->ce_srt = (uint32_t *)malloc(4 * (hb.n + 1));
+    uint32_t *cur = (uint32_t *)malloc(4 * (size_t)T);
+    memcpy(cur, s->ce_cs, 4 * (size_t)T);
+    for (size_t k = 0; k < hb.n; k++) s->ce_srt[cur[hb.d[k]]++] = eb.d[k];
+    free(cur); free(hb.d); free(eb.d);
+}
+/* closest points of two segments (edge_collision.wgsl:96-149) */
+static float eseg_closest(v3 p0, v3 p1, v3 q0, v3 q1, float *s_out, float *t_out) {
+    v3 d1 = vsub(p1, p0), d2 = vsub(q1, q0), r = vsub(p0, q0);
+    float a = vdot(d1, d1), e = vdot(d2, d2), f = vdot(d2, r);
+    float s = 0.0f, t = 0.0f;
+    if (a <= 1e-12f && e <= 1e-12f) { *s_out = 0.0f; *t_out = 0.0f; return vlen(vsub(p0, q0)); }
+    if (a <= 1e-12f) {
+        t = clampf(f / e, 0.0f, 1.0f);
+    } else {
+        float c = vdot(d1, r);
+        if (e <= 1e-12f) {
+            s = clampf(-c / a, 0.0f, 1.0f);
+        } else {
+            float b = vdot(d1, d2);
+            float denom = a * e - b * b;
+            if (denom > a * e * 1e-7f) s = clampf((b * f - c * e) / denom, 0.0f, 1.0f);
+            t = (b * s + f) / e;
+            if (t < 0.0f) { t = 0.0f; s = clampf(-c / a, 0.0f, 1.0f); }
+            else if (t > 1.0f) { t = 1.0f; s = clampf((b - c) / a, 0.0f, 1.0f); }
+        }
+    }
+    *s_out = s; *t_out = t;
+    return vlen(vsub(vadd(p0, vmul(d1, s)), vadd(q0, vmul(d2, t))));
+}
+static void add_pin(OSim *s, uint32_t v, v3 d);
+static void k_apply(OSim *s);
+/* shaders/edge_collision.wgsl:150-276, then the apply pass (dispatch.rs:254-283) */
+static void k_edge_collision(OSim *s) {
+    if (s->nce > 0) {
+        for (int ei = 0; ei < s->ne; ei++) {
+            uint32_t u0 = s->edges[2 * ei], u1 = s->edges[2 * ei + 1];
+            float w0 = s->w[u0], w1 = s->w[u1];
+            if (w0 + w1 <= EPS) continue;
+            v3 p0 = s->p[u0], p1 = s->p[u1];
+            v3 pmid = vmul(vadd(p0, p1), 0.5f);
+            float cth = fmaxf(s->thick[u0], s->thick[u1]);
+            int32_t cc[3]; cell_of(pmid, s->ce_cell, cc);
+            v3 lo = vmin(p0, p1), hi = vmax(p0, p1);
+            for (int dz = -1; dz <= 1; dz++)
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        uint32_t h = hash3(cc[0] + dx, cc[1] + dy, cc[2] + dz, 32768u);
+                        for (uint32_t k = s->ce_cs[h]; k < s->ce_cs[h + 1]; k++) {
+                            const OCEdge *ce = &s->ce[s->ce_srt[k]];
+                            float tgt = (cth + ce->th) * s->emscale + s->emoff;
+                            v3 clo = vmin(ce->p0, ce->p1), chi = vmax(ce->p0, ce->p1);
+                            if (hi.x + tgt < clo.x || lo.x - tgt > chi.x || hi.y + tgt < clo.y || lo.y - tgt > chi.y ||
+                                hi.z + tgt < clo.z || lo.z - tgt > chi.z)
+                                continue;
+                            float sp_, tp_;
+                            float dist = eseg_closest(p0, p1, ce->p0, ce->p1, &sp_, &tp_);
+                            if (!(dist < tgt)) continue;
+                            v3 diff = vsub(vadd(p0, vmul(vsub(p1, p0), sp_)), vadd(ce->p0, vmul(vsub(ce->p1, ce->p0), tp_)));
+                            int single = (ce->flags & 1u) != 0u;
+                            int has_n = vdot(ce->nrm, ce->nrm) > 0.25f;
+                            v3 nrm = V3(0.0f, 0.0f, 1.0f);
+                            float pen = tgt - dist;
+                            if (single && has_n) {
+                                float sd = vdot(diff, ce->nrm);
+                                if (sd >= 0.0f) { nrm = dist > EPS ? vdiv(diff, dist) : ce->nrm; pen = tgt - dist; }
+                                else { nrm = ce->nrm; pen = fminf(tgt - sd, tgt * 2.0f); }
+                            } else if (dist > EPS) {
+                                nrm = vdiv(diff, dist);
+                            } else {
+                                v3 cr = vcross(vsub(p1, p0), vsub(ce->p1, ce->p0));
+                                float cl = vlen(cr);
+                                if (cl > EPS) nrm = vdiv(cr, cl);
+                            }
+                            v3 push = vmul(nrm, pen);
+                            float ca = 1.0f - sp_, cb = sp_;
+                            float den = ca * ca * w0 + cb * cb * w1;
+                            if (den > EPS) {
+                                float f0 = fminf((ca * w0) / den, 2.0f), f1 = fminf((cb * w1) / den, 2.0f);
+                                if (w0 > 0.0f) add_pin(s, u0, vmul(push, f0));
+                                if (w1 > 0.0f) add_pin(s, u1, vmul(push, f1));
+                            }
+                        }
+                    }
+        }
+    }
+    k_apply(s);
+}
+
+void ocl_set_edge_collision(OSim *s, int enable, float margin_scale, float margin_offset) {
+    s->edge_collision = enable != 0;
+    s->emscale = fmaxf(margin_scale, 1.0f);
+    s->emoff = fmaxf(margin_offset, 0.0f);
+}
+int ocl_num_collider_edges(const OSim *s) { return s->nce; }
+
 void ocl_set_mesh_triangles(OSim *s, const float *tris, int T, float fric, float thick, float rest,
                             int single_sided, const float *attrs) {
     free(s->tris); free(s->bounds);
@@ -1092,7 +1294,7 @@ void ocl_set_mesh_triangles(OSim *s, const float *tris, int T, float fric, float
         }
         s->tris[t] = o;
     }
-    if (T <= 0) return;
+    if (T <= 0) { build_collider_edges(s); return; }
     /* Morton sort of triangle centroids (stable) */
     v3 bmin = V3(3.4028235e38f, 3.4028235e38f, 3.4028235e38f), bmax = vneg(bmin);
     for (int t = 0; t < T; t++) {
@@ -1125,10 +1327,12 @@ void ocl_set_mesh_triangles(OSim *s, const float *tris, int T, float fric, float
         float r = sqrtf(fmaxf(fmaxf(d0, d1), d2)) + o->thick;
         s->bounds[4 * t] = cx; s->bounds[4 * t + 1] = cy; s->bounds[4 * t + 2] = cz; s->bounds[4 * t + 3] = r;
     }
+    build_collider_edges(s);
 }
 void ocl_clear_colliders(OSim *s) {
     free(s->cols); s->cols = NULL; s->ncols = 0;
     free(s->tris); s->tris = NULL; free(s->bounds); s->bounds = NULL; s->ntris = 0;
+    build_collider_edges(s);
 }
 /* simulation/mod.rs:2768-2791 */
 void ocl_set_pin(OSim *s, uint32_t v, const float *target, float w) {
@@ -2688,6 +2892,7 @@ void ocl_step(OSim *s, float dt, int substeps) {
         }
         if (hascol && !coupled) k_collision(s, dts);
         if (s->npins > 0) k_pin(s, dts);
+        if (s->edge_collision && hascol && s->ne > 0) k_edge_collision(s); /* dispatch.rs:254-283 */
         if (do_sc) self_collision(s, run_ee);
         for (int c = 0; c < s->nsc; c++) if (s->sc_cnt[c]) k_sewing(s, c, dts); /* final sewing, dispatch.rs:323-337 */
         k_update_vel(s, dts);

@@ -66,6 +66,9 @@ void ocl_add_plane(OSim *s, const float *pt, const float *nrm, float fric, float
 void ocl_set_mesh_triangles(OSim *s, const float *tris, int T, float fric, float thick,
                             float rest, int single_sided, const float *attrs);
 void ocl_clear_colliders(OSim *s);
+/* edge colliders (edge_collision.wgsl; mod.rs:1007-1025), off by default */
+void ocl_set_edge_collision(OSim *s, int enable, float margin_scale, float margin_offset);
+int ocl_num_collider_edges(const OSim *s);
 void ocl_set_pin(OSim *s, uint32_t v, const float *target, float w);
 void ocl_clear_pins(OSim *s);
 void ocl_set_coupled_collider(OSim *s, int on);

@@ -41,6 +41,10 @@ SIGNATURES = {
     "tc_set_positions_and_velocities": [_P, _P, _P, _U],
     "tc_reset": [_P],
     "tc_set_gravity": [_P, _F, _F, _F],
+    "tc_set_enable_edge_collision": [_P, _I],
+    "tc_set_edge_margin_scale": [_P, _F],
+    "tc_set_edge_margin_offset": [_P, _F],
+    "tc_get_num_collider_edges": [_P, C.POINTER(_U)],
     "tc_get_num_sewing_constraints": [_P, C.POINTER(_U)],
     "tc_set_sewing_stiffness": [_P, _F],
     "tc_set_sewing_shrink_speed": [_P, _F],

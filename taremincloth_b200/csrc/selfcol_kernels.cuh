@@ -1373,6 +1373,123 @@ __global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
   }
 }
 
+// ---------------- edge colliders: shaders/edge_collision.wgsl:82-276
+// Collider edge (mesh.rs:1503-1565): endpoints, the largest thickness and the
+// mean friction of its triangles, their summed then normalised normals, and
+// bit 0 set when every triangle is single-sided.
+struct ColEdge {
+  float4 p0t;  // p0, thickness
+  float4 p1f;  // p1, friction
+  float4 nfl;  // normal, flags bits
+};
+struct EdgeColArgs {
+  uint32_t ne, nce;            // cloth edges, collider edges
+  const uint2* edges;
+  const float4* x4;
+  const float4* p4;
+  const ColEdge* ce;
+  const uint32_t* cs;          // collider-edge grid: cell starts [table + 1]
+  const uint32_t* srt;         // and edge indices
+  float cell;
+  uint32_t table;
+  float mscale, moff;          // contact distance = thickness sum * mscale + moff
+  int32_t* acc;
+};
+// closest points of segments p0-p1 and q0-q1 (edge_collision.wgsl:96-149)
+__device__ __forceinline__ float seg_closest(V3 p0, V3 p1, V3 q0, V3 q1, float& s, float& t) {
+  const V3 d1 = p1 - p0, d2 = q1 - q0, r = p0 - q0;
+  const float a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+  s = 0.0f;
+  t = 0.0f;
+  if (a <= 1e-12f && e <= 1e-12f) return length(p0 - q0);
+  if (a <= 1e-12f) {
+    t = clampf(f / e, 0.0f, 1.0f);
+  } else {
+    const float c = dot(d1, r);
+    if (e <= 1e-12f) {
+      s = clampf(-c / a, 0.0f, 1.0f);
+    } else {
+      const float b = dot(d1, d2);
+      const float denom = a * e - b * b;
+      s = denom > a * e * 1e-7f ? clampf((b * f - c * e) / denom, 0.0f, 1.0f) : 0.0f;
+      t = (b * s + f) / e;
+      if (t < 0.0f) {
+        t = 0.0f;
+        s = clampf(-c / a, 0.0f, 1.0f);
+      } else if (t > 1.0f) {
+        t = 1.0f;
+        s = clampf((b - c) / a, 0.0f, 1.0f);
+      }
+    }
+  }
+  return length((p0 + d1 * s) - (q0 + d2 * t));
+}
+// One thread per cloth edge: collider edges of the 27 cells around its
+// midpoint; a contact pushes both endpoints out (collider edges do not move)
+// through the pin channel of the self-collision accumulator.
+__global__ void __launch_bounds__(256) k_edge_collision(EdgeColArgs a) {
+  const uint32_t ei = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ei >= a.ne || a.nce == 0u) return;
+  const uint2 e = a.edges[ei];
+  const uint32_t u0 = e.x, u1 = e.y;
+  const float w0 = a.x4[u0].w, w1 = a.x4[u1].w;
+  if (w0 + w1 <= kEps) return;
+  const float4 q0v = a.p4[u0], q1v = a.p4[u1];
+  const V3 p0 = mk(q0v), p1 = mk(q1v);
+  const V3 pmid = (p0 + p1) * 0.5f;
+  const float cth = fmaxf(q0v.w, q1v.w);
+  const I3 cc = cell_of(pmid, a.cell);
+  const V3 lo = vmin(p0, p1), hi = vmax(p0, p1);
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const uint32_t h = hash3(cc.x + dx, cc.y + dy, cc.z + dz, a.table);
+        const uint32_t st = a.cs[h], en = a.cs[h + 1];
+        for (uint32_t k = st; k < en; ++k) {
+          const ColEdge ce = a.ce[a.srt[k]];
+          const V3 c0 = mk(ce.p0t), c1 = mk(ce.p1f);
+          const float tgt = (cth + ce.p0t.w) * a.mscale + a.moff;
+          const V3 clo = vmin(c0, c1), chi = vmax(c0, c1);
+          if (hi.x + tgt < clo.x || lo.x - tgt > chi.x || hi.y + tgt < clo.y || lo.y - tgt > chi.y ||
+              hi.z + tgt < clo.z || lo.z - tgt > chi.z)
+            continue;
+          float s, t;
+          const float dist = seg_closest(p0, p1, c0, c1, s, t);
+          if (!(dist < tgt)) continue;
+          const V3 diff = (p0 + (p1 - p0) * s) - (c0 + (c1 - c0) * t);
+          const V3 en_ = mk(ce.nfl);
+          const bool single = (__float_as_uint(ce.nfl.w) & 1u) != 0u;
+          const bool has_n = dot(en_, en_) > 0.25f;
+          V3 nrm = mk(0.0f, 0.0f, 1.0f);
+          float pen = tgt - dist;
+          if (single && has_n) {
+            const float sp = dot(diff, en_);
+            if (sp >= 0.0f) {
+              nrm = dist > kEps ? diff / dist : en_;
+              pen = tgt - dist;
+            } else {
+              nrm = en_;
+              pen = fminf(tgt - sp, tgt * 2.0f);
+            }
+          } else if (dist > kEps) {
+            nrm = diff / dist;
+          } else {
+            const V3 cr = cross(p1 - p0, c1 - c0);
+            const float cl = length(cr);
+            if (cl > kEps) nrm = cr / cl;
+          }
+          const V3 push = nrm * pen;
+          const float ca = 1.0f - s, cb = s;
+          const float den = ca * ca * w0 + cb * cb * w1;
+          if (den > kEps) {
+            const float f0 = fminf((ca * w0) / den, 2.0f), f1 = fminf((cb * w1) / den, 2.0f);
+            if (w0 > 0.0f) add_pin(a.acc, u0, push * f0);
+            if (w1 > 0.0f) add_pin(a.acc, u1, push * f1);
+          }
+        }
+      }
+}
+
 // ---------------- sc_apply: shaders/self_collision_apply.wgsl:57-177
 __global__ void k_apply(uint32_t n, const float4* __restrict__ x4, float4* __restrict__ p4,
                         const float* __restrict__ local_len, int32_t* __restrict__ acc, float relief, int enable_relief,

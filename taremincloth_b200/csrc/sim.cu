@@ -353,6 +353,97 @@ struct BoneSdfState {
   BakeGpu bake;
 };
 
+// Collider edges of the mesh-collider triangles (extract_collider_edges,
+// mesh.rs:1503-1565) and their grid (build_collider_edge_grid,
+// spatial_hash.rs:463-528): every cell an edge passes through, sampled at
+// half-cell steps, registered once per distinct hash bucket.  Edges are kept
+// in first-seen order (the reference's hash-map order differs; the contacts
+// are integer sums with no cap, so the result does not depend on it).
+constexpr uint32_t kColEdgeTable = 32768;
+inline int32_t sat_i32(float f) {
+  if (!(f == f)) return 0;
+  if (f <= -2147483648.f) return INT32_MIN;
+  if (f >= 2147483647.f) return INT32_MAX;
+  return int32_t(f);
+}
+static void build_collider_edges(const std::vector<MeshTri>& tris, float cell, std::vector<ColEdge>& out,
+                                 std::vector<uint32_t>& cs, std::vector<uint32_t>& srt) {
+  out.clear();
+  std::map<std::array<uint32_t, 6>, uint32_t> at;
+  auto bits = [](const float* p, uint32_t* b) { std::memcpy(b, p, 12); };
+  for (const MeshTri& t : tris) {
+    const float* P[3] = {&t.p0f.x, &t.p1t.x, &t.p2r.x};
+    const float e1[3] = {P[1][0] - P[0][0], P[1][1] - P[0][1], P[1][2] - P[0][2]};
+    const float e2[3] = {P[2][0] - P[0][0], P[2][1] - P[0][1], P[2][2] - P[0][2]};
+    const float cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    const float cl = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    const float tn[3] = {cl > 1e-12f ? cr[0] / cl : 0.f, cl > 1e-12f ? cr[1] / cl : 0.f, cl > 1e-12f ? cr[2] / cl : 0.f};
+    uint32_t tf;
+    std::memcpy(&tf, &t.fl.x, 4);
+    const uint32_t single = tf & 1u;
+    for (int k = 0; k < 3; ++k) {
+      const float *a = P[k], *b = P[(k + 1) % 3];
+      std::array<uint32_t, 6> key;
+      uint32_t ba[3], bb[3];
+      bits(a, ba);
+      bits(b, bb);
+      const bool a_first = std::lexicographical_compare(ba, ba + 3, bb, bb + 3);
+      for (int j = 0; j < 3; ++j) { key[j] = a_first ? ba[j] : bb[j]; key[3 + j] = a_first ? bb[j] : ba[j]; }
+      auto it = at.find(key);
+      if (it == at.end()) {
+        at.emplace(key, uint32_t(out.size()));
+        float fb;
+        std::memcpy(&fb, &single, 4);
+        out.push_back(ColEdge{make_float4(a[0], a[1], a[2], t.p1t.w), make_float4(b[0], b[1], b[2], t.p0f.w),
+                              make_float4(tn[0], tn[1], tn[2], fb)});
+      } else {
+        ColEdge& c = out[it->second];
+        c.p0t.w = std::fmax(c.p0t.w, t.p1t.w);
+        c.p1f.w = (c.p1f.w + t.p0f.w) * 0.5f;
+        c.nfl.x += tn[0]; c.nfl.y += tn[1]; c.nfl.z += tn[2];
+        uint32_t f;
+        std::memcpy(&f, &c.nfl.w, 4);
+        f &= single;
+        std::memcpy(&c.nfl.w, &f, 4);
+      }
+    }
+  }
+  for (ColEdge& c : out) {
+    const float nl = std::sqrt(c.nfl.x * c.nfl.x + c.nfl.y * c.nfl.y + c.nfl.z * c.nfl.z);
+    if (nl > 1e-6f) { c.nfl.x /= nl; c.nfl.y /= nl; c.nfl.z /= nl; }
+    else { c.nfl.x = c.nfl.y = c.nfl.z = 0.f; }
+  }
+  const float safe = std::fmax(cell, 1e-4f), pitch = safe * 0.5f;
+  const uint32_t T = kColEdgeTable;
+  std::vector<uint32_t> cnt(T, 0), hs;
+  std::vector<std::pair<uint32_t, uint32_t>> ent;
+  for (uint32_t ei = 0; ei < out.size(); ++ei) {
+    const ColEdge& c = out[ei];
+    const float dx = c.p1f.x - c.p0t.x, dy = c.p1f.y - c.p0t.y, dz = c.p1f.z - c.p0t.z;
+    const float len = std::sqrt(dx * dx + dy * dy + dz * dz);
+    const float sf = std::ceil(len / pitch);
+    size_t steps = (sf == sf && sf > 0.f) ? (sf >= 4096.f ? 4096 : size_t(sf)) : 0;
+    steps = std::min<size_t>(std::max<size_t>(steps, 1), 4096);
+    hs.clear();
+    for (size_t k = 0; k <= steps; ++k) {
+      const float t = float(k) / float(steps);
+      const float px = c.p0t.x + dx * t, py = c.p0t.y + dy * t, pz = c.p0t.z + dz * t;
+      const uint32_t h = ((uint32_t)sat_i32(std::floor(px / safe)) * 73856093u ^
+                          (uint32_t)sat_i32(std::floor(py / safe)) * 19349663u ^
+                          (uint32_t)sat_i32(std::floor(pz / safe)) * 83492791u) % T;
+      hs.push_back(h);
+    }
+    std::sort(hs.begin(), hs.end());
+    hs.erase(std::unique(hs.begin(), hs.end()), hs.end());
+    for (uint32_t h : hs) { cnt[h]++; ent.push_back({h, ei}); }
+  }
+  cs.assign(T + 1, 0);
+  for (uint32_t i = 0; i < T; ++i) cs[i + 1] = cs[i] + cnt[i];
+  std::vector<uint32_t> cur(cs.begin(), cs.end() - 1);
+  srt.assign(ent.size(), 0);
+  for (const auto& e : ent) srt[cur[e.first]++] = e.second;
+}
+
 // Learned warm start state of one simulator: the network, the correction of
 // the previous substep, the in-kernel residual judge and the recorded
 // training snapshots (features, target correction / L, free mask).
@@ -411,6 +502,34 @@ struct Sim {
   // colliders
   std::vector<Prim> prims_h;
   std::vector<MeshTri> tris_h;
+  // edge colliders (edge_collision.wgsl; simulation/mod.rs:1007-1025): off by default
+  bool edge_collision = false;
+  float edge_mscale = 1.f, edge_moff = 0.f;
+  std::vector<ColEdge> cedges_h;
+  DBuf<ColEdge> cedges;
+  DBuf<uint32_t> ce_cs, ce_srt;
+  float ce_cell = 0.01f;  // the grid's cell, fixed when it is built (the reference's is fixed at creation)
+  bool edge_active() const { return edge_collision && has_colliders() && ne > 0; }
+  void rebuild_collider_edges() {
+    std::vector<uint32_t> cs, srt;
+    ce_cell = m.cell;
+    build_collider_edges(tris_h, ce_cell, cedges_h, cs, srt);
+    cedges.upload(cedges_h, st);
+    ce_cs.upload(cs, st);
+    ce_srt.upload(srt, st);
+    TC_CK(cudaStreamSynchronize(st));
+    mark();
+  }
+  // edge colliders after the final pins, then the apply pass (dispatch.rs:254-283)
+  void encode_edge_collision() {
+    EdgeColArgs a{ne, uint32_t(cedges_h.size()), edges.p, x4.p, p4.p, cedges.p, ce_cs.p, ce_srt.p, ce_cell,
+                  kColEdgeTable, edge_mscale, edge_moff, acc.p};
+    timed("edge_collision", [&] { k_edge_collision<<<grid(ne, 256), 256, 0, st>>>(a); });
+    timed("edge_apply", [&] {
+      k_apply<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, local_len.p, acc.p, relief, enable_relief ? 1 : 0,
+                                             max_disp_ratio);
+    });
+  }
   DBuf<Prim> prims;
   DBuf<MeshTri> tris;
   DBuf<float4> bounds, cl16, cl256;
@@ -799,7 +918,7 @@ struct Sim {
   // (simulation/mod.rs:2613-2670) and the two conservative culling levels.
   void upload_tris() {
     const uint32_t T = uint32_t(tris_h.size());
-    if (T == 0) { mark(); graph_ntris = 0; return; }
+    if (T == 0) { mark(); graph_ntris = 0; rebuild_collider_edges(); return; }
     auto cen = [](const MeshTri& t, int a) {
       const float* p0 = &t.p0f.x; const float* p1 = &t.p1t.x; const float* p2 = &t.p2r.x;
       return (p0[a] + p1[a] + p2[a]) / 3.0f;
@@ -857,6 +976,7 @@ struct Sim {
     const void* after[4] = {tris.p, bounds.p, cl16.p, cl256.p};
     if (T != graph_ntris || std::memcmp(before, after, sizeof before) != 0) mark();
     graph_ntris = T;
+    rebuild_collider_edges();
   }
 
   // ---- pins
@@ -1132,7 +1252,9 @@ struct Sim {
     a.fallbacks = nullptr;
     return a;
   }
-  bool can_cluster() const { return !inst_vert_off.empty() && cl_max_active > 0 && !self_collision && nsw == 0; }
+  bool can_cluster() const {
+    return !inst_vert_off.empty() && cl_max_active > 0 && !self_collision && nsw == 0 && !edge_collision;
+  }
   // bins: contiguous runs of instances, balanced by vertex count; the
   // constraint permutations are sorted by (bin, colour, original index)
   void build_cluster_tables() {
@@ -1292,7 +1414,7 @@ struct Sim {
         encode_substep_ws_colors(sp, use_coupled, itn, kk, fa);
       } else {
         timed("predict", [&] { k_predict<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp); });
-        SolverArgs a = solver_args(sp, 1, use_coupled, !self_collision);
+        SolverArgs a = solver_args(sp, 1, use_coupled, !(self_collision || edge_active()));
         timed("ws_check", [&] { encode_ws_res_pred(sp.dt, a.ca.bone.nbones > 0); });
         timed("ws_mlp", [&] { ws.net.infer(nullptr, &fa, ws.ppred.p, nullptr, x4.p, p4.p, local_len.p); });
         a.skip_predict = true;
@@ -1309,7 +1431,8 @@ struct Sim {
         a.fallbacks = ws.fallbacks.p;
         timed("solver", [&] { launch_persistent(a); });
       }
-      if (self_collision) {
+      if (self_collision || edge_active()) {
+        if (edge_active()) encode_edge_collision();
         if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
         if (nsw) timed("final_sewing", [&] { launch_sewing(sp.dt); });
         timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp.dt); });
@@ -1485,11 +1608,12 @@ struct Sim {
     }
     if (persistent && can_persist() && !profiling && !track_residual && !ws_recording()) {
       const SubstepParams sp = make_sp(dt / float(substeps));
-      if (!self_collision) {
+      if (!self_collision && !edge_active()) {
         launch_persistent(solver_args(sp, substeps, use_coupled, true));
       } else {
         for (uint32_t s = 0; s < substeps; ++s) {
           launch_persistent(solver_args(sp, 1, use_coupled, false));
+          if (edge_active()) encode_edge_collision();
           if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
           launch_sewing(sp.dt);  // final sewing (dispatch.rs:323-337)
           k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp.dt);
@@ -1551,6 +1675,7 @@ struct Sim {
       }
       if (hascol && !use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
       if (npins) timed("pin", [&] { launch_k(k_pin, grid(npins, 128), 128, npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
+      if (edge_active()) encode_edge_collision();
       if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
       if (nsw) timed("final_sewing", [&] { launch_sewing(dts); });
       timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, dts); });
@@ -2117,6 +2242,20 @@ tc_status tc_reset(tc_sim* s) {
   });
 }
 
+// ---- edge colliders (simulation/mod.rs:1007-1025, lib.rs:2736-2749)
+tc_status tc_set_enable_edge_collision(tc_sim* s, int enable) {
+  return guard([&] { Sim& m = S(s); m.edge_collision = enable != 0; m.mark(); });
+}
+tc_status tc_set_edge_margin_scale(tc_sim* s, float scale) {
+  return guard([&] { Sim& m = S(s); m.edge_mscale = std::fmax(scale, 1.f); m.mark(); });
+}
+tc_status tc_set_edge_margin_offset(tc_sim* s, float offset) {
+  return guard([&] { Sim& m = S(s); m.edge_moff = std::fmax(offset, 0.f); m.mark(); });
+}
+tc_status tc_get_num_collider_edges(tc_sim* s, uint32_t* count) {
+  return guard([&] { need(count != nullptr, "count required"); *count = uint32_t(S(s).cedges_h.size()); });
+}
+
 // ---- sewing settings (simulation/mod.rs:1211-1420, lib.rs:2798-2925)
 tc_status tc_get_num_sewing_constraints(tc_sim* s, uint32_t* count) {
   return guard([&] { need(count != nullptr, "count required"); *count = S(s).nsw; });
@@ -2340,7 +2479,14 @@ tc_status tc_set_mesh_collider_triangles(tc_sim* s, const float* t, uint32_t T, 
   });
 }
 tc_status tc_clear_colliders(tc_sim* s) {
-  return guard([&] { Sim& m = S(s); m.prims_h.clear(); m.tris_h.clear(); m.graph_ntris = 0; m.mark(); });
+  return guard([&] {
+    Sim& m = S(s);
+    m.prims_h.clear();
+    m.tris_h.clear();
+    m.graph_ntris = 0;
+    m.rebuild_collider_edges();  // no triangles: no collider edges (mod.rs:2731-2736)
+    m.mark();
+  });
 }
 
 tc_status tc_set_pin(tc_sim* s, uint32_t v, const float target[3], float w) {

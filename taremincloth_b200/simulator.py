@@ -219,6 +219,21 @@ class ClothSimulator:
         out = self._out(out_array)
         self._c(self._L.tc_get_positions(self._h, _ptr(out), out.size))
 
+    # ---------------- edge colliders (lib.rs:2736-2749)
+    def set_enable_edge_collision(self, enable):
+        self._c(self._L.tc_set_enable_edge_collision(self._h, int(bool(enable))))
+
+    def set_edge_margin_scale(self, scale):
+        self._c(self._L.tc_set_edge_margin_scale(self._h, float(scale)))
+
+    def set_edge_margin_offset(self, offset):
+        self._c(self._L.tc_set_edge_margin_offset(self._h, float(offset)))
+
+    def get_num_collider_edges(self):
+        v = C.c_uint32()
+        self._c(self._L.tc_get_num_collider_edges(self._h, C.byref(v)))
+        return v.value
+
     # ---------------- sewing (lib.rs:2798-2925)
     def get_num_sewing_constraints(self):
         v = C.c_uint32()
