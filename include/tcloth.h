@@ -247,6 +247,19 @@ tc_status tc_bake_bone_sdf(const float *mesh_verts, uint32_t n_verts, const int3
                            uint32_t resolution, float margin, float weight_threshold, float blend_k, float friction,
                            float thickness, float restitution, int close_open_boundaries, int device, tc_bake **out);
 /* out = width, height, depth, number of active bones */
+/* bake_mesh_sdf_gpu (lib.rs:1349-1416; sdf_baker.rs:939-1060, :1114-1326):
+ * the signed distance field of one mesh (open boundary loops capped first
+ * when close_open_boundaries) over its bounding box padded by
+ * max(size x margin, 0.04) + thickness + 0.02 per axis, at voxel_size
+ * (8..2048 voxels per axis): per voxel the distance to the nearest triangle
+ * (the first of equal distances), negative behind its normal, packed as
+ * fp16 (distance, 1).  tc_bake_get gives the texels and infos[20] = local
+ * min, 0, local max, width, uvw scale (4), uvw offset (4), friction,
+ * thickness, restitution, 0; no active bones.  No vertices:
+ * TC_ERR_CUDA, like the reference's error. */
+tc_status tc_bake_mesh_sdf(const float *mesh_verts, uint32_t nv, const int32_t *mesh_tris, uint32_t nt,
+                           float voxel_size, float margin, float friction, float thickness, float restitution,
+                           int close_open_boundaries, int device, tc_bake **out);
 tc_status tc_bake_dims(tc_bake *b, uint32_t out[4]);
 /* texels (w*h*d), infos (n_active x 20), active (source bone index per
  * active bone), bind (n_active x 16); any may be NULL */

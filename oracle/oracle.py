@@ -48,6 +48,8 @@ def lib():
         L.ocl_get_sewing.argtypes = [P, P, P, P, P, P, P]
         L.ocl_get_sewing.restype = C.c_int
         L.ocl_get_bending_gate.argtypes = [P, fp]
+        L.ocl_bake_mesh_sdf.argtypes = [P, C.c_int, P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                         C.c_float, P, P, P]
         L.ocl_set_edge_collision.argtypes = [P, C.c_int, C.c_float, C.c_float]
         L.ocl_num_collider_edges.argtypes = [P]
         L.ocl_num_collider_edges.restype = C.c_int
@@ -392,3 +394,18 @@ def _set_ee_interval(self, interval):
 
 OracleSim.set_self_collision_substep_interval = _set_sc_interval
 OracleSim.set_self_collision_ee_substep_interval = _set_ee_interval
+
+
+def bake_mesh_sdf(verts, tris, voxel_size=0.004, margin=0.02, friction=0.5, thickness=0.005, restitution=0.0):
+    """Single-mesh SDF of a closed mesh: (dims (3,), info (20,), texels (d, h, w) uint32)."""
+    L = lib()
+    v = np.ascontiguousarray(verts, dtype=_f).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 3)
+    dims = np.zeros(3, _u)
+    info = np.zeros(20, _f)
+    L.ocl_bake_mesh_sdf(_ptr(v), v.shape[0], _ptr(t), t.shape[0], voxel_size, margin, friction, thickness,
+                        restitution, _ptr(dims), _ptr(info), None)
+    tex = np.zeros(int(dims[0]) * int(dims[1]) * int(dims[2]), _u)
+    L.ocl_bake_mesh_sdf(_ptr(v), v.shape[0], _ptr(t), t.shape[0], voxel_size, margin, friction, thickness,
+                        restitution, _ptr(dims), _ptr(info), _ptr(tex))
+    return dims, info, tex.reshape(int(dims[2]), int(dims[1]), int(dims[0]))

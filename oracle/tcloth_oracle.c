@@ -1729,6 +1729,91 @@ void ocl_bone_prep(int nt, const float *skinned4, const float *inv_mats, const u
         o[12] = nrm.x; o[13] = nrm.y; o[14] = nrm.z; o[15] = srcw[4 * t + 3];
     }
 }
+/* bake_mesh_sdf_gpu without boundary capping (closed meshes):
+ * mesh_sdf_domain / mesh_sdf_bone_info / collect_mesh_bake_triangles
+ * (sdf_baker.rs:939-1060) and bake_mesh_sdf.wgsl, every triangle of every
+ * voxel in order.  dims and info are written; texels (w x h x d) when given. */
+void ocl_bake_mesh_sdf(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
+                       float friction, float thickness, float restitution, uint32_t *dims, float *info,
+                       uint32_t *texels) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, size[3];
+    for (int v = 0; v < nv; v++)
+        for (int k = 0; k < 3; k++) { lo[k] = fminf(lo[k], verts[3 * v + k]); hi[k] = fmaxf(hi[k], verts[3 * v + k]); }
+    float vs = fmaxf(voxel, 0.001f);
+    for (int k = 0; k < 3; k++) {
+        size[k] = fmaxf(hi[k] - lo[k], 0.05f);
+        float pad = fmaxf(size[k] * margin, 0.04f) + fmaxf(thickness, 0.0f) + 0.02f;
+        lo[k] -= pad; hi[k] += pad;
+        size[k] = hi[k] - lo[k];
+        float raw = ceilf(size[k] / vs);
+        double r = (raw == raw && raw > 0.0f) ? (double)raw : 0.0;
+        dims[k] = (uint32_t)(r < 8.0 ? 8.0 : (r > 2048.0 ? 2048.0 : r));
+    }
+    for (int k = 0; k < 20; k++) info[k] = 0.0f;
+    for (int k = 0; k < 3; k++) {
+        info[k] = lo[k]; info[4 + k] = hi[k]; info[8 + k] = 1.0f / size[k]; info[12 + k] = -lo[k] / size[k];
+    }
+    info[7] = (float)dims[0]; info[16] = friction; info[17] = thickness; info[18] = restitution;
+    if (!texels) return;
+    /* triangles and unit normals (zero cross product: (0, 1, 0)) */
+    float *T = (float *)malloc(sizeof(float) * 12 * ((size_t)nt + 1));
+    int m = 0;
+    for (int t = 0; t < nt; t++) {
+        int i0 = tris[3 * t], i1 = tris[3 * t + 1], i2 = tris[3 * t + 2];
+        if (i0 < 0 || i1 < 0 || i2 < 0 || i0 >= nv || i1 >= nv || i2 >= nv) continue;
+        const float *p0 = verts + 3 * i0, *p1 = verts + 3 * i1, *p2 = verts + 3 * i2;
+        v3 a = V3(p0[0], p0[1], p0[2]), b = V3(p1[0], p1[1], p1[2]), c = V3(p2[0], p2[1], p2[2]);
+        v3 cr = vcross(vsub(b, a), vsub(c, a));
+        float l2 = cr.x * cr.x + cr.y * cr.y + cr.z * cr.z;
+        v3 n = V3(0.0f, 1.0f, 0.0f);
+        if (l2 > 1e-12f) { float il = 1.0f / sqrtf(l2); n = V3(cr.x * il, cr.y * il, cr.z * il); }
+        float *q = T + 12 * m++;
+        q[0] = a.x; q[1] = a.y; q[2] = a.z; q[3] = b.x; q[4] = b.y; q[5] = b.z;
+        q[6] = c.x; q[7] = c.y; q[8] = c.z; q[9] = n.x; q[10] = n.y; q[11] = n.z;
+    }
+    if (m == 0) { memset(T, 0, 12 * sizeof(float)); T[10] = 1.0f; m = 1; }
+    uint32_t W = dims[0], H = dims[1], D = dims[2];
+    float iw = 1.0f / (float)W, ih = 1.0f / (float)H, id = 1.0f / (float)D;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int z = 0; z < (int)D; z++)
+        for (uint32_t y = 0; y < H; y++)
+            for (uint32_t x = 0; x < W; x++) {
+                v3 p = V3(lo[0] + ((float)x + 0.5f) * iw * (hi[0] - lo[0]), lo[1] + ((float)y + 0.5f) * ih * (hi[1] - lo[1]),
+                          lo[2] + ((float)z + 0.5f) * id * (hi[2] - lo[2]));
+                float md = 1e10f, best = 10.0f;
+                for (int t = 0; t < m; t++) {
+                    const float *q = T + 12 * t;
+                    v3 a = V3(q[0], q[1], q[2]), b = V3(q[3], q[4], q[5]), c = V3(q[6], q[7], q[8]);
+                    v3 ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a), cp;
+                    float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+                    v3 bp = vsub(p, b);
+                    float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+                    v3 cpv = vsub(p, c);
+                    float d5 = vdot(ab, cpv), d6 = vdot(ac, cpv);
+                    float vc = d1 * d4 - d3 * d2, vb = d5 * d2 - d1 * d6, va = d3 * d6 - d5 * d4;
+                    if (d1 <= 0.0f && d2 <= 0.0f) cp = a;
+                    else if (d3 >= 0.0f && d4 <= d3) cp = b;
+                    else if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) cp = vadd(a, vmul(ab, d1 / (d1 - d3)));
+                    else if (d6 >= 0.0f && d5 <= d6) cp = c;
+                    else if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) cp = vadd(a, vmul(ac, d2 / (d2 - d6)));
+                    else if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f)
+                        cp = vadd(b, vmul(vsub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
+                    else {
+                        float den = 1.0f / (va + vb + vc);
+                        cp = vadd(vadd(a, vmul(ab, vb * den)), vmul(ac, vc * den));
+                    }
+                    v3 diff = vsub(p, cp);
+                    float dsq = vdot(diff, diff);
+                    if (dsq < md) {
+                        md = dsq;
+                        best = sqrtf(dsq) * (vdot(diff, V3(q[9], q[10], q[11])) >= 0.0f ? 1.0f : -1.0f);
+                    }
+                }
+                texels[((size_t)z * H + y) * W + x] = (uint32_t)f2h(best) | ((uint32_t)f2h(1.0f) << 16);
+            }
+    free(T);
+}
+
 /* params: 16 words per bone (GpuBakeParams); every triangle of the bone in order */
 void ocl_bone_bake(int np, const uint32_t *params, const float *tris16, uint32_t *atlas) {
     for (int bi = 0; bi < np; bi++) {

@@ -115,6 +115,11 @@ void ocl_bone_skin(int nv, const float *rest4, const uint32_t *bidx4, const floa
 void ocl_bone_prep(int nt, const float *skinned4, const float *inv_mats16, const uint32_t *src4,
                    const float *srcw4, float *out16);
 void ocl_bone_bake(int nparams, const uint32_t *params16, const float *tris16, uint32_t *atlas);
+/* single-mesh SDF bake of a closed mesh (sdf_baker.rs:939-1060,
+ * bake_mesh_sdf.wgsl): dims[3], info[20]; texels (w x h x d) when non-NULL */
+void ocl_bake_mesh_sdf(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
+                       float friction, float thickness, float restitution, uint32_t *dims, float *info,
+                       uint32_t *texels);
 void ocl_set_bone_sdf(OSim *s, uint32_t w, uint32_t h, uint32_t d, const uint32_t *atlas, int nbones,
                       const float *infos20, const float *xforms32);
 

@@ -3,5 +3,5 @@
 Re-exports the B200 implementation so code written against
 ``import taremin_cloth_core`` runs unchanged for the XPBD substep.
 """
-from taremincloth_b200.simulator import (ClothSimulator, bake_bone_sdf_gpu, get_gpu_device_name,  # noqa: F401
-                                        is_gpu_available)
+from taremincloth_b200.simulator import (ClothSimulator, bake_bone_sdf_gpu, bake_mesh_sdf_gpu,  # noqa: F401
+                                        get_gpu_device_name, is_gpu_available)

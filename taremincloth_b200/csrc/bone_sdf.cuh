@@ -286,6 +286,88 @@ __global__ void __launch_bounds__(256) k_bone_bake(const BakeParams* __restrict_
   atlas[(size_t(gz) * P.total_h + gy) * pitch + gx] = pack_half2(s.best_signed, s.best_alpha);
 }
 
+// ---- single-mesh SDF (bake_mesh_sdf.wgsl:1-121; sdf_baker.rs:1114-1326):
+// per voxel the signed distance to the nearest triangle, the first of equal
+// distances winning (strict <), the sign from the triangle's normal; alpha 1.
+// Voxel centres at local_min + ((i + 0.5) * (1 / dim)) * (local_max - local_min).
+// Same brick layout and conservative sphere culling as k_bone_bake (a triangle
+// is skipped only when no point of its sphere can come closer).
+struct MeshBakeParams {
+  float lmin[3], lmax[3];
+  uint32_t w, h, d, ntri;
+};
+__device__ __forceinline__ void mesh_visit(BakeState& s, V3 p, const BakeTri& tri) {
+  const V3 a = mk(tri.p0w0), b = mk(tri.p1w1), c = mk(tri.p2w2);
+  const V3 ab = b - a, ac = c - a, ap = p - a;
+  const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+  V3 cp;
+  if (d1 <= 0.f && d2 <= 0.f) {
+    cp = a;
+  } else {
+    const V3 bp = p - b;
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    const float vc = d1 * d4 - d3 * d2;
+    if (d3 >= 0.f && d4 <= d3) {
+      cp = b;
+    } else if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+      cp = a + ab * (d1 / (d1 - d3));
+    } else {
+      const V3 cpv = p - c;
+      const float d5 = dot(ab, cpv), d6 = dot(ac, cpv);
+      const float vb = d5 * d2 - d1 * d6;
+      const float va = d3 * d6 - d5 * d4;
+      if (d6 >= 0.f && d5 <= d6) {
+        cp = c;
+      } else if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+        cp = a + ac * (d2 / (d2 - d6));
+      } else if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
+        cp = b + (c - b) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)));
+      } else {
+        const float denom = 1.0f / ((va + vb) + vc);
+        cp = (a + ab * (vb * denom)) + ac * (vc * denom);
+      }
+    }
+  }
+  const V3 diff = p - cp;
+  const float d_sq = dot(diff, diff);
+  if (d_sq < s.min_d2) {
+    s.min_d2 = d_sq;
+    s.reach = bake_reach(d_sq);
+    s.best_signed = sqrtf(d_sq) * (dot(diff, mk(tri.n_bmask)) >= 0.0f ? 1.0f : -1.0f);
+  }
+}
+__global__ void __launch_bounds__(256) k_mesh_bake(MeshBakeParams P, const BakeTri* __restrict__ tris,
+                                                   const float4* __restrict__ sph, const float4* __restrict__ tsph,
+                                                   uint32_t* __restrict__ out) {
+  const uint32_t bx = (P.w + 7) / 8, by = (P.h + 7) / 8;
+  const uint32_t blk = blockIdx.x;
+  const uint32_t ox = (blk % bx) * 8, oy = ((blk / bx) % by) * 8, oz = (blk / (bx * by)) * 4;
+  if (oz >= P.d) return;  // whole block
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t vx = ox + (warp & 1) * 4 + (lane & 3);
+  const uint32_t vy = oy + ((warp >> 1) & 1) * 4 + ((lane >> 2) & 3);
+  const uint32_t vz = oz + (warp >> 2) * 2 + (lane >> 4);
+  const bool valid = vx < P.w && vy < P.h && vz < P.d;
+  const V3 inv = mk(1.0f / float(P.w), 1.0f / float(P.h), 1.0f / float(P.d));
+  const V3 uvw = mk((float(vx) + 0.5f) * inv.x, (float(vy) + 0.5f) * inv.y, (float(vz) + 0.5f) * inv.z);
+  const V3 p = mk(P.lmin[0] + uvw.x * (P.lmax[0] - P.lmin[0]), P.lmin[1] + uvw.y * (P.lmax[1] - P.lmin[1]),
+                  P.lmin[2] + uvw.z * (P.lmax[2] - P.lmin[2]));
+  BakeState s{1e10f, -1.0f, 10.0f, 1.0f, bake_reach(1e10f)};
+  for (uint32_t k = 0; k * 32u < P.ntri; ++k) {
+    const bool skip_tile = !valid || bake_far(s, p, __ldg(tsph + k));
+    if (__all_sync(0xffffffffu, skip_tile)) continue;
+    const uint32_t e = min(32u, P.ntri - k * 32u);
+    for (uint32_t q = 0; q < e; ++q) {
+      const uint32_t t = k * 32u + q;
+      if (skip_tile || bake_far(s, p, __ldg(sph + t))) continue;
+      const BakeTri tri{__ldg(&tris[t].p0w0), __ldg(&tris[t].p1w1), __ldg(&tris[t].p2w2), __ldg(&tris[t].n_bmask)};
+      mesh_visit(s, p, tri);
+    }
+  }
+  if (!valid) return;
+  out[(size_t(vz) * P.h + vy) * P.w + vx] = pack_half2(s.best_signed, 1.0f);
+}
+
 // ---- sampling: trilinear, clamp to edge, texel centres at (i + 0.5) / size
 __device__ __forceinline__ float2 unpack_half2(uint32_t u) {
   return make_float2(__half2float(__ushort_as_half((unsigned short)(u & 0xFFFFu))),

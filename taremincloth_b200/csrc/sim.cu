@@ -3407,6 +3407,98 @@ tc_status tc_bake_bone_sdf(const float* mesh_verts, uint32_t nv, const int32_t* 
   });
 }
 
+// bake_mesh_sdf_gpu (lib.rs:1349-1416; sdf_baker.rs:939-1060, :1114-1326):
+// the signed distance field of one mesh over its padded bounding box.
+tc_status tc_bake_mesh_sdf(const float* mesh_verts, uint32_t nv, const int32_t* mesh_tris, uint32_t nt,
+                           float voxel_size, float margin, float friction, float thickness, float restitution,
+                           int close_open_boundaries, int device, tc_bake** out) {
+  return guard([&] {
+    need(out != nullptr, "out required");
+    *out = nullptr;
+    if (nv == 0) throw TcError(TC_ERR_CUDA, "GPU mesh SDF bake failed: the mesh has no vertices");
+    need(mesh_verts != nullptr && (nt == 0 || mesh_tris != nullptr), "arrays required");
+    std::vector<float> verts(mesh_verts, mesh_verts + 3 * size_t(nv));
+    std::vector<int32_t> tris(mesh_tris, mesh_tris + 3 * size_t(nt));
+    std::vector<std::vector<float>> no_weights;
+    if (close_open_boundaries) close_open_loops(verts, tris, no_weights);
+    const size_t NV = verts.size() / 3, NT = tris.size() / 3;
+    // mesh_sdf_domain (sdf_baker.rs:939-982)
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t v = 0; v < NV; ++v)
+      for (int k = 0; k < 3; ++k) { lo[k] = std::fmin(lo[k], verts[3 * v + k]); hi[k] = std::fmax(hi[k], verts[3 * v + k]); }
+    float size[3];
+    uint32_t dim[3];
+    const float vs = std::fmax(voxel_size, 0.001f);
+    for (int k = 0; k < 3; ++k) {
+      size[k] = std::fmax(hi[k] - lo[k], 0.05f);
+      const float pad = (std::fmax(size[k] * margin, 0.04f) + std::fmax(thickness, 0.f)) + 0.02f;
+      lo[k] -= pad;
+      hi[k] += pad;
+      size[k] = hi[k] - lo[k];
+      const float raw = std::ceil(size[k] / vs);
+      const double r = (raw == raw && raw > 0.f) ? double(raw) : 0.0;
+      dim[k] = uint32_t(std::min(std::max(r, 8.0), 2048.0));
+    }
+    std::unique_ptr<tc_bake> R(new tc_bake);
+    R->w = dim[0]; R->h = dim[1]; R->d = dim[2];
+    // mesh_sdf_bone_info (sdf_baker.rs:984-1016)
+    R->infos.assign(20, 0.f);
+    for (int k = 0; k < 3; ++k) {
+      R->infos[k] = lo[k];
+      R->infos[4 + k] = hi[k];
+      R->infos[8 + k] = 1.0f / size[k];
+      R->infos[12 + k] = -lo[k] / size[k];
+    }
+    R->infos[7] = float(dim[0]);
+    R->infos[16] = friction; R->infos[17] = thickness; R->infos[18] = restitution;
+    // collect_mesh_bake_triangles (sdf_baker.rs:1018-1060)
+    std::vector<tcloth::BakeTri> all;
+    for (size_t t = 0; t < NT; ++t) {
+      const int32_t i0 = tris[3 * t], i1 = tris[3 * t + 1], i2 = tris[3 * t + 2];
+      if (i0 < 0 || i1 < 0 || i2 < 0 || size_t(i0) >= NV || size_t(i1) >= NV || size_t(i2) >= NV) continue;
+      const float* p0 = &verts[3 * size_t(i0)];
+      const float* p1 = &verts[3 * size_t(i1)];
+      const float* p2 = &verts[3 * size_t(i2)];
+      const float e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+      const float e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+      const float c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      const float l2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+      float nrm[3] = {0.f, 1.f, 0.f};
+      if (l2 > 1e-12f) {
+        const float il = 1.0f / std::sqrt(l2);
+        nrm[0] = c[0] * il; nrm[1] = c[1] * il; nrm[2] = c[2] * il;
+      }
+      all.push_back(tcloth::BakeTri{make_float4(p0[0], p0[1], p0[2], 0.f), make_float4(p1[0], p1[1], p1[2], 0.f),
+                                    make_float4(p2[0], p2[1], p2[2], 0.f), make_float4(nrm[0], nrm[1], nrm[2], 0.f)});
+    }
+    if (all.empty())
+      all.push_back(tcloth::BakeTri{make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
+                                    make_float4(0, 1, 0, 0)});
+    TC_CK(cudaSetDevice(device));
+    cudaStream_t st = nullptr;
+    TC_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); } } sg{st};
+    tcloth::BakeGpu G;
+    G.nt = uint32_t(all.size());
+    G.tris.upload(all, st);
+    G.setup_tiles(tcloth::make_bake_tiles({0u}, {G.nt}), st);
+    tcloth::k_bone_tri_spheres<<<(G.nt + 255) / 256, 256, 0, st>>>(G.nt, G.tris.p, G.sph.p);
+    tcloth::k_bone_tile_spheres<<<(G.ntiles + 127) / 128, 128, 0, st>>>(G.ntiles, G.tile_first.p, G.tile_cnt.p,
+                                                                         G.sph.p, G.tsph.p);
+    tcloth::MeshBakeParams P{{lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}, dim[0], dim[1], dim[2], G.nt};
+    const size_t nvox = size_t(dim[0]) * dim[1] * dim[2];
+    tcloth::DBuf<uint32_t> vox;
+    vox.alloc(nvox);
+    const uint32_t nblk = ((dim[0] + 7) / 8) * ((dim[1] + 7) / 8) * ((dim[2] + 3) / 4);
+    tcloth::k_mesh_bake<<<nblk, 256, 0, st>>>(P, G.tris.p, G.sph.p, G.tsph.p, vox.p);
+    R->texels.resize(nvox);
+    TC_CK(cudaMemcpyAsync(R->texels.data(), vox.p, nvox * 4, cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaStreamSynchronize(st));
+    TC_CK(cudaGetLastError());
+    *out = R.release();
+  });
+}
+
 tc_status tc_bake_dims(tc_bake* b, uint32_t out[4]) {
   return guard([&] {
     need(b && out, "bake result and output required");

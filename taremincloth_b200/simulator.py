@@ -81,6 +81,35 @@ def bake_bone_sdf_gpu(mesh_verts, mesh_tris, bone_names, bone_weights, bone_bind
             "active_bones": [names[int(i)] for i in active], "bind_matrices": bind}
 
 
+def bake_mesh_sdf_gpu(mesh_verts, mesh_tris, voxel_size=0.004, margin=0.02, friction=0.5, thickness=0.005,
+                      restitution=0.0, close_open_boundaries=True, device=0):
+    """Signed distance field of one mesh on the GPU (lib.rs:1349-1416).
+    Returns dict(texture_bytes, width, height, depth, bone_info (20,))."""
+    v = np.ascontiguousarray(np.asarray(mesh_verts, _f32))
+    if v.ndim != 2 or v.shape[1] < 3:
+        raise ValueError("mesh_verts must have shape (N, 3)")
+    v = np.ascontiguousarray(v[:, :3])
+    t = np.ascontiguousarray(np.asarray(mesh_tris, np.int32))
+    if t.ndim != 2 or t.shape[1] < 3:
+        raise ValueError("mesh_tris must have shape (M, 3)")
+    t = np.ascontiguousarray(t[:, :3])
+    L = _lib.load()
+    h = C.c_void_p()
+    _lib.check(L.tc_bake_mesh_sdf(_ptr(v), v.shape[0], _ptr(t), t.shape[0], float(voxel_size), float(margin),
+                                  float(friction), float(thickness), float(restitution),
+                                  int(bool(close_open_boundaries)), int(device), C.byref(h)))
+    try:
+        dims = np.zeros(4, _u32)
+        _lib.check(L.tc_bake_dims(h, _ptr(dims)))
+        W, H, D = (int(x) for x in dims[:3])
+        tex = np.zeros(W * H * D, _u32)
+        info = np.zeros(20, _f32)
+        _lib.check(L.tc_bake_get(h, _ptr(tex), _ptr(info), None, None))
+    finally:
+        L.tc_bake_destroy(h)
+    return {"texture_bytes": tex.tobytes(), "width": W, "height": H, "depth": D, "bone_info": info}
+
+
 def is_gpu_available() -> bool:
     try:
         return bool(_lib.load().tc_gpu_available())
