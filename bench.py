@@ -321,15 +321,22 @@ def _warm_start_case(sim, n, dt, sub, iters, steps, ks, rec_frames, every, workl
 
 
 def warm_start_extra(steps):
-    """Learned warm start on the 64x64 sheet (latency-bound, 4,096 vertices)
-    and on the config 4 batch (657,683 vertices, per-colour launches, the
-    launch mode the autotuner picks for it)."""
+    """Learned warm start on the 64x64 sheet (latency-bound, 4,096 vertices),
+    on config 2 (131,072 vertices, self-collision on) and on the config 4
+    batch (657,683 vertices, per-colour launches, the launch mode the
+    autotuner picks for it)."""
     from taremincloth_b200 import ClothSimulator, scenes
     sc = scenes.config1()
     s = scenes.build(ClothSimulator, sc)
     out = {"config1": _warm_start_case(s, len(sc["positions"]), sc["dt"], sc["substeps"], sc["iterations"], steps,
                                        (1, 2), 10, 2, "64x64 poke-grid sheet (4096 vertices), 10 substeps x 5 "
                                        "iterations")}
+    sc = scenes.config2()
+    s2 = scenes.build(ClothSimulator, sc)
+    out["config2"] = _warm_start_case(s2, len(sc["positions"]), sc["dt"], sc["substeps"], sc["iterations"], steps,
+                                      (1, 2), 2, 5, "two 256x256 sheets (131072 vertices) on the icosphere, "
+                                      "self-collision on, 20 substeps x 4 iterations")
+    del s2
     sc = scenes.config4()
     b = scenes.build_batch(sc)
     b.set_launch_config(False)

@@ -509,16 +509,27 @@ struct Sim {
   DBuf<ColEdge> cedges;
   DBuf<uint32_t> ce_cs, ce_srt;
   float ce_cell = 0.01f;  // the grid's cell, fixed when it is built (the reference's is fixed at creation)
+  bool ce_stale = true;   // triangles changed since the collider edges were built
   bool edge_active() const { return edge_collision && has_colliders() && ne > 0; }
+  // built when first needed after the triangles change: frames without edge
+  // collision never pay for it (the reference extracts on every upload)
+  void ensure_collider_edges() {
+    if (ce_stale) rebuild_collider_edges();
+  }
   void rebuild_collider_edges() {
+    ce_stale = false;
     std::vector<uint32_t> cs, srt;
     ce_cell = m.cell;
+    const size_t n_before = cedges_h.size();
     build_collider_edges(tris_h, ce_cell, cedges_h, cs, srt);
+    const void* before[3] = {cedges.p, ce_cs.p, ce_srt.p};
     cedges.upload(cedges_h, st);
     ce_cs.upload(cs, st);
     ce_srt.upload(srt, st);
     TC_CK(cudaStreamSynchronize(st));
-    mark();
+    // a recorded frame holds the pointers and the edge count only
+    const void* after[3] = {cedges.p, ce_cs.p, ce_srt.p};
+    if (cedges_h.size() != n_before || std::memcmp(before, after, sizeof before) != 0) mark();
   }
   // edge colliders after the final pins, then the apply pass (dispatch.rs:254-283)
   void encode_edge_collision() {
@@ -918,7 +929,7 @@ struct Sim {
   // (simulation/mod.rs:2613-2670) and the two conservative culling levels.
   void upload_tris() {
     const uint32_t T = uint32_t(tris_h.size());
-    if (T == 0) { mark(); graph_ntris = 0; rebuild_collider_edges(); return; }
+    if (T == 0) { mark(); graph_ntris = 0; ce_stale = true; return; }
     auto cen = [](const MeshTri& t, int a) {
       const float* p0 = &t.p0f.x; const float* p1 = &t.p1t.x; const float* p2 = &t.p2r.x;
       return (p0[a] + p1[a] + p2[a]) / 3.0f;
@@ -976,7 +987,7 @@ struct Sim {
     const void* after[4] = {tris.p, bounds.p, cl16.p, cl256.p};
     if (T != graph_ntris || std::memcmp(before, after, sizeof before) != 0) mark();
     graph_ntris = T;
-    rebuild_collider_edges();
+    ce_stale = true;
   }
 
   // ---- pins
@@ -1697,6 +1708,7 @@ struct Sim {
   void launch_frame(float dt, uint32_t substeps) {
     if (n == 0) return;
     if (cluster_mode && can_cluster() && cl_stale) build_cluster_tables();  // before any capture
+    if (edge_active()) ensure_collider_edges();                             // before any capture
     // the frame's device time (last_frame_ms) includes the dynamic bone SDF rebake
     TC_CK(cudaEventRecord(ev0, st));
     dynamic_bone_update();
@@ -2253,7 +2265,12 @@ tc_status tc_set_edge_margin_offset(tc_sim* s, float offset) {
   return guard([&] { Sim& m = S(s); m.edge_moff = std::fmax(offset, 0.f); m.mark(); });
 }
 tc_status tc_get_num_collider_edges(tc_sim* s, uint32_t* count) {
-  return guard([&] { need(count != nullptr, "count required"); *count = uint32_t(S(s).cedges_h.size()); });
+  return guard([&] {
+    need(count != nullptr, "count required");
+    Sim& m = S(s);
+    m.ensure_collider_edges();
+    *count = uint32_t(m.cedges_h.size());
+  });
 }
 
 // ---- sewing settings (simulation/mod.rs:1211-1420, lib.rs:2798-2925)
@@ -2484,7 +2501,7 @@ tc_status tc_clear_colliders(tc_sim* s) {
     m.prims_h.clear();
     m.tris_h.clear();
     m.graph_ntris = 0;
-    m.rebuild_collider_edges();  // no triangles: no collider edges (mod.rs:2731-2736)
+    m.ce_stale = true;  // no triangles: no collider edges (mod.rs:2731-2736)
     m.mark();
   });
 }
