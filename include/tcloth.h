@@ -156,6 +156,37 @@ tc_status tc_set_enable_self_collision(tc_sim *s, int enable);
 /* set_self_collision_options (simulation/mod.rs:920-950) */
 tc_status tc_set_self_collision_options(tc_sim *s, float relief_factor, float max_displacement_ratio,
                                         int exclude_neighbors, int enable_normal_untangling, uint32_t max_iterations);
+/* Contact-pair cache ("Active Pair Caching", self-collision algorithm 1;
+ * simulation/mod.rs:36-41, :582-600, :703-715, :799-893; dispatch.rs:1111-1132,
+ * :1249-1290, :1540-1670; lib.rs:2029-2105), off by default.  At the first
+ * substep of a frame one pass over the vertex hash keeps, per vertex, the
+ * quota nearest vertex-triangle and edge-edge candidates within the
+ * thickness plus the safety margin plus (margin_mode 1) a velocity horizon
+ * min(|v| dt_frame horizon_scale, max_horizon); every substep then solves
+ * only those pairs.  quota = clamp(max_pairs / vertices, 1, 8).  With the
+ * final fallback on (default) the last substep of a frame runs the direct
+ * pass on a fresh hash.  set_self_collision_algorithm: 0 direct, 1 pair
+ * cache; 2 (virtual particles) returns TC_ERR_INVALID. */
+tc_status tc_set_enable_pair_cache(tc_sim *s, int enable);
+tc_status tc_get_enable_pair_cache(tc_sim *s, int *enabled);
+tc_status tc_set_self_collision_algorithm(tc_sim *s, uint32_t algo);
+tc_status tc_get_self_collision_algorithm(tc_sim *s, uint32_t *algo);
+/* max pairs clamped to [64, 262144], margin_mode 0 fixed / else velocity
+ * horizon, safety_margin to [0, 0.05], horizon_scale to [0, 4], max_horizon
+ * to [0, 0.1] (set_pair_cache_options, simulation/mod.rs:826-848) */
+tc_status tc_set_pair_cache_options(tc_sim *s, uint32_t max_vt_pairs, uint32_t max_ee_pairs, uint32_t margin_mode,
+                                    float safety_margin, float horizon_scale, float max_horizon);
+tc_status tc_set_enable_pair_cache_final_fallback(tc_sim *s, int enable);
+tc_status tc_get_enable_pair_cache_final_fallback(tc_sim *s, int *enabled);
+/* out = (V-T candidates accepted, E-E candidates accepted, max_vt_pairs,
+ * max_ee_pairs) of the latest broad phase (get_pair_cache_stats) */
+tc_status tc_get_pair_cache_stats(tc_sim *s, uint32_t out[4]);
+/* get_active_pairs (dispatch.rs:1249-1290): counts = (V-T accepted, E-E
+ * accepted, stored V-T pairs, stored E-E pairs); the stored pairs, four
+ * vertex ids each in slot order, go to vt_pairs / ee_pairs up to the given
+ * capacities in pairs (NULL to query the counts only). */
+tc_status tc_get_active_pairs(tc_sim *s, uint32_t counts[4], uint32_t *vt_pairs, size_t vt_capacity,
+                              uint32_t *ee_pairs, size_t ee_capacity);
 tc_status tc_set_coupled_collider(tc_sim *s, int enable);
 tc_status tc_set_auto_coupled_on_low_substeps(tc_sim *s, int enable);
 tc_status tc_set_collider_options(tc_sim *s, int enable_cluster_culling, int enable_single_sided_recovery,

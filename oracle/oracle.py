@@ -89,6 +89,10 @@ def lib():
         L.ocl_get_mesh_triangles.argtypes = [P, fp]
         L.ocl_half_roundtrip.argtypes = [P, C.c_int, P, P]
         L.ocl_set_self_collision_intervals.argtypes = [P, C.c_int, C.c_int]
+        L.ocl_set_pair_cache.argtypes = [P, C.c_int, C.c_int]
+        L.ocl_set_pair_cache_options.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float,
+                                                 C.c_float]
+        L.ocl_get_active_pairs.argtypes = [P, up, P, C.c_size_t, P, C.c_size_t]
         L.ocl_bone_skin_mats.argtypes = [C.c_int, P, P, P]
         L.ocl_bone_skin.argtypes = [C.c_int, P, P, P, P, P]
         L.ocl_bone_prep.argtypes = [C.c_int, P, P, P, P, P]
@@ -239,6 +243,24 @@ class OracleSim:
         lib().ocl_get_bending(self._h, v, r, cp, p0)
         lib().ocl_get_bending_gate(self._h, p1)
         return dict(v=v[:4 * nb].reshape(-1, 4), rest=r[:nb], comp=cp[:nb], pad0=p0[:nb], pad1=p1[:nb])
+
+    # --- contact-pair cache ---------------------------------------------
+    def set_pair_cache(self, enable=True, final_fallback=True):
+        lib().ocl_set_pair_cache(self._h, int(bool(enable)), int(bool(final_fallback)))
+
+    def set_pair_cache_options(self, max_vt_pairs=65536, max_ee_pairs=65536, margin_mode=1, safety_margin=0.005,
+                               horizon_scale=1.3, max_horizon=0.02):
+        lib().ocl_set_pair_cache_options(self._h, int(max_vt_pairs), int(max_ee_pairs), int(margin_mode),
+                                         safety_margin, horizon_scale, max_horizon)
+
+    def active_pairs(self):
+        """(vt_accepted, ee_accepted, vt_pairs (k x 4), ee_pairs (k x 4)) of the latest broad phase."""
+        c = np.zeros(4, _u)
+        lib().ocl_get_active_pairs(self._h, c, None, 0, None, 0)
+        vt = np.zeros((max(int(c[2]), 1), 4), _u)
+        ee = np.zeros((max(int(c[3]), 1), 4), _u)
+        lib().ocl_get_active_pairs(self._h, c, vt.ctypes.data, int(c[2]), ee.ctypes.data, int(c[3]))
+        return int(c[0]), int(c[1]), vt[:int(c[2])], ee[:int(c[3])]
 
     # --- edge colliders -------------------------------------------------
     def set_edge_collision(self, enable=True, margin_scale=1.0, margin_offset=0.0):

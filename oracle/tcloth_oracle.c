@@ -190,7 +190,20 @@ struct OSim {
     int32_t *acc;  /* n * A_N */
     v3 *nrm;
     uint32_t *cs, *srt, *ecs, *esrt;
+    /* contact-pair cache (self-collision algorithm 1), off by default
+     * (simulation/mod.rs:582-600) */
+    int pair_cache, pair_fallback, pair_margin_mode;
+    uint32_t pair_qvt, pair_qee, pair_max_vt, pair_max_ee;
+    float pair_safety, pair_hscale, pair_maxh;
+    uint32_t *pvt, *pee; /* n * 8 slots of four vertex ids */
+    uint32_t pcnt[4];
 };
+/* quota_for_budget, simulation/mod.rs:36-41 (PAIR_QUOTA_MAX = 8) */
+static uint32_t quota_for_budget(uint32_t budget, uint32_t nv) {
+    if (nv == 0) return 1u;
+    uint32_t q = budget / nv;
+    return q < 1u ? 1u : (q > 8u ? 8u : q);
+}
 
 /* ------------------------------------------------------------------ */
 /* Welsh-Powell colouring, crates/cloth_core/src/coloring.rs:6-173       */
@@ -1016,6 +1029,18 @@ OSim *ocl_create_sewn(const float *pos, int n, const uint32_t *edges, int ne_in,
     s->srt = (uint32_t *)calloc(N, 4);
     s->ecs = (uint32_t *)calloc((size_t)s->table + 1, 4);
     s->esrt = (uint32_t *)calloc((size_t)s->ne + 1, 4);
+    s->pair_fallback = 1; s->pair_margin_mode = 1;
+    s->pair_safety = 0.005f; s->pair_hscale = 1.3f; s->pair_maxh = 0.02f;
+    {
+        uint32_t b = (uint32_t)n * 8u;
+        b = b < 8192u ? 8192u : (b > 262144u ? 262144u : b);
+        s->pair_max_vt = s->pair_max_ee = b;
+        s->pair_qvt = s->pair_qee = quota_for_budget(b, (uint32_t)n);
+    }
+    s->pvt = (uint32_t *)malloc(N * 8 * 16);
+    s->pee = (uint32_t *)malloc(N * 8 * 16);
+    memset(s->pvt, 0xFF, N * 8 * 16);
+    memset(s->pee, 0xFF, N * 8 * 16);
     for (int i = 0; i < n; i++) { free(adj[i].d); free(oadj[i].d); free(chop[i].d); }
     free(oadj); free(chop); free(has_sew);
     free(adj); free(lsum); free(lcnt); free(isface); free(eo); free(dl); free(vf);
@@ -1031,7 +1056,7 @@ void ocl_destroy(OSim *s) {
                     s->star_off, s->star_idx, s->edges, s->ebits, s->island, s->cols, s->tris,
                     s->bounds, s->pins, s->acc, s->nrm, s->cs, s->srt, s->ecs, s->esrt,
                     s->atlas, s->binfo, s->bxf, s->sew, s->sc_off, s->sc_cnt, s->slam, s->rep,
-                    s->ce, s->ce_cs, s->ce_srt};
+                    s->ce, s->ce_cs, s->ce_srt, s->pvt, s->pee};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(s);
 }
@@ -2928,10 +2953,549 @@ static void k_apply(OSim *s) {
     }
 }
 
-/* dispatch_self_collision_passes, simulation/dispatch.rs:1460-1717
- * (DIRECT algorithm, pair cache off) */
-static void self_collision(OSim *s, int run_ee) {
+/* ------------------------------------------------------------------ */
+/* Contact-pair cache (self-collision algorithm 1, "Active Pair        */
+/* Caching"): broad phase once per frame into per-vertex top-K slots,  */
+/* narrow phase per substep over the slots.                             */
+/* ------------------------------------------------------------------ */
+/* |cell_a - cell_b| > 1 on one axis, 32-bit wrap and abs(INT_MIN) = INT_MIN */
+static int pc_far_axis(int32_t a, int32_t b) {
+    uint32_t d = (uint32_t)a - (uint32_t)b;
+    uint32_t ad = ((int32_t)d < 0) ? 0u - d : d;
+    return (int32_t)ad > 1;
+}
+/* velocity horizon, collect_pairs.wgsl:328-330 */
+static float pc_horizon(const OSim *s, float dt, uint32_t i) {
+    return fminf(vlen(s->v[i]) * dt * s->pair_hscale, s->pair_maxh);
+}
+/* can_ee_anchor_reach, shaders/self_collision_collect_pairs.wgsl:262-283 */
+static int pc_anchor_reach(const OSim *s, float dt, uint32_t u, uint32_t w) {
+    if (s->w[u] <= 0.0f) return 0;
+    int32_t cu[3], cw[3];
+    cell_of(s->p[u], s->cell, cu);
+    cell_of(s->p[w], s->cell, cw);
+    if (pc_far_axis(cu[0], cw[0]) || pc_far_axis(cu[1], cw[1]) || pc_far_axis(cu[2], cw[2])) return 0;
+    v3 d = vsub(s->p[u], s->p[w]);
+    float d2 = vdot(d, d);
+    float mf = (float)s->pair_margin_mode;
+    float hu = pc_horizon(s, dt, u) * mf, hw = pc_horizon(s, dt, w) * mf;
+    float b = s->thick[u] + s->thick[w] + (s->local_len[u] + s->local_len[w]) * 1.3f + s->pair_safety + hu + hw;
+    if (d2 > b * b) return 0;
+    if ((s->island[u] == s->island[w]) && s->exclude_neighbors) {
+        float dist = sqrtf(fmaxf(d2, 0.0f));
+        if (near_folded(s, u, w, dist)) return 0;
+    }
+    return 1;
+}
+/* is_smaller_anchor_reachable, :286-292 */
+static int pc_smaller_anchor(const OSim *s, float dt, uint32_t u, uint32_t w, uint32_t cu, uint32_t cw) {
+    if (u > cu || (u == cu && w >= cw)) return 0;
+    return pc_anchor_reach(s, dt, u, w);
+}
+typedef struct { uint32_t n, eval, drop; float d[8]; uint32_t k[8][3]; } OTopK;
+/* top-K insertion with duplicate rejection, :428-475 and :558-604 */
+static void topk_insert(OTopK *t, uint32_t quota, float d, uint32_t k0, uint32_t k1, uint32_t k2) {
+    for (uint32_t q = 0; q < 8u; q++) {
+        if (q >= t->n) break;
+        if (t->k[q][0] == k0 && t->k[q][1] == k1 && t->k[q][2] == k2) return;
+    }
+    t->eval++;
+    uint32_t pos = t->n;
+    for (uint32_t q = 0; q < 8u; q++) {
+        if (q < t->n) {
+            const uint32_t *e = t->k[q];
+            int tie = (d == t->d[q]) && (k0 < e[0] || (k0 == e[0] && (k1 < e[1] || (k1 == e[1] && k2 < e[2]))));
+            if (d < t->d[q] || tie) { pos = q; break; }
+        }
+    }
+    if (pos < quota) {
+        uint32_t up = t->n < quota - 1u ? t->n : quota - 1u;
+        for (uint32_t q = up; q > pos; q--) {
+            t->d[q] = t->d[q - 1];
+            t->k[q][0] = t->k[q - 1][0]; t->k[q][1] = t->k[q - 1][1]; t->k[q][2] = t->k[q - 1][2];
+        }
+        t->d[pos] = d;
+        t->k[pos][0] = k0; t->k[pos][1] = k1; t->k[pos][2] = k2;
+        if (t->n < quota) t->n++;
+    } else {
+        t->drop++;
+    }
+}
+/* pair_collect, shaders/self_collision_collect_pairs.wgsl:293-661 */
+static void k_pair_collect(OSim *s, float dt) {
+    const float cs = s->cell;
+    const uint32_t n = (uint32_t)s->n;
+    const uint32_t qvt = s->pair_qvt < 1u ? 1u : (s->pair_qvt > 8u ? 8u : s->pair_qvt);
+    const uint32_t qee = s->pair_qee < 1u ? 1u : (s->pair_qee > 8u ? 8u : s->pair_qee);
+    uint64_t c_vt = 0, c_ee = 0, c_vtd = 0, c_eed = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : c_vt, c_ee, c_vtd, c_eed)
+    for (uint32_t index = 0; index < n; index++) {
+        int pin_i = s->w[index] <= 0.0f;
+        v3 p_i = s->p[index];
+        float ll_i = s->local_len[index];
+        int32_t base[3];
+        cell_of(p_i, cs, base);
+        OTopK vt, ee;
+        memset(&vt, 0, sizeof vt);
+        memset(&ee, 0, sizeof ee);
+        float margin = s->pair_safety;
+        float h_i = pc_horizon(s, dt, index);
+        for (int gx = -1; gx <= 1; gx++)
+            for (int gy = -1; gy <= 1; gy++)
+                for (int gz = -1; gz <= 1; gz++) {
+                    int32_t cx = base[0] + gx, cy = base[1] + gy, cz = base[2] + gz;
+                    uint32_t h = hash3(cx, cy, cz, s->table);
+                    uint32_t st = s->cs[h], en = s->cs[h + 1];
+                    if (st >= en) continue;
+                    for (uint32_t k = st; k < en; k++) {
+                        uint32_t j = s->srt[k];
+                        if (j >= n || j == index) continue;
+                        v3 p_j = s->p[j];
+                        int32_t jc[3];
+                        cell_of(p_j, cs, jc);
+                        if (!cell_eq(jc, cx, cy, cz)) continue;
+                        int pin_j = s->w[j] <= 0.0f;
+                        if (!(pin_i && pin_j)) {
+                            float mf = (float)s->pair_margin_mode;
+                            float h_j = pc_horizon(s, dt, j) * mf;
+                            float h_ie = h_i * mf;
+                            v3 dvv = vsub(p_i, p_j);
+                            float d2vv = vdot(dvv, dvv);
+                            float eth = s->thick[index] + s->thick[j];
+                            float ll_j = s->local_len[j];
+                            float broad = eth + (ll_i + ll_j) * 1.3f + margin + h_ie + h_j;
+                            if (d2vv <= broad * broad) {
+                                int same_island = s->island[index] == s->island[j];
+                                float dvvl = sqrtf(fmaxf(d2vv, 0.0f));
+                                int near_topo = same_island && s->exclude_neighbors && near_folded(s, index, j, dvvl);
+                                if (!near_topo) {
+                                    /* 1. vertex-triangle */
+                                    float vtb = eth + ll_j * 1.3f + margin + h_ie + h_j;
+                                    int near2 = s->exclude_neighbors && within2(s, index, j);
+                                    if (d2vv <= vtb * vtb && !near2) {
+                                        uint32_t ss = s->star_off[j], se = s->star_off[j + 1];
+                                        if (ss < se) {
+                                            uint32_t ns = se - ss < 8u ? se - ss : 8u;
+                                            for (uint32_t t = 0; t < ns; t++) {
+                                                uint32_t v0 = s->star_idx[2 * (ss + t)], v1 = s->star_idx[2 * (ss + t) + 1];
+                                                if (index != v0 && index != v1 && v0 < n && v1 < n) {
+                                                    uint32_t c0 = j, c1 = v0, c2 = v1;
+                                                    if (v0 < j && v0 < v1) { c0 = v0; c1 = v1; c2 = j; }
+                                                    else if (v1 < j && v1 < v0) { c0 = v1; c1 = j; c2 = v0; }
+                                                    int isf; v3 bary;
+                                                    v3 cp = closest_tri(p_i, s->p[c0], s->p[c1], s->p[c2], &isf, &bary);
+                                                    v3 dvt = vsub(p_i, cp);
+                                                    float d2vt = vdot(dvt, dvt);
+                                                    float chk = eth + margin + h_ie + h_j;
+                                                    if (d2vt < chk * chk) {
+                                                        if (s->exclude_neighbors) {
+                                                            if (within2(s, index, v0) || within2(s, index, v1)) continue;
+                                                        }
+                                                        topk_insert(&vt, qvt, d2vt, c0, c1, c2);
+                                                    }
+                                                }
+                                            }
+                                        }
+                                    }
+                                    /* 2. edge-edge */
+                                    float eeb = eth + (ll_i + ll_j) * 1.3f + margin + h_ie + h_j;
+                                    if (d2vv <= eeb * eeb) {
+                                        uint32_t ai0 = s->adj_off[index], ai1 = s->adj_off[index + 1];
+                                        uint32_t aj0 = s->adj_off[j], aj1 = s->adj_off[j + 1];
+                                        if (ai0 < ai1 && aj0 < aj1) {
+                                            uint32_t nei = ai1 - ai0 < 8u ? ai1 - ai0 : 8u;
+                                            uint32_t nej = aj1 - aj0 < 8u ? aj1 - aj0 : 8u;
+                                            for (uint32_t e1 = 0; e1 < nei; e1++) {
+                                                uint32_t ui = s->adj_idx[ai0 + e1];
+                                                if (ui >= n) continue;
+                                                v3 p_ui = s->p[ui];
+                                                float ll_ui = s->local_len[ui];
+                                                v3 li = vsub(p_ui, p_i);
+                                                float lsi = vdot(li, li);
+                                                float mli = (ll_i + ll_ui) * 1.5f;
+                                                if (lsi > mli * mli || lsi <= 1e-12f) continue;
+                                                for (uint32_t e2 = 0; e2 < nej; e2++) {
+                                                    uint32_t vj = s->adj_idx[aj0 + e2];
+                                                    if (vj >= n) continue;
+                                                    if (ui != j && ui != vj && index != vj) {
+                                                        uint32_t cj = j < vj ? j : vj, cvj = j < vj ? vj : j;
+                                                        int smaller = pc_smaller_anchor(s, dt, index, vj, index, j) ||
+                                                                      pc_smaller_anchor(s, dt, ui, j, index, j) ||
+                                                                      pc_smaller_anchor(s, dt, ui, vj, index, j) ||
+                                                                      pc_smaller_anchor(s, dt, j, index, index, j) ||
+                                                                      pc_smaller_anchor(s, dt, j, ui, index, j) ||
+                                                                      pc_smaller_anchor(s, dt, vj, index, index, j) ||
+                                                                      pc_smaller_anchor(s, dt, vj, ui, index, j);
+                                                        if (!pin_i && !smaller) {
+                                                            v3 p_vj = s->p[vj];
+                                                            float ll_vj = s->local_len[vj];
+                                                            v3 lj = vsub(p_vj, p_j);
+                                                            float lsj = vdot(lj, lj);
+                                                            float mlj = (ll_j + ll_vj) * 1.5f;
+                                                            if (lsj > mlj * mlj || lsj <= 1e-12f) continue;
+                                                            v3 pcj = j < vj ? p_j : p_vj, pcvj = j < vj ? p_vj : p_j;
+                                                            float sp, tp;
+                                                            seg_seg(p_i, p_ui, pcj, pcvj, &sp, &tp);
+                                                            v3 pt1 = vadd(p_i, vmul(vsub(p_ui, p_i), sp));
+                                                            v3 pt2 = vadd(pcj, vmul(vsub(pcvj, pcj), tp));
+                                                            v3 dee = vsub(pt1, pt2);
+                                                            float d2ee = vdot(dee, dee);
+                                                            float chk = eth + margin + h_ie + h_j;
+                                                            if (d2ee < chk * chk && d2ee > EPS * EPS) {
+                                                                if (s->exclude_neighbors) {
+                                                                    if (near_folded(s, index, vj, vlen(vsub(p_i, p_vj))) ||
+                                                                        near_folded(s, ui, j, vlen(vsub(p_ui, p_j))) ||
+                                                                        near_folded(s, ui, vj, vlen(vsub(p_ui, p_vj))))
+                                                                        continue;
+                                                                }
+                                                                topk_insert(&ee, qee, d2ee, ui, cj, cvj);
+                                                            }
+                                                        }
+                                                    }
+                                                }
+                                            }
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+        uint32_t *bv = s->pvt + (size_t)index * qvt * 4;
+        for (uint32_t q = 0; q < qvt; q++) {
+            if (q < vt.n) { bv[4 * q] = index; bv[4 * q + 1] = vt.k[q][0]; bv[4 * q + 2] = vt.k[q][1]; bv[4 * q + 3] = vt.k[q][2]; }
+            else { bv[4 * q] = 0xFFFFFFFFu; bv[4 * q + 1] = bv[4 * q + 2] = bv[4 * q + 3] = 0u; }
+        }
+        uint32_t *be = s->pee + (size_t)index * qee * 4;
+        for (uint32_t q = 0; q < qee; q++) {
+            if (q < ee.n) { be[4 * q] = index; be[4 * q + 1] = ee.k[q][0]; be[4 * q + 2] = ee.k[q][1]; be[4 * q + 3] = ee.k[q][2]; }
+            else { be[4 * q] = 0xFFFFFFFFu; be[4 * q + 1] = be[4 * q + 2] = be[4 * q + 3] = 0u; }
+        }
+        c_vt += vt.eval; c_vtd += vt.drop; c_ee += ee.eval; c_eed += ee.drop;
+    }
+    s->pcnt[0] += (uint32_t)c_vt; s->pcnt[1] += (uint32_t)c_ee;
+    s->pcnt[2] += (uint32_t)c_vtd; s->pcnt[3] += (uint32_t)c_eed;
+}
+static inline void acc_umax(int32_t *a, uint32_t v) {
+    uint32_t *u = (uint32_t *)a;
+    uint32_t cur = __atomic_load_n(u, __ATOMIC_RELAXED);
+    while (v > cur && !__atomic_compare_exchange_n(u, &cur, v, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {}
+}
+/* record_untangle_cand, shaders/self_collision_solve_vt.wgsl:99-108 */
+static void pc_untangle_cand(OSim *s, uint32_t vi, uint32_t j, float dist, float cap) {
+    if (vi >= (uint32_t)s->n || j >= 0x3FFFFEu || dist >= cap) return;
+    float ratio = clampf(dist / fmaxf(cap, EPS), 0.0f, 1.0f);
+    uint32_t rank = 1023u - (uint32_t)(ratio * 1023.0f);
+    uint32_t packed = (rank << 22) | ((j + 1u) & 0x3FFFFFu);
+    acc_umax(&s->acc[(size_t)vi * A_N + A_UT], packed);
+}
+/* pair_vt, shaders/self_collision_solve_vt.wgsl:227-414 */
+static void k_pair_vt(OSim *s, int untangle) {
+    const uint32_t n = (uint32_t)s->n;
+    const uint32_t slots = n * s->pair_qvt;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (uint32_t slot = 0; slot < slots; slot++) {
+        const uint32_t *pr = s->pvt + 4 * (size_t)slot;
+        if (pr[0] == 0xFFFFFFFFu) continue;
+        uint32_t index = pr[0], j = pr[1], v0 = pr[2], v1 = pr[3];
+        if (index >= n || j >= n || v0 >= n || v1 >= n) continue;
+        if (index == j || index == v0 || index == v1 || v0 == v1 || j == v0 || j == v1) continue;
+        int pin_i = s->w[index] <= 0.0f;
+        v3 p_i = s->p[index], xo = s->x[index];
+        v3 p_j = s->p[j], p_v0 = s->p[v0], p_v1 = s->p[v1];
+        v3 p_jo = s->x[j], p_v0o = s->x[v0], p_v1o = s->x[v1];
+        float w_i = s->w[index], w_j = s->w[j], w_v0 = s->w[v0], w_v1 = s->w[v1];
+        float eth = s->thick[index] + s->thick[j];
+        v3 tmove = vdiv(vadd(vadd(vsub(p_j, p_jo), vsub(p_v0, p_v0o)), vsub(p_v1, p_v1o)), 3.0f);
+        int tpin = (w_j <= 0.0f) || (w_v0 <= 0.0f) || (w_v1 <= 0.0f);
+        int upair = untangle && !pin_i && (s->layer[index] > s->layer[j]);
+        v3 niraw = upair ? s->nrm[index] : V3(0, 0, 0);
+        float nil = vlen(niraw);
+        v3 niu = nil > 0.5f ? vdiv(niraw, fmaxf(nil, EPS)) : V3(0, 0, 0);
+        v3 rel = vadd(xo, tmove);
+        float ht = 0.0f, hu = 0.0f, hv = 0.0f;
+        if (seg_tri(rel, p_i, p_j, p_v0, p_v1, &ht, &hu, &hv)) {
+            v3 mv = vsub(p_i, rel);
+            v3 hp = vadd(rel, vmul(mv, ht));
+            v3 tc = vcross(vsub(p_v0, p_j), vsub(p_v1, p_j));
+            float tl = vlen(tc);
+            v3 tn = tl > 1e-12f ? vdiv(tc, tl) : V3(0, 1, 0);
+            float hor = vdot(vsub(rel, p_j), tn);
+            int utc = 0;
+            if (upair && tl > 1e-12f) {
+                int allow = tpin || (nil <= 0.5f) || (vdot(niu, tn) > 0.0f);
+                int ret = (hor < 0.0f) && (vdot(mv, tn) > 0.0f);
+                utc = allow && ret;
+            }
+            if (!utc) {
+                float sgn = fabsf(hor) > 1e-6f ? hor : vdot(vneg(mv), tn);
+                v3 ns = sgn >= 0.0f ? tn : vneg(tn);
+                float ho = fmaxf(vdot(vsub(rel, hp), ns), 0.0f);
+                float hs = fmaxf(ho, eth * 0.25f);
+                v3 psafe = vadd(hp, vmul(ns, hs));
+                v3 tccd = vsub(psafe, p_i);
+                float pcs = fmaxf(0.0f, eth - hs);
+                if (tpin) {
+                    if (!pin_i) add_ccd(s, index, vadd(tccd, vmul(ns, pcs)), 0);
+                } else if (pin_i) {
+                    v3 bc = V3(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
+                    float wt = bc.x * bc.x * w_j + bc.y * bc.y * w_v0 + bc.z * bc.z * w_v1;
+                    if (wt > EPS) {
+                        v3 full = vadd(tccd, vmul(ns, pcs));
+                        if (w_j > 0.0f) add_ccd(s, j, vmul(vneg(full), bc.x * w_j / wt), 0);
+                        if (w_v0 > 0.0f) add_ccd(s, v0, vmul(vneg(full), bc.y * w_v0 / wt), 0);
+                        if (w_v1 > 0.0f) add_ccd(s, v1, vmul(vneg(full), bc.z * w_v1 / wt), 0);
+                    }
+                } else {
+                    v3 bc = V3(clampf(1.0f - hu - hv, 0.0f, 1.0f), clampf(hu, 0.0f, 1.0f), clampf(hv, 0.0f, 1.0f));
+                    float wt = bc.x * bc.x * w_j + bc.y * bc.y * w_v0 + bc.z * bc.z * w_v1;
+                    float wtot = w_i + wt;
+                    if (wtot > EPS) {
+                        add_ccd(s, index, vmul(tccd, w_i / wtot), 0);
+                        if (w_j > 0.0f) add_ccd(s, j, vmul(vneg(tccd), bc.x * w_j / wtot), 0);
+                        if (w_v0 > 0.0f) add_ccd(s, v0, vmul(vneg(tccd), bc.y * w_v0 / wtot), 0);
+                        if (w_v1 > 0.0f) add_ccd(s, v1, vmul(vneg(tccd), bc.z * w_v1 / wtot), 0);
+                        if (pcs > EPS) {
+                            v3 tp = vmul(ns, pcs * 0.6f);
+                            add_disp(s, index, vmul(tp, w_i / wtot));
+                            if (w_j > 0.0f) add_disp(s, j, vmul(vneg(tp), bc.x * w_j / wtot));
+                            if (w_v0 > 0.0f) add_disp(s, v0, vmul(vneg(tp), bc.y * w_v0 / wtot));
+                            if (w_v1 > 0.0f) add_disp(s, v1, vmul(vneg(tp), bc.z * w_v1 / wtot));
+                        }
+                    }
+                }
+            } else {
+                pc_untangle_cand(s, index, j, vlen(vsub(p_i, hp)), eth * 2.5f);
+            }
+        } else {
+            int isf; v3 bary;
+            v3 cp = closest_tri(p_i, p_j, p_v0, p_v1, &isf, &bary);
+            v3 dvt = vsub(p_i, cp);
+            float dist = vlen(dvt);
+            v3 tc = vcross(vsub(p_v0, p_j), vsub(p_v1, p_j));
+            float tl = vlen(tc);
+            v3 tn = tl > EPS ? vdiv(tc, fmaxf(tl, EPS)) : V3(0, 0, 0);
+            float hvt = tl > EPS ? vdot(dvt, tn) : 0.0f;
+            int allow = tpin || (nil <= 0.5f) || (vdot(niu, tn) > 0.0f);
+            int utv = upair && (tl > EPS) && allow && (hvt < 0.0f);
+            if (utv) pc_untangle_cand(s, index, j, dist, eth * 2.5f);
+            if (!pin_i && !utv && dist < eth && dist > EPS) {
+                v3 nvt = vdiv(dvt, dist);
+                float pen = eth - dist;
+                if (tpin) {
+                    add_pin(s, index, vadd(vmul(nvt, pen), vmul(tmove, 0.5f)));
+                } else {
+                    float wt = bary.x * bary.x * w_j + bary.y * bary.y * w_v0 + bary.z * bary.z * w_v1;
+                    float wtot = w_i + wt;
+                    if (wtot > EPS) {
+                        v3 tp = vmul(nvt, pen * 0.6f);
+                        add_disp(s, index, vmul(tp, w_i / wtot));
+                        if (w_j > 0.0f) add_disp(s, j, vmul(vneg(tp), bary.x * w_j / wtot));
+                        if (w_v0 > 0.0f) add_disp(s, v0, vmul(vneg(tp), bary.y * w_v0 / wtot));
+                        if (w_v1 > 0.0f) add_disp(s, v1, vmul(vneg(tp), bary.z * w_v1 / wtot));
+                    }
+                }
+            }
+        }
+    }
+}
+/* pair_ee, shaders/self_collision_solve_ee.wgsl:230-589 */
+static void k_pair_ee(OSim *s, int untangle) {
+    const uint32_t n = (uint32_t)s->n;
+    const uint32_t slots = n * s->pair_qee;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (uint32_t slot = 0; slot < slots; slot++) {
+        const uint32_t *pr = s->pee + 4 * (size_t)slot;
+        if (pr[0] == 0xFFFFFFFFu) continue;
+        uint32_t u0 = pr[0], u1 = pr[1], j = pr[2], vj = pr[3];
+        if (u0 >= n || u1 >= n || j >= n || vj >= n) continue;
+        if (u0 == u1 || j == vj || u0 == j || u0 == vj || u1 == j || u1 == vj) continue;
+        float w_u0 = s->w[u0], w_u1 = s->w[u1], w_j = s->w[j], w_vj = s->w[vj];
+        int apin = (w_u0 <= 0.0f) || (w_u1 <= 0.0f);
+        int bpin = (w_j <= 0.0f) || (w_vj <= 0.0f);
+        if (apin && bpin) continue;
+        v3 p_u0 = s->p[u0], p_u1 = s->p[u1], p_j = s->p[j], p_vj = s->p[vj];
+        v3 p_u0o = s->x[u0], p_u1o = s->x[u1], p_jo = s->x[j], p_vjo = s->x[vj];
+        float thu0 = s->thick[u0], thu1 = s->thick[u1], thj = s->thick[j], thvj = s->thick[vj];
+        float s1, t1;
+        seg_seg(p_u0, p_u1, p_j, p_vj, &s1, &t1);
+        v3 d1c = vsub(vmix(p_u0, p_u1, s1), vmix(p_j, p_vj, t1));
+        float d2c = vdot(d1c, d1c);
+        float eth = mixf(thu0, thu1, s1) + mixf(thj, thvj, t1);
+        float meth = fmaxf(thu0, thu1) + fmaxf(thj, thvj);
+        v3 dv0 = vsub(p_u0, p_u0o), dv1 = vsub(p_u1, p_u1o), dvj = vsub(p_j, p_jo), dvvj = vsub(p_vj, p_vjo);
+        v3 va = vmul(vadd(dv0, dv1), 0.5f), vb = vmul(vadd(dvj, dvvj), 0.5f);
+        float rd = vlen(vsub(va, vb)) + 0.5f * (vlen(vsub(dv1, dv0)) + vlen(vsub(dvvj, dvj)));
+        float reach = meth + rd;
+        if (d2c > reach * reach) continue;
+        v3 d0g = vsub(vmix(p_u0o, p_u1o, s1), vmix(p_jo, p_vjo, t1));
+        int run_ccd = (rd > eth * 0.5f) || (vdot(d0g, d1c) <= 0.0f);
+        uint32_t la = s->layer[u0], lb = s->layer[j];
+        if (run_ccd) {
+            float msd = 1e20f, btau = 0.0f, hs = 0.125f, ms = 0, mt = 0;
+            float pv = seg_vol(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, 0.0f);
+            float zc = -1.0f;
+            for (uint32_t k = 0; k <= 8u; k++) {
+                float tk = (float)k * 0.125f;
+                float es, et;
+                float ed = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, tk, &es, &et);
+                if (ed < msd) { msd = ed; btau = tk; ms = es; mt = et; }
+                if (k > 0u) {
+                    float vol = seg_vol(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, tk);
+                    if (pv * vol <= 0.0f && zc < 0.0f) zc = tk - 0.0625f;
+                    pv = vol;
+                }
+            }
+            if (zc >= 0.0f) {
+                float es, et;
+                float ed = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, zc, &es, &et);
+                if (ed < msd) { msd = ed; btau = zc; hs = 0.0625f; ms = es; mt = et; }
+            }
+            float tlo = fmaxf(0.0f, btau - hs), thi = fminf(1.0f, btau + hs);
+            float dstar = msd, ss = ms, ts = mt;
+            for (int it = 0; it < 6; it++) {
+                float m1 = tlo + (thi - tlo) * (1.0f / 3.0f);
+                float mm2 = thi - (thi - tlo) * (1.0f / 3.0f);
+                float e1s, e1t, e2s, e2t;
+                float e1 = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, m1, &e1s, &e1t);
+                float e2 = seg_eval(p_u0o, p_u0, p_u1o, p_u1, p_jo, p_j, p_vjo, p_vj, mm2, &e2s, &e2t);
+                if (e1 < dstar) { dstar = e1; ss = e1s; ts = e1t; }
+                if (e2 < dstar) { dstar = e2; ss = e2s; ts = e2t; }
+                if (e1 < e2) thi = mm2; else tlo = m1;
+            }
+            float ets = mixf(thu0, thu1, ss) + mixf(thj, thvj, ts);
+            if (dstar >= ets * ets) continue;
+            int utc = 0;
+            if (untangle && la != lb) {
+                int afx = (w_u0 == 0.0f) && (w_u1 == 0.0f);
+                int bfx = (w_j == 0.0f) && (w_vj == 0.0f);
+                v3 d0u = vmul(vsub(vadd(p_u0o, p_u1o), vadd(p_jo, p_vjo)), 0.5f);
+                v3 d1u = vmul(vsub(vadd(p_u0, p_u1), vadd(p_j, p_vj)), 0.5f);
+                v3 mu = vsub(d1u, d0u);
+                if (la > lb && !afx) {
+                    v3 ni = s->nrm[j], no = s->nrm[u0];
+                    int allow = bfx || (vdot(no, no) <= 0.25f);
+                    utc = allow && (vdot(ni, ni) > 0.25f) && (vdot(d0u, ni) < 0.0f) && (vdot(mu, ni) > 0.0f);
+                } else if (lb > la && !bfx) {
+                    v3 ni = s->nrm[u0], no = s->nrm[j];
+                    int allow = afx || (vdot(no, no) <= 0.25f);
+                    utc = allow && (vdot(ni, ni) > 0.25f) && (vdot(vneg(d0u), ni) < 0.0f) && (vdot(vneg(mu), ni) > 0.0f);
+                }
+            }
+            if (utc) continue;
+            float s0, t0p;
+            seg_seg(p_u0o, p_u1o, p_jo, p_vjo, &s0, &t0p);
+            v3 d0 = vsub(vmix(p_u0o, p_u1o, s0), vmix(p_jo, p_vjo, t0p));
+            float dist0 = vlen(d0);
+            if (dist0 > EPS) {
+                v3 n0 = vdiv(d0, dist0);
+                v3 de = vsub(vmix(p_u0, p_u1, ss), vmix(p_j, p_vj, ts));
+                float he = vdot(de, n0);
+                int crossed = (he <= 0.0f) || (vdot(d1c, n0) <= 0.0f);
+                if (he < ets && crossed) {
+                    float pc = ets - he;
+                    int aall = (w_u0 == 0.0f) && (w_u1 == 0.0f);
+                    int ball = (w_j == 0.0f) && (w_vj == 0.0f);
+                    int cpe = !(aall || ball);
+                    if (bpin) {
+                        v3 em = vmul(vadd(vsub(p_j, p_jo), vsub(p_vj, p_vjo)), 0.5f);
+                        float a = 1.0f - ss, b = ss;
+                        float den = a * a * w_u0 + b * b * w_u1;
+                        if (den > EPS) {
+                            v3 pb = vadd(vmul(n0, pc), vmul(em, 0.5f));
+                            if (w_u0 > 0.0f) add_ccd(s, u0, vmul(pb, fminf((a * w_u0) / den, 2.0f)), cpe);
+                            if (w_u1 > 0.0f) add_ccd(s, u1, vmul(pb, fminf((b * w_u1) / den, 2.0f)), cpe);
+                        }
+                    } else if (apin) {
+                        v3 em = vmul(vadd(vsub(p_u0, p_u0o), vsub(p_u1, p_u1o)), 0.5f);
+                        float a = 1.0f - ts, b = ts;
+                        float den = a * a * w_j + b * b * w_vj;
+                        if (den > EPS) {
+                            v3 pb = vadd(vmul(vneg(n0), pc), vmul(em, 0.5f));
+                            if (w_j > 0.0f) add_ccd(s, j, vmul(pb, fminf((a * w_j) / den, 2.0f)), cpe);
+                            if (w_vj > 0.0f) add_ccd(s, vj, vmul(pb, fminf((b * w_vj) / den, 2.0f)), cpe);
+                        }
+                    } else {
+                        float we1 = (1.0f - ss) * (1.0f - ss) * w_u0 + ss * ss * w_u1;
+                        float we2 = (1.0f - ts) * (1.0f - ts) * w_j + ts * ts * w_vj;
+                        float wtot = we1 + we2;
+                        if (wtot > EPS) {
+                            v3 tcc = vmul(n0, pc);
+                            if (w_u0 > 0.0f) add_ccd(s, u0, vmul(tcc, (1.0f - ss) * w_u0 / wtot), 1);
+                            if (w_u1 > 0.0f) add_ccd(s, u1, vmul(tcc, ss * w_u1 / wtot), 1);
+                            if (w_j > 0.0f) add_ccd(s, j, vmul(vneg(tcc), (1.0f - ts) * w_j / wtot), 1);
+                            if (w_vj > 0.0f) add_ccd(s, vj, vmul(vneg(tcc), ts * w_vj / wtot), 1);
+                        }
+                    }
+                    continue;
+                }
+            }
+        }
+        /* discrete segment repulsion */
+        if (d2c >= eth * eth || d2c <= EPS * EPS) continue;
+        float del = sqrtf(d2c);
+        int ute = 0;
+        if (untangle) {
+            int afx = (w_u0 <= 0.0f) && (w_u1 <= 0.0f);
+            int bfx = (w_j <= 0.0f) && (w_vj <= 0.0f);
+            ute = outer_behind(s, la, lb, u0, u1, j, vj, afx, bfx, d1c);
+        }
+        if (ute) continue;
+        v3 ne = vdiv(d1c, del);
+        float pen = eth - del;
+        if (bpin) {
+            v3 em = vmul(vadd(vsub(p_j, p_jo), vsub(p_vj, p_vjo)), 0.5f);
+            float a = 1.0f - s1, b = s1;
+            float den = a * a * w_u0 + b * b * w_u1;
+            if (den > EPS) {
+                v3 pb = vadd(vmul(ne, pen), vmul(em, 0.5f));
+                if (w_u0 > 0.0f) add_pin(s, u0, vmul(pb, fminf((a * w_u0) / den, 2.0f)));
+                if (w_u1 > 0.0f) add_pin(s, u1, vmul(pb, fminf((b * w_u1) / den, 2.0f)));
+            }
+        } else if (apin) {
+            v3 em = vmul(vadd(vsub(p_u0, p_u0o), vsub(p_u1, p_u1o)), 0.5f);
+            float a = 1.0f - t1, b = t1;
+            float den = a * a * w_j + b * b * w_vj;
+            if (den > EPS) {
+                v3 pb = vadd(vmul(vneg(ne), pen), vmul(em, 0.5f));
+                if (w_j > 0.0f) add_pin(s, j, vmul(pb, fminf((a * w_j) / den, 2.0f)));
+                if (w_vj > 0.0f) add_pin(s, vj, vmul(pb, fminf((b * w_vj) / den, 2.0f)));
+            }
+        } else {
+            float we1 = (1.0f - s1) * (1.0f - s1) * w_u0 + s1 * s1 * w_u1;
+            float we2 = (1.0f - t1) * (1.0f - t1) * w_j + t1 * t1 * w_vj;
+            float wtot = we1 + we2;
+            if (wtot > EPS) {
+                v3 td = vmul(ne, pen * 0.6f);
+                if (w_u0 > 0.0f) add_disp(s, u0, vmul(td, (1.0f - s1) * w_u0 / wtot));
+                if (w_u1 > 0.0f) add_disp(s, u1, vmul(td, s1 * w_u1 / wtot));
+                if (w_j > 0.0f) add_disp(s, j, vmul(vneg(td), (1.0f - t1) * w_j / wtot));
+                if (w_vj > 0.0f) add_disp(s, vj, vmul(vneg(td), t1 * w_vj / wtot));
+            }
+        }
+    }
+}
+
+/* dispatch_self_collision_passes, simulation/dispatch.rs:1460-1717: the
+ * direct pass, or with the pair cache on the cached pass (:1556-1645) with
+ * the hash and broad phase at the first substep only; the final fallback
+ * runs the direct pass on the last substep. */
+static void self_collision(OSim *s, int run_ee, int sub, int substeps, float dt) {
     int untangle = s->untangle_opt && s->multi_layer;
+    int force_direct = s->pair_cache && s->pair_fallback && sub + 1 == substeps;
+    if (s->pair_cache && !force_direct) {
+        if (untangle) k_normals(s);
+        if (sub == 0) {
+            build_hash(s, 0);
+            memset(s->pcnt, 0, sizeof s->pcnt);
+            k_pair_collect(s, dt);
+        }
+        k_pair_vt(s, untangle);
+        if (run_ee) k_pair_ee(s, untangle);
+        if (untangle) k_untangle(s);
+        k_apply(s);
+        return;
+    }
     if (untangle) k_normals(s);
     build_hash(s, 0);
     if (run_ee && s->ne > 0) build_hash(s, 1);
@@ -2939,6 +3503,46 @@ static void self_collision(OSim *s, int run_ee) {
     if (untangle) k_untangle(s);
     if (run_ee && s->ne > 0) k_ee(s, untangle);
     k_apply(s);
+}
+/* set_enable_pair_cache / set_enable_pair_cache_final_fallback
+ * (simulation/mod.rs:805-810, :852-854) */
+void ocl_set_pair_cache(OSim *s, int enable, int final_fallback) {
+    s->pair_cache = enable != 0;
+    s->pair_fallback = final_fallback != 0;
+}
+/* set_pair_cache_options, simulation/mod.rs:826-848 */
+void ocl_set_pair_cache_options(OSim *s, uint32_t max_vt, uint32_t max_ee, uint32_t margin_mode, float safety,
+                                float hscale, float maxh) {
+    s->pair_max_vt = max_vt < 64u ? 64u : (max_vt > 262144u ? 262144u : max_vt);
+    s->pair_max_ee = max_ee < 64u ? 64u : (max_ee > 262144u ? 262144u : max_ee);
+    s->pair_qvt = quota_for_budget(s->pair_max_vt, (uint32_t)s->n);
+    s->pair_qee = quota_for_budget(s->pair_max_ee, (uint32_t)s->n);
+    s->pair_margin_mode = margin_mode == 0 ? 0 : 1;
+    s->pair_safety = fminf(fmaxf(safety, 0.0f), 0.05f);
+    s->pair_hscale = fminf(fmaxf(hscale, 0.0f), 4.0f);
+    s->pair_maxh = fminf(fmaxf(maxh, 0.0f), 0.1f);
+}
+/* get_pair_cache_stats (dispatch.rs:1111-1119) and get_active_pairs
+ * (dispatch.rs:1249-1290): counts = (V-T accepted, E-E accepted, stored V-T,
+ * stored E-E); stored pairs in slot order, up to the capacities */
+void ocl_get_active_pairs(const OSim *s, uint32_t *counts, uint32_t *vt, size_t vt_cap, uint32_t *ee, size_t ee_cap) {
+    counts[0] = s->pcnt[0]; counts[1] = s->pcnt[1];
+    uint32_t k = 0;
+    for (size_t q = 0; q < (size_t)s->n * s->pair_qvt; q++) {
+        const uint32_t *e = s->pvt + 4 * q;
+        if (e[0] == 0xFFFFFFFFu) continue;
+        if (vt && k < vt_cap) memcpy(vt + 4 * (size_t)k, e, 16);
+        k++;
+    }
+    counts[2] = k;
+    k = 0;
+    for (size_t q = 0; q < (size_t)s->n * s->pair_qee; q++) {
+        const uint32_t *e = s->pee + 4 * q;
+        if (e[0] == 0xFFFFFFFFu) continue;
+        if (ee && k < ee_cap) memcpy(ee + 4 * (size_t)k, e, 16);
+        k++;
+    }
+    counts[3] = k;
 }
 void ocl_set_self_collision_intervals(OSim *s, int sc_interval, int ee_interval) {
     s->sc_interval = sc_interval < 1 ? 1 : sc_interval;
@@ -2978,7 +3582,7 @@ void ocl_step(OSim *s, float dt, int substeps) {
         if (hascol && !coupled) k_collision(s, dts);
         if (s->npins > 0) k_pin(s, dts);
         if (s->edge_collision && hascol && s->ne > 0) k_edge_collision(s); /* dispatch.rs:254-283 */
-        if (do_sc) self_collision(s, run_ee);
+        if (do_sc) self_collision(s, run_ee, sub, substeps, dt);
         for (int c = 0; c < s->nsc; c++) if (s->sc_cnt[c]) k_sewing(s, c, dts); /* final sewing, dispatch.rs:323-337 */
         k_update_vel(s, dts);
     }

@@ -17,6 +17,7 @@
  */
 #ifndef TCLOTH_ORACLE_H
 #define TCLOTH_ORACLE_H
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -104,6 +105,11 @@ void ocl_build_hash(OSim *s, int which, uint32_t *cell_starts, uint32_t *sorted)
 void ocl_get_mesh_triangles(const OSim *s, float *tris16);  /* T x 16 floats (sorted) */
 /* self-collision / E-E substep intervals (dispatch.rs:105-114); defaults 1 / 1 */
 void ocl_set_self_collision_intervals(OSim *s, int sc_interval, int ee_interval);
+/* contact-pair cache (self-collision algorithm 1) */
+void ocl_set_pair_cache(OSim *s, int enable, int final_fallback);
+void ocl_set_pair_cache_options(OSim *s, uint32_t max_vt, uint32_t max_ee, uint32_t margin_mode, float safety,
+                                float hscale, float maxh);
+void ocl_get_active_pairs(const OSim *s, uint32_t *counts, uint32_t *vt, size_t vt_cap, uint32_t *ee, size_t ee_cap);
 
 /* Bone SDF (skinning.wgsl, prep_bone_triangles.wgsl, bake_sdf.wgsl,
  * collision.wgsl:116-265).  Matrices: 16 floats, column-major

@@ -42,6 +42,15 @@ SIGNATURES = {
     "tc_reset": [_P],
     "tc_set_gravity": [_P, _F, _F, _F],
     "tc_set_enable_edge_collision": [_P, _I],
+    "tc_set_enable_pair_cache": [_P, _I],
+    "tc_get_enable_pair_cache": [_P, C.POINTER(_I)],
+    "tc_set_self_collision_algorithm": [_P, _U],
+    "tc_get_self_collision_algorithm": [_P, C.POINTER(_U)],
+    "tc_set_pair_cache_options": [_P, _U, _U, _U, _F, _F, _F],
+    "tc_set_enable_pair_cache_final_fallback": [_P, _I],
+    "tc_get_enable_pair_cache_final_fallback": [_P, C.POINTER(_I)],
+    "tc_get_pair_cache_stats": [_P, _P],
+    "tc_get_active_pairs": [_P, _P, _P, C.c_size_t, _P, C.c_size_t],
     "tc_set_edge_margin_scale": [_P, _F],
     "tc_set_edge_margin_offset": [_P, _F],
     "tc_get_num_collider_edges": [_P, C.POINTER(_U)],

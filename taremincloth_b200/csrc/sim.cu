@@ -25,6 +25,7 @@
 #include "adaptive.hpp"
 #include "mesh.hpp"
 #include "selfcol_kernels.cuh"
+#include "paircache_kernels.cuh"
 #include "solver_kernels.cuh"
 #include "warmstart.cuh"
 
@@ -499,6 +500,41 @@ struct Sim {
   DBuf<int4> vs_c, es_c;
   DBuf<uint2> es_v, ccd_q;
   DBuf<uint32_t> ccd_n;
+  // contact-pair cache (self-collision algorithm 1; simulation/mod.rs:582-600,
+  // :799-893, dispatch.rs:1540-1670), off by default; buffers on first use
+  bool pair_cache = false, pair_final_fallback = true;
+  uint32_t sc_algorithm = 0;
+  uint32_t pair_max_vt = 0, pair_max_ee = 0, pair_qvt = 1, pair_qee = 1;
+  uint32_t pair_margin_mode = 1;
+  float pair_safety = 0.005f, pair_hscale = 1.3f, pair_max_h = 0.02f;
+  DBuf<uint4> pair_vt, pair_ee;
+  DBuf<uint32_t> pair_cnt, island_d;
+  // quota_for_budget (simulation/mod.rs:36-41)
+  static uint32_t quota_for_budget(uint32_t budget, uint32_t nv) {
+    return nv == 0 ? 1u : std::min(std::max(budget / nv, 1u), kPairQuotaMax);
+  }
+  void pair_defaults() {
+    pair_max_vt = pair_max_ee = std::min(std::max(n * 8u, 8192u), 262144u);
+    pair_qvt = quota_for_budget(pair_max_vt, n);
+    pair_qee = quota_for_budget(pair_max_ee, n);
+  }
+  void ensure_pair_buffers() {
+    if (pair_vt.p) return;
+    const size_t slots = std::max<size_t>(size_t(n) * kPairQuotaMax, 64);
+    pair_vt.alloc(slots);
+    pair_ee.alloc(slots);
+    pair_cnt.alloc(4);
+    island_d.upload(m.island, st);
+    TC_CK(cudaMemsetAsync(pair_vt.p, 0xFF, slots * sizeof(uint4), st));
+    TC_CK(cudaMemsetAsync(pair_ee.p, 0xFF, slots * sizeof(uint4), st));
+    TC_CK(cudaMemsetAsync(pair_cnt.p, 0, 4 * sizeof(uint32_t), st));
+    TC_CK(cudaStreamSynchronize(st));
+  }
+  void set_pair_cache(bool on) {
+    if (on) ensure_pair_buffers();
+    pair_cache = on;
+    mark();
+  }
   // colliders
   std::vector<Prim> prims_h;
   std::vector<MeshTri> tris_h;
@@ -860,6 +896,7 @@ struct Sim {
     nsw = uint32_t(sew_h.size());
     sew_speed = std::fmax(in.sew_shrink_speed, 0.f);
     upload_sew();
+    pair_defaults();
     bar.alloc(2);
     TC_CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(GridBar), st));
     TC_CK(cudaHostAlloc(&h_err, sizeof(int), cudaHostAllocDefault));
@@ -1091,7 +1128,42 @@ struct Sim {
   // atomic add / max / min, which commute with the vertex side's; so outside
   // profiling it runs on a second stream concurrently with the vertex side
   // (vertex hash, V-V / V-T, untangle), joined before apply.
-  void encode_self_collision(bool run_ee = true) {
+  PairArgs pair_args(float dt) {
+    PairArgs p;
+    p.safety = pair_safety; p.dt_frame = dt; p.hscale = pair_hscale; p.max_h = pair_max_h;
+    p.margin_mode = pair_margin_mode; p.quota_vt = pair_qvt; p.quota_ee = pair_qee;
+    p.island = island_d.p; p.vt = pair_vt.p; p.ee = pair_ee.p; p.counters = pair_cnt.p;
+    return p;
+  }
+  // Pair-cache pass (dispatch.rs:1556-1645): the vertex hash and the broad
+  // phase only at the first substep of the frame, the narrow phase over the
+  // cached slots at every substep.  With the final fallback on (default) the
+  // last substep runs the direct pass on a fresh hash instead.
+  void encode_pair_self_collision(bool run_ee, bool rebuild, float dt) {
+    SCArgs a = sc_args();
+    const PairArgs p = pair_args(dt);
+    if (a.untangle) timed("sc_normals", [&] { k_normals<<<grid(n, 256), 256, 0, st>>>(n, x4.p, star_off.p, star_idx.p, nrm.p); });
+    if (rebuild) {
+      encode_hash(0);
+      TC_CK(cudaMemsetAsync(pair_cnt.p, 0, 4 * sizeof(uint32_t), st));
+      timed("pair_collect", [&] { k_pair_collect<<<grid(n, 128), 128, 0, st>>>(a, p); });
+    }
+    const uint32_t vts = n * pair_qvt, ees = n * pair_qee;
+    timed("pair_vt", [&] { k_pair_vt<<<grid(vts, 128), 128, 0, st>>>(a, p, vts); });
+    if (run_ee) timed("pair_ee", [&] { k_pair_ee<<<grid(ees, 128), 128, 0, st>>>(a, p, ees); });
+    if (a.untangle) timed("sc_untangle", [&] { k_untangle<<<grid(n, 128), 128, 0, st>>>(a); });
+    timed("sc_apply", [&] {
+      k_apply<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, local_len.p, acc.p, relief, enable_relief ? 1 : 0,
+                                             max_disp_ratio);
+    });
+  }
+
+  void encode_self_collision(bool run_ee, uint32_t s, uint32_t substeps, float dt) {
+    const bool force_direct = pair_cache && pair_final_fallback && s + 1 == substeps;
+    if (pair_cache && !force_direct) {
+      encode_pair_self_collision(run_ee, s == 0, dt);
+      return;
+    }
     SCArgs a = sc_args();
     if (a.untangle) timed("sc_normals", [&] { k_normals<<<grid(n, 256), 256, 0, st>>>(n, x4.p, star_off.p, star_idx.p, nrm.p); });
     const bool edges_on = run_ee && ne > 0;
@@ -1444,7 +1516,7 @@ struct Sim {
       }
       if (self_collision || edge_active()) {
         if (edge_active()) encode_edge_collision();
-        if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
+        if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps), s, substeps, dt);
         if (nsw) timed("final_sewing", [&] { launch_sewing(sp.dt); });
         timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, sp.dt); });
       } else if (colors) {
@@ -1625,7 +1697,7 @@ struct Sim {
         for (uint32_t s = 0; s < substeps; ++s) {
           launch_persistent(solver_args(sp, 1, use_coupled, false));
           if (edge_active()) encode_edge_collision();
-          if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
+          if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps), s, substeps, dt);
           launch_sewing(sp.dt);  // final sewing (dispatch.rs:323-337)
           k_update_vel<<<grid(n, 256), 256, 0, st>>>(n, x4.p, p4.p, v4.p, sp.dt);
         }
@@ -1687,7 +1759,7 @@ struct Sim {
       if (hascol && !use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
       if (npins) timed("pin", [&] { launch_k(k_pin, grid(npins, 128), 128, npins, pin_v.p, pin_t.p, x4.p, p4.p, dts); });
       if (edge_active()) encode_edge_collision();
-      if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps));
+      if (sc_due(s, substeps)) encode_self_collision(ee_due(s, substeps), s, substeps, dt);
       if (nsw) timed("final_sewing", [&] { launch_sewing(dts); });
       timed("update_vel", [&] { launch_k(k_update_vel, grid(n, 256), 256, n, x4.p, p4.p, v4.p, dts); });
     }
@@ -2460,6 +2532,85 @@ tc_status tc_set_self_collision_options(tc_sim* s, float relief, float ratio, in
     m.relief = relief; m.max_disp_ratio = ratio; m.enable_relief = relief < 0.999f;
     m.exclude_neighbors = excl != 0; m.untangle_opt = untangle != 0; m.max_search = maxit;
     m.mark();
+  });
+}
+tc_status tc_set_enable_pair_cache(tc_sim* s, int enable) {
+  return guard([&] { S(s).set_pair_cache(enable != 0); });
+}
+tc_status tc_get_enable_pair_cache(tc_sim* s, int* enabled) {
+  return guard([&] { need(enabled != nullptr, "enabled required"); *enabled = S(s).pair_cache ? 1 : 0; });
+}
+tc_status tc_set_self_collision_algorithm(tc_sim* s, uint32_t algo) {
+  return guard([&] {
+    need(algo <= 1u, "self-collision algorithm 2 (virtual-particle vertex-vertex) is not built");
+    Sim& m = S(s);
+    m.set_pair_cache(algo == 1u);
+    m.sc_algorithm = algo;
+  });
+}
+tc_status tc_get_self_collision_algorithm(tc_sim* s, uint32_t* algo) {
+  return guard([&] { need(algo != nullptr, "algo required"); *algo = S(s).sc_algorithm; });
+}
+tc_status tc_set_pair_cache_options(tc_sim* s, uint32_t max_vt_pairs, uint32_t max_ee_pairs, uint32_t margin_mode,
+                                    float safety_margin, float horizon_scale, float max_horizon) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.pair_max_vt = std::min(std::max(max_vt_pairs, 64u), 262144u);
+    m.pair_max_ee = std::min(std::max(max_ee_pairs, 64u), 262144u);
+    m.pair_qvt = Sim::quota_for_budget(m.pair_max_vt, m.n);
+    m.pair_qee = Sim::quota_for_budget(m.pair_max_ee, m.n);
+    m.pair_margin_mode = margin_mode == 0 ? 0u : 1u;
+    m.pair_safety = std::min(std::max(safety_margin, 0.f), 0.05f);
+    m.pair_hscale = std::min(std::max(horizon_scale, 0.f), 4.f);
+    m.pair_max_h = std::min(std::max(max_horizon, 0.f), 0.1f);
+    m.mark();
+  });
+}
+tc_status tc_set_enable_pair_cache_final_fallback(tc_sim* s, int enable) {
+  return guard([&] { Sim& m = S(s); m.pair_final_fallback = enable != 0; m.mark(); });
+}
+tc_status tc_get_enable_pair_cache_final_fallback(tc_sim* s, int* enabled) {
+  return guard([&] { need(enabled != nullptr, "enabled required"); *enabled = S(s).pair_final_fallback ? 1 : 0; });
+}
+tc_status tc_get_pair_cache_stats(tc_sim* s, uint32_t out[4]) {
+  return guard([&] {
+    need(out != nullptr, "out required");
+    Sim& m = S(s);
+    uint32_t c[4] = {0u, 0u, 0u, 0u};
+    if (m.pair_cnt.p) {
+      TC_CK(cudaMemcpyAsync(c, m.pair_cnt.p, sizeof c, cudaMemcpyDeviceToHost, m.st));
+      TC_CK(cudaStreamSynchronize(m.st));
+    }
+    out[0] = c[0]; out[1] = c[1]; out[2] = m.pair_max_vt; out[3] = m.pair_max_ee;
+  });
+}
+tc_status tc_get_active_pairs(tc_sim* s, uint32_t counts[4], uint32_t* vt_pairs, size_t vt_cap, uint32_t* ee_pairs,
+                              size_t ee_cap) {
+  return guard([&] {
+    need(counts != nullptr, "counts required");
+    Sim& m = S(s);
+    counts[0] = counts[1] = counts[2] = counts[3] = 0u;
+    if (!m.pair_cnt.p) return;
+    uint32_t c[4];
+    TC_CK(cudaMemcpyAsync(c, m.pair_cnt.p, sizeof c, cudaMemcpyDeviceToHost, m.st));
+    const size_t nvt = size_t(m.n) * m.pair_qvt, nee = size_t(m.n) * m.pair_qee;
+    std::vector<uint4> hv(nvt), he(nee);
+    if (nvt) TC_CK(cudaMemcpyAsync(hv.data(), m.pair_vt.p, nvt * sizeof(uint4), cudaMemcpyDeviceToHost, m.st));
+    if (nee) TC_CK(cudaMemcpyAsync(he.data(), m.pair_ee.p, nee * sizeof(uint4), cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    counts[0] = c[0];
+    counts[1] = c[1];
+    auto take = [](const std::vector<uint4>& src, uint32_t* dst, size_t cap) {
+      uint32_t k = 0;
+      for (const uint4& q : src) {
+        if (q.x == tcloth::kPairSentinel) continue;
+        if (dst && k < cap) { dst[4 * size_t(k)] = q.x; dst[4 * size_t(k) + 1] = q.y; dst[4 * size_t(k) + 2] = q.z; dst[4 * size_t(k) + 3] = q.w; }
+        ++k;
+      }
+      return k;
+    };
+    counts[2] = take(hv, vt_pairs, vt_cap);
+    counts[3] = take(he, ee_pairs, ee_cap);
   });
 }
 tc_status tc_set_coupled_collider(tc_sim* s, int on) {

@@ -179,6 +179,10 @@ class ClothSimulator:
         self._L = L
         self._n = n
         self._solver_iterations = 2
+        if enable_pair_cache is not None:
+            self.set_enable_pair_cache(enable_pair_cache)
+        if self_collision_algorithm is not None:
+            self.set_self_collision_algorithm(self_collision_algorithm)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -247,6 +251,57 @@ class ClothSimulator:
     def get_positions(self, out_array):
         out = self._out(out_array)
         self._c(self._L.tc_get_positions(self._h, _ptr(out), out.size))
+
+    # ---------------- contact-pair cache (lib.rs:2029-2105)
+    def set_enable_pair_cache(self, enable):
+        self._c(self._L.tc_set_enable_pair_cache(self._h, int(bool(enable))))
+
+    def set_pair_cache_enabled(self, enabled):
+        self.set_enable_pair_cache(enabled)
+
+    def get_enable_pair_cache(self):
+        v = C.c_int()
+        self._c(self._L.tc_get_enable_pair_cache(self._h, C.byref(v)))
+        return bool(v.value)
+
+    def set_self_collision_algorithm(self, algo):
+        """0: direct, 1: contact-pair cache; 2 (virtual particles) is not built."""
+        if int(algo) == 2:
+            raise NotImplementedError("self-collision algorithm 2 (virtual-particle vertex-vertex) is not built")
+        self._c(self._L.tc_set_self_collision_algorithm(self._h, int(algo)))
+
+    def get_self_collision_algorithm(self):
+        v = C.c_uint32()
+        self._c(self._L.tc_get_self_collision_algorithm(self._h, C.byref(v)))
+        return v.value
+
+    def set_pair_cache_options(self, max_vt_pairs=65536, max_ee_pairs=65536, margin_mode=1, safety_margin=0.005,
+                               horizon_scale=1.3, max_horizon=0.02):
+        self._c(self._L.tc_set_pair_cache_options(self._h, int(max_vt_pairs), int(max_ee_pairs), int(margin_mode),
+                                                  float(safety_margin), float(horizon_scale), float(max_horizon)))
+
+    def set_enable_pair_cache_final_fallback(self, enable):
+        self._c(self._L.tc_set_enable_pair_cache_final_fallback(self._h, int(bool(enable))))
+
+    def get_enable_pair_cache_final_fallback(self):
+        v = C.c_int()
+        self._c(self._L.tc_get_enable_pair_cache_final_fallback(self._h, C.byref(v)))
+        return bool(v.value)
+
+    def get_pair_cache_stats(self):
+        """(vt_count, ee_count, max_vt_pairs, max_ee_pairs) of the latest broad phase."""
+        out = np.zeros(4, _u32)
+        self._c(self._L.tc_get_pair_cache_stats(self._h, _ptr(out)))
+        return tuple(int(x) for x in out)
+
+    def get_active_pairs(self):
+        """(vt_count, ee_count, V-T pairs, E-E pairs): the stored pairs as lists of four vertex ids."""
+        c = np.zeros(4, _u32)
+        self._c(self._L.tc_get_active_pairs(self._h, _ptr(c), None, 0, None, 0))
+        vt = np.zeros((max(int(c[2]), 1), 4), _u32)
+        ee = np.zeros((max(int(c[3]), 1), 4), _u32)
+        self._c(self._L.tc_get_active_pairs(self._h, _ptr(c), _ptr(vt), int(c[2]), _ptr(ee), int(c[3])))
+        return (int(c[0]), int(c[1]), vt[:int(c[2])].tolist(), ee[:int(c[3])].tolist())
 
     # ---------------- edge colliders (lib.rs:2736-2749)
     def set_enable_edge_collision(self, enable):
