@@ -276,6 +276,42 @@ def sewing_extra(steps):
             "sewing_constraints": s.get_num_sewing_constraints()}
 
 
+def pair_cache_extra(steps):
+    """Config 2 (131,072 vertices) with the contact-pair cache (self-collision
+    algorithm 1, the reference's defaults: quota 2 from the 262,144-pair
+    budget, velocity horizon, direct pass on the last substep) and with the
+    final fallback off, against the direct pass; device time per frame over
+    the same frames (4..), and a per-pass profile of one frame."""
+    from taremincloth_b200 import ClothSimulator, scenes
+    sc = scenes.config2()
+    n = len(sc["positions"])
+    dt, sub = sc["dt"], sc["substeps"]
+    out = {"workload": f"two 256x256 sheets ({n} vertices) on the icosphere, self-collision on, {sub} substeps x "
+                       f"{sc['iterations']} iterations"}
+    for name, pc, fb in [("direct", False, True), ("pair_cache", True, True), ("pair_cache_no_fallback", True, False)]:
+        s = scenes.build(ClothSimulator, sc)
+        s.set_enable_pair_cache(pc)
+        s.set_enable_pair_cache_final_fallback(fb)
+        for _ in range(3):
+            s.step(dt, sub)
+        ms = 0.0
+        for _ in range(steps):
+            s.step(dt, sub)
+            ms += s.last_frame_ms()
+        ms /= steps
+        s.set_profiling_enabled(True)
+        s.step(dt, sub)
+        prof = sorted(s.take_profile(), key=lambda r: -r[1])
+        s.set_profiling_enabled(False)
+        r = {"ms_per_frame": ms, "vertex_substeps_per_s": n * sub / (ms / 1e3),
+             "profile_ms_per_frame": {k: round(v, 3) for k, v, _ in prof[:8]}}
+        if pc:
+            r["pair_stats"] = list(s.get_pair_cache_stats())
+        out[name] = r
+        del s
+    return out
+
+
 def _warm_start_case(sim, n, dt, sub, iters, steps, ks, rec_frames, every, workload):
     """Record plain-solver snapshots, train, calibrate the relative residual
     threshold on plain substeps (p90 of final / predicted residual), then
@@ -489,6 +525,7 @@ def main():
         line["warm_start"] = warm_start_extra(3)
         line["bone_sdf_config3"] = bone_sdf_extra(3)
         line["sewing"] = sewing_extra(3)
+        line["pair_cache_config2"] = pair_cache_extra(3)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

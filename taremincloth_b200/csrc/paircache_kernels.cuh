@@ -35,6 +35,7 @@ struct PairArgs {
   uint32_t margin_mode;  // 0 fixed, 1 velocity horizon
   uint32_t quota_vt, quota_ee;
   const uint32_t* island;
+  float* hz;          // per-vertex horizon x mode (k_pair_horizon)
   uint4* vt;          // n * quota_vt slots (vert_i, c0, c1, c2)
   uint4* ee;          // n * quota_ee slots (v_i, v_ui, c_j, c_vj)
   uint32_t* counters; // vt_count, ee_count, vt_dropped, ee_dropped
@@ -52,29 +53,39 @@ __device__ __forceinline__ float pc_horizon(const PairArgs& a, float4 v) {
   return fminf(length(mk(v)) * a.dt_frame * a.hscale, a.max_h);
 }
 
-// can_ee_anchor_reach (self_collision_collect_pairs.wgsl:262-283)
+// Per-vertex velocity horizon times the margin mode, the term every bound of
+// the broad phase adds per vertex (collect_pairs.wgsl:328-330, :354-360,
+// :277-278): min(|v| dt_frame scale, max_horizon) * mode.
+__global__ void k_pair_horizon(uint32_t n, const float4* __restrict__ v4, PairArgs a) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a.hz[i] = pc_horizon(a, v4[i]) * (float)a.margin_mode;
+}
+
+// can_ee_anchor_reach (self_collision_collect_pairs.wgsl:262-283); the cells
+// are the hash pass's floor(p / cell) of the same positions
 __device__ __forceinline__ bool pc_anchor_reach(const SCArgs& s, const PairArgs& a, uint32_t u, uint32_t w) {
   if (s.x4[u].w <= 0.0f) return false;
-  const float4 pu = s.p4[u], pw = s.p4[w];
-  const I3 cu = cell_of(mk(pu), s.cell), cw = cell_of(mk(pw), s.cell);
+  const int4 cu = s.vcell[u], cw = s.vcell[w];
   if (pc_far_axis(cu.x, cw.x) || pc_far_axis(cu.y, cw.y) || pc_far_axis(cu.z, cw.z)) return false;
+  const float4 pu = s.p4[u], pw = s.p4[w];
   const V3 d = mk(pu) - mk(pw);
   const float d2 = dot(d, d);
-  const float mf = (float)a.margin_mode;
-  const float hu = pc_horizon(a, s.v4[u]) * mf;
-  const float hw = pc_horizon(a, s.v4[w]) * mf;
-  const float b = pu.w + pw.w + (s.local_len[u] + s.local_len[w]) * 1.3f + a.safety + hu + hw;
+  const float b = pu.w + pw.w + (s.local_len[u] + s.local_len[w]) * 1.3f + a.safety + a.hz[u] + a.hz[w];
   if (d2 > b * b) return false;
   if (a.island[u] == a.island[w] && s.exclude_neighbors) {
     if (near_folded(s, u, w, sqrtf(fmaxf(d2, 0.0f)))) return false;
   }
   return true;
 }
-// is_smaller_anchor_reachable (:286-292)
+// is_smaller_anchor_reachable (:286-292): anchor (u, w) before (cu, cw) in
+// lexicographic order, and reachable
+__device__ __forceinline__ bool pc_lex_lt(uint32_t u, uint32_t w, uint32_t cu, uint32_t cw) {
+  return !(u > cu || (u == cu && w >= cw));
+}
 __device__ __forceinline__ bool pc_smaller_anchor(const SCArgs& s, const PairArgs& a, uint32_t u, uint32_t w,
                                                   uint32_t cu, uint32_t cw) {
-  if (u > cu || (u == cu && w >= cw)) return false;
-  return pc_anchor_reach(s, a, u, w);
+  return pc_lex_lt(u, w, cu, cw) && pc_anchor_reach(s, a, u, w);
 }
 
 __device__ __forceinline__ bool key_lt(uint3 a, uint3 b) {
@@ -93,6 +104,13 @@ __device__ __forceinline__ void topk_init(TopK& t) {
   t.n = t.eval = t.drop = 0u;
 #pragma unroll
   for (int q = 0; q < (int)kPairQuotaMax; ++q) { t.d[q] = 0.0f; t.k[q] = make_uint3(0u, 0u, 0u); }
+}
+__device__ __forceinline__ bool topk_has(const TopK& t, uint3 key) {
+  bool f = false;
+#pragma unroll
+  for (uint32_t q = 0; q < kPairQuotaMax; ++q)
+    if (q < t.n && t.k[q].x == key.x && t.k[q].y == key.y && t.k[q].z == key.z) f = true;
+  return f;
 }
 __device__ __forceinline__ void topk_insert(TopK& t, uint32_t quota, float d, uint3 key) {
   bool dup = false;
@@ -125,6 +143,16 @@ __device__ __forceinline__ void topk_insert(TopK& t, uint32_t quota, float d, ui
 }
 
 // ---------------- broad phase: self_collision_collect_pairs.wgsl:293-661
+// Same visiting order and predicates as the reference; pure predicates are
+// evaluated in a cheaper order, which changes no outcome:
+// * candidates come from the hash pass's sorted records (p, thickness,
+//   cell, index, local length, inverse mass);
+// * a key already in the list is skipped before its distance is computed
+//   (the insert would reject it as a duplicate);
+// * the seven "smaller anchor" terms of an edge pair are split by what they
+//   depend on: (j, index) once per j, (ui, j) and (j, ui) once per ui,
+//   (index, vj) and (vj, index) once per j as a mask over vj, and only
+//   (ui, vj) and (vj, ui) per pair; any true term skips the pair.
 __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
   const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
   if (index >= s.n) return;
@@ -133,13 +161,11 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
   const V3 pi = mk(pi4);
   const float lli = s.local_len[index];
   const float thi = pi4.w;
-  const I3 base = cell_of(pi, s.cell);
+  const int4 base = s.vcell[index];
   const uint32_t qvt = min(max(a.quota_vt, 1u), kPairQuotaMax);
   const uint32_t qee = min(max(a.quota_ee, 1u), kPairQuotaMax);
   const float margin = a.safety;
-  const float hi_raw = pc_horizon(a, s.v4[index]);
-  const float mf = (float)a.margin_mode;
-  const float hie = hi_raw * mf;
+  const float hie = a.hz[index];
   const uint32_t isl_i = a.island[index];
   TopK vt, ee;
   topk_init(vt);
@@ -151,24 +177,24 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
         const uint32_t h = hash3(cx, cy, cz, s.table);
         const uint32_t b0 = s.cs[h], b1 = s.cs[h + 1];
         for (uint32_t k = b0; k < b1; ++k) {
-          const uint32_t j = s.srt[k];
+          const int4 jc = s.vs_c[k];
+          const uint32_t j = (uint32_t)jc.w;
           if (j >= s.n || j == index) continue;
-          const float4 pj4 = s.p4[j];
-          const V3 pj = mk(pj4);
-          const I3 jc = cell_of(pj, s.cell);
           if (jc.x != cx || jc.y != cy || jc.z != cz) continue;
-          const bool pin_j = s.x4[j].w <= 0.0f;
+          const float4 q = s.vs_q[k];  // local length, layer, inverse mass, |p - x|
+          const bool pin_j = q.z <= 0.0f;
           if (pin_i && pin_j) continue;
-          const float hj = pc_horizon(a, s.v4[j]) * mf;
+          const float4 pj4 = s.vs_p[k];
+          const V3 pj = mk(pj4);
+          const float hj = a.hz[j];
           const V3 dvv = pi - pj;
           const float d2vv = dot(dvv, dvv);
           const float eth = thi + pj4.w;
-          const float llj = s.local_len[j];
+          const float llj = q.x;
           const float broad = eth + (lli + llj) * 1.3f + margin + hie + hj;
           if (!(d2vv <= broad * broad)) continue;
           const bool same_island = isl_i == a.island[j];
-          const float dvvl = sqrtf(fmaxf(d2vv, 0.0f));
-          if (same_island && s.exclude_neighbors && near_folded(s, index, j, dvvl)) continue;
+          if (same_island && s.exclude_neighbors && near_folded(s, index, j, sqrtf(fmaxf(d2vv, 0.0f)))) continue;
           const float check = eth + margin + hie + hj;
           // 1. vertex-triangle candidates over j's star (:380-476)
           const float vtb = eth + llj * 1.3f + margin + hie + hj;
@@ -185,6 +211,8 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
                 uint32_t c0 = j, c1 = v0, c2 = v1;
                 if (v0 < j && v0 < v1) { c0 = v0; c1 = v1; c2 = j; }
                 else if (v1 < j && v1 < v0) { c0 = v1; c1 = j; c2 = v0; }
+                const uint3 key = make_uint3(c0, c1, c2);
+                if (topk_has(vt, key)) continue;
                 bool isf;
                 V3 bary;
                 const V3 cp = closest_tri(pi, mk(s.p4[c0]), mk(s.p4[c1]), mk(s.p4[c2]), isf, bary);
@@ -192,18 +220,28 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
                 const float d2vt = dot(dvt, dvt);
                 if (d2vt < check * check) {
                   if (s.exclude_neighbors && (within2(s, index, v0) || within2(s, index, v1))) continue;
-                  topk_insert(vt, qvt, d2vt, make_uint3(c0, c1, c2));
+                  topk_insert(vt, qvt, d2vt, key);
                 }
               }
             }
           }
-          // 2. edge-edge candidates over both one-rings (:478-612)
+          // 2. edge-edge candidates over both one-rings (:478-612); only a
+          // free vertex collects them
+          if (pin_i) continue;
           const float eeb = eth + (lli + llj) * 1.3f + margin + hie + hj;
           if (!(d2vv <= eeb * eeb)) continue;
           const uint32_t ai0 = s.adj_off[index], ai1 = s.adj_off[index + 1];
           const uint32_t aj0 = s.adj_off[j], aj1 = s.adj_off[j + 1];
           if (!(ai0 < ai1 && aj0 < aj1)) continue;
+          if (pc_smaller_anchor(s, a, j, index, index, j)) continue;
           const uint32_t nei = min(ai1 - ai0, 8u), nej = min(aj1 - aj0, 8u);
+          uint32_t skipv = 0u;
+          for (uint32_t e2 = 0; e2 < nej; ++e2) {
+            const uint32_t vj = s.adj_idx[aj0 + e2];
+            if (vj >= s.n) continue;
+            if (pc_smaller_anchor(s, a, index, vj, index, j) || pc_smaller_anchor(s, a, vj, index, index, j))
+              skipv |= 1u << e2;
+          }
           for (uint32_t e1 = 0; e1 < nei; ++e1) {
             const uint32_t ui = s.adj_idx[ai0 + e1];
             if (ui >= s.n) continue;
@@ -213,23 +251,22 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
             const float lsi = dot(li, li);
             const float mli = (lli + llui) * 1.5f;
             if (lsi > mli * mli || lsi <= 1e-12f) continue;
+            if (pc_smaller_anchor(s, a, ui, j, index, j) || pc_smaller_anchor(s, a, j, ui, index, j)) continue;
             for (uint32_t e2 = 0; e2 < nej; ++e2) {
               const uint32_t vj = s.adj_idx[aj0 + e2];
               if (vj >= s.n) continue;
               if (!(ui != j && ui != vj && index != vj)) continue;
+              if ((skipv >> e2) & 1u) continue;
               const uint32_t cj = min(j, vj), cvj = max(j, vj);
-              const bool smaller =
-                  pc_smaller_anchor(s, a, index, vj, index, j) || pc_smaller_anchor(s, a, ui, j, index, j) ||
-                  pc_smaller_anchor(s, a, ui, vj, index, j) || pc_smaller_anchor(s, a, j, index, index, j) ||
-                  pc_smaller_anchor(s, a, j, ui, index, j) || pc_smaller_anchor(s, a, vj, index, index, j) ||
-                  pc_smaller_anchor(s, a, vj, ui, index, j);
-              if (pin_i || smaller) continue;
+              const uint3 key = make_uint3(ui, cj, cvj);
+              if (topk_has(ee, key)) continue;
               const V3 pvj = mk(s.p4[vj]);
               const float llvj = s.local_len[vj];
               const V3 lj = pvj - pj;
               const float lsj = dot(lj, lj);
               const float mlj = (llj + llvj) * 1.5f;
               if (lsj > mlj * mlj || lsj <= 1e-12f) continue;
+              if (pc_smaller_anchor(s, a, ui, vj, index, j) || pc_smaller_anchor(s, a, vj, ui, index, j)) continue;
               const V3 pcj = j < vj ? pj : pvj;
               const V3 pcvj = j < vj ? pvj : pj;
               float sp, tp;
@@ -244,7 +281,7 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
                       near_folded(s, ui, vj, length(pui - pvj)))
                     continue;
                 }
-                topk_insert(ee, qee, d2ee, make_uint3(ui, cj, cvj));
+                topk_insert(ee, qee, d2ee, key);
               }
             }
           }

@@ -509,6 +509,7 @@ struct Sim {
   float pair_safety = 0.005f, pair_hscale = 1.3f, pair_max_h = 0.02f;
   DBuf<uint4> pair_vt, pair_ee;
   DBuf<uint32_t> pair_cnt, island_d;
+  DBuf<float> pair_hz;
   // quota_for_budget (simulation/mod.rs:36-41)
   static uint32_t quota_for_budget(uint32_t budget, uint32_t nv) {
     return nv == 0 ? 1u : std::min(std::max(budget / nv, 1u), kPairQuotaMax);
@@ -524,6 +525,7 @@ struct Sim {
     pair_vt.alloc(slots);
     pair_ee.alloc(slots);
     pair_cnt.alloc(4);
+    pair_hz.alloc(n);
     island_d.upload(m.island, st);
     TC_CK(cudaMemsetAsync(pair_vt.p, 0xFF, slots * sizeof(uint4), st));
     TC_CK(cudaMemsetAsync(pair_ee.p, 0xFF, slots * sizeof(uint4), st));
@@ -1132,7 +1134,7 @@ struct Sim {
     PairArgs p;
     p.safety = pair_safety; p.dt_frame = dt; p.hscale = pair_hscale; p.max_h = pair_max_h;
     p.margin_mode = pair_margin_mode; p.quota_vt = pair_qvt; p.quota_ee = pair_qee;
-    p.island = island_d.p; p.vt = pair_vt.p; p.ee = pair_ee.p; p.counters = pair_cnt.p;
+    p.island = island_d.p; p.hz = pair_hz.p; p.vt = pair_vt.p; p.ee = pair_ee.p; p.counters = pair_cnt.p;
     return p;
   }
   // Pair-cache pass (dispatch.rs:1556-1645): the vertex hash and the broad
@@ -1146,7 +1148,10 @@ struct Sim {
     if (rebuild) {
       encode_hash(0);
       TC_CK(cudaMemsetAsync(pair_cnt.p, 0, 4 * sizeof(uint32_t), st));
-      timed("pair_collect", [&] { k_pair_collect<<<grid(n, 128), 128, 0, st>>>(a, p); });
+      timed("pair_collect", [&] {
+        k_pair_horizon<<<grid(n, 256), 256, 0, st>>>(n, v4.p, p);
+        k_pair_collect<<<grid(n, 128), 128, 0, st>>>(a, p);
+      });
     }
     const uint32_t vts = n * pair_qvt, ees = n * pair_qee;
     timed("pair_vt", [&] { k_pair_vt<<<grid(vts, 128), 128, 0, st>>>(a, p, vts); });
