@@ -291,6 +291,26 @@ tc_status tc_bake_bone_sdf(const float *mesh_verts, uint32_t n_verts, const int3
 tc_status tc_bake_mesh_sdf(const float *mesh_verts, uint32_t nv, const int32_t *mesh_tris, uint32_t nt,
                            float voxel_size, float margin, float friction, float thickness, float restitution,
                            int close_open_boundaries, int device, tc_bake **out);
+/* bake_mesh_sdf_hierarchical_gpu (lib.rs:1418-1488; sdf_baker.rs:1603-1900,
+ * bake_mesh_sdf_hier_*.wgsl): the same field in two passes.  The coarse
+ * pass keeps, per cell of max(voxel x 4, 0.001), the 8 nearest triangles.
+ * A fine voxel whose parent cell is at least band + half a cell diagonal
+ * from the surface copies the parent's value (band = 4 fine voxels); the
+ * others take the nearest of the candidates of the 5 x 5 x 5 cells around
+ * the parent, rescanning every triangle when the best two are within
+ * 0.2 mm with opposite signs.  A band wider than two coarse cells, or no
+ * vertices: TC_ERR_CUDA, like the reference's errors. */
+tc_status tc_bake_mesh_sdf_hierarchical(const float *mesh_verts, uint32_t nv, const int32_t *mesh_tris, uint32_t nt,
+                                        float voxel_size, float margin, float friction, float thickness,
+                                        float restitution, int close_open_boundaries, int device, tc_bake **out);
+/* bake_mesh_sdf_coarse_gpu (lib.rs:1490-1540; sdf_baker.rs:1328-1600), the
+ * coarse pass alone (open loops always capped): texels = packed distance per
+ * coarse voxel; tc_bake_get_nearest gives the 8 nearest triangle indices per
+ * voxel (voxel * 8 + k, nearest first) and the coarse voxel size. */
+tc_status tc_bake_mesh_sdf_coarse(const float *mesh_verts, uint32_t nv, const int32_t *mesh_tris, uint32_t nt,
+                                  float voxel_size, float margin, float friction, float thickness, float restitution,
+                                  int device, tc_bake **out);
+tc_status tc_bake_get_nearest(tc_bake *b, uint32_t *nearest, float *coarse_voxel);
 tc_status tc_bake_dims(tc_bake *b, uint32_t out[4]);
 /* texels (w*h*d), infos (n_active x 20), active (source bone index per
  * active bone), bind (n_active x 16); any may be NULL */

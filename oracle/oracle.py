@@ -50,6 +50,10 @@ def lib():
         L.ocl_get_bending_gate.argtypes = [P, fp]
         L.ocl_bake_mesh_sdf.argtypes = [P, C.c_int, P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
                                          C.c_float, P, P, P]
+        L.ocl_bake_mesh_sdf_coarse.argtypes = [P, C.c_int, P, C.c_int, C.c_float, C.c_float, C.c_float, P, P, P, P]
+        L.ocl_bake_mesh_sdf_hier.argtypes = [P, C.c_int, P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                             C.c_float, P, P, P]
+        L.ocl_bake_mesh_sdf_hier.restype = C.c_int
         L.ocl_set_edge_collision.argtypes = [P, C.c_int, C.c_float, C.c_float]
         L.ocl_num_collider_edges.argtypes = [P]
         L.ocl_num_collider_edges.restype = C.c_int
@@ -430,4 +434,41 @@ def bake_mesh_sdf(verts, tris, voxel_size=0.004, margin=0.02, friction=0.5, thic
     tex = np.zeros(int(dims[0]) * int(dims[1]) * int(dims[2]), _u)
     L.ocl_bake_mesh_sdf(_ptr(v), v.shape[0], _ptr(t), t.shape[0], voxel_size, margin, friction, thickness,
                         restitution, _ptr(dims), _ptr(info), _ptr(tex))
+    return dims, info, tex.reshape(int(dims[2]), int(dims[1]), int(dims[0]))
+
+
+def bake_mesh_sdf_coarse(verts, tris, voxel_size=0.004, margin=0.02, thickness=0.005):
+    """Coarse pass of the hierarchical bake of a closed mesh:
+    (dims (3,), coarse_voxel, dist (d, h, w) uint32, nearest (d, h, w, 8) uint32)."""
+    L = lib()
+    v = np.ascontiguousarray(verts, dtype=_f).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 3)
+    dims = np.zeros(3, _u)
+    cv = np.zeros(1, _f)
+    L.ocl_bake_mesh_sdf_coarse(_ptr(v), v.shape[0], _ptr(t), t.shape[0], voxel_size, margin, thickness, _ptr(dims),
+                               _ptr(cv), None, None)
+    n = int(dims[0]) * int(dims[1]) * int(dims[2])
+    dist = np.zeros(n, _u)
+    near = np.zeros(n * 8, _u)
+    L.ocl_bake_mesh_sdf_coarse(_ptr(v), v.shape[0], _ptr(t), t.shape[0], voxel_size, margin, thickness, _ptr(dims),
+                               _ptr(cv), _ptr(dist), _ptr(near))
+    shape = (int(dims[2]), int(dims[1]), int(dims[0]))
+    return dims, float(cv[0]), dist.reshape(shape), near.reshape(shape + (8,))
+
+
+def bake_mesh_sdf_hierarchical(verts, tris, voxel_size=0.004, margin=0.02, friction=0.5, thickness=0.005,
+                               restitution=0.0):
+    """Hierarchical bake of a closed mesh: (dims, info, texels (d, h, w)); raises
+    RuntimeError when the band is wider than two coarse cells."""
+    L = lib()
+    v = np.ascontiguousarray(verts, dtype=_f).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 3)
+    dims = np.zeros(3, _u)
+    info = np.zeros(20, _f)
+    if L.ocl_bake_mesh_sdf_hier(_ptr(v), v.shape[0], _ptr(t), t.shape[0], voxel_size, margin, friction, thickness,
+                                restitution, _ptr(dims), _ptr(info), None):
+        raise RuntimeError("band wider than two coarse cells")
+    tex = np.zeros(int(dims[0]) * int(dims[1]) * int(dims[2]), _u)
+    L.ocl_bake_mesh_sdf_hier(_ptr(v), v.shape[0], _ptr(t), t.shape[0], voxel_size, margin, friction, thickness,
+                             restitution, _ptr(dims), _ptr(info), _ptr(tex))
     return dims, info, tex.reshape(int(dims[2]), int(dims[1]), int(dims[0]))

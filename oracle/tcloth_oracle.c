@@ -1758,10 +1758,10 @@ void ocl_bone_prep(int nt, const float *skinned4, const float *inv_mats, const u
  * mesh_sdf_domain / mesh_sdf_bone_info / collect_mesh_bake_triangles
  * (sdf_baker.rs:939-1060) and bake_mesh_sdf.wgsl, every triangle of every
  * voxel in order.  dims and info are written; texels (w x h x d) when given. */
-void ocl_bake_mesh_sdf(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
-                       float friction, float thickness, float restitution, uint32_t *dims, float *info,
-                       uint32_t *texels) {
-    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, size[3];
+/* mesh_sdf_domain / mesh_sdf_bone_info, sdf_baker.rs:939-1016 */
+static void mesh_domain(const float *verts, int nv, float voxel, float margin, float friction, float thickness,
+                        float restitution, float *lo, float *hi, float *size, uint32_t *dims, float *info) {
+    for (int k = 0; k < 3; k++) { lo[k] = INFINITY; hi[k] = -INFINITY; }
     for (int v = 0; v < nv; v++)
         for (int k = 0; k < 3; k++) { lo[k] = fminf(lo[k], verts[3 * v + k]); hi[k] = fmaxf(hi[k], verts[3 * v + k]); }
     float vs = fmaxf(voxel, 0.001f);
@@ -1774,13 +1774,17 @@ void ocl_bake_mesh_sdf(const float *verts, int nv, const int32_t *tris, int nt, 
         double r = (raw == raw && raw > 0.0f) ? (double)raw : 0.0;
         dims[k] = (uint32_t)(r < 8.0 ? 8.0 : (r > 2048.0 ? 2048.0 : r));
     }
+    if (!info) return;
     for (int k = 0; k < 20; k++) info[k] = 0.0f;
     for (int k = 0; k < 3; k++) {
         info[k] = lo[k]; info[4 + k] = hi[k]; info[8 + k] = 1.0f / size[k]; info[12 + k] = -lo[k] / size[k];
     }
     info[7] = (float)dims[0]; info[16] = friction; info[17] = thickness; info[18] = restitution;
-    if (!texels) return;
-    /* triangles and unit normals (zero cross product: (0, 1, 0)) */
+}
+/* collect_mesh_bake_triangles, sdf_baker.rs:1018-1060: 12 floats per valid
+ * triangle (corners, unit normal; zero cross product: (0, 1, 0)); at least
+ * one (degenerate) entry.  *m = count. */
+static float *mesh_tris12(const float *verts, int nv, const int32_t *tris, int nt, int *m_out) {
     float *T = (float *)malloc(sizeof(float) * 12 * ((size_t)nt + 1));
     int m = 0;
     for (int t = 0; t < nt; t++) {
@@ -1797,46 +1801,203 @@ void ocl_bake_mesh_sdf(const float *verts, int nv, const int32_t *tris, int nt, 
         q[6] = c.x; q[7] = c.y; q[8] = c.z; q[9] = n.x; q[10] = n.y; q[11] = n.z;
     }
     if (m == 0) { memset(T, 0, 12 * sizeof(float)); T[10] = 1.0f; m = 1; }
-    uint32_t W = dims[0], H = dims[1], D = dims[2];
+    *m_out = m;
+    return T;
+}
+/* closest_point_on_triangle + sign by the normal, bake_mesh_sdf.wgsl and
+ * bake_mesh_sdf_hier_common.wgsl:30-78: squared distance, *sd = signed distance */
+static float tri_sdist(v3 p, const float *q, float *sd) {
+    v3 a = V3(q[0], q[1], q[2]), b = V3(q[3], q[4], q[5]), c = V3(q[6], q[7], q[8]);
+    v3 ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a), cp;
+    float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+    v3 bp = vsub(p, b);
+    float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+    v3 cpv = vsub(p, c);
+    float d5 = vdot(ab, cpv), d6 = vdot(ac, cpv);
+    float vc = d1 * d4 - d3 * d2, vb = d5 * d2 - d1 * d6, va = d3 * d6 - d5 * d4;
+    if (d1 <= 0.0f && d2 <= 0.0f) cp = a;
+    else if (d3 >= 0.0f && d4 <= d3) cp = b;
+    else if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) cp = vadd(a, vmul(ab, d1 / (d1 - d3)));
+    else if (d6 >= 0.0f && d5 <= d6) cp = c;
+    else if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) cp = vadd(a, vmul(ac, d2 / (d2 - d6)));
+    else if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f)
+        cp = vadd(b, vmul(vsub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
+    else {
+        float den = 1.0f / (va + vb + vc);
+        cp = vadd(vadd(a, vmul(ab, vb * den)), vmul(ac, vc * den));
+    }
+    v3 diff = vsub(p, cp);
+    float dsq = vdot(diff, diff);
+    *sd = sqrtf(dsq) * (vdot(diff, V3(q[9], q[10], q[11])) >= 0.0f ? 1.0f : -1.0f);
+    return dsq;
+}
+static inline v3 voxel_centre(const float *lo, const float *hi, uint32_t x, uint32_t y, uint32_t z, uint32_t W,
+                              uint32_t H, uint32_t D) {
     float iw = 1.0f / (float)W, ih = 1.0f / (float)H, id = 1.0f / (float)D;
+    return V3(lo[0] + ((float)x + 0.5f) * iw * (hi[0] - lo[0]), lo[1] + ((float)y + 0.5f) * ih * (hi[1] - lo[1]),
+              lo[2] + ((float)z + 0.5f) * id * (hi[2] - lo[2]));
+}
+static inline uint32_t pack_h2(float a, float b) { return (uint32_t)f2h(a) | ((uint32_t)f2h(b) << 16); }
+
+/* Single-mesh SDF of an already capped mesh (bake_mesh_sdf_gpu_ext without
+ * capping): mesh_sdf_domain / mesh_sdf_bone_info / collect_mesh_bake_triangles
+ * (sdf_baker.rs:939-1060) and bake_mesh_sdf.wgsl, every triangle of every
+ * voxel in order.  dims and info are written; texels (w x h x d) when given. */
+void ocl_bake_mesh_sdf(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
+                       float friction, float thickness, float restitution, uint32_t *dims, float *info,
+                       uint32_t *texels) {
+    float lo[3], hi[3], size[3];
+    mesh_domain(verts, nv, voxel, margin, friction, thickness, restitution, lo, hi, size, dims, info);
+    if (!texels) return;
+    int m;
+    float *T = mesh_tris12(verts, nv, tris, nt, &m);
+    uint32_t W = dims[0], H = dims[1], D = dims[2];
 #pragma omp parallel for schedule(dynamic, 4)
     for (int z = 0; z < (int)D; z++)
         for (uint32_t y = 0; y < H; y++)
             for (uint32_t x = 0; x < W; x++) {
-                v3 p = V3(lo[0] + ((float)x + 0.5f) * iw * (hi[0] - lo[0]), lo[1] + ((float)y + 0.5f) * ih * (hi[1] - lo[1]),
-                          lo[2] + ((float)z + 0.5f) * id * (hi[2] - lo[2]));
+                v3 p = voxel_centre(lo, hi, x, y, (uint32_t)z, W, H, D);
                 float md = 1e10f, best = 10.0f;
                 for (int t = 0; t < m; t++) {
-                    const float *q = T + 12 * t;
-                    v3 a = V3(q[0], q[1], q[2]), b = V3(q[3], q[4], q[5]), c = V3(q[6], q[7], q[8]);
-                    v3 ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a), cp;
-                    float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
-                    v3 bp = vsub(p, b);
-                    float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
-                    v3 cpv = vsub(p, c);
-                    float d5 = vdot(ab, cpv), d6 = vdot(ac, cpv);
-                    float vc = d1 * d4 - d3 * d2, vb = d5 * d2 - d1 * d6, va = d3 * d6 - d5 * d4;
-                    if (d1 <= 0.0f && d2 <= 0.0f) cp = a;
-                    else if (d3 >= 0.0f && d4 <= d3) cp = b;
-                    else if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) cp = vadd(a, vmul(ab, d1 / (d1 - d3)));
-                    else if (d6 >= 0.0f && d5 <= d6) cp = c;
-                    else if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) cp = vadd(a, vmul(ac, d2 / (d2 - d6)));
-                    else if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f)
-                        cp = vadd(b, vmul(vsub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
-                    else {
-                        float den = 1.0f / (va + vb + vc);
-                        cp = vadd(vadd(a, vmul(ab, vb * den)), vmul(ac, vc * den));
-                    }
-                    v3 diff = vsub(p, cp);
-                    float dsq = vdot(diff, diff);
-                    if (dsq < md) {
-                        md = dsq;
-                        best = sqrtf(dsq) * (vdot(diff, V3(q[9], q[10], q[11])) >= 0.0f ? 1.0f : -1.0f);
-                    }
+                    float sd, dsq = tri_sdist(p, T + 12 * t, &sd);
+                    if (dsq < md) { md = dsq; best = sd; }
                 }
-                texels[((size_t)z * H + y) * W + x] = (uint32_t)f2h(best) | ((uint32_t)f2h(1.0f) << 16);
+                texels[((size_t)z * H + y) * W + x] = pack_h2(best, 1.0f);
             }
     free(T);
+}
+
+/* Coarse pass of the hierarchical bake (bake_mesh_sdf_coarse_ext without
+ * capping, sdf_baker.rs:1350-1600; bake_mesh_sdf_hier_coarse_main.wgsl):
+ * domain at max(voxel x 4, 0.001); per voxel the 8 nearest triangles by an
+ * in-order insertion with strict <; dist = fp16 (signed distance of the
+ * first, 1), near8[voxel * 8 + k].  dims and *coarse_voxel always written. */
+void ocl_bake_mesh_sdf_coarse(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
+                              float thickness, uint32_t *dims, float *coarse_voxel, uint32_t *dist, uint32_t *near8) {
+    float lo[3], hi[3], size[3];
+    float cv = fmaxf(voxel * 4.0f, 0.001f);
+    *coarse_voxel = cv;
+    mesh_domain(verts, nv, cv, margin, 0.0f, thickness, 0.0f, lo, hi, size, dims, NULL);
+    if (!dist) return;
+    int m;
+    float *T = mesh_tris12(verts, nv, tris, nt, &m);
+    uint32_t W = dims[0], H = dims[1], D = dims[2];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int z = 0; z < (int)D; z++)
+        for (uint32_t y = 0; y < H; y++)
+            for (uint32_t x = 0; x < W; x++) {
+                v3 p = voxel_centre(lo, hi, x, y, (uint32_t)z, W, H, D);
+                float bsq[8], bsg[8];
+                uint32_t bid[8];
+                for (int k = 0; k < 8; k++) { bsq[k] = 1e10f; bsg[k] = 10.0f; bid[k] = 0u; }
+                for (int t = 0; t < m; t++) {
+                    float sd, dsq = tri_sdist(p, T + 12 * t, &sd);
+                    if (dsq < bsq[7]) {
+                        float isq = dsq, isg = sd;
+                        uint32_t iid = (uint32_t)t;
+                        for (int k = 0; k < 8; k++) {
+                            if (isq < bsq[k]) {
+                                float tq = bsq[k], ts = bsg[k];
+                                uint32_t ti = bid[k];
+                                bsq[k] = isq; bsg[k] = isg; bid[k] = iid;
+                                isq = tq; isg = ts; iid = ti;
+                            }
+                        }
+                    }
+                }
+                size_t flat = ((size_t)z * H + y) * W + x;
+                dist[flat] = pack_h2(bsg[0], 1.0f);
+                for (int k = 0; k < 8; k++) near8[flat * 8 + k] = bid[k];
+            }
+    free(T);
+}
+
+/* Hierarchical bake of an already capped mesh (bake_mesh_sdf_hierarchical_ext
+ * without capping, sdf_baker.rs:1625-1900; bake_mesh_sdf_hier_fine_main.wgsl).
+ * Returns 0, or 1 when the band is wider than two coarse cells (the
+ * reference's error).  dims and info written; texels when given. */
+int ocl_bake_mesh_sdf_hier(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
+                           float friction, float thickness, float restitution, uint32_t *dims, float *info,
+                           uint32_t *texels) {
+    float lo[3], hi[3], size[3];
+    mesh_domain(verts, nv, voxel, margin, friction, thickness, restitution, lo, hi, size, dims, info);
+    uint32_t cd[3];
+    float cv;
+    ocl_bake_mesh_sdf_coarse(verts, nv, tris, nt, voxel, margin, thickness, cd, &cv, NULL, NULL);
+    float h_fine = fmaxf(fmaxf(size[0] / (float)dims[0], size[1] / (float)dims[1]), size[2] / (float)dims[2]);
+    float band = 4.0f * h_fine;
+    float hcm = fminf(fminf(size[0] / (float)cd[0], size[1] / (float)cd[1]), size[2] / (float)cd[2]);
+    if (band > 2.0f * hcm) return 1;
+    if (!texels) return 0;
+    size_t ncv = (size_t)cd[0] * cd[1] * cd[2];
+    uint32_t *cdist = (uint32_t *)malloc(4 * ncv), *cnear = (uint32_t *)malloc(32 * ncv);
+    ocl_bake_mesh_sdf_coarse(verts, nv, tris, nt, voxel, margin, thickness, cd, &cv, cdist, cnear);
+    int m;
+    float *T = mesh_tris12(verts, nv, tris, nt, &m);
+    uint32_t W = dims[0], H = dims[1], D = dims[2];
+    v3 vlo = V3(lo[0], lo[1], lo[2]);
+    v3 sz = vsub(V3(hi[0], hi[1], hi[2]), vlo);
+    v3 cdf = V3((float)cd[0], (float)cd[1], (float)cd[2]);
+    v3 spacing = V3(sz.x / cdf.x, sz.y / cdf.y, sz.z / cdf.z);
+    float halfdiag = 0.5f * vlen(spacing);
+    int32_t hx = (int32_t)cd[0] - 1, hy = (int32_t)cd[1] - 1, hz = (int32_t)cd[2] - 1;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int z = 0; z < (int)D; z++)
+        for (uint32_t y = 0; y < H; y++)
+            for (uint32_t x = 0; x < W; x++) {
+                float iw = 1.0f / (float)W, ih = 1.0f / (float)H, id = 1.0f / (float)D;
+                v3 p = V3(vlo.x + ((float)x + 0.5f) * iw * sz.x, vlo.y + ((float)y + 0.5f) * ih * sz.y,
+                          vlo.z + ((float)z + 0.5f) * id * sz.z);
+                v3 rel = vsub(p, vlo);
+                int32_t px = f2i(floorf(rel.x / spacing.x)), py = f2i(floorf(rel.y / spacing.y)),
+                        pz = f2i(floorf(rel.z / spacing.z));
+                px = px < 0 ? 0 : (px > hx ? hx : px);
+                py = py < 0 ? 0 : (py > hy ? hy : py);
+                pz = pz < 0 ? 0 : (pz > hz ? hz : pz);
+                size_t flat = ((size_t)z * H + y) * W + x;
+                uint32_t pidx = ((uint32_t)pz * cd[1] + (uint32_t)py) * cd[0] + (uint32_t)px;
+                uint32_t dcp = cdist[pidx];
+                float dc = h2f((uint16_t)(dcp & 0xFFFFu));
+                if (fabsf(dc) - halfdiag >= band) { texels[flat] = dcp; continue; }
+                uint32_t bi = 0xFFFFFFFFu;
+                float bsq = 1e10f, bsg = 10.0f, ssq = 1e10f, ssg = 10.0f;
+                for (int dz = -2; dz <= 2; dz++)
+                    for (int dy = -2; dy <= 2; dy++)
+                        for (int dx = -2; dx <= 2; dx++) {
+                            int32_t cx = px + dx, cy = py + dy, cz = pz + dz;
+                            cx = cx < 0 ? 0 : (cx > hx ? hx : cx);
+                            cy = cy < 0 ? 0 : (cy > hy ? hy : cy);
+                            cz = cz < 0 ? 0 : (cz > hz ? hz : cz);
+                            size_t base = (((size_t)cz * cd[1] + (size_t)cy) * cd[0] + (size_t)cx) * 8u;
+                            for (int k = 0; k < 8; k++) {
+                                uint32_t ti = cnear[base + k];
+                                if (ti >= (uint32_t)m || ti == bi) continue;
+                                const float *q = T + 12 * (size_t)ti;
+                                v3 a = V3(q[0], q[1], q[2]), b = V3(q[3], q[4], q[5]), c = V3(q[6], q[7], q[8]);
+                                v3 tmin = vmin(a, vmin(b, c)), tmax = vmax(a, vmax(b, c));
+                                v3 dv = vadd(vmax(vsub(tmin, p), V3(0, 0, 0)), vmax(vsub(p, tmax), V3(0, 0, 0)));
+                                if (vdot(dv, dv) >= ssq) continue;
+                                float sd, dsq = tri_sdist(p, q, &sd);
+                                if (dsq < bsq) { ssq = bsq; ssg = bsg; bsq = dsq; bsg = sd; bi = ti; }
+                                else if (dsq < ssq) { ssq = dsq; ssg = sd; }
+                            }
+                        }
+                int amb = (sqrtf(ssq) - sqrtf(bsq) <= 0.0002f);
+                if (amb) {
+                    float sb = bsg >= 0.0f ? 1.0f : -1.0f, ss = ssg >= 0.0f ? 1.0f : -1.0f;
+                    amb = sb != ss;
+                }
+                if (amb) {
+                    bsq = 1e10f; bsg = 10.0f;
+                    for (int t = 0; t < m; t++) {
+                        float sd, dsq = tri_sdist(p, T + 12 * t, &sd);
+                        if (dsq < bsq) { bsq = dsq; bsg = sd; }
+                    }
+                }
+                texels[flat] = pack_h2(bsg, 1.0f);
+            }
+    free(T); free(cdist); free(cnear);
+    return 0;
 }
 
 /* params: 16 words per bone (GpuBakeParams); every triangle of the bone in order */

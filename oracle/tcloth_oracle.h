@@ -126,6 +126,11 @@ void ocl_bone_bake(int nparams, const uint32_t *params16, const float *tris16, u
 void ocl_bake_mesh_sdf(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
                        float friction, float thickness, float restitution, uint32_t *dims, float *info,
                        uint32_t *texels);
+void ocl_bake_mesh_sdf_coarse(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
+                              float thickness, uint32_t *dims, float *coarse_voxel, uint32_t *dist, uint32_t *near8);
+int ocl_bake_mesh_sdf_hier(const float *verts, int nv, const int32_t *tris, int nt, float voxel, float margin,
+                           float friction, float thickness, float restitution, uint32_t *dims, float *info,
+                           uint32_t *texels);
 void ocl_set_bone_sdf(OSim *s, uint32_t w, uint32_t h, uint32_t d, const uint32_t *atlas, int nbones,
                       const float *infos20, const float *xforms32);
 

@@ -128,6 +128,9 @@ SIGNATURES = {
     "tc_get_bone_infos": [_P, _P, C.c_size_t, C.POINTER(_U)],
     "tc_bake_bone_sdf": [_P, _U, _P, _U, _U, _P, _P, _U, _F, _F, _F, _F, _F, _F, _I, _I, C.POINTER(_P)],
     "tc_bake_mesh_sdf": [_P, _U, _P, _U, _F, _F, _F, _F, _F, _I, _I, C.POINTER(_P)],
+    "tc_bake_mesh_sdf_hierarchical": [_P, _U, _P, _U, _F, _F, _F, _F, _F, _I, _I, C.POINTER(_P)],
+    "tc_bake_mesh_sdf_coarse": [_P, _U, _P, _U, _F, _F, _F, _F, _F, _I, C.POINTER(_P)],
+    "tc_bake_get_nearest": [_P, _P, C.POINTER(_F)],
     "tc_bake_dims": [_P, _P],
     "tc_bake_get": [_P, _P, _P, _P, _P],
     "tc_bake_destroy": [_P],

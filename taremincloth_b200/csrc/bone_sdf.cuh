@@ -368,6 +368,111 @@ __global__ void __launch_bounds__(256) k_mesh_bake(MeshBakeParams P, const BakeT
   out[(size_t(vz) * P.h + vy) * P.w + vx] = pack_half2(s.best_signed, 1.0f);
 }
 
+// Point-triangle closest point of bake_mesh_sdf_hier_common.wgsl:30-78 (the
+// legacy bake's formula): squared distance and the distance signed by the
+// triangle normal.
+__device__ __forceinline__ float mesh_tri_dist(V3 p, const BakeTri& tri, float& signed_d) {
+  const V3 a = mk(tri.p0w0), b = mk(tri.p1w1), c = mk(tri.p2w2);
+  const V3 ab = b - a, ac = c - a, ap = p - a;
+  const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+  V3 cp;
+  if (d1 <= 0.f && d2 <= 0.f) {
+    cp = a;
+  } else {
+    const V3 bp = p - b;
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    const float vc = d1 * d4 - d3 * d2;
+    if (d3 >= 0.f && d4 <= d3) {
+      cp = b;
+    } else if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+      cp = a + ab * (d1 / (d1 - d3));
+    } else {
+      const V3 cpv = p - c;
+      const float d5 = dot(ab, cpv), d6 = dot(ac, cpv);
+      const float vb = d5 * d2 - d1 * d6;
+      const float va = d3 * d6 - d5 * d4;
+      if (d6 >= 0.f && d5 <= d6) {
+        cp = c;
+      } else if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+        cp = a + ac * (d2 / (d2 - d6));
+      } else if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
+        cp = b + (c - b) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)));
+      } else {
+        const float denom = 1.0f / ((va + vb) + vc);
+        cp = (a + ab * (vb * denom)) + ac * (vc * denom);
+      }
+    }
+  }
+  const V3 diff = p - cp;
+  const float d_sq = dot(diff, diff);
+  signed_d = sqrtf(d_sq) * (dot(diff, mk(tri.n_bmask)) >= 0.0f ? 1.0f : -1.0f);
+  return d_sq;
+}
+
+// ---- hierarchical bake pass 1, the coarse grid
+// (bake_mesh_sdf_hier_coarse_main.wgsl; sdf_baker.rs:1328-1600): per coarse
+// voxel the 8 nearest triangles by an in-order insertion with strict <
+// (equal distances keep the earlier triangle), the signed distance of the
+// first packed as fp16 (distance, 1), the 8 indices at voxel * 8 + k.
+// Voxels are linear (z, y, x).  The brick layout and sphere culling of
+// k_mesh_bake skip a triangle only when no point of its sphere can come
+// under the 8th distance, which the insertion needs.
+__global__ void __launch_bounds__(256) k_mesh_bake_coarse(MeshBakeParams P, const BakeTri* __restrict__ tris,
+                                                          const float4* __restrict__ sph,
+                                                          const float4* __restrict__ tsph,
+                                                          uint32_t* __restrict__ dist, uint32_t* __restrict__ near8) {
+  const uint32_t bx = (P.w + 7) / 8, by = (P.h + 7) / 8;
+  const uint32_t blk = blockIdx.x;
+  const uint32_t ox = (blk % bx) * 8, oy = ((blk / bx) % by) * 8, oz = (blk / (bx * by)) * 4;
+  if (oz >= P.d) return;  // whole block
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t vx = ox + (warp & 1) * 4 + (lane & 3);
+  const uint32_t vy = oy + ((warp >> 1) & 1) * 4 + ((lane >> 2) & 3);
+  const uint32_t vz = oz + (warp >> 2) * 2 + (lane >> 4);
+  const bool valid = vx < P.w && vy < P.h && vz < P.d;
+  const V3 inv = mk(1.0f / float(P.w), 1.0f / float(P.h), 1.0f / float(P.d));
+  const V3 uvw = mk((float(vx) + 0.5f) * inv.x, (float(vy) + 0.5f) * inv.y, (float(vz) + 0.5f) * inv.z);
+  const V3 p = mk(P.lmin[0] + uvw.x * (P.lmax[0] - P.lmin[0]), P.lmin[1] + uvw.y * (P.lmax[1] - P.lmin[1]),
+                  P.lmin[2] + uvw.z * (P.lmax[2] - P.lmin[2]));
+  float bsq[8], bsg[8];
+  uint32_t bid[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) { bsq[k] = 1e10f; bsg[k] = 10.0f; bid[k] = 0u; }
+  BakeState s{1e10f, -1.0f, 10.0f, 1.0f, bake_reach(1e10f)};
+  for (uint32_t k = 0; k * 32u < P.ntri; ++k) {
+    const bool skip_tile = !valid || bake_far(s, p, __ldg(tsph + k));
+    if (__all_sync(0xffffffffu, skip_tile)) continue;
+    const uint32_t e = min(32u, P.ntri - k * 32u);
+    for (uint32_t q = 0; q < e; ++q) {
+      const uint32_t t = k * 32u + q;
+      if (skip_tile || bake_far(s, p, __ldg(sph + t))) continue;
+      const BakeTri tri{__ldg(&tris[t].p0w0), __ldg(&tris[t].p1w1), __ldg(&tris[t].p2w2), __ldg(&tris[t].n_bmask)};
+      float sd;
+      const float dsq = mesh_tri_dist(p, tri, sd);
+      if (dsq < bsq[7]) {
+        float isq = dsq, isg = sd;
+        uint32_t iid = t;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (isq < bsq[j]) {
+            const float tq = bsq[j], ts = bsg[j];
+            const uint32_t ti = bid[j];
+            bsq[j] = isq; bsg[j] = isg; bid[j] = iid;
+            isq = tq; isg = ts; iid = ti;
+          }
+        }
+        s.min_d2 = bsq[7];
+        s.reach = bake_reach(bsq[7]);
+      }
+    }
+  }
+  if (!valid) return;
+  const size_t flat = (size_t(vz) * P.h + vy) * P.w + vx;
+  dist[flat] = pack_half2(bsg[0], 1.0f);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) near8[flat * 8 + k] = bid[k];
+}
+
 // ---- sampling: trilinear, clamp to edge, texel centres at (i + 0.5) / size
 __device__ __forceinline__ float2 unpack_half2(uint32_t u) {
   return make_float2(__half2float(__ushort_as_half((unsigned short)(u & 0xFFFFu))),
@@ -488,6 +593,93 @@ __device__ __noinline__ bool bone_sdf_contact(const BoneSdfArgs& a, V3 p, float 
     return true;
   }
   return false;
+}
+
+// ---- hierarchical bake pass 2, the fine grid
+// (bake_mesh_sdf_hier_fine_main.wgsl; sdf_baker.rs:1603-1900): a fine voxel
+// whose parent coarse cell is at least band + half a cell diagonal from the
+// surface copies the parent's packed value; else the candidates are the
+// 8 nearest triangles of the 5 x 5 x 5 coarse cells around the parent
+// (clamped), visited z, y, x, with an AABB lower bound that skips a triangle
+// unable to enter the running top 2; when the top 2 lie within 0.2 mm with
+// opposite signs the voxel is rescanned over every triangle in order.
+struct HierFineParams {
+  uint32_t cw, ch, cd;
+  float band;
+};
+__device__ __forceinline__ void hier_eval(V3 p, const BakeTri* __restrict__ tris, uint32_t ntri, uint32_t ti,
+                                          uint32_t& best_i, float& best_sq, float& best_sg, float& sec_sq,
+                                          float& sec_sg) {
+  if (ti >= ntri || ti == best_i) return;
+  const BakeTri tri{__ldg(&tris[ti].p0w0), __ldg(&tris[ti].p1w1), __ldg(&tris[ti].p2w2), __ldg(&tris[ti].n_bmask)};
+  const V3 a = mk(tri.p0w0), b = mk(tri.p1w1), c = mk(tri.p2w2);
+  const V3 tmin = vmin(a, vmin(b, c)), tmax = vmax(a, vmax(b, c));
+  const V3 z = mk(0.0f, 0.0f, 0.0f);
+  const V3 dv = vmax(tmin - p, z) + vmax(p - tmax, z);
+  if (dot(dv, dv) >= sec_sq) return;
+  float sd;
+  const float dsq = mesh_tri_dist(p, tri, sd);
+  if (dsq < best_sq) {
+    sec_sq = best_sq; sec_sg = best_sg;
+    best_sq = dsq; best_sg = sd; best_i = ti;
+  } else if (dsq < sec_sq) {
+    sec_sq = dsq; sec_sg = sd;
+  }
+}
+__global__ void __launch_bounds__(128) k_mesh_bake_fine(MeshBakeParams P, HierFineParams H,
+                                                        const BakeTri* __restrict__ tris,
+                                                        const uint32_t* __restrict__ cdist,
+                                                        const uint32_t* __restrict__ cnear, uint32_t* __restrict__ out) {
+  const size_t flat = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t nvox = size_t(P.w) * P.h * P.d;
+  if (flat >= nvox) return;
+  const uint32_t vx = uint32_t(flat % P.w), vy = uint32_t((flat / P.w) % P.h), vz = uint32_t(flat / (size_t(P.w) * P.h));
+  const V3 lmin = mk(P.lmin[0], P.lmin[1], P.lmin[2]);
+  const V3 size = mk(P.lmax[0], P.lmax[1], P.lmax[2]) - lmin;
+  const V3 inv = mk(1.0f / float(P.w), 1.0f / float(P.h), 1.0f / float(P.d));
+  const V3 uvw = mk((float(vx) + 0.5f) * inv.x, (float(vy) + 0.5f) * inv.y, (float(vz) + 0.5f) * inv.z);
+  const V3 p = mk(lmin.x + uvw.x * size.x, lmin.y + uvw.y * size.y, lmin.z + uvw.z * size.z);
+  const V3 cdf = mk(float(H.cw), float(H.ch), float(H.cd));
+  const V3 spacing = mk(size.x / cdf.x, size.y / cdf.y, size.z / cdf.z);
+  const float halfdiag = 0.5f * length(spacing);
+  const V3 rel = p - lmin;
+  const int32_t hx = f2i(cdf.x) - 1, hy = f2i(cdf.y) - 1, hz = f2i(cdf.z) - 1;
+  const int32_t px = min(max(f2i(floorf(rel.x / spacing.x)), 0), hx);
+  const int32_t py = min(max(f2i(floorf(rel.y / spacing.y)), 0), hy);
+  const int32_t pz = min(max(f2i(floorf(rel.z / spacing.z)), 0), hz);
+  const uint32_t pidx = (uint32_t(pz) * H.ch + uint32_t(py)) * H.cw + uint32_t(px);
+  const uint32_t dc_packed = cdist[pidx];
+  const float dc = unpack_half2(dc_packed).x;
+  if (fabsf(dc) - halfdiag >= H.band) {
+    out[flat] = dc_packed;
+    return;
+  }
+  uint32_t best_i = 0xFFFFFFFFu;
+  float best_sq = 1e10f, best_sg = 10.0f, sec_sq = 1e10f, sec_sg = 10.0f;
+  for (int dz = -2; dz <= 2; ++dz)
+    for (int dy = -2; dy <= 2; ++dy)
+      for (int dx = -2; dx <= 2; ++dx) {
+        const int32_t cx = min(max(px + dx, 0), hx), cy = min(max(py + dy, 0), hy), cz = min(max(pz + dz, 0), hz);
+        const size_t base = (size_t(uint32_t(cz) * H.ch + uint32_t(cy)) * H.cw + uint32_t(cx)) * 8u;
+        for (uint32_t k = 0; k < 8u; ++k)
+          hier_eval(p, tris, P.ntri, __ldg(cnear + base + k), best_i, best_sq, best_sg, sec_sq, sec_sg);
+      }
+  bool amb = (sqrtf(sec_sq) - sqrtf(best_sq) <= 0.0002f);
+  if (amb) {
+    const float sb = best_sg >= 0.0f ? 1.0f : -1.0f, ss = sec_sg >= 0.0f ? 1.0f : -1.0f;
+    amb = sb != ss;
+  }
+  if (amb) {
+    best_sq = 1e10f;
+    best_sg = 10.0f;
+    for (uint32_t t = 0; t < P.ntri; ++t) {
+      const BakeTri tri{__ldg(&tris[t].p0w0), __ldg(&tris[t].p1w1), __ldg(&tris[t].p2w2), __ldg(&tris[t].n_bmask)};
+      float sd;
+      const float dsq = mesh_tri_dist(p, tri, sd);
+      if (dsq < best_sq) { best_sq = dsq; best_sg = sd; }
+    }
+  }
+  out[flat] = pack_half2(best_sg, 1.0f);
 }
 
 }  // namespace tcloth

@@ -3304,6 +3304,8 @@ struct tc_bake {
   std::vector<float> infos;        // n_active x 20
   std::vector<uint32_t> active;    // source bone index per active bone
   std::vector<float> bind;         // n_active x 16 (row-major, as given)
+  std::vector<uint32_t> nearest;   // coarse bake: 8 nearest triangles per voxel
+  float coarse_voxel = 0.f;
 };
 
 namespace {
@@ -3582,6 +3584,112 @@ tc_status tc_bake_bone_sdf(const float* mesh_verts, uint32_t nv, const int32_t* 
 
 // bake_mesh_sdf_gpu (lib.rs:1349-1416; sdf_baker.rs:939-1060, :1114-1326):
 // the signed distance field of one mesh over its padded bounding box.
+namespace {
+// The host half of every single-mesh bake: mesh_sdf_domain (sdf_baker.rs:939-982),
+// mesh_sdf_bone_info (:984-1016) and collect_mesh_bake_triangles (:1018-1060).
+struct MeshBakeSetup {
+  float lo[3], hi[3], size[3];
+  uint32_t dim[3];
+  std::vector<float> infos;
+  std::vector<tcloth::BakeTri> tris;
+};
+MeshBakeSetup mesh_bake_setup(const std::vector<float>& verts, const std::vector<int32_t>& tris, float voxel_size,
+                              float margin, float friction, float thickness, float restitution) {
+  MeshBakeSetup S;
+  const size_t NV = verts.size() / 3, NT = tris.size() / 3;
+  for (int k = 0; k < 3; ++k) { S.lo[k] = INFINITY; S.hi[k] = -INFINITY; }
+  for (size_t v = 0; v < NV; ++v)
+    for (int k = 0; k < 3; ++k) { S.lo[k] = std::fmin(S.lo[k], verts[3 * v + k]); S.hi[k] = std::fmax(S.hi[k], verts[3 * v + k]); }
+  const float vs = std::fmax(voxel_size, 0.001f);
+  for (int k = 0; k < 3; ++k) {
+    S.size[k] = std::fmax(S.hi[k] - S.lo[k], 0.05f);
+    const float pad = (std::fmax(S.size[k] * margin, 0.04f) + std::fmax(thickness, 0.f)) + 0.02f;
+    S.lo[k] -= pad;
+    S.hi[k] += pad;
+    S.size[k] = S.hi[k] - S.lo[k];
+    const float raw = std::ceil(S.size[k] / vs);
+    const double r = (raw == raw && raw > 0.f) ? double(raw) : 0.0;
+    S.dim[k] = uint32_t(std::min(std::max(r, 8.0), 2048.0));
+  }
+  S.infos.assign(20, 0.f);
+  for (int k = 0; k < 3; ++k) {
+    S.infos[k] = S.lo[k];
+    S.infos[4 + k] = S.hi[k];
+    S.infos[8 + k] = 1.0f / S.size[k];
+    S.infos[12 + k] = -S.lo[k] / S.size[k];
+  }
+  S.infos[7] = float(S.dim[0]);
+  S.infos[16] = friction; S.infos[17] = thickness; S.infos[18] = restitution;
+  for (size_t t = 0; t < NT; ++t) {
+    const int32_t i0 = tris[3 * t], i1 = tris[3 * t + 1], i2 = tris[3 * t + 2];
+    if (i0 < 0 || i1 < 0 || i2 < 0 || size_t(i0) >= NV || size_t(i1) >= NV || size_t(i2) >= NV) continue;
+    const float* p0 = &verts[3 * size_t(i0)];
+    const float* p1 = &verts[3 * size_t(i1)];
+    const float* p2 = &verts[3 * size_t(i2)];
+    const float e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    const float e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+    const float c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    const float l2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+    float nrm[3] = {0.f, 1.f, 0.f};
+    if (l2 > 1e-12f) {
+      const float il = 1.0f / std::sqrt(l2);
+      nrm[0] = c[0] * il; nrm[1] = c[1] * il; nrm[2] = c[2] * il;
+    }
+    S.tris.push_back(tcloth::BakeTri{make_float4(p0[0], p0[1], p0[2], 0.f), make_float4(p1[0], p1[1], p1[2], 0.f),
+                                     make_float4(p2[0], p2[1], p2[2], 0.f), make_float4(nrm[0], nrm[1], nrm[2], 0.f)});
+  }
+  if (S.tris.empty())
+    S.tris.push_back(tcloth::BakeTri{make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
+                                     make_float4(0, 1, 0, 0)});
+  return S;
+}
+// triangles on the device with their culling spheres (one tile run)
+void mesh_bake_upload(const MeshBakeSetup& S, tcloth::BakeGpu& G, cudaStream_t st) {
+  G.nt = uint32_t(S.tris.size());
+  G.tris.upload(S.tris, st);
+  G.setup_tiles(tcloth::make_bake_tiles({0u}, {G.nt}), st);
+  tcloth::k_bone_tri_spheres<<<(G.nt + 255) / 256, 256, 0, st>>>(G.nt, G.tris.p, G.sph.p);
+  tcloth::k_bone_tile_spheres<<<(G.ntiles + 127) / 128, 128, 0, st>>>(G.ntiles, G.tile_first.p, G.tile_cnt.p, G.sph.p,
+                                                                       G.tsph.p);
+}
+tcloth::MeshBakeParams mesh_bake_params(const MeshBakeSetup& S, uint32_t ntri) {
+  return tcloth::MeshBakeParams{{S.lo[0], S.lo[1], S.lo[2]}, {S.hi[0], S.hi[1], S.hi[2]}, S.dim[0], S.dim[1], S.dim[2],
+                                ntri};
+}
+uint32_t brick_blocks(const uint32_t dim[3]) {
+  return ((dim[0] + 7) / 8) * ((dim[1] + 7) / 8) * ((dim[2] + 3) / 4);
+}
+struct OwnStream {
+  cudaStream_t s = nullptr;
+  explicit OwnStream(int device) {
+    TC_CK(cudaSetDevice(device));
+    TC_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  }
+  ~OwnStream() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+};
+// the coarse pass (bake_mesh_sdf_coarse_ext, sdf_baker.rs:1350-1600): domain
+// at max(voxel x 4, 0.001), packed distance and the 8 nearest triangles per
+// coarse voxel; device buffers are left in G / dist / near8 for the fine pass
+struct CoarseBake {
+  MeshBakeSetup S;
+  float coarse_voxel = 0.f;
+  tcloth::BakeGpu G;
+  tcloth::DBuf<uint32_t> dist, near8;
+};
+void coarse_bake(const std::vector<float>& verts, const std::vector<int32_t>& tris, float voxel_size, float margin,
+                 float friction, float thickness, float restitution, CoarseBake& C, cudaStream_t st) {
+  C.coarse_voxel = std::fmax(voxel_size * 4.0f, 0.001f);
+  C.S = mesh_bake_setup(verts, tris, C.coarse_voxel, margin, friction, thickness, restitution);
+  mesh_bake_upload(C.S, C.G, st);
+  const size_t nvox = size_t(C.S.dim[0]) * C.S.dim[1] * C.S.dim[2];
+  C.dist.alloc(nvox);
+  C.near8.alloc(nvox * 8);
+  tcloth::k_mesh_bake_coarse<<<brick_blocks(C.S.dim), 256, 0, st>>>(mesh_bake_params(C.S, C.G.nt), C.G.tris.p,
+                                                                    C.G.sph.p, C.G.tsph.p, C.dist.p, C.near8.p);
+  TC_CK(cudaGetLastError());
+}
+}  // namespace
+
 tc_status tc_bake_mesh_sdf(const float* mesh_verts, uint32_t nv, const int32_t* mesh_tris, uint32_t nt,
                            float voxel_size, float margin, float friction, float thickness, float restitution,
                            int close_open_boundaries, int device, tc_bake** out) {
@@ -3594,81 +3702,106 @@ tc_status tc_bake_mesh_sdf(const float* mesh_verts, uint32_t nv, const int32_t* 
     std::vector<int32_t> tris(mesh_tris, mesh_tris + 3 * size_t(nt));
     std::vector<std::vector<float>> no_weights;
     if (close_open_boundaries) close_open_loops(verts, tris, no_weights);
-    const size_t NV = verts.size() / 3, NT = tris.size() / 3;
-    // mesh_sdf_domain (sdf_baker.rs:939-982)
-    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (size_t v = 0; v < NV; ++v)
-      for (int k = 0; k < 3; ++k) { lo[k] = std::fmin(lo[k], verts[3 * v + k]); hi[k] = std::fmax(hi[k], verts[3 * v + k]); }
-    float size[3];
-    uint32_t dim[3];
-    const float vs = std::fmax(voxel_size, 0.001f);
-    for (int k = 0; k < 3; ++k) {
-      size[k] = std::fmax(hi[k] - lo[k], 0.05f);
-      const float pad = (std::fmax(size[k] * margin, 0.04f) + std::fmax(thickness, 0.f)) + 0.02f;
-      lo[k] -= pad;
-      hi[k] += pad;
-      size[k] = hi[k] - lo[k];
-      const float raw = std::ceil(size[k] / vs);
-      const double r = (raw == raw && raw > 0.f) ? double(raw) : 0.0;
-      dim[k] = uint32_t(std::min(std::max(r, 8.0), 2048.0));
-    }
+    const MeshBakeSetup S = mesh_bake_setup(verts, tris, voxel_size, margin, friction, thickness, restitution);
     std::unique_ptr<tc_bake> R(new tc_bake);
-    R->w = dim[0]; R->h = dim[1]; R->d = dim[2];
-    // mesh_sdf_bone_info (sdf_baker.rs:984-1016)
-    R->infos.assign(20, 0.f);
-    for (int k = 0; k < 3; ++k) {
-      R->infos[k] = lo[k];
-      R->infos[4 + k] = hi[k];
-      R->infos[8 + k] = 1.0f / size[k];
-      R->infos[12 + k] = -lo[k] / size[k];
-    }
-    R->infos[7] = float(dim[0]);
-    R->infos[16] = friction; R->infos[17] = thickness; R->infos[18] = restitution;
-    // collect_mesh_bake_triangles (sdf_baker.rs:1018-1060)
-    std::vector<tcloth::BakeTri> all;
-    for (size_t t = 0; t < NT; ++t) {
-      const int32_t i0 = tris[3 * t], i1 = tris[3 * t + 1], i2 = tris[3 * t + 2];
-      if (i0 < 0 || i1 < 0 || i2 < 0 || size_t(i0) >= NV || size_t(i1) >= NV || size_t(i2) >= NV) continue;
-      const float* p0 = &verts[3 * size_t(i0)];
-      const float* p1 = &verts[3 * size_t(i1)];
-      const float* p2 = &verts[3 * size_t(i2)];
-      const float e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
-      const float e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
-      const float c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-      const float l2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
-      float nrm[3] = {0.f, 1.f, 0.f};
-      if (l2 > 1e-12f) {
-        const float il = 1.0f / std::sqrt(l2);
-        nrm[0] = c[0] * il; nrm[1] = c[1] * il; nrm[2] = c[2] * il;
-      }
-      all.push_back(tcloth::BakeTri{make_float4(p0[0], p0[1], p0[2], 0.f), make_float4(p1[0], p1[1], p1[2], 0.f),
-                                    make_float4(p2[0], p2[1], p2[2], 0.f), make_float4(nrm[0], nrm[1], nrm[2], 0.f)});
-    }
-    if (all.empty())
-      all.push_back(tcloth::BakeTri{make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
-                                    make_float4(0, 1, 0, 0)});
-    TC_CK(cudaSetDevice(device));
-    cudaStream_t st = nullptr;
-    TC_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); } } sg{st};
+    R->w = S.dim[0]; R->h = S.dim[1]; R->d = S.dim[2];
+    R->infos = S.infos;
+    OwnStream os(device);
     tcloth::BakeGpu G;
-    G.nt = uint32_t(all.size());
-    G.tris.upload(all, st);
-    G.setup_tiles(tcloth::make_bake_tiles({0u}, {G.nt}), st);
-    tcloth::k_bone_tri_spheres<<<(G.nt + 255) / 256, 256, 0, st>>>(G.nt, G.tris.p, G.sph.p);
-    tcloth::k_bone_tile_spheres<<<(G.ntiles + 127) / 128, 128, 0, st>>>(G.ntiles, G.tile_first.p, G.tile_cnt.p,
-                                                                         G.sph.p, G.tsph.p);
-    tcloth::MeshBakeParams P{{lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}, dim[0], dim[1], dim[2], G.nt};
-    const size_t nvox = size_t(dim[0]) * dim[1] * dim[2];
+    mesh_bake_upload(S, G, os.s);
+    const size_t nvox = size_t(S.dim[0]) * S.dim[1] * S.dim[2];
     tcloth::DBuf<uint32_t> vox;
     vox.alloc(nvox);
-    const uint32_t nblk = ((dim[0] + 7) / 8) * ((dim[1] + 7) / 8) * ((dim[2] + 3) / 4);
-    tcloth::k_mesh_bake<<<nblk, 256, 0, st>>>(P, G.tris.p, G.sph.p, G.tsph.p, vox.p);
+    tcloth::k_mesh_bake<<<brick_blocks(S.dim), 256, 0, os.s>>>(mesh_bake_params(S, G.nt), G.tris.p, G.sph.p, G.tsph.p,
+                                                                vox.p);
     R->texels.resize(nvox);
-    TC_CK(cudaMemcpyAsync(R->texels.data(), vox.p, nvox * 4, cudaMemcpyDeviceToHost, st));
-    TC_CK(cudaStreamSynchronize(st));
+    TC_CK(cudaMemcpyAsync(R->texels.data(), vox.p, nvox * 4, cudaMemcpyDeviceToHost, os.s));
+    TC_CK(cudaStreamSynchronize(os.s));
     TC_CK(cudaGetLastError());
     *out = R.release();
+  });
+}
+
+tc_status tc_bake_mesh_sdf_coarse(const float* mesh_verts, uint32_t nv, const int32_t* mesh_tris, uint32_t nt,
+                                  float voxel_size, float margin, float friction, float thickness, float restitution,
+                                  int device, tc_bake** out) {
+  return guard([&] {
+    need(out != nullptr, "out required");
+    *out = nullptr;
+    if (nv == 0) throw TcError(TC_ERR_CUDA, "GPU coarse-grid bake failed: the mesh has no vertices");
+    need(mesh_verts != nullptr && (nt == 0 || mesh_tris != nullptr), "arrays required");
+    std::vector<float> verts(mesh_verts, mesh_verts + 3 * size_t(nv));
+    std::vector<int32_t> tris(mesh_tris, mesh_tris + 3 * size_t(nt));
+    std::vector<std::vector<float>> no_weights;
+    close_open_loops(verts, tris, no_weights);  // bake_mesh_sdf_coarse always caps
+    OwnStream os(device);
+    CoarseBake C;
+    coarse_bake(verts, tris, voxel_size, margin, friction, thickness, restitution, C, os.s);
+    std::unique_ptr<tc_bake> R(new tc_bake);
+    R->w = C.S.dim[0]; R->h = C.S.dim[1]; R->d = C.S.dim[2];
+    R->infos = C.S.infos;
+    R->coarse_voxel = C.coarse_voxel;
+    const size_t nvox = size_t(R->w) * R->h * R->d;
+    R->texels.resize(nvox);
+    R->nearest.resize(nvox * 8);
+    TC_CK(cudaMemcpyAsync(R->texels.data(), C.dist.p, nvox * 4, cudaMemcpyDeviceToHost, os.s));
+    TC_CK(cudaMemcpyAsync(R->nearest.data(), C.near8.p, nvox * 32, cudaMemcpyDeviceToHost, os.s));
+    TC_CK(cudaStreamSynchronize(os.s));
+    TC_CK(cudaGetLastError());
+    *out = R.release();
+  });
+}
+
+tc_status tc_bake_mesh_sdf_hierarchical(const float* mesh_verts, uint32_t nv, const int32_t* mesh_tris, uint32_t nt,
+                                        float voxel_size, float margin, float friction, float thickness,
+                                        float restitution, int close_open_boundaries, int device, tc_bake** out) {
+  return guard([&] {
+    need(out != nullptr, "out required");
+    *out = nullptr;
+    if (nv == 0) throw TcError(TC_ERR_CUDA, "GPU hierarchical mesh SDF bake failed: the mesh has no vertices");
+    need(mesh_verts != nullptr && (nt == 0 || mesh_tris != nullptr), "arrays required");
+    std::vector<float> verts(mesh_verts, mesh_verts + 3 * size_t(nv));
+    std::vector<int32_t> tris(mesh_tris, mesh_tris + 3 * size_t(nt));
+    std::vector<std::vector<float>> no_weights;
+    if (close_open_boundaries) close_open_loops(verts, tris, no_weights);
+    const MeshBakeSetup S = mesh_bake_setup(verts, tris, voxel_size, margin, friction, thickness, restitution);
+    OwnStream os(device);
+    CoarseBake C;
+    coarse_bake(verts, tris, voxel_size, margin, friction, thickness, restitution, C, os.s);
+    // band = 4 fine voxels, at most two coarse cells (sdf_baker.rs:1655-1667)
+    const float h_fine = std::fmax(std::fmax(S.size[0] / float(S.dim[0]), S.size[1] / float(S.dim[1])),
+                                   S.size[2] / float(S.dim[2]));
+    const float band = 4.0f * h_fine;
+    const float h_coarse_min = std::fmin(std::fmin(S.size[0] / float(C.S.dim[0]), S.size[1] / float(C.S.dim[1])),
+                                         S.size[2] / float(C.S.dim[2]));
+    if (band > 2.0f * h_coarse_min) {
+      char msg[160];
+      std::snprintf(msg, sizeof msg, "GPU hierarchical mesh SDF bake failed: band (%.4f m) too wide for the coarse "
+                    "cell (%.4f m)", band, h_coarse_min);
+      throw TcError(TC_ERR_CUDA, msg);
+    }
+    std::unique_ptr<tc_bake> R(new tc_bake);
+    R->w = S.dim[0]; R->h = S.dim[1]; R->d = S.dim[2];
+    R->infos = S.infos;
+    const size_t nvox = size_t(S.dim[0]) * S.dim[1] * S.dim[2];
+    tcloth::DBuf<uint32_t> vox;
+    vox.alloc(nvox);
+    const tcloth::HierFineParams H{C.S.dim[0], C.S.dim[1], C.S.dim[2], band};
+    tcloth::k_mesh_bake_fine<<<unsigned((nvox + 127) / 128), 128, 0, os.s>>>(mesh_bake_params(S, C.G.nt), H,
+                                                                            C.G.tris.p, C.dist.p, C.near8.p, vox.p);
+    R->texels.resize(nvox);
+    TC_CK(cudaMemcpyAsync(R->texels.data(), vox.p, nvox * 4, cudaMemcpyDeviceToHost, os.s));
+    TC_CK(cudaStreamSynchronize(os.s));
+    TC_CK(cudaGetLastError());
+    *out = R.release();
+  });
+}
+
+tc_status tc_bake_get_nearest(tc_bake* b, uint32_t* nearest, float* coarse_voxel) {
+  return guard([&] {
+    need(b != nullptr, "bake result required");
+    if (nearest) std::memcpy(nearest, b->nearest.data(), b->nearest.size() * 4);
+    if (coarse_voxel) *coarse_voxel = b->coarse_voxel;
   });
 }
 

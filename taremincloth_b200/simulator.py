@@ -110,6 +110,63 @@ def bake_mesh_sdf_gpu(mesh_verts, mesh_tris, voxel_size=0.004, margin=0.02, fric
     return {"texture_bytes": tex.tobytes(), "width": W, "height": H, "depth": D, "bone_info": info}
 
 
+def _mesh_arrays(mesh_verts, mesh_tris):
+    v = np.ascontiguousarray(np.asarray(mesh_verts, _f32))
+    if v.ndim != 2 or v.shape[1] < 3:
+        raise ValueError("mesh_verts must have shape (N, 3)")
+    t = np.ascontiguousarray(np.asarray(mesh_tris, np.int32))
+    if t.ndim != 2 or t.shape[1] < 3:
+        raise ValueError("mesh_tris must have shape (M, 3)")
+    return np.ascontiguousarray(v[:, :3]), np.ascontiguousarray(t[:, :3])
+
+
+def bake_mesh_sdf_hierarchical_gpu(mesh_verts, mesh_tris, voxel_size=0.004, margin=0.02, friction=0.5,
+                                   thickness=0.005, restitution=0.0, close_open_boundaries=True, device=0):
+    """Two-pass (coarse grid, then fine grid) mesh SDF (lib.rs:1418-1488).
+    Returns dict(texture_bytes, width, height, depth, bone_info (20,))."""
+    v, t = _mesh_arrays(mesh_verts, mesh_tris)
+    L = _lib.load()
+    h = C.c_void_p()
+    _lib.check(L.tc_bake_mesh_sdf_hierarchical(_ptr(v), v.shape[0], _ptr(t), t.shape[0], float(voxel_size),
+                                               float(margin), float(friction), float(thickness), float(restitution),
+                                               int(bool(close_open_boundaries)), int(device), C.byref(h)))
+    try:
+        dims = np.zeros(4, _u32)
+        _lib.check(L.tc_bake_dims(h, _ptr(dims)))
+        W, H, D = (int(x) for x in dims[:3])
+        tex = np.zeros(W * H * D, _u32)
+        info = np.zeros(20, _f32)
+        _lib.check(L.tc_bake_get(h, _ptr(tex), _ptr(info), None, None))
+    finally:
+        L.tc_bake_destroy(h)
+    return {"texture_bytes": tex.tobytes(), "width": W, "height": H, "depth": D, "bone_info": info}
+
+
+def bake_mesh_sdf_coarse_gpu(mesh_verts, mesh_tris, voxel_size=0.004, margin=0.02, friction=0.5, thickness=0.005,
+                             restitution=0.0, device=0):
+    """Coarse pass of the hierarchical bake (lib.rs:1490-1540).  Returns
+    dict(dist_packed (uint32 per coarse voxel), nearest_tri (8 per voxel),
+    width, height, depth, coarse_voxel)."""
+    v, t = _mesh_arrays(mesh_verts, mesh_tris)
+    L = _lib.load()
+    h = C.c_void_p()
+    _lib.check(L.tc_bake_mesh_sdf_coarse(_ptr(v), v.shape[0], _ptr(t), t.shape[0], float(voxel_size), float(margin),
+                                         float(friction), float(thickness), float(restitution), int(device),
+                                         C.byref(h)))
+    try:
+        dims = np.zeros(4, _u32)
+        _lib.check(L.tc_bake_dims(h, _ptr(dims)))
+        W, H, D = (int(x) for x in dims[:3])
+        dist = np.zeros(W * H * D, _u32)
+        near = np.zeros(W * H * D * 8, _u32)
+        cv = C.c_float()
+        _lib.check(L.tc_bake_get(h, _ptr(dist), None, None, None))
+        _lib.check(L.tc_bake_get_nearest(h, _ptr(near), C.byref(cv)))
+    finally:
+        L.tc_bake_destroy(h)
+    return {"dist_packed": dist, "nearest_tri": near, "width": W, "height": H, "depth": D, "coarse_voxel": cv.value}
+
+
 def is_gpu_available() -> bool:
     try:
         return bool(_lib.load().tc_gpu_available())
