@@ -82,6 +82,9 @@ tc_status tc_batch_instance_offsets(tc_sim *s, uint32_t *offsets, uint32_t max_e
  * one frame of `substeps` substeps (0 -> 20), synchronous.  The frame is
  * recorded once into a CUDA graph and replayed while parameters are unchanged. */
 tc_status tc_step(tc_sim *s, float dt, uint32_t substeps, uint32_t *effective_substeps);
+/* step_single_substep (dispatch.rs:674-688): one substep of dt_sub,
+ * synchronous, without adaptive planning or displacement feedback. */
+tc_status tc_step_single_substep(tc_sim *s, float dt_sub);
 /* step_async (dispatch.rs:740-806): enqueue a frame on the simulator's stream
  * and return; fetch_positions (lib.rs:1834-1846) waits and copies. */
 tc_status tc_step_async(tc_sim *s, float dt, uint32_t substeps);
@@ -152,6 +155,17 @@ tc_status tc_set_stiffness_all(tc_sim *s, float tension, float compression, floa
  * the reference reaches compliance only through stiffness. */
 tc_status tc_set_compliance_all(tc_sim *s, float tension, float compression, float shear, float bending);
 tc_status tc_set_edge_stiffness_multipliers(tc_sim *s, const uint32_t *edge_idx, const float *mult, uint32_t count);
+/* reset_edge_stiffness_multipliers (simulation/mod.rs:1526-1532) */
+tc_status tc_reset_edge_stiffness_multipliers(tc_sim *s);
+/* set_edge_rest_length_scales / reset_edge_rest_lengths (simulation/mod.rs:1450-1491):
+ * the distance constraint of input edge idx[i] gets rest = initial rest x
+ * max(scales[i], 0.01); edges without one are skipped. */
+tc_status tc_set_edge_rest_length_scales(tc_sim *s, const uint32_t *idx, const float *scales, uint32_t count);
+tc_status tc_reset_edge_rest_lengths(tc_sim *s);
+/* get_edge_rest_length, get_edge_initial_rest_length, get_edge_tension_compliance
+ * (simulation/mod.rs:1535-1568): out = (rest, initial rest, tension compliance)
+ * of input edge edge_idx, zeros when it has no distance constraint. */
+tc_status tc_get_edge_constraint(tc_sim *s, uint32_t edge_idx, float out[3]);
 tc_status tc_set_enable_self_collision(tc_sim *s, int enable);
 /* set_self_collision_options (simulation/mod.rs:920-950) */
 tc_status tc_set_self_collision_options(tc_sim *s, float relief_factor, float max_displacement_ratio,
@@ -311,6 +325,18 @@ tc_status tc_bake_mesh_sdf_coarse(const float *mesh_verts, uint32_t nv, const in
                                   float voxel_size, float margin, float friction, float thickness, float restitution,
                                   int device, tc_bake **out);
 tc_status tc_bake_get_nearest(tc_bake *b, uint32_t *nearest, float *coarse_voxel);
+/* compute_combined_inv_masses / compute_areal_inv_masses (mesh.rs:237-312,
+ * lib.rs:553-640), host only: a third of each valid triangle's area x
+ * areal_density to its corners and half of each strand edge's length x
+ * linear_density to its ends; out[i] = 0 for pin >= 1, else
+ * (1 - pin) / max(mass, 1e-9) with pin clamped to [0, 1] (entries past npin:
+ * 0).  faces, strand_edges and pin_weights may be NULL. */
+tc_status tc_compute_combined_inv_masses(const float *positions, uint32_t n, const uint32_t *faces, uint32_t nf,
+                                         const uint32_t *strand_edges, uint32_t ns, const float *pin_weights,
+                                         uint32_t npin, float areal_density, float linear_density, float *out);
+/* color_edge_pairs (coloring.rs:180-233, lib.rs:642-652), host only:
+ * Welsh-Powell colours of vertex pairs, order (-degree, index). */
+tc_status tc_color_edge_pairs(uint32_t num_vertices, const uint32_t *pairs, uint32_t np, uint32_t *colors);
 tc_status tc_bake_dims(tc_bake *b, uint32_t out[4]);
 /* texels (w*h*d), infos (n_active x 20), active (source bone index per
  * active bone), bind (n_active x 16); any may be NULL */
@@ -327,6 +353,10 @@ tc_status tc_get_vertex_inv_masses(tc_sim *s, float *out, uint32_t n);
 
 /* counts (lib.rs:2928-2950): out[8] = n, distance, bending, edges,
  * distance colours, bending colours, hash table size, multi-layer flag */
+/* get_num_virtual_vertices (lib.rs:2045-2048): the virtual-particle count of
+ * the mesh (pipelines.rs:170-185, capped at 150,000); the particles
+ * themselves (self-collision algorithm 2) are not built. */
+tc_status tc_get_num_virtual_vertices(tc_sim *s, uint32_t *count);
 tc_status tc_get_counts(tc_sim *s, uint32_t out[8]);
 tc_status tc_get_cell_size(tc_sim *s, float *cell);
 

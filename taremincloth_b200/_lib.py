@@ -42,6 +42,14 @@ SIGNATURES = {
     "tc_reset": [_P],
     "tc_set_gravity": [_P, _F, _F, _F],
     "tc_set_enable_edge_collision": [_P, _I],
+    "tc_compute_combined_inv_masses": [_P, _U, _P, _U, _P, _U, _P, _U, _F, _F, _P],
+    "tc_color_edge_pairs": [_U, _P, _U, _P],
+    "tc_reset_edge_stiffness_multipliers": [_P],
+    "tc_set_edge_rest_length_scales": [_P, _P, _P, _U],
+    "tc_reset_edge_rest_lengths": [_P],
+    "tc_get_edge_constraint": [_P, _U, _P],
+    "tc_step_single_substep": [_P, _F],
+    "tc_get_num_virtual_vertices": [_P, C.POINTER(_U)],
     "tc_set_enable_pair_cache": [_P, _I],
     "tc_get_enable_pair_cache": [_P, C.POINTER(_I)],
     "tc_set_self_collision_algorithm": [_P, _U],

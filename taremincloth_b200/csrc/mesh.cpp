@@ -776,4 +776,96 @@ MeshData build_mesh(const MeshInput& in) {
   return m;
 }
 
+// compute_combined_inv_masses (mesh.rs:237-312): a third of each valid
+// triangle's area x areal density to each corner, half of each strand edge's
+// length x linear density to each end, in input order; then
+// w = (1 - pin) / max(mass, 1e-9), with pin clamped to [0, 1] (missing = 0)
+// and 0 for pin >= 1.
+std::vector<float> combined_inv_masses(const float* pos, uint32_t n, const uint32_t* faces, uint32_t nf,
+                                       const uint32_t* strands, uint32_t ns, const float* pins, uint32_t npin,
+                                       float areal_density, float linear_density) {
+  std::vector<float> m(n, 0.f);
+  if (areal_density > 0.f && faces) {
+    for (uint32_t f = 0; f < nf; ++f) {
+      const uint32_t a = faces[3 * f], b = faces[3 * f + 1], c = faces[3 * f + 2];
+      if (a >= n || b >= n || c >= n || a == b || b == c || c == a) continue;
+      const float* pa = pos + 3 * size_t(a);
+      const float* pb = pos + 3 * size_t(b);
+      const float* pc = pos + 3 * size_t(c);
+      const float ab[3] = {pb[0] - pa[0], pb[1] - pa[1], pb[2] - pa[2]};
+      const float ac[3] = {pc[0] - pa[0], pc[1] - pa[1], pc[2] - pa[2]};
+      const float cr[3] = {ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2], ab[0] * ac[1] - ab[1] * ac[0]};
+      const float area = 0.5f * std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      const float share = area * areal_density / 3.0f;
+      m[a] += share;
+      m[b] += share;
+      m[c] += share;
+    }
+  }
+  if (linear_density > 0.f && strands) {
+    for (uint32_t e = 0; e < ns; ++e) {
+      const uint32_t a = strands[2 * e], b = strands[2 * e + 1];
+      if (a >= n || b >= n || a == b) continue;
+      const float* pa = pos + 3 * size_t(a);
+      const float* pb = pos + 3 * size_t(b);
+      const float dx = pa[0] - pb[0], dy = pa[1] - pb[1], dz = pa[2] - pb[2];
+      const float len = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const float share = len * linear_density / 2.0f;
+      m[a] += share;
+      m[b] += share;
+    }
+  }
+  std::vector<float> w(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    float pin = (pins && i < npin) ? pins[i] : 0.f;
+    if (!std::isnan(pin)) pin = std::min(std::max(pin, 0.f), 1.f);
+    w[i] = pin >= 1.f ? 0.f : (1.f - pin) / std::fmax(m[i], 1e-9f);
+  }
+  return w;
+}
+
+// color_edge_pairs (coloring.rs:180-233): Welsh-Powell over vertex-sharing
+// pairs, order (-degree, index), first free colour; a pair's out-of-range
+// ends register nothing.
+std::vector<uint32_t> color_edge_pairs(uint32_t nv, const uint32_t* pairs, uint32_t np) {
+  std::vector<uint32_t> color(np, 0u);
+  if (np == 0 || nv == 0) return color;
+  std::vector<uint32_t> off(size_t(nv) + 1, 0u);
+  for (uint32_t i = 0; i < np; ++i)
+    for (int k = 0; k < 2; ++k)
+      if (pairs[2 * i + k] < nv) ++off[pairs[2 * i + k] + 1];
+  for (uint32_t v = 0; v < nv; ++v) off[v + 1] += off[v];
+  std::vector<uint32_t> fill(off.begin(), off.end() - 1), v2c(off[nv]);
+  for (uint32_t i = 0; i < np; ++i)
+    for (int k = 0; k < 2; ++k)
+      if (pairs[2 * i + k] < nv) v2c[fill[pairs[2 * i + k]]++] = i;
+  auto deg = [&](uint32_t v) { return v < nv ? off[v + 1] - off[v] : 0u; };
+  std::vector<uint32_t> order(np);
+  for (uint32_t i = 0; i < np; ++i) order[i] = i;
+  std::vector<uint32_t> key(np);
+  for (uint32_t i = 0; i < np; ++i) key[i] = deg(pairs[2 * i]) + deg(pairs[2 * i + 1]);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] > key[b]; });
+  std::fill(color.begin(), color.end(), UINT32_MAX);
+  std::vector<uint32_t> used_stamp;
+  uint32_t stamp = 0;
+  for (uint32_t i : order) {
+    ++stamp;
+    for (int k = 0; k < 2; ++k) {
+      const uint32_t v = pairs[2 * i + k];
+      if (v >= nv) continue;
+      for (uint32_t q = off[v]; q < off[v + 1]; ++q) {
+        const uint32_t adj = v2c[q];
+        if (adj != i && color[adj] != UINT32_MAX) {
+          if (color[adj] >= used_stamp.size()) used_stamp.resize(size_t(color[adj]) + 1, 0u);
+          used_stamp[color[adj]] = stamp;
+        }
+      }
+    }
+    uint32_t c = 0;
+    while (c < used_stamp.size() && used_stamp[c] == stamp) ++c;
+    color[i] = c;
+  }
+  return color;
+}
+
 }  // namespace tcloth

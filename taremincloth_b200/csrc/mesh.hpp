@@ -84,5 +84,9 @@ struct MeshData {
 float stiffness_to_compliance(float k);
 MeshData build_mesh(const MeshInput& in);
 uint32_t morton3(float px, float py, float pz, const float bmin[3], const float inv[3]);
+std::vector<float> combined_inv_masses(const float* pos, uint32_t n, const uint32_t* faces, uint32_t nf,
+                                       const uint32_t* strands, uint32_t ns, const float* pins, uint32_t npin,
+                                       float areal_density, float linear_density);
+std::vector<uint32_t> color_edge_pairs(uint32_t nv, const uint32_t* pairs, uint32_t np);
 
 }  // namespace tcloth

@@ -2217,6 +2217,18 @@ tc_status tc_step(tc_sim* s, float dt, uint32_t substeps, uint32_t* eff) {
   });
 }
 
+// step_single_substep (dispatch.rs:674-688): one substep of dt_sub, no
+// adaptive planning and no displacement feedback
+tc_status tc_step_single_substep(tc_sim* s, float dt_sub) {
+  return guard([&] {
+    Sim& m = S(s);
+    m.launch_frame(dt_sub, 1);
+    TC_CK(cudaStreamSynchronize(m.st));
+    TC_CK(cudaGetLastError());
+    m.check_barrier_status();
+  });
+}
+
 tc_status tc_step_async(tc_sim* s, float dt, uint32_t substeps) {
   return guard([&] {
     Sim& m = S(s);
@@ -2528,6 +2540,58 @@ tc_status tc_set_edge_stiffness_multipliers(tc_sim* s, const uint32_t* idx, cons
     if (changed) m.apply_distance_compliances();
   });
 }
+// reset_edge_stiffness_multipliers (simulation/mod.rs:1526-1532)
+tc_status tc_reset_edge_stiffness_multipliers(tc_sim* s) {
+  return guard([&] {
+    Sim& m = S(s);
+    bool all_one = true;
+    for (float v : m.mult) all_one = all_one && std::fabs(v - 1.f) <= 1e-6f;
+    if (all_one) return;
+    std::fill(m.mult.begin(), m.mult.end(), 1.f);
+    m.apply_distance_compliances();
+  });
+}
+// set_edge_rest_length_scales / reset_edge_rest_lengths (simulation/mod.rs:1450-1491):
+// rest = initial rest x max(scale, 0.01) for each listed input edge
+tc_status tc_set_edge_rest_length_scales(tc_sim* s, const uint32_t* idx, const float* scales, uint32_t count) {
+  return guard([&] {
+    need(count == 0 || (idx != nullptr && scales != nullptr), "indices and scales required");
+    Sim& m = S(s);
+    bool changed = false;
+    for (uint32_t i = 0; i < count; ++i) {
+      const uint32_t e = idx[i];
+      if (e >= m.orig_edge_to_dist.size()) continue;
+      const int64_t ci = m.orig_edge_to_dist[e];
+      if (ci < 0 || size_t(ci) >= m.dist_h.size()) continue;
+      m.dist_h[size_t(ci)].rest = m.base_rest[size_t(ci)] * std::fmax(scales[i], 0.01f);
+      changed = true;
+    }
+    if (changed && m.nd) { m.upload_dist(); m.mark(); }
+  });
+}
+tc_status tc_reset_edge_rest_lengths(tc_sim* s) {
+  return guard([&] {
+    Sim& m = S(s);
+    for (uint32_t i = 0; i < m.nd; ++i) m.dist_h[i].rest = m.base_rest[i];
+    if (m.nd) { m.upload_dist(); m.mark(); }
+  });
+}
+// get_edge_rest_length / get_edge_initial_rest_length / get_edge_tension_compliance
+// (simulation/mod.rs:1535-1568): the distance constraint of an input edge,
+// 0 for an edge without one; out = (rest, initial rest, tension compliance)
+tc_status tc_get_edge_constraint(tc_sim* s, uint32_t edge_idx, float out[3]) {
+  return guard([&] {
+    need(out != nullptr, "out required");
+    Sim& m = S(s);
+    out[0] = out[1] = out[2] = 0.f;
+    if (edge_idx >= m.orig_edge_to_dist.size()) return;
+    const int64_t ci = m.orig_edge_to_dist[edge_idx];
+    if (ci < 0 || size_t(ci) >= m.dist_h.size()) return;
+    out[0] = m.dist_h[size_t(ci)].rest;
+    out[1] = m.base_rest[size_t(ci)];
+    out[2] = m.dist_h[size_t(ci)].tc;
+  });
+}
 tc_status tc_set_enable_self_collision(tc_sim* s, int on) {
   return guard([&] { Sim& m = S(s); m.self_collision = on != 0; m.mark(); });
 }
@@ -2729,6 +2793,9 @@ tc_status tc_get_counts(tc_sim* s, uint32_t out[8]) {
     out[4] = uint32_t(m.m.dist_cnt.size()); out[5] = uint32_t(m.m.bend_cnt.size());
     out[6] = m.m.table; out[7] = m.m.multi_layer ? 1u : 0u;
   });
+}
+tc_status tc_get_num_virtual_vertices(tc_sim* s, uint32_t* count) {
+  return guard([&] { need(count != nullptr, "count required"); *count = S(s).m.num_virtual; });
 }
 tc_status tc_get_cell_size(tc_sim* s, float* cell) {
   return guard([&] { Sim& m = S(s); *cell = m.m.cell; });
@@ -3802,6 +3869,25 @@ tc_status tc_bake_get_nearest(tc_bake* b, uint32_t* nearest, float* coarse_voxel
     need(b != nullptr, "bake result required");
     if (nearest) std::memcpy(nearest, b->nearest.data(), b->nearest.size() * 4);
     if (coarse_voxel) *coarse_voxel = b->coarse_voxel;
+  });
+}
+
+tc_status tc_compute_combined_inv_masses(const float* positions, uint32_t n, const uint32_t* faces, uint32_t nf,
+                                         const uint32_t* strand_edges, uint32_t ns, const float* pin_weights,
+                                         uint32_t npin, float areal_density, float linear_density, float* out) {
+  return guard([&] {
+    need(out != nullptr && (n == 0 || positions != nullptr), "positions and output required");
+    const std::vector<float> w = tcloth::combined_inv_masses(positions, n, faces, faces ? nf : 0u, strand_edges,
+                                                             strand_edges ? ns : 0u, pin_weights,
+                                                             pin_weights ? npin : 0u, areal_density, linear_density);
+    std::copy(w.begin(), w.end(), out);
+  });
+}
+tc_status tc_color_edge_pairs(uint32_t num_vertices, const uint32_t* pairs, uint32_t np, uint32_t* colors) {
+  return guard([&] {
+    need(np == 0 || (pairs != nullptr && colors != nullptr), "pairs and colours required");
+    const std::vector<uint32_t> c = tcloth::color_edge_pairs(num_vertices, pairs, np);
+    std::copy(c.begin(), c.end(), colors);
   });
 }
 

@@ -110,6 +110,53 @@ def bake_mesh_sdf_gpu(mesh_verts, mesh_tris, voxel_size=0.004, margin=0.02, fric
     return {"texture_bytes": tex.tobytes(), "width": W, "height": H, "depth": D, "bone_info": info}
 
 
+def _rows(a, width, dtype, name):
+    if a is None:
+        return None
+    x = np.asarray(a)
+    if x.size == 0:
+        return None
+    if x.ndim != 2 or x.shape[1] < width:
+        raise ValueError(f"{name} must have shape (M, {width})")
+    return np.ascontiguousarray(x[:, :width], dtype=dtype)
+
+
+def compute_combined_inv_masses(positions, faces=None, strand_edges=None, pin_weights=None, areal_density=0.15,
+                                linear_density=0.0):
+    """Inverse masses from areal and linear density (lib.rs:553-611, mesh.rs:237-312); host only."""
+    pos = np.asarray(positions, _f32)
+    if pos.ndim != 2 or pos.shape[1] != 3:
+        raise ValueError("each vertex of positions must have 3 coordinates")
+    pos = np.ascontiguousarray(pos)
+    f = _rows(faces, 3, _u32, "faces")
+    st = _rows(strand_edges, 2, _u32, "strand_edges")
+    pw = None if pin_weights is None else np.ascontiguousarray(np.asarray(pin_weights, _f32).reshape(-1))
+    out = np.zeros(pos.shape[0], _f32)
+    L = _lib.load()
+    _lib.check(L.tc_compute_combined_inv_masses(_ptr(pos), pos.shape[0], _ptr(f), 0 if f is None else f.shape[0],
+                                                _ptr(st), 0 if st is None else st.shape[0], _ptr(pw),
+                                                0 if pw is None else pw.size, float(areal_density),
+                                                float(linear_density), _ptr(out)))
+    return out
+
+
+def compute_areal_inv_masses(positions, faces=None, pin_weights=None, areal_density=0.15, strand_edges=None,
+                             linear_density=0.0):
+    """The same with the reference's older argument order (lib.rs:613-640)."""
+    return compute_combined_inv_masses(positions, faces, strand_edges, pin_weights, areal_density, linear_density)
+
+
+def color_edge_pairs(num_vertices, edges):
+    """Welsh-Powell colour per vertex pair (lib.rs:642-652, coloring.rs:180-233); host only."""
+    e = _rows(edges, 2, _u32, "edges")
+    if e is None:
+        return []
+    out = np.zeros(e.shape[0], _u32)
+    L = _lib.load()
+    _lib.check(L.tc_color_edge_pairs(int(num_vertices), _ptr(e), e.shape[0], _ptr(out)))
+    return [int(c) for c in out]
+
+
 def _mesh_arrays(mesh_verts, mesh_tris):
     v = np.ascontiguousarray(np.asarray(mesh_verts, _f32))
     if v.ndim != 2 or v.shape[1] < 3:
@@ -309,6 +356,48 @@ class ClothSimulator:
         out = self._out(out_array)
         self._c(self._L.tc_get_positions(self._h, _ptr(out), out.size))
 
+    # ---------------- settings the CUDA path has no use for, kept for the API
+    # (lib.rs:1898-1906, :1935-1937, :2828-2836, :2030-2060)
+    def set_workgroup_size(self, wg_size):
+        self._wg = int(wg_size)
+
+    def get_workgroup_size(self):
+        return getattr(self, "_wg", 32)
+
+    def get_solver_mode(self):
+        return 0
+
+    def set_solver_mode(self, mode):
+        if int(mode) != 0:
+            raise NotImplementedError("only the graph-coloured solver (solver_mode=0) is built")
+
+    def set_coupled_self_collision_options(self, mode, relaxation_iters=0):
+        """mode 0 (self-collision once per substep after the final pins) is the one built."""
+        if int(mode) != 0:
+            raise NotImplementedError("coupled self-collision modes 1-3 are not built")
+
+    def set_areal_density(self, density):
+        d = float(density)
+        if np.isfinite(d):
+            self._areal_density = min(max(d, 0.0), 100.0)
+
+    def set_enable_compact_readback(self, enable):
+        self._compact = bool(enable)
+
+    def get_enable_compact_readback(self):
+        return getattr(self, "_compact", False)
+
+    def get_effective_normal_untangling(self):
+        return getattr(self, "_untangle", True) and bool(self._counts()[7])
+
+    def get_num_virtual_vertices(self):
+        v = C.c_uint32()
+        self._c(self._L.tc_get_num_virtual_vertices(self._h, C.byref(v)))
+        return v.value
+
+    def step_single_substep(self, dt_sub):
+        self._c(self._L.tc_step_single_substep(self._h, float(dt_sub)))
+
     # ---------------- contact-pair cache (lib.rs:2029-2105)
     def set_enable_pair_cache(self, enable):
         self._c(self._L.tc_set_enable_pair_cache(self._h, int(bool(enable))))
@@ -477,6 +566,32 @@ class ClothSimulator:
         """Set XPBD compliances (m/N) directly (no stiffness mapping)."""
         self._c(self._L.tc_set_compliance_all(self._h, tension, compression, shear, bending))
 
+    def reset_edge_stiffness_multipliers(self):
+        self._c(self._L.tc_reset_edge_stiffness_multipliers(self._h))
+
+    # ---------------- rest lengths per input edge (lib.rs:2684-2733)
+    def set_edge_rest_length_scales(self, edge_indices, scales):
+        i = np.ascontiguousarray(edge_indices, _u32).reshape(-1)
+        m = np.ascontiguousarray(scales, _f32).reshape(-1)
+        self._c(self._L.tc_set_edge_rest_length_scales(self._h, _ptr(i), _ptr(m), min(i.size, m.size)))
+
+    def reset_edge_rest_lengths(self):
+        self._c(self._L.tc_reset_edge_rest_lengths(self._h))
+
+    def _edge_constraint(self, edge_idx):
+        out = np.zeros(3, _f32)
+        self._c(self._L.tc_get_edge_constraint(self._h, int(edge_idx), _ptr(out)))
+        return out
+
+    def get_edge_rest_length(self, edge_idx):
+        return float(self._edge_constraint(edge_idx)[0])
+
+    def get_edge_initial_rest_length(self, edge_idx):
+        return float(self._edge_constraint(edge_idx)[1])
+
+    def get_edge_tension_compliance(self, edge_idx):
+        return float(self._edge_constraint(edge_idx)[2])
+
     def set_edge_stiffness_multipliers(self, edge_indices, multipliers):
         i = np.ascontiguousarray(edge_indices, _u32)
         m = np.ascontiguousarray(multipliers, _f32)
@@ -491,6 +606,7 @@ class ClothSimulator:
         self._c(self._L.tc_set_self_collision_options(self._h, relief_factor, max_displacement_ratio,
                                                       int(exclude_neighbors), int(enable_normal_untangling),
                                                       int(max_iterations)))
+        self._untangle = bool(enable_normal_untangling)
 
     def set_coupled_collider(self, enabled):
         self._c(self._L.tc_set_coupled_collider(self._h, int(bool(enabled))))

@@ -1,0 +1,81 @@
+"""Per-edge rest lengths, compliance reset and single-substep stepping on the
+GPU (lib.rs:1809-1813, :2684-2733; simulation/mod.rs:1450-1568;
+dispatch.rs:674-688).
+
+* set_edge_rest_length_scales: the constraint of each listed input edge gets
+  initial rest x max(scale, 0.01); the getters report it; reset restores it;
+  a sheet whose rest lengths are all scaled by 0.9 contracts.
+* reset_edge_stiffness_multipliers restores the tension compliance.
+* step_single_substep(dt) gives the same bits as step(dt, 1).
+"""
+import numpy as np
+import pytest
+
+from taremincloth_b200 import ClothSimulator, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _sheet():
+    sc = scenes.config1()
+    s = ClothSimulator(sc["positions"], sc["edges"], sc["faces"], sc["inv_masses"], thickness=0.005,
+                       stiffness=1000.0)
+    return sc, s
+
+
+def test_edge_rest_length_scales():
+    sc, s = _sheet()
+    e = np.asarray(sc["edges"])
+    L0 = np.linalg.norm(sc["positions"][e[:, 0]] - sc["positions"][e[:, 1]], axis=1)
+    for k in (0, 5, 100):
+        assert s.get_edge_initial_rest_length(k) == pytest.approx(L0[k], rel=1e-6)
+        assert s.get_edge_rest_length(k) == s.get_edge_initial_rest_length(k)
+    s.set_edge_rest_length_scales([0, 5, 100], [0.5, 1.2, -3.0])
+    assert s.get_edge_rest_length(0) == np.float32(s.get_edge_initial_rest_length(0)) * np.float32(0.5)
+    assert s.get_edge_rest_length(5) == np.float32(s.get_edge_initial_rest_length(5)) * np.float32(1.2)
+    assert s.get_edge_rest_length(100) == np.float32(s.get_edge_initial_rest_length(100)) * np.float32(0.01)
+    assert s.get_edge_rest_length(len(e) + 10) == 0.0
+    s.reset_edge_rest_lengths()
+    assert s.get_edge_rest_length(0) == s.get_edge_initial_rest_length(0)
+    # every edge at 0.9: the free sheet contracts against an unscaled twin
+    _, twin = _sheet()
+    s.set_edge_rest_length_scales(np.arange(len(e)), np.full(len(e), 0.9, np.float32))
+    ratio = []
+    for sim in (s, twin):
+        sim.set_gravity(0.0, 0.0, 0.0)
+        for _ in range(20):
+            sim.step(1.0 / 60.0, 10)
+        x, _, _ = sim.get_state()
+        ratio.append(float(np.median(np.linalg.norm(x[e[:, 0]] - x[e[:, 1]], axis=1) / L0)))
+    assert ratio[0] < 0.98 and ratio[0] < ratio[1] - 0.02, ratio
+
+
+def test_reset_edge_stiffness_multipliers():
+    _, s = _sheet()
+    c0 = s.get_edge_tension_compliance(3)
+    assert c0 == pytest.approx(1.0 / 1000.0, rel=1e-6)
+    s.set_edge_stiffness_multipliers([3], [4.0])
+    assert s.get_edge_tension_compliance(3) == pytest.approx(c0 / 4.0, rel=1e-6)
+    s.reset_edge_stiffness_multipliers()
+    assert s.get_edge_tension_compliance(3) == c0
+
+
+def test_step_single_substep_equals_one_substep_frame():
+    sc = scenes.config1()
+    a = scenes.build(ClothSimulator, sc)
+    b = scenes.build(ClothSimulator, sc)
+    for _ in range(3):
+        a.step(sc["dt"] / 10, 1)
+        b.step_single_substep(sc["dt"] / 10)
+        xa, _, va = a.get_state()
+        xb, _, vb = b.get_state()
+        np.testing.assert_array_equal(xa, xb)
+        np.testing.assert_array_equal(va, vb)
+    assert b.get_workgroup_size() == 32 and b.get_solver_mode() == 0
+    b.set_coupled_self_collision_options(0, 0)
+    with pytest.raises(NotImplementedError):
+        b.set_coupled_self_collision_options(2, 0)
+    assert b.get_effective_normal_untangling() == bool(b.get_counts()["multi_layer"])
+    b.set_self_collision_options(enable_normal_untangling=False)
+    assert not b.get_effective_normal_untangling()
+    assert b.get_num_virtual_vertices() >= 0
