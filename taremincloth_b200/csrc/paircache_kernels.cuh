@@ -143,6 +143,9 @@ __device__ __forceinline__ void topk_insert(TopK& t, uint32_t quota, float d, ui
 }
 
 // ---------------- broad phase: self_collision_collect_pairs.wgsl:293-661
+// Two launches over the same scan, one per list (kList 0: vertex-triangle,
+// 1: edge-edge): each list and its counters see the reference's insertion
+// sequence, and each launch holds one top-K in registers.
 // Same visiting order and predicates as the reference; pure predicates are
 // evaluated in a cheaper order, which changes no outcome:
 // * candidates come from the hash pass's sorted records (p, thickness,
@@ -153,6 +156,7 @@ __device__ __forceinline__ void topk_insert(TopK& t, uint32_t quota, float d, ui
 //   depend on: (j, index) once per j, (ui, j) and (j, ui) once per ui,
 //   (index, vj) and (vj, index) once per j as a mask over vj, and only
 //   (ui, vj) and (vj, ui) per pair; any true term skips the pair.
+template <int kList>  // 0: vertex-triangle list, 1: edge-edge list
 __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
   const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
   if (index >= s.n) return;
@@ -170,7 +174,9 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
   TopK vt, ee;
   topk_init(vt);
   topk_init(ee);
-  for (int gx = -1; gx <= 1; ++gx)
+  // a pinned vertex collects no edge pairs (:525)
+  const int gx0 = (kList == 1 && pin_i) ? 2 : -1;
+  for (int gx = gx0; gx <= 1; ++gx)
     for (int gy = -1; gy <= 1; ++gy)
       for (int gz = -1; gz <= 1; ++gz) {
         const int32_t cx = base.x + gx, cy = base.y + gy, cz = base.z + gz;
@@ -197,6 +203,7 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
           if (same_island && s.exclude_neighbors && near_folded(s, index, j, sqrtf(fmaxf(d2vv, 0.0f)))) continue;
           const float check = eth + margin + hie + hj;
           // 1. vertex-triangle candidates over j's star (:380-476)
+          if constexpr (kList == 0) {
           const float vtb = eth + llj * 1.3f + margin + hie + hj;
           const bool near2 = s.exclude_neighbors && within2(s, index, j);
           if (d2vv <= vtb * vtb && !near2) {
@@ -224,6 +231,8 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
                 }
               }
             }
+          }
+          continue;
           }
           // 2. edge-edge candidates over both one-rings (:478-612); only a
           // free vertex collects them
@@ -288,22 +297,25 @@ __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
         }
       }
   // vertex-major slots, sentinel-filled (:614-640)
-  const size_t bv = (size_t)index * qvt;
+  if constexpr (kList == 0) {
+    const size_t bv = (size_t)index * qvt;
 #pragma unroll
-  for (uint32_t q = 0; q < kPairQuotaMax; ++q)
-    if (q < qvt)
-      a.vt[bv + q] = q < vt.n ? make_uint4(index, vt.k[q].x, vt.k[q].y, vt.k[q].z)
-                              : make_uint4(kPairSentinel, 0u, 0u, 0u);
-  const size_t be = (size_t)index * qee;
+    for (uint32_t q = 0; q < kPairQuotaMax; ++q)
+      if (q < qvt)
+        a.vt[bv + q] = q < vt.n ? make_uint4(index, vt.k[q].x, vt.k[q].y, vt.k[q].z)
+                                : make_uint4(kPairSentinel, 0u, 0u, 0u);
+    if (vt.eval) atomicAdd(&a.counters[0], vt.eval);
+    if (vt.drop) atomicAdd(&a.counters[2], vt.drop);
+  } else {
+    const size_t be = (size_t)index * qee;
 #pragma unroll
-  for (uint32_t q = 0; q < kPairQuotaMax; ++q)
-    if (q < qee)
-      a.ee[be + q] = q < ee.n ? make_uint4(index, ee.k[q].x, ee.k[q].y, ee.k[q].z)
-                              : make_uint4(kPairSentinel, 0u, 0u, 0u);
-  if (vt.eval) atomicAdd(&a.counters[0], vt.eval);
-  if (vt.drop) atomicAdd(&a.counters[2], vt.drop);
-  if (ee.eval) atomicAdd(&a.counters[1], ee.eval);
-  if (ee.drop) atomicAdd(&a.counters[3], ee.drop);
+    for (uint32_t q = 0; q < kPairQuotaMax; ++q)
+      if (q < qee)
+        a.ee[be + q] = q < ee.n ? make_uint4(index, ee.k[q].x, ee.k[q].y, ee.k[q].z)
+                                : make_uint4(kPairSentinel, 0u, 0u, 0u);
+    if (ee.eval) atomicAdd(&a.counters[1], ee.eval);
+    if (ee.drop) atomicAdd(&a.counters[3], ee.drop);
+  }
 }
 
 // record_untangle_cand (self_collision_solve_vt.wgsl:99-108): the nearest

@@ -1150,7 +1150,17 @@ struct Sim {
       TC_CK(cudaMemsetAsync(pair_cnt.p, 0, 4 * sizeof(uint32_t), st));
       timed("pair_collect", [&] {
         k_pair_horizon<<<grid(n, 256), 256, 0, st>>>(n, v4.p, p);
-        k_pair_collect<<<grid(n, 128), 128, 0, st>>>(a, p);
+        if (profiling) {
+          k_pair_collect<0><<<grid(n, 128), 128, 0, st>>>(a, p);
+          k_pair_collect<1><<<grid(n, 128), 128, 0, st>>>(a, p);
+        } else {  // the two lists are independent: the edge-edge scan runs beside
+          TC_CK(cudaEventRecord(ev_fork, st));
+          TC_CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+          k_pair_collect<1><<<grid(n, 128), 128, 0, st2>>>(a, p);
+          TC_CK(cudaEventRecord(ev_join, st2));
+          k_pair_collect<0><<<grid(n, 128), 128, 0, st>>>(a, p);
+          TC_CK(cudaStreamWaitEvent(st, ev_join, 0));
+        }
       });
     }
     const uint32_t vts = n * pair_qvt, ees = n * pair_qee;
