@@ -158,8 +158,12 @@ __device__ __forceinline__ void topk_insert(TopK& t, uint32_t quota, float d, ui
 //   (ui, vj) and (vj, ui) per pair; any true term skips the pair.
 template <int kList>  // 0: vertex-triangle list, 1: edge-edge list
 __global__ void __launch_bounds__(128) k_pair_collect(SCArgs s, PairArgs a) {
-  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  if (index >= s.n) return;
+  // thread k takes the k-th vertex in hash order: the lanes of a warp share
+  // cells and so walk the same candidates (each vertex's result does not
+  // depend on which thread computes it)
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= s.n) return;
+  const uint32_t index = s.srt[tid];
   const float4 xi4 = s.x4[index], pi4 = s.p4[index];
   const bool pin_i = xi4.w <= 0.0f;
   const V3 pi = mk(pi4);
