@@ -196,3 +196,33 @@ def test_pair_cache_ee_ccd_blocks_high_speed_crossing(oracle_lib, fallback):
     else:
         _, _, _, ee = s.get_active_pairs()
         assert [0, 1, 4, 5] not in ee and len(ee) > 0
+
+
+@pytest.mark.parametrize("case", ["sewn", "intervals"])
+def test_pair_cache_with_sewing_and_intervals(oracle_lib, case):
+    """The pair cache over a sewn garment (sewing-contracted topology, seams
+    closing), and with self-collision every 3rd substep and no edge-edge pass:
+    pairs, counters and positions against the oracle."""
+    if case == "sewn":
+        sc = scenes.sewn_garment(n=24)
+    else:
+        sc = scenes.config2(n=32, subdiv=2)
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    g.set_enable_pair_cache(True)
+    g.set_enable_pair_cache_final_fallback(False)
+    o.set_pair_cache(True, False)
+    if case == "intervals":
+        for sim in (g, o):
+            sim.set_self_collision_substep_interval(3)
+            sim.set_self_collision_ee_substep_interval(0)
+    ext = extent(sc["positions"])
+    for frame in range(4):
+        worst, same = compare_frames(g, o, 1, sc["dt"], sc["substeps"], ext)
+        assert worst.max() <= 1e-5, (frame, worst, same)
+        gvt_n, gee_n, gvt, gee = g.get_active_pairs()
+        ovt_n, oee_n, ovt, oee = o.active_pairs()
+        gvt, gee = _pair_sets(gvt, gee)
+        assert (gvt_n, gee_n) == (ovt_n, oee_n), frame
+        np.testing.assert_array_equal(gvt, ovt)
+        np.testing.assert_array_equal(gee, oee)
