@@ -978,11 +978,22 @@ struct Sim {
       for (int a = 0; a < 3; ++a) { bmin[a] = std::fmin(bmin[a], cen(t, a)); bmax[a] = std::fmax(bmax[a], cen(t, a)); }
     float inv[3];
     for (int a = 0; a < 3; ++a) inv[a] = 1.f / std::fmax(bmax[a] - bmin[a], 1e-5f);
-    std::vector<std::pair<uint32_t, uint32_t>> ki(T);
-    for (uint32_t t = 0; t < T; ++t) ki[t] = {morton3(cen(tris_h[t], 0), cen(tris_h[t], 1), cen(tris_h[t], 2), bmin, inv), t};
-    std::sort(ki.begin(), ki.end());
+    // stable order by code: LSD radix sort, four 8-bit passes over indices
+    // that start ascending (the order of a sort by (code, index))
+    std::vector<uint32_t> code(T), ord(T), tmp(T);
+    for (uint32_t t = 0; t < T; ++t) {
+      code[t] = morton3(cen(tris_h[t], 0), cen(tris_h[t], 1), cen(tris_h[t], 2), bmin, inv);
+      ord[t] = t;
+    }
+    for (int sh = 0; sh < 32; sh += 8) {
+      uint32_t hist[257] = {0};
+      for (uint32_t t = 0; t < T; ++t) ++hist[((code[ord[t]] >> sh) & 255u) + 1];
+      for (int b = 0; b < 256; ++b) hist[b + 1] += hist[b];
+      for (uint32_t t = 0; t < T; ++t) tmp[hist[(code[ord[t]] >> sh) & 255u]++] = ord[t];
+      ord.swap(tmp);
+    }
     std::vector<MeshTri> sorted(T);
-    for (uint32_t t = 0; t < T; ++t) sorted[t] = tris_h[ki[t].second];
+    for (uint32_t t = 0; t < T; ++t) sorted[t] = tris_h[ord[t]];
     tris_h.swap(sorted);
     std::vector<float4> bd(T);
     for (uint32_t t = 0; t < T; ++t) {
