@@ -762,6 +762,7 @@ struct Sim {
     if (st) cudaStreamDestroy(st);
     if (h_err) cudaFreeHost(h_err);
     if (h_fb) cudaFreeHost(h_fb);
+    if (h_pos3) cudaFreeHost(h_pos3);
   }
 
   void mark() { graph_dirty = true; }
@@ -1931,11 +1932,21 @@ struct Sim {
     if (buffered < kMaxBuffered) ++buffered;
     return buffered;
   }
+  // positions packed xyz on the device, one copy into a pinned staging
+  // buffer, then into the caller's array
+  DBuf<float> pos3;
+  float* h_pos3 = nullptr;
   void get_positions(float* out) {
-    std::vector<float4> h(n);
-    TC_CK(cudaMemcpyAsync(h.data(), x4.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    if (n == 0) return;
+    if (!h_pos3) {
+      pos3.alloc(size_t(n) * 3);
+      TC_CK(cudaHostAlloc(&h_pos3, size_t(n) * 3 * sizeof(float), cudaHostAllocDefault));
+    }
+    k_extract_positions<<<grid(n, 256), 256, 0, st>>>(n, x4.p, pos3.p);
+    TC_CK(cudaGetLastError());
+    TC_CK(cudaMemcpyAsync(h_pos3, pos3.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaStreamSynchronize(st));
-    for (uint32_t i = 0; i < n; ++i) { out[3 * i] = h[i].x; out[3 * i + 1] = h[i].y; out[3 * i + 2] = h[i].z; }
+    std::memcpy(out, h_pos3, size_t(n) * 3 * sizeof(float));
   }
 };
 
