@@ -226,3 +226,20 @@ def test_pair_cache_with_sewing_and_intervals(oracle_lib, case):
         assert (gvt_n, gee_n) == (ovt_n, oee_n), frame
         np.testing.assert_array_equal(gvt, ovt)
         np.testing.assert_array_equal(gee, oee)
+
+
+def test_pair_cache_600_substeps_within_tolerance(oracle_lib):
+    """600 substeps (30 frames x 20) with the pair cache on: positions within
+    1e-4 of the extent of the oracle's, and the stored pairs equal at the end."""
+    sc = scenes.config2(n=48, subdiv=3)
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    g.set_enable_pair_cache(True)
+    o.set_pair_cache(True, True)
+    worst, same = compare_frames(g, o, 30, sc["dt"], sc["substeps"], extent(sc["positions"]), 1e-4)
+    assert worst.max() <= 1e-4, (worst.max(), same.min())
+    _, _, gvt, gee = g.get_active_pairs()
+    _, _, ovt, oee = o.active_pairs()
+    gvt, gee = _pair_sets(gvt, gee)
+    np.testing.assert_array_equal(gvt, ovt)
+    np.testing.assert_array_equal(gee, oee)
