@@ -243,3 +243,22 @@ def test_pair_cache_600_substeps_within_tolerance(oracle_lib):
     gvt, gee = _pair_sets(gvt, gee)
     np.testing.assert_array_equal(gvt, ovt)
     np.testing.assert_array_equal(gee, oee)
+
+
+def test_pair_cache_options_and_empty_state():
+    """Option clamps (simulation/mod.rs:826-848) and the state before any
+    broad phase: no counters, no stored pairs."""
+    pos = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], np.float32)
+    s = ClothSimulator(pos, np.array([[0, 1], [1, 2], [2, 3], [3, 0], [0, 2]]), np.array([[0, 1, 2], [0, 2, 3]]))
+    assert s.get_pair_cache_stats() == (0, 0, 8192, 8192)
+    assert not s.get_enable_pair_cache() and s.get_enable_pair_cache_final_fallback()
+    s.set_enable_pair_cache(True)
+    assert s.get_active_pairs() == (0, 0, [], [])
+    s.set_pair_cache_options(10, 10 ** 7, 5, 1.0, 9.0, 1.0)
+    assert s.get_pair_cache_stats()[2:] == (64, 262144)
+    s.set_enable_pair_cache_final_fallback(False)
+    assert not s.get_enable_pair_cache_final_fallback()
+    s.set_enable_self_collision(True)
+    s.step(1.0 / 60.0, 2)
+    x, _, _ = s.get_state()
+    assert np.isfinite(x).all()
