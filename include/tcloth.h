@@ -337,6 +337,35 @@ tc_status tc_compute_combined_inv_masses(const float *positions, uint32_t n, con
 /* color_edge_pairs (coloring.rs:180-233, lib.rs:642-652), host only:
  * Welsh-Powell colours of vertex pairs, order (-degree, index). */
 tc_status tc_color_edge_pairs(uint32_t num_vertices, const uint32_t *pairs, uint32_t np, uint32_t *colors);
+/* The settings record of the reference (SimConfig,
+ * crates/cloth_core/src/config.rs:40-140, written by
+ * simulation/config_impl.rs:16-78; cloth_py lib.rs:3029-3042).
+ * tc_get_config_json writes the compact JSON text (fields in the record's
+ * order, floats as the shortest f32 digits) into buf when capacity > 0,
+ * truncated to capacity - 1 bytes and NUL-terminated, and its full length in
+ * *length.  tc_get_config_hash is the 64-bit FNV-1a of that text
+ * (config.rs:205-214, lib.rs:3044-3047).  Applying a record is the host's
+ * job: parse it and call the setters in config_impl.rs:80-155's order. */
+tc_status tc_get_config_json(tc_sim *s, char *buf, size_t capacity, size_t *length);
+tc_status tc_get_config_hash(tc_sim *s, uint64_t *hash);
+/* set_workgroup_size (mod.rs:2987-2994): 64 or else 32, stored for the
+ * record; the CUDA path's launch shapes do not depend on it. */
+tc_status tc_set_workgroup_size(tc_sim *s, uint32_t wg_size);
+/* set_areal_density (mod.rs:1241-1245): finite values clamped to [0, 100]. */
+tc_status tc_set_areal_density(tc_sim *s, float density);
+/* set_coupled_self_collision_options (mod.rs:1055-1058): mode 0 only (the
+ * others are TC_ERR_INVALID); the relaxation count is stored. */
+tc_status tc_set_coupled_self_collision_options(tc_sim *s, uint32_t mode, uint32_t relaxation_iters);
+/* find_triangle_intersections (crates/cloth_core/src/geometry.rs:506-633,
+ * crates/cloth_py/src/lib.rs:856-879), host only: face pairs (f0 < f1,
+ * ascending) whose triangles share a point; with ignore_adjacent, pairs that
+ * share a vertex (or a vertex cluster joined by the optional sewing springs)
+ * are skipped; faces with repeated or out-of-range indices are skipped.
+ * cell_size <= 0 picks the broad-phase cell.  Writes min(count, capacity)
+ * pairs (2 words each) and the total in *count. */
+tc_status tc_find_triangle_intersections(const float *positions, uint32_t n, const uint32_t *faces, uint32_t nf,
+                                         int ignore_adjacent, float cell_size, const uint32_t *sewing, uint32_t nsew,
+                                         uint32_t *pairs, uint32_t capacity, uint32_t *count);
 tc_status tc_bake_dims(tc_bake *b, uint32_t out[4]);
 /* texels (w*h*d), infos (n_active x 20), active (source bone index per
  * active bone), bind (n_active x 16); any may be NULL */
@@ -509,14 +538,20 @@ tc_status tc_mlp_grad(uint32_t n, const float *feat, const uint32_t *adj_off, co
  * For callers that cannot allocate device memory: applications whose device
  * buffers all come from their own allocator, threads that must not call
  * cudaMalloc / cudaFree (they synchronise the device), memory-capped hosts.
- * Builds the same cell_starts / sorted arrays as tc_get_hash_state from
- * `positions` (device, n x 4 floats: x, y, z, unused), on `stream`
- * (cudaStream_t, NULL = legacy default stream).  All buffers are the
- * caller's device memory; scratch is a static array in the library of fixed
- * size, so n <= 262144 and 1024 <= table_size <= 65536, else TC_ERR_INVALID.
- * The first call on a device looks up that array's device address, so make
- * it before any stream capture.  All calls on a device share the array:
- * calls that overlap on the GPU (different streams, or threads) race. */
+ * Builds cell_starts (table_size + 1 entries, exclusive prefix sums of the
+ * bucket counts, last = n) and sorted (n vertex indices grouped by bucket,
+ * ascending index within each bucket) from `positions` (device, n x 4
+ * floats: x, y, z, unused; 16-byte aligned), on `stream` (cudaStream_t,
+ * NULL = legacy default stream).  Given the simulator's predicted positions
+ * (tc_get_state's p), cell size and table size, the output equals
+ * tc_get_hash_state(which = 0).  All buffers are the caller's device memory;
+ * scratch is a static array in the library of fixed size, so n <= 262144
+ * and 1024 <= table_size <= 65536, and cell_size must be positive, else
+ * TC_ERR_INVALID.  n = 0 gives all-zero cell_starts.  The first call on a
+ * device looks up that array's device address, so make it before any stream
+ * capture; after a reset of the device's primary context the library needs
+ * a fresh process.  All calls on a device share the array: calls that
+ * overlap on the GPU (different streams, or threads) race. */
 tc_status tc_hash_build_static(const float *positions, uint32_t n, float cell_size, uint32_t table_size,
                                uint32_t *cell_starts, uint32_t *sorted, void *stream);
 

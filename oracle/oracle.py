@@ -64,6 +64,7 @@ def lib():
         L.ocl_set_solver_iterations.argtypes = [P, C.c_int]
         L.ocl_set_enable_self_collision.argtypes = [P, C.c_int]
         L.ocl_set_coupled_collider.argtypes = [P, C.c_int]
+        L.ocl_set_collider_options.argtypes = [P, C.c_int, C.c_int, C.c_float]
         L.ocl_set_self_collision_options.argtypes = [P, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int]
         L.ocl_add_sphere.argtypes = [P, fp, C.c_float, C.c_float, C.c_float]
         L.ocl_add_capsule.argtypes = [P, fp, fp, C.c_float, C.c_float, C.c_float]
@@ -171,6 +172,11 @@ class OracleSim:
     def set_compliance_all(self, tension, compression, shear, bending):
         lib().ocl_set_compliance_all(self._h, tension, compression, shear, bending)
 
+    def set_collider_options(self, enable_cluster_culling=False, enable_single_sided_recovery=True,
+                             sweep_margin=0.05):
+        lib().ocl_set_collider_options(self._h, int(enable_cluster_culling), int(enable_single_sided_recovery),
+                                       sweep_margin)
+
     def add_sphere_collider(self, center, radius, friction=0.0, restitution=0.0):
         lib().ocl_add_sphere(self._h, np.asarray(center, _f), radius, friction, restitution)
 
@@ -217,6 +223,12 @@ class OracleSim:
         v = np.empty((self.n, 3), _f)
         lib().ocl_get_state(self._h, _ptr(x), _ptr(p), _ptr(v))
         return x, p, v
+
+    def set_positions_and_velocities(self, positions, velocities=None):
+        self.set_state(positions, velocities)
+
+    def step_single_substep(self, dt_sub):
+        lib().ocl_step(self._h, dt_sub, 1)
 
     def set_state(self, x, v=None):
         x = np.ascontiguousarray(x, _f).reshape(-1)

@@ -1072,6 +1072,13 @@ void ocl_set_damping_all(OSim *s, float t, float c, float sh, float b) {
 void ocl_set_solver_iterations(OSim *s, int it) { s->iters = it < 1 ? 1 : it; }
 void ocl_set_enable_self_collision(OSim *s, int on) { s->self_collision = on != 0; }
 void ocl_set_coupled_collider(OSim *s, int on) { s->coupled = on != 0; }
+/* set_collider_options (simulation/mod.rs set_collider_options): only the
+ * single-sided recovery flag changes results; cluster culling and the sweep
+ * margin select broadphase variants whose contacts are the same. */
+void ocl_set_collider_options(OSim *s, int cluster, int recovery, float sweep) {
+    (void)cluster; (void)sweep;
+    s->single_sided_recovery = recovery != 0;
+}
 /* simulation/mod.rs:920-950 */
 void ocl_set_self_collision_options(OSim *s, float relief, float max_disp_ratio, int exclude_neighbors,
                                     int untangle, int max_iter) {

@@ -73,6 +73,7 @@ int ocl_num_collider_edges(const OSim *s);
 void ocl_set_pin(OSim *s, uint32_t v, const float *target, float w);
 void ocl_clear_pins(OSim *s);
 void ocl_set_coupled_collider(OSim *s, int on);
+void ocl_set_collider_options(OSim *s, int cluster, int recovery, float sweep);
 
 /* time stepping: GpuClothSimulator::step (simulation/dispatch.rs:610-671) */
 void ocl_step(OSim *s, float dt, int substeps);

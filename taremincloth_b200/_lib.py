@@ -44,6 +44,12 @@ SIGNATURES = {
     "tc_set_enable_edge_collision": [_P, _I],
     "tc_compute_combined_inv_masses": [_P, _U, _P, _U, _P, _U, _P, _U, _F, _F, _P],
     "tc_color_edge_pairs": [_U, _P, _U, _P],
+    "tc_get_config_json": [_P, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)],
+    "tc_get_config_hash": [_P, C.POINTER(C.c_uint64)],
+    "tc_set_workgroup_size": [_P, _U],
+    "tc_set_areal_density": [_P, _F],
+    "tc_set_coupled_self_collision_options": [_P, _U, _U],
+    "tc_find_triangle_intersections": [_P, _U, _P, _U, _I, _F, _P, _U, _P, _U, C.POINTER(_U)],
     "tc_reset_edge_stiffness_multipliers": [_P],
     "tc_set_edge_rest_length_scales": [_P, _P, _P, _U],
     "tc_reset_edge_rest_lengths": [_P],

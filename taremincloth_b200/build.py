@@ -21,7 +21,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
     "-shared",
 ]
-SOURCES = ["sim.cu", "mesh.cpp"]
+SOURCES = ["sim.cu", "mesh.cpp", "geometry.cpp", "config.cpp"]
 
 
 def _stale(target, deps):

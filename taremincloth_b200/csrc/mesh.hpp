@@ -89,4 +89,11 @@ std::vector<float> combined_inv_masses(const float* pos, uint32_t n, const uint3
                                        float areal_density, float linear_density);
 std::vector<uint32_t> color_edge_pairs(uint32_t nv, const uint32_t* pairs, uint32_t np);
 
+// Face pairs (f0 < f1, ascending, flattened) whose triangles intersect,
+// skipping pairs that share a vertex (or a sewn vertex cluster) when
+// ignore_adjacent (geometry.rs:506-633); cell_size <= 0 picks one.
+std::vector<uint32_t> find_triangle_intersections(const float* pos, uint32_t n, const uint32_t* faces, uint32_t nf,
+                                                  bool ignore_adjacent, float cell_size, const uint32_t* sew,
+                                                  uint32_t nsew);
+
 }  // namespace tcloth

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -23,6 +24,7 @@
 
 #include "../../include/tcloth.h"
 #include "adaptive.hpp"
+#include "config.hpp"
 #include "mesh.hpp"
 #include "selfcol_kernels.cuh"
 #include "paircache_kernels.cuh"
@@ -697,6 +699,12 @@ struct Sim {
     return ee_interval == 0 ? false : (ee_interval == 1 ? true : (s % ee_interval == 0 || s + 1 == substeps));
   }
   bool coupled = false, auto_coupled = true, recovery = true;
+  // settings the CUDA path stores for the config record only: the shader
+  // workgroup size (pipeline_cache.rs:25-31), the post-collision relaxation
+  // count of the coupled modes (mod.rs:1055-1058), the areal density
+  // (mod.rs:1241-1245)
+  uint32_t wg_size = 32, relax_iters = 1;
+  float areal_density = 0.15f;
   float cloth_thickness = 0.005f;
   float last_max_disp = 0.f, last_eff_disp = 0.f;
   std::vector<float> prev_frame_pos;
@@ -766,6 +774,45 @@ struct Sim {
   }
 
   void mark() { graph_dirty = true; }
+
+  // the settings as the reference's SimConfig record (config_impl.rs:16-92)
+  tcloth::SimSettings settings() const {
+    tcloth::SimSettings c;
+    for (int k = 0; k < 3; ++k) c.gravity[k] = g[k];
+    c.damping = damping;
+    c.tension_damping = td; c.compression_damping = cd; c.shear_damping = sd; c.bending_damping = bd;
+    c.tension_stiffness = tcloth::compliance_to_stiffness(base_tc);
+    c.compression_stiffness = tcloth::compliance_to_stiffness(base_cc);
+    c.shear_stiffness = tcloth::compliance_to_stiffness(base_shc);
+    c.bending_stiffness = base_bk;
+    for (const auto& q : bend_h)
+      if (q.pad0 <= 1.5f) { c.bending_stiffness = tcloth::compliance_to_stiffness(q.comp); break; }
+    c.solver_iterations = iters;
+    c.solver_mode = 0;
+    c.workgroup_size = wg_size;
+    c.enable_self_collision = self_collision;
+    c.relief_factor = relief; c.max_displacement_ratio = max_disp_ratio;
+    c.exclude_neighbors = exclude_neighbors; c.enable_normal_untangling = untangle_opt;
+    c.self_collision_max_iterations = max_search;
+    c.coupled_mode = 0; c.coupled_collider = coupled; c.post_relaxation_iters = relax_iters;
+    c.substep_interval = sc_interval; c.ee_substep_interval = ee_interval;
+    c.self_collision_algorithm = sc_algorithm; c.enable_pair_cache = pair_cache;
+    c.pair_margin_mode = pair_margin_mode; c.pair_safety_margin = pair_safety;
+    c.pair_horizon_scale = pair_hscale; c.pair_max_horizon = pair_max_h;
+    c.pair_max_pairs = std::max(pair_max_vt, pair_max_ee);
+    c.enable_pair_final_fallback = pair_final_fallback;
+    c.enable_edge_collision = edge_collision; c.edge_margin_scale = edge_mscale; c.edge_margin_offset = edge_moff;
+    c.sewing_stiffness = sew_stiffness; c.sewing_shrink_speed = sew_speed;
+    c.enable_sewing_lock = sew_lock; c.sewing_lock_distance = sew_lock_dist;
+    c.areal_density = areal_density;
+    c.sewing_priority_enabled = pri.enabled; c.sewing_priority_threshold = pri.threshold;
+    c.sewing_priority_merge_dist = pri.merge; c.sewing_priority_ramp_frames = pri.ramp_frames;
+    c.sewing_priority_max_frames = pri.max_frames;
+    c.enable_adaptive_substep = ad.enabled; c.min_substeps = ad.min_substeps; c.max_substeps = ad.max_substeps;
+    c.auto_coupled_on_low_substeps = auto_coupled; c.auto_compensate_iterations = ad.auto_compensate;
+    c.enable_strain_adaptive = ad.strain_adaptive; c.strain_tolerance = ad.strain_tolerance;
+    return c;
+  }
 
   // ---- upload of the vertex state from host arrays
   void upload_vertices(const float* pos, const float* vel, const float* w) {
@@ -1936,11 +1983,15 @@ struct Sim {
   // buffer, then into the caller's array
   DBuf<float> pos3;
   float* h_pos3 = nullptr;
+  uint32_t pos3_cap = 0;  // vertices the two staging buffers hold
   void get_positions(float* out) {
     if (n == 0) return;
-    if (!h_pos3) {
+    if (pos3_cap < n) {
+      if (h_pos3) TC_CK(cudaFreeHost(h_pos3));
+      h_pos3 = nullptr;
       pos3.alloc(size_t(n) * 3);
       TC_CK(cudaHostAlloc(&h_pos3, size_t(n) * 3 * sizeof(float), cudaHostAllocDefault));
+      pos3_cap = n;
     }
     k_extract_positions<<<grid(n, 256), 256, 0, st>>>(n, x4.p, pos3.p);
     TC_CK(cudaGetLastError());
@@ -3923,6 +3974,21 @@ tc_status tc_color_edge_pairs(uint32_t num_vertices, const uint32_t* pairs, uint
   });
 }
 
+tc_status tc_find_triangle_intersections(const float* positions, uint32_t n, const uint32_t* faces, uint32_t nf,
+                                         int ignore_adjacent, float cell_size, const uint32_t* sewing, uint32_t nsew,
+                                         uint32_t* pairs, uint32_t capacity, uint32_t* count) {
+  return guard([&] {
+    need(count != nullptr, "count required");
+    need((positions != nullptr || n == 0) && (faces != nullptr || nf == 0), "positions and faces required");
+    need(capacity == 0 || pairs != nullptr, "pairs required when capacity > 0");
+    const std::vector<uint32_t> r = tcloth::find_triangle_intersections(
+        positions, n, faces, nf, ignore_adjacent != 0, cell_size, sewing, sewing ? nsew : 0);
+    const uint32_t k = uint32_t(r.size() / 2);
+    *count = k;
+    std::copy(r.begin(), r.begin() + 2 * size_t(std::min(k, capacity)), pairs);
+  });
+}
+
 tc_status tc_bake_dims(tc_bake* b, uint32_t out[4]) {
   return guard([&] {
     need(b && out, "bake result and output required");
@@ -3943,6 +4009,40 @@ tc_status tc_bake_get(tc_bake* b, uint32_t* texels, float* infos, uint32_t* acti
 tc_status tc_bake_destroy(tc_bake* b) {
   delete b;
   return TC_OK;
+}
+
+// ---- settings record (simulation/config_impl.rs, cloth_py lib.rs:3029-3047)
+tc_status tc_set_workgroup_size(tc_sim* s, uint32_t wg) {
+  return guard([&] { S(s).wg_size = wg == 64 ? 64u : 32u; });
+}
+tc_status tc_set_areal_density(tc_sim* s, float density) {
+  return guard([&] {
+    if (std::isfinite(density)) S(s).areal_density = std::min(std::max(density, 0.f), 100.f);
+  });
+}
+tc_status tc_set_coupled_self_collision_options(tc_sim* s, uint32_t mode, uint32_t relaxation_iters) {
+  return guard([&] {
+    need(mode == 0, "coupled self-collision modes 1-3 are not built");
+    S(s).relax_iters = relaxation_iters;
+  });
+}
+tc_status tc_get_config_json(tc_sim* s, char* buf, size_t capacity, size_t* length) {
+  return guard([&] {
+    need(length != nullptr, "length required");
+    const std::string j = tcloth::settings_json(S(s).settings());
+    *length = j.size();
+    if (buf && capacity) {
+      const size_t k = std::min(j.size(), capacity - 1);
+      std::memcpy(buf, j.data(), k);
+      buf[k] = '\0';
+    }
+  });
+}
+tc_status tc_get_config_hash(tc_sim* s, uint64_t* hash) {
+  return guard([&] {
+    need(hash != nullptr, "hash required");
+    *hash = tcloth::settings_hash(tcloth::settings_json(S(s).settings()));
+  });
 }
 
 // ---- diagnostics of the latest self-collision pass: pairs handed to the
@@ -4238,16 +4338,23 @@ __global__ void k_static_hash_count(uint32_t n, const float4* __restrict__ pos, 
 static StaticHashScratch* static_scratch_for_current_device() {
   // One device address per device, looked up on the first call with that
   // device current (the host-side name of the array is not a device address).
-  static StaticHashScratch* ptrs[64] = {};
+  // Threads making their first call on one device at the same time both look
+  // the address up and publish the same value; the atomics make that a
+  // well-defined race.  The address belongs to the device's primary context:
+  // after a reset of that context (cudaDeviceReset) the library must be used
+  // from a fresh process.
+  static std::atomic<StaticHashScratch*> ptrs[64] = {};
   int dev = 0;
   TC_CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) throw TcError(TC_ERR_CUDA, "device index out of range for the static scratch table");
-  if (!ptrs[dev]) {
+  StaticHashScratch* cached = ptrs[dev].load(std::memory_order_acquire);
+  if (!cached) {
     void* p = nullptr;
     TC_CK(cudaGetSymbolAddress(&p, g_static_hash_scratch));
-    ptrs[dev] = static_cast<StaticHashScratch*>(p);
+    cached = static_cast<StaticHashScratch*>(p);
+    ptrs[dev].store(cached, std::memory_order_release);
   }
-  return ptrs[dev];
+  return cached;
 }
 
 extern "C" tc_status tc_hash_build_static(const float* positions, uint32_t n, float cell_size, uint32_t table_size,
@@ -4259,6 +4366,8 @@ extern "C" tc_status tc_hash_build_static(const float* positions, uint32_t n, fl
     need(cell_size > 0.f, "tc_hash_build_static: cell_size must be positive");
     need(cell_starts != nullptr && (sorted != nullptr || n == 0) && (positions != nullptr || n == 0),
          "tc_hash_build_static: positions, cell_starts and sorted are required");
+    need(reinterpret_cast<uintptr_t>(positions) % 16 == 0,
+         "tc_hash_build_static: positions must be 16-byte aligned (rows of 4 floats read as float4)");
     StaticHashScratch* sc = static_scratch_for_current_device();
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const float4* pos = reinterpret_cast<const float4*>(positions);

@@ -9,6 +9,7 @@ names, same exceptions (``ValueError`` for bad shapes or indices,
 from __future__ import annotations
 
 import ctypes as C
+import json
 
 import numpy as np
 
@@ -155,6 +156,50 @@ def color_edge_pairs(num_vertices, edges):
     L = _lib.load()
     _lib.check(L.tc_color_edge_pairs(int(num_vertices), _ptr(e), e.shape[0], _ptr(out)))
     return [int(c) for c in out]
+
+
+# SimConfig::default (crates/cloth_core/src/config.rs:3-37, :142-196): the
+# value of every field a settings JSON record leaves out
+CONFIG_DEFAULTS = {
+    "version": 1, "gravity": [0.0, 0.0, -9.81], "damping": 1.0, "tension_damping": 5.0,
+    "compression_damping": 5.0, "shear_damping": 5.0, "bending_damping": 0.5, "tension_stiffness": 1500.0,
+    "compression_stiffness": 150.0, "shear_stiffness": 100.0, "bending_stiffness": 15.0, "solver_iterations": 2,
+    "solver_mode": 0, "workgroup_size": 32, "enable_self_collision": False, "relief_factor": 1.0,
+    "max_displacement_ratio": 0.5, "exclude_neighbors": True, "enable_normal_untangling": True,
+    "self_collision_max_iterations": 256, "coupled_mode": 0, "coupled_collider": False, "post_relaxation_iters": 2,
+    "substep_interval": 1, "ee_substep_interval": 1, "self_collision_algorithm": 0, "enable_pair_cache": False,
+    "pair_margin_mode": 1, "pair_safety_margin": 0.005, "pair_horizon_scale": 1.3, "pair_max_horizon": 0.02,
+    "pair_max_pairs": 65536, "enable_pair_final_fallback": True, "enable_edge_collision": False,
+    "edge_margin_scale": 1.0, "edge_margin_offset": 0.0, "sewing_stiffness": 10000.0, "sewing_shrink_speed": 1.0,
+    "enable_sewing_lock": True, "sewing_lock_distance": 0.02, "sewing_priority_enabled": False,
+    "sewing_priority_threshold": 0.9, "sewing_priority_merge_dist": 0.005, "sewing_priority_ramp_frames": 3,
+    "sewing_priority_max_frames": 600, "areal_density": 0.15, "enable_adaptive_substep": False, "min_substeps": 4,
+    "max_substeps": 64, "auto_coupled_on_low_substeps": True, "auto_compensate_iterations": True,
+    "enable_strain_adaptive": True, "strain_tolerance": 0.008,
+}
+
+
+def find_triangle_intersections(positions, faces, ignore_adjacent=True, cell_size=None, sewing_springs=None):
+    """Self-intersecting face pairs [(f0, f1), ...], f0 < f1 ascending
+    (lib.rs:856-879, geometry.rs:506-633); host only, no GPU needed."""
+    pos = _arr(positions, _f32, 3, "positions")
+    f = _rows(faces, 3, _u32, "faces")
+    if f is None:
+        return []
+    sew = _rows(sewing_springs, 2, _u32, "sewing_springs") if sewing_springs is not None else None
+    L = _lib.load()
+    cnt = C.c_uint32(0)
+    cap = max(64, f.shape[0])
+    while True:
+        out = np.zeros(2 * cap, _u32)
+        _lib.check(L.tc_find_triangle_intersections(_ptr(pos), pos.shape[0], _ptr(f), f.shape[0],
+                                                    int(bool(ignore_adjacent)),
+                                                    float(cell_size) if cell_size else 0.0, _ptr(sew),
+                                                    0 if sew is None else sew.shape[0], _ptr(out), cap,
+                                                    C.byref(cnt)))
+        if cnt.value <= cap:
+            return [(int(a), int(b)) for a, b in out[:2 * cnt.value].reshape(-1, 2)]
+        cap = cnt.value
 
 
 def _mesh_arrays(mesh_verts, mesh_tris):
@@ -359,7 +404,8 @@ class ClothSimulator:
     # ---------------- settings the CUDA path has no use for, kept for the API
     # (lib.rs:1898-1906, :1935-1937, :2828-2836, :2030-2060)
     def set_workgroup_size(self, wg_size):
-        self._wg = int(wg_size)
+        self._wg = 64 if int(wg_size) == 64 else 32
+        self._c(self._L.tc_set_workgroup_size(self._h, int(wg_size)))
 
     def get_workgroup_size(self):
         return getattr(self, "_wg", 32)
@@ -375,11 +421,93 @@ class ClothSimulator:
         """mode 0 (self-collision once per substep after the final pins) is the one built."""
         if int(mode) != 0:
             raise NotImplementedError("coupled self-collision modes 1-3 are not built")
+        self._c(self._L.tc_set_coupled_self_collision_options(self._h, 0, int(relaxation_iters)))
+
+    # ---------------- settings record (lib.rs:3029-3047, config_impl.rs:16-160)
+    def get_config_json(self):
+        """Every settable parameter as the reference's SimConfig JSON text."""
+        n = C.c_size_t(0)
+        self._c(self._L.tc_get_config_json(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value + 1)
+        self._c(self._L.tc_get_config_json(self._h, buf, n.value + 1, C.byref(n)))
+        return buf.value.decode("ascii")
+
+    def get_config_hash(self):
+        """64-bit FNV-1a of get_config_json() (change detection between frames)."""
+        h = C.c_uint64(0)
+        self._c(self._L.tc_get_config_hash(self._h, C.byref(h)))
+        return h.value
+
+    def apply_config_json(self, json_str):
+        """Apply a SimConfig JSON record through the setters, in the reference's
+        order (config_impl.rs:80-155); absent fields take SimConfig's defaults
+        (config.rs:142-196), unknown fields are ignored; malformed text or
+        mistyped fields raise ValueError before anything is applied."""
+        try:
+            d = json.loads(json_str)
+        except (TypeError, ValueError) as e:
+            raise ValueError(f"could not parse the settings JSON: {e}") from None
+        if not isinstance(d, dict):
+            raise ValueError("the settings JSON must be an object")
+        c = dict(CONFIG_DEFAULTS)
+        for k, v in d.items():
+            if k not in c:
+                continue
+            want = type(CONFIG_DEFAULTS[k])
+            if want is bool:
+                ok = isinstance(v, bool)
+            elif want is int:
+                ok = isinstance(v, int) and not isinstance(v, bool) and 0 <= v <= 0xFFFFFFFF
+            elif want is float:
+                ok = isinstance(v, (int, float)) and not isinstance(v, bool)
+            else:
+                ok = isinstance(v, list) and len(v) == 3 and all(
+                    isinstance(x, (int, float)) and not isinstance(x, bool) for x in v)
+            if not ok:
+                raise ValueError(f"settings field {k!r} has an invalid value {v!r}")
+            c[k] = v
+        self.set_gravity(*c["gravity"])
+        self.set_damping(c["damping"])
+        self.set_damping_all(c["tension_damping"], c["compression_damping"], c["shear_damping"],
+                             c["bending_damping"])
+        self.set_stiffness_all(c["tension_stiffness"], c["compression_stiffness"], c["shear_stiffness"],
+                               c["bending_stiffness"])
+        self.set_solver_iterations(c["solver_iterations"])
+        self.set_solver_mode(c["solver_mode"])
+        self.set_workgroup_size(c["workgroup_size"])
+        self.set_enable_self_collision(c["enable_self_collision"])
+        self.set_self_collision_options(c["relief_factor"], c["max_displacement_ratio"], c["exclude_neighbors"],
+                                        c["enable_normal_untangling"], c["self_collision_max_iterations"])
+        self.set_coupled_self_collision_options(c["coupled_mode"], c["post_relaxation_iters"])
+        self.set_coupled_collider(c["coupled_collider"])
+        self.set_auto_coupled_on_low_substeps(c["auto_coupled_on_low_substeps"])
+        self.set_self_collision_substep_interval(max(c["substep_interval"], 1))
+        self.set_self_collision_ee_substep_interval(c["ee_substep_interval"])
+        self.set_self_collision_algorithm(c["self_collision_algorithm"])
+        self.set_enable_pair_cache(c["enable_pair_cache"])
+        self.set_pair_cache_options(c["pair_max_pairs"], c["pair_max_pairs"], c["pair_margin_mode"],
+                                    c["pair_safety_margin"], c["pair_horizon_scale"], c["pair_max_horizon"])
+        self.set_enable_pair_cache_final_fallback(c["enable_pair_final_fallback"])
+        self.set_enable_edge_collision(c["enable_edge_collision"])
+        self.set_edge_margin_scale(c["edge_margin_scale"])
+        self.set_edge_margin_offset(c["edge_margin_offset"])
+        self.set_sewing_stiffness(c["sewing_stiffness"])
+        self.set_sewing_shrink_speed(c["sewing_shrink_speed"])
+        self.set_enable_sewing_lock(c["enable_sewing_lock"])
+        self.set_sewing_lock_distance(c["sewing_lock_distance"])
+        self.set_areal_density(c["areal_density"])
+        self.set_sewing_priority_options(c["sewing_priority_enabled"], c["sewing_priority_threshold"],
+                                         c["sewing_priority_merge_dist"], c["sewing_priority_ramp_frames"],
+                                         c["sewing_priority_max_frames"])
+        self.set_adaptive_substep_options(c["enable_adaptive_substep"], c["min_substeps"], c["max_substeps"])
+        self.set_auto_compensate_iterations(c["auto_compensate_iterations"])
+        self.set_strain_adaptive_options(c["enable_strain_adaptive"], c["strain_tolerance"])
 
     def set_areal_density(self, density):
         d = float(density)
         if np.isfinite(d):
             self._areal_density = min(max(d, 0.0), 100.0)
+        self._c(self._L.tc_set_areal_density(self._h, d))
 
     def set_enable_compact_readback(self, enable):
         self._compact = bool(enable)

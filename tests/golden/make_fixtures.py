@@ -1,7 +1,8 @@
 """Copies the reference's golden-master vectors into tests/golden/.
 
-Run once in a container where the reference checkout is mounted:
-    python tests/golden/make_fixtures.py /root/reference
+Run once in a container where the reference checkout is mounted, giving
+the checkout's root:
+    python tests/golden/make_fixtures.py <reference checkout>
 The files are the reference's own fixtures
 (tests/fixtures/golden_master/*.npz): initial positions, edges, faces,
 inverse masses and 26 frames produced by the reference GPU solver, plus the
@@ -25,4 +26,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <reference checkout root>")
+    main(sys.argv[1])

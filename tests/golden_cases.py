@@ -70,3 +70,72 @@ def step_input(case):
     sd = np.load(os.path.join(GOLDEN, f"step_{case}_f1.npz"))
     pin = sd["pos_in"] if "pos_in" in sd.files else pos
     return pin, sd["pos_out"]
+
+
+def _edge_len(p, e):
+    e = np.asarray(e, np.int64)
+    return np.linalg.norm(p[e[:, 0]] - p[e[:, 1]], axis=1)
+
+
+def _segment_distance(points, a, b):
+    """Smallest distance of the points to segment ab
+    (test_golden_regression.py:53-66)."""
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    ab = b - a
+    ap = points.astype(np.float64) - a
+    t = np.clip(ap @ ab / float(ab @ ab), 0.0, 1.0)
+    return float(np.linalg.norm(points - (a + t[:, None] * ab), axis=1).min())
+
+
+# the reference's per-case strain limits (test_golden_regression.py:123, :176, :238, :297)
+STRAIN = {"case1": 1.15, "case2": 1.15, "case3": 1.20, "case4": 1.25}
+
+
+def golden_trajectory(sim_cls, case):
+    """Steps a simulator through a golden case and checks every criterion of
+    the reference's test_golden_regression.py:76-300 except case 2's
+    all-frame bound (test_case2_all_frame_bound).  Returns the largest
+    all-frame vertex error."""
+    import taremin_cloth_core as core
+    c, d, pos, inv = load(case)
+    s = make(sim_cls, case)
+    gp = d["positions"]
+    rest = _edge_len(pos, d["edges"])
+    nshort, tol_short = c["short"]
+    worst = 0.0
+    a = None
+    for fi in range(1, len(gp)):
+        s.step(1.0 / 60.0, 20, 2)
+        out = np.empty(len(pos) * 3, np.float32)
+        s.get_positions(out)
+        a = out.reshape(-1, 3)
+        assert not np.isnan(a).any()
+        diff = float(np.linalg.norm(a - gp[fi], axis=1).max())
+        worst = max(worst, diff)
+        if fi <= nshort:
+            assert diff < tol_short, f"{case} frame {fi}: {diff * 1e3:.4f} mm"
+        if c["full"] is not None and case != "case2":
+            assert diff < c["full"], f"{case} frame {fi}: {diff * 1e3:.4f} mm over all frames"
+        com = float(np.linalg.norm(a.mean(0) - gp[fi].mean(0)))
+        assert com < c["com"], f"{case} frame {fi}: centre of mass {com * 1e3:.3f} mm"
+        strain = float((_edge_len(a, d["edges"]) / np.maximum(rest, 1e-6)).max())
+        assert strain < STRAIN[case], f"{case} frame {fi}: strain {strain:.4f}"
+        if case == "case1":
+            pinned = inv == 0.0
+            assert float(np.linalg.norm(a[pinned] - pos[pinned], axis=1).max()) < 1e-5
+        if case == "case2":
+            assert float(np.linalg.norm(a - np.array([0, 0, 0.16], np.float32), axis=1).min()) >= 0.14 - 0.002
+        if case == "case3":
+            assert float(a[:, 2].min()) >= -0.002
+            assert float(np.linalg.norm(a - np.array([0, 0, 0.3], np.float32), axis=1).min()) >= 0.12 - 0.003
+            assert _segment_distance(a, [-0.3, -0.3, 0.4], [0.3, -0.3, 0.5]) >= 0.08 - 0.003
+            assert _segment_distance(a, [-0.3, 0.3, 0.5], [0.3, 0.3, 0.4]) >= 0.08 - 0.003
+        if case == "case4":
+            assert float(np.linalg.norm(a - np.array([0, 0, 0.2], np.float32), axis=1).min()) >= 0.20 - 0.003
+            if fi >= 20:
+                n_x = len(core.find_triangle_intersections(a, d["faces"]))
+                assert n_x <= 12, f"case4 frame {fi}: {n_x} self-intersections"
+    if case == "case4":
+        n_x = len(core.find_triangle_intersections(a, d["faces"]))
+        assert n_x <= 2, f"case4 final frame: {n_x} self-intersections"
+    return worst

@@ -79,3 +79,39 @@ def test_step_single_substep_equals_one_substep_frame():
     b.set_self_collision_options(enable_normal_untangling=False)
     assert not b.get_effective_normal_untangling()
     assert b.get_num_virtual_vertices() >= 0
+
+
+def test_config_json_roundtrip_and_hash():
+    """get_config_json / apply_config_json / get_config_hash (lib.rs:3029-3047,
+    config_impl.rs:16-160): a fresh simulator exports the constructor's
+    settings; a changed record applied to another simulator exports the same
+    text and hash; the hash follows every setter; bad text raises ValueError."""
+    import json
+    sc, s = _sheet()
+    d = json.loads(s.get_config_json())
+    assert d["gravity"] == [0.0, 0.0, -9.81] and d["damping"] == 1.0 and d["solver_iterations"] == 2
+    assert d["enable_self_collision"] is True and d["relief_factor"] == 0.2
+    # stiffness is exported from the stored f32 compliance 1/k (config_impl.rs:80-91)
+    back = lambda k: float(np.float32(1.0) / (np.float32(1.0) / np.float32(k)))  # noqa: E731
+    assert d["tension_stiffness"] == back(1000.0) and d["compression_stiffness"] == back(1000.0)
+    assert d["shear_stiffness"] == back(500.0) and d["bending_stiffness"] == back(10.0)
+    h0 = s.get_config_hash()
+    d.update(damping=2.5, tension_damping=3.0, solver_iterations=5, enable_edge_collision=True,
+             edge_margin_offset=0.002, strain_tolerance=0.01, areal_density=0.2, gravity=[0.0, -9.81, 0.0],
+             tension_stiffness=800.0, sewing_lock_distance=0.03)
+    s.apply_config_json(json.dumps(d))
+    text = s.get_config_json()
+    assert json.loads(text)["solver_iterations"] == 5 and json.loads(text)["gravity"] == [0.0, -9.81, 0.0]
+    assert s.get_config_hash() != h0
+    _, s2 = _sheet()
+    s2.apply_config_json(text)
+    assert s2.get_config_json() == text and s2.get_config_hash() == s.get_config_hash()
+    s2.set_damping(1.5)
+    assert s2.get_config_hash() != s.get_config_hash()
+    # absent fields take SimConfig::default
+    _, s3 = _sheet()
+    s3.apply_config_json("{}")
+    assert json.loads(s3.get_config_json())["tension_damping"] == 5.0
+    for bad in ("not json", "[1, 2]", '{"solver_iterations": -1}', '{"damping": "x"}'):
+        with pytest.raises(ValueError):
+            s3.apply_config_json(bad)

@@ -41,6 +41,18 @@ def test_golden_trajectories_match_oracle(oracle_lib, case):
     assert worst[:5].max() <= 1e-5, worst
 
 
+@pytest.mark.parametrize("case", ["case1", "case2", "case3", "case4"])
+def test_golden_regression_criteria(case):
+    """The reference's test_golden_regression.py:76-300 criteria on the CUDA path."""
+    gc.golden_trajectory(ClothSimulator, case)
+
+
+@pytest.mark.xfail(strict=True, reason="like the oracle, the CUDA path reaches about 19 mm (frame 25) against the "
+                                       "reference's 15 mm all-frame bound for case 2 (test_golden_regression.py:170)")
+def test_golden_case2_all_frame_bound():
+    assert gc.golden_trajectory(ClothSimulator, "case2") < 15e-3
+
+
 def test_config1_600_substeps(oracle_lib):
     sc = scenes.config1()
     g = scenes.build(ClothSimulator, sc)

@@ -55,3 +55,29 @@ def test_static_hash_build_rejects_oversize():
                                         C.c_void_p(dummy.data_ptr()), None)
         with pytest.raises(ValueError):
             _lib.check(status)
+
+
+def test_static_hash_build_empty_and_invalid_arguments():
+    import torch
+    from taremincloth_b200 import _lib
+    L = _lib.load()
+    # n = 0: every bucket empty, twice in a row (the second call sees the first's scratch)
+    for table in (1024, 4096):
+        status, cs, _ = _static_build(L, np.zeros((0, 3), np.float32), 0.01, table, torch)
+        _lib.check(status)
+        assert cs.shape == (table + 1,) and not cs.any()
+    buf = torch.zeros(64, dtype=torch.float32, device="cuda")
+    base = buf.data_ptr()
+    for cell in (0.0, -1.0, float("nan")):
+        status = L.tc_hash_build_static(C.c_void_p(base), 4, cell, 1024, C.c_void_p(base), C.c_void_p(base), None)
+        with pytest.raises(ValueError):
+            _lib.check(status)
+    # positions are read as float4 rows: a pointer off a 16-byte boundary is refused
+    status = L.tc_hash_build_static(C.c_void_p(base + 4), 4, 0.01, 1024, C.c_void_p(base), C.c_void_p(base), None)
+    with pytest.raises(ValueError):
+        _lib.check(status)
+    # a null sorted array with vertices to sort is refused
+    status = L.tc_hash_build_static(C.c_void_p(base), 4, 0.01, 1024, C.c_void_p(base), None, None)
+    with pytest.raises(ValueError):
+        _lib.check(status)
+    torch.cuda.synchronize()
