@@ -24,7 +24,8 @@ typedef enum {
   TC_ERR_INVALID = 1, /* bad shape / index / argument (PyO3 ValueError)  */
   TC_ERR_CUDA = 2,    /* device unavailable or CUDA failure (RuntimeError) */
   TC_ERR_NOMEM = 3,   /* device or host allocation failed                 */
-  TC_ERR_TIMEOUT = 4  /* a bounded device-side wait gave up               */
+  TC_ERR_TIMEOUT = 4, /* a bounded device-side wait gave up               */
+  TC_ERR_NONFINITE = 5 /* a checked read-back found NaN or Inf             */
 } tc_status;
 
 typedef struct tc_sim tc_sim;
@@ -337,6 +338,38 @@ tc_status tc_compute_combined_inv_masses(const float *positions, uint32_t n, con
 /* color_edge_pairs (coloring.rs:180-233, lib.rs:642-652), host only:
  * Welsh-Powell colours of vertex pairs, order (-degree, index). */
 tc_status tc_color_edge_pairs(uint32_t num_vertices, const uint32_t *pairs, uint32_t np, uint32_t *colors);
+/* Device health (crates/cloth_core/src/context.rs:101-140, test :499): a
+ * per-device lost flag and context epoch.  tc_mark_device_lost marks the
+ * device lost (anomaly handling, tests; host-side only).  The next
+ * simulator creation on that device re-initialises it (synchronise, epoch
+ * + 1, flag cleared; TC_ERR_CUDA when the device does not answer, which
+ * needs a fresh process).  Simulators created in an older epoch refuse every
+ * call with TC_ERR_CUDA; destroying them still works. */
+tc_status tc_mark_device_lost(int device);
+tc_status tc_device_status(int device, int *lost, uint64_t *epoch);
+/* Read-back sentinel (the NaN / Inf invariant of docs/architecture.md
+ * section 5): when on, tc_get_positions, tc_fetch_positions and
+ * tc_fetch_buffered_positions return TC_ERR_NONFINITE if the copied
+ * positions hold NaN or Inf (the copy is still written).  Off by default, as
+ * in the reference, whose read-backs return whatever the GPU holds. */
+tc_status tc_set_nonfinite_check(tc_sim *s, int enable);
+/* Narrow-phase pair lists of the direct self-collision pass, for parity
+ * (no counterpart in the reference's API; the passes are
+ * shaders/self_collision.wgsl:317-681 and
+ * shaders/self_collision_ee_direct.wgsl:266-776).  With recording on, every
+ * self-collision pass clears and refills two lists: the (vertex, triangle)
+ * pairs that pass the cheap tests of the vertex-triangle search (triangle
+ * ownership, swept bounds, two-hop exclusion) and reach the contact math,
+ * and the (edge, edge) pairs counted within max_search.  The pair-cache
+ * pass records none.  tc_get_pair_lists returns the latest pass's lists,
+ * canonical and sorted: V-T rows (vertex, a, b, c) with a < b < c the
+ * triangle's vertices, E-E rows (e0, e1) with e0 < e1; counts[0..1] are the
+ * list lengths.  A list longer than its recording capacity is
+ * TC_ERR_INVALID, as is an output array smaller than the list.  Recording
+ * adds one atomic per recorded pair. */
+tc_status tc_set_pair_recording(tc_sim *s, int enable, uint32_t max_vt_pairs, uint32_t max_ee_pairs);
+tc_status tc_get_pair_lists(tc_sim *s, uint32_t *vt, uint32_t vt_capacity, uint32_t *ee, uint32_t ee_capacity,
+                            uint32_t counts[2]);
 /* The settings record of the reference (SimConfig,
  * crates/cloth_core/src/config.rs:40-140, written by
  * simulation/config_impl.rs:16-78; cloth_py lib.rs:3029-3042).
@@ -465,7 +498,11 @@ tc_status tc_set_persistent_solver(tc_sim *s, int enable);
  * solver with blocks_per_sm (1..limit); 2 the cluster solver for batched
  * instances without self-collision (each thread-block cluster of 8 CTAs runs
  * a bin of whole instances through the frame, colour steps separated by the
- * cluster barrier; TC_ERR_INVALID when not applicable).  Used by the
+ * cluster barrier); 3 the staged cluster solver (the same bins with the
+ * bin's vertex records held in the cluster's shared memory for the whole
+ * frame, split into one slice per CTA and reached across CTAs through
+ * distributed shared memory; needs every instance within 8 x the per-CTA
+ * capacity).  TC_ERR_INVALID when a mode is not applicable.  Used by the
  * autotuner.  Results do not change. */
 tc_status tc_set_launch_config(tc_sim *s, int persistent, uint32_t blocks_per_sm);
 tc_status tc_get_launch_limits(tc_sim *s, uint32_t *max_blocks_per_sm, uint32_t *num_sms);

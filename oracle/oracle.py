@@ -65,6 +65,8 @@ def lib():
         L.ocl_set_enable_self_collision.argtypes = [P, C.c_int]
         L.ocl_set_coupled_collider.argtypes = [P, C.c_int]
         L.ocl_set_collider_options.argtypes = [P, C.c_int, C.c_int, C.c_float]
+        L.ocl_set_pair_recording.argtypes = [P, C.c_int]
+        L.ocl_get_pair_lists.argtypes = [P, P, C.c_size_t, P, C.c_size_t, P]
         L.ocl_set_self_collision_options.argtypes = [P, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int]
         L.ocl_add_sphere.argtypes = [P, fp, C.c_float, C.c_float, C.c_float]
         L.ocl_add_capsule.argtypes = [P, fp, fp, C.c_float, C.c_float, C.c_float]
@@ -279,6 +281,17 @@ class OracleSim:
         return int(c[0]), int(c[1]), vt[:int(c[2])], ee[:int(c[3])]
 
     # --- edge colliders -------------------------------------------------
+    def set_pair_recording(self, enable=True):
+        lib().ocl_set_pair_recording(self._h, int(bool(enable)))
+
+    def get_pair_lists(self):
+        cnt = np.zeros(2, _u)
+        lib().ocl_get_pair_lists(self._h, None, 0, None, 0, _ptr(cnt))
+        vt = np.zeros((max(int(cnt[0]), 1), 4), _u)
+        ee = np.zeros((max(int(cnt[1]), 1), 2), _u)
+        lib().ocl_get_pair_lists(self._h, _ptr(vt), vt.shape[0], _ptr(ee), ee.shape[0], _ptr(cnt))
+        return dict(vt=vt[:int(cnt[0])], ee=ee[:int(cnt[1])])
+
     def set_edge_collision(self, enable=True, margin_scale=1.0, margin_offset=0.0):
         lib().ocl_set_edge_collision(self._h, int(bool(enable)), margin_scale, margin_offset)
 

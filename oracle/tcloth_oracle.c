@@ -175,6 +175,10 @@ struct OSim {
     float cloth_thickness;
     int single_sided_recovery;
     int sc_interval, ee_interval; /* self-collision / E-E substep intervals (dispatch.rs:105-114) */
+    /* narrow-phase pair record of the latest self-collision pass (ocl_set_pair_recording) */
+    int rec;
+    uint32_t *rec_vt, *rec_ee;
+    size_t rec_vt_n, rec_vt_cap, rec_ee_n, rec_ee_cap;
     /* bone SDF colliders (collision.wgsl:116-265) */
     uint32_t *atlas; uint32_t aw, ah, ad; int nbones;
     float *binfo;   /* nbones x 20 */
@@ -1056,7 +1060,7 @@ void ocl_destroy(OSim *s) {
                     s->star_off, s->star_idx, s->edges, s->ebits, s->island, s->cols, s->tris,
                     s->bounds, s->pins, s->acc, s->nrm, s->cs, s->srt, s->ecs, s->esrt,
                     s->atlas, s->binfo, s->bxf, s->sew, s->sc_off, s->sc_cnt, s->slam, s->rep,
-                    s->ce, s->ce_cs, s->ce_srt, s->pvt, s->pee};
+                    s->ce, s->ce_cs, s->ce_srt, s->pvt, s->pee, s->rec_vt, s->rec_ee};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(s);
 }
@@ -2429,6 +2433,27 @@ static int near_folded_sq(const OSim *s, uint32_t a, uint32_t b, float d2) {
 static inline int cell_eq(const int32_t *a, int32_t x, int32_t y, int32_t z) { return a[0] == x && a[1] == y && a[2] == z; }
 
 /* sc_solve, shaders/self_collision.wgsl:317-681 */
+/* Pair record: rows appended from the parallel loops under a lock, put in
+ * canonical order when read (ocl_get_pair_lists). */
+static void rec_push(uint32_t **buf, size_t *n, size_t *cap, const uint32_t *row, int width) {
+    if (*n == *cap) {
+        *cap = *cap ? 2 * *cap : 1024;
+        *buf = (uint32_t *)realloc(*buf, *cap * (size_t)width * sizeof(uint32_t));
+    }
+    memcpy(*buf + *n * (size_t)width, row, (size_t)width * sizeof(uint32_t));
+    (*n)++;
+}
+static void rec_vt(OSim *s, uint32_t i, uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t row[4] = {i, a, b, c};
+#pragma omp critical(ocl_rec)
+    rec_push(&s->rec_vt, &s->rec_vt_n, &s->rec_vt_cap, row, 4);
+}
+static void rec_ee(OSim *s, uint32_t ea, uint32_t eb) {
+    uint32_t row[2] = {ea, eb};
+#pragma omp critical(ocl_rec)
+    rec_push(&s->rec_ee, &s->rec_ee_n, &s->rec_ee_cap, row, 2);
+}
+
 static void k_sc_solve(OSim *s, int untangle) {
     const float cs = s->cell;
 #pragma omp parallel for schedule(dynamic, 64)
@@ -2544,6 +2569,7 @@ static void k_sc_solve(OSim *s, int untangle) {
                     if (smin.x > tmax.x || smin.y > tmax.y || smin.z > tmax.z ||
                         smax.x < tmin.x || smax.y < tmin.y || smax.z < tmin.z) continue;
                     if (within2(s, index, v0) || within2(s, index, v1)) continue;
+                    if (s->rec) rec_vt(s, index, j, v0, v1);
                     v3 mv = vsub(pi, rel);
                     float msq = vdot(mv, mv);
                     float ht = 1.0f, hu = 0.0f, hv = 0.0f; int hit = 0;
@@ -2865,6 +2891,7 @@ static void k_ee(OSim *s, int untangle) {
                     amax.x < bmin.x || amax.y < bmin.y || amax.z < bmin.z) continue;
                 search++;
                 if (search > (uint32_t)s->max_search) { stop = 1; break; }
+                if (s->rec) rec_ee(s, ei, eb);
                 float w_j = s->w[j], w_vj = s->w[vj];
                 float thj = s->thick[j], thvj = s->thick[vj];
                 uint32_t lb = s->layer[j];
@@ -3650,6 +3677,7 @@ static void k_pair_ee(OSim *s, int untangle) {
  * runs the direct pass on the last substep. */
 static void self_collision(OSim *s, int run_ee, int sub, int substeps, float dt) {
     int untangle = s->untangle_opt && s->multi_layer;
+    s->rec_vt_n = s->rec_ee_n = 0;
     int force_direct = s->pair_cache && s->pair_fallback && sub + 1 == substeps;
     if (s->pair_cache && !force_direct) {
         if (untangle) k_normals(s);
@@ -3671,6 +3699,39 @@ static void self_collision(OSim *s, int run_ee, int sub, int substeps, float dt)
     if (untangle) k_untangle(s);
     if (run_ee && s->ne > 0) k_ee(s, untangle);
     k_apply(s);
+}
+void ocl_set_pair_recording(OSim *s, int on) {
+    s->rec = on != 0;
+    s->rec_vt_n = s->rec_ee_n = 0;
+}
+static int cmp_rows(const uint32_t *a, const uint32_t *b, int w) {
+    for (int k = 0; k < w; k++)
+        if (a[k] != b[k]) return a[k] < b[k] ? -1 : 1;
+    return 0;
+}
+static int cmp_row4(const void *a, const void *b) { return cmp_rows((const uint32_t *)a, (const uint32_t *)b, 4); }
+static int cmp_row2(const void *a, const void *b) { return cmp_rows((const uint32_t *)a, (const uint32_t *)b, 2); }
+static void sort3(uint32_t *r) {
+    uint32_t t;
+    if (r[0] > r[1]) { t = r[0]; r[0] = r[1]; r[1] = t; }
+    if (r[1] > r[2]) { t = r[1]; r[1] = r[2]; r[2] = t; }
+    if (r[0] > r[1]) { t = r[0]; r[0] = r[1]; r[1] = t; }
+}
+/* the latest pass's lists: V-T rows (vertex, a < b < c), E-E rows (e0 < e1),
+ * each sorted; counts[0..1] are their lengths, rows past the capacities are
+ * left out */
+void ocl_get_pair_lists(OSim *s, uint32_t *vt, size_t vt_cap, uint32_t *ee, size_t ee_cap, uint32_t counts[2]) {
+    for (size_t i = 0; i < s->rec_vt_n; i++) sort3(s->rec_vt + 4 * i + 1);
+    for (size_t i = 0; i < s->rec_ee_n; i++) {
+        uint32_t *r = s->rec_ee + 2 * i;
+        if (r[0] > r[1]) { uint32_t t = r[0]; r[0] = r[1]; r[1] = t; }
+    }
+    if (s->rec_vt_n) qsort(s->rec_vt, s->rec_vt_n, 16, cmp_row4);
+    if (s->rec_ee_n) qsort(s->rec_ee, s->rec_ee_n, 8, cmp_row2);
+    counts[0] = (uint32_t)s->rec_vt_n;
+    counts[1] = (uint32_t)s->rec_ee_n;
+    if (vt) memcpy(vt, s->rec_vt, (s->rec_vt_n < vt_cap ? s->rec_vt_n : vt_cap) * 16);
+    if (ee) memcpy(ee, s->rec_ee, (s->rec_ee_n < ee_cap ? s->rec_ee_n : ee_cap) * 8);
 }
 /* set_enable_pair_cache / set_enable_pair_cache_final_fallback
  * (simulation/mod.rs:805-810, :852-854) */

@@ -74,6 +74,11 @@ void ocl_set_pin(OSim *s, uint32_t v, const float *target, float w);
 void ocl_clear_pins(OSim *s);
 void ocl_set_coupled_collider(OSim *s, int on);
 void ocl_set_collider_options(OSim *s, int cluster, int recovery, float sweep);
+/* narrow-phase pair record of the direct self-collision pass: V-T pairs that
+ * pass the cheap tests (self_collision.wgsl:477-520), E-E pairs counted within
+ * max_search (self_collision_ee_direct.wgsl:330-360) */
+void ocl_set_pair_recording(OSim *s, int on);
+void ocl_get_pair_lists(OSim *s, uint32_t *vt, size_t vt_cap, uint32_t *ee, size_t ee_cap, uint32_t counts[2]);
 
 /* time stepping: GpuClothSimulator::step (simulation/dispatch.rs:610-671) */
 void ocl_step(OSim *s, float dt, int substeps);

@@ -12,7 +12,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtcloth.so")
 
-TC_OK, TC_ERR_INVALID, TC_ERR_CUDA, TC_ERR_NOMEM, TC_ERR_TIMEOUT = range(5)
+TC_OK, TC_ERR_INVALID, TC_ERR_CUDA, TC_ERR_NOMEM, TC_ERR_TIMEOUT, TC_ERR_NONFINITE = range(6)
 
 _P = C.c_void_p
 _U = C.c_uint32
@@ -44,6 +44,11 @@ SIGNATURES = {
     "tc_set_enable_edge_collision": [_P, _I],
     "tc_compute_combined_inv_masses": [_P, _U, _P, _U, _P, _U, _P, _U, _F, _F, _P],
     "tc_color_edge_pairs": [_U, _P, _U, _P],
+    "tc_set_pair_recording": [_P, _I, _U, _U],
+    "tc_mark_device_lost": [_I],
+    "tc_device_status": [_I, C.POINTER(_I), C.POINTER(C.c_uint64)],
+    "tc_set_nonfinite_check": [_P, _I],
+    "tc_get_pair_lists": [_P, _P, _U, _P, _U, _P],
     "tc_get_config_json": [_P, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)],
     "tc_get_config_hash": [_P, C.POINTER(C.c_uint64)],
     "tc_set_workgroup_size": [_P, _U],
@@ -208,4 +213,6 @@ def check(status: int) -> None:
         raise BarrierTimeout(msg)
     if status == TC_ERR_NOMEM:
         raise MemoryError(msg)
+    if status == TC_ERR_NONFINITE:
+        raise FloatingPointError(msg)
     raise RuntimeError(msg)

@@ -3,7 +3,8 @@
 Tries the launch-per-colour path, the persistent solver at every
 blocks-per-SM value the occupancy allows and, for batched instances without
 self-collision, the cluster solver (one thread-block cluster per bin of
-instances); times a few frames of each with CUDA events, keeps the fastest
+instances) and the staged cluster solver (the same bins, vertex records in
+the clusters' shared memory); times a few frames of each with CUDA events, keeps the fastest
 and restores the simulation state after every trial (the settings never
 change results, only speed).
 
@@ -20,11 +21,12 @@ def autotune(sim, dt, substeps, frames=3, verbose=False):
     x, v = x.copy(), v.copy()
     max_per_sm, _ = sim.get_launch_limits()
     trials = [(False, 0)] + [(True, b) for b in range(1, min(max_per_sm, 4) + 1)]
-    try:
-        sim.set_launch_config(2, 1)
-        trials.append((2, 0))
-    except ValueError:
-        pass
+    for mode in (2, 3):  # cluster solver, staged cluster solver
+        try:
+            sim.set_launch_config(mode, 1)
+            trials.append((mode, 0))
+        except ValueError:
+            pass
     results = []
     for persistent, bps in trials:
         sim.set_launch_config(persistent, bps if persistent is True else 1)

@@ -67,7 +67,24 @@ struct SCArgs {
   uint2* ccd_q;
   uint32_t* ccd_n;
   uint32_t ccd_cap;
+  // optional record of the narrow-phase input (null when off): the
+  // (vertex, triangle) pairs that pass the cheap tests of sc_solve and the
+  // (edge, edge) pairs counted within max_search; rec_n[0] / rec_n[1] count
+  // them, entries past the capacities are dropped
+  uint4* rec_vt;
+  uint2* rec_ee;
+  uint32_t* rec_n;
+  uint32_t rec_vt_cap, rec_ee_cap;
 };
+
+__device__ __forceinline__ void record_vt(const SCArgs& s, uint32_t i, uint32_t a, uint32_t b, uint32_t c) {
+  const uint32_t k = atomicAdd(&s.rec_n[0], 1u);
+  if (k < s.rec_vt_cap) s.rec_vt[k] = make_uint4(i, a, b, c);
+}
+__device__ __forceinline__ void record_ee(const SCArgs& s, uint32_t ea, uint32_t eb) {
+  const uint32_t k = atomicAdd(&s.rec_n[1], 1u);
+  if (k < s.rec_ee_cap) s.rec_ee[k] = make_uint2(ea, eb);
+}
 
 // A vertex's sorted two-hop list (and rest lengths), in shared memory when it
 // fits, else in global memory; binary search as in
@@ -809,6 +826,10 @@ __global__ void __launch_bounds__(256, 4) k_sc_solve(SCArgs s) {
           ps = pr_slot[warp][lo];
           pst = pr_sb[warp][lo] + (e - pr_ex[warp][lo]);
           pass = vt_entry<false>(s, c, th, ps, pst, pr_rec0[warp][lo], pr_rec1[warp][lo]);
+          if (pass && s.rec_vt) {
+            const uint2 tv = s.star_idx[pst];
+            record_vt(s, index, __float_as_uint(pr_rec1[warp][lo].w), tv.x, tv.y);
+          }
         }
         const uint32_t b = __ballot_sync(0xffffffffu, pass);
         if (pass) {
@@ -1367,6 +1388,7 @@ __global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
       const uint32_t eb = (uint32_t)s.es_c[slot].w;
       const uint2 ebv = s.es_v[slot];
       const float4 qj = s.p4[ebv.x], qvj = s.p4[ebv.y], xj = s.x4[ebv.x], xvj = s.x4[ebv.y];
+      if (s.rec_ee) record_ee(s, ei, eb);
       ee_pair(s, c, th0, th1, eb, ebv.x, ebv.y, qj, qvj, xj, xvj, true);
     }
     __syncwarp();

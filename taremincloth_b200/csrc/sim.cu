@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <new>
 #include <stdexcept>
@@ -470,6 +471,8 @@ struct WarmStart {
 
 struct Sim {
   int device = 0;
+  uint64_t epoch = 0;       // device-context epoch at creation (device health below)
+  bool nonfinite_check = false;  // read-backs refuse non-finite positions
   cudaStream_t st = nullptr;
   MeshData m;
   uint32_t n = 0, nd = 0, nb = 0, ne = 0;
@@ -593,6 +596,17 @@ struct Sim {
   uint32_t cl_bins = 0;
   DBuf<uint2> cl_vrange, cl_pins, cl_dist, cl_bend;
   DBuf<uint32_t> cl_dperm, cl_bperm;
+  // staged cluster solver: the same bins with each bin's vertex records in
+  // the shared memory of its cluster (k_solver_staged); st_cap vertices per
+  // CTA slice, kStageCtas slices per bin
+  static constexpr uint32_t kStageCtas = 8;
+  static constexpr uint32_t kStageThreads = 512;
+  bool stage_mode = false, st_stale = true;
+  int st_max_active = 0;
+  uint32_t st_cap = 0, st_bins = 0;
+  size_t st_smem = 0;
+  DBuf<uint2> st_vrange, st_pins;
+  DBuf<uint32_t> st_dist, st_bend, st_dperm, st_bperm;
   std::vector<uint2> inst_prims_h;
   DBuf<uint32_t> vinst;
   DBuf<uint2> inst_prims;
@@ -979,6 +993,33 @@ struct Sim {
         }
         cl_max_active = ncl;
       }
+      {  // staged cluster solver: slice capacity from the opt-in shared memory, co-resident clusters
+        int optin = 0;
+        TC_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        st_cap = uint32_t(optin) / (3u * sizeof(float4));
+        st_smem = size_t(st_cap) * 3u * sizeof(float4);
+        int ncl = 0;
+        if (st_cap > 0 &&
+            cudaFuncSetAttribute(k_solver_staged<kStageCtas, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(st_smem)) == cudaSuccess &&
+            cudaFuncSetAttribute(k_solver_staged<kStageCtas, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(st_smem)) == cudaSuccess) {
+          cudaLaunchConfig_t cfg = {};
+          cfg.gridDim = dim3(kStageCtas * 16);
+          cfg.blockDim = dim3(kStageThreads);
+          cfg.dynamicSmemBytes = st_smem;
+          cudaLaunchAttribute attr[1];
+          attr[0].id = cudaLaunchAttributeClusterDimension;
+          attr[0].val.clusterDim.x = kStageCtas;
+          attr[0].val.clusterDim.y = 1;
+          attr[0].val.clusterDim.z = 1;
+          cfg.attrs = attr;
+          cfg.numAttrs = 1;
+          if (cudaOccupancyMaxActiveClusters(&ncl, k_solver_staged<kStageCtas, false>, &cfg) != cudaSuccess) ncl = 0;
+        }
+        cudaGetLastError();
+        st_max_active = ncl;
+      }
       num_sms = unsigned(nsm);
       if (!persist_blocks) persistent = false;
     }
@@ -1091,6 +1132,7 @@ struct Sim {
   // ---- pins
   void upload_pins() {
     cl_stale = true;
+    st_stale = true;
     std::vector<uint32_t> v;
     std::vector<float4> t;
     for (const auto& kv : pins) {
@@ -1139,8 +1181,19 @@ struct Sim {
     a.vcell = vcell.p; a.mlen = mlen.p; a.ecell = ecell.p; a.eamin = eamin.p; a.eamax = eamax.p;
     a.ccd_q = ccd_q.p; a.ccd_n = ccd_n.p; a.ccd_cap = uint32_t(ccd_q.n);
     a.vs_p = vs_p.p; a.vs_q = vs_q.p; a.vs_c = vs_c.p; a.es_c = es_c.p; a.es_v = es_v.p; a.es_lo = es_lo.p; a.es_hi = es_hi.p;
+    a.rec_vt = rec_pairs ? rec_vt.p : nullptr;
+    a.rec_ee = rec_pairs ? rec_ee.p : nullptr;
+    a.rec_n = rec_pairs ? rec_n.p : nullptr;
+    a.rec_vt_cap = rec_pairs ? rec_vt_cap : 0u;
+    a.rec_ee_cap = rec_pairs ? rec_ee_cap : 0u;
     return a;
   }
+  // narrow-phase pair record of the latest self-collision pass (off by default)
+  bool rec_pairs = false;
+  DBuf<uint4> rec_vt;
+  DBuf<uint2> rec_ee;
+  DBuf<uint32_t> rec_n;
+  uint32_t rec_vt_cap = 0, rec_ee_cap = 0;
 
   static unsigned grid(uint32_t cnt, unsigned b) { return (cnt + b - 1) / b; }
 
@@ -1233,6 +1286,7 @@ struct Sim {
   }
 
   void encode_self_collision(bool run_ee, uint32_t s, uint32_t substeps, float dt) {
+    if (rec_pairs) TC_CK(cudaMemsetAsync(rec_n.p, 0, 2 * sizeof(uint32_t), st));
     const bool force_direct = pair_cache && pair_final_fallback && s + 1 == substeps;
     if (pair_cache && !force_direct) {
       encode_pair_self_collision(run_ee, s == 0, dt);
@@ -1485,6 +1539,111 @@ struct Sim {
     cfg.numAttrs = 1;
     if (a.ca.bone.nbones > 0) TC_CK(cudaLaunchKernelEx(&cfg, k_solver_cluster<true>, a, t));
     else TC_CK(cudaLaunchKernelEx(&cfg, k_solver_cluster<false>, a, t));
+  }
+  // the staged solver applies where the cluster solver does and every
+  // instance fits the shared memory of one cluster
+  bool can_stage() const {
+    if (!can_cluster() || st_max_active <= 0 || st_cap == 0) return false;
+    for (size_t k = 0; k + 1 < inst_vert_off.size(); ++k)
+      if (inst_vert_off[k + 1] - inst_vert_off[k] > kStageCtas * st_cap) return false;
+    return true;
+  }
+  // bins: contiguous runs of instances balanced by vertex count (at least
+  // as many as fit on the device at once, more while a bin is over a
+  // cluster's capacity); each bin's range is cut into kStageCtas slices and
+  // each (bin, colour) constraint range is ordered by the slice that owns
+  // the constraint's first vertex
+  void build_stage_tables() {
+    const uint32_t K = kStageCtas;
+    const uint32_t ninst = uint32_t(inst_vert_off.size() - 1);
+    const uint64_t bin_cap = uint64_t(K) * st_cap;
+    std::vector<uint32_t> bin_of_inst(ninst);
+    uint32_t B = std::max(1u, std::min(ninst, uint32_t(st_max_active)));
+    for (;; ++B) {
+      const uint64_t target = (uint64_t(n) + B - 1) / B;
+      std::vector<uint64_t> size(B, 0);
+      for (uint32_t k = 0; k < ninst; ++k) {
+        const uint64_t mid = uint64_t(inst_vert_off[k]) + (inst_vert_off[k + 1] - inst_vert_off[k]) / 2;
+        bin_of_inst[k] = uint32_t(std::min<uint64_t>(B - 1, mid / std::max<uint64_t>(target, 1)));
+        size[bin_of_inst[k]] += inst_vert_off[k + 1] - inst_vert_off[k];
+      }
+      if (*std::max_element(size.begin(), size.end()) <= bin_cap || B >= ninst) break;
+    }
+    std::vector<uint2> vr(B, make_uint2(0, 0));
+    std::vector<char> seen(B, 0);
+    for (uint32_t k = 0; k < ninst; ++k) {
+      const uint32_t b = bin_of_inst[k];
+      if (!seen[b]) { vr[b] = make_uint2(inst_vert_off[k], inst_vert_off[k + 1]); seen[b] = 1; }
+      else vr[b].y = inst_vert_off[k + 1];
+    }
+    for (uint32_t b = 0; b < B; ++b)
+      if (!seen[b]) vr[b] = make_uint2(b ? vr[b - 1].y : 0u, b ? vr[b - 1].y : 0u);
+    std::vector<uint32_t> bin_of_v(n), owner(n);
+    for (uint32_t b = 0; b < B; ++b) {
+      const uint32_t nv = vr[b].y - vr[b].x, chunk = nv ? (nv + K - 1) / K : 1u;
+      for (uint32_t v = vr[b].x; v < vr[b].y; ++v) {
+        bin_of_v[v] = b;
+        owner[v] = (v - vr[b].x) / chunk;
+      }
+    }
+    std::vector<uint32_t> pv;
+    std::vector<uint2> pr(size_t(B) * K, make_uint2(0, 0));
+    for (const auto& kv : pins) pv.push_back(kv.first);  // pin_v order: ascending vertex
+    for (uint32_t q = 0; q < uint32_t(pv.size());) {
+      const uint32_t slot = bin_of_v[pv[q]] * K + owner[pv[q]];
+      uint32_t e = q;
+      while (e < pv.size() && bin_of_v[pv[e]] * K + owner[pv[e]] == slot) ++e;
+      pr[slot] = make_uint2(q, e - q);
+      q = e;
+    }
+    auto perm_of = [&](const std::vector<uint32_t>& off, const std::vector<uint32_t>& cnt, auto vert_of,
+                       std::vector<uint32_t>& perm, std::vector<uint32_t>& tab) {
+      const uint32_t nc = uint32_t(off.size());
+      std::vector<std::vector<uint32_t>> bucket(size_t(B) * nc * K);
+      for (uint32_t c = 0; c < nc; ++c)
+        for (uint32_t k = off[c]; k < off[c] + cnt[c]; ++k) {
+          const uint32_t v = vert_of(k);
+          bucket[(size_t(bin_of_v[v]) * nc + c) * K + owner[v]].push_back(k);
+        }
+      perm.clear();
+      tab.assign(size_t(B) * nc * (K + 1), 0u);
+      for (size_t bc = 0; bc < size_t(B) * nc; ++bc) {
+        for (uint32_t r = 0; r < K; ++r) {
+          tab[bc * (K + 1) + r] = uint32_t(perm.size());
+          perm.insert(perm.end(), bucket[bc * K + r].begin(), bucket[bc * K + r].end());
+        }
+        tab[bc * (K + 1) + K] = uint32_t(perm.size());
+      }
+    };
+    std::vector<uint32_t> dperm, bperm, dtab, btab;
+    perm_of(m.dist_off, m.dist_cnt, [&](uint32_t k) { return dist_h[k].v0; }, dperm, dtab);
+    perm_of(m.bend_off, m.bend_cnt, [&](uint32_t k) { return bend_h[k].v0; }, bperm, btab);
+    st_vrange.upload(vr, st);
+    st_pins.upload(pr, st);
+    st_dist.upload(dtab, st);
+    st_bend.upload(btab, st);
+    st_dperm.upload(dperm, st);
+    st_bperm.upload(bperm, st);
+    TC_CK(cudaStreamSynchronize(st));
+    st_bins = B;
+    st_stale = false;
+  }
+  void launch_staged(const SolverArgs& a) {
+    const StageTables t{st_vrange.p, st_pins.p, st_dist.p, st_bend.p, st_dperm.p, st_bperm.p, st_cap};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(st_bins * kStageCtas);
+    cfg.blockDim = dim3(kStageThreads);
+    cfg.dynamicSmemBytes = st_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kStageCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (a.ca.bone.nbones > 0) TC_CK(cudaLaunchKernelEx(&cfg, k_solver_staged<kStageCtas, true>, a, t));
+    else TC_CK(cudaLaunchKernelEx(&cfg, k_solver_staged<kStageCtas, false>, a, t));
   }
   // the persistent path is available: cooperative launch, and with bone
   // colliders the bone instantiation fits on an SM
@@ -1757,6 +1916,12 @@ struct Sim {
       encode_frame_ws(dt, substeps, use_coupled);
       return;
     }
+    if (stage_mode && can_stage() && !st_stale && !profiling && !track_residual && !ws_recording()) {
+      const SubstepParams sp = make_sp(dt / float(substeps));
+      launch_staged(solver_args(sp, substeps, use_coupled, true));
+      TC_CK(cudaGetLastError());
+      return;
+    }
     if (cluster_mode && can_cluster() && !cl_stale && !profiling && !track_residual && !ws_recording()) {
       const SubstepParams sp = make_sp(dt / float(substeps));
       launch_cluster(solver_args(sp, substeps, use_coupled, true));
@@ -1854,6 +2019,7 @@ struct Sim {
   void launch_frame(float dt, uint32_t substeps) {
     if (n == 0) return;
     if (cluster_mode && can_cluster() && cl_stale) build_cluster_tables();  // before any capture
+    if (stage_mode && can_stage() && st_stale) build_stage_tables();        // before any capture
     if (edge_active()) ensure_collider_edges();                             // before any capture
     // the frame's device time (last_frame_ms) includes the dynamic bone SDF rebake
     TC_CK(cudaEventRecord(ev0, st));
@@ -2108,10 +2274,58 @@ static tc_status guard(F&& f) {
 static void need(bool ok, const char* msg) {
   if (!ok) throw TcError(TC_ERR_INVALID, msg);
 }
+// ---- device health (crates/cloth_core/src/context.rs:101-140): a per-device
+// "lost" flag and context epoch.  A device marked lost is re-initialised by
+// the next simulator creation on it (epoch + 1); simulators of an older epoch
+// refuse every call with TC_ERR_CUDA and must be re-created.  Marking is
+// host-side (tc_mark_device_lost) and never touches the GPU; re-initialising
+// synchronises the device and gives up when it does not answer, since a real
+// sticky fault needs a fresh process.
+namespace {
+struct DeviceHealth {
+  std::atomic<bool> lost{false};
+  std::atomic<uint64_t> epoch{1};
+};
+DeviceHealth g_health[64];
+std::mutex g_health_mu;
+DeviceHealth& health(int dev) {
+  if (dev < 0 || dev >= 64) throw TcError(TC_ERR_CUDA, "device index out of range");
+  return g_health[dev];
+}
+uint64_t acquire_device(int dev) {
+  DeviceHealth& h = health(dev);
+  if (!h.lost.load()) return h.epoch.load();
+  std::lock_guard<std::mutex> lk(g_health_mu);
+  if (h.lost.load()) {
+    TC_CK(cudaSetDevice(dev));
+    cudaGetLastError();
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess)
+      throw TcError(TC_ERR_CUDA, std::string("device lost and not recoverable in this process: ") +
+                                     cudaGetErrorString(e));
+    h.epoch.fetch_add(1);
+    h.lost.store(false);
+  }
+  return h.epoch.load();
+}
+}  // namespace
+
 static Sim& S(tc_sim* s) {
   need(s != nullptr, "null simulator handle");
+  DeviceHealth& h = health(s->s.device);
+  if (h.lost.load() || h.epoch.load() != s->s.epoch)
+    throw TcError(TC_ERR_CUDA, "the device of this simulator was lost (context epoch " + std::to_string(s->s.epoch) +
+                                   ", now " + std::to_string(h.epoch.load()) + (h.lost.load() ? ", lost" : "") +
+                                   "); create a new simulator");
   TC_CK(cudaSetDevice(s->s.device));
   return s->s;
+}
+// read-back guard: with the check on, non-finite positions are an error
+static void check_finite(const Sim& m, const float* out, size_t count) {
+  if (!m.nonfinite_check) return;
+  for (size_t i = 0; i < count; ++i)
+    if (!std::isfinite(out[i]))
+      throw TcError(TC_ERR_NONFINITE, "non-finite position at vertex " + std::to_string(i / 3));
 }
 
 extern "C" {
@@ -2183,8 +2397,10 @@ tc_status tc_create_sewn(tc_sim** out, const float* positions, uint32_t n, const
     in.sew = sewing; in.nsew = nsew; in.sew_shrink_speed = sewing_shrink_speed;
     in.sew_stiffness = std::isnan(sewing_stiffness) ? 10000.0f : sewing_stiffness;
     in.sew_lock = enable_sewing_lock != 0;
+    const uint64_t epoch = acquire_device(device);
     std::unique_ptr<tc_sim> h(new tc_sim);
     h->s.init(in, device);
+    h->s.epoch = epoch;
     if (!std::isnan(sewing_lock_distance)) h->s.sew_lock_dist = std::fmax(sewing_lock_distance, 0.f);
     *out = h.release();
   });
@@ -2229,9 +2445,11 @@ tc_status tc_batch_create(tc_sim** out, uint32_t ninst, const uint32_t* vcount, 
     in.faces = NF ? gf.data() : nullptr; in.nf = uint32_t(NF);
     in.inv_masses = inv_masses; in.layer_ids = layers.data(); in.thickness = thickness;
     in.tension_k = in.compression_k = in.shear_k = in.bending_k = 1000.f;
+    const uint64_t epoch = acquire_device(device);
     std::unique_ptr<tc_sim> h(new tc_sim);
     Sim& m = h->s;
     m.init(in, device);
+    m.epoch = epoch;
     m.self_collision = false;
     // per-instance compliances (tension, compression, shear, bending)
     std::vector<uint32_t> vi(N);
@@ -2331,6 +2549,7 @@ tc_status tc_fetch_positions(tc_sim* s, float* out, size_t out_len, int* ok) {
     need(out != nullptr && out_len >= size_t(m.n) * 3, "out_array too small");
     m.get_positions(out);
     m.async_pending = false;
+    check_finite(m, out, size_t(m.n) * 3);
     m.check_barrier_status();
     m.consume_feedback();
     float md = 0.f;
@@ -2382,6 +2601,7 @@ tc_status tc_fetch_buffered_positions(tc_sim* s, float* out, size_t out_len, uin
     }
     m.buffered = 0;
     *count = c;
+    check_finite(m, out, len);
   });
 }
 
@@ -2390,7 +2610,22 @@ tc_status tc_get_positions(tc_sim* s, float* out, size_t out_len) {
     Sim& m = S(s);
     need(out != nullptr && out_len >= size_t(m.n) * 3, "output array too small");
     m.get_positions(out);
+    check_finite(m, out, size_t(m.n) * 3);
   });
+}
+
+tc_status tc_mark_device_lost(int device) {
+  return guard([&] { health(device).lost.store(true); });
+}
+tc_status tc_device_status(int device, int* lost, uint64_t* epoch) {
+  return guard([&] {
+    DeviceHealth& h = health(device);
+    if (lost) *lost = h.lost.load() ? 1 : 0;
+    if (epoch) *epoch = h.epoch.load();
+  });
+}
+tc_status tc_set_nonfinite_check(tc_sim* s, int enable) {
+  return guard([&] { S(s).nonfinite_check = enable != 0; });
 }
 
 tc_status tc_set_positions_and_velocities(tc_sim* s, const float* pos, const float* vel, uint32_t n) {
@@ -3132,9 +3367,20 @@ tc_status tc_set_launch_config(tc_sim* s, int persistent, uint32_t blocks_per_sm
       need(m.can_cluster(), "the cluster solver needs batched instances, no self-collision and cluster launch");
       m.cluster_mode = true;
       m.cl_stale = true;
+      m.stage_mode = false;
       m.mark();
       return;
     }
+    if (persistent == 3) {  // staged cluster solver (the same, vertex records in shared memory)
+      need(m.can_stage(), "the staged solver needs batched instances, no self-collision, cluster launch and "
+                          "every instance within one cluster's shared memory");
+      m.stage_mode = true;
+      m.st_stale = true;
+      m.cluster_mode = false;
+      m.mark();
+      return;
+    }
+    m.stage_mode = false;
     if (persistent) {
       need(m.persist_max_per_sm > 0, "cooperative launch is not available on this device");
       need(blocks_per_sm >= 1 && blocks_per_sm <= m.persist_max_per_sm, "blocks_per_sm out of the occupancy range");
@@ -4009,6 +4255,55 @@ tc_status tc_bake_get(tc_bake* b, uint32_t* texels, float* infos, uint32_t* acti
 tc_status tc_bake_destroy(tc_bake* b) {
   delete b;
   return TC_OK;
+}
+
+// ---- narrow-phase pair lists of the direct self-collision pass
+tc_status tc_set_pair_recording(tc_sim* s, int enable, uint32_t max_vt_pairs, uint32_t max_ee_pairs) {
+  return guard([&] {
+    Sim& m = S(s);
+    if (enable) {
+      need(max_vt_pairs > 0 && max_ee_pairs > 0, "pair record capacities must be positive");
+      m.rec_vt.alloc(max_vt_pairs);
+      m.rec_ee.alloc(max_ee_pairs);
+      m.rec_n.alloc(2);
+      m.rec_vt_cap = max_vt_pairs;
+      m.rec_ee_cap = max_ee_pairs;
+      TC_CK(cudaMemsetAsync(m.rec_n.p, 0, 2 * sizeof(uint32_t), m.st));
+    }
+    m.rec_pairs = enable != 0;
+    m.mark();
+  });
+}
+tc_status tc_get_pair_lists(tc_sim* s, uint32_t* vt, uint32_t vt_capacity, uint32_t* ee, uint32_t ee_capacity,
+                            uint32_t counts[2]) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(counts != nullptr, "counts required");
+    need(m.rec_pairs, "pair recording is off (tc_set_pair_recording)");
+    uint32_t c[2];
+    TC_CK(cudaMemcpyAsync(c, m.rec_n.p, sizeof c, cudaMemcpyDeviceToHost, m.st));
+    TC_CK(cudaStreamSynchronize(m.st));
+    counts[0] = c[0];
+    counts[1] = c[1];
+    need(c[0] <= m.rec_vt_cap && c[1] <= m.rec_ee_cap,
+         "the pair record overflowed its capacity; enable it again with larger capacities");
+    need(vt_capacity >= c[0] || vt == nullptr, "vt output too small for the recorded pairs");
+    need(ee_capacity >= c[1] || ee == nullptr, "ee output too small for the recorded pairs");
+    if (vt && c[0]) {
+      std::vector<std::array<uint32_t, 4>> h(c[0]);
+      TC_CK(cudaMemcpy(h.data(), m.rec_vt.p, size_t(c[0]) * 16, cudaMemcpyDeviceToHost));
+      for (auto& r : h) std::sort(r.begin() + 1, r.end());
+      std::sort(h.begin(), h.end());
+      std::memcpy(vt, h.data(), size_t(c[0]) * 16);
+    }
+    if (ee && c[1]) {
+      std::vector<std::array<uint32_t, 2>> h(c[1]);
+      TC_CK(cudaMemcpy(h.data(), m.rec_ee.p, size_t(c[1]) * 8, cudaMemcpyDeviceToHost));
+      for (auto& r : h) std::sort(r.begin(), r.end());
+      std::sort(h.begin(), h.end());
+      std::memcpy(ee, h.data(), size_t(c[1]) * 8);
+    }
+  });
 }
 
 // ---- settings record (simulation/config_impl.rs, cloth_py lib.rs:3029-3047)

@@ -36,6 +36,25 @@ __device__ __forceinline__ float ld1(const float* p) {
   if constexpr (kCg) return __ldcg(p); else return *p;
 }
 
+// Where a per-element function reads and writes the vertex records.  GMem:
+// the global arrays (kCg: loads through L2, for launches in which other
+// blocks write the same records between barriers).  The staged cluster
+// solver passes a policy over its shared-memory slices instead; the
+// arithmetic is the same either way.
+template <bool kCgLoads>
+struct GMem {
+  static constexpr bool kCg = kCgLoads;
+  float4* x4;
+  float4* p4;
+  float4* v4;
+  __device__ __forceinline__ float4 ldx(uint32_t i) const { return ld4<kCg>(x4 + i); }
+  __device__ __forceinline__ float4 ldp(uint32_t i) const { return ld4<kCg>(p4 + i); }
+  __device__ __forceinline__ float4 ldv(uint32_t i) const { return ld4<kCg>(v4 + i); }
+  __device__ __forceinline__ void stx(uint32_t i, float4 v) const { x4[i] = v; }
+  __device__ __forceinline__ void stp(uint32_t i, float4 v) const { p4[i] = v; }
+  __device__ __forceinline__ void stv(uint32_t i, float4 v) const { v4[i] = v; }
+};
+
 struct SubstepParams {
   float dt;       // substep dt (already max(dt, 1e-8) where the shaders do so)
   float gx, gy, gz;
@@ -44,10 +63,9 @@ struct SubstepParams {
 };
 
 // shaders/predict.wgsl:33-55
-template <bool kCg>
-__device__ __forceinline__ void predict_vertex(uint32_t i, const float4* __restrict__ x4, float4* __restrict__ p4,
-                                               float4* __restrict__ v4, const SubstepParams& sp) {
-  float4 x = ld4<kCg>(x4 + i), p = ld4<kCg>(p4 + i), v = ld4<kCg>(v4 + i);
+template <class M>
+__device__ __forceinline__ void predict_vertex_m(uint32_t i, const M& m, const SubstepParams& sp) {
+  float4 x = m.ldx(i), p = m.ldp(i), v = m.ldv(i);
   const float dt = fmaxf(sp.dt, 1e-8f);
   if (x.w <= 0.0f) {
     v.x = 0.f; v.y = 0.f; v.z = 0.f;
@@ -59,8 +77,13 @@ __device__ __forceinline__ void predict_vertex(uint32_t i, const float4* __restr
     v.x = vv.x; v.y = vv.y; v.z = vv.z;
     p.x = pp.x; p.y = pp.y; p.z = pp.z;
   }
-  p4[i] = p;
-  v4[i] = v;
+  m.stp(i, p);
+  m.stv(i, v);
+}
+template <bool kCg>
+__device__ __forceinline__ void predict_vertex(uint32_t i, const float4* __restrict__ x4, float4* __restrict__ p4,
+                                               float4* __restrict__ v4, const SubstepParams& sp) {
+  predict_vertex_m(i, GMem<kCg>{const_cast<float4*>(x4), p4, v4}, sp);
 }
 __global__ void k_predict(uint32_t n, const float4* __restrict__ x4, float4* __restrict__ p4,
                           float4* __restrict__ v4, SubstepParams sp) {
@@ -71,19 +94,18 @@ __global__ void k_predict(uint32_t n, const float4* __restrict__ x4, float4* __r
 }
 
 // shaders/pin.wgsl:56-92; pins are on distinct vertices, so order is free
-template <bool kCg>
-__device__ __forceinline__ void pin_one(uint32_t k, const uint32_t* __restrict__ pin_v,
-                                        const float4* __restrict__ pin_t, const float4* __restrict__ x4,
-                                        float4* __restrict__ p4, float dt_sub) {
+template <class M>
+__device__ __forceinline__ void pin_one_m(uint32_t k, const uint32_t* __restrict__ pin_v,
+                                          const float4* __restrict__ pin_t, const M& m, float dt_sub) {
   const uint32_t vi = pin_v[k];
   const float4 t = pin_t[k];  // target xyz, weight
   const float w = clampf(t.w, 0.0f, 1.0f);
   if (w <= 0.0f) return;
-  const float im = ld4<kCg>(x4 + vi).w;
-  float4 p = ld4<kCg>(p4 + vi);
+  const float im = m.ldx(vi).w;
+  float4 p = m.ldp(vi);
   if (im <= 0.0f) {
     p.x = t.x; p.y = t.y; p.z = t.z;
-    p4[vi] = p;
+    m.stp(vi, p);
     return;
   }
   V3 d = mk(p) - mk(t);
@@ -96,7 +118,13 @@ __device__ __forceinline__ void pin_one(uint32_t k, const uint32_t* __restrict__
   float corr = -dist / (im + alpha);
   V3 np = mk(p) + nn * (im * corr);
   p.x = np.x; p.y = np.y; p.z = np.z;
-  p4[vi] = p;
+  m.stp(vi, p);
+}
+template <bool kCg>
+__device__ __forceinline__ void pin_one(uint32_t k, const uint32_t* __restrict__ pin_v,
+                                        const float4* __restrict__ pin_t, const float4* __restrict__ x4,
+                                        float4* __restrict__ p4, float dt_sub) {
+  pin_one_m(k, pin_v, pin_t, GMem<kCg>{const_cast<float4*>(x4), p4, nullptr}, dt_sub);
 }
 __global__ void k_pin(uint32_t npins, const uint32_t* __restrict__ pin_v, const float4* __restrict__ pin_t,
                       const float4* __restrict__ x4, float4* __restrict__ p4, float dt_sub) {
@@ -108,18 +136,17 @@ __global__ void k_pin(uint32_t npins, const uint32_t* __restrict__ pin_v, const 
 
 // One distance constraint (shaders/distance.wgsl:60-124).  dist_par =
 // (rest, tension compliance, compression compliance, shear flag).
-template <bool kCg>
-__device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __restrict__ ids,
-                                                 const float4* __restrict__ par, float4* __restrict__ x4,
-                                                 float4* __restrict__ p4, float* __restrict__ lam,
-                                                 const SubstepParams& sp, bool damped) {
+template <class M>
+__device__ __forceinline__ void project_distance_m(uint32_t ci, const uint2* __restrict__ ids,
+                                                   const float4* __restrict__ par, const M& m,
+                                                   float* __restrict__ lam, const SubstepParams& sp, bool damped) {
   const uint2 e = ids[ci];
   const float4 c = par[ci];
   // every load of the constraint issued together: within a colour no other
   // thread writes these addresses, so this changes latency, not results
-  const float4 xa = ld4<kCg>(x4 + e.x), xb = ld4<kCg>(x4 + e.y);
-  const float4 q0 = ld4<kCg>(p4 + e.x), q1 = ld4<kCg>(p4 + e.y);
-  const float l = ld1<kCg>(lam + ci);
+  const float4 xa = m.ldx(e.x), xb = m.ldx(e.y);
+  const float4 q0 = m.ldp(e.x), q1 = m.ldp(e.y);
+  const float l = ld1<M::kCg>(lam + ci);
   const float w0 = xa.w, w1 = xb.w;
   const float ws = w0 + w1;
   if (ws <= kEps) return;
@@ -142,16 +169,23 @@ __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __res
     const float dl = (-cv - alpha * l - gamma * vp) / ((1.0f + gamma) * ws + alpha);
     lam[ci] = l + dl;
     const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
-    p4[e.x] = make_float4(n0.x, n0.y, n0.z, q0.w);
-    p4[e.y] = make_float4(n1.x, n1.y, n1.z, q1.w);
+    m.stp(e.x, make_float4(n0.x, n0.y, n0.z, q0.w));
+    m.stp(e.y, make_float4(n1.x, n1.y, n1.z, q1.w));
     return;
   }
   // gamma == 0: (-cv - alpha*l - 0*vp) / (1*ws + alpha)
   const float dl = (-cv - alpha * l) / (1.0f * ws + alpha);
   lam[ci] = l + dl;
   const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
-  p4[e.x] = make_float4(n0.x, n0.y, n0.z, q0.w);
-  p4[e.y] = make_float4(n1.x, n1.y, n1.z, q1.w);
+  m.stp(e.x, make_float4(n0.x, n0.y, n0.z, q0.w));
+  m.stp(e.y, make_float4(n1.x, n1.y, n1.z, q1.w));
+}
+template <bool kCg>
+__device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __restrict__ ids,
+                                                 const float4* __restrict__ par, float4* __restrict__ x4,
+                                                 float4* __restrict__ p4, float* __restrict__ lam,
+                                                 const SubstepParams& sp, bool damped) {
+  project_distance_m(ci, ids, par, GMem<kCg>{x4, p4, nullptr}, lam, sp, damped);
 }
 
 __global__ void k_distance(uint32_t off, uint32_t cnt, const uint2* __restrict__ ids, const float4* __restrict__ par,
@@ -165,18 +199,17 @@ __global__ void k_distance(uint32_t off, uint32_t cnt, const uint2* __restrict__
 
 // One bending constraint (shaders/bending.wgsl:59-126).  bend_par =
 // (rest, compliance, kind, seam gap).
-template <bool kCg>
-__device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __restrict__ ids,
-                                                const float4* __restrict__ par, float4* __restrict__ x4,
-                                                float4* __restrict__ p4, float* __restrict__ lam,
-                                                const SubstepParams& sp, bool damped) {
+template <class M>
+__device__ __forceinline__ void project_bending_m(uint32_t ci, const uint4* __restrict__ ids,
+                                                  const float4* __restrict__ par, const M& m,
+                                                  float* __restrict__ lam, const SubstepParams& sp, bool damped) {
   const float4 c = par[ci];
   const uint4 e = ids[ci];
   if (c.y >= 1e9f) return;
   // loads of the written pair issued together (see project_distance)
-  const float4 xc = ld4<kCg>(x4 + e.z), xd = ld4<kCg>(x4 + e.w);
-  const float4 q2 = ld4<kCg>(p4 + e.z), q3 = ld4<kCg>(p4 + e.w);
-  const float l = ld1<kCg>(lam + ci);
+  const float4 xc = m.ldx(e.z), xd = m.ldx(e.w);
+  const float4 q2 = m.ldp(e.z), q3 = m.ldp(e.w);
+  const float l = ld1<M::kCg>(lam + ci);
   const float w2 = xc.w, w3 = xd.w;
   const float ws = w2 + w3;
   if (ws <= kEps) return;
@@ -186,7 +219,7 @@ __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __rest
   if (dist <= kEps) return;
   if (c.z > 0.5f && c.z < 1.5f) {
     if (dist >= c.x) return;
-    float gap = length(mk(ld4<kCg>(p4 + e.x)) - mk(ld4<kCg>(p4 + e.y)));
+    float gap = length(mk(m.ldp(e.x)) - mk(m.ldp(e.y)));
     if (gap > c.w) return;
   }
   const V3 dir = delta / dist;
@@ -205,8 +238,15 @@ __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __rest
   }
   lam[ci] = l + dl;
   const V3 n2 = p2 + dir * (w2 * dl), n3 = p3 + dir * (-w3 * dl);
-  p4[e.z] = make_float4(n2.x, n2.y, n2.z, q2.w);
-  p4[e.w] = make_float4(n3.x, n3.y, n3.z, q3.w);
+  m.stp(e.z, make_float4(n2.x, n2.y, n2.z, q2.w));
+  m.stp(e.w, make_float4(n3.x, n3.y, n3.z, q3.w));
+}
+template <bool kCg>
+__device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __restrict__ ids,
+                                                const float4* __restrict__ par, float4* __restrict__ x4,
+                                                float4* __restrict__ p4, float* __restrict__ lam,
+                                                const SubstepParams& sp, bool damped) {
+  project_bending_m(ci, ids, par, GMem<kCg>{x4, p4, nullptr}, lam, sp, damped);
 }
 
 __global__ void k_bending(uint32_t off, uint32_t cnt, const uint4* __restrict__ ids, const float4* __restrict__ par,
@@ -283,12 +323,11 @@ __global__ void k_sewing(uint32_t off, uint32_t cnt, const uint2* __restrict__ i
 }
 
 // shaders/update_vel.wgsl:33-53
-template <bool kCg>
-__device__ __forceinline__ void update_vertex(uint32_t i, float4* __restrict__ x4, const float4* __restrict__ p4,
-                                              float4* __restrict__ v4, float dt_sub) {
-  float4 x = ld4<kCg>(x4 + i);
-  const float4 p = ld4<kCg>(p4 + i);
-  float4 v = ld4<kCg>(v4 + i);
+template <class M>
+__device__ __forceinline__ void update_vertex_m(uint32_t i, const M& m, float dt_sub) {
+  float4 x = m.ldx(i);
+  const float4 p = m.ldp(i);
+  float4 v = m.ldv(i);
   const float dt = fmaxf(dt_sub, 1e-8f);
   if (x.w > 0.0f) {
     V3 vv = (mk(p) - mk(x)) / dt;
@@ -297,8 +336,13 @@ __device__ __forceinline__ void update_vertex(uint32_t i, float4* __restrict__ x
     v.x = 0.f; v.y = 0.f; v.z = 0.f;
   }
   x.x = p.x; x.y = p.y; x.z = p.z;
-  x4[i] = x;
-  v4[i] = v;
+  m.stx(i, x);
+  m.stv(i, v);
+}
+template <bool kCg>
+__device__ __forceinline__ void update_vertex(uint32_t i, float4* __restrict__ x4, const float4* __restrict__ p4,
+                                              float4* __restrict__ v4, float dt_sub) {
+  update_vertex_m(i, GMem<kCg>{x4, const_cast<float4*>(p4), v4}, dt_sub);
 }
 __global__ void k_update_vel(uint32_t n, float4* __restrict__ x4, const float4* __restrict__ p4,
                              float4* __restrict__ v4, float dt_sub) {
@@ -431,12 +475,11 @@ __device__ __forceinline__ bool group_far(V3 a, V3 b, float4 g, float th) {
 // exactly like the reference; two levels of conservative bounding spheres
 // skip runs of triangles none of which could pass the per-triangle test, so
 // the sequence of applied contacts is unchanged.
-template <bool kCg, bool kBone = false>
-__device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ x4, float4* __restrict__ p4,
-                                               const ColliderArgs& ca, float dt) {
-  float4 x = ld4<kCg>(x4 + i);
+template <bool kBone, class M>
+__device__ __forceinline__ void collide_vertex_m(uint32_t i, const M& m, const ColliderArgs& ca, float dt) {
+  float4 x = m.ldx(i);
   if (x.w <= 0.0f) return;
-  float4 pr = ld4<kCg>(p4 + i);
+  float4 pr = m.ldp(i);
   V3 p = mk(pr), pinit = p, xn = mk(x);
   const V3 xpos = mk(x);
   const float th = pr.w;
@@ -510,8 +553,13 @@ __device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ 
       contact(tgt, bn, bf, br, dt, pb, xn, p);
     }
   }
-  p4[i] = make_float4(p.x, p.y, p.z, pr.w);
-  x4[i] = make_float4(xn.x, xn.y, xn.z, x.w);
+  m.stp(i, make_float4(p.x, p.y, p.z, pr.w));
+  m.stx(i, make_float4(xn.x, xn.y, xn.z, x.w));
+}
+template <bool kCg, bool kBone = false>
+__device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ x4, float4* __restrict__ p4,
+                                               const ColliderArgs& ca, float dt) {
+  collide_vertex_m<kBone>(i, GMem<kCg>{x4, p4, nullptr}, ca, dt);
 }
 // kBone: with the bone SDF phase (a separate instantiation, so that kernels
 // without bone colliders keep their register budget)
@@ -944,6 +992,119 @@ __global__ void __launch_bounds__(256) k_solver_cluster(SolverArgs a, ClusterTab
     }
     for (uint32_t i = vr.x + tid; i < vr.y; i += stride) update_vertex<true>(i, a.x4, a.p4, a.v4, dts);
     cl.sync();
+  }
+}
+
+
+// ---------------------------------------------------------------------
+// staged cluster solver for batched instances
+// ---------------------------------------------------------------------
+// The bins of the cluster solver with their vertex records on chip for the
+// whole frame.  A bin's vertex range is split into K contiguous slices, one
+// per CTA of the cluster; each CTA keeps its slice's x4, p4 and v4 records
+// in shared memory.  A constraint reads and writes its two (bending: four)
+// vertices in their owners' slices, its own CTA's directly and the others'
+// through distributed shared memory, so the colour steps touch no global
+// vertex data and are separated only by the cluster barrier.  Each (bin,
+// colour) constraint range is split by the owner of the constraint's first
+// vertex, so most accesses stay in the CTA.  Per-vertex passes (predict,
+// pins, collision, velocity update) run on the owner's slice.  The
+// per-element functions and the colour order are those of the other paths,
+// so the results are the same bits.
+struct SMem {
+  static constexpr bool kCg = false;  // constraint lambdas: written and read by the same thread
+  float4* sx;
+  float4* sp;
+  float4* sv;
+  uint32_t base, chunk, rank;
+  __device__ __forceinline__ float4* at(float4* a, uint32_t i) const {
+    const uint32_t o = i - base;
+    const uint32_t r = o / chunk;
+    float4* q = a + (o - r * chunk);
+    return r == rank ? q : cooperative_groups::this_cluster().map_shared_rank(q, r);
+  }
+  __device__ __forceinline__ float4 ldx(uint32_t i) const { return *at(sx, i); }
+  __device__ __forceinline__ float4 ldp(uint32_t i) const { return *at(sp, i); }
+  __device__ __forceinline__ float4 ldv(uint32_t i) const { return *at(sv, i); }
+  __device__ __forceinline__ void stx(uint32_t i, float4 v) const { *at(sx, i) = v; }
+  __device__ __forceinline__ void stp(uint32_t i, float4 v) const { *at(sp, i) = v; }
+  __device__ __forceinline__ void stv(uint32_t i, float4 v) const { *at(sv, i) = v; }
+};
+struct StageTables {
+  const uint2* vrange;        // [bins] vertex range [x, y)
+  const uint2* pins;          // [bins * K] (first, count) into pin_v / pin_t, by owning slice
+  const uint32_t* dist;       // [bins * ndc * (K + 1)] offsets into dist_perm per (bin, colour, owner)
+  const uint32_t* bend;       // [bins * nbc * (K + 1)]
+  const uint32_t* dist_perm;
+  const uint32_t* bend_perm;
+  uint32_t cap;               // vertices per slice (the shared-memory capacity)
+};
+template <uint32_t K, bool kBone>
+__global__ void __launch_bounds__(512, 1) k_solver_staged(SolverArgs a, StageTables t) {
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  extern __shared__ float4 stage[];
+  const uint32_t rank = cl.block_rank();
+  const uint32_t bin = blockIdx.x / K;
+  const uint2 vr = t.vrange[bin];
+  const uint32_t nv = vr.y - vr.x;
+  const uint32_t chunk = nv > 0 ? (nv + K - 1) / K : 1u;
+  const SMem m{stage, stage + t.cap, stage + 2 * t.cap, vr.x, chunk, rank};
+  const uint32_t lo = vr.x + min(rank * chunk, nv), hi = vr.x + min((rank + 1u) * chunk, nv);
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    m.sx[i - lo] = a.x4[i];
+    m.sp[i - lo] = a.p4[i];
+    m.sv[i - lo] = a.v4[i];
+  }
+  const uint2 pr = t.pins[bin * K + rank];
+  const uint32_t* dtab = t.dist + size_t(bin) * a.ndc * (K + 1u);
+  const uint32_t* btab = t.bend + size_t(bin) * a.nbc * (K + 1u);
+  const float dts = a.sp.dt;
+  for (uint32_t sub = 0; sub < a.nsub; ++sub) {
+    for (uint32_t c = 0; c < a.ndc; ++c)
+      for (uint32_t k = dtab[c * (K + 1u) + rank] + threadIdx.x; k < dtab[c * (K + 1u) + rank + 1u]; k += blockDim.x)
+        a.dlam[t.dist_perm[k]] = 0.f;
+    for (uint32_t c = 0; c < a.nbc; ++c)
+      for (uint32_t k = btab[c * (K + 1u) + rank] + threadIdx.x; k < btab[c * (K + 1u) + rank + 1u]; k += blockDim.x)
+        a.blam[t.bend_perm[k]] = 0.f;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) predict_vertex_m(i, m, a.sp);
+    cl.sync();
+    for (uint32_t it = 0; it < a.iters; ++it) {
+      if (a.npins) {
+        for (uint32_t k = pr.x + threadIdx.x; k < pr.x + pr.y; k += blockDim.x) pin_one_m(k, a.pin_v, a.pin_t, m, dts);
+        cl.sync();
+      }
+      for (uint32_t c = 0; c < a.ndc; ++c) {
+        const uint32_t* r = dtab + c * (K + 1u);
+        if (r[0] == r[K]) continue;  // the bin has no constraint of this colour (same test in every CTA)
+        for (uint32_t k = r[rank] + threadIdx.x; k < r[rank + 1u]; k += blockDim.x)
+          project_distance_m(t.dist_perm[k], a.dist_ids, a.dist_par, m, a.dlam, a.sp, a.ddamp);
+        cl.sync();
+      }
+      for (uint32_t c = 0; c < a.nbc; ++c) {
+        const uint32_t* r = btab + c * (K + 1u);
+        if (r[0] == r[K]) continue;
+        for (uint32_t k = r[rank] + threadIdx.x; k < r[rank + 1u]; k += blockDim.x)
+          project_bending_m(t.bend_perm[k], a.bend_ids, a.bend_par, m, a.blam, a.sp, a.bdamp);
+        cl.sync();
+      }
+      if (a.hascol && a.coupled) {
+        for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) collide_vertex_m<kBone>(i, m, a.ca, dts);
+        cl.sync();
+      }
+    }
+    // the rest of the substep touches only the CTA's own slice
+    if (a.hascol && !a.coupled)
+      for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) collide_vertex_m<kBone>(i, m, a.ca, dts);
+    __syncthreads();
+    for (uint32_t k = pr.x + threadIdx.x; k < pr.x + pr.y; k += blockDim.x) pin_one_m(k, a.pin_v, a.pin_t, m, dts);
+    __syncthreads();
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) update_vertex_m(i, m, dts);
+    cl.sync();
+  }
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    a.x4[i] = m.sx[i - lo];
+    a.p4[i] = m.sp[i - lo];
+    a.v4[i] = m.sv[i - lo];
   }
 }
 

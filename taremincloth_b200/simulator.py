@@ -158,6 +158,19 @@ def color_edge_pairs(num_vertices, edges):
     return [int(c) for c in out]
 
 
+def mark_device_lost(device=0):
+    """Mark a device's context lost (context.rs:131-134); the next simulator
+    created on it re-initialises the context, older simulators refuse calls."""
+    _lib.check(_lib.load().tc_mark_device_lost(int(device)))
+
+
+def device_status(device=0):
+    """(lost, epoch) of a device's context (context.rs:126-129)."""
+    lost, epoch = C.c_int(0), C.c_uint64(0)
+    _lib.check(_lib.load().tc_device_status(int(device), C.byref(lost), C.byref(epoch)))
+    return bool(lost.value), int(epoch.value)
+
+
 # SimConfig::default (crates/cloth_core/src/config.rs:3-37, :142-196): the
 # value of every field a settings JSON record leaves out
 CONFIG_DEFAULTS = {
@@ -422,6 +435,26 @@ class ClothSimulator:
         if int(mode) != 0:
             raise NotImplementedError("coupled self-collision modes 1-3 are not built")
         self._c(self._L.tc_set_coupled_self_collision_options(self._h, 0, int(relaxation_iters)))
+
+    def set_nonfinite_check(self, enable=True):
+        """Make position read-backs raise FloatingPointError on NaN / Inf."""
+        self._c(self._L.tc_set_nonfinite_check(self._h, int(bool(enable))))
+
+    # ---------------- narrow-phase pair lists (parity instrumentation)
+    def set_pair_recording(self, enable=True, max_vt_pairs=1 << 20, max_ee_pairs=1 << 20):
+        """Record, at every self-collision pass, the direct pass's V-T pairs that
+        reach the contact math and its E-E pairs counted within max_search."""
+        self._c(self._L.tc_set_pair_recording(self._h, int(bool(enable)), int(max_vt_pairs), int(max_ee_pairs)))
+
+    def get_pair_lists(self):
+        """dict(vt=(k, 4) uint32 rows (vertex, a < b < c), ee=(m, 2) rows (e0 < e1)),
+        sorted, of the latest self-collision pass."""
+        cnt = np.zeros(2, _u32)
+        self._c(self._L.tc_get_pair_lists(self._h, None, 0, None, 0, _ptr(cnt)))
+        vt = np.zeros((max(int(cnt[0]), 1), 4), _u32)
+        ee = np.zeros((max(int(cnt[1]), 1), 2), _u32)
+        self._c(self._L.tc_get_pair_lists(self._h, _ptr(vt), vt.shape[0], _ptr(ee), ee.shape[0], _ptr(cnt)))
+        return dict(vt=vt[:int(cnt[0])], ee=ee[:int(cnt[1])])
 
     # ---------------- settings record (lib.rs:3029-3047, config_impl.rs:16-160)
     def get_config_json(self):
@@ -912,8 +945,10 @@ class ClothSimulator:
 
     def set_launch_config(self, persistent=True, blocks_per_sm=4):
         """persistent: False = one launch per colour, True = persistent cooperative
-        solver with `blocks_per_sm`, 2 = cluster solver (batched instances)."""
-        mode = 2 if persistent == 2 else int(bool(persistent))
+        solver with `blocks_per_sm`, 2 = cluster solver (batched instances),
+        3 = staged cluster solver (batched instances, vertex records in the
+        clusters' shared memory)."""
+        mode = int(persistent) if persistent in (2, 3) and persistent is not True else int(bool(persistent))
         self._c(self._L.tc_set_launch_config(self._h, mode, int(blocks_per_sm)))
 
     def get_launch_limits(self):

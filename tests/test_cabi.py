@@ -50,3 +50,15 @@ def test_create_without_gpu_raises_runtime_error():
 def test_drop_in_module_imports():
     import taremin_cloth_core
     assert hasattr(taremin_cloth_core, "ClothSimulator")
+
+
+def test_device_lost_flag_is_host_side():
+    """Marking a device lost and reading its status need no GPU (no CUDA call)."""
+    from taremincloth_b200 import _lib
+    from taremincloth_b200.simulator import device_status, mark_device_lost
+    lost, epoch = device_status(5)
+    assert not lost and epoch >= 1
+    mark_device_lost(5)
+    assert device_status(5) == (True, epoch)
+    with pytest.raises(RuntimeError):
+        _lib.check(_lib.load().tc_mark_device_lost(64))

@@ -115,3 +115,44 @@ def test_config_json_roundtrip_and_hash():
     for bad in ("not json", "[1, 2]", '{"solver_iterations": -1}', '{"damping": "x"}'):
         with pytest.raises(ValueError):
             s3.apply_config_json(bad)
+
+
+def test_device_lost_marks_and_recovers():
+    """context.rs:499 restated: a device marked lost is re-initialised by the
+    next simulator creation (new epoch); a simulator of the old epoch refuses
+    calls with RuntimeError and can still be destroyed."""
+    from taremincloth_b200.simulator import device_status, mark_device_lost
+    _, old = _sheet()
+    old.step(1.0 / 60.0, 2)
+    lost, epoch = device_status(0)
+    assert not lost
+    mark_device_lost(0)
+    assert device_status(0) == (True, epoch)
+    with pytest.raises(RuntimeError, match="lost"):
+        old.step(1.0 / 60.0, 2)
+    _, fresh = _sheet()
+    assert device_status(0) == (False, epoch + 1)
+    fresh.step(1.0 / 60.0, 2)
+    out = np.empty(fresh.get_num_vertices() * 3, np.float32)
+    fresh.get_positions(out)
+    assert np.isfinite(out).all()
+    with pytest.raises(RuntimeError, match="epoch"):
+        old.get_positions(out)
+    del old
+
+
+def test_nonfinite_readback_check():
+    """The NaN / Inf sentinel on the host copy: off by default (positions are
+    returned as they are), FloatingPointError when on."""
+    sc, s = _sheet()
+    p = np.array(sc["positions"], np.float32)
+    p[7, 1] = np.nan
+    s.set_positions_and_velocities(p)
+    out = np.empty(len(p) * 3, np.float32)
+    s.get_positions(out)
+    assert np.isnan(out[3 * 7 + 1])
+    s.set_nonfinite_check(True)
+    with pytest.raises(FloatingPointError, match="vertex 7"):
+        s.get_positions(out)
+    s.set_nonfinite_check(False)
+    s.get_positions(out)

@@ -7,6 +7,8 @@ oracle's operation order, so in practice the match is bit-exact; the tests
 also report the fraction of bit-identical coordinates.  Integer outputs (hash
 cell starts, sorted indices) must be bit-exact.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -15,6 +17,8 @@ from gpu_common import compare_frames, extent
 from taremincloth_b200 import ClothSimulator, scenes
 
 pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 @pytest.mark.parametrize("case", ["case1", "case2", "case3"])
@@ -70,16 +74,105 @@ def test_config2_small_with_mesh_and_self_collision(oracle_lib):
 
 
 def test_config2_full_one_substep(oracle_lib):
-    """Full-size configuration, one substep (the oracle takes ~30 s)."""
+    """Full-size configuration, one substep (the oracle takes ~30 s), with
+    the direct pass's V-T and E-E pair lists bit-exact."""
     sc = scenes.config2()
     g = scenes.build(ClothSimulator, sc)
     o = scenes.build(oracle_lib.OracleSim, sc)
+    g.set_pair_recording(True, 1 << 22, 1 << 22)
+    o.set_pair_recording(True)
     dts = sc["dt"] / sc["substeps"]
     g.step(dts, 1)
     o.step(dts, 1)
     xg, _, _ = g.get_state()
     xo, _, _ = o.get_state()
     assert float(np.abs(xg - xo).max()) / extent(sc["positions"]) <= 1e-5
+    a, b = g.get_pair_lists(), o.get_pair_lists()
+    assert len(b["vt"]) > 10000 and len(b["ee"]) > 10000, (len(b["vt"]), len(b["ee"]))
+    np.testing.assert_array_equal(a["vt"], b["vt"])
+    np.testing.assert_array_equal(a["ee"], b["ee"])
+
+
+@pytest.mark.parametrize("n,subdiv,frames", [(48, 3, 3), (96, 4, 6)])
+def test_pair_lists_bit_exact(oracle_lib, n, subdiv, frames):
+    """Pair lists of one direct pass from the same draped state: every V-T
+    pair that reaches the contact math and every counted E-E pair."""
+    sc = scenes.config2(n=n, subdiv=subdiv)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    for _ in range(frames):
+        o.step(sc["dt"], sc["substeps"])
+    x, _, v = o.get_state()
+    g = scenes.build(ClothSimulator, sc)
+    g.set_positions_and_velocities(x, v)
+    o.set_state(x, v)
+    g.set_pair_recording(True)
+    o.set_pair_recording(True)
+    dts = sc["dt"] / sc["substeps"]
+    for _ in range(2):  # two passes in a row: the lists restart every pass
+        g.step(dts, 1)
+        o.step(dts, 1)
+        a, b = g.get_pair_lists(), o.get_pair_lists()
+        assert len(b["vt"]) > 500 and len(b["ee"]) > 500, (len(b["vt"]), len(b["ee"]))
+        np.testing.assert_array_equal(a["vt"], b["vt"])
+        np.testing.assert_array_equal(a["ee"], b["ee"])
+    g.set_pair_recording(False)
+    with pytest.raises(ValueError):
+        g.get_pair_lists()
+
+
+def test_pair_record_overflow_is_reported():
+    sc = scenes.config2(n=48, subdiv=3)
+    g = scenes.build(ClothSimulator, sc)
+    g.set_pair_recording(True, 16, 16)
+    g.step(sc["dt"] / sc["substeps"], 1)
+    with pytest.raises(ValueError):
+        g.get_pair_lists()
+
+
+def test_config2_full_frame_against_oracle_fixture():
+    """One full-size frame (20 substeps) against the oracle's frame from
+    tests/golden/make_oracle_frames.py, within 1e-5 of the extent; colouring,
+    vertex and edge hash of the full scene bit-exact against the oracle."""
+    sc = scenes.config2()
+    g = scenes.build(ClothSimulator, sc)
+    g.step(sc["dt"], sc["substeps"])
+    ref = np.load(os.path.join(GOLDEN, "oracle_frames.npz"))["full_f1"]
+    xg, _, _ = g.get_state()
+    assert float(np.abs(xg.astype(np.float64) - ref).max()) / extent(sc["positions"]) <= 1e-5
+
+
+def test_config2_full_coloring_and_hash_bit_exact(oracle_lib):
+    sc = scenes.config2()
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    col, oc = g.get_coloring(), o.colors()
+    for k in ("dist_off", "dist_cnt", "bend_off", "bend_cnt"):
+        np.testing.assert_array_equal(col[k], oc[k])
+    np.testing.assert_array_equal(col["dist_v"], o.distance_constraints()["v"])
+    g.step(sc["dt"], 2)
+    x, _, v = g.get_state()
+    o.set_state(x, v)
+    g.set_positions_and_velocities(x, v)
+    for which in (0, 1):
+        cs_g, s_g = g.get_hash_state(which)
+        cs_o, s_o = o.build_hash(which)
+        np.testing.assert_array_equal(cs_g, cs_o)
+        np.testing.assert_array_equal(s_g, s_o)
+
+
+def test_config2_128_600_substeps_against_oracle_fixture():
+    """Two 128 x 128 sheets on the icosphere, 600 substeps (30 frames),
+    within 1e-4 of the extent of the oracle's frames 1, 10, 20, 30."""
+    sc = scenes.config2(n=128)
+    g = scenes.build(ClothSimulator, sc)
+    ref = np.load(os.path.join(GOLDEN, "oracle_frames.npz"))
+    ext = extent(sc["positions"])
+    for f in range(1, 31):
+        g.step(sc["dt"], sc["substeps"])
+        if f in (1, 10, 20, 30):
+            xg, _, _ = g.get_state()
+            err = float(np.abs(xg.astype(np.float64) - ref[f"mid_f{f}"]).max()) / ext
+            assert err <= (1e-5 if f == 1 else 1e-4), (f, err)
 
 
 def test_hash_state_bit_exact(oracle_lib):
