@@ -93,12 +93,41 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(pass_name, sim_counts, n_tris):
+def topology_sizes(sc):
+    """(adjacency, two-hop, star) entry counts of a scene's host-built topology
+    (the lists the self-collision passes read)."""
+    import ctypes as C
+    from taremincloth_b200 import _lib
+    L = _lib.load()
+    pos = np.ascontiguousarray(sc["positions"], np.float32)
+    e = np.ascontiguousarray(sc["edges"], np.uint32)
+    f = np.ascontiguousarray(sc["faces"], np.uint32)
+    li = np.ascontiguousarray(sc["layer_ids"], np.uint32) if "layer_ids" in sc else None
+    inv = np.ascontiguousarray(sc["inv_masses"], np.float32)
+    p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    h = C.c_void_p()
+    _lib.check(L.tc_mesh_build_sewn(C.byref(h), p(pos), len(pos), p(e), len(e), p(f), len(f), p(inv), p(li), None,
+                                    0, float(sc["thickness"]), 1000.0, 1000.0, 500.0, 10.0, None, 0, 1.0,
+                                    float("nan"), 1))
+    try:
+        a, t, st = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _lib.check(L.tc_mesh_topology_sizes(h, C.byref(a), C.byref(t), C.byref(st)))
+        return {"adj": a.value, "two_hop": t.value, "star": st.value}
+    finally:
+        L.tc_mesh_destroy(h)
+
+
+def algorithmic_bytes(pass_name, sim_counts, n_tris, topo=None):
     """Compulsory DRAM/L2 bytes of one launch group of a pass (each array read
     and written once).  Layout: x4/p4/v4 float4 records (16 B), distance
     constraint = uint2 ids + float4 params (24 B), bending = uint4 + float4
-    (32 B), lambda 4 B, self-collision accumulator 64 B per vertex."""
+    (32 B), lambda 4 B, self-collision accumulator 64 B per vertex.  The
+    self-collision passes also read the per-substep caches and hash-ordered
+    candidate records, the star (8 B per entry) and two-hop (index + rest
+    length, 8 B per entry) lists and the cell starts."""
     n, nd, nb, ne = sim_counts["n"], sim_counts["nd"], sim_counts["nb"], sim_counts["n_edges"]
+    topo = topo or {"adj": 0, "two_hop": 0, "star": 0}
+    cells = 4 * (sim_counts.get("table_size", 65536) + 1)
     if pass_name == "distance":       # all colours of one iteration
         return nd * (24 + 4 + 4) + 2 * nd * (16 + 16 + 16)  # constraint+lambda r/w, 2x (p read, x.w read, p write)
     if pass_name == "bending":
@@ -110,9 +139,14 @@ def algorithmic_bytes(pass_name, sim_counts, n_tris):
     if pass_name == "collision":
         return n * (16 + 16 + 16 + 16) + n_tris * (64 + 16)  # x, p r/w + triangles + bounds once
     if pass_name == "sc_solve":
-        return n * (16 + 16 + 16 + 4 + 64) + 8 * 65537  # x, p, v, local len, accum + cell starts
+        # per vertex: x, p, v (layer), local length, |p - x|, cell, three candidate records, star box,
+        # star and two-hop offsets, normal, accumulator; plus star / two-hop entries and cell starts
+        return (n * (16 + 16 + 16 + 4 + 4 + 16 + 48 + 48 + 4 + 4 + 16 + 64) + 8 * topo["star"]
+                + 8 * topo["two_hop"] + cells)
     if pass_name == "sc_solve_ee":
-        return ne * 8 + n * (16 + 16 + 16 + 64) + 4 * 65537
+        # per edge: endpoints, cell, swept box, four candidate records; per vertex: x, p, v, normal,
+        # accumulator, two-hop offsets; two-hop entries and cell starts
+        return ne * (8 + 16 + 32 + 56) + n * (16 + 16 + 16 + 16 + 64 + 4) + 8 * topo["two_hop"] + cells
     if pass_name == "sc_apply":
         return n * (16 + 16 + 16 + 4 + 64 + 64)
     if pass_name.startswith("hash"):
@@ -383,6 +417,33 @@ def warm_start_extra(steps):
     return out
 
 
+def learned_batched_summary(batched, ws4):
+    """The metric as named, on the config 4 workload: plain = the 64 cloths as
+    separate simulators (plain CUDA XPBD), batched = one simulator over all
+    of them (autotuned launch shape), learned+batched = the batched
+    simulator with the learned warm start replacing k of the 5 iterations
+    (every warm-started substep judged against the plain solver's residual
+    on the device, full iterations on a miss).  Ratios of vertex-substeps/s."""
+    plain = batched["separate_vertex_substeps_per_s"]
+    bat = batched["batched_vertex_substeps_per_s"]
+    ks = sorted((k for k in ws4 if k.startswith("k") and k[1:].isdigit()),
+                key=lambda k: -ws4[k]["vertex_substeps_per_s"])
+    best = ks[0] if ks else None
+    lb = ws4[best]["vertex_substeps_per_s"] if best else None
+    return {"workload": batched["workload"],
+            "plain_vertex_substeps_per_s": plain, "batched_vertex_substeps_per_s": bat,
+            "batched_launch": batched["launch_config"],
+            "learned_batched_vertex_substeps_per_s": lb, "learned_k": best,
+            "learned_fallback_rate": ws4[best]["fallback_rate"] if best else None,
+            "learned_path_plain_vertex_substeps_per_s": ws4["plain_vertex_substeps_per_s"],
+            "batched_vs_plain": bat / plain,
+            "learned_batched_vs_plain": lb / plain if lb else None,
+            "learned_vs_batched_same_launch_path": ws4[best]["speedup_vs_plain"] if best else None,
+            "learned_batched_vs_best_batched": lb / bat if lb else None,
+            "residual": "warm-started substeps fall back to the full iteration count when their RMS residual "
+                        "exceeds the plain solver's (threshold_ratio in warm_start.config4)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -413,6 +474,7 @@ def main():
     sim = scenes.build(ClothSimulator, sc, device=local)
     dt, sub = sc["dt"], sc["substeps"]
     counts = sim.get_counts()
+    topo = topology_sizes(sc)
     for _ in range(max(args.warmup, 3)):
         sim.step(dt, sub)
     # launch shape (per-colour launches vs persistent solver): results are
@@ -480,17 +542,22 @@ def main():
     prof.sort(key=lambda r: -r[1])
     top_name, top_ms, top_launches = prof[0]
     avg_ms = top_ms / max(top_launches, 1)
-    alg = algorithmic_bytes(top_name, counts, len(tris))
+    alg = algorithmic_bytes(top_name, counts, len(tris), topo)
     peak, peak_kind = peaks()
     achieved = alg / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
-    traffic = None
+    traffic, l2 = None, None
     tj = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tj):
-        traffic = json.load(open(tj)).get(top_name)
+        tr = json.load(open(tj))
+        traffic = tr.get(top_name)
+        if tr.get("l2_bytes", {}).get(top_name):
+            # L2 throughput: lts__t_bytes of one launch (ncu) over the launch's measured duration
+            l2 = {"bytes_per_launch": tr["l2_bytes"][top_name],
+                  "achieved_gbs": tr["l2_bytes"][top_name] / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else None}
     # whole-step roofline: compulsory bytes of every pass of a frame (launch
     # groups of the two profiled frames / 2) per vertex-substep, at the timed
     # throughput
-    frame_bytes = sum(algorithmic_bytes(k, counts, len(tris)) * c for k, _, c in prof) / 2.0
+    frame_bytes = sum(algorithmic_bytes(k, counts, len(tris), topo) * c for k, _, c in prof) / 2.0
     step_b = frame_bytes / (n * sub)
     step_achieved = step_b * value / 1e9
     line = {
@@ -506,7 +573,7 @@ def main():
                    is True else "one launch per colour (programmatic dependent launch)"},
         "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs", "traffic": traffic,
-                     "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms},
+                     "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms, "l2": l2},
         "roofline_step": {"bound": "hbm", "achieved": step_achieved, "peak": peak, "unit": "GB/s",
                           "frac": step_achieved / peak, "bytes_per_vertex_substep": step_b,
                           "note": "compulsory bytes of all passes per vertex-substep x vertex-substeps/s"},
@@ -523,6 +590,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         line["batched_config4"] = batch_extra(3)
         line["warm_start"] = warm_start_extra(3)
+        line["learned_batched_vs_plain"] = learned_batched_summary(line["batched_config4"],
+                                                                   line["warm_start"]["config4"])
         line["bone_sdf_config3"] = bone_sdf_extra(3)
         line["sewing"] = sewing_extra(3)
         line["pair_cache_config2"] = pair_cache_extra(3)
