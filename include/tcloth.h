@@ -353,6 +353,11 @@ tc_status tc_device_status(int device, int *lost, uint64_t *epoch);
  * positions hold NaN or Inf (the copy is still written).  Off by default, as
  * in the reference, whose read-backs return whatever the GPU holds. */
 tc_status tc_set_nonfinite_check(tc_sim *s, int enable);
+/* Kernel shape of the direct pass's edge-edge search (new; results and pair
+ * lists do not change): 0 = one warp per edge over the 27 neighbour cells;
+ * 1 = one lane per edge, a warp taking 32 edges of the hash-sorted order and
+ * building each distinct cell's candidate list once in shared memory. */
+tc_status tc_set_self_collision_variant(tc_sim *s, uint32_t ee_variant);
 /* Narrow-phase pair lists of the direct self-collision pass, for parity
  * (no counterpart in the reference's API; the passes are
  * shaders/self_collision.wgsl:317-681 and

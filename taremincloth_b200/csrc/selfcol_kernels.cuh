@@ -1395,6 +1395,161 @@ __global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
   }
 }
 
+// Grouped variant of k_ee, one lane per edge.  A warp takes 32 consecutive
+// slots of the hash-sorted edge order, which are mostly edges of one
+// midpoint cell, so they share the reference's 27-cell candidate set.  For
+// each distinct cell among its edges the warp builds the cell-matched
+// candidates (es_* records) in shared memory, in the reference's visiting
+// order (dz outer, dx inner, bucket order), up to kEeChunk at a time; every
+// lane of that cell then walks them for its own edge with the reference's
+// tests (e_a < e_b, no shared vertex, swept boxes) and per-edge count cap
+// (search_count > max_search_iterations ends the edge's search,
+// shaders/self_collision_ee_direct.wgsl:330-360).  Counted pairs go to a
+// per-warp queue whose contact work (ee_pair) runs 32 pairs at a time.
+// The set of counted pairs and the work on each are those of k_ee.
+constexpr uint32_t kEeChunk = 128;
+constexpr uint32_t kEeWarps = 4;
+__global__ void __launch_bounds__(128) k_ee_grouped(SCArgs s) {
+  __shared__ int4 ch_c[kEeWarps][kEeChunk];
+  __shared__ uint2 ch_v[kEeWarps][kEeChunk];
+  __shared__ float4 ch_lo[kEeWarps][kEeChunk], ch_hi[kEeWarps][kEeChunk];
+  __shared__ uint32_t q_a[kEeWarps][64], q_b[kEeWarps][64];
+  __shared__ uint32_t sh_start[kEeWarps][28], sh_end[kEeWarps][28], sh_beg[kEeWarps][28];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t slot0 = (blockIdx.x * kEeWarps + uint32_t(warp)) * 32u;
+  if (slot0 >= s.ne) return;  // whole warp
+  const uint32_t my = slot0 + uint32_t(lane);
+  const bool valid = my < s.ne;
+  // this lane's edge: what the filter needs
+  uint32_t ei = 0, u0 = 0, u1 = 0;
+  V3 amin = mk(0.f, 0.f, 0.f), amax = amin;
+  int4 bc = make_int4(0, 0, 0, 0);
+  if (valid) {
+    ei = (uint32_t)s.es_c[my].w;
+    const EdgeCtx c = edge_ctx(s, ei);
+    u0 = c.u0;
+    u1 = c.u1;
+    amin = c.amin;
+    amax = c.amax;
+    bc = s.ecell[ei];
+  }
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  uint32_t qn = 0;
+  // contact work on the first 32 queued pairs, one per lane
+  auto drain32 = [&](uint32_t m) {
+    if (uint32_t(lane) < m) {
+      const uint32_t a = q_a[warp][lane], b = q_b[warp][lane];
+      const EdgeCtx c = edge_ctx(s, a);
+      TwoHop th0, th1;
+      th0.idx = s.th_idx + s.th_off[c.u0];
+      th0.rest = s.th_rest + s.th_off[c.u0];
+      th0.n = s.th_off[c.u0 + 1] - s.th_off[c.u0];
+      th1.idx = s.th_idx + s.th_off[c.u1];
+      th1.rest = s.th_rest + s.th_off[c.u1];
+      th1.n = s.th_off[c.u1 + 1] - s.th_off[c.u1];
+      const uint2 ebv = s.edges[b];
+      if (s.rec_ee) record_ee(s, a, b);
+      ee_pair(s, c, th0, th1, b, ebv.x, ebv.y, s.p4[ebv.x], s.p4[ebv.y], s.x4[ebv.x], s.x4[ebv.y], true);
+    }
+    __syncwarp();
+  };
+  uint32_t todo = __ballot_sync(0xffffffffu, valid);
+  while (todo) {
+    const int leader = __ffs(todo) - 1;
+    const int32_t cx = __shfl_sync(0xffffffffu, bc.x, leader);
+    const int32_t cy = __shfl_sync(0xffffffffu, bc.y, leader);
+    const int32_t cz = __shfl_sync(0xffffffffu, bc.z, leader);
+    const bool mine = valid && bc.x == cx && bc.y == cy && bc.z == cz;
+    todo &= ~__ballot_sync(0xffffffffu, mine);
+    // bucket ranges of the cell's 27 neighbours, lane k = (dz+1)*9 + (dy+1)*3 + (dx+1)
+    uint32_t cnt = 0, beg = 0;
+    if (lane < 27) {
+      const uint32_t h = hash3(cx - 1 + lane % 3, cy - 1 + (lane / 3) % 3, cz - 1 + lane / 9, s.table);
+      beg = s.ecs[h];
+      cnt = s.ecs[h + 1] - beg;
+    }
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane < 27) {
+      sh_start[warp][lane] = incl - cnt;
+      sh_end[warp][lane] = incl;
+      sh_beg[warp][lane] = beg;
+    }
+    __syncwarp();
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 26);
+    uint32_t counted = 0;
+    bool active = mine;
+    int k = 0;
+    for (uint32_t t0 = 0; t0 < total && __any_sync(0xffffffffu, active);) {
+      // the next cell-matched candidates, in order, into the chunk
+      uint32_t nch = 0;
+      while (t0 < total && nch + 32u <= kEeChunk) {
+        const uint32_t t = t0 + uint32_t(lane);
+        bool keep = false;
+        uint32_t slot = 0;
+        int4 c4 = make_int4(0, 0, 0, 0);
+        if (t < total) {
+          while (t >= sh_end[warp][k]) ++k;
+          slot = sh_beg[warp][k] + (t - sh_start[warp][k]);
+          c4 = s.es_c[slot];
+          keep = c4.x == cx - 1 + k % 3 && c4.y == cy - 1 + (k / 3) % 3 && c4.z == cz - 1 + k / 9;
+        }
+        const uint32_t b = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const uint32_t o = nch + __popc(b & lt_mask);
+          ch_c[warp][o] = c4;
+          ch_v[warp][o] = s.es_v[slot];
+          ch_lo[warp][o] = s.es_lo[slot];
+          ch_hi[warp][o] = s.es_hi[slot];
+        }
+        nch += __popc(b);
+        t0 += 32u;
+      }
+      __syncwarp();
+      // every lane of the cell walks the chunk for its own edge
+      for (uint32_t j = 0; j < nch; ++j) {
+        bool pass = false;
+        uint32_t eb = 0;
+        if (active) {
+          const int4 c4 = ch_c[warp][j];
+          const uint2 v = ch_v[warp][j];
+          eb = (uint32_t)c4.w;
+          const float4 lo = ch_lo[warp][j], hi = ch_hi[warp][j];
+          pass = ei < eb && !(v.x == u0 || v.x == u1 || v.y == u0 || v.y == u1) &&
+                 !(amin.x > hi.x || amin.y > hi.y || amin.z > hi.z || amax.x < lo.x || amax.y < lo.y ||
+                   amax.z < lo.z);
+          if (pass && ++counted > s.max_search) {
+            pass = false;
+            active = false;
+          }
+        }
+        const uint32_t b = __ballot_sync(0xffffffffu, pass);
+        if (pass) {
+          const uint32_t o = qn + __popc(b & lt_mask);
+          q_a[warp][o] = ei;
+          q_b[warp][o] = eb;
+        }
+        qn += __popc(b);
+        __syncwarp();
+        if (qn >= 32u) {
+          drain32(32u);
+          qn -= 32u;
+          if (uint32_t(lane) < qn) {
+            q_a[warp][lane] = q_a[warp][32 + lane];
+            q_b[warp][lane] = q_b[warp][32 + lane];
+          }
+          __syncwarp();
+        }
+      }
+      __syncwarp();
+    }
+  }
+  if (qn) drain32(qn);
+}
+
 // ---------------- edge colliders: shaders/edge_collision.wgsl:82-276
 // Collider edge (mesh.rs:1503-1565): endpoints, the largest thickness and the
 // mean friction of its triangles, their summed then normalised normals, and

@@ -1188,6 +1188,10 @@ struct Sim {
     a.rec_ee_cap = rec_pairs ? rec_ee_cap : 0u;
     return a;
   }
+  // E-E kernel: false = one warp per edge (k_ee), true = one lane per edge
+  // with per-cell candidate lists in shared memory (k_ee_grouped); same pairs
+  // and results
+  bool ee_grouped = false;
   // narrow-phase pair record of the latest self-collision pass (off by default)
   bool rec_pairs = false;
   DBuf<uint4> rec_vt;
@@ -1232,7 +1236,8 @@ struct Sim {
   void encode_ee(const SCArgs& a, cudaStream_t ss) {
     timed("sc_solve_ee", [&] {
       TC_CK(cudaMemsetAsync(ccd_n.p, 0, sizeof(uint32_t), ss));
-      k_ee<<<grid(ne, 8), 256, 0, ss>>>(a);
+      if (ee_grouped) k_ee_grouped<<<grid(ne, 32 * tcloth::kEeWarps), 32 * tcloth::kEeWarps, 0, ss>>>(a);
+      else k_ee<<<grid(ne, 8), 256, 0, ss>>>(a);
     });
     timed("sc_solve_ee_ccd", [&] { k_ee_ccd<<<148 * 8, 256, 0, ss>>>(a); });
   }
@@ -4255,6 +4260,16 @@ tc_status tc_bake_get(tc_bake* b, uint32_t* texels, float* infos, uint32_t* acti
 tc_status tc_bake_destroy(tc_bake* b) {
   delete b;
   return TC_OK;
+}
+
+// ---- kernel variants of the self-collision pass (results identical)
+tc_status tc_set_self_collision_variant(tc_sim* s, uint32_t ee_variant) {
+  return guard([&] {
+    need(ee_variant <= 1u, "ee_variant: 0 (warp per edge) or 1 (grouped by cell)");
+    Sim& m = S(s);
+    m.ee_grouped = ee_variant == 1u;
+    m.mark();
+  });
 }
 
 // ---- narrow-phase pair lists of the direct self-collision pass

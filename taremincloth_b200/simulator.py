@@ -440,6 +440,10 @@ class ClothSimulator:
         """Make position read-backs raise FloatingPointError on NaN / Inf."""
         self._c(self._L.tc_set_nonfinite_check(self._h, int(bool(enable))))
 
+    def set_self_collision_variant(self, ee_variant=1):
+        """Edge-edge kernel shape: 0 warp per edge, 1 grouped by cell (same results)."""
+        self._c(self._L.tc_set_self_collision_variant(self._h, int(ee_variant)))
+
     # ---------------- narrow-phase pair lists (parity instrumentation)
     def set_pair_recording(self, enable=True, max_vt_pairs=1 << 20, max_ee_pairs=1 << 20):
         """Record, at every self-collision pass, the direct pass's V-T pairs that

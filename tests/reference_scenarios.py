@@ -540,3 +540,30 @@ def self_collision_symmetry(cls, inv_top, inv_bottom):
     x, _ = _state(s)
     d = x[:, 2] - np.asarray(pos)[:, 2]
     return dict(bottom=float(d[:nx * ny].sum()), top=float(d[nx * ny:].sum()), x=x)
+
+
+# --------------------------------------------------------------------------
+# bone SDF collider (collision.wgsl bone phase; simulation/tests.rs:443-554)
+
+def bone_plane_atlas(size=16):
+    """16^3 atlas of one bone over [-0.5, 0.5]^3 whose distance is the texel
+    centre's z (f16 distance, f16 alpha 1), and its 20-float bone info
+    (AABB, uvw scale with blend 0.05, uvw offset, friction 0.3, thickness
+    0.02)."""
+    z = -0.5 + (np.arange(size) + 0.5) / size
+    d = np.repeat(z.astype(np.float16), size * size).view(np.uint16).astype(np.uint32)
+    alpha = np.uint32(np.float16(1.0).view(np.uint16))
+    tex = (d | (alpha << np.uint32(16))).astype(np.uint32)
+    info = np.array([[-0.5, -0.5, -0.5, 0.0, 0.5, 0.5, 0.5, 0.0, 1.0, 1.0, 1.0, 0.05,
+                      0.5, 0.5, 0.5, 0.0, 0.3, 0.02, 0.0, 0.0]], _f32)
+    return tex, info
+
+
+def bone_mats(dz):
+    """(world, inverse world) of a bone translated by dz along z, as the
+    shaders store them (translation in the last column)."""
+    w = np.eye(4, dtype=_f32)[None].copy()
+    w[0, 3, 2] = dz
+    iw = np.eye(4, dtype=_f32)[None].copy()
+    iw[0, 3, 2] = -dz
+    return w, iw

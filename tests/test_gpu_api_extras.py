@@ -92,9 +92,11 @@ def test_config_json_roundtrip_and_hash():
     assert d["gravity"] == [0.0, 0.0, -9.81] and d["damping"] == 1.0 and d["solver_iterations"] == 2
     assert d["enable_self_collision"] is True and d["relief_factor"] == 0.2
     # stiffness is exported from the stored f32 compliance 1/k (config_impl.rs:80-91)
-    back = lambda k: float(np.float32(1.0) / (np.float32(1.0) / np.float32(k)))  # noqa: E731
-    assert d["tension_stiffness"] == back(1000.0) and d["compression_stiffness"] == back(1000.0)
-    assert d["shear_stiffness"] == back(500.0) and d["bending_stiffness"] == back(10.0)
+    # (the text holds the shortest f32 digits: compare as f32)
+    back = lambda k: np.float32(1.0) / (np.float32(1.0) / np.float32(k))  # noqa: E731
+    f32 = lambda key: np.float32(d[key])  # noqa: E731
+    assert f32("tension_stiffness") == back(1000.0) and f32("compression_stiffness") == back(1000.0)
+    assert f32("shear_stiffness") == back(500.0) and f32("bending_stiffness") == back(10.0)
     h0 = s.get_config_hash()
     d.update(damping=2.5, tension_damping=3.0, solver_iterations=5, enable_edge_collision=True,
              edge_margin_offset=0.002, strain_tolerance=0.01, areal_density=0.2, gravity=[0.0, -9.81, 0.0],

@@ -123,9 +123,15 @@ def test_pair_lists_bit_exact(oracle_lib, n, subdiv, frames):
 def test_pair_record_overflow_is_reported():
     sc = scenes.config2(n=48, subdiv=3)
     g = scenes.build(ClothSimulator, sc)
+    for _ in range(3):  # into contact
+        g.step(sc["dt"], sc["substeps"])
+    g.set_pair_recording(True)
+    g.step(sc["dt"] / sc["substeps"], 1)
+    n_vt, n_ee = (len(v) for v in g.get_pair_lists().values())
+    assert n_vt > 16 and n_ee > 16, (n_vt, n_ee)
     g.set_pair_recording(True, 16, 16)
     g.step(sc["dt"] / sc["substeps"], 1)
-    with pytest.raises(ValueError):
+    with pytest.raises(ValueError, match="overflowed"):
         g.get_pair_lists()
 
 
@@ -271,3 +277,36 @@ def test_barrier_timeout_reports_status_and_context_survives(oracle_lib):
     o = scenes.build(oracle_lib.OracleSim, sc)
     worst, _ = compare_frames(g, o, 2, sc["dt"], sc["substeps"], extent(sc["positions"]))
     assert worst.max() <= 1e-5
+
+
+@pytest.mark.parametrize("n,subdiv,frames", [(96, 4, 3), (256, 5, 1)])
+def test_grouped_ee_kernel_matches(oracle_lib, n, subdiv, frames):
+    """The grouped edge-edge kernel (one lane per edge, per-cell candidate
+    lists in shared memory) against the warp-per-edge kernel: identical pair
+    lists and bit-identical positions; at the smaller size also the oracle's
+    pair lists."""
+    sc = scenes.config2(n=n, subdiv=subdiv)
+    a = scenes.build(ClothSimulator, sc)
+    b = scenes.build(ClothSimulator, sc)
+    b.set_self_collision_variant(1)
+    for s in (a, b):
+        s.set_pair_recording(True, 1 << 22, 1 << 22)
+    for _ in range(frames):
+        a.step(sc["dt"], sc["substeps"])
+        b.step(sc["dt"], sc["substeps"])
+        la, lb = a.get_pair_lists(), b.get_pair_lists()
+        assert len(la["ee"]) > 100
+        np.testing.assert_array_equal(la["ee"], lb["ee"])
+        np.testing.assert_array_equal(la["vt"], lb["vt"])
+        np.testing.assert_array_equal(a.get_state()[0], b.get_state()[0])
+        np.testing.assert_array_equal(a.get_state()[2], b.get_state()[2])
+    if n <= 96:
+        x, _, v = b.get_state()
+        o = scenes.build(oracle_lib.OracleSim, sc)
+        o.set_state(x, v)
+        b.set_positions_and_velocities(x, v)
+        o.set_pair_recording(True)
+        dts = sc["dt"] / sc["substeps"]
+        b.step(dts, 1)
+        o.step(dts, 1)
+        np.testing.assert_array_equal(b.get_pair_lists()["ee"], o.get_pair_lists()["ee"])

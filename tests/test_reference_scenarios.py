@@ -238,3 +238,38 @@ def test_scenario_matches_oracle(oracle_lib, name):
     ext = max(float(np.linalg.norm(o.max(0) - o.min(0))), 1e-3)
     err = float(np.abs(g - o).max()) / ext
     assert err <= 1e-5, (name, err)
+
+
+@pytest.mark.gpu
+def test_bone_sdf_collision(oracle_lib):
+    """simulation/tests.rs:443-554: a vertex falling onto a bone SDF whose
+    surface is z = 0 stops at the summed thickness (0.04, within 2 mm, not
+    above 0.06); moving the bone up 0.1 pushes it to z >= 0.14 - 2 mm.  The
+    CUDA path's positions are also compared with the oracle's, given the same
+    atlas, bone infos and transforms."""
+    from taremincloth_b200 import ClothSimulator
+    tex, info = rs.bone_plane_atlas()
+    g = rs._mk(ClothSimulator, [[0.0, 0.0, 0.4]], np.zeros((0, 2)))
+    o = rs._mk(oracle_lib.OracleSim, [[0.0, 0.0, 0.4]], np.zeros((0, 2)))
+    g.set_bone_sdf_colliders(16, 16, 16, tex.tobytes(), info)
+
+    def pose(dz):
+        w, iw = rs.bone_mats(dz)
+        g.update_bone_transforms(w, iw)
+        xf = np.concatenate([w.reshape(1, 16), iw.reshape(1, 16)], 1)
+        o.set_bone_sdf((16, 16, 16), tex, g.get_bone_infos(), xf)
+
+    pose(0.0)
+    for _ in range(60):
+        g.step(1.0 / 60.0, 20)
+        o.step(1.0 / 60.0, 20)
+    z = float(g.get_state()[0][0, 2])
+    assert 0.04 - 2e-3 <= z <= 0.06, z
+    assert abs(z - float(o.get_state()[0][0, 2])) <= 1e-6
+    pose(0.1)
+    for _ in range(30):
+        g.step(1.0 / 60.0, 20)
+        o.step(1.0 / 60.0, 20)
+    zm = float(g.get_state()[0][0, 2])
+    assert zm >= 0.14 - 2e-3, zm
+    assert abs(zm - float(o.get_state()[0][0, 2])) <= 1e-6
