@@ -607,6 +607,10 @@ struct Sim {
   size_t st_smem = 0;
   DBuf<uint2> st_vrange, st_pins;
   DBuf<uint32_t> st_dist, st_bend, st_dperm, st_bperm;
+  DBuf<uint2> st_dids;
+  DBuf<uint4> st_bids;
+  DBuf<float4> st_dpar, st_bpar;
+  DBuf<float> st_dlam, st_blam;
   std::vector<uint2> inst_prims_h;
   DBuf<uint32_t> vinst;
   DBuf<uint2> inst_prims;
@@ -856,6 +860,7 @@ struct Sim {
     }
     dist_ids.upload(ids, st);
     dist_par.upload(par, st);
+    st_stale = true;  // the staged solver's copies follow on its next frame
     TC_CK(cudaStreamSynchronize(st));
   }
   void upload_bend() {
@@ -867,6 +872,7 @@ struct Sim {
       par[i] = make_float4(c.rest, c.comp, c.pad0, c.pad1);
     }
     bend_ids.upload(ids, st);
+    st_stale = true;
     bend_par.upload(par, st);
     TC_CK(cudaStreamSynchronize(st));
   }
@@ -1629,12 +1635,27 @@ struct Sim {
     st_bend.upload(btab, st);
     st_dperm.upload(dperm, st);
     st_bperm.upload(bperm, st);
+    // the records in staged order
+    const uint32_t ndp = uint32_t(dperm.size()), nbp = uint32_t(bperm.size());
+    st_dids.alloc(ndp); st_dpar.alloc(ndp); st_dlam.alloc(ndp);
+    st_bids.alloc(nbp); st_bpar.alloc(nbp); st_blam.alloc(nbp);
+    if (ndp) {
+      k_stage_gather<<<grid(ndp, 256), 256, 0, st>>>(ndp, st_dperm.p, dist_ids.p, st_dids.p);
+      k_stage_gather<<<grid(ndp, 256), 256, 0, st>>>(ndp, st_dperm.p, dist_par.p, st_dpar.p);
+    }
+    if (nbp) {
+      k_stage_gather<<<grid(nbp, 256), 256, 0, st>>>(nbp, st_bperm.p, bend_ids.p, st_bids.p);
+      k_stage_gather<<<grid(nbp, 256), 256, 0, st>>>(nbp, st_bperm.p, bend_par.p, st_bpar.p);
+    }
+    TC_CK(cudaGetLastError());
     TC_CK(cudaStreamSynchronize(st));
     st_bins = B;
     st_stale = false;
+    mark();  // a captured frame holds the old tables
   }
   void launch_staged(const SolverArgs& a) {
-    const StageTables t{st_vrange.p, st_pins.p, st_dist.p, st_bend.p, st_dperm.p, st_bperm.p, st_cap};
+    const StageTables t{st_vrange.p, st_pins.p, st_dist.p, st_bend.p, st_dids.p, st_dpar.p, st_dlam.p,
+                        st_bids.p,   st_bpar.p, st_blam.p, st_cap};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(st_bins * kStageCtas);
     cfg.blockDim = dim3(kStageThreads);

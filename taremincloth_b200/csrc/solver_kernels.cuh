@@ -136,17 +136,15 @@ __global__ void k_pin(uint32_t npins, const uint32_t* __restrict__ pin_v, const 
 
 // One distance constraint (shaders/distance.wgsl:60-124).  dist_par =
 // (rest, tension compliance, compression compliance, shear flag).
+// distance_core takes the constraint's record (ids e, params c) and lambda l
+// already loaded and writes the new lambda to *lam_out.
 template <class M>
-__device__ __forceinline__ void project_distance_m(uint32_t ci, const uint2* __restrict__ ids,
-                                                   const float4* __restrict__ par, const M& m,
-                                                   float* __restrict__ lam, const SubstepParams& sp, bool damped) {
-  const uint2 e = ids[ci];
-  const float4 c = par[ci];
+__device__ __forceinline__ void distance_core(uint2 e, float4 c, float l, float* __restrict__ lam_out, const M& m,
+                                              const SubstepParams& sp, bool damped) {
   // every load of the constraint issued together: within a colour no other
   // thread writes these addresses, so this changes latency, not results
   const float4 xa = m.ldx(e.x), xb = m.ldx(e.y);
   const float4 q0 = m.ldp(e.x), q1 = m.ldp(e.y);
-  const float l = ld1<M::kCg>(lam + ci);
   const float w0 = xa.w, w1 = xb.w;
   const float ws = w0 + w1;
   if (ws <= kEps) return;
@@ -167,7 +165,7 @@ __device__ __forceinline__ void project_distance_m(uint32_t ci, const uint2* __r
     const V3 rel = (p0 - mk(xa)) - (p1 - mk(xb));
     const float vp = dot(dir, rel);
     const float dl = (-cv - alpha * l - gamma * vp) / ((1.0f + gamma) * ws + alpha);
-    lam[ci] = l + dl;
+    *lam_out = l + dl;
     const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
     m.stp(e.x, make_float4(n0.x, n0.y, n0.z, q0.w));
     m.stp(e.y, make_float4(n1.x, n1.y, n1.z, q1.w));
@@ -175,10 +173,16 @@ __device__ __forceinline__ void project_distance_m(uint32_t ci, const uint2* __r
   }
   // gamma == 0: (-cv - alpha*l - 0*vp) / (1*ws + alpha)
   const float dl = (-cv - alpha * l) / (1.0f * ws + alpha);
-  lam[ci] = l + dl;
+  *lam_out = l + dl;
   const V3 n0 = p0 + dir * (w0 * dl), n1 = p1 + dir * (-w1 * dl);
   m.stp(e.x, make_float4(n0.x, n0.y, n0.z, q0.w));
   m.stp(e.y, make_float4(n1.x, n1.y, n1.z, q1.w));
+}
+template <class M>
+__device__ __forceinline__ void project_distance_m(uint32_t ci, const uint2* __restrict__ ids,
+                                                   const float4* __restrict__ par, const M& m,
+                                                   float* __restrict__ lam, const SubstepParams& sp, bool damped) {
+  distance_core(ids[ci], par[ci], ld1<M::kCg>(lam + ci), lam + ci, m, sp, damped);
 }
 template <bool kCg>
 __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __restrict__ ids,
@@ -199,17 +203,14 @@ __global__ void k_distance(uint32_t off, uint32_t cnt, const uint2* __restrict__
 
 // One bending constraint (shaders/bending.wgsl:59-126).  bend_par =
 // (rest, compliance, kind, seam gap).
+// bending_core: the record (ids e, params c) and lambda l already loaded
 template <class M>
-__device__ __forceinline__ void project_bending_m(uint32_t ci, const uint4* __restrict__ ids,
-                                                  const float4* __restrict__ par, const M& m,
-                                                  float* __restrict__ lam, const SubstepParams& sp, bool damped) {
-  const float4 c = par[ci];
-  const uint4 e = ids[ci];
+__device__ __forceinline__ void bending_core(uint4 e, float4 c, float l, float* __restrict__ lam_out, const M& m,
+                                             const SubstepParams& sp, bool damped) {
   if (c.y >= 1e9f) return;
   // loads of the written pair issued together (see project_distance)
   const float4 xc = m.ldx(e.z), xd = m.ldx(e.w);
   const float4 q2 = m.ldp(e.z), q3 = m.ldp(e.w);
-  const float l = ld1<M::kCg>(lam + ci);
   const float w2 = xc.w, w3 = xd.w;
   const float ws = w2 + w3;
   if (ws <= kEps) return;
@@ -236,10 +237,18 @@ __device__ __forceinline__ void project_bending_m(uint32_t ci, const uint4* __re
   } else {
     dl = (-cv - alpha * l) / (1.0f * ws + alpha);
   }
-  lam[ci] = l + dl;
+  *lam_out = l + dl;
   const V3 n2 = p2 + dir * (w2 * dl), n3 = p3 + dir * (-w3 * dl);
   m.stp(e.z, make_float4(n2.x, n2.y, n2.z, q2.w));
   m.stp(e.w, make_float4(n3.x, n3.y, n3.z, q3.w));
+}
+template <class M>
+__device__ __forceinline__ void project_bending_m(uint32_t ci, const uint4* __restrict__ ids,
+                                                  const float4* __restrict__ par, const M& m,
+                                                  float* __restrict__ lam, const SubstepParams& sp, bool damped) {
+  const float4 c = par[ci];
+  if (c.y >= 1e9f) return;
+  bending_core(ids[ci], c, ld1<M::kCg>(lam + ci), lam + ci, m, sp, damped);
 }
 template <bool kCg>
 __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __restrict__ ids,
@@ -1030,15 +1039,52 @@ struct SMem {
   __device__ __forceinline__ void stp(uint32_t i, float4 v) const { *at(sp, i) = v; }
   __device__ __forceinline__ void stv(uint32_t i, float4 v) const { *at(sv, i) = v; }
 };
+// The constraint records are copied into staged arrays in (bin, colour,
+// owner) order, so a colour step reads them coalesced without an index
+// indirection; the staged lambdas are the solver's lambdas in that order
+// (cleared every substep, read and written only by their own constraint).
 struct StageTables {
   const uint2* vrange;        // [bins] vertex range [x, y)
   const uint2* pins;          // [bins * K] (first, count) into pin_v / pin_t, by owning slice
-  const uint32_t* dist;       // [bins * ndc * (K + 1)] offsets into dist_perm per (bin, colour, owner)
+  const uint32_t* dist;       // [bins * ndc * (K + 1)] offsets into the staged distance arrays
   const uint32_t* bend;       // [bins * nbc * (K + 1)]
-  const uint32_t* dist_perm;
-  const uint32_t* bend_perm;
+  const uint2* dist_ids;      // staged records and lambdas
+  const float4* dist_par;
+  float* dist_lam;
+  const uint4* bend_ids;
+  const float4* bend_par;
+  float* bend_lam;
   uint32_t cap;               // vertices per slice (the shared-memory capacity)
 };
+// gather of the staged records: out[k] = in[perm[k]]
+template <class T>
+__global__ void k_stage_gather(uint32_t cnt, const uint32_t* __restrict__ perm, const T* __restrict__ in,
+                               T* __restrict__ out) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < cnt) out[k] = in[perm[k]];
+}
+// Records of a colour step held one step ahead: the first kStagePf
+// constraints of this thread in the colour (k = lo + tid + q * blockDim).
+constexpr int kStagePf = 2;
+template <class Id>
+struct StageBuf {
+  Id e[kStagePf];
+  float4 c[kStagePf];
+  float l[kStagePf];
+};
+template <class Id>
+__device__ __forceinline__ void stage_fetch(StageBuf<Id>& b, uint32_t lo, uint32_t hi, const Id* ids,
+                                            const float4* par, const float* lam) {
+#pragma unroll
+  for (int q = 0; q < kStagePf; ++q) {
+    const uint32_t k = lo + threadIdx.x + uint32_t(q) * blockDim.x;
+    if (k < hi) {
+      b.e[q] = ids[k];
+      b.c[q] = par[k];
+      b.l[q] = lam[k];
+    }
+  }
+}
 template <uint32_t K, bool kBone>
 __global__ void __launch_bounds__(512, 1) k_solver_staged(SolverArgs a, StageTables t) {
   cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
@@ -1060,12 +1106,13 @@ __global__ void __launch_bounds__(512, 1) k_solver_staged(SolverArgs a, StageTab
   const uint32_t* btab = t.bend + size_t(bin) * a.nbc * (K + 1u);
   const float dts = a.sp.dt;
   for (uint32_t sub = 0; sub < a.nsub; ++sub) {
+    // each CTA clears the lambdas of its own constraints (which only it reads)
     for (uint32_t c = 0; c < a.ndc; ++c)
       for (uint32_t k = dtab[c * (K + 1u) + rank] + threadIdx.x; k < dtab[c * (K + 1u) + rank + 1u]; k += blockDim.x)
-        a.dlam[t.dist_perm[k]] = 0.f;
+        t.dist_lam[k] = 0.f;
     for (uint32_t c = 0; c < a.nbc; ++c)
       for (uint32_t k = btab[c * (K + 1u) + rank] + threadIdx.x; k < btab[c * (K + 1u) + rank + 1u]; k += blockDim.x)
-        a.blam[t.bend_perm[k]] = 0.f;
+        t.bend_lam[k] = 0.f;
     for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) predict_vertex_m(i, m, a.sp);
     cl.sync();
     for (uint32_t it = 0; it < a.iters; ++it) {
@@ -1073,19 +1120,49 @@ __global__ void __launch_bounds__(512, 1) k_solver_staged(SolverArgs a, StageTab
         for (uint32_t k = pr.x + threadIdx.x; k < pr.x + pr.y; k += blockDim.x) pin_one_m(k, a.pin_v, a.pin_t, m, dts);
         cl.sync();
       }
-      for (uint32_t c = 0; c < a.ndc; ++c) {
-        const uint32_t* r = dtab + c * (K + 1u);
-        if (r[0] == r[K]) continue;  // the bin has no constraint of this colour (same test in every CTA)
-        for (uint32_t k = r[rank] + threadIdx.x; k < r[rank + 1u]; k += blockDim.x)
-          project_distance_m(t.dist_perm[k], a.dist_ids, a.dist_par, m, a.dlam, a.sp, a.ddamp);
-        cl.sync();
+      // colour steps; each loads the next colour's first records before its
+      // own work, so their latency overlaps the work and the barrier
+      if (a.ndc) {
+        StageBuf<uint2> cur, nxt;
+        stage_fetch(cur, dtab[rank], dtab[rank + 1u], t.dist_ids, t.dist_par, t.dist_lam);
+        for (uint32_t c = 0; c < a.ndc; ++c) {
+          const uint32_t* r = dtab + c * (K + 1u);
+          if (c + 1u < a.ndc)
+            stage_fetch(nxt, r[K + 1u + rank], r[K + 2u + rank], t.dist_ids, t.dist_par, t.dist_lam);
+          if (r[0] != r[K]) {  // the bin has constraints of this colour (same test in every CTA)
+            const uint32_t lo = r[rank], hi = r[rank + 1u];
+#pragma unroll
+            for (int q = 0; q < kStagePf; ++q) {
+              const uint32_t k = lo + threadIdx.x + uint32_t(q) * blockDim.x;
+              if (k < hi) distance_core(cur.e[q], cur.c[q], cur.l[q], t.dist_lam + k, m, a.sp, a.ddamp);
+            }
+            for (uint32_t k = lo + threadIdx.x + kStagePf * blockDim.x; k < hi; k += blockDim.x)
+              distance_core(t.dist_ids[k], t.dist_par[k], t.dist_lam[k], t.dist_lam + k, m, a.sp, a.ddamp);
+            cl.sync();
+          }
+          cur = nxt;
+        }
       }
-      for (uint32_t c = 0; c < a.nbc; ++c) {
-        const uint32_t* r = btab + c * (K + 1u);
-        if (r[0] == r[K]) continue;
-        for (uint32_t k = r[rank] + threadIdx.x; k < r[rank + 1u]; k += blockDim.x)
-          project_bending_m(t.bend_perm[k], a.bend_ids, a.bend_par, m, a.blam, a.sp, a.bdamp);
-        cl.sync();
+      if (a.nbc) {
+        StageBuf<uint4> cur, nxt;
+        stage_fetch(cur, btab[rank], btab[rank + 1u], t.bend_ids, t.bend_par, t.bend_lam);
+        for (uint32_t c = 0; c < a.nbc; ++c) {
+          const uint32_t* r = btab + c * (K + 1u);
+          if (c + 1u < a.nbc)
+            stage_fetch(nxt, r[K + 1u + rank], r[K + 2u + rank], t.bend_ids, t.bend_par, t.bend_lam);
+          if (r[0] != r[K]) {
+            const uint32_t lo = r[rank], hi = r[rank + 1u];
+#pragma unroll
+            for (int q = 0; q < kStagePf; ++q) {
+              const uint32_t k = lo + threadIdx.x + uint32_t(q) * blockDim.x;
+              if (k < hi) bending_core(cur.e[q], cur.c[q], cur.l[q], t.bend_lam + k, m, a.sp, a.bdamp);
+            }
+            for (uint32_t k = lo + threadIdx.x + kStagePf * blockDim.x; k < hi; k += blockDim.x)
+              bending_core(t.bend_ids[k], t.bend_par[k], t.bend_lam[k], t.bend_lam + k, m, a.sp, a.bdamp);
+            cl.sync();
+          }
+          cur = nxt;
+        }
       }
       if (a.hascol && a.coupled) {
         for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) collide_vertex_m<kBone>(i, m, a.ca, dts);

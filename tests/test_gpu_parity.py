@@ -290,7 +290,7 @@ def test_grouped_ee_kernel_matches(oracle_lib, n, subdiv, frames):
     b = scenes.build(ClothSimulator, sc)
     b.set_self_collision_variant(1)
     for s in (a, b):
-        s.set_pair_recording(True, 1 << 22, 1 << 22)
+        s.set_pair_recording(True, 1 << 24, 1 << 23)
     for _ in range(frames):
         a.step(sc["dt"], sc["substeps"])
         b.step(sc["dt"], sc["substeps"])
