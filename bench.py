@@ -241,7 +241,9 @@ def batch_extra(steps):
     return {"workload": "64 uneven cloths (sides log-uniform 32..192, 657683 vertices), 10 substeps x 5 iterations",
             "batched_vertex_substeps_per_s": vs / (tb / 1e3), "separate_vertex_substeps_per_s": vs / (ts / 1e3),
             "separate_wall_vertex_substeps_per_s": vs / wall, "speedup_device": ts / tb,
-            "batched_ms_per_frame": tb / steps, "launch_config": {k: tune[k] for k in ("persistent", "blocks_per_sm")}}
+            "batched_ms_per_frame": tb / steps,
+            "launch_config": {k: tune[k] for k in ("persistent", "blocks_per_sm", "block")},
+            "launch_trials": tune["trials"]}
 
 
 def bone_sdf_extra(steps):
@@ -480,7 +482,10 @@ def main():
     # launch shape (per-colour launches vs persistent solver): results are
     # bit-identical, the autotuner keeps the faster and restores the state
     from taremincloth_b200.autotune import autotune
-    tune = autotune(sim, dt, sub, frames=2)
+    # hash cells tried besides the reference formula's (the parity setting):
+    # BASELINE's 2 x thickness and two larger ones; kept only within tolerance
+    tune = autotune(sim, dt, sub, frames=2,
+                    tune_cell_sizes=[2.0 * sc["thickness"], 1.25 * sim.get_cell_size(), 1.5 * sim.get_cell_size()])
     # the end-to-end loop below restarts from this state, so both numbers
     # cover the same frames of the drape (later frames cost more)
     x_warm, _, v_warm = sim.get_state()
@@ -570,7 +575,11 @@ def main():
                    "l2": "256 MB buffer written before every timed step", "parallelism": f"replicas x{world}",
                    "path": "plain XPBD, CUDA graph per frame",
                    "launch_shape": ("persistent solver, %d blocks/SM" % tune["blocks_per_sm"]) if tune["persistent"]
-                   is True else "one launch per colour (programmatic dependent launch)"},
+                   is True else "one launch per colour (programmatic dependent launch), %d threads per block"
+                   % tune["block"],
+                   "hash_cell": "reference formula (%.4g m)" % sim.get_cell_size() if tune.get("hash_cell") is None
+                   else "autotuned %.4g m" % tune["hash_cell"]},
+        "autotune": {"launch_trials": tune["trials"], "hash_cell_trials": tune.get("hash_cell_trials")},
         "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs", "traffic": traffic,
                      "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms, "l2": l2},

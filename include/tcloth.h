@@ -353,6 +353,16 @@ tc_status tc_device_status(int device, int *lost, uint64_t *epoch);
  * positions hold NaN or Inf (the copy is still written).  Off by default, as
  * in the reference, whose read-backs return whatever the GPU holds. */
 tc_status tc_set_nonfinite_check(tc_sim *s, int enable);
+/* Autotuned settings (new).  tc_set_launch_block: threads per block of the
+ * one-launch-per-colour constraint kernels (64 .. 1024, powers of two);
+ * results do not change.  tc_set_hash_cell_size: the spatial-hash cell of
+ * the self-collision passes; cell <= 0 restores the reference formula's
+ * value (pipelines.rs:898-912), which is the parity setting.  Another cell
+ * changes which neighbours are seen, so it is a physics setting: the
+ * autotuner keeps one only when positions and residual stay within stated
+ * bounds of the reference cell's. */
+tc_status tc_set_launch_block(tc_sim *s, uint32_t threads);
+tc_status tc_set_hash_cell_size(tc_sim *s, float cell);
 /* Kernel shape of the direct pass's edge-edge search (new; results and pair
  * lists do not change): 0 = one warp per edge over the 27 neighbour cells;
  * 1 = one lane per edge, a warp taking 32 edges of the hash-sorted order and

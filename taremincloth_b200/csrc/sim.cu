@@ -884,6 +884,7 @@ struct Sim {
     TC_CK(cudaEventCreate(&ev0));
     TC_CK(cudaEventCreate(&ev1));
     m = build_mesh(in);
+    cell_ref = m.cell;
     n = m.n;
     nd = uint32_t(m.dist.size());
     nb = uint32_t(m.bend.size());
@@ -1194,6 +1195,10 @@ struct Sim {
     a.rec_ee_cap = rec_pairs ? rec_ee_cap : 0u;
     return a;
   }
+  // threads per block of the per-colour constraint launches (autotuned;
+  // results do not depend on it)
+  uint32_t col_block = 256;
+  float cell_ref = 0.f;  // the reference formula's hash cell (tc_set_hash_cell_size can override m.cell)
   // E-E kernel: false = one warp per edge (k_ee), true = one lane per edge
   // with per-cell candidate lists in shared memory (k_ee_grouped); same pairs
   // and results
@@ -1833,20 +1838,20 @@ struct Sim {
       for (size_t c = 0; c < m.dist_cnt.size(); ++c)
         if (m.dist_cnt[c]) {
           if (gate)
-            launch_k(k_distance_gated, grid(m.dist_cnt[c], 256), 256, gate, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
+            launch_k(k_distance_gated, grid(m.dist_cnt[c], col_block), col_block, gate, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
                      dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
           else
-            launch_k(k_distance, grid(m.dist_cnt[c], 256), 256, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
+            launch_k(k_distance, grid(m.dist_cnt[c], col_block), col_block, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
                      dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
         }
       if (nsw) launch_sewing(dts, gate);
       for (size_t c = 0; c < m.bend_cnt.size(); ++c)
         if (m.bend_cnt[c]) {
           if (gate)
-            launch_k(k_bending_gated, grid(m.bend_cnt[c], 256), 256, gate, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
+            launch_k(k_bending_gated, grid(m.bend_cnt[c], col_block), col_block, gate, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
                      bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
           else
-            launch_k(k_bending, grid(m.bend_cnt[c], 256), 256, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
+            launch_k(k_bending, grid(m.bend_cnt[c], col_block), col_block, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
                      bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
         }
       if (hascol && use_coupled) {
@@ -2002,14 +2007,14 @@ struct Sim {
         timed("distance", [&] {
           for (size_t c = 0; c < m.dist_cnt.size(); ++c)
             if (m.dist_cnt[c])
-              launch_k(k_distance, grid(m.dist_cnt[c], 256), 256, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
+              launch_k(k_distance, grid(m.dist_cnt[c], col_block), col_block, m.dist_off[c], m.dist_cnt[c], dist_ids.p,
                        dist_par.p, x4.p, p4.p, dlam.p, sp, ddamp);
         });
         if (nsw) timed("sewing", [&] { launch_sewing(dts); });
         timed("bending", [&] {
           for (size_t c = 0; c < m.bend_cnt.size(); ++c)
             if (m.bend_cnt[c])
-              launch_k(k_bending, grid(m.bend_cnt[c], 256), 256, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
+              launch_k(k_bending, grid(m.bend_cnt[c], col_block), col_block, m.bend_off[c], m.bend_cnt[c], bend_ids.p,
                        bend_par.p, x4.p, p4.p, blam.p, sp, bdamp);
         });
         if (hascol && use_coupled) timed("collision", [&] { launch_collision(ca, dts); });
@@ -2247,11 +2252,11 @@ void Sim::encode_residual(const SubstepParams& sp) {
   const size_t kd = m.dist_cnt.size();
   for (size_t c = 0; c < kd; ++c)
     if (m.dist_cnt[c])
-      k_residual_dist<<<grid(m.dist_cnt[c], 256), 256, 0, st>>>(m.dist_off[c], m.dist_cnt[c], dist_ids.p, dist_par.p,
+      k_residual_dist<<<grid(m.dist_cnt[c], col_block), col_block, 0, st>>>(m.dist_off[c], m.dist_cnt[c], dist_ids.p, dist_par.p,
                                                                  p4.p, dlam.p, dt, res_sum.p + c, res_max.p + c);
   for (size_t c = 0; c < m.bend_cnt.size(); ++c)
     if (m.bend_cnt[c])
-      k_residual_bend<<<grid(m.bend_cnt[c], 256), 256, 0, st>>>(m.bend_off[c], m.bend_cnt[c], bend_ids.p, bend_par.p,
+      k_residual_bend<<<grid(m.bend_cnt[c], col_block), col_block, 0, st>>>(m.bend_off[c], m.bend_cnt[c], bend_ids.p, bend_par.p,
                                                                  p4.p, blam.p, dt, res_sum.p + kd + c,
                                                                  res_max.p + kd + c);
 }
@@ -4289,6 +4294,30 @@ tc_status tc_set_self_collision_variant(tc_sim* s, uint32_t ee_variant) {
     need(ee_variant <= 1u, "ee_variant: 0 (warp per edge) or 1 (grouped by cell)");
     Sim& m = S(s);
     m.ee_grouped = ee_variant == 1u;
+    m.mark();
+  });
+}
+
+// ---- autotuned knobs
+tc_status tc_set_launch_block(tc_sim* s, uint32_t threads) {
+  return guard([&] {
+    need(threads == 64 || threads == 128 || threads == 256 || threads == 512 || threads == 1024,
+         "threads per block: 64, 128, 256, 512 or 1024");
+    Sim& m = S(s);
+    m.col_block = threads;
+    m.mark();
+  });
+}
+// spatial-hash cell size (pipelines.rs:898-912 computes the default); a
+// different cell changes which neighbours the self-collision passes see, so
+// it is a physics setting, not a launch shape.  cell <= 0 restores the
+// reference formula's value.
+tc_status tc_set_hash_cell_size(tc_sim* s, float cell) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(std::isfinite(cell), "cell size must be finite");
+    m.m.cell = cell > 0.f ? cell : m.cell_ref;
+    m.ce_stale = true;  // the collider-edge grid uses the same cell
     m.mark();
   });
 }

@@ -440,6 +440,14 @@ class ClothSimulator:
         """Make position read-backs raise FloatingPointError on NaN / Inf."""
         self._c(self._L.tc_set_nonfinite_check(self._h, int(bool(enable))))
 
+    def set_launch_block(self, threads=256):
+        """Threads per block of the per-colour constraint launches (same results)."""
+        self._c(self._L.tc_set_launch_block(self._h, int(threads)))
+
+    def set_hash_cell_size(self, cell=None):
+        """Spatial-hash cell; None restores the reference formula's value."""
+        self._c(self._L.tc_set_hash_cell_size(self._h, 0.0 if cell is None else float(cell)))
+
     def set_self_collision_variant(self, ee_variant=1):
         """Edge-edge kernel shape: 0 warp per edge, 1 grouped by cell (same results)."""
         self._c(self._L.tc_set_self_collision_variant(self._h, int(ee_variant)))

@@ -158,3 +158,30 @@ def test_nonfinite_readback_check():
         s.get_positions(out)
     s.set_nonfinite_check(False)
     s.get_positions(out)
+
+
+def test_launch_block_and_cell_knobs():
+    """Threads per block of the per-colour launches change no bit; a hash cell
+    override changes the cell, None restores the reference formula's value,
+    and the autotuner returns its launch and cell choices."""
+    from taremincloth_b200.autotune import autotune
+    sc = scenes.config2(n=32, subdiv=2)
+    a = scenes.build(ClothSimulator, sc)
+    b = scenes.build(ClothSimulator, sc)
+    for s_ in (a, b):
+        s_.set_launch_config(False)
+    b.set_launch_block(128)
+    for _ in range(3):
+        a.step(sc["dt"], sc["substeps"])
+        b.step(sc["dt"], sc["substeps"])
+    np.testing.assert_array_equal(a.get_state()[0], b.get_state()[0])
+    with pytest.raises(ValueError):
+        b.set_launch_block(100)
+    ref = a.get_cell_size()
+    a.set_hash_cell_size(0.02)
+    assert abs(a.get_cell_size() - 0.02) < 1e-9
+    a.set_hash_cell_size(None)
+    assert a.get_cell_size() == ref
+    t = autotune(a, sc["dt"], sc["substeps"], frames=1, tune_cell_sizes=[1.5 * ref])
+    assert t["block"] in (128, 256, 512) and len(t["hash_cell_trials"]) == 2
+    assert t["hash_cell_trials"][0]["accepted"]
