@@ -1003,7 +1003,7 @@ struct Sim {
       {  // staged cluster solver: slice capacity from the opt-in shared memory, co-resident clusters
         int optin = 0;
         TC_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-        st_cap = uint32_t(optin) / (3u * sizeof(float4));
+        st_cap = std::min<uint32_t>(uint32_t(optin) / uint32_t(3u * sizeof(float4)), 65535u);  // slots fit 16 bits
         st_smem = size_t(st_cap) * 3u * sizeof(float4);
         int ncl = 0;
         if (st_cap > 0 &&
@@ -1644,14 +1644,26 @@ struct Sim {
     const uint32_t ndp = uint32_t(dperm.size()), nbp = uint32_t(bperm.size());
     st_dids.alloc(ndp); st_dpar.alloc(ndp); st_dlam.alloc(ndp);
     st_bids.alloc(nbp); st_bpar.alloc(nbp); st_blam.alloc(nbp);
-    if (ndp) {
-      k_stage_gather<<<grid(ndp, 256), 256, 0, st>>>(ndp, st_dperm.p, dist_ids.p, st_dids.p);
-      k_stage_gather<<<grid(ndp, 256), 256, 0, st>>>(ndp, st_dperm.p, dist_par.p, st_dpar.p);
+    // vertex ids as staged ids: owning slice << 16 | slot in that slice
+    std::vector<uint32_t> sid(n);
+    for (uint32_t b = 0; b < B; ++b) {
+      const uint32_t nv = vr[b].y - vr[b].x, chunk = nv ? (nv + K - 1) / K : 1u;
+      for (uint32_t v = vr[b].x; v < vr[b].y; ++v) {
+        const uint32_t o = v - vr[b].x;
+        sid[v] = ((o / chunk) << 16) | (o % chunk);
+      }
     }
-    if (nbp) {
-      k_stage_gather<<<grid(nbp, 256), 256, 0, st>>>(nbp, st_bperm.p, bend_ids.p, st_bids.p);
-      k_stage_gather<<<grid(nbp, 256), 256, 0, st>>>(nbp, st_bperm.p, bend_par.p, st_bpar.p);
+    std::vector<uint2> dids(ndp);
+    for (uint32_t k = 0; k < ndp; ++k) dids[k] = make_uint2(sid[dist_h[dperm[k]].v0], sid[dist_h[dperm[k]].v1]);
+    std::vector<uint4> bids(nbp);
+    for (uint32_t k = 0; k < nbp; ++k) {
+      const BendC& c = bend_h[bperm[k]];
+      bids[k] = make_uint4(sid[c.v0], sid[c.v1], sid[c.v2], sid[c.v3]);
     }
+    st_dids.upload(dids, st);
+    st_bids.upload(bids, st);
+    if (ndp) k_stage_gather<<<grid(ndp, 256), 256, 0, st>>>(ndp, st_dperm.p, dist_par.p, st_dpar.p);
+    if (nbp) k_stage_gather<<<grid(nbp, 256), 256, 0, st>>>(nbp, st_bperm.p, bend_par.p, st_bpar.p);
     TC_CK(cudaGetLastError());
     TC_CK(cudaStreamSynchronize(st));
     st_bins = B;

@@ -1043,12 +1043,30 @@ struct SMem {
 // owner) order, so a colour step reads them coalesced without an index
 // indirection; the staged lambdas are the solver's lambdas in that order
 // (cleared every substep, read and written only by their own constraint).
+// The same slices addressed by staged vertex ids (owner rank << 16 | slot in
+// the owner's slice), which the staged constraint records carry: no division
+// per access.
+struct SMemE {
+  static constexpr bool kCg = false;
+  float4* sx;
+  float4* sp;
+  uint32_t rank;
+  __device__ __forceinline__ float4* at(float4* a, uint32_t id) const {
+    const uint32_t r = id >> 16;
+    float4* q = a + (id & 0xFFFFu);
+    return r == rank ? q : cooperative_groups::this_cluster().map_shared_rank(q, r);
+  }
+  __device__ __forceinline__ float4 ldx(uint32_t i) const { return *at(sx, i); }
+  __device__ __forceinline__ float4 ldp(uint32_t i) const { return *at(sp, i); }
+  __device__ __forceinline__ void stx(uint32_t i, float4 v) const { *at(sx, i) = v; }
+  __device__ __forceinline__ void stp(uint32_t i, float4 v) const { *at(sp, i) = v; }
+};
 struct StageTables {
   const uint2* vrange;        // [bins] vertex range [x, y)
   const uint2* pins;          // [bins * K] (first, count) into pin_v / pin_t, by owning slice
   const uint32_t* dist;       // [bins * ndc * (K + 1)] offsets into the staged distance arrays
   const uint32_t* bend;       // [bins * nbc * (K + 1)]
-  const uint2* dist_ids;      // staged records and lambdas
+  const uint2* dist_ids;      // staged records (vertex ids as staged ids, see SMemE) and lambdas
   const float4* dist_par;
   float* dist_lam;
   const uint4* bend_ids;
@@ -1095,6 +1113,7 @@ __global__ void __launch_bounds__(512, 1) k_solver_staged(SolverArgs a, StageTab
   const uint32_t nv = vr.y - vr.x;
   const uint32_t chunk = nv > 0 ? (nv + K - 1) / K : 1u;
   const SMem m{stage, stage + t.cap, stage + 2 * t.cap, vr.x, chunk, rank};
+  const SMemE me{stage, stage + t.cap, rank};
   const uint32_t lo = vr.x + min(rank * chunk, nv), hi = vr.x + min((rank + 1u) * chunk, nv);
   for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     m.sx[i - lo] = a.x4[i];
@@ -1134,10 +1153,10 @@ __global__ void __launch_bounds__(512, 1) k_solver_staged(SolverArgs a, StageTab
 #pragma unroll
             for (int q = 0; q < kStagePf; ++q) {
               const uint32_t k = lo + threadIdx.x + uint32_t(q) * blockDim.x;
-              if (k < hi) distance_core(cur.e[q], cur.c[q], cur.l[q], t.dist_lam + k, m, a.sp, a.ddamp);
+              if (k < hi) distance_core(cur.e[q], cur.c[q], cur.l[q], t.dist_lam + k, me, a.sp, a.ddamp);
             }
             for (uint32_t k = lo + threadIdx.x + kStagePf * blockDim.x; k < hi; k += blockDim.x)
-              distance_core(t.dist_ids[k], t.dist_par[k], t.dist_lam[k], t.dist_lam + k, m, a.sp, a.ddamp);
+              distance_core(t.dist_ids[k], t.dist_par[k], t.dist_lam[k], t.dist_lam + k, me, a.sp, a.ddamp);
             cl.sync();
           }
           cur = nxt;
@@ -1155,10 +1174,10 @@ __global__ void __launch_bounds__(512, 1) k_solver_staged(SolverArgs a, StageTab
 #pragma unroll
             for (int q = 0; q < kStagePf; ++q) {
               const uint32_t k = lo + threadIdx.x + uint32_t(q) * blockDim.x;
-              if (k < hi) bending_core(cur.e[q], cur.c[q], cur.l[q], t.bend_lam + k, m, a.sp, a.bdamp);
+              if (k < hi) bending_core(cur.e[q], cur.c[q], cur.l[q], t.bend_lam + k, me, a.sp, a.bdamp);
             }
             for (uint32_t k = lo + threadIdx.x + kStagePf * blockDim.x; k < hi; k += blockDim.x)
-              bending_core(t.bend_ids[k], t.bend_par[k], t.bend_lam[k], t.bend_lam + k, m, a.sp, a.bdamp);
+              bending_core(t.bend_ids[k], t.bend_par[k], t.bend_lam[k], t.bend_lam + k, me, a.sp, a.bdamp);
             cl.sync();
           }
           cur = nxt;

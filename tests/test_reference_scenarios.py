@@ -273,3 +273,20 @@ def test_bone_sdf_collision(oracle_lib):
     zm = float(g.get_state()[0][0, 2])
     assert zm >= 0.14 - 2e-3, zm
     assert abs(zm - float(o.get_state()[0][0, 2])) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_single_layer_disables_effective_untangling():
+    """simulation/tests.rs:392-441: untangling is on by default but effective
+    only with several layers; turning the option off disables it."""
+    from taremincloth_b200 import ClothSimulator
+    quad = dict(positions=[[0, 0, 0.5], [1, 0, 0.5], [1, 1, 0.5], [0, 1, 0.5]],
+                edges=[[0, 1], [1, 2], [2, 3], [3, 0], [0, 2]], faces=[[0, 1, 2], [0, 2, 3]])
+    s = rs._mk(ClothSimulator, quad["positions"], quad["edges"], faces=quad["faces"])
+    assert not s.get_has_multiple_layers()
+    assert not s.get_effective_normal_untangling()
+    s2 = rs._mk(ClothSimulator, quad["positions"], quad["edges"], faces=quad["faces"], layer_ids=[0, 0, 1, 1])
+    assert s2.get_has_multiple_layers()
+    assert s2.get_effective_normal_untangling()
+    s2.set_self_collision_options(0.2, 0.2, True, False, 128)
+    assert not s2.get_effective_normal_untangling()
