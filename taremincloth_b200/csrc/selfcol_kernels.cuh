@@ -338,6 +338,52 @@ __global__ void k_hash_sort_buckets(uint32_t table, const uint32_t* __restrict__
   }
 }
 
+// The same canonical order (each bucket ascending), one warp per bucket: up
+// to 64 entries are sorted in registers by a bitonic network (two per lane,
+// padding 0xFFFFFFFF, which no index reaches); longer buckets fall back to
+// the serial insertion sort on lane 0.
+__global__ void k_hash_sort_buckets_warp(uint32_t table, const uint32_t* __restrict__ starts,
+                                         uint32_t* __restrict__ sorted) {
+  const uint32_t h = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t lane = threadIdx.x & 31u;
+  if (h >= table) return;  // whole warp
+  const uint32_t b = starts[h], e = starts[h + 1];
+  const uint32_t n = e - b;
+  if (n < 2) return;
+  if (n > 64) {
+    if (lane == 0)
+      for (uint32_t k = b + 1; k < e; ++k) {
+        const uint32_t v = sorted[k];
+        uint32_t j = k;
+        while (j > b && sorted[j - 1] > v) { sorted[j] = sorted[j - 1]; --j; }
+        sorted[j] = v;
+      }
+    return;
+  }
+  uint32_t a0 = lane < n ? sorted[b + lane] : 0xFFFFFFFFu;
+  uint32_t a1 = lane + 32u < n ? sorted[b + lane + 32u] : 0xFFFFFFFFu;
+  const uint32_t kmax = n > 32 ? 64u : 32u;
+  for (uint32_t k = 2; k <= kmax; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      if (j == 32u) {  // partners lane and lane + 32 live in one lane
+        const uint32_t lo = min(a0, a1), hi = max(a0, a1);
+        const bool up = (lane & k) == 0u;
+        a0 = up ? lo : hi;
+        a1 = up ? hi : lo;
+      } else {
+        const uint32_t o0 = __shfl_xor_sync(0xffffffffu, a0, j);
+        const uint32_t o1 = __shfl_xor_sync(0xffffffffu, a1, j);
+        const bool lower = (lane & j) == 0u;
+        const bool up0 = (lane & k) == 0u, up1 = ((lane + 32u) & k) == 0u;
+        a0 = (lower == up0) ? min(a0, o0) : max(a0, o0);
+        a1 = (lower == up1) ? min(a1, o1) : max(a1, o1);
+      }
+    }
+  }
+  if (lane < n) sorted[b + lane] = a0;
+  if (lane + 32u < n) sorted[b + lane + 32u] = a1;
+}
+
 // ---------------- accumulation helpers (shaders/self_collision.wgsl:77-118)
 __device__ __forceinline__ int32_t to_fixed(float x) { return f2i(clampf(x * 1000000.0f, -50000000.0f, 50000000.0f)); }
 __device__ __forceinline__ void add_disp(int32_t* acc, uint32_t v, V3 d) {
@@ -474,7 +520,11 @@ __device__ __forceinline__ bool sc_work_vv(const SCArgs& s, const VertCtx& c, co
   const float eth = fmaxf(thi + thj, fminf(lli, llj) * 0.06f);
   const uint32_t lj = __float_as_uint(q.y);
   const float dvl = sqrtf(fmaxf(d2, 0.0f));
-  if (near_folded_t(th, index, j, dvl)) return false;
+  // one search of i's two-hop list serves both tests on j: near_folded
+  // (:268-293) and, below, within_two_hops (:243-264); j != index here
+  uint32_t thq = 0;
+  const bool j_in2 = th_find(th, j, thq);
+  if (j_in2 && !(dvl < th.rest[thq] * 0.5f)) return false;
   const V3 pjo = mk(s.x4[j]);
   const float wj = q.z;
   const bool both = wj > 0.0f;
@@ -517,7 +567,7 @@ __device__ __forceinline__ bool sc_work_vv(const SCArgs& s, const VertCtx& c, co
   // 2. vertex-triangle
   const float mlj = q.w;
   const float vtb = eth + llj * 1.3f + mli + mlj;
-  if (!(d2 <= vtb * vtb) || within2_t(th, index, j)) return false;
+  if (!(d2 <= vtb * vtb) || j_in2) return false;
   {
     // Every triangle of j's star is skipped by its own swept-box test
     // (smin > tmax or smax < tmin on an axis) when the widest possible swept
@@ -588,24 +638,31 @@ __device__ __forceinline__ bool vt_entry(const SCArgs& s, const VertCtx& c, cons
   const uint32_t v0 = pr.x, v1 = pr.y;
   if (v0 == index || v1 == index) return false;
   const float4 q0 = s.p4[v0], q1 = s.p4[v1];
+  const V3 pv0 = mk(q0), pv1 = mk(q1);
+  // ownership (:486-500): the triangle is tested from its in-range vertex of
+  // smallest index, so only a vertex below j can take it away; the in-range
+  // test of v0 (v1) runs, and loads its data, only when v0 < j (v1 < j)
+  if (j > v0) {
+    const V3 d0 = pi - pv0;
+    const float ll0 = s.local_len[v0];
+    const float et0 = fmaxf(thi + q0.w, fminf(lli, ll0) * 0.06f);
+    const float b0 = et0 + ll0 * 1.3f + mli + s.mlen[v0];
+    const int4 c0 = s.vcell[v0];
+    if (abs(c0.x - cell.x) <= 1 && abs(c0.y - cell.y) <= 1 && abs(c0.z - cell.z) <= 1 && (dot(d0, d0) <= b0 * b0))
+      return false;
+  }
+  if (j > v1) {
+    const V3 d1 = pi - pv1;
+    const float ll1 = s.local_len[v1];
+    const float et1 = fmaxf(thi + q1.w, fminf(lli, ll1) * 0.06f);
+    const float b1 = et1 + ll1 * 1.3f + mli + s.mlen[v1];
+    const int4 c1 = s.vcell[v1];
+    if (abs(c1.x - cell.x) <= 1 && abs(c1.y - cell.y) <= 1 && abs(c1.z - cell.z) <= 1 && (dot(d1, d1) <= b1 * b1))
+      return false;
+  }
   const float4 o0 = s.x4[v0], o1 = s.x4[v1];
-  const V3 pv0 = mk(q0), pv1 = mk(q1), pv0o = mk(o0), pv1o = mk(o1);
+  const V3 pv0o = mk(o0), pv1o = mk(o1);
   const float wv0 = o0.w, wv1 = o1.w;
-  const V3 d0 = pi - pv0;
-  const float ll0 = s.local_len[v0];
-  const float et0 = fmaxf(thi + q0.w, fminf(lli, ll0) * 0.06f);
-  const float b0 = et0 + ll0 * 1.3f + mli + s.mlen[v0];
-  const int4 c0 = s.vcell[v0];
-  const bool in0 = abs(c0.x - cell.x) <= 1 && abs(c0.y - cell.y) <= 1 && abs(c0.z - cell.z) <= 1 &&
-                   (dot(d0, d0) <= b0 * b0);
-  const V3 d1 = pi - pv1;
-  const float ll1 = s.local_len[v1];
-  const float et1 = fmaxf(thi + q1.w, fminf(lli, ll1) * 0.06f);
-  const float b1 = et1 + ll1 * 1.3f + mli + s.mlen[v1];
-  const int4 c1 = s.vcell[v1];
-  const bool in1 = abs(c1.x - cell.x) <= 1 && abs(c1.y - cell.y) <= 1 && abs(c1.z - cell.z) <= 1 &&
-                   (dot(d1, d1) <= b1 * b1);
-  if ((in0 && j > v0) || (in1 && j > v1)) return false;
   const V3 tmove = (((pj - pjo) + (pv0 - pv0o)) + (pv1 - pv1o)) / 3.0f;
   const bool tpin = (wj <= 0.0f) || (wv0 <= 0.0f) || (wv1 <= 0.0f);
   const V3 rel = xi + tmove;

@@ -1234,7 +1234,7 @@ struct Sim {
       k_scan_blocks<<<ntiles, 1024, 0, ss>>>(T, cnts, start, tsum);
       k_scan_finish<<<ntiles, 1024, 0, ss>>>(T, ntiles, tsum, start);
       if (cnt) k_hash_scatter<<<grid(cnt, 256), 256, 0, ss>>>(cnt, k, start, curs, sorted);
-      k_hash_sort_buckets<<<grid(T, 256), 256, 0, ss>>>(T, start, sorted);
+      k_hash_sort_buckets_warp<<<grid(T, 8), 256, 0, ss>>>(T, start, sorted);
       if (cnt && which == 0)
         k_gather_vertices<<<grid(cnt, 256), 256, 0, ss>>>(cnt, sorted, x4.p, p4.p, v4.p, local_len.p, mlen.p, vcell.p,
                                                            vs_p.p, vs_c.p, vs_q.p);
