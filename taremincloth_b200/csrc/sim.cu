@@ -886,6 +886,24 @@ struct Sim {
     m = build_mesh(in);
     cell_ref = m.cell;
     n = m.n;
+    {  // vertices of one warp close in space for the collider pass (any order is exact)
+      float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (uint32_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = std::fmin(lo[k], m.pos[3 * size_t(i) + k]);
+          hi[k] = std::fmax(hi[k], m.pos[3 * size_t(i) + k]);
+        }
+      float inv[3];
+      for (int k = 0; k < 3; ++k) inv[k] = hi[k] > lo[k] ? 1.f / (hi[k] - lo[k]) : 0.f;
+      std::vector<std::pair<uint32_t, uint32_t>> code(n);
+      for (uint32_t i = 0; i < n; ++i)
+        code[i] = {tcloth::morton3(m.pos[3 * size_t(i)], m.pos[3 * size_t(i) + 1], m.pos[3 * size_t(i) + 2], lo, inv),
+                   i};
+      std::sort(code.begin(), code.end());
+      std::vector<uint32_t> ord(n);
+      for (uint32_t i = 0; i < n; ++i) ord[i] = code[i].second;
+      col_order.upload(ord, st);
+    }
     nd = uint32_t(m.dist.size());
     nb = uint32_t(m.bend.size());
     ne = uint32_t(m.edges.size() / 2);
@@ -1198,6 +1216,8 @@ struct Sim {
   // threads per block of the per-colour constraint launches (autotuned;
   // results do not depend on it)
   uint32_t col_block = 256;
+  // the collider pass's vertex order: Morton order of the initial positions
+  DBuf<uint32_t> col_order;
   float cell_ref = 0.f;  // the reference formula's hash cell (tc_set_hash_cell_size can override m.cell)
   // E-E kernel: false = one warp per edge (k_ee), true = one lane per edge
   // with per-cell candidate lists in shared memory (k_ee_grouped); same pairs
@@ -1868,8 +1888,8 @@ struct Sim {
         }
       if (hascol && use_coupled) {
         if (!gate) launch_collision(ca, dts);
-        else if (bone_col) launch_k(k_collision_gated<true>, grid(n, 128), 128, gate, n, x4.p, p4.p, ca, dts);
-        else launch_k(k_collision_gated<false>, grid(n, 128), 128, gate, n, x4.p, p4.p, ca, dts);
+        else if (bone_col) launch_k(k_collision_gated<true>, grid(n, 128), 128, gate, n, x4.p, p4.p, ca, dts, col_order.p);
+        else launch_k(k_collision_gated<false>, grid(n, 128), 128, gate, n, x4.p, p4.p, ca, dts, col_order.p);
       }
     };
     timed("solver", [&] {
@@ -1949,8 +1969,8 @@ struct Sim {
     TC_CK(cudaLaunchKernelEx(&cfg, kern, args...));
   }
   void launch_collision(const ColliderArgs& ca, float dts) {
-    if (ca.bone.nbones > 0) launch_k(k_collision<true>, grid(n, 128), 128, n, x4.p, p4.p, ca, dts);
-    else launch_k(k_collision<false>, grid(n, 128), 128, n, x4.p, p4.p, ca, dts);
+    if (ca.bone.nbones > 0) launch_k(k_collision<true>, grid(n, 128), 128, n, x4.p, p4.p, ca, dts, col_order.p);
+    else launch_k(k_collision<false>, grid(n, 128), 128, n, x4.p, p4.p, ca, dts, col_order.p);
   }
 
   // encode_simulation_steps (dispatch.rs:7-354) for one frame

@@ -573,11 +573,16 @@ __device__ __forceinline__ void collide_vertex(uint32_t i, float4* __restrict__ 
 // kBone: with the bone SDF phase (a separate instantiation, so that kernels
 // without bone colliders keep their register budget)
 template <bool kBone>
+// order: null, or a permutation of the vertices that keeps a warp's vertices
+// close in space (they then visit nearly the same collider triangles); each
+// vertex's contacts depend on that vertex alone, so any order gives the
+// same results.
 __global__ void k_collision(uint32_t n, float4* __restrict__ x4, float4* __restrict__ p4, ColliderArgs ca,
-                            float dt) {
+                            float dt, const uint32_t* __restrict__ order) {
   pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (order) i = order[i];
   collide_vertex<false, kBone>(i, x4, p4, ca, dt);
 }
 
@@ -818,10 +823,12 @@ __global__ void k_bending_gated(const unsigned int* gate, uint32_t off, uint32_t
 }
 template <bool kBone>
 __global__ void k_collision_gated(const unsigned int* gate, uint32_t n, float4* __restrict__ x4,
-                                  float4* __restrict__ p4, ColliderArgs ca, float dt) {
+                                  float4* __restrict__ p4, ColliderArgs ca, float dt,
+                                  const uint32_t* __restrict__ order) {
   pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !*gate) return;
+  if (order) i = order[i];
   collide_vertex<false, kBone>(i, x4, p4, ca, dt);
 }
 
