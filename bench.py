@@ -419,6 +419,21 @@ def warm_start_extra(steps):
     return out
 
 
+def ws_config4_frames(frames=2, k=2):
+    """The warm-started config 4 batch for a profiler's launch list: the 64
+    cloths in one simulator, per-colour launches, the learned warm start
+    replacing k of the 5 iterations at its seeded initial weights (the
+    timing does not depend on them), `frames` frames."""
+    from taremincloth_b200 import scenes
+    sc = scenes.config4()
+    b = scenes.build_batch(sc)
+    b.set_launch_config(False)
+    b.ws_enable(k, float("inf"))
+    for _ in range(frames):
+        b.step(sc["dt"], sc["substeps"])
+    return b
+
+
 def learned_batched_summary(batched, ws4):
     """The metric as named, on the config 4 workload: plain = the 64 cloths as
     separate simulators (plain CUDA XPBD), batched = one simulator over all

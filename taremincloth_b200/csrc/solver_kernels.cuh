@@ -192,13 +192,23 @@ __device__ __forceinline__ void project_distance(uint32_t ci, const uint2* __res
   project_distance_m(ci, ids, par, GMem<kCg>{x4, p4, nullptr}, lam, sp, damped);
 }
 
+// The constraint records are written only by host uploads, never by a
+// kernel, so they are loaded before griddepcontrol.wait, while the previous
+// kernel of the stream may still run; lambda and the vertices, which the
+// previous kernel may write, are loaded after it.
 __global__ void k_distance(uint32_t off, uint32_t cnt, const uint2* __restrict__ ids, const float4* __restrict__ par,
                            float4* __restrict__ x4, float4* __restrict__ p4, float* __restrict__ lam,
                            SubstepParams sp, bool damped) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  uint2 e = make_uint2(0u, 0u);
+  float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (k < cnt) {
+    e = ids[off + k];
+    c = par[off + k];
+  }
   pdl_enter();
-  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= cnt) return;
-  project_distance<false>(off + k, ids, par, x4, p4, lam, sp, damped);
+  distance_core(e, c, lam[off + k], lam + off + k, GMem<false>{x4, p4, nullptr}, sp, damped);
 }
 
 // One bending constraint (shaders/bending.wgsl:59-126).  bend_par =
@@ -258,13 +268,20 @@ __device__ __forceinline__ void project_bending(uint32_t ci, const uint4* __rest
   project_bending_m(ci, ids, par, GMem<kCg>{x4, p4, nullptr}, lam, sp, damped);
 }
 
+// (records loaded before griddepcontrol.wait, as in k_distance)
 __global__ void k_bending(uint32_t off, uint32_t cnt, const uint4* __restrict__ ids, const float4* __restrict__ par,
                           float4* __restrict__ x4, float4* __restrict__ p4, float* __restrict__ lam,
                           SubstepParams sp, bool damped) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  uint4 e = make_uint4(0u, 0u, 0u, 0u);
+  float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (k < cnt) {
+    e = ids[off + k];
+    c = par[off + k];
+  }
   pdl_enter();
-  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= cnt) return;
-  project_bending<false>(off + k, ids, par, x4, p4, lam, sp, damped);
+  if (k >= cnt || c.y >= 1e9f) return;
+  bending_core(e, c, lam[off + k], lam + off + k, GMem<false>{x4, p4, nullptr}, sp, damped);
 }
 
 // Sewing settings of a frame (dispatch.rs:29-35): compliance 0 when the
