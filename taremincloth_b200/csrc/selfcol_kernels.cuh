@@ -67,11 +67,6 @@ struct SCArgs {
   uint2* ccd_q;
   uint32_t* ccd_n;
   uint32_t ccd_cap;
-  // survivor records in hash order (slot k of the sorted arrays): x of
-  // vertex srt[k], its star box (three float4, as sbox) and its star range
-  const float4* vs_x;
-  const float4* vs_sb;
-  const uint2* vs_st;
   // optional record of the narrow-phase input (null when off): the
   // (vertex, triangle) pairs that pass the cheap tests of sc_solve and the
   // (edge, edge) pairs counted within max_search; rec_n[0] / rec_n[1] count
@@ -172,21 +167,6 @@ __global__ void k_star_box(uint32_t n, const uint32_t* __restrict__ star_off, co
   sbox[3 * size_t(j)] = make_float4(lo.x, lo.y, lo.z, mlo.x);
   sbox[3 * size_t(j) + 1] = make_float4(hi.x, hi.y, hi.z, mlo.y);
   sbox[3 * size_t(j) + 2] = make_float4(mhi.x, mhi.y, mhi.z, mlo.z);
-}
-
-// The survivor records of the vertex-triangle pass in hash order (after
-// k_star_box): x, star box and star range of vertex srt[k] at slot k.
-__global__ void k_gather_stars(uint32_t n, const uint32_t* __restrict__ srt, const float4* __restrict__ x4,
-                               const float4* __restrict__ sbox, const uint32_t* __restrict__ star_off,
-                               float4* __restrict__ vs_x, float4* __restrict__ vs_sb, uint2* __restrict__ vs_st) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const uint32_t j = srt[k];
-  vs_x[k] = x4[j];
-  vs_sb[3 * size_t(k)] = sbox[3 * size_t(j)];
-  vs_sb[3 * size_t(k) + 1] = sbox[3 * size_t(j) + 1];
-  vs_sb[3 * size_t(k) + 2] = sbox[3 * size_t(j) + 2];
-  vs_st[k] = make_uint2(star_off[j], star_off[j + 1]);
 }
 
 // ---------------- normals: shaders/compute_normals.wgsl:25-58
@@ -545,7 +525,7 @@ __device__ __forceinline__ bool sc_work_vv(const SCArgs& s, const VertCtx& c, co
   uint32_t thq = 0;
   const bool j_in2 = th_find(th, j, thq);
   if (j_in2 && !(dvl < th.rest[thq] * 0.5f)) return false;
-  const V3 pjo = mk(s.vs_x[slot]);
+  const V3 pjo = mk(s.x4[j]);
   const float wj = q.z;
   const bool both = wj > 0.0f;
   const float eth2 = eth * eth;
@@ -593,7 +573,7 @@ __device__ __forceinline__ bool sc_work_vv(const SCArgs& s, const VertCtx& c, co
     // (smin > tmax or smax < tmin on an axis) when the widest possible swept
     // box of i, over the star's motion range plus a 10 um rounding margin,
     // misses the star's box: skipping the whole star is then exact.
-    const float4 b0 = s.vs_sb[3 * size_t(slot)], b1 = s.vs_sb[3 * size_t(slot) + 1], b2 = s.vs_sb[3 * size_t(slot) + 2];
+    const float4 b0 = s.sbox[3 * size_t(j)], b1 = s.sbox[3 * size_t(j) + 1], b2 = s.sbox[3 * size_t(j) + 2];
     const V3 xi = c.xi;
     const float sl = 1e-5f;
     const float rl[3] = {xi.x + b0.w - sl, xi.y + b1.w - sl, xi.z + b2.w - sl};
@@ -607,9 +587,8 @@ __device__ __forceinline__ bool sc_work_vv(const SCArgs& s, const VertCtx& c, co
       if (smin_lb > hi[ax] || smax_ub < lo[ax]) return false;
     }
   }
-  const uint2 sr = s.vs_st[slot];
-  st_b = sr.x;
-  st_e = sr.y;
+  st_b = s.star_off[j];
+  st_e = s.star_off[j + 1];
   // what the triangle filter needs of j: p, contact thickness, x, index
   rec0 = make_float4(pj.x, pj.y, pj.z, eth);
   rec1 = make_float4(pjo.x, pjo.y, pjo.z, __uint_as_float(j));
@@ -645,7 +624,7 @@ __device__ __forceinline__ bool vt_entry(const SCArgs& s, const VertCtx& c, cons
     pj = mk(pj4);
     eth = fmaxf(thi + pj4.w, fminf(lli, q.x) * 0.06f);
     lj = __float_as_uint(q.y);
-    pjo = mk(s.vs_x[slot]);
+    pjo = mk(s.x4[j]);
     wj = q.z;
   } else {
     pj = mk(rec0);

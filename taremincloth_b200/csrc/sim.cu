@@ -500,8 +500,7 @@ struct Sim {
   DBuf<float4> sbox;
   DBuf<float> mlen;
   DBuf<float4> eamin, eamax;
-  DBuf<float4> vs_p, vs_q, es_lo, es_hi, vs_x, vs_sb;
-  DBuf<uint2> vs_st;
+  DBuf<float4> vs_p, vs_q, es_lo, es_hi;
   DBuf<uint32_t> tile_sum;
   DBuf<int4> vs_c, es_c;
   DBuf<uint2> es_v, ccd_q;
@@ -974,7 +973,7 @@ struct Sim {
     acc.alloc(size_t(n) * A_N);
     vcell.alloc(n); mlen.alloc(n); sbox.alloc(3 * size_t(n)); ecell.alloc(ne); eamin.alloc(ne); eamax.alloc(ne);
     ccd_q.alloc(size_t(ne) * 4 + 1024); ccd_n.alloc(1);
-    vs_p.alloc(n); vs_q.alloc(n); vs_c.alloc(n); vs_x.alloc(n); vs_sb.alloc(3 * size_t(n)); vs_st.alloc(n); tile_sum.alloc(64); es_c.alloc(ne); es_v.alloc(ne); es_lo.alloc(ne); es_hi.alloc(ne);
+    vs_p.alloc(n); vs_q.alloc(n); vs_c.alloc(n); tile_sum.alloc(64); es_c.alloc(ne); es_v.alloc(ne); es_lo.alloc(ne); es_hi.alloc(ne);
     TC_CK(cudaMemsetAsync(acc.p, 0, size_t(n) * A_N * sizeof(int32_t), st));
     TC_CK(cudaMemsetAsync(nrm.p, 0, size_t(n) * sizeof(float4), st));
     res_sum.alloc(m.dist_cnt.size() + m.bend_cnt.size() + 1);
@@ -1206,7 +1205,6 @@ struct Sim {
     a.sbox = sbox.p;
     a.vcell = vcell.p; a.mlen = mlen.p; a.ecell = ecell.p; a.eamin = eamin.p; a.eamax = eamax.p;
     a.ccd_q = ccd_q.p; a.ccd_n = ccd_n.p; a.ccd_cap = uint32_t(ccd_q.n);
-    a.vs_x = vs_x.p; a.vs_sb = vs_sb.p; a.vs_st = vs_st.p;
     a.vs_p = vs_p.p; a.vs_q = vs_q.p; a.vs_c = vs_c.p; a.es_c = es_c.p; a.es_v = es_v.p; a.es_lo = es_lo.p; a.es_hi = es_hi.p;
     a.rec_vt = rec_pairs ? rec_vt.p : nullptr;
     a.rec_ee = rec_pairs ? rec_ee.p : nullptr;
@@ -1342,10 +1340,7 @@ struct Sim {
       TC_CK(cudaEventRecord(ev_join, st2));
     }
     encode_hash(0);
-    timed("sc_star_box", [&] {
-      k_star_box<<<grid(n, 256), 256, 0, st>>>(n, star_off.p, star_idx.p, x4.p, p4.p, sbox.p);
-      k_gather_stars<<<grid(n, 256), 256, 0, st>>>(n, srt.p, x4.p, sbox.p, star_off.p, vs_x.p, vs_sb.p, vs_st.p);
-    });
+    timed("sc_star_box", [&] { k_star_box<<<grid(n, 256), 256, 0, st>>>(n, star_off.p, star_idx.p, x4.p, p4.p, sbox.p); });
     if (edges_on && !fork) encode_hash(1);
     timed("sc_solve", [&] { k_sc_solve<<<grid(n, 8), 256, 0, st>>>(a); });
     if (a.untangle) timed("sc_untangle", [&] { k_untangle<<<grid(n, 128), 128, 0, st>>>(a); });
