@@ -364,10 +364,19 @@ tc_status tc_set_nonfinite_check(tc_sim *s, int enable);
 tc_status tc_set_launch_block(tc_sim *s, uint32_t threads);
 tc_status tc_set_hash_cell_size(tc_sim *s, float cell);
 /* Kernel shape of the direct pass's edge-edge search (new; results and pair
- * lists do not change): 0 = one warp per edge over the 27 neighbour cells;
- * 1 = one lane per edge, a warp taking 32 edges of the hash-sorted order and
- * building each distinct cell's candidate list once in shared memory. */
+ * lists do not change): 0 (default) = one warp per edge over the 27
+ * neighbour cells, the counted pairs listed and their contact work done one
+ * lane per pair by a second kernel; 1 = one lane per edge, a warp taking 32
+ * edges of the hash-sorted order and building each distinct cell's
+ * candidate list once in shared memory; 2 = as 0 with the contact work done
+ * by the edge's own warp. */
 tc_status tc_set_self_collision_variant(tc_sim *s, uint32_t ee_variant);
+/* Capacity, in (edge, edge) pairs, of the list through which variant 0
+ * hands its counted pairs to the contact kernel (new; 0 = the default,
+ * 24 per edge + 1024).  The list is split evenly among 256 segments; pairs
+ * past their segment's share are worked by the search kernel itself, so
+ * results do not depend on it. */
+tc_status tc_set_ee_pair_list_capacity(tc_sim *s, uint64_t entries);
 /* Narrow-phase pair lists of the direct self-collision pass, for parity
  * (no counterpart in the reference's API; the passes are
  * shaders/self_collision.wgsl:317-681 and

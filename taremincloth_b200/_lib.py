@@ -46,6 +46,7 @@ SIGNATURES = {
     "tc_color_edge_pairs": [_U, _P, _U, _P],
     "tc_set_pair_recording": [_P, _I, _U, _U],
     "tc_set_self_collision_variant": [_P, _U],
+    "tc_set_ee_pair_list_capacity": [_P, C.c_uint64],
     "tc_set_launch_block": [_P, _U],
     "tc_set_hash_cell_size": [_P, _F],
     "tc_mark_device_lost": [_I],

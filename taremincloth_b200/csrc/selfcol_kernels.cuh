@@ -67,6 +67,16 @@ struct SCArgs {
   uint2* ccd_q;
   uint32_t* ccd_n;
   uint32_t ccd_cap;
+  // (edge, edge) pairs counted by k_ee, worked one lane each by k_ee_pairs.
+  // The list is split into kEeSeg segments of ee_cap / kEeSeg entries with a
+  // counter each (ee_n[kEeSeg]); block b of k_ee appends to segment
+  // b % kEeSeg, so that no one counter takes every warp's atomic.  A counter
+  // may run past its segment's capacity (k_ee_pairs reads min(count, cap));
+  // the pairs past it are worked inside k_ee.  ee_cap = 0 keeps all of the
+  // contact work inside k_ee.
+  uint2* ee_q;
+  uint32_t* ee_n;
+  uint32_t ee_cap;
   // optional record of the narrow-phase input (null when off): the
   // (vertex, triangle) pairs that pass the cheap tests of sc_solve and the
   // (edge, edge) pairs counted within max_search; rec_n[0] / rec_n[1] count
@@ -124,6 +134,8 @@ __device__ __forceinline__ bool near_folded_sq_t(const TwoHop& t, uint32_t a, ui
 }
 constexpr uint32_t kTwoHopCache = 64;
 constexpr uint32_t kRounds = 4;  // candidates per warp chunk = 32 * kRounds
+constexpr uint32_t kEeSeg = 256;       // segments of the E-E pair list
+constexpr uint32_t kEePairBlocks = 4;  // k_ee_pairs blocks per segment
 // Stage vertex v's two-hop list in shared memory (whole warp participates).
 __device__ __forceinline__ TwoHop stage_two_hop(const uint32_t* th_off, const uint32_t* th_idx, const float* th_rest,
                                                uint32_t v, uint32_t* sh_idx, float* sh_rest, int lane) {
@@ -1342,23 +1354,47 @@ __device__ __forceinline__ EdgeCtx edge_ctx(const SCArgs& s, uint32_t ei) {
   return c;
 }
 
+// Contact work for a listed (edge, edge) pair, with the two-hop lists of
+// the first edge's endpoints read from global memory.
+__device__ __forceinline__ void ee_listed_pair(const SCArgs& s, uint2 pr, bool defer_ccd) {
+  const EdgeCtx c = edge_ctx(s, pr.x);
+  TwoHop th0, th1;
+  th0.idx = s.th_idx + s.th_off[c.u0];
+  th0.rest = s.th_rest + s.th_off[c.u0];
+  th0.n = s.th_off[c.u0 + 1] - s.th_off[c.u0];
+  th1.idx = s.th_idx + s.th_off[c.u1];
+  th1.rest = s.th_rest + s.th_off[c.u1];
+  th1.n = s.th_off[c.u1 + 1] - s.th_off[c.u1];
+  const uint2 ebv = s.edges[pr.y];
+  ee_pair(s, c, th0, th1, pr.y, ebv.x, ebv.y, s.p4[ebv.x], s.p4[ebv.y], s.x4[ebv.x], s.x4[ebv.y], defer_ccd);
+}
+
+// ee_listed_pair outside the caller's register allocation, for the rare
+// pairs that do not fit the pair list.
+__device__ __noinline__ void ee_listed_pair_call(const SCArgs& s, uint2 pr) { ee_listed_pair(s, pr, true); }
+
+// Counted pairs listed by k_ee, one thread each: the CCD gate of
+// shaders/self_collision_ee_direct.wgsl:361-403 and the discrete contact
+// from :632 on; pairs that need the CCD search go on to k_ee_ccd.
+// Grid: kEeSeg * kEePairBlocks blocks of 256 threads.
+__global__ void __launch_bounds__(256, 4) k_ee_pairs(SCArgs s) {
+  const uint32_t seg = blockIdx.x / kEePairBlocks, segcap = s.ee_cap / kEeSeg;
+  const uint32_t total = min(s.ee_n[seg], segcap);
+  const uint2* list = s.ee_q + size_t(seg) * segcap;
+  for (uint32_t q = (blockIdx.x % kEePairBlocks) * blockDim.x + threadIdx.x; q < total;
+       q += kEePairBlocks * blockDim.x) {
+    const uint2 pr = list[q];
+    if (s.rec_ee) record_ee(s, pr.x, pr.y);
+    ee_listed_pair(s, pr, true);
+  }
+}
+
 // Deferred CCD pairs, one thread each (the CCD search plus the discrete
 // fall-through of shaders/self_collision_ee_direct.wgsl:404-774).
 __global__ void __launch_bounds__(256) k_ee_ccd(SCArgs s) {
   const uint32_t total = min(*s.ccd_n, s.ccd_cap);
-  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
-    const uint2 pr = s.ccd_q[q];
-    const EdgeCtx c = edge_ctx(s, pr.x);
-    TwoHop th0, th1;
-    th0.idx = s.th_idx + s.th_off[c.u0];
-    th0.rest = s.th_rest + s.th_off[c.u0];
-    th0.n = s.th_off[c.u0 + 1] - s.th_off[c.u0];
-    th1.idx = s.th_idx + s.th_off[c.u1];
-    th1.rest = s.th_rest + s.th_off[c.u1];
-    th1.n = s.th_off[c.u1 + 1] - s.th_off[c.u1];
-    const uint2 ebv = s.edges[pr.y];
-    ee_pair(s, c, th0, th1, pr.y, ebv.x, ebv.y, s.p4[ebv.x], s.p4[ebv.y], s.x4[ebv.x], s.x4[ebv.y], false);
-  }
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x)
+    ee_listed_pair(s, s.ccd_q[q], false);
 }
 
 // One warp per edge; candidates of the 27 cells around the edge midpoint are
@@ -1366,7 +1402,14 @@ __global__ void __launch_bounds__(256) k_ee_ccd(SCArgs s) {
 // round.  The per-edge cap on counted candidates (search_count >
 // max_search_iterations, :356-359) is applied with a ballot prefix count, so
 // exactly the reference's first max_search counted pairs are processed.
-__global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
+// kList: the counted pairs are appended to the pair list for k_ee_pairs
+// (the two-hop lists are then not staged here); otherwise the warp does
+// their contact work itself.
+// (__grid_constant__: the overflow call takes the arguments' address without
+// a per-thread copy.)  The filter alone is latency-bound and needs few
+// registers, so list mode asks for 8 blocks (64 warps) per SM.
+template <bool kList>
+__global__ void __launch_bounds__(256, kList ? 8 : 4) k_ee(const __grid_constant__ SCArgs s) {
   __shared__ uint32_t sh_start[8][28], sh_end[8][28], sh_beg[8][28];
   __shared__ uint32_t sh_th[8][2][kTwoHopCache];
   __shared__ float sh_thr[8][2][kTwoHopCache];
@@ -1377,8 +1420,11 @@ __global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
   const EdgeCtx c = edge_ctx(s, ei);
   const int4 bc4 = s.ecell[ei];
   const I3 base = I3{bc4.x, bc4.y, bc4.z};
-  const TwoHop th0 = stage_two_hop(s.th_off, s.th_idx, s.th_rest, c.u0, sh_th[warp][0], sh_thr[warp][0], lane);
-  const TwoHop th1 = stage_two_hop(s.th_off, s.th_idx, s.th_rest, c.u1, sh_th[warp][1], sh_thr[warp][1], lane);
+  TwoHop th0{}, th1{};
+  if (!kList) {
+    th0 = stage_two_hop(s.th_off, s.th_idx, s.th_rest, c.u0, sh_th[warp][0], sh_thr[warp][0], lane);
+    th1 = stage_two_hop(s.th_off, s.th_idx, s.th_rest, c.u1, sh_th[warp][1], sh_thr[warp][1], lane);
+  }
   // lane k = (dz+1)*9 + (dy+1)*3 + (dx+1)
   uint32_t cnt = 0, beg = 0;
   if (lane < 27) {
@@ -1417,7 +1463,7 @@ __global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
     for (uint32_t r = 0; r < kRounds; ++r) {
       const uint32_t t = chunk + r * 32u + lane;
       bool pass = false;
-      uint32_t slot = 0;
+      uint32_t slot = 0, eb_l = 0;
       if (t < total) {
         while (t >= sh_end[warp][k]) ++k;
         slot = sh_beg[warp][k] + (t - sh_start[warp][k]);
@@ -1426,6 +1472,7 @@ __global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
         const uint2 ebv = s.es_v[slot];
         const float4 bmin = s.es_lo[slot], bmax = s.es_hi[slot];
         const uint32_t eb = (uint32_t)bc.w;
+        eb_l = eb;
         pass = ei < eb && !(ebv.x == c.u0 || ebv.x == c.u1 || ebv.y == c.u0 || ebv.y == c.u1) &&
                bc.x == base.x - 1 + k % 3 && bc.y == base.y - 1 + (k / 3) % 3 && bc.z == base.z - 1 + k / 9 &&
                !(c.amin.x > bmax.x || c.amin.y > bmax.y || c.amin.z > bmax.z || c.amax.x < bmin.x ||
@@ -1433,20 +1480,40 @@ __global__ void __launch_bounds__(256, 4) k_ee(SCArgs s) {
       }
       const uint32_t b = __ballot_sync(0xffffffffu, pass);
       const uint32_t rank = counted + __popc(b & lt_mask);
-      if (pass && rank < s.max_search) queue[qn + __popc(b & lt_mask)] = slot;
+      // list mode queues the edge index, otherwise the slot of its records
+      if (pass && rank < s.max_search) queue[qn + __popc(b & lt_mask)] = kList ? eb_l : slot;
       const uint32_t nb = __popc(b);
       qn += counted + nb <= s.max_search ? nb : (counted < s.max_search ? s.max_search - counted : 0u);
       counted += nb;
     }
     __syncwarp();
-    // phase 2: contact work on the queued pairs
-    for (uint32_t q = lane; q < qn; q += 32u) {
-      const uint32_t slot = queue[q];
-      const uint32_t eb = (uint32_t)s.es_c[slot].w;
-      const uint2 ebv = s.es_v[slot];
-      const float4 qj = s.p4[ebv.x], qvj = s.p4[ebv.y], xj = s.x4[ebv.x], xvj = s.x4[ebv.y];
-      if (s.rec_ee) record_ee(s, ei, eb);
-      ee_pair(s, c, th0, th1, eb, ebv.x, ebv.y, qj, qvj, xj, xvj, true);
+    if constexpr (kList) {
+      // phase 2: the queued pairs are appended to this block's segment of
+      // the pair list of k_ee_pairs; those past its capacity get their
+      // contact work here
+      const uint32_t seg = blockIdx.x % kEeSeg, segcap = s.ee_cap / kEeSeg;
+      uint32_t lbase = segcap;
+      if (lane == 0 && qn && segcap) lbase = atomicAdd(s.ee_n + seg, qn);
+      lbase = __shfl_sync(0xffffffffu, lbase, 0);
+      for (uint32_t q = lane; q < qn; q += 32u) {
+        const uint32_t eb = queue[q];
+        if (lbase < segcap && q < segcap - lbase) {
+          s.ee_q[size_t(seg) * segcap + lbase + q] = make_uint2(ei, eb);
+        } else {
+          if (s.rec_ee) record_ee(s, ei, eb);
+          ee_listed_pair_call(s, make_uint2(ei, eb));
+        }
+      }
+    } else {
+      // phase 2: contact work on the queued pairs
+      for (uint32_t q = lane; q < qn; q += 32u) {
+        const uint32_t slot = queue[q];
+        const uint32_t eb = (uint32_t)s.es_c[slot].w;
+        const uint2 ebv = s.es_v[slot];
+        const float4 qj = s.p4[ebv.x], qvj = s.p4[ebv.y], xj = s.x4[ebv.x], xvj = s.x4[ebv.y];
+        if (s.rec_ee) record_ee(s, ei, eb);
+        ee_pair(s, c, th0, th1, eb, ebv.x, ebv.y, qj, qvj, xj, xvj, true);
+      }
     }
     __syncwarp();
   }

@@ -503,8 +503,8 @@ struct Sim {
   DBuf<float4> vs_p, vs_q, es_lo, es_hi;
   DBuf<uint32_t> tile_sum;
   DBuf<int4> vs_c, es_c;
-  DBuf<uint2> es_v, ccd_q;
-  DBuf<uint32_t> ccd_n;
+  DBuf<uint2> es_v, ccd_q, ee_q;
+  DBuf<uint32_t> ccd_n;  // [0] deferred CCD pairs, [1 + g] listed E-E pairs of segment g
   // contact-pair cache (self-collision algorithm 1; simulation/mod.rs:582-600,
   // :799-893, dispatch.rs:1540-1670), off by default; buffers on first use
   bool pair_cache = false, pair_final_fallback = true;
@@ -972,7 +972,8 @@ struct Sim {
     nrm.alloc(n);
     acc.alloc(size_t(n) * A_N);
     vcell.alloc(n); mlen.alloc(n); sbox.alloc(3 * size_t(n)); ecell.alloc(ne); eamin.alloc(ne); eamax.alloc(ne);
-    ccd_q.alloc(size_t(ne) * 4 + 1024); ccd_n.alloc(1);
+    ccd_q.alloc(size_t(ne) * 4 + 1024); ccd_n.alloc(1 + tcloth::kEeSeg);
+    ee_q.alloc(size_t(ne) * 24 + 1024);
     vs_p.alloc(n); vs_q.alloc(n); vs_c.alloc(n); tile_sum.alloc(64); es_c.alloc(ne); es_v.alloc(ne); es_lo.alloc(ne); es_hi.alloc(ne);
     TC_CK(cudaMemsetAsync(acc.p, 0, size_t(n) * A_N * sizeof(int32_t), st));
     TC_CK(cudaMemsetAsync(nrm.p, 0, size_t(n) * sizeof(float4), st));
@@ -1205,6 +1206,9 @@ struct Sim {
     a.sbox = sbox.p;
     a.vcell = vcell.p; a.mlen = mlen.p; a.ecell = ecell.p; a.eamin = eamin.p; a.eamax = eamax.p;
     a.ccd_q = ccd_q.p; a.ccd_n = ccd_n.p; a.ccd_cap = uint32_t(ccd_q.n);
+    a.ee_q = ee_q.p; a.ee_n = ccd_n.p ? ccd_n.p + 1 : nullptr;
+    const size_t ee_entries = ee_list_entries ? std::min(ee_list_entries, ee_q.n) : ee_q.n;
+    a.ee_cap = ee_list ? uint32_t(std::min<size_t>(ee_entries, 0xffffffffu)) : 0u;
     a.vs_p = vs_p.p; a.vs_q = vs_q.p; a.vs_c = vs_c.p; a.es_c = es_c.p; a.es_v = es_v.p; a.es_lo = es_lo.p; a.es_hi = es_hi.p;
     a.rec_vt = rec_pairs ? rec_vt.p : nullptr;
     a.rec_ee = rec_pairs ? rec_ee.p : nullptr;
@@ -1223,6 +1227,11 @@ struct Sim {
   // with per-cell candidate lists in shared memory (k_ee_grouped); same pairs
   // and results
   bool ee_grouped = false;
+  // k_ee lists its counted pairs for k_ee_pairs (one lane per pair) instead
+  // of working them in the edge's warp; same pairs and results.  The list
+  // holds ee_list_entries pairs (0: all of ee_q, 24 per edge + 1024).
+  bool ee_list = true;
+  size_t ee_list_entries = 0;
   // narrow-phase pair record of the latest self-collision pass (off by default)
   bool rec_pairs = false;
   DBuf<uint4> rec_vt;
@@ -1266,9 +1275,14 @@ struct Sim {
   void encode_hash(int which) { encode_hash(which, st); }
   void encode_ee(const SCArgs& a, cudaStream_t ss) {
     timed("sc_solve_ee", [&] {
-      TC_CK(cudaMemsetAsync(ccd_n.p, 0, sizeof(uint32_t), ss));
-      if (ee_grouped) k_ee_grouped<<<grid(ne, 32 * tcloth::kEeWarps), 32 * tcloth::kEeWarps, 0, ss>>>(a);
-      else k_ee<<<grid(ne, 8), 256, 0, ss>>>(a);
+      TC_CK(cudaMemsetAsync(ccd_n.p, 0, (1 + tcloth::kEeSeg) * sizeof(uint32_t), ss));
+      if (ee_grouped) {
+        k_ee_grouped<<<grid(ne, 32 * tcloth::kEeWarps), 32 * tcloth::kEeWarps, 0, ss>>>(a);
+      } else {
+        if (a.ee_cap) k_ee<true><<<grid(ne, 8), 256, 0, ss>>>(a);
+        else k_ee<false><<<grid(ne, 8), 256, 0, ss>>>(a);
+        if (a.ee_cap) k_ee_pairs<<<tcloth::kEeSeg * tcloth::kEePairBlocks, 256, 0, ss>>>(a);
+      }
     });
     timed("sc_solve_ee_ccd", [&] { k_ee_ccd<<<148 * 8, 256, 0, ss>>>(a); });
   }
@@ -4323,9 +4337,24 @@ tc_status tc_bake_destroy(tc_bake* b) {
 // ---- kernel variants of the self-collision pass (results identical)
 tc_status tc_set_self_collision_variant(tc_sim* s, uint32_t ee_variant) {
   return guard([&] {
-    need(ee_variant <= 1u, "ee_variant: 0 (warp per edge) or 1 (grouped by cell)");
+    need(ee_variant <= 2u,
+         "ee_variant: 0 (warp per edge, pair list), 1 (grouped by cell) or 2 (warp per edge, contact in the warp)");
     Sim& m = S(s);
     m.ee_grouped = ee_variant == 1u;
+    m.ee_list = ee_variant == 0u;
+    m.mark();
+  });
+}
+
+tc_status tc_set_ee_pair_list_capacity(tc_sim* s, uint64_t entries) {
+  return guard([&] {
+    Sim& m = S(s);
+    need(entries <= 0xffffffffull, "entries: at most 2^32 - 1");
+    if (entries > m.ee_q.n && m.ee_q.p) {
+      TC_CK(cudaStreamSynchronize(m.st));
+      m.ee_q.alloc(size_t(entries));
+    }
+    m.ee_list_entries = size_t(entries);
     m.mark();
   });
 }

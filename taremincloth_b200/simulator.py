@@ -448,9 +448,16 @@ class ClothSimulator:
         """Spatial-hash cell; None restores the reference formula's value."""
         self._c(self._L.tc_set_hash_cell_size(self._h, 0.0 if cell is None else float(cell)))
 
-    def set_self_collision_variant(self, ee_variant=1):
-        """Edge-edge kernel shape: 0 warp per edge, 1 grouped by cell (same results)."""
+    def set_self_collision_variant(self, ee_variant=0):
+        """Edge-edge kernel shape (same results): 0 warp per edge with the counted
+        pairs worked one lane each (default), 1 grouped by cell, 2 warp per edge
+        with the contact work in the edge's warp."""
         self._c(self._L.tc_set_self_collision_variant(self._h, int(ee_variant)))
+
+    def set_ee_pair_list_capacity(self, entries=0):
+        """Capacity of the E-E pair list of variant 0 (0 = 24 per edge + 1024);
+        pairs past it are worked by the search kernel, with the same results."""
+        self._c(self._L.tc_set_ee_pair_list_capacity(self._h, int(entries)))
 
     # ---------------- narrow-phase pair lists (parity instrumentation)
     def set_pair_recording(self, enable=True, max_vt_pairs=1 << 20, max_ee_pairs=1 << 20):

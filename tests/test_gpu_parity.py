@@ -279,16 +279,24 @@ def test_barrier_timeout_reports_status_and_context_survives(oracle_lib):
     assert worst.max() <= 1e-5
 
 
-@pytest.mark.parametrize("n,subdiv,frames", [(96, 4, 3), (256, 5, 1)])
-def test_grouped_ee_kernel_matches(oracle_lib, n, subdiv, frames):
-    """The grouped edge-edge kernel (one lane per edge, per-cell candidate
-    lists in shared memory) against the warp-per-edge kernel: identical pair
-    lists and bit-identical positions; at the smaller size also the oracle's
-    pair lists."""
+@pytest.mark.parametrize("variant,list_cap,n,subdiv,frames", [
+    (1, 0, 96, 4, 3), (1, 0, 256, 5, 1),  # grouped by cell
+    (2, 0, 96, 4, 3), (2, 0, 256, 5, 1),  # contact work in the edge's warp
+    (0, 256 * 6, 96, 4, 3),               # pair list of 6 per segment: most pairs overflow
+    (0, 256, 96, 4, 2),                   # 1 per segment
+    (0, 1, 96, 4, 2),                     # none: every pair worked by the search kernel
+])
+def test_ee_kernel_variants_match(oracle_lib, variant, list_cap, n, subdiv, frames):
+    """The edge-edge kernel shapes against the default (warp per edge, counted
+    pairs listed and worked one lane each): identical pair lists and
+    bit-identical positions; the default with a pair list too small for the
+    scene works the overflowing pairs in the search kernel with the same
+    results.  At the smaller size also the oracle's pair lists."""
     sc = scenes.config2(n=n, subdiv=subdiv)
     a = scenes.build(ClothSimulator, sc)
     b = scenes.build(ClothSimulator, sc)
-    b.set_self_collision_variant(1)
+    b.set_self_collision_variant(variant)
+    b.set_ee_pair_list_capacity(list_cap)
     for s in (a, b):
         s.set_pair_recording(True, 1 << 24, 1 << 23)
     for _ in range(frames):
