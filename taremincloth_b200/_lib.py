@@ -159,6 +159,7 @@ SIGNATURES = {
     "tc_bake_destroy": [_P],
     "tc_ws_param_count": [],
     "tc_ws_enable": [_P, _I, _U, _F],
+    "tc_ws_set_kernel": [_P, _U],
     "tc_ws_record": [_P, _U, _U],
     "tc_ws_recorded": [_P, C.POINTER(_U)],
     "tc_ws_train": [_P, _U, _F, C.c_uint64, C.POINTER(_F), C.POINTER(_F)],

@@ -136,6 +136,12 @@ struct Mlp {
   DBuf<float> z0, z1, z2, dy, dh, dx;
   DBuf<uint32_t> ell;  // inference: [n][16] degree, first 15 neighbours
   unsigned mp_grid = 1;
+  // message-passing inference on the tcgen05 tensor cores (k_mlp_infer_mp_tc)
+  // or, with tc = false, on warp-level mma.sync (k_mlp_infer_mp); err: the
+  // device word a timed-out tensor-core wait sets to 2
+  bool tc = true;
+  unsigned mp_grid_tc = 1;
+  int* err = nullptr;
   uint32_t adam_t = 0;
 
   static unsigned grid(size_t cnt, unsigned b) { return unsigned((cnt + b - 1) / b); }
@@ -151,6 +157,12 @@ struct Mlp {
     const unsigned tiles = grid(n, kWsRows);
     TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp, 256, 0));
     mp_grid = std::max(1u, std::min(tiles, unsigned(std::max(per_sm, 1) * sms)));
+    // persistent tcgen05 CTAs: at most 512 / 64 of them per SM, so that every
+    // resident CTA's TMEM allocation succeeds at once
+    TC_CK(cudaFuncSetAttribute(k_mlp_infer_mp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kWsTcSmemMp)));
+    TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp_tc, kWsTcRows, kWsTcSmemMp));
+    per_sm = std::min(std::max(per_sm, 1), int(512 / kWsTcCols));
+    mp_grid_tc = std::max(1u, std::min(unsigned(grid(n, kWsTcRows)), unsigned(per_sm * sms)));
   }
   // the ELL table of the inference kernels from the host CSR
   void set_ell(const uint32_t* h_off, const uint32_t* h_idx) {
@@ -226,13 +238,17 @@ struct Mlp {
     a.n = n; a.x_feat = feat; if (fa) a.fa = *fa; a.ppred = ppred; a.fscale = w.p + kP_FS;
     a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0; a.h_out = h0.p;
     k_mlp_infer_l0<<<grid(n, kWsL0Rows), kWsL0Rows, 0, st>>>(a);
-    a.ell = ell.p; a.adj_off = adj_off; a.adj_idx = adj_idx;
+    a.ell = ell.p; a.adj_off = adj_off; a.adj_idx = adj_idx; a.err = err;
+    auto mp = [&]() {
+      if (tc) k_mlp_infer_mp_tc<<<mp_grid_tc, kWsTcRows, kWsTcSmemMp, st>>>(a);
+      else k_mlp_infer_mp<<<mp_grid, 256, 0, st>>>(a);
+    };
     a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1; a.h_out = h1.p;
-    k_mlp_infer_mp<<<mp_grid, 256, 0, st>>>(a);
+    mp();
     a.h_prev = h1.p; a.wt = wbt.p + kT_W2; a.bias = w.p + kP_b2; a.h_out = nullptr;
     a.w3 = wb.p + kP_W3; a.b3 = w.p + kP_b3; a.yscale = w.p + kP_YS; a.y_out = y_out; a.x4 = x4; a.p4 = p4;
     a.local_len = local_len;
-    k_mlp_infer_mp<<<mp_grid, 256, 0, st>>>(a);
+    mp();
   }
   // gradients of the loss of the last forward(train, target) into gw (layer
   // 0's input is the scaled copy x0 that forward kept)
@@ -1752,6 +1768,7 @@ struct Sim {
   void ws_setup() {
     if (ws.ready) return;
     ws.net.setup(st, n, adj_off.p, adj_idx.p);
+    ws.net.err = &bar.p->err;  // read back with the frame's barrier status
     ws.net.set_ell(m.adj_off.data(), m.adj_idx.data());
     const std::vector<float> blob = Mlp::init_blob(1);
     ws.net.set_params(blob.data());
@@ -2154,10 +2171,13 @@ struct Sim {
   uint32_t graph_kernels = 0;
   void check_barrier_status() {
     if (*h_err != 0) {
+      const int e = *h_err;
       *h_err = 0;
       TC_CK(cudaMemsetAsync(bar.p, 0, sizeof(GridBar), st));
       TC_CK(cudaStreamSynchronize(st));
-      throw TcError(TC_ERR_TIMEOUT, "a grid barrier of the persistent solver timed out; the frame is incomplete");
+      throw TcError(TC_ERR_TIMEOUT, e == 2 ? "a tensor-core completion wait of the warm-start network timed out; "
+                                             "the frame is incomplete"
+                                           : "a grid barrier of the persistent solver timed out; the frame is incomplete");
     }
   }
   // ---- adaptive substeps: plan before a frame, GPU feedback after it
@@ -4576,6 +4596,16 @@ tc_status tc_ws_enable(tc_sim* s, int enable, uint32_t k_replaced, float res_thr
   });
 }
 
+tc_status tc_ws_set_kernel(tc_sim* s, uint32_t kind) {
+  return guard([&] {
+    need(kind <= 1u, "kind: 0 (tcgen05) or 1 (mma.sync)");
+    Sim& m = S(s);
+    m.ws_setup();
+    m.ws.net.tc = kind == 0u;
+    m.mark();
+  });
+}
+
 tc_status tc_ws_record(tc_sim* s, uint32_t capacity, uint32_t every) {
   return guard([&] {
     Sim& m = S(s);
@@ -4709,10 +4739,17 @@ tc_status tc_mlp_grad(uint32_t n, const float* feat, const uint32_t* adj_off, co
     TC_CK(cudaMemcpyAsync(y, net.y.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
     if (y_infer) {
       tcloth::DBuf<float> d_yi;
+      tcloth::DBuf<int> d_err;
       d_yi.alloc(size_t(n) * 3);
+      d_err.alloc(1);
+      TC_CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), st));
+      net.err = d_err.p;
       net.infer(d_f.p, nullptr, nullptr, d_yi.p, nullptr, nullptr, nullptr);
+      int herr = 0;
       TC_CK(cudaMemcpyAsync(y_infer, d_yi.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+      TC_CK(cudaMemcpyAsync(&herr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
       TC_CK(cudaStreamSynchronize(st));
+      if (herr) throw TcError(TC_ERR_TIMEOUT, "a tensor-core completion wait of the network timed out");
     }
     TC_CK(cudaStreamSynchronize(st));
     TC_CK(cudaGetLastError());

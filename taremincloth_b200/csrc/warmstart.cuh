@@ -17,6 +17,7 @@
 #pragma once
 #include <cuda_bf16.h>
 
+#include "tcgen05.cuh"
 #include "vmath.cuh"
 
 namespace tcloth {
@@ -605,6 +606,7 @@ struct MlpInferArgs {
   const float4* x4;
   float4* p4;
   const float* local_len;
+  int* err;  // tcgen05 kernels: set to 2 when an MMA completion wait ran out (may be null)
 };
 
 // Layer 0: X0 = bf16(bf16(features) * FS), H0 = bf16(SiLU(X0 W0 + b0)).
@@ -801,6 +803,115 @@ __global__ void __launch_bounds__(256, 3) k_mlp_infer_mp(MlpInferArgs a) {
     }
     __syncthreads();  // xs is rewritten by the next tile's gather
   }
+}
+
+// The same message-passing layer on the tcgen05 tensor cores.  A CTA of 128
+// threads takes tiles of 128 vertices, one thread per vertex row: the
+// threads gather X = [H_i, bf16(mean_j H_j)] (128 x 128 bf16) into shared
+// memory in the core-matrix layout of tcgen05.cuh, thread 0 issues eight
+// MMAs of K = 16 into a 128 x 64 fp32 accumulator in tensor memory (TMEM
+// lane = tile row) and commits them to an mbarrier, and every thread reads
+// its row back with tcgen05.ld for the epilogue (bias, SiLU, bf16; or the
+// fused head).  W^T stays in shared memory for the CTA's lifetime.  A
+// completion wait that runs out of polls sets *err = 2 and ends the kernel
+// after one more bounded wait, freeing its TMEM.
+constexpr int kWsTcRows = 128;
+constexpr uint32_t kWsTcCols = 64;         // TMEM columns: the fp32 accumulator
+constexpr uint32_t kWsTcSpin = 1u << 22;   // polls (64 ns sleep each) of an MMA completion wait
+constexpr uint32_t kWsTcSmemMp = kWsTcRows * 128 * 2 + kWsH * 128 * 2;  // X tile + W^T
+__global__ void __launch_bounds__(kWsTcRows, 4) k_mlp_infer_mp_tc(MlpInferArgs a) {
+  extern __shared__ __align__(1024) uint8_t ws_dsm[];
+  uint8_t* xs = ws_dsm;                        // X tile [128 rows][K 128]
+  uint8_t* wsm = ws_dsm + kWsTcRows * 128 * 2;  // W^T [64 outputs][K 128]
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int e = tid; e < kWsH * 16; e += blockDim.x)
+    *reinterpret_cast<uint4*>(wsm + cm_offset(e >> 4, (e & 15) * 8, 128)) =
+        __ldg(reinterpret_cast<const uint4*>(a.wt) + e);
+  if (warp == 0) tmem_alloc(&tslot, kWsTcCols);
+  if (tid == 0) mbar_init(&mbar, 1);
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tslot, xa = smem_addr(xs), wa = smem_addr(wsm);
+  constexpr uint32_t idesc = idesc_bf16_f32(kWsTcRows, kWsH);
+  auto row = [&](uint32_t j, int cg) { return __ldg(reinterpret_cast<const uint4*>(a.h_prev + size_t(j) * kWsH + cg)); };
+  const uint32_t ntiles = (a.n + kWsTcRows - 1) / kWsTcRows;
+  uint32_t parity = 0;
+  bool ok = true;
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint32_t row0 = tile * kWsTcRows;
+#pragma unroll 1
+    for (int m = 0; m < 8; ++m) {
+      const int r = (tid >> 3) + 16 * m, cg = (tid & 7) * 8;
+      const uint32_t v = row0 + r;
+      uint4 self = make_uint4(0, 0, 0, 0), mean = make_uint4(0, 0, 0, 0);
+      if (v < a.n) {
+        self = row(v, cg);
+        mean = ws_neighbour_mean(a, v, cg);
+      }
+      *reinterpret_cast<uint4*>(xs + cm_offset(r, cg, 128)) = self;
+      *reinterpret_cast<uint4*>(xs + cm_offset(r, kWsH + cg, 128)) = mean;
+    }
+    fence_async_smem();
+    tc_fence_before();  // the previous tile's TMEM reads come before this tile's MMAs
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (uint32_t s = 0; s < 8; ++s)
+        mma_bf16(tbase, smem_desc(xa + 256 * s, 128, 2048), smem_desc(wa + 256 * s, 128, 2048), idesc, s > 0);
+      mma_commit(&mbar);
+    }
+    ok = __syncthreads_and(mbar_wait(&mbar, parity, kWsTcSpin));
+    if (!ok) break;
+    parity ^= 1u;
+    tc_fence_after();
+    float z[kWsH];
+    const uint32_t taddr = tbase + (uint32_t(warp * 32) << 16);
+#pragma unroll
+    for (int q = 0; q < kWsH / 16; ++q) tmem_ld16(taddr + 16 * q, z + 16 * q);
+    const uint32_t v = row0 + tid;
+    if (v < a.n) {
+      if (a.w3) {
+        float y[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int c = 0; c < kWsH; ++c) {
+          const float h = __bfloat162float(__float2bfloat16(silu(z[c] + __ldg(a.bias + c))));
+#pragma unroll
+          for (int j = 0; j < 3; ++j) y[j] += h * __bfloat162float(a.w3[c * 3 + j]);
+        }
+        const float Y[3] = {y[0] + a.b3[0], y[1] + a.b3[1], y[2] + a.b3[2]};
+        if (a.y_out)
+          for (int j = 0; j < 3; ++j) a.y_out[size_t(v) * 3 + j] = Y[j];
+        if (a.p4 && a.x4[v].w > 0.f) {
+          const float L = fmaxf(a.local_len[v], 1e-6f), ys = out_scale(a.yscale);
+          float4 p = a.p4[v];
+          p.x += Y[0] * ys * L;
+          p.y += Y[1] * ys * L;
+          p.z += Y[2] * ys * L;
+          a.p4[v] = p;
+        }
+      } else {
+#pragma unroll
+        for (int cg = 0; cg < kWsH; cg += 8) {
+          float hv[8];
+#pragma unroll
+          for (int c = 0; c < 8; ++c) hv[c] = silu(z[cg + c] + __ldg(a.bias + cg + c));
+          *reinterpret_cast<uint4*>(a.h_out + size_t(v) * kWsH + cg) = f32_to_bf16x8(hv);
+        }
+      }
+    }
+  }
+  if (!ok) {
+    if (tid == 0 && a.err) atomicExch(a.err, 2);
+    mbar_wait(&mbar, parity, kWsTcSpin);  // the MMAs still in flight, if any
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tbase, kWsTcCols);
 }
 
 __global__ void k_copy4(uint32_t n, const float4* __restrict__ src, float4* __restrict__ dst) {

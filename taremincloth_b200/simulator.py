@@ -1143,6 +1143,11 @@ class ClothSimulator:
     def ws_disable(self):
         self._c(self._L.tc_ws_enable(self._h, 0, 0, 0.0))
 
+    def ws_set_kernel(self, kind=0):
+        """Tensor-core path of the network's inference: 0 tcgen05 (default),
+        1 warp-level mma.sync."""
+        self._c(self._L.tc_ws_set_kernel(self._h, int(kind)))
+
     def ws_record(self, capacity, every=1):
         """Record `capacity` training snapshots, one every `every` substeps,
         during the following plain frames."""

@@ -61,6 +61,27 @@ def test_mlp_inference_large_graph_matches_reference():
     assert _nrel(y_inf, y_r) <= 5e-3
 
 
+def test_tcgen05_inference_matches_mma_sync():
+    """The warm start's message-passing layers on tcgen05 (TMEM accumulator,
+    the default) against the warp-level mma.sync kernels: same rounding
+    points, so one warm-started substep of config 1 with a random network
+    agrees to fp32 summation order (and the network does move vertices)."""
+    sc = scenes.config1()
+    rng = np.random.default_rng(11)
+    blob = W.random_params(rng)
+    a, b, c = _scene_sims(sc, 3)
+    for s, kind in ((a, 0), (b, 1)):
+        s.ws_set_params(blob)
+        s.ws_set_kernel(kind)
+        s.ws_enable(2, float("inf"))
+    for s in (a, b, c):
+        s.step(sc["dt"] / sc["substeps"], 1)
+    xa, xb, xc = (_state(s)[0] for s in (a, b, c))
+    ext = float(np.linalg.norm(xc.max(0) - xc.min(0)))
+    assert np.abs(xa - xc).max() > 1e-4 * ext  # the network moved the cloth
+    assert np.abs(xa - xb).max() <= 1e-5 * ext, np.abs(xa - xb).max() / ext
+
+
 def _state(sim):
     x, _, v = sim.get_state()
     return x.copy(), v.copy()
