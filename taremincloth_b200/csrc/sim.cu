@@ -157,11 +157,16 @@ struct Mlp {
     const unsigned tiles = grid(n, kWsRows);
     TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp, 256, 0));
     mp_grid = std::max(1u, std::min(tiles, unsigned(std::max(per_sm, 1) * sms)));
-    // persistent tcgen05 CTAs: at most 512 / 64 of them per SM, so that every
-    // resident CTA's TMEM allocation succeeds at once
+    // persistent tcgen05 CTAs: the launch bounds' 3 per SM (the occupancy
+    // query reports a shared-memory limit of 0 blocks for this kernel,
+    // although 3 x 51 KB fit the 233 KB carveout; CTAs never wait for one
+    // another, so any that do not fit simply start later), and at most
+    // 512 / 64 per SM so that every resident CTA's TMEM allocation succeeds
     TC_CK(cudaFuncSetAttribute(k_mlp_infer_mp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kWsTcSmemMp)));
-    TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp_tc, kWsTcRows, kWsTcSmemMp));
-    per_sm = std::min(std::max(per_sm, 1), int(512 / kWsTcCols));
+    TC_CK(cudaFuncSetAttribute(k_mlp_infer_mp_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               int(cudaSharedmemCarveoutMaxShared)));
+    TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp_tc, kWsTcThreads, kWsTcSmemMp));
+    per_sm = std::min(std::max(per_sm, kWsTcMinBlocks), int(512 / kWsTcCols));
     mp_grid_tc = std::max(1u, std::min(unsigned(grid(n, kWsTcRows)), unsigned(per_sm * sms)));
   }
   // the ELL table of the inference kernels from the host CSR
@@ -240,7 +245,7 @@ struct Mlp {
     k_mlp_infer_l0<<<grid(n, kWsL0Rows), kWsL0Rows, 0, st>>>(a);
     a.ell = ell.p; a.adj_off = adj_off; a.adj_idx = adj_idx; a.err = err;
     auto mp = [&]() {
-      if (tc) k_mlp_infer_mp_tc<<<mp_grid_tc, kWsTcRows, kWsTcSmemMp, st>>>(a);
+      if (tc) k_mlp_infer_mp_tc<<<mp_grid_tc, kWsTcThreads, kWsTcSmemMp, st>>>(a);
       else k_mlp_infer_mp<<<mp_grid, 256, 0, st>>>(a);
     };
     a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1; a.h_out = h1.p;

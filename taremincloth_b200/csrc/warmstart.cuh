@@ -805,27 +805,32 @@ __global__ void __launch_bounds__(256, 3) k_mlp_infer_mp(MlpInferArgs a) {
   }
 }
 
-// The same message-passing layer on the tcgen05 tensor cores.  A CTA of 128
-// threads takes tiles of 128 vertices, one thread per vertex row: the
-// threads gather X = [H_i, bf16(mean_j H_j)] (128 x 128 bf16) into shared
-// memory in the core-matrix layout of tcgen05.cuh, thread 0 issues eight
-// MMAs of K = 16 into a 128 x 64 fp32 accumulator in tensor memory (TMEM
-// lane = tile row) and commits them to an mbarrier, and every thread reads
-// its row back with tcgen05.ld for the epilogue (bias, SiLU, bf16; or the
-// fused head).  W^T stays in shared memory for the CTA's lifetime.  A
-// completion wait that runs out of polls sets *err = 2 and ends the kernel
-// after one more bounded wait, freeing its TMEM.
+// The same message-passing layer on the tcgen05 tensor cores.  A CTA of 256
+// threads takes tiles of 128 vertices: the threads gather
+// X = [H_i, bf16(mean_j H_j)] (128 x 128 bf16, four (row, 8-column) pieces
+// per thread) into shared memory in the core-matrix layout of tcgen05.cuh,
+// thread 0 issues eight MMAs of K = 16 into a 128 x 64 fp32 accumulator in
+// tensor memory (TMEM lane = tile row) and commits them to an mbarrier, and
+// the epilogue reads the accumulator back with tcgen05.ld: warps w and w + 4
+// share lane quadrant w, taking columns 0-31 and 32-63 (bias, SiLU, bf16;
+// or the fused head, whose two column halves meet in shared memory).  W^T
+// stays in shared memory for the CTA's lifetime.  A completion wait that
+// runs out of polls sets *err = 2 and ends the kernel after one more bounded
+// wait, freeing its TMEM.
 constexpr int kWsTcRows = 128;
+constexpr int kWsTcThreads = 256;
+constexpr int kWsTcMinBlocks = 3;  // CTAs per SM (launch bounds: 80 registers)
 constexpr uint32_t kWsTcCols = 64;         // TMEM columns: the fp32 accumulator
 constexpr uint32_t kWsTcSpin = 1u << 22;   // polls (64 ns sleep each) of an MMA completion wait
 constexpr uint32_t kWsTcSmemMp = kWsTcRows * 128 * 2 + kWsH * 128 * 2;  // X tile + W^T
-__global__ void __launch_bounds__(kWsTcRows, 4) k_mlp_infer_mp_tc(MlpInferArgs a) {
-  extern __shared__ __align__(1024) uint8_t ws_dsm[];
+__global__ void __launch_bounds__(kWsTcThreads, kWsTcMinBlocks) k_mlp_infer_mp_tc(MlpInferArgs a) {
+  extern __shared__ __align__(128) uint8_t ws_dsm[];
   uint8_t* xs = ws_dsm;                        // X tile [128 rows][K 128]
   uint8_t* wsm = ws_dsm + kWsTcRows * 128 * 2;  // W^T [64 outputs][K 128]
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tslot;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  __shared__ float ypart[kWsTcRows][3];  // fused head: columns 32-63 of each row
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int e = tid; e < kWsH * 16; e += blockDim.x)
     *reinterpret_cast<uint4*>(wsm + cm_offset(e >> 4, (e & 15) * 8, 128)) =
         __ldg(reinterpret_cast<const uint4*>(a.wt) + e);
@@ -839,13 +844,14 @@ __global__ void __launch_bounds__(kWsTcRows, 4) k_mlp_infer_mp_tc(MlpInferArgs a
   constexpr uint32_t idesc = idesc_bf16_f32(kWsTcRows, kWsH);
   auto row = [&](uint32_t j, int cg) { return __ldg(reinterpret_cast<const uint4*>(a.h_prev + size_t(j) * kWsH + cg)); };
   const uint32_t ntiles = (a.n + kWsTcRows - 1) / kWsTcRows;
+  const int quad = warp & 3, half = warp >> 2, er = quad * 32 + lane;  // epilogue: row er, columns 32 half ..
   uint32_t parity = 0;
   bool ok = true;
   for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const uint32_t row0 = tile * kWsTcRows;
 #pragma unroll 1
-    for (int m = 0; m < 8; ++m) {
-      const int r = (tid >> 3) + 16 * m, cg = (tid & 7) * 8;
+    for (int m = 0; m < 4; ++m) {
+      const int r = (tid >> 3) + 32 * m, cg = (tid & 7) * 8;
       const uint32_t v = row0 + r;
       uint4 self = make_uint4(0, 0, 0, 0), mean = make_uint4(0, 0, 0, 0);
       if (v < a.n) {
@@ -869,21 +875,26 @@ __global__ void __launch_bounds__(kWsTcRows, 4) k_mlp_infer_mp_tc(MlpInferArgs a
     if (!ok) break;
     parity ^= 1u;
     tc_fence_after();
-    float z[kWsH];
-    const uint32_t taddr = tbase + (uint32_t(warp * 32) << 16);
+    float z[32];
+    const uint32_t taddr = tbase + (uint32_t(quad * 32) << 16) + uint32_t(half * 32);
+    tmem_ld16(taddr, z);
+    tmem_ld16(taddr + 16, z + 16);
+    const uint32_t v = row0 + er;
+    const int c0 = half * 32;
+    if (a.w3) {
+      float y[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-    for (int q = 0; q < kWsH / 16; ++q) tmem_ld16(taddr + 16 * q, z + 16 * q);
-    const uint32_t v = row0 + tid;
-    if (v < a.n) {
-      if (a.w3) {
-        float y[3] = {0.f, 0.f, 0.f};
+      for (int c = 0; c < 32; ++c) {
+        const float h = __bfloat162float(__float2bfloat16(silu(z[c] + __ldg(a.bias + c0 + c))));
 #pragma unroll
-        for (int c = 0; c < kWsH; ++c) {
-          const float h = __bfloat162float(__float2bfloat16(silu(z[c] + __ldg(a.bias + c))));
-#pragma unroll
-          for (int j = 0; j < 3; ++j) y[j] += h * __bfloat162float(a.w3[c * 3 + j]);
-        }
-        const float Y[3] = {y[0] + a.b3[0], y[1] + a.b3[1], y[2] + a.b3[2]};
+        for (int j = 0; j < 3; ++j) y[j] += h * __bfloat162float(a.w3[(c0 + c) * 3 + j]);
+      }
+      if (half)
+        for (int j = 0; j < 3; ++j) ypart[er][j] = y[j];
+      __syncthreads();
+      if (!half && v < a.n) {
+        const float Y[3] = {(y[0] + ypart[er][0]) + a.b3[0], (y[1] + ypart[er][1]) + a.b3[1],
+                            (y[2] + ypart[er][2]) + a.b3[2]};
         if (a.y_out)
           for (int j = 0; j < 3; ++j) a.y_out[size_t(v) * 3 + j] = Y[j];
         if (a.p4 && a.x4[v].w > 0.f) {
@@ -894,14 +905,14 @@ __global__ void __launch_bounds__(kWsTcRows, 4) k_mlp_infer_mp_tc(MlpInferArgs a
           p.z += Y[2] * ys * L;
           a.p4[v] = p;
         }
-      } else {
+      }
+    } else if (v < a.n) {
 #pragma unroll
-        for (int cg = 0; cg < kWsH; cg += 8) {
-          float hv[8];
+      for (int cg = 0; cg < 32; cg += 8) {
+        float hv[8];
 #pragma unroll
-          for (int c = 0; c < 8; ++c) hv[c] = silu(z[cg + c] + __ldg(a.bias + cg + c));
-          *reinterpret_cast<uint4*>(a.h_out + size_t(v) * kWsH + cg) = f32_to_bf16x8(hv);
-        }
+        for (int c = 0; c < 8; ++c) hv[c] = silu(z[cg + c] + __ldg(a.bias + c0 + cg + c));
+        *reinterpret_cast<uint4*>(a.h_out + size_t(v) * kWsH + c0 + cg) = f32_to_bf16x8(hv);
       }
     }
   }
