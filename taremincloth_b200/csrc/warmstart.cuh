@@ -808,7 +808,7 @@ __global__ void __launch_bounds__(256, 3) k_mlp_infer_mp(MlpInferArgs a) {
 // The same message-passing layer on the tcgen05 tensor cores.  A CTA of 256
 // threads takes tiles of 128 vertices: the threads gather
 // X = [H_i, bf16(mean_j H_j)] (128 x 128 bf16, four (row, 8-column) pieces
-// per thread) into shared memory in the core-matrix layout of tcgen05.cuh,
+// per thread) into shared memory as core matrices (layout below),
 // thread 0 issues eight MMAs of K = 16 into a 128 x 64 fp32 accumulator in
 // tensor memory (TMEM lane = tile row) and commits them to an mbarrier, and
 // the epilogue reads the accumulator back with tcgen05.ld: warps w and w + 4
@@ -822,11 +822,21 @@ constexpr int kWsTcThreads = 256;
 constexpr int kWsTcMinBlocks = 3;  // CTAs per SM (launch bounds: 80 registers)
 constexpr uint32_t kWsTcCols = 64;         // TMEM columns: the fp32 accumulator
 constexpr uint32_t kWsTcSpin = 1u << 22;   // polls (64 ns sleep each) of an MMA completion wait
-constexpr uint32_t kWsTcSmemMp = kWsTcRows * 128 * 2 + kWsH * 128 * 2;  // X tile + W^T
+// X tile layout: K chunk c of all 16 row groups is one run of 16 core
+// matrices (2,048 bytes), and the runs are kWsTcLbo = 2,064 bytes apart
+// (the descriptor's leading byte offset; stride byte offset 128).  The 16
+// extra bytes put the 8 chunks of one row, which a quarter-warp stores at
+// once, in 8 different bank groups.
+constexpr uint32_t kWsTcLbo = 16 * 128 + 16;
+constexpr uint32_t kWsTcXBytes = 16 * kWsTcLbo;
+constexpr uint32_t kWsTcSmemMp = kWsTcXBytes + kWsH * 128 * 2;  // X tile + W^T
+__device__ __forceinline__ uint32_t xs_offset(uint32_t row, uint32_t k) {
+  return (k >> 3) * kWsTcLbo + (row >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
+}
 __global__ void __launch_bounds__(kWsTcThreads, kWsTcMinBlocks) k_mlp_infer_mp_tc(MlpInferArgs a) {
   extern __shared__ __align__(128) uint8_t ws_dsm[];
-  uint8_t* xs = ws_dsm;                        // X tile [128 rows][K 128]
-  uint8_t* wsm = ws_dsm + kWsTcRows * 128 * 2;  // W^T [64 outputs][K 128]
+  uint8_t* xs = ws_dsm;                 // X tile [128 rows][K 128] (xs_offset)
+  uint8_t* wsm = ws_dsm + kWsTcXBytes;  // W^T [64 outputs][K 128] (cm_offset)
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tslot;
   __shared__ float ypart[kWsTcRows][3];  // fused head: columns 32-63 of each row
@@ -858,8 +868,8 @@ __global__ void __launch_bounds__(kWsTcThreads, kWsTcMinBlocks) k_mlp_infer_mp_t
         self = row(v, cg);
         mean = ws_neighbour_mean(a, v, cg);
       }
-      *reinterpret_cast<uint4*>(xs + cm_offset(r, cg, 128)) = self;
-      *reinterpret_cast<uint4*>(xs + cm_offset(r, kWsH + cg, 128)) = mean;
+      *reinterpret_cast<uint4*>(xs + xs_offset(r, cg)) = self;
+      *reinterpret_cast<uint4*>(xs + xs_offset(r, kWsH + cg)) = mean;
     }
     fence_async_smem();
     tc_fence_before();  // the previous tile's TMEM reads come before this tile's MMAs
@@ -868,7 +878,8 @@ __global__ void __launch_bounds__(kWsTcThreads, kWsTcMinBlocks) k_mlp_infer_mp_t
       tc_fence_after();
 #pragma unroll
       for (uint32_t s = 0; s < 8; ++s)
-        mma_bf16(tbase, smem_desc(xa + 256 * s, 128, 2048), smem_desc(wa + 256 * s, 128, 2048), idesc, s > 0);
+        mma_bf16(tbase, smem_desc(xa + 2 * s * kWsTcLbo, kWsTcLbo, 128), smem_desc(wa + 256 * s, 128, 2048), idesc,
+                 s > 0);
       mma_commit(&mbar);
     }
     ok = __syncthreads_and(mbar_wait(&mbar, parity, kWsTcSpin));
