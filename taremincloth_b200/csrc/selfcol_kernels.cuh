@@ -352,17 +352,34 @@ __global__ void k_hash_sort_buckets(uint32_t table, const uint32_t* __restrict__
 
 // The same canonical order (each bucket ascending), one warp per bucket: up
 // to 64 entries are sorted in registers by a bitonic network (two per lane,
-// padding 0xFFFFFFFF, which no index reaches); longer buckets fall back to
-// the serial insertion sort on lane 0.
-__global__ void k_hash_sort_buckets_warp(uint32_t table, const uint32_t* __restrict__ starts,
-                                         uint32_t* __restrict__ sorted) {
+// padding 0xFFFFFFFF, which no index reaches); up to kSortRankCap entries by
+// rank in shared memory; longer buckets fall back to the serial insertion
+// sort on lane 0.  Blocks of 8 warps.
+constexpr uint32_t kSortRankCap = 1024;
+__global__ void __launch_bounds__(256) k_hash_sort_buckets_warp(uint32_t table, const uint32_t* __restrict__ starts,
+                                                                uint32_t* __restrict__ sorted) {
+  __shared__ uint32_t sh_sort[8][kSortRankCap];
   const uint32_t h = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const uint32_t lane = threadIdx.x & 31u;
   if (h >= table) return;  // whole warp
   const uint32_t b = starts[h], e = starts[h + 1];
   const uint32_t n = e - b;
   if (n < 2) return;
-  if (n > 64) {
+  if (n > 64 && n <= kSortRankCap) {
+    // rank sort in shared memory: the entries are distinct indices, so the
+    // rank of v (the number of smaller entries) is its sorted position
+    uint32_t* buf = sh_sort[threadIdx.x >> 5];
+    for (uint32_t i = lane; i < n; i += 32u) buf[i] = sorted[b + i];
+    __syncwarp();
+    for (uint32_t i = lane; i < n; i += 32u) {
+      const uint32_t v = buf[i];
+      uint32_t r = 0;
+      for (uint32_t k = 0; k < n; ++k) r += buf[k] < v ? 1u : 0u;
+      sorted[b + r] = v;
+    }
+    return;
+  }
+  if (n > 64) {  // larger than kSortRankCap: insertion sort by one lane
     if (lane == 0)
       for (uint32_t k = b + 1; k < e; ++k) {
         const uint32_t v = sorted[k];
@@ -1391,7 +1408,7 @@ __global__ void __launch_bounds__(256, 4) k_ee_pairs(SCArgs s) {
 
 // Deferred CCD pairs, one thread each (the CCD search plus the discrete
 // fall-through of shaders/self_collision_ee_direct.wgsl:404-774).
-__global__ void __launch_bounds__(256) k_ee_ccd(SCArgs s) {
+__global__ void __launch_bounds__(256, 3) k_ee_ccd(SCArgs s) {
   const uint32_t total = min(*s.ccd_n, s.ccd_cap);
   for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x)
     ee_listed_pair(s, s.ccd_q[q], false);

@@ -993,7 +993,7 @@ struct Sim {
     nrm.alloc(n);
     acc.alloc(size_t(n) * A_N);
     vcell.alloc(n); mlen.alloc(n); sbox.alloc(3 * size_t(n)); ecell.alloc(ne); eamin.alloc(ne); eamax.alloc(ne);
-    ccd_q.alloc(size_t(ne) * 4 + 1024); ccd_n.alloc(1 + tcloth::kEeSeg);
+    ccd_q.alloc(size_t(ne) * 8 + 1024); ccd_n.alloc(1 + tcloth::kEeSeg);
     ee_q.alloc(size_t(ne) * 24 + 1024);
     vs_p.alloc(n); vs_q.alloc(n); vs_c.alloc(n); tile_sum.alloc(64); es_c.alloc(ne); es_v.alloc(ne); es_lo.alloc(ne); es_hi.alloc(ne);
     TC_CK(cudaMemsetAsync(acc.p, 0, size_t(n) * A_N * sizeof(int32_t), st));

@@ -198,6 +198,36 @@ def test_hash_state_bit_exact(oracle_lib):
         np.testing.assert_array_equal(s_g, s_o)
 
 
+@pytest.mark.parametrize("cell", [0.08, 0.12, 0.5])
+def test_hash_crowded_buckets_match_static_build(cell):
+    """Coarse hash cells crowd the buckets past the 64 entries of the
+    register sort (rank sort in shared memory up to 1,024, the serial
+    fallback beyond): the simulator's vertex hash equals the allocation-free
+    build's (whose bucket sort is a separate kernel) bit for bit."""
+    import ctypes as C
+    import torch
+    from taremincloth_b200 import _lib
+    L = _lib.load()
+    sc = scenes.config2(n=96, subdiv=3)
+    g = scenes.build(ClothSimulator, sc)
+    g.step(sc["dt"], sc["substeps"])
+    g.set_hash_cell_size(cell)
+    cs_ref, srt_ref = g.get_hash_state(0)
+    _, p, _ = g.get_state()
+    n, table = len(p), g.get_counts()["table_size"]
+    assert np.diff(cs_ref.astype(np.int64)).max() > 64
+    pos = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    pos[:, :3] = torch.from_numpy(np.ascontiguousarray(p)).cuda()
+    cs = torch.full((table + 1,), -1, dtype=torch.int32, device="cuda")
+    srt = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    _lib.check(L.tc_hash_build_static(C.c_void_p(pos.data_ptr()), n, float(cell), int(table),
+                                      C.c_void_p(cs.data_ptr()), C.c_void_p(srt.data_ptr()),
+                                      C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(cs.cpu().numpy().view(np.uint32), cs_ref)
+    np.testing.assert_array_equal(srt.cpu().numpy().view(np.uint32), srt_ref)
+
+
 def test_colouring_on_device_matches_oracle(oracle_lib):
     sc = scenes.config1()
     g = scenes.build(ClothSimulator, sc)
