@@ -555,10 +555,10 @@ tc_status tc_last_frame_ms(tc_sim *s, float *ms);
  * runs the k_replaced remaining iterations.  Needs cooperative launch. */
 uint32_t tc_ws_param_count(void);
 tc_status tc_ws_enable(tc_sim *s, int enable, uint32_t k_replaced, float res_thresh);
-/* Tensor-core path of the network's message-passing layers at inference:
- * 0 (default) = tcgen05.mma with the accumulator in tensor memory, 1 =
- * warp-level mma.sync.  Both round at the same points; the fp32 sums may
- * differ in order. */
+/* Tensor-core path of the network's message-passing layers (inference, and
+ * training forward and backward): 0 (default) = tcgen05.mma with the
+ * accumulators in tensor memory, 1 = warp-level mma.sync.  Both round at the
+ * same points; the fp32 sums may differ in order. */
 tc_status tc_ws_set_kernel(tc_sim *s, uint32_t kind);
 /* Record training snapshots during the following plain frames: every
  * `every`-th substep until `capacity` snapshots are held; a new recording

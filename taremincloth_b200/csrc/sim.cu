@@ -140,7 +140,7 @@ struct Mlp {
   // or, with tc = false, on warp-level mma.sync (k_mlp_infer_mp); err: the
   // device word a timed-out tensor-core wait sets to 2
   bool tc = true;
-  unsigned mp_grid_tc = 1;
+  unsigned mp_grid_tc = 1, bwd_grid_tc = 1;
   int* err = nullptr;
   uint32_t adam_t = 0;
 
@@ -168,6 +168,11 @@ struct Mlp {
     TC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer_mp_tc, kWsTcThreads, kWsTcSmemMp));
     per_sm = std::min(std::max(per_sm, kWsTcMinBlocks), int(512 / kWsTcCols));
     mp_grid_tc = std::max(1u, std::min(unsigned(grid(n, kWsTcRows)), unsigned(per_sm * sms)));
+    // backward: 2 CTAs per SM (80 KB of shared memory and 256 TMEM columns each)
+    TC_CK(cudaFuncSetAttribute(k_mlp_layer_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kWsBwdSmem)));
+    TC_CK(cudaFuncSetAttribute(k_mlp_layer_bwd_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               int(cudaSharedmemCarveoutMaxShared)));
+    bwd_grid_tc = std::max(1u, std::min(unsigned(grid(n, 128)), unsigned(2 * sms)));
   }
   // the ELL table of the inference kernels from the host CSR
   void set_ell(const uint32_t* h_off, const uint32_t* h_idx) {
@@ -224,12 +229,23 @@ struct Mlp {
     a.kin = kWsF; a.x_feat = feat; a.fscale = w.p + kP_FS; a.wt = wbt.p + kT_W0; a.bias = w.p + kP_b0;
     a.x_out = train ? x0.p : nullptr; a.z_out = train ? z0.p : nullptr; a.h_out = h0.p;
     k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
-    a.kin = 128; a.x_feat = nullptr; a.fscale = nullptr; a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1;
-    a.x_out = train ? x1.p : nullptr; a.z_out = train ? z1.p : nullptr; a.h_out = h1.p;
-    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
-    a.h_prev = h1.p; a.wt = wbt.p + kT_W2; a.bias = w.p + kP_b2;
-    a.x_out = train ? x2.p : nullptr; a.z_out = train ? z2.p : nullptr; a.h_out = h2.p;
-    k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    if (tc) {  // the message-passing layers on tcgen05, with the training outputs
+      MlpInferArgs b{};
+      b.n = n; b.ell = ell.p; b.adj_off = adj_off; b.adj_idx = adj_idx; b.err = err;
+      b.h_prev = h0.p; b.wt = wbt.p + kT_W1; b.bias = w.p + kP_b1; b.h_out = h1.p;
+      b.x_out = train ? x1.p : nullptr; b.z_out = train ? z1.p : nullptr;
+      k_mlp_infer_mp_tc<<<mp_grid_tc, kWsTcThreads, kWsTcSmemMp, st>>>(b);
+      b.h_prev = h1.p; b.wt = wbt.p + kT_W2; b.bias = w.p + kP_b2; b.h_out = h2.p;
+      b.x_out = train ? x2.p : nullptr; b.z_out = train ? z2.p : nullptr;
+      k_mlp_infer_mp_tc<<<mp_grid_tc, kWsTcThreads, kWsTcSmemMp, st>>>(b);
+    } else {
+      a.kin = 128; a.x_feat = nullptr; a.fscale = nullptr; a.h_prev = h0.p; a.wt = wbt.p + kT_W1; a.bias = w.p + kP_b1;
+      a.x_out = train ? x1.p : nullptr; a.z_out = train ? z1.p : nullptr; a.h_out = h1.p;
+      k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+      a.h_prev = h1.p; a.wt = wbt.p + kT_W2; a.bias = w.p + kP_b2;
+      a.x_out = train ? x2.p : nullptr; a.z_out = train ? z2.p : nullptr; a.h_out = h2.p;
+      k_mlp_layer_fwd<<<grid(n, kWsRows), kWsFwdThreads, 0, st>>>(a);
+    }
     k_mlp_head<<<grid(n, 256), 256, 0, st>>>(n, h2.p, wb.p + kP_W3, w.p + kP_b3, y.p, target, mask, w.p + kP_YS,
                                              1.0f / float(n), target ? dy.p : nullptr, loss);
   }
@@ -263,10 +279,17 @@ struct Mlp {
     const unsigned gh = grid(size_t(n) * kWsH, 256), gt = grid(n, kWsRows);
     k_mlp_head_bwd<<<grid(n, 256), 256, 0, st>>>(n, h2.p, wb.p + kP_W3, dy.p, dh.p, gw.p + kP_W3, gw.p + kP_b3);
     k_mlp_act_bwd<<<gh, 256, 0, st>>>(n, dh.p, z2.p, dz.p, gw.p + kP_b2);
-    k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, 128, x2.p, dz.p, wb.p + kP_W2, gw.p + kP_W2, dx.p});
+    auto bwd128 = [&](const __nv_bfloat16* x, uint32_t wo) {
+      if (tc)
+        k_mlp_layer_bwd_tc<<<bwd_grid_tc, 256, kWsBwdSmem, st>>>(
+            MlpBwdTcArgs{n, x, dz.p, wb.p + wo, gw.p + wo, dx.p, err});
+      else
+        k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, 128, x, dz.p, wb.p + wo, gw.p + wo, dx.p});
+    };
+    bwd128(x2.p, kP_W2);
     k_mlp_agg_bwd<<<gh, 256, 0, st>>>(n, dx.p, adj_off, adj_idx, dh.p);
     k_mlp_act_bwd<<<gh, 256, 0, st>>>(n, dh.p, z1.p, dz.p, gw.p + kP_b1);
-    k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, 128, x1.p, dz.p, wb.p + kP_W1, gw.p + kP_W1, dx.p});
+    bwd128(x1.p, kP_W1);
     k_mlp_agg_bwd<<<gh, 256, 0, st>>>(n, dx.p, adj_off, adj_idx, dh.p);
     k_mlp_act_bwd<<<gh, 256, 0, st>>>(n, dh.p, z0.p, dz.p, gw.p + kP_b0);
     k_mlp_layer_bwd<<<gt, 128, 0, st>>>(MlpBwdArgs{n, kWsF, x0.p, dz.p, wb.p + kP_W0, gw.p + kP_W0, nullptr});
@@ -1975,8 +1998,10 @@ struct Sim {
     }
     std::vector<float> h(size_t(epochs) * cnt);
     TC_CK(cudaMemcpyAsync(h.data(), ws.losses.p, h.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaMemcpyAsync(h_err, &bar.p->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaStreamSynchronize(st));
     TC_CK(cudaGetLastError());
+    check_barrier_status();
     double a = 0, b = 0;
     for (uint32_t j = 0; j < cnt; ++j) { a += h[j]; b += h[size_t(epochs - 1) * cnt + j]; }
     if (first) *first = float(a / cnt);
@@ -4737,26 +4762,25 @@ tc_status tc_mlp_grad(uint32_t n, const float* feat, const uint32_t* adj_off, co
     net.set_ell(adj_off, adj_idx);
     net.alloc_train();
     net.set_params(params);
+    tcloth::DBuf<int> d_err;
+    d_err.alloc(1);
+    TC_CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), st));
+    net.err = d_err.p;
     net.forward(d_f.p, true, d_t.p, d_m.p, d_loss.p);
     net.backward();
     TC_CK(cudaMemcpyAsync(loss, d_loss.p, sizeof(float), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaMemcpyAsync(grads, net.gw.p, tcloth::kP_N * sizeof(float), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaMemcpyAsync(y, net.y.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    tcloth::DBuf<float> d_yi;
     if (y_infer) {
-      tcloth::DBuf<float> d_yi;
-      tcloth::DBuf<int> d_err;
       d_yi.alloc(size_t(n) * 3);
-      d_err.alloc(1);
-      TC_CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), st));
-      net.err = d_err.p;
       net.infer(d_f.p, nullptr, nullptr, d_yi.p, nullptr, nullptr, nullptr);
-      int herr = 0;
       TC_CK(cudaMemcpyAsync(y_infer, d_yi.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
-      TC_CK(cudaMemcpyAsync(&herr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-      TC_CK(cudaStreamSynchronize(st));
-      if (herr) throw TcError(TC_ERR_TIMEOUT, "a tensor-core completion wait of the network timed out");
     }
+    int herr = 0;
+    TC_CK(cudaMemcpyAsync(&herr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaStreamSynchronize(st));
+    if (herr) throw TcError(TC_ERR_TIMEOUT, "a tensor-core completion wait of the network timed out");
     TC_CK(cudaGetLastError());
   });
 }

@@ -25,6 +25,7 @@ namespace tcloth {
 constexpr int kWsF = 16;   // input features
 constexpr int kWsH = 64;   // hidden width
 constexpr int kWsRows = 64;  // vertices per block tile (4 warps x 16 rows)
+constexpr uint32_t kWsTcSpin = 1u << 22;  // polls (64 ns sleep each) of a tcgen05 MMA completion wait
 
 // fp32 parameter blob: weights row-major [in][out], then the bias; then the
 // normalizer, which training does not change (its gradient is zero): the
@@ -394,6 +395,133 @@ __global__ void __launch_bounds__(128) k_mlp_layer_bwd(MlpBwdArgs a) {
   }
 }
 
+// Backward of a 128-wide layer on the tcgen05 tensor cores.  Persistent CTAs
+// of 256 threads take tiles of 128 rows; per tile they stage, as K-major core
+// matrices: X^T (M = 128 inputs x K = 128 rows) and dZ^T (N = 64 x K = 128
+// rows) for dW, and dZ (M = 128 rows x K = 64) for dX; W (N = 128 x K = 64)
+// is staged once.  Thread 0 issues 4 MMAs of dX = dZ W^T into TMEM columns
+// 64-191 (fresh per tile) and 8 MMAs of dW += X^T dZ into columns 0-63,
+// which accumulate over all of the CTA's tiles; one commit per tile.  dX
+// rows go out from the per-tile epilogue, and each CTA adds its dW to the
+// global sum once at the end.  A completion wait that runs out of polls sets
+// *err = 2.  Grid: the resident CTAs (2 per SM: 80 KB of shared memory,
+// 256 TMEM columns each).
+struct MlpBwdTcArgs {
+  uint32_t n;
+  const __nv_bfloat16* x;   // [n][128]
+  const __nv_bfloat16* dz;  // [n][64]
+  const __nv_bfloat16* w;   // [128][64] row-major weights
+  float* dw;                // [128][64], added to
+  float* dx;                // [n][128] or null
+  int* err;
+};
+constexpr uint32_t kWsBwdCols = 256;
+constexpr uint32_t kWsBwdSmem = 128 * 128 * 2 + 64 * 128 * 2 + 128 * 64 * 2 + 128 * 64 * 2;
+__global__ void __launch_bounds__(256, 2) k_mlp_layer_bwd_tc(MlpBwdTcArgs a) {
+  extern __shared__ __align__(128) uint8_t bw_dsm[];
+  uint8_t* adw = bw_dsm;                    // X^T  [128 inputs][K 128 rows]
+  uint8_t* bdw = adw + 128 * 128 * 2;       // dZ^T [64 outputs][K 128 rows]
+  uint8_t* adx = bdw + 64 * 128 * 2;        // dZ   [128 rows][K 64]
+  uint8_t* bdx = adx + 128 * 64 * 2;        // W    [128 inputs][K 64]
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int e = tid; e < 128 * 8; e += blockDim.x)  // W row c, 8 outputs per uint4
+    *reinterpret_cast<uint4*>(bdx + cm_offset(e >> 3, (e & 7) * 8, 64)) = __ldg(reinterpret_cast<const uint4*>(a.w) + e);
+  if (warp == 0) tmem_alloc(&tslot, kWsBwdCols);
+  if (tid == 0) mbar_init(&mbar, 1);
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tslot;
+  const uint32_t a_dw = smem_addr(adw), b_dw = smem_addr(bdw), a_dx = smem_addr(adx), b_dx = smem_addr(bdx);
+  constexpr uint32_t id_dw = idesc_bf16_f32(128, 64), id_dx = idesc_bf16_f32(128, 128);
+  const uint32_t ntiles = (a.n + 127) / 128;
+  const int quad = warp & 3, half = warp >> 2;
+  uint32_t parity = 0;
+  bool ok = true, any = false;
+  auto pair = [](uint16_t lo, uint16_t hi) { return uint32_t(lo) | (uint32_t(hi) << 16); };
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint32_t row0 = tile * 128;
+    // X^T: rows 2p, 2p + 1 and inputs c0 .. c0 + 7 per item (1024 items)
+    for (int e = tid; e < 64 * 16; e += blockDim.x) {
+      const int rp = e & 63, c0 = (e >> 6) * 8, r = 2 * rp;
+      const uint32_t v0 = row0 + r, v1 = v0 + 1;
+      const uint4 u0 = v0 < a.n ? __ldg(reinterpret_cast<const uint4*>(a.x + size_t(v0) * 128 + c0)) : make_uint4(0, 0, 0, 0);
+      const uint4 u1 = v1 < a.n ? __ldg(reinterpret_cast<const uint4*>(a.x + size_t(v1) * 128 + c0)) : make_uint4(0, 0, 0, 0);
+      const uint16_t* h0 = reinterpret_cast<const uint16_t*>(&u0);
+      const uint16_t* h1 = reinterpret_cast<const uint16_t*>(&u1);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) *reinterpret_cast<uint32_t*>(adw + cm_offset(c0 + i, r, 128)) = pair(h0[i], h1[i]);
+    }
+    // dZ^T (rows 2p, 2p + 1, outputs n0 .. n0 + 7) and dZ itself
+    for (int e = tid; e < 64 * 8; e += blockDim.x) {
+      const int rp = e & 63, n0 = (e >> 6) * 8, r = 2 * rp;
+      const uint32_t v0 = row0 + r, v1 = v0 + 1;
+      const uint4 u0 = v0 < a.n ? __ldg(reinterpret_cast<const uint4*>(a.dz + size_t(v0) * kWsH + n0)) : make_uint4(0, 0, 0, 0);
+      const uint4 u1 = v1 < a.n ? __ldg(reinterpret_cast<const uint4*>(a.dz + size_t(v1) * kWsH + n0)) : make_uint4(0, 0, 0, 0);
+      const uint16_t* h0 = reinterpret_cast<const uint16_t*>(&u0);
+      const uint16_t* h1 = reinterpret_cast<const uint16_t*>(&u1);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) *reinterpret_cast<uint32_t*>(bdw + cm_offset(n0 + i, r, 128)) = pair(h0[i], h1[i]);
+      *reinterpret_cast<uint4*>(adx + cm_offset(r, n0, 64)) = u0;
+      *reinterpret_cast<uint4*>(adx + cm_offset(r + 1, n0, 64)) = u1;
+    }
+    fence_async_smem();
+    tc_fence_before();  // the previous tile's TMEM reads come before this tile's MMAs
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        mma_bf16(tbase + 64, smem_desc(a_dx + 256 * s, 128, 1024), smem_desc(b_dx + 256 * s, 128, 1024), id_dx, s > 0);
+#pragma unroll
+      for (uint32_t s = 0; s < 8; ++s)
+        mma_bf16(tbase, smem_desc(a_dw + 256 * s, 128, 2048), smem_desc(b_dw + 256 * s, 128, 2048), id_dw,
+                 any || s > 0);
+      mma_commit(&mbar);
+    }
+    any = true;
+    ok = __syncthreads_and(mbar_wait(&mbar, parity, kWsTcSpin));
+    if (!ok) break;
+    parity ^= 1u;
+    tc_fence_after();
+    if (a.dx) {
+      const uint32_t r = quad * 32 + lane, v = row0 + r;
+#pragma unroll
+      for (int c0 = 0; c0 < 64; c0 += 32) {
+        float z[32];
+        const uint32_t taddr = tbase + (uint32_t(quad * 32) << 16) + 64u + uint32_t(half * 64 + c0);
+        tmem_ld16(taddr, z);
+        tmem_ld16(taddr + 16, z + 16);
+        if (v < a.n) {
+          float4* o = reinterpret_cast<float4*>(a.dx + size_t(v) * 128 + half * 64 + c0);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) o[q] = make_float4(z[4 * q], z[4 * q + 1], z[4 * q + 2], z[4 * q + 3]);
+        }
+      }
+    }
+  }
+  if (ok && any) {
+    // dW rows (TMEM lanes) c = 32 quad + lane, outputs 32 half .. 32 half + 31
+    const uint32_t c = quad * 32 + lane;
+    float z[32];
+    const uint32_t taddr = tbase + (uint32_t(quad * 32) << 16) + uint32_t(half * 32);
+    tmem_ld16(taddr, z);
+    tmem_ld16(taddr + 16, z + 16);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) atomicAdd(&a.dw[c * kWsH + half * 32 + k], z[k]);
+  }
+  if (!ok) {
+    if (tid == 0 && a.err) atomicExch(a.err, 2);
+    mbar_wait(&mbar, parity, kWsTcSpin);  // the MMAs still in flight, if any
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tbase, kWsBwdCols);
+}
+
 // dH_prev[j] = dX[j][0:64] + sum_{i in N(j)} dX[i][64:128] / deg(i)
 // (the adjacency is symmetric, so the transpose of the mean is a gather).
 __global__ void k_mlp_agg_bwd(uint32_t n, const float* __restrict__ dx, const uint32_t* __restrict__ adj_off,
@@ -607,6 +735,10 @@ struct MlpInferArgs {
   float4* p4;
   const float* local_len;
   int* err;  // tcgen05 kernels: set to 2 when an MMA completion wait ran out (may be null)
+  // training forward (k_mlp_infer_mp_tc without the head): the gathered X
+  // rows [n][128] and Z = X W + b [n][64] (both may be null)
+  __nv_bfloat16* x_out;
+  float* z_out;
 };
 
 // Layer 0: X0 = bf16(bf16(features) * FS), H0 = bf16(SiLU(X0 W0 + b0)).
@@ -821,7 +953,6 @@ constexpr int kWsTcRows = 128;
 constexpr int kWsTcThreads = 256;
 constexpr int kWsTcMinBlocks = 3;  // CTAs per SM (launch bounds: 80 registers)
 constexpr uint32_t kWsTcCols = 64;         // TMEM columns: the fp32 accumulator
-constexpr uint32_t kWsTcSpin = 1u << 22;   // polls (64 ns sleep each) of an MMA completion wait
 // X tile layout: K chunk c of all 16 row groups is one run of 16 core
 // matrices (2,048 bytes), and the runs are kWsTcLbo = 2,064 bytes apart
 // (the descriptor's leading byte offset; stride byte offset 128).  The 16
@@ -870,6 +1001,10 @@ __global__ void __launch_bounds__(kWsTcThreads, kWsTcMinBlocks) k_mlp_infer_mp_t
       }
       *reinterpret_cast<uint4*>(xs + xs_offset(r, cg)) = self;
       *reinterpret_cast<uint4*>(xs + xs_offset(r, kWsH + cg)) = mean;
+      if (a.x_out && v < a.n) {
+        *reinterpret_cast<uint4*>(a.x_out + size_t(v) * 128 + cg) = self;
+        *reinterpret_cast<uint4*>(a.x_out + size_t(v) * 128 + kWsH + cg) = mean;
+      }
     }
     fence_async_smem();
     tc_fence_before();  // the previous tile's TMEM reads come before this tile's MMAs
@@ -920,9 +1055,17 @@ __global__ void __launch_bounds__(kWsTcThreads, kWsTcMinBlocks) k_mlp_infer_mp_t
     } else if (v < a.n) {
 #pragma unroll
       for (int cg = 0; cg < 32; cg += 8) {
-        float hv[8];
+        float zb[8], hv[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) hv[c] = silu(z[cg + c] + __ldg(a.bias + c0 + cg + c));
+        for (int c = 0; c < 8; ++c) {
+          zb[c] = z[cg + c] + __ldg(a.bias + c0 + cg + c);
+          hv[c] = silu(zb[c]);
+        }
+        if (a.z_out) {
+          float4* zo = reinterpret_cast<float4*>(a.z_out + size_t(v) * kWsH + c0 + cg);
+          zo[0] = make_float4(zb[0], zb[1], zb[2], zb[3]);
+          zo[1] = make_float4(zb[4], zb[5], zb[6], zb[7]);
+        }
         *reinterpret_cast<uint4*>(a.h_out + size_t(v) * kWsH + c0 + cg) = f32_to_bf16x8(hv);
       }
     }

@@ -1144,8 +1144,8 @@ class ClothSimulator:
         self._c(self._L.tc_ws_enable(self._h, 0, 0, 0.0))
 
     def ws_set_kernel(self, kind=0):
-        """Tensor-core path of the network's inference: 0 tcgen05 (default),
-        1 warp-level mma.sync."""
+        """Tensor-core path of the network's message-passing layers (inference
+        and training): 0 tcgen05 (default), 1 warp-level mma.sync."""
         self._c(self._L.tc_ws_set_kernel(self._h, int(kind)))
 
     def ws_record(self, capacity, every=1):
