@@ -630,7 +630,7 @@ struct Sim {
   }
   DBuf<Prim> prims;
   DBuf<MeshTri> tris;
-  DBuf<float4> bounds, cl16, cl256;
+  DBuf<float4> bounds, cl16, cl256, cl4096;
   // batched instances (empty for a single cloth)
   std::vector<uint32_t> inst_vert_off;  // n_instances + 1
   // cluster solver: bins of whole instances, one thread-block cluster each
@@ -1023,7 +1023,7 @@ struct Sim {
     TC_CK(cudaMemsetAsync(nrm.p, 0, size_t(n) * sizeof(float4), st));
     res_sum.alloc(m.dist_cnt.size() + m.bend_cnt.size() + 1);
     res_max.alloc(m.dist_cnt.size() + m.bend_cnt.size() + 1);
-    prims.alloc(1); tris.alloc(1); bounds.alloc(1); cl16.alloc(1); cl256.alloc(1);
+    prims.alloc(1); tris.alloc(1); bounds.alloc(1); cl16.alloc(1); cl256.alloc(1); cl4096.alloc(1);
     dist_offc.upload(m.dist_off, st); dist_cntc.upload(m.dist_cnt, st);
     bend_offc.upload(m.bend_off, st); bend_cntc.upload(m.bend_cnt, st);
     sew_h = m.sew;
@@ -1181,19 +1181,21 @@ struct Sim {
       Rg = Rg * (1.0 + 1e-5) + 1e-7;
       return make_float4(float(C[0]), float(C[1]), float(C[2]), float(Rg));
     };
-    const uint32_t n16 = (T + 15) / 16, n256 = (T + 255) / 256;
-    std::vector<float4> g16(n16), g256(n256);
+    const uint32_t n16 = (T + 15) / 16, n256 = (T + 255) / 256, n4096 = (T + 4095) / 4096;
+    std::vector<float4> g16(n16), g256(n256), g4096(n4096);
     for (uint32_t g = 0; g < n16; ++g) g16[g] = group(g * 16, std::min(T, g * 16 + 16));
     for (uint32_t g = 0; g < n256; ++g) g256[g] = group(g * 256, std::min(T, g * 256 + 256));
-    const void* before[4] = {tris.p, bounds.p, cl16.p, cl256.p};
+    for (uint32_t g = 0; g < n4096; ++g) g4096[g] = group(g * 4096, std::min(T, g * 4096 + 4096));
+    const void* before[5] = {tris.p, bounds.p, cl16.p, cl256.p, cl4096.p};
     tris.upload(tris_h, st);
     bounds.upload(bd, st);
     cl16.upload(g16, st);
     cl256.upload(g256, st);
+    cl4096.upload(g4096, st);
     TC_CK(cudaStreamSynchronize(st));
     // the recorded frame only holds pointers and the triangle count: new
     // contents of the same size replay without re-recording
-    const void* after[4] = {tris.p, bounds.p, cl16.p, cl256.p};
+    const void* after[5] = {tris.p, bounds.p, cl16.p, cl256.p, cl4096.p};
     if (T != graph_ntris || std::memcmp(before, after, sizeof before) != 0) mark();
     graph_ntris = T;
     ce_stale = true;
@@ -1413,7 +1415,7 @@ struct Sim {
   ColliderArgs collider_args() {
     ColliderArgs c;
     c.prims = prims.p; c.nprims = uint32_t(prims_h.size());
-    c.tris = tris.p; c.bounds = bounds.p; c.cl16 = cl16.p; c.cl256 = cl256.p; c.ntris = uint32_t(tris_h.size());
+    c.tris = tris.p; c.bounds = bounds.p; c.cl16 = cl16.p; c.cl256 = cl256.p; c.cl4096 = cl4096.p; c.ntris = uint32_t(tris_h.size());
     c.recovery = recovery;
     c.vinst = inst_prims_h.empty() ? nullptr : vinst.p;
     c.inst_prims = inst_prims_h.empty() ? nullptr : inst_prims.p;

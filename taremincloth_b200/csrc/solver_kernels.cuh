@@ -483,6 +483,7 @@ struct ColliderArgs {
   const float4* bounds;   // per triangle: centroid, r
   const float4* cl16;     // per 16 triangles: conservative sphere for 1.5 r
   const float4* cl256;    // per 256 triangles
+  const float4* cl4096;   // per 4,096 triangles
   uint32_t ntris;
   bool recovery;
   BoneSdfArgs bone;       // bone SDF colliders (nbones == 0: off)
@@ -498,9 +499,10 @@ __device__ __forceinline__ bool group_far(V3 a, V3 b, float4 g, float th) {
 
 // shaders/collision.wgsl:378-652 (cluster culling off, the reference
 // default).  The triangle loop visits triangles in ascending (Morton) order
-// exactly like the reference; two levels of conservative bounding spheres
-// skip runs of triangles none of which could pass the per-triangle test, so
-// the sequence of applied contacts is unchanged.
+// exactly like the reference; three levels of conservative bounding spheres
+// (4,096, 256 and 16 triangles, each enclosing its members' own test
+// spheres) skip runs of triangles none of which could pass the per-triangle
+// test, so the sequence of applied contacts is unchanged.
 template <bool kBone, class M>
 __device__ __forceinline__ void collide_vertex_m(uint32_t i, const M& m, const ColliderArgs& ca, float dt) {
   float4 x = m.ldx(i);
@@ -553,18 +555,22 @@ __device__ __forceinline__ void collide_vertex_m(uint32_t i, const M& m, const C
     MeshState st;
     st.bpos = p;
     st.bn = mk(0.f, 0.f, 0.f);
-    const uint32_t ng256 = (ca.ntris + 255u) / 256u;
-    for (uint32_t g = 0; g < ng256; ++g) {
-      if (group_far(xpos, p, ca.cl256[g], th)) continue;
-      const uint32_t c_end = min((g + 1u) * 16u, (ca.ntris + 15u) / 16u);
-      for (uint32_t cgi = g * 16u; cgi < c_end; ++cgi) {
-        if (group_far(xpos, p, ca.cl16[cgi], th)) continue;
-        const uint32_t t_end = min((cgi + 1u) * 16u, ca.ntris);
-        for (uint32_t t = cgi * 16u; t < t_end; ++t) {
-          const float4 b = ca.bounds[t];
-          const float r = b.w * 1.5f + th;
-          if (seg_point_d2(xpos, p, mk(b)) > r * r) continue;
-          mesh_triangle(ca.tris[t], th, xpos, p, xn, dt, pinit, ca.recovery, st);
+    const uint32_t ng256 = (ca.ntris + 255u) / 256u, ng4096 = (ca.ntris + 4095u) / 4096u;
+    for (uint32_t g4 = 0; g4 < ng4096; ++g4) {
+      if (group_far(xpos, p, ca.cl4096[g4], th)) continue;
+      const uint32_t g_end = min((g4 + 1u) * 16u, ng256);
+      for (uint32_t g = g4 * 16u; g < g_end; ++g) {
+        if (group_far(xpos, p, ca.cl256[g], th)) continue;
+        const uint32_t c_end = min((g + 1u) * 16u, (ca.ntris + 15u) / 16u);
+        for (uint32_t cgi = g * 16u; cgi < c_end; ++cgi) {
+          if (group_far(xpos, p, ca.cl16[cgi], th)) continue;
+          const uint32_t t_end = min((cgi + 1u) * 16u, ca.ntris);
+          for (uint32_t t = cgi * 16u; t < t_end; ++t) {
+            const float4 b = ca.bounds[t];
+            const float r = b.w * 1.5f + th;
+            if (seg_point_d2(xpos, p, mk(b)) > r * r) continue;
+            mesh_triangle(ca.tris[t], th, xpos, p, xn, dt, pinit, ca.recovery, st);
+          }
         }
       }
     }
