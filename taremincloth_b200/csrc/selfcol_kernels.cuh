@@ -61,8 +61,8 @@ struct SCArgs {
   const float4* vs_q;   // local edge length, layer bits, inverse mass, |p - x| of vertex srt[k]
   const int4* es_c;     // cell, index of edge esrt[k]
   const uint2* es_v;    // endpoints of edge esrt[k]
-  const float4* es_lo;  // swept AABB of edge esrt[k]
-  const float4* es_hi;
+  const float4* es_lo;  // swept AABB of edge esrt[k]; .w: bits of its first endpoint
+  const float4* es_hi;  // .w: bits of its second endpoint
   // pairs that need the continuous (CCD) search are deferred to k_ee_ccd
   uint2* ccd_q;
   uint32_t* ccd_n;
@@ -315,9 +315,15 @@ __global__ void k_gather_edges(uint32_t ne, const uint32_t* __restrict__ esrt, c
   const uint32_t e = esrt[k];
   const int4 c = ecell[e];
   es_c[k] = make_int4(c.x, c.y, c.z, (int)e);
-  es_v[k] = edges[e];
-  es_lo[k] = amin[e];
-  es_hi[k] = amax[e];
+  const uint2 v = edges[e];
+  es_v[k] = v;
+  // the box records also carry the endpoints (bits in .w), so the E-E
+  // filter needs no separate endpoint load
+  float4 lo = amin[e], hi = amax[e];
+  lo.w = __uint_as_float(v.x);
+  hi.w = __uint_as_float(v.y);
+  es_lo[k] = lo;
+  es_hi[k] = hi;
 }
 
 // Canonical in-bucket order: ascending index.  Buckets hold a few to a few
@@ -1486,8 +1492,8 @@ __global__ void __launch_bounds__(256, kList ? 8 : 4) k_ee(const __grid_constant
         slot = sh_beg[warp][k] + (t - sh_start[warp][k]);
         // one level of loads for the whole filter
         const int4 bc = s.es_c[slot];
-        const uint2 ebv = s.es_v[slot];
         const float4 bmin = s.es_lo[slot], bmax = s.es_hi[slot];
+        const uint2 ebv = make_uint2(__float_as_uint(bmin.w), __float_as_uint(bmax.w));
         const uint32_t eb = (uint32_t)bc.w;
         eb_l = eb;
         pass = ei < eb && !(ebv.x == c.u0 || ebv.x == c.u1 || ebv.y == c.u0 || ebv.y == c.u1) &&
