@@ -14,12 +14,15 @@
 // pins either, so this row is parity unpinned against the reference and
 // bit-exact against the oracle).
 //
-// The bake visits each bone's triangles in the reference's order for every
-// voxel.  A triangle, or a tile of 32, is skipped only when a conservative
-// bounding-sphere lower bound on its squared distance exceeds the voxel's
-// running minimum plus the tie tolerance: such a triangle cannot be accepted
-// by the sequential rule, so the state after it is unchanged and the result
-// equals the full scan.
+// The bake reproduces, per voxel, the reference's sequential scan of a bone's
+// triangles (the first triangle within the tie tolerance of the running
+// minimum with a larger |projection| wins, so the result depends on the
+// order).  It runs in two passes: an order-free search for the minimum
+// squared distance m, then the sequential rule over the triangles within a
+// small window above m, started at a triangle where the full scan provably
+// resets its state (k_bone_bake states the argument).  A triangle, or a tile
+// of 32, is skipped only when a conservative bounding-sphere lower bound on
+// its squared distance shows that it cannot matter.
 #pragma once
 #include <cuda_fp16.h>
 
@@ -137,6 +140,12 @@ __global__ void k_bone_tile_spheres(uint32_t ntiles, const uint32_t* __restrict_
   tsph[k] = make_float4(m.x, m.y, m.z, r * 1.001f + 1e-5f);
 }
 
+__global__ void k_bake_perm_spheres(uint32_t nt, const uint32_t* __restrict__ perm, const float4* __restrict__ sph,
+                                    float4* __restrict__ psph) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nt) psph[i] = sph[perm[i]];
+}
+
 __device__ __forceinline__ uint32_t pack_half2(float lo, float hi) {
   return (uint32_t)__half_as_ushort(__float2half_rn(lo)) | ((uint32_t)__half_as_ushort(__float2half_rn(hi)) << 16);
 }
@@ -149,7 +158,9 @@ struct BakeState {
 __device__ __forceinline__ float bake_reach(float min_d2) {
   return sqrtf((min_d2 + 1e-7f * fmaxf(1.0f, min_d2)) * 1.0001f);
 }
-__device__ __forceinline__ void bake_visit(BakeState& s, V3 p, const BakeTri& tri) {
+// Closest point of the triangle to p (bake_sdf.wgsl:71-130): returns the squared
+// distance and leaves p - closest point in `diff` and the barycentrics in `bary`.
+__device__ __forceinline__ float bake_closest(V3 p, const BakeTri& tri, V3& diff, V3& bary_out) {
   const V3 a = mk(tri.p0w0), b = mk(tri.p1w1), c = mk(tri.p2w2);
   const V3 ab = b - a, ac = c - a, ap = p - a;
   const float d1 = dot(ab, ap), d2 = dot(ac, ap);
@@ -198,8 +209,15 @@ __device__ __forceinline__ void bake_visit(BakeState& s, V3 p, const BakeTri& tr
       }
     }
   }
-  const V3 diff = p - cp;
-  const float d_sq = dot(diff, diff);
+  diff = p - cp;
+  bary_out = bary;
+  return dot(diff, diff);
+}
+// The sequential rule for one triangle whose closest point is known
+// (bake_sdf.wgsl:131-183): accepted when closer by more than the tolerance, or
+// within it with a larger |projection|.
+__device__ __forceinline__ void bake_accept(BakeState& s, const BakeTri& tri, V3 diff, V3 bary, float d_sq) {
+  const V3 a = mk(tri.p0w0), b = mk(tri.p1w1), c = mk(tri.p2w2);
   const V3 nrm = mk(tri.n_bmask);
   const float proj = dot(diff, nrm);
   const float aproj = fabsf(proj);
@@ -235,49 +253,375 @@ __device__ __forceinline__ void bake_visit(BakeState& s, V3 p, const BakeTri& tr
     s.best_alpha = (bary.x * tri.p0w0.w + bary.y * tri.p1w1.w) + bary.z * tri.p2w2.w;
   }
 }
+__device__ __forceinline__ void bake_visit(BakeState& s, V3 p, const BakeTri& tri) {
+  V3 diff, bary;
+  const float d_sq = bake_closest(p, tri, diff, bary);
+  bake_accept(s, tri, diff, bary, d_sq);
+}
 // true when nothing in the sphere can be accepted for this voxel state
 // |p - c| - r > reach, tested on squares with a 1e-5 relative margin for
 // rounding (no square root per test)
-__device__ __forceinline__ bool bake_far(const BakeState& s, V3 p, float4 sph) {
+__device__ __forceinline__ bool bake_far_r(float reach, V3 p, float4 sph) {
   const V3 d = p - mk(sph);
-  const float rr = sph.w + s.reach;
+  const float rr = sph.w + reach;
   return dot(d, d) > (rr * rr) * 1.00001f;
 }
+__device__ __forceinline__ bool bake_far(const BakeState& s, V3 p, float4 sph) { return bake_far_r(s.reach, p, sph); }
 
 // ---- bake_sdf.wgsl:33-196.  Block = 8 warps = an 8 x 8 x 4 voxel region of
-// one bone; each warp owns a 4 x 4 x 2 brick.  blockIdx.y = entry of `params`.
-__global__ void __launch_bounds__(256) k_bone_bake(const BakeParams* __restrict__ params, const BakeTri* __restrict__ tris,
+// one bone; each warp owns a 4 x 4 x 2 brick, a lane one voxel.
+// blockIdx.y = entry of `params`.
+//
+// Per voxel the reference keeps, in triangle order, the state (running
+// minimum R of the accepted squared distances, the last accepted triangle),
+// accepting d when d + eps(R) < R, or when |d - R| <= eps(R) with a larger
+// |projection| (eps(R) = 1e-7 max(1, R)).  The kernel gets the same state
+// without an ordered walk over every triangle:
+//  A. a first bound on m, the minimum squared distance, from the spatial
+//     tile (`perm`, tile spheres `stsph`) nearest to the brick;
+//  B. one order-free pass over the spatial tiles: (voxel, triangle) pairs
+//     that the sphere bound cannot rule out are queued and evaluated 32 at a
+//     time, lowering m by a shared-memory atomic min and listing every
+//     triangle with d <= m + W (W = 4e-6 max(1, m)) for its voxel;
+//  C. per voxel, the listed window G = {d <= T}, T = m + W, sorted by
+//     triangle index, runs through the rule from its first "hard record": a
+//     member below T and below every earlier member by more than
+//     gap = 1e-6 max(1, qmin).
+// Exact: every triangle outside G has d > T, so at a hard record the full
+// scan's running minimum is >= qmin and the rule resets the state to that
+// triangle alone (closer by more than eps, with room for fp32 rounding); after
+// it R < T - gap, so every triangle outside G is rejected.  The full scan thus
+// ends in the state of the windowed scan.  A voxel whose list overflowed, or
+// whose window holds no hard record, collects its window again in rounds of
+// kBakeList sorted indices (retried four times wider, since any T is valid),
+// and after three retries takes the ordered full scan over the
+// triangle-order tiles (`tsph`).
+constexpr uint32_t kBakeList = 16;
+constexpr uint32_t kBakeCol = 256;  // threads (voxels) per block: 8 warps, an 8 x 8 x 4 region
+__device__ __forceinline__ float bake_window(float m) { return 4.0e-6f * fmaxf(1.0f, m); }
+__device__ __forceinline__ V3 bake_voxel(const BakeParams& P, float fr, uint32_t vx, uint32_t vy, uint32_t vz) {
+  const V3 uvw = mk((float(vx) + 0.5f) / fr, (float(vy) + 0.5f) / fr, (float(vz) + 0.5f) / fr);
+  return mk(P.lmin[0] + uvw.x * (P.lmax[0] - P.lmin[0]), P.lmin[1] + uvw.y * (P.lmax[1] - P.lmin[1]),
+            P.lmin[2] + uvw.z * (P.lmax[2] - P.lmin[2]));
+}
+__device__ __forceinline__ void bake_list_insert(uint32_t* lst, uint32_t& n, bool& more, uint32_t o) {
+  // ascending list in shared memory, stride kBakeCol (one column per thread)
+  uint32_t j;
+  if (n < kBakeList) {
+    j = n++;
+  } else {
+    more = true;
+    if (o > lst[(kBakeList - 1) * kBakeCol]) return;
+    j = kBakeList - 1;
+  }
+  while (j > 0 && lst[(j - 1) * kBakeCol] > o) {
+    lst[j * kBakeCol] = lst[(j - 1) * kBakeCol];
+    --j;
+  }
+  lst[j * kBakeCol] = o;
+}
+__device__ __forceinline__ BakeTri bake_tri(const BakeTri* __restrict__ tris, uint32_t o) {
+  return BakeTri{__ldg(&tris[o].p0w0), __ldg(&tris[o].p1w1), __ldg(&tris[o].p2w2), __ldg(&tris[o].n_bmask)};
+}
+// pair evaluation of phase B: voxel slot `slot` of this block at p
+__device__ __forceinline__ void bake_pair(const BakeTri* __restrict__ tris, V3 p, uint32_t o, uint32_t slot,
+                                          uint32_t* sh_m, uint32_t* sh_cnt, uint32_t* sh_ct, float* sh_cd) {
+  V3 diff, bary;
+  const float d = bake_closest(p, bake_tri(tris, o), diff, bary);
+  if (!(d <= 3.0e38f)) return;  // NaN or inf: never accepted by the rule
+  atomicMin(&sh_m[slot], __float_as_uint(d));
+  const float mv = __uint_as_float(sh_m[slot]);
+  if (d <= mv + bake_window(mv)) {
+    const uint32_t c = atomicAdd(&sh_cnt[slot], 1u);
+    if (c < kBakeList) {
+      sh_ct[c * kBakeCol + slot] = o;
+      sh_cd[c * kBakeCol + slot] = d;
+    }
+  }
+}
+__global__ void __launch_bounds__(kBakeCol, 3) k_bone_bake(const BakeParams* __restrict__ params, const BakeTri* __restrict__ tris,
                                                    const float4* __restrict__ sph, const float4* __restrict__ tsph,
+                                                   const uint32_t* __restrict__ perm, const float4* __restrict__ psph,
+                                                   const float4* __restrict__ stsph,
                                                    const uint32_t* __restrict__ bone_tile_off,
                                                    const uint32_t* __restrict__ param_bone,
                                                    uint32_t* __restrict__ atlas) {
+  __shared__ uint32_t sh_list[kBakeList * kBakeCol];  // phase-B candidate indices, then the rounds' lists
+  __shared__ float sh_cd[kBakeList * kBakeCol];       // phase-B candidate squared distances
+  __shared__ uint32_t sh_m[kBakeCol], sh_cnt[kBakeCol];  // per voxel: running minimum (bits), candidates
+  __shared__ uint32_t sh_qv[8][64], sh_qt[8][64];       // per warp: queued (voxel lane, triangle) pairs
+  __shared__ float4 sh_sph[8][32];                       // per warp: the current tile's triangle spheres
+  __shared__ uint32_t sh_tri[8][32];                     // and triangle indices
   const BakeParams P = params[blockIdx.y];
   const uint32_t res = P.res;
-  const uint32_t bx = (res + 7) / 8, by = (res + 7) / 8;
+  const uint32_t nbx = (res + 7) / 8, nby = (res + 7) / 8;
   const uint32_t blk = blockIdx.x;
-  const uint32_t ox = (blk % bx) * 8, oy = ((blk / bx) % by) * 8, oz = (blk / (bx * by)) * 4;
+  const uint32_t ox = (blk % nbx) * 8, oy = ((blk / nbx) % nby) * 8, oz = (blk / (nbx * nby)) * 4;
   if (oz >= res) return;  // whole block
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t vx = ox + (warp & 1) * 4 + (lane & 3);
-  const uint32_t vy = oy + ((warp >> 1) & 1) * 4 + ((lane >> 2) & 3);
-  const uint32_t vz = oz + (warp >> 2) * 2 + (lane >> 4);
+  const uint32_t bx0 = ox + (warp & 1) * 4, by0 = oy + ((warp >> 1) & 1) * 4, bz0 = oz + (warp >> 2) * 2;
+  const uint32_t vx = bx0 + (lane & 3), vy = by0 + ((lane >> 2) & 3), vz = bz0 + (lane >> 4);
   const bool valid = vx < res && vy < res && vz < res;
   const float fr = float(res);
-  const V3 uvw = mk((float(vx) + 0.5f) / fr, (float(vy) + 0.5f) / fr, (float(vz) + 0.5f) / fr);
-  const V3 p = mk(P.lmin[0] + uvw.x * (P.lmax[0] - P.lmin[0]), P.lmin[1] + uvw.y * (P.lmax[1] - P.lmin[1]),
-                  P.lmin[2] + uvw.z * (P.lmax[2] - P.lmin[2]));
-  BakeState s{1e10f, -1.0f, 10.0f, 0.0f, bake_reach(1e10f)};
+  const V3 p = bake_voxel(P, fr, vx, vy, vz);
   const uint32_t t0 = P.tri_start, tn = P.tri_count;
   const uint32_t tile0 = bone_tile_off[param_bone[blockIdx.y]];
-  for (uint32_t k = 0; k * 32u < tn; ++k) {
-    const bool skip_tile = !valid || bake_far(s, p, __ldg(tsph + tile0 + k));
-    if (__all_sync(0xffffffffu, skip_tile)) continue;
-    const uint32_t e = min(32u, tn - k * 32u);
+  const uint32_t ntile = (tn + 31u) / 32u;
+  const uint32_t me = threadIdx.x;  // this voxel's slot
+  uint32_t* lst = sh_list + me;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+
+  // A. first bound on m from the spatial tile nearest to the brick
+  uint32_t bt = 0;
+  {
+    const V3 pc = bake_voxel(P, fr, bx0 + 1, by0 + 1, bz0);
+    float bk = 1.0e30f;
+    for (uint32_t k = lane; k < ntile; k += 32u) {
+      const float4 ts = __ldg(stsph + tile0 + k);
+      const float key = length(pc - mk(ts)) - ts.w;
+      if (key < bk) { bk = key; bt = k; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ok = __shfl_xor_sync(0xffffffffu, bk, o);
+      const uint32_t ot = __shfl_xor_sync(0xffffffffu, bt, o);
+      if (ok < bk || (ok == bk && ot < bt)) { bk = ok; bt = ot; }
+    }
+  }
+  float m = 1.0e30f;
+  if (valid && bt < ntile) {
+    const uint32_t e = min(32u, tn - bt * 32u);
     for (uint32_t q = 0; q < e; ++q) {
-      const uint32_t t = t0 + k * 32u + q;
-      if (skip_tile || bake_far(s, p, __ldg(sph + t))) continue;
-      const BakeTri tri{__ldg(&tris[t].p0w0), __ldg(&tris[t].p1w1), __ldg(&tris[t].p2w2), __ldg(&tris[t].n_bmask)};
-      bake_visit(s, p, tri);
+      V3 diff, bary;
+      const float d = bake_closest(p, bake_tri(tris, __ldg(perm + t0 + bt * 32u + q)), diff, bary);
+      m = fminf(m, d);
+    }
+  }
+  sh_m[me] = __float_as_uint(m);
+  sh_cnt[me] = 0u;
+  __syncwarp();
+
+  // B. order-free pass over the spatial tiles in rings of growing distance
+  // from the brick, nearest first, so that m tightens early: (voxel,
+  // triangle) pairs that the sphere bound cannot rule out are queued and
+  // evaluated 32 at a time, lowering m by a shared-memory atomic min and
+  // listing every triangle with d <= m + W for its voxel.  A tile is left out
+  // of a ring only when its sphere lies farther from every voxel of the brick
+  // than the largest reach sqrt((m + W) * 1.0001) of the brick.
+  {
+    uint32_t* qv = sh_qv[warp];
+    uint32_t* qt = sh_qt[warp];
+    float4* ssph = sh_sph[warp];
+    uint32_t* stri = sh_tri[warp];
+    uint32_t qn = 0;
+    const V3 ca = bake_voxel(P, fr, bx0, by0, bz0), cb = bake_voxel(P, fr, bx0 + 3, by0 + 3, bz0 + 1);
+    const V3 pc = (ca + cb) * 0.5f;
+    const float brad = length(cb - ca) * 0.5f * 1.001f + 1e-5f;  // every voxel of the brick lies within brad of pc
+    float lim = -INFINITY;
+    while (true) {
+      float rmax = 0.f;
+      if (valid) {
+        const float mv = __uint_as_float(sh_m[me]);
+        rmax = sqrtf((mv + bake_window(mv)) * 1.0001f);
+      }
+      for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+      const float cut = rmax * 1.0001f + 1e-5f;
+      float next = 3.0e38f;
+      for (uint32_t k = lane; k < ntile; k += 32u) {
+        const float4 ts = __ldg(stsph + tile0 + k);
+        float key = length(pc - mk(ts)) - ts.w - brad;
+        if (!(key == key)) key = -3.0e38f;  // a tile with a NaN sphere goes first
+        if (key > lim && key < next) next = key;
+      }
+      for (int o = 16; o > 0; o >>= 1) next = fminf(next, __shfl_xor_sync(0xffffffffu, next, o));
+      if (!(next <= cut)) break;
+      const float hi = fminf(cut, next + fmaxf(2.0f * brad, 0.5f * (cut - next)));
+      for (uint32_t kb = 0; kb < ntile; kb += 32u) {
+        bool sel = false;
+        if (kb + lane < ntile) {
+          const float4 ts = __ldg(stsph + tile0 + kb + lane);
+          float key = length(pc - mk(ts)) - ts.w - brad;
+          if (!(key == key)) key = -3.0e38f;
+          sel = key > lim && key <= hi;
+        }
+        uint32_t bm = __ballot_sync(0xffffffffu, sel);
+        while (bm) {
+          const uint32_t k = kb + uint32_t(__ffs(bm) - 1);
+          bm &= bm - 1u;
+          const uint32_t e = min(32u, tn - k * 32u);
+          __syncwarp();
+          if (lane < e) {
+            ssph[lane] = __ldg(psph + t0 + k * 32u + lane);
+            stri[lane] = __ldg(perm + t0 + k * 32u + lane);
+          }
+          __syncwarp();
+          uint32_t mask = 0u;
+          if (valid) {
+            const float mv = __uint_as_float(sh_m[me]);
+            const float reach = sqrtf((mv + bake_window(mv)) * 1.0001f);
+            for (uint32_t q = 0; q < e; ++q)
+              if (!bake_far_r(reach, p, ssph[q])) mask |= 1u << q;
+          }
+          while (__any_sync(0xffffffffu, mask != 0u)) {
+            const bool has = mask != 0u;
+            const uint32_t q = has ? uint32_t(__ffs(mask) - 1) : 0u;
+            mask &= mask - 1u;
+            const uint32_t b = __ballot_sync(0xffffffffu, has);
+            if (has) {
+              const uint32_t at = qn + __popc(b & lt_mask);
+              qv[at] = lane;
+              qt[at] = stri[q];
+            }
+            qn += __popc(b);
+            if (qn >= 32u) {
+              __syncwarp();
+              const uint32_t v = qv[lane];
+              bake_pair(tris, bake_voxel(P, fr, bx0 + (v & 3), by0 + ((v >> 2) & 3), bz0 + (v >> 4)), qt[lane],
+                        warp * 32u + v, sh_m, sh_cnt, sh_list, sh_cd);
+              __syncwarp();
+              qn -= 32u;
+              if (lane < qn) {
+                qv[lane] = qv[32 + lane];
+                qt[lane] = qt[32 + lane];
+              }
+              // drop candidates above this voxel's window
+              const float mv = __uint_as_float(sh_m[me]);
+              const uint32_t c = sh_cnt[me];
+              if (c > kBakeList / 2 && c <= kBakeList) {
+                uint32_t kept = 0;
+                for (uint32_t i = 0; i < c; ++i) {
+                  const float d = sh_cd[i * kBakeCol + me];
+                  if (d <= mv + bake_window(mv)) {
+                    lst[kept * kBakeCol] = lst[i * kBakeCol];
+                    sh_cd[kept * kBakeCol + me] = d;
+                    ++kept;
+                  }
+                }
+                sh_cnt[me] = kept;
+              }
+              __syncwarp();
+            }
+          }
+        }
+      }
+      lim = hi;
+    }
+    __syncwarp();
+    if (lane < qn) {
+      const uint32_t v = qv[lane];
+      bake_pair(tris, bake_voxel(P, fr, bx0 + (v & 3), by0 + ((v >> 2) & 3), bz0 + (v >> 4)), qt[lane],
+                warp * 32u + v, sh_m, sh_cnt, sh_list, sh_cd);
+    }
+    __syncwarp();
+  }
+
+  // C. the listed window in the reference's order
+  m = __uint_as_float(sh_m[me]);
+  const float T0 = m + bake_window(m);
+  BakeState s{1e10f, -1.0f, 10.0f, 0.0f, bake_reach(1e10f)};
+  bool started = false;
+  {
+    const uint32_t c = sh_cnt[me];
+    if (valid && c <= kBakeList) {
+      uint32_t n = 0;
+      for (uint32_t i = 0; i < c; ++i) {  // members of G, insertion-sorted by index
+        if (!(sh_cd[i * kBakeCol + me] <= T0)) continue;
+        const uint32_t o = lst[i * kBakeCol];
+        uint32_t j = n++;
+        while (j > 0 && lst[(j - 1) * kBakeCol] > o) {
+          lst[j * kBakeCol] = lst[(j - 1) * kBakeCol];
+          --j;
+        }
+        lst[j * kBakeCol] = o;
+      }
+      float qmin = T0;
+      for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t o = lst[i * kBakeCol];
+        const BakeTri tri = bake_tri(tris, o);
+        V3 diff, bary;
+        const float d_sq = bake_closest(p, tri, diff, bary);
+        if (started) {
+          bake_accept(s, tri, diff, bary, d_sq);
+        } else if (d_sq + 1.0e-6f * fmaxf(1.0f, qmin) < qmin) {
+          started = true;
+          bake_accept(s, tri, diff, bary, d_sq);
+        } else {
+          qmin = fminf(qmin, d_sq);
+        }
+      }
+    }
+  }
+  __syncwarp();
+
+  // the window again in rounds, for voxels whose list overflowed or held no
+  // hard record
+  float W = bake_window(m);
+  float T = m + W;
+  float qmin = T;
+  uint32_t lo = t0, retries = 0;
+  bool need = valid && !started, full = false;
+  if (need) s = BakeState{1e10f, -1.0f, 10.0f, 0.0f, bake_reach(1e10f)};
+  while (__any_sync(0xffffffffu, need)) {
+    const float rT = sqrtf(T * 1.0001f);
+    uint32_t n = 0;
+    bool more = false;
+    for (uint32_t k = 0; k < ntile; ++k) {
+      const float r = started ? fminf(rT, s.reach) : rT;
+      const bool skip_tile = !need || bake_far_r(r, p, __ldg(stsph + tile0 + k));
+      if (__all_sync(0xffffffffu, skip_tile)) continue;
+      const uint32_t e = min(32u, tn - k * 32u);
+      for (uint32_t q = 0; q < e; ++q) {
+        const uint32_t pos = t0 + k * 32u + q;
+        if (skip_tile || bake_far_r(started ? fminf(rT, s.reach) : rT, p, __ldg(psph + pos))) continue;
+        const uint32_t o = __ldg(perm + pos);
+        if (o < lo) continue;
+        V3 diff, bary;
+        if (bake_closest(p, bake_tri(tris, o), diff, bary) <= T) bake_list_insert(lst, n, more, o);
+      }
+    }
+    if (need) {
+      for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t o = lst[i * kBakeCol];
+        const BakeTri tri = bake_tri(tris, o);
+        V3 diff, bary;
+        const float d_sq = bake_closest(p, tri, diff, bary);
+        if (started) {
+          bake_accept(s, tri, diff, bary, d_sq);
+        } else if (d_sq + 1.0e-6f * fmaxf(1.0f, qmin) < qmin) {
+          started = true;
+          bake_accept(s, tri, diff, bary, d_sq);
+        } else {
+          qmin = fminf(qmin, d_sq);
+        }
+      }
+      if (more) {
+        lo = lst[(kBakeList - 1) * kBakeCol] + 1u;
+      } else if (started) {
+        need = false;
+      } else if (retries < 3) {
+        ++retries;
+        W *= 4.0f;
+        T = m + W;
+        qmin = T;
+        lo = t0;
+      } else {
+        need = false;
+        full = true;
+      }
+    }
+  }
+
+  // the ordered full scan for voxels whose windows held no hard record
+  if (__any_sync(0xffffffffu, full)) {
+    if (full) s = BakeState{1e10f, -1.0f, 10.0f, 0.0f, bake_reach(1e10f)};
+    for (uint32_t k = 0; k < ntile; ++k) {
+      const bool skip_tile = !full || bake_far(s, p, __ldg(tsph + tile0 + k));
+      if (__all_sync(0xffffffffu, skip_tile)) continue;
+      const uint32_t e = min(32u, tn - k * 32u);
+      for (uint32_t q = 0; q < e; ++q) {
+        const uint32_t t = t0 + k * 32u + q;
+        if (skip_tile || bake_far(s, p, __ldg(sph + t))) continue;
+        bake_visit(s, p, bake_tri(tris, t));
+      }
     }
   }
   if (!valid) return;

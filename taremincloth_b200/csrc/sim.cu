@@ -345,11 +345,58 @@ static BakeTiles make_bake_tiles(const std::vector<uint32_t>& start, const std::
   return t;
 }
 
-// Device side of a bake: triangles, spheres, tiles, parameters.
+// Spatial order of each bone's triangles for the bake's order-free passes:
+// within [start[b], start[b] + count[b]) the triangle indices sorted by the
+// 30-bit Morton code of their centroid in the bone range's bounding box
+// (stable, so equal codes keep the triangle order).  Only the culling depends
+// on this order, not the baked values.
+static std::vector<uint32_t> bake_spatial_perm(const std::vector<float>& cent, const std::vector<uint32_t>& start,
+                                               const std::vector<uint32_t>& count, uint32_t nt) {
+  std::vector<uint32_t> perm(nt);
+  for (uint32_t t = 0; t < nt; ++t) perm[t] = t;
+  // ranges that overlap or leave [0, nt) keep the triangle order everywhere
+  std::vector<std::pair<uint32_t, uint32_t>> rg;
+  for (size_t b = 0; b < start.size(); ++b)
+    if (count[b]) rg.emplace_back(start[b], count[b]);
+  std::sort(rg.begin(), rg.end());
+  for (size_t i = 0; i < rg.size(); ++i)
+    if (uint64_t(rg[i].first) + rg[i].second > nt || (i && uint64_t(rg[i - 1].first) + rg[i - 1].second > rg[i].first))
+      return perm;
+  for (size_t b = 0; b < start.size(); ++b) {
+    const uint32_t s0 = start[b], c = count[b];
+    if (c < 2) continue;
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    for (uint32_t i = s0; i < s0 + c; ++i)
+      for (int a = 0; a < 3; ++a) {
+        const float v = cent[3 * size_t(i) + a];
+        if (std::isfinite(v)) { lo[a] = std::min(lo[a], v); hi[a] = std::max(hi[a], v); }
+      }
+    std::vector<std::pair<uint32_t, uint32_t>> key(c);
+    for (uint32_t i = 0; i < c; ++i) {
+      uint32_t code = 0;
+      for (int a = 0; a < 3; ++a) {
+        const float span = hi[a] > lo[a] ? hi[a] - lo[a] : 1.f;
+        const float v = cent[3 * size_t(s0 + i) + a];
+        const float u = std::isfinite(v) ? (v - lo[a]) / span : 0.f;
+        const uint32_t q = uint32_t(std::min(std::max(u, 0.f), 1.f) * 1023.f);
+        for (int bit = 0; bit < 10; ++bit) code |= ((q >> bit) & 1u) << (3 * bit + a);
+      }
+      key[i] = {code, s0 + i};
+    }
+    std::stable_sort(key.begin(), key.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    for (uint32_t i = 0; i < c; ++i) perm[s0 + i] = key[i].second;
+  }
+  return perm;
+}
+
+// Device side of a bake: triangles, spheres, tiles, parameters.  Two tile
+// sets share one layout (32 positions per tile, the same tiles per bone):
+// triangle-order tiles over the triangles themselves (`tsph`) and spatial
+// tiles over `perm` (`psph`, the triangle spheres in perm order; `stsph`).
 struct BakeGpu {
   DBuf<BakeTri> tris;
-  DBuf<float4> sph, tsph;
-  DBuf<uint32_t> tile_first, tile_cnt, tile_off, param_bone;
+  DBuf<float4> sph, tsph, psph, stsph;
+  DBuf<uint32_t> tile_first, tile_cnt, tile_off, param_bone, perm;
   DBuf<BakeParams> params;
   uint32_t nt = 0, ntiles = 0;
   void setup_tiles(const BakeTiles& t, cudaStream_t st) {
@@ -359,19 +406,30 @@ struct BakeGpu {
     tile_off.upload(t.bone_off, st);
     sph.alloc(std::max<uint32_t>(nt, 1));
     tsph.alloc(std::max<uint32_t>(ntiles, 1));
+    psph.alloc(std::max<uint32_t>(nt, 1));
+    stsph.alloc(std::max<uint32_t>(ntiles, 1));
+  }
+  // the bone bake needs the spatial order (bake_spatial_perm) as well
+  void setup_spatial(const std::vector<uint32_t>& p, cudaStream_t st) {
+    if (p.size() != nt) throw std::runtime_error("bake permutation size");
+    if (nt) perm.upload(p, st);
   }
   // spheres of the current triangles, then the bake of the listed entries
   void bake(const std::vector<BakeParams>& ps, const std::vector<uint32_t>& bones, uint32_t* atlas, cudaStream_t st) {
     if (ps.empty()) return;
+    if (nt && !perm.p) throw std::runtime_error("bone bake without its spatial order");
     if (nt) k_bone_tri_spheres<<<(nt + 255) / 256, 256, 0, st>>>(nt, tris.p, sph.p);
+    if (nt) k_bake_perm_spheres<<<(nt + 255) / 256, 256, 0, st>>>(nt, perm.p, sph.p, psph.p);
     if (ntiles) k_bone_tile_spheres<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, tile_first.p, tile_cnt.p, sph.p, tsph.p);
+    if (ntiles)
+      k_bone_tile_spheres<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, tile_first.p, tile_cnt.p, psph.p, stsph.p);
     params.upload(ps, st);
     param_bone.upload(bones, st);
     uint32_t res = 0;
     for (const auto& q : ps) res = std::max(res, q.res);
-    const uint32_t nblk = ((res + 7) / 8) * ((res + 7) / 8) * ((res + 3) / 4);
-    k_bone_bake<<<dim3(nblk, uint32_t(ps.size())), 256, 0, st>>>(params.p, tris.p, sph.p, tsph.p, tile_off.p,
-                                                                 param_bone.p, atlas);
+    const uint32_t nblk = ((res + 7) / 8) * ((res + 7) / 8) * ((res + 3) / 4);  // 8 x 8 x 4 regions
+    k_bone_bake<<<dim3(nblk, uint32_t(ps.size())), kBakeCol, 0, st>>>(params.p, tris.p, sph.p, tsph.p, perm.p, psph.p,
+                                                                 stsph.p, tile_off.p, param_bone.p, atlas);
   }
 };
 
@@ -3766,6 +3824,17 @@ tc_status tc_setup_dynamic_bone_sdf(tc_sim* s, uint32_t width, uint32_t height, 
     B.bake.nt = nt;
     B.bake.tris.alloc(nt);
     B.bake.setup_tiles(tcloth::make_bake_tiles(start, count), m.st);
+    {
+      // rest-pose centroids order the spatial tiles (culling only)
+      std::vector<float> cent(3 * size_t(nt));
+      for (uint32_t t = 0; t < nt; ++t) {
+        const uint32_t* q = tri_sources + 4 * size_t(t);
+        for (int a = 0; a < 3; ++a)
+          cent[3 * size_t(t) + a] = (rest_verts[size_t(rest_cols) * q[0] + a] + rest_verts[size_t(rest_cols) * q[1] + a] +
+                                     rest_verts[size_t(rest_cols) * q[2] + a]) / 3.0f;
+      }
+      B.bake.setup_spatial(tcloth::bake_spatial_perm(cent, start, count, nt), m.st);
+    }
     B.bind_inv.assign(bind_inv, bind_inv + 16 * size_t(n_bones));
     B.nv = nv; B.nb = n_bones; B.res = res;
     B.w = width; B.h = height; B.d = depth;
@@ -4094,6 +4163,16 @@ tc_status tc_bake_bone_sdf(const float* mesh_verts, uint32_t nv, const int32_t* 
     G.nt = uint32_t(all.size());
     G.tris.upload(all, st);
     G.setup_tiles(tcloth::make_bake_tiles(starts, counts), st);
+    {
+      std::vector<float> cent(3 * all.size());
+      for (size_t t = 0; t < all.size(); ++t) {
+        const tcloth::BakeTri& q = all[t];
+        cent[3 * t] = (q.p0w0.x + q.p1w1.x + q.p2w2.x) / 3.0f;
+        cent[3 * t + 1] = (q.p0w0.y + q.p1w1.y + q.p2w2.y) / 3.0f;
+        cent[3 * t + 2] = (q.p0w0.z + q.p1w1.z + q.p2w2.z) / 3.0f;
+      }
+      G.setup_spatial(tcloth::bake_spatial_perm(cent, starts, counts, G.nt), st);
+    }
     tcloth::DBuf<uint32_t> atlas;
     const size_t nvox = size_t(R->w) * R->h * R->d;
     atlas.alloc(nvox);

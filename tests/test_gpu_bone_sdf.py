@@ -246,3 +246,90 @@ def test_cloth_on_bone_sdf_matches_oracle(small_body, frame):
     assert np.array_equal(xg, xo)
     if frame == 0:  # arm horizontal at rest: part of the sheet lies on it
         assert int((xg[:, 1] > 1.44).sum()) > 20, "the cloth never met the bone SDF"
+
+
+def _grid_box(n, lo, hi):
+    """Closed box [lo, hi] with every face split into an n x n grid of quads
+    (two triangles each), vertices shared along the edges."""
+    lo, hi = np.asarray(lo, F), np.asarray(hi, F)
+    verts, index, tris = [], {}, []
+
+    def vid(p):
+        key = tuple(np.round(p, 7))
+        if key not in index:
+            index[key] = len(verts)
+            verts.append(p)
+        return index[key]
+
+    for ax in range(3):
+        u, v = (ax + 1) % 3, (ax + 2) % 3
+        for side in (0, 1):
+            for i in range(n):
+                for j in range(n):
+                    c = []
+                    for di, dj in ((0, 0), (1, 0), (1, 1), (0, 1)):
+                        p = np.empty(3, F)
+                        p[ax] = hi[ax] if side else lo[ax]
+                        p[u] = lo[u] + (hi[u] - lo[u]) * F((i + di) / n)
+                        p[v] = lo[v] + (hi[v] - lo[v]) * F((j + dj) / n)
+                        c.append(vid(p))
+                    a, b, cc, d = c
+                    tris += [[a, b, cc], [a, cc, d]] if side else [[a, cc, b], [a, d, cc]]
+    return np.asarray(verts, F), np.asarray(tris, np.int32)
+
+
+def _slab(ncol, length=0.1, width=0.002, height=0.01):
+    """Closed thin slab along x whose long faces are strips of ncol quads in x
+    order: for a voxel above a face the squared distances of successive
+    triangles fall by steps far below the tie tolerance's scale."""
+    xs = np.linspace(0.0, length, ncol + 1).astype(F)
+    corners = [(0.0, 0.0), (width, 0.0), (width, height), (0.0, height)]  # (y, z) around the section
+    verts = np.asarray([[x, y, z] for x in xs for (y, z) in corners], F)
+    tris = []
+    for i in range(ncol):
+        for k in range(4):
+            a, b = 4 * i + k, 4 * i + (k + 1) % 4
+            c, d = a + 4, b + 4
+            tris += [[a, b, d], [a, d, c]]
+    last = 4 * ncol
+    tris += [[0, 2, 1], [0, 3, 2], [last, last + 1, last + 2], [last, last + 2, last + 3]]
+    return verts, np.asarray(tris, np.int32)
+
+
+def _single_bone_bake(verts, tris, res):
+    W = np.ones((1, len(verts)), F)
+    bind = np.eye(4, dtype=F)[None]
+    bake = bake_bone_sdf_gpu(verts, tris, ["b"], list(W), bind, resolution=res)
+    _, dims, params, btris = _prepare_bake(verts, tris, W, bind, res)
+    tex = np.frombuffer(bake["texture_bytes"], np.uint32)
+    return tex, O.bone_bake(params, btris, dims)
+
+
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_bake_many_ties_matches_oracle(shuffle):
+    """Grid faces give many exactly equal distances (shared vertices and edges),
+    decided by the |projection| tie rule; a shuffled triangle order changes
+    which triangle wins, and the GPU must follow the order."""
+    verts, tris = _grid_box(10, (-0.05, -0.03, -0.02), (0.05, 0.03, 0.02))
+    if shuffle:
+        tris = tris[np.random.default_rng(5).permutation(len(tris))]
+    tex, ref = _single_bone_bake(verts, tris, 24)
+    assert np.array_equal(tex, ref), int((tex != ref).sum())
+
+
+def test_bake_slowly_descending_order_matches_oracle():
+    """Triangles ordered along the slab, so that above a face the distances
+    descend in steps well inside the tie tolerance's window: these voxels take
+    the kernel's full sequential scan."""
+    verts, tris = _slab(1000)
+    tex, ref = _single_bone_bake(verts, tris, 20)
+    assert np.array_equal(tex, ref), int((tex != ref).sum())
+
+
+def test_static_bake_default_resolution_matches_oracle(small_body):
+    b = small_body
+    bake = bake_bone_sdf_gpu(b["verts"], b["tris"], b["names"], list(b["weights"]), b["bind_inv"], resolution=40)
+    _, dims, params, tris = _prepare_bake(b["verts"], b["tris"], b["weights"], b["bind_inv"], 40)
+    tex = np.frombuffer(bake["texture_bytes"], np.uint32)
+    ref = O.bone_bake(params, tris, dims)
+    assert np.array_equal(tex, ref), int((tex != ref).sum())
