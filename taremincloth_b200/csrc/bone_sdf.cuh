@@ -278,7 +278,8 @@ __device__ __forceinline__ bool bake_far(const BakeState& s, V3 p, float4 sph) {
 // |projection| (eps(R) = 1e-7 max(1, R)).  The kernel gets the same state
 // without an ordered walk over every triangle:
 //  A. a first bound on m, the minimum squared distance, from the spatial
-//     tile (`perm`, tile spheres `stsph`) nearest to the brick;
+//     tile (`perm`, tile spheres `stsph`, sub-tiles of 8 with spheres
+//     `ssph8`) nearest to the brick;
 //  B. one order-free pass over the spatial tiles: (voxel, triangle) pairs
 //     that the sphere bound cannot rule out are queued and evaluated 32 at a
 //     time, lowering m by a shared-memory atomic min and listing every
@@ -343,7 +344,9 @@ __global__ void __launch_bounds__(kBakeCol, 3) k_bone_bake(const BakeParams* __r
                                                    const float4* __restrict__ sph, const float4* __restrict__ tsph,
                                                    const uint32_t* __restrict__ perm, const float4* __restrict__ psph,
                                                    const float4* __restrict__ stsph,
+                                                   const float4* __restrict__ ssph8,
                                                    const uint32_t* __restrict__ bone_tile_off,
+                                                   const uint32_t* __restrict__ bone_sub_off,
                                                    const uint32_t* __restrict__ param_bone,
                                                    uint32_t* __restrict__ atlas) {
   __shared__ uint32_t sh_list[kBakeList * kBakeCol];  // phase-B candidate indices, then the rounds' lists
@@ -366,6 +369,7 @@ __global__ void __launch_bounds__(kBakeCol, 3) k_bone_bake(const BakeParams* __r
   const V3 p = bake_voxel(P, fr, vx, vy, vz);
   const uint32_t t0 = P.tri_start, tn = P.tri_count;
   const uint32_t tile0 = bone_tile_off[param_bone[blockIdx.y]];
+  const uint32_t sub0 = bone_sub_off[param_bone[blockIdx.y]];
   const uint32_t ntile = (tn + 31u) / 32u;
   const uint32_t me = threadIdx.x;  // this voxel's slot
   uint32_t* lst = sh_list + me;
@@ -453,13 +457,30 @@ __global__ void __launch_bounds__(kBakeCol, 3) k_bone_bake(const BakeParams* __r
             ssph[lane] = __ldg(psph + t0 + k * 32u + lane);
             stri[lane] = __ldg(perm + t0 + k * 32u + lane);
           }
+          const uint32_t nsubk = (e + 7u) / 8u;
+          float4 s8 = make_float4(0.f, 0.f, 0.f, -1.f);
+          if (lane < nsubk) s8 = __ldg(ssph8 + sub0 + k * 4u + lane);
           __syncwarp();
           uint32_t mask = 0u;
+          float reach = 0.f;
           if (valid) {
             const float mv = __uint_as_float(sh_m[me]);
-            const float reach = sqrtf((mv + bake_window(mv)) * 1.0001f);
-            for (uint32_t q = 0; q < e; ++q)
-              if (!bake_far_r(reach, p, ssph[q])) mask |= 1u << q;
+            reach = sqrtf((mv + bake_window(mv)) * 1.0001f);
+          }
+          // sub-tiles of 8 that no voxel of the brick can use are skipped
+          uint32_t subs = 0u;
+          for (uint32_t u = 0; u < nsubk; ++u) {
+            const float4 su = make_float4(__shfl_sync(0xffffffffu, s8.x, u), __shfl_sync(0xffffffffu, s8.y, u),
+                                          __shfl_sync(0xffffffffu, s8.z, u), __shfl_sync(0xffffffffu, s8.w, u));
+            if (__any_sync(0xffffffffu, valid && !bake_far_r(reach, p, su))) subs |= 1u << u;
+          }
+          if (valid) {
+            for (uint32_t u = 0; u < nsubk; ++u) {
+              if (!((subs >> u) & 1u)) continue;
+              const uint32_t qe = min(e, 8u * u + 8u);
+              for (uint32_t q = 8u * u; q < qe; ++q)
+                if (!bake_far_r(reach, p, ssph[q])) mask |= 1u << q;
+            }
           }
           while (__any_sync(0xffffffffu, mask != 0u)) {
             const bool has = mask != 0u;

@@ -331,14 +331,15 @@ struct Mlp {
 struct BakeTiles {
   std::vector<uint32_t> first, cnt, bone_off;  // per tile; per bone: first tile
 };
-static BakeTiles make_bake_tiles(const std::vector<uint32_t>& start, const std::vector<uint32_t>& count) {
+static BakeTiles make_bake_tiles(const std::vector<uint32_t>& start, const std::vector<uint32_t>& count,
+                                 uint32_t size = 32) {
   BakeTiles t;
   t.bone_off.resize(start.size() + 1);
   for (size_t b = 0; b < start.size(); ++b) {
     t.bone_off[b] = uint32_t(t.first.size());
-    for (uint32_t k = 0; k < count[b]; k += 32) {
+    for (uint32_t k = 0; k < count[b]; k += size) {
       t.first.push_back(start[b] + k);
-      t.cnt.push_back(std::min(32u, count[b] - k));
+      t.cnt.push_back(std::min(size, count[b] - k));
     }
   }
   t.bone_off[start.size()] = uint32_t(t.first.size());
@@ -395,10 +396,10 @@ static std::vector<uint32_t> bake_spatial_perm(const std::vector<float>& cent, c
 // tiles over `perm` (`psph`, the triangle spheres in perm order; `stsph`).
 struct BakeGpu {
   DBuf<BakeTri> tris;
-  DBuf<float4> sph, tsph, psph, stsph;
-  DBuf<uint32_t> tile_first, tile_cnt, tile_off, param_bone, perm;
+  DBuf<float4> sph, tsph, psph, stsph, ssph;
+  DBuf<uint32_t> tile_first, tile_cnt, tile_off, param_bone, perm, sub_first, sub_cnt, sub_off;
   DBuf<BakeParams> params;
-  uint32_t nt = 0, ntiles = 0;
+  uint32_t nt = 0, ntiles = 0, nsub = 0;
   void setup_tiles(const BakeTiles& t, cudaStream_t st) {
     ntiles = uint32_t(t.first.size());
     tile_first.upload(t.first, st);
@@ -409,10 +410,18 @@ struct BakeGpu {
     psph.alloc(std::max<uint32_t>(nt, 1));
     stsph.alloc(std::max<uint32_t>(ntiles, 1));
   }
-  // the bone bake needs the spatial order (bake_spatial_perm) as well
-  void setup_spatial(const std::vector<uint32_t>& p, cudaStream_t st) {
+  // the bone bake needs the spatial order (bake_spatial_perm) as well, and
+  // sub-tiles of 8 positions (`sub`, spheres `ssph`) within its spatial tiles
+  void setup_spatial(const std::vector<uint32_t>& p, const std::vector<uint32_t>& start,
+                     const std::vector<uint32_t>& count, cudaStream_t st) {
     if (p.size() != nt) throw std::runtime_error("bake permutation size");
     if (nt) perm.upload(p, st);
+    const BakeTiles sub = make_bake_tiles(start, count, 8);
+    nsub = uint32_t(sub.first.size());
+    sub_first.upload(sub.first, st);
+    sub_cnt.upload(sub.cnt, st);
+    sub_off.upload(sub.bone_off, st);
+    ssph.alloc(std::max<uint32_t>(nsub, 1));
   }
   // spheres of the current triangles, then the bake of the listed entries
   void bake(const std::vector<BakeParams>& ps, const std::vector<uint32_t>& bones, uint32_t* atlas, cudaStream_t st) {
@@ -423,13 +432,15 @@ struct BakeGpu {
     if (ntiles) k_bone_tile_spheres<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, tile_first.p, tile_cnt.p, sph.p, tsph.p);
     if (ntiles)
       k_bone_tile_spheres<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, tile_first.p, tile_cnt.p, psph.p, stsph.p);
+    if (nsub) k_bone_tile_spheres<<<(nsub + 127) / 128, 128, 0, st>>>(nsub, sub_first.p, sub_cnt.p, psph.p, ssph.p);
     params.upload(ps, st);
     param_bone.upload(bones, st);
     uint32_t res = 0;
     for (const auto& q : ps) res = std::max(res, q.res);
     const uint32_t nblk = ((res + 7) / 8) * ((res + 7) / 8) * ((res + 3) / 4);  // 8 x 8 x 4 regions
     k_bone_bake<<<dim3(nblk, uint32_t(ps.size())), kBakeCol, 0, st>>>(params.p, tris.p, sph.p, tsph.p, perm.p, psph.p,
-                                                                 stsph.p, tile_off.p, param_bone.p, atlas);
+                                                                 stsph.p, ssph.p, tile_off.p, sub_off.p,
+                                                                 param_bone.p, atlas);
   }
 };
 
@@ -3833,7 +3844,7 @@ tc_status tc_setup_dynamic_bone_sdf(tc_sim* s, uint32_t width, uint32_t height, 
           cent[3 * size_t(t) + a] = (rest_verts[size_t(rest_cols) * q[0] + a] + rest_verts[size_t(rest_cols) * q[1] + a] +
                                      rest_verts[size_t(rest_cols) * q[2] + a]) / 3.0f;
       }
-      B.bake.setup_spatial(tcloth::bake_spatial_perm(cent, start, count, nt), m.st);
+      B.bake.setup_spatial(tcloth::bake_spatial_perm(cent, start, count, nt), start, count, m.st);
     }
     B.bind_inv.assign(bind_inv, bind_inv + 16 * size_t(n_bones));
     B.nv = nv; B.nb = n_bones; B.res = res;
@@ -4171,7 +4182,7 @@ tc_status tc_bake_bone_sdf(const float* mesh_verts, uint32_t nv, const int32_t* 
         cent[3 * t + 1] = (q.p0w0.y + q.p1w1.y + q.p2w2.y) / 3.0f;
         cent[3 * t + 2] = (q.p0w0.z + q.p1w1.z + q.p2w2.z) / 3.0f;
       }
-      G.setup_spatial(tcloth::bake_spatial_perm(cent, starts, counts, G.nt), st);
+      G.setup_spatial(tcloth::bake_spatial_perm(cent, starts, counts, G.nt), starts, counts, st);
     }
     tcloth::DBuf<uint32_t> atlas;
     const size_t nvox = size_t(R->w) * R->h * R->d;
