@@ -214,7 +214,9 @@ tc_status tc_add_capsule_collider(tc_sim *s, const float a[3], const float b[3],
 tc_status tc_add_plane_collider(tc_sim *s, const float point[3], const float normal[3], float friction,
                                 float restitution);
 /* triangles: T x 3 x 3 floats; attributes (nullable): T x 4 (friction,
- * thickness, restitution, flags) */
+ * thickness, restitution, flags).  The floats are copied into pinned host
+ * memory before the call returns; the Morton order and the culling spheres
+ * are computed on the device ahead of the next step. */
 tc_status tc_set_mesh_collider_triangles(tc_sim *s, const float *triangles, uint32_t T, float friction,
                                          float thickness, float restitution, int single_sided, const float *attributes);
 tc_status tc_clear_colliders(tc_sim *s);

@@ -8,6 +8,7 @@
 // defaults: decoupled colliders (coupled when the auto-coupling test fires),
 // self-collision once per substep after the final pin pass.
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <array>
@@ -29,6 +30,7 @@
 #include "mesh.hpp"
 #include "selfcol_kernels.cuh"
 #include "paircache_kernels.cuh"
+#include "collider_prep.cuh"
 #include "solver_kernels.cuh"
 #include "warmstart.cuh"
 
@@ -677,7 +679,7 @@ struct Sim {
     std::vector<uint32_t> cs, srt;
     ce_cell = m.cell;
     const size_t n_before = cedges_h.size();
-    build_collider_edges(tris_h, ce_cell, cedges_h, cs, srt);
+    build_collider_edges(host_tris(), ce_cell, cedges_h, cs, srt);
     const void* before[3] = {cedges.p, ce_cs.p, ce_srt.p};
     cedges.upload(cedges_h, st);
     ce_cs.upload(cs, st);
@@ -700,6 +702,18 @@ struct Sim {
   DBuf<Prim> prims;
   DBuf<MeshTri> tris;
   DBuf<float4> bounds, cl16, cl256, cl4096;
+  // device-side upload of the mesh collider (collider_prep.cuh): input floats
+  // through a pinned staging buffer, packed triangles, Morton keys, sort scratch
+  uint32_t ntris = 0;         // triangles in `tris`
+  bool tris_h_valid = true;   // tris_h mirrors `tris` (refreshed when a host step needs it)
+  DBuf<float> col_in, col_box;
+  DBuf<MeshTri> col_raw;
+  DBuf<uint32_t> col_code, col_code2, col_idx, col_idx2;
+  DBuf<unsigned char> col_tmp;
+  float* h_col = nullptr;
+  size_t h_col_cap = 0;       // floats the staging buffer holds
+  cudaEvent_t col_ev = nullptr;
+  bool col_ev_used = false;   // col_ev marks the last copy out of h_col
   // batched instances (empty for a single cloth)
   std::vector<uint32_t> inst_vert_off;  // n_instances + 1
   // cluster solver: bins of whole instances, one thread-block cluster each
@@ -902,6 +916,11 @@ struct Sim {
     if (h_err) cudaFreeHost(h_err);
     if (h_fb) cudaFreeHost(h_fb);
     if (h_pos3) cudaFreeHost(h_pos3);
+    if (col_ev) {
+      if (col_ev_used) cudaEventSynchronize(col_ev);
+      cudaEventDestroy(col_ev);
+    }
+    if (h_col) cudaFreeHost(h_col);
   }
 
   void mark() { graph_dirty = true; }
@@ -1173,101 +1192,69 @@ struct Sim {
     mark();
   }
   uint32_t graph_ntris = UINT32_MAX;
+  // The triangles go to the device as floats and are packed, Morton-sorted and
+  // bounded there (collider_prep.cuh, simulation/mod.rs:2613-2670), in the
+  // stream ahead of the next frame; the host only copies them into pinned
+  // memory, after the previous upload's copy out of it has finished.
   void set_mesh(const float* t9, uint32_t T, float fric, float thick, float rest, bool single, const float* attr) {
-    std::vector<MeshTri> v(T);
-    for (uint32_t t = 0; t < T; ++t) {
-      const float* q = t9 + 9 * size_t(t);
-      float f = fric, th = thick, r = rest;
-      uint32_t flags = single ? 1u : 0u;
-      if (attr) {
-        f = attr[4 * t]; th = attr[4 * t + 1]; r = attr[4 * t + 2];
-        float fl = std::round(attr[4 * t + 3]);
-        flags = fl > 0.f ? (fl >= 4294967295.f ? UINT32_MAX : uint32_t(fl)) : 0u;
-      }
-      float fb;
-      std::memcpy(&fb, &flags, 4);
-      v[t] = MeshTri{make_float4(q[0], q[1], q[2], f), make_float4(q[3], q[4], q[5], th),
-                     make_float4(q[6], q[7], q[8], r), make_float4(fb, 0.f, 0.f, 0.f)};
-    }
-    tris_h.swap(v);
-    upload_tris();
-  }
-  // Morton sort of centroids (stable), bounding spheres
-  // (simulation/mod.rs:2613-2670) and the two conservative culling levels.
-  void upload_tris() {
-    const uint32_t T = uint32_t(tris_h.size());
+    tris_h.clear();
+    tris_h_valid = T == 0;
+    ntris = T;
     if (T == 0) { mark(); graph_ntris = 0; ce_stale = true; return; }
-    auto cen = [](const MeshTri& t, int a) {
-      const float* p0 = &t.p0f.x; const float* p1 = &t.p1t.x; const float* p2 = &t.p2r.x;
-      return (p0[a] + p1[a] + p2[a]) / 3.0f;
-    };
-    float bmin[3] = {3.4028235e38f, 3.4028235e38f, 3.4028235e38f}, bmax[3] = {-3.4028235e38f, -3.4028235e38f, -3.4028235e38f};
-    for (const auto& t : tris_h)
-      for (int a = 0; a < 3; ++a) { bmin[a] = std::fmin(bmin[a], cen(t, a)); bmax[a] = std::fmax(bmax[a], cen(t, a)); }
-    float inv[3];
-    for (int a = 0; a < 3; ++a) inv[a] = 1.f / std::fmax(bmax[a] - bmin[a], 1e-5f);
-    // stable order by code: LSD radix sort, four 8-bit passes over indices
-    // that start ascending (the order of a sort by (code, index))
-    std::vector<uint32_t> code(T), ord(T), tmp(T);
-    for (uint32_t t = 0; t < T; ++t) {
-      code[t] = morton3(cen(tris_h[t], 0), cen(tris_h[t], 1), cen(tris_h[t], 2), bmin, inv);
-      ord[t] = t;
+    const size_t nf = size_t(T) * (attr ? 13 : 9);
+    if (!col_ev) TC_CK(cudaEventCreateWithFlags(&col_ev, cudaEventDisableTiming));
+    if (col_ev_used) TC_CK(cudaEventSynchronize(col_ev));
+    if (h_col_cap < nf) {
+      if (h_col) TC_CK(cudaFreeHost(h_col));
+      h_col = nullptr;
+      h_col_cap = 0;
+      TC_CK(cudaMallocHost(&h_col, nf * sizeof(float)));
+      h_col_cap = nf;
     }
-    for (int sh = 0; sh < 32; sh += 8) {
-      uint32_t hist[257] = {0};
-      for (uint32_t t = 0; t < T; ++t) ++hist[((code[ord[t]] >> sh) & 255u) + 1];
-      for (int b = 0; b < 256; ++b) hist[b + 1] += hist[b];
-      for (uint32_t t = 0; t < T; ++t) tmp[hist[(code[ord[t]] >> sh) & 255u]++] = ord[t];
-      ord.swap(tmp);
-    }
-    std::vector<MeshTri> sorted(T);
-    for (uint32_t t = 0; t < T; ++t) sorted[t] = tris_h[ord[t]];
-    tris_h.swap(sorted);
-    std::vector<float4> bd(T);
-    for (uint32_t t = 0; t < T; ++t) {
-      const MeshTri& q = tris_h[t];
-      float cx = cen(q, 0), cy = cen(q, 1), cz = cen(q, 2);
-      auto d2 = [&](const float4& p) {
-        float ax = p.x - cx, ay = p.y - cy, az = p.z - cz;
-        return ax * ax + ay * ay + az * az;
-      };
-      float r = std::sqrt(std::fmax(std::fmax(d2(q.p0f), d2(q.p1t)), d2(q.p2r))) + q.p1t.w;
-      bd[t] = make_float4(cx, cy, cz, r);
-    }
-    auto group = [&](uint32_t b, uint32_t e) {
-      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-      for (uint32_t t = b; t < e; ++t) {
-        double R = 1.5 * double(bd[t].w);
-        const double c[3] = {bd[t].x, bd[t].y, bd[t].z};
-        for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], c[a] - R); hi[a] = std::max(hi[a], c[a] + R); }
-      }
-      double C[3] = {(lo[0] + hi[0]) * 0.5, (lo[1] + hi[1]) * 0.5, (lo[2] + hi[2]) * 0.5};
-      double Rg = 0.0;
-      for (uint32_t t = b; t < e; ++t) {
-        double dx = bd[t].x - C[0], dy = bd[t].y - C[1], dz = bd[t].z - C[2];
-        Rg = std::max(Rg, std::sqrt(dx * dx + dy * dy + dz * dz) + 1.5 * double(bd[t].w));
-      }
-      Rg = Rg * (1.0 + 1e-5) + 1e-7;
-      return make_float4(float(C[0]), float(C[1]), float(C[2]), float(Rg));
-    };
+    std::memcpy(h_col, t9, size_t(T) * 9 * sizeof(float));
+    if (attr) std::memcpy(h_col + size_t(T) * 9, attr, size_t(T) * 4 * sizeof(float));
+    col_in.alloc(nf);
+    TC_CK(cudaMemcpyAsync(col_in.p, h_col, nf * sizeof(float), cudaMemcpyHostToDevice, st));
+    TC_CK(cudaEventRecord(col_ev, st));
+    col_ev_used = true;
     const uint32_t n16 = (T + 15) / 16, n256 = (T + 255) / 256, n4096 = (T + 4095) / 4096;
-    std::vector<float4> g16(n16), g256(n256), g4096(n4096);
-    for (uint32_t g = 0; g < n16; ++g) g16[g] = group(g * 16, std::min(T, g * 16 + 16));
-    for (uint32_t g = 0; g < n256; ++g) g256[g] = group(g * 256, std::min(T, g * 256 + 256));
-    for (uint32_t g = 0; g < n4096; ++g) g4096[g] = group(g * 4096, std::min(T, g * 4096 + 4096));
     const void* before[5] = {tris.p, bounds.p, cl16.p, cl256.p, cl4096.p};
-    tris.upload(tris_h, st);
-    bounds.upload(bd, st);
-    cl16.upload(g16, st);
-    cl256.upload(g256, st);
-    cl4096.upload(g4096, st);
-    TC_CK(cudaStreamSynchronize(st));
+    col_raw.alloc(T);
+    col_box.alloc(6);
+    col_code.alloc(T); col_code2.alloc(T); col_idx.alloc(T); col_idx2.alloc(T);
+    tris.alloc(T); bounds.alloc(T); cl16.alloc(n16); cl256.alloc(n256); cl4096.alloc(n4096);
+    k_col_pack<<<grid(T, 256), 256, 0, st>>>(T, col_in.p, attr ? col_in.p + size_t(T) * 9 : nullptr, fric, thick,
+                                             rest, single ? 1u : 0u, col_raw.p);
+    k_col_bounds<<<1, 1024, 0, st>>>(T, col_raw.p, col_box.p);
+    k_col_codes<<<grid(T, 256), 256, 0, st>>>(T, col_raw.p, col_box.p, col_code.p, col_idx.p);
+    // stable LSD radix sort of the 30-bit codes: equal codes keep index order
+    size_t tmp_bytes = 0;
+    TC_CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, col_code.p, col_code2.p, col_idx.p, col_idx2.p, int(T),
+                                          0, 30, st));
+    col_tmp.alloc(std::max<size_t>(tmp_bytes, 1));
+    TC_CK(cub::DeviceRadixSort::SortPairs(col_tmp.p, tmp_bytes, col_code.p, col_code2.p, col_idx.p, col_idx2.p,
+                                          int(T), 0, 30, st));
+    k_col_gather<<<grid(T, 256), 256, 0, st>>>(T, col_raw.p, col_idx2.p, tris.p, bounds.p);
+    k_col_groups<<<n16, 256, 0, st>>>(T, 16, bounds.p, cl16.p);
+    k_col_groups<<<n256, 256, 0, st>>>(T, 256, bounds.p, cl256.p);
+    k_col_groups<<<n4096, 256, 0, st>>>(T, 4096, bounds.p, cl4096.p);
+    TC_CK(cudaGetLastError());
     // the recorded frame only holds pointers and the triangle count: new
     // contents of the same size replay without re-recording
     const void* after[5] = {tris.p, bounds.p, cl16.p, cl256.p, cl4096.p};
     if (T != graph_ntris || std::memcmp(before, after, sizeof before) != 0) mark();
     graph_ntris = T;
     ce_stale = true;
+  }
+  // the sorted triangles on the host, for the host-side collider-edge build
+  const std::vector<MeshTri>& host_tris() {
+    if (!tris_h_valid) {
+      tris_h.resize(ntris);
+      if (ntris) TC_CK(cudaMemcpyAsync(tris_h.data(), tris.p, size_t(ntris) * sizeof(MeshTri), cudaMemcpyDeviceToHost, st));
+      TC_CK(cudaStreamSynchronize(st));
+      tris_h_valid = true;
+    }
+    return tris_h;
   }
 
   // ---- pins
@@ -1484,7 +1471,7 @@ struct Sim {
   ColliderArgs collider_args() {
     ColliderArgs c;
     c.prims = prims.p; c.nprims = uint32_t(prims_h.size());
-    c.tris = tris.p; c.bounds = bounds.p; c.cl16 = cl16.p; c.cl256 = cl256.p; c.cl4096 = cl4096.p; c.ntris = uint32_t(tris_h.size());
+    c.tris = tris.p; c.bounds = bounds.p; c.cl16 = cl16.p; c.cl256 = cl256.p; c.cl4096 = cl4096.p; c.ntris = ntris;
     c.recovery = recovery;
     c.vinst = inst_prims_h.empty() ? nullptr : vinst.p;
     c.inst_prims = inst_prims_h.empty() ? nullptr : inst_prims.p;
@@ -1493,7 +1480,7 @@ struct Sim {
                          bone.w, bone.h, bone.d};
     return c;
   }
-  bool has_colliders() const { return !prims_h.empty() || !tris_h.empty() || bone.enabled; }
+  bool has_colliders() const { return !prims_h.empty() || ntris != 0 || bone.enabled; }
 
   // ---- bone SDF
   // update_bone_transforms (simulation/mod.rs:1865-1935): store the
@@ -3236,6 +3223,8 @@ tc_status tc_clear_colliders(tc_sim* s) {
     Sim& m = S(s);
     m.prims_h.clear();
     m.tris_h.clear();
+    m.tris_h_valid = true;
+    m.ntris = 0;
     m.graph_ntris = 0;
     m.ce_stale = true;  // no triangles: no collider edges (mod.rs:2731-2736)
     m.mark();
