@@ -1201,6 +1201,7 @@ struct Sim {
     tris_h_valid = T == 0;
     ntris = T;
     if (T == 0) { mark(); graph_ntris = 0; ce_stale = true; return; }
+    if (T > 0x7FFFFFFFu) throw TcError(TC_ERR_INVALID, "too many collider triangles");  // the device sort counts in int
     const size_t nf = size_t(T) * (attr ? 13 : 9);
     if (!col_ev) TC_CK(cudaEventCreateWithFlags(&col_ev, cudaEventDisableTiming));
     if (col_ev_used) TC_CK(cudaEventSynchronize(col_ev));
