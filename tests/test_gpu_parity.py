@@ -73,6 +73,22 @@ def test_config2_small_with_mesh_and_self_collision(oracle_lib):
     assert worst[0] <= 1e-5 and worst.max() <= 1e-4, (worst, same)
 
 
+def test_config2_small_with_per_triangle_collider_attributes(oracle_lib):
+    """Per-triangle friction, thickness, restitution and one-sided flags
+    (set_mesh_collider_triangles(attributes=...)) on the CUDA path and the oracle."""
+    sc = scenes.config2(n=40, subdiv=3)
+    g = scenes.build(ClothSimulator, sc)
+    o = scenes.build(oracle_lib.OracleSim, sc)
+    tris = np.asarray(sc["mesh"]["triangles"], np.float32)
+    rng = np.random.default_rng(11)
+    attr = np.stack([rng.uniform(0.0, 0.5, len(tris)), rng.uniform(0.005, 0.015, len(tris)),
+                     np.zeros(len(tris)), rng.integers(0, 2, len(tris))], 1).astype(np.float32)
+    for s in (g, o):
+        s.set_mesh_collider_triangles(tris, friction=0.3, thickness=0.01, single_sided=True, attributes=attr)
+    worst, same = compare_frames(g, o, 8, sc["dt"], sc["substeps"], extent(sc["positions"]))
+    assert worst[0] <= 1e-5 and worst.max() <= 1e-4, (worst, same)
+
+
 def test_config2_full_one_substep(oracle_lib):
     """Full-size configuration, one substep (the oracle takes ~30 s), with
     the direct pass's V-T and E-E pair lists bit-exact."""
