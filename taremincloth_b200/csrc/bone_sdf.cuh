@@ -280,9 +280,10 @@ __device__ __forceinline__ bool bake_far(const BakeState& s, V3 p, float4 sph) {
 //  A. a first bound on m, the minimum squared distance, from the spatial
 //     tile (`perm`, tile spheres `stsph`, sub-tiles of 8 with spheres
 //     `ssph8`) nearest to the brick;
-//  B. one order-free pass over the spatial tiles: (voxel, triangle) pairs
-//     that the sphere bound cannot rule out are queued and evaluated 32 at a
-//     time, lowering m by a shared-memory atomic min and listing every
+//  B. one order-free pass over the spatial tiles, in rings of growing
+//     distance from the brick: (voxel, triangle) pairs that the sphere bounds
+//     (tile, sub-tile, triangle) cannot rule out are queued and evaluated 32
+//     at a time, lowering m by a shared-memory atomic min and listing every
 //     triangle with d <= m + W (W = 4e-6 max(1, m)) for its voxel;
 //  C. per voxel, the listed window G = {d <= T}, T = m + W, sorted by
 //     triangle index, runs through the rule from its first "hard record": a
